@@ -1,0 +1,289 @@
+"""Benchmark: grid-point substage updates per second (GPSU/s) of the plain
+RHS + RK path on the 256^3 periodic H2/air ignition-kernel workload
+(mixture-averaged transport, 21-step mechanism, FP64).
+
+A "step" is one RK4(3)5 time step = 5 substages over the whole box, so
+GPSU per step = 5 * nx*ny*nz. Inputs are synthetic (seeded turbulence and
+hot kernels, see cases.py). The state (1.9 GB for 256^3 H2) is far larger
+than L2, so no cache flush is needed between timed steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N>1 runs N independent replicas (one box per GPU, no inter-GPU exchange:
+the path does not shard in this build), value = sum over ranks.
+--impl reference times the CPU restatement of the reference (the oracle:
+the Fortran reference cannot be compiled here) with all host threads on a
+bounded 64^3 sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "senga-versiona_b200"))
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def peaks():
+    try:
+        with open(PEAKS) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def compulsory_bytes_per_gpsu(nspec):
+    # read+write of the S and U registers and of T (Newton seed): 8*(4*Nc+2)
+    return 8 * (4 * (5 + nspec) + 2)
+
+
+def kernel_bytes_per_point(nspec, adaptive=False):
+    """Algorithmic bytes per interior point of each kernel family: distinct
+    fields read + written, 8 B each (the interval index 4 B); stencil halo
+    re-reads count zero."""
+    S, nc = nspec, 5 + nspec
+    # reads U (nc), T, ITNDEX; writes T, ITNDEX, p, lambda, lambda/cp, mu,
+    # rho*D_k, h_k, h_mix, wdot_k, u, v, w, E, Y_k
+    thermo = 8 * (nc + 1) + 4 + 8 * (10 + 4 * S) + 4
+    flow = 8 * (4 + 3 + 1 + 1 + 1 + 1 + 1) + 8 * (5 + 1)
+    species_a = 8 * (3 + 1 + 1 + 4 * S) + 8 * (S + 3 + 1 + 1)
+    species_b = 8 * (3 + 1 + 5 + 1 + 2 * S + nc) + 8 * (2 * nc) + (16 * nc if adaptive else 0)
+    return {"thermo": thermo, "flow": flow, "species_a": species_a, "species_b_rk": species_b}
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.fh.flush()
+        self.fh.seek(0)
+        rows = [r.split(",") for r in self.fh.read().strip().splitlines() if r.strip()]
+        os.unlink(self.fh.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].strip().lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(steps, warmup, n=64):
+    """Times the oracle (CPU restatement of the reference) on a bounded n^3
+    sample of the workload with all host threads; returns (GPSU/s, info)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cases
+    from oracle import Oracle
+
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    c = cases.make_case("h2_kernels", n=n, seed=1)
+    o = Oracle(c["shape"], c["lengths"], c["chem"], c["diff"], c["dt"])
+    o.upload(c["fields"], c["T"], c["itn"])
+    for _ in range(warmup):
+        o.step(1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(1)
+    dt = time.perf_counter() - t0
+    pts = n ** 3
+    return pts * 5 * steps / dt, {"cores": int(os.environ["OMP_NUM_THREADS"]),
+                                   "sample": f"{n}^3 periodic H2 kernels, {steps} RK step(s), oracle (C++ port)",
+                                   "seconds": dt}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="grid extent (cubic); 256 is the named workload")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    metric, unit = "grid-point substage updates/s", "GPSU/s"
+    workload = {"workload": f"h2_kernels_{args.n}^3", "grid": [args.n] * 3, "mechanism": "H2/air 9 sp 21 steps",
+                "transport": "mixture-averaged", "boundaries": "triply periodic", "substages_per_step": 5,
+                "parallelism": f"replicas x{args.gpus}", "l2": "inputs larger than L2 (no flush needed)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        n = 64
+        v, info = cpu_reference_sample(max(args.steps, 1), args.warmup if args.warmup < 2 else 1, n=n)
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * info["seconds"] / max(args.steps, 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": workload,
+                "cpu_baseline": {"value": v, "unit": unit, "cores": info["cores"], "kind": "port",
+                                 "sample": info["sample"]},
+                "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    import cases
+    import senga
+
+    c = cases.make_case("h2_kernels", n=args.n, seed=1 + rank)
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(c["diff"], chem)
+    box = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"], device=local)
+    box.upload(c["fields"], c["T"], c["itn"])
+    npts = c["shape"][0] * c["shape"][1] * c["shape"][2]
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # warm-up (graph capture happens here)
+    box.step(max(args.warmup, 3), graph=True)
+    box.sync()
+    # per-kernel profile of one step (device events, after warm-up)
+    prof, launches_per_step = box.profile_step()
+    box.sync()
+
+    stream = torch.cuda.ExternalStream(box.stream, device=local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    time.sleep(0.4)
+    ev0.record(stream)
+    box.step(args.steps, graph=True)
+    ev1.record(stream)
+    box.sync()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    status = box.status()
+    gpsu = npts * 5 * args.steps * world / (ms / 1e3)
+
+    # end-to-end through the host C ABI: per step, upload the state from pinned
+    # host memory, advance one RK step, download the state.
+    nc = 5 + chem.nspec
+    pin_f = torch.empty((nc,) + box.shape, dtype=torch.float64, pin_memory=True).numpy()
+    pin_t = torch.empty(box.shape, dtype=torch.float64, pin_memory=True).numpy()
+    pin_i = torch.empty(box.shape, dtype=torch.int32, pin_memory=True).numpy()
+    f0, t0_, i0 = box.download()
+    pin_f[...] = f0
+    pin_t[...] = t0_
+    pin_i[...] = i0
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    t_e0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        box.upload(pin_f, pin_t, pin_i)
+        box.step(1, graph=True)
+        f1, t1_, i1 = box.download()
+    t_e = time.perf_counter() - t_e0
+    if world > 1:
+        t = torch.tensor([t_e], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_e = float(t.item())
+    state_bytes = nc * npts * 8 + npts * 8 + npts * 4
+    e2e = {"value": npts * 5 * e2e_steps * world / t_e, "unit": unit, "h2d_bytes_per_step": state_bytes,
+           "d2h_bytes_per_step": state_bytes,
+           "call": "senga_upload_state_host + senga_step_graph(1) + senga_download_state_host per step"}
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    hbm, peak_kind = peaks()
+    kb = kernel_bytes_per_point(chem.nspec)
+    kern = {}
+    tot = sum(prof.values())
+    for k, t_ms in prof.items():
+        launch_ms = t_ms / 5.0
+        ach = kb[k] * npts / (launch_ms / 1e3) / 1e9
+        kern[k] = {"ms_per_launch": launch_ms, "share": t_ms / tot, "alg_bytes_per_point": kb[k],
+                   "achieved_gbs": ach, "frac_hbm": ach / hbm}
+    stencil = max(("flow", "species_a", "species_b_rk"), key=lambda k: prof[k])
+    dom = max(prof, key=prof.get)
+    rk = kern[stencil]
+    step_ms = ms / args.steps
+    whole = gpsu / world * compulsory_bytes_per_gpsu(chem.nspec) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        v, info = cpu_reference_sample(1, 0, n=48)
+        cpu = {"value": v, "unit": unit, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
+    line = {
+        "metric": metric, "value": gpsu, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload,
+        "roofline": {"bound": "hbm", "kernel": stencil, "achieved": rk["achieved_gbs"], "peak": hbm,
+                     "unit": "GB/s", "frac": rk["frac_hbm"], "traffic": None, "peak_kind": peak_kind},
+        "dominant_kernel": dom,
+        "kernels": kern,
+        "whole_step_hbm_frac": whole / hbm,
+        "compulsory_bytes_per_gpsu": compulsory_bytes_per_gpsu(chem.nspec),
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks,
+        "status_word": status,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

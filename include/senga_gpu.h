@@ -1,0 +1,185 @@
+/*
+ * senga_gpu.h — C ABI of the B200 (sm_100a) implementation of SENGA2's
+ * per-substage right-hand side and low-storage Runge-Kutta advance.
+ *
+ * Conventions (match the reference's Fortran call surfaces):
+ *   - every entry point returns int: 0 = ok, > 0 = error code (see
+ *     senga_status below); nothing aborts, no C++ exception crosses the ABI;
+ *   - arrays are Fortran column-major (x fastest); an "interior" array has
+ *     nx*ny*nz elements (the reference's FDERIV/STD arrays), a species array
+ *     is (nx,ny,nz,nspec) with species slowest (the reference's YRUN layout);
+ *   - "_host" entry points take host pointers and copy inside the call; the
+ *     others take device pointers and run asynchronously on the context's
+ *     stream (synchronise with senga_sync);
+ *   - the chemistry/transport tables use the reference's COMMON/CHEMIC and
+ *     COMMON/DIFFUS array shapes (src/com_senga2.h:121-214), so a Fortran host
+ *     can pass its COMMON blocks field by field.
+ */
+#ifndef SENGA_GPU_H
+#define SENGA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Table dimensions: src/com_senga2.h:80-100,189 */
+#define SENGA_NSPCMX 9
+#define SENGA_NSTPMX 21
+#define SENGA_NTINMX 2
+#define SENGA_NCOFMX 7
+#define SENGA_NSSMAX 10
+#define SENGA_NBDYMX 10
+#define SENGA_NLLMAX 10
+#define SENGA_NDCFMX 4
+
+/* End conditions per face: src/com_senga2.h (NOBC/NBOUND/NPERI) */
+#define SENGA_NOBC 0
+#define SENGA_NBOUND 1
+#define SENGA_NPERI 2
+
+enum senga_status {
+  SENGA_OK = 0,
+  SENGA_ERR_ARG = 1,        /* bad argument / size                         */
+  SENGA_ERR_CUDA = 2,       /* CUDA runtime error                          */
+  SENGA_ERR_IO = 3,         /* cannot read an input file                   */
+  SENGA_ERR_TEMPER = 4,     /* Newton T inversion did not converge         */
+  SENGA_ERR_UNSUPPORTED = 5,/* option not built                            */
+  SENGA_ERR_NONFINITE = 6,  /* NaN/Inf detected in the state               */
+  SENGA_ERR_NOMEM = 7       /* device memory exhausted                     */
+};
+
+/* COMMON/CHEMIC (src/com_senga2.h:121-178) after CHEMIN's derived-quantity
+ * pass (src/chemin.f:822-983). C index order [a][b][c] == Fortran (c,b,a). */
+typedef struct senga_chem {
+  int nspec, nstep, nbody, ngibb, nlind, ntroe, nsrif;
+  int ntint[SENGA_NSPCMX];
+  int ncofcp[SENGA_NSPCMX][SENGA_NTINMX], ncpoly[SENGA_NSPCMX][SENGA_NTINMX];
+  int ncpom1[SENGA_NSPCMX][SENGA_NTINMX], ncenth[SENGA_NSPCMX][SENGA_NTINMX];
+  int ncenpy[SENGA_NSPCMX][SENGA_NTINMX];
+  int nsslen[SENGA_NSTPMX], nrslen[SENGA_NSTPMX], npslen[SENGA_NSTPMX];
+  int nrclen[SENGA_NSTPMX], npclen[SENGA_NSTPMX];
+  int nsspec[SENGA_NSTPMX][SENGA_NSSMAX], nrspec[SENGA_NSTPMX][SENGA_NSSMAX];
+  int npspec[SENGA_NSTPMX][SENGA_NSSMAX], nrcpec[SENGA_NSTPMX][SENGA_NSSMAX];
+  int npcpec[SENGA_NSTPMX][SENGA_NSSMAX];
+  int mblist[SENGA_NSTPMX], mglist[SENGA_NSTPMX], mllist[SENGA_NSTPMX];
+  int mtlist[SENGA_NSTPMX], mslist[SENGA_NSTPMX];
+  double prefgb, alamda;
+  double tintlo[SENGA_NSPCMX][SENGA_NTINMX], tinthi[SENGA_NSPCMX][SENGA_NTINMX];
+  double amolcp[SENGA_NSPCMX][SENGA_NTINMX][SENGA_NCOFMX];
+  double amolgb[SENGA_NSPCMX][SENGA_NTINMX][SENGA_NCOFMX];
+  double amascp[SENGA_NSPCMX][SENGA_NTINMX][SENGA_NCOFMX];
+  double amasct[SENGA_NSPCMX][SENGA_NTINMX][SENGA_NCOFMX];
+  double amasch[SENGA_NSPCMX][SENGA_NTINMX][SENGA_NCOFMX];
+  double amascs[SENGA_NSPCMX][SENGA_NTINMX][SENGA_NCOFMX];
+  double rparam[SENGA_NSTPMX][3];
+  double rclind[SENGA_NLLMAX][4], rctroe[SENGA_NLLMAX][12], rcsrif[SENGA_NLLMAX][8];
+  double diffmu[SENGA_NSTPMX][SENGA_NSSMAX], diffmw[SENGA_NSTPMX][SENGA_NSSMAX];
+  double crspec[SENGA_NSTPMX][SENGA_NSSMAX], cpspec[SENGA_NSTPMX][SENGA_NSSMAX];
+  double effy3b[SENGA_NBDYMX][SENGA_NSPCMX];
+  double wmolar[SENGA_NSPCMX], ovwmol[SENGA_NSPCMX], rgspec[SENGA_NSPCMX];
+  double clewis[SENGA_NSPCMX], olewis[SENGA_NSPCMX];
+} senga_chem;
+
+/* COMMON/DIFFUS (src/com_senga2.h:189-214) after DIFFIN's derived pass
+ * (src/diffin.f:328-405). flmavt = 0 selects constant-Lewis transport. */
+typedef struct senga_diff {
+  int flmavt, ncodif, ncotdr, ncovis, ncocon;
+  double pdifgb, tdifgb;
+  double diffco[SENGA_NSPCMX][SENGA_NSPCMX][SENGA_NDCFMX];
+  double tdrcco[SENGA_NSPCMX][SENGA_NSPCMX][SENGA_NDCFMX];
+  double wilko1[SENGA_NSPCMX][SENGA_NSPCMX], wilko2[SENGA_NSPCMX][SENGA_NSPCMX];
+  double viscco[SENGA_NSPCMX][SENGA_NDCFMX], condco[SENGA_NSPCMX][SENGA_NDCFMX];
+} senga_diff;
+
+/* Run configuration of one box (cont.dat's grid, domain, BC and dt lines). */
+typedef struct senga_config {
+  int nx, ny, nz;              /* grid points (NXGLBL..; one rank)          */
+  double xgdlen, ygdlen, zgdlen; /* domain lengths [m]; spacing L/(N-1)    */
+  int nend[6];                 /* NENDXL,XR,YL,YR,ZL,ZR: SENGA_NPERI/NBOUND */
+  double tstep;                /* fixed time step TSTEP [s]                 */
+  int adaptive;                /* 1: keep the RK error register (ADAPTT)    */
+  int device;                  /* CUDA device ordinal                       */
+} senga_config;
+
+typedef struct senga_ctx senga_ctx;
+
+/* ---- tables: host-side CHEMIN / DIFFIN ------------------------------------
+ * senga_chem_load restates chem.dat reading (src/chemin.f:146-344) and the
+ * derived-table pass (src/chemin.f:822-983).
+ * senga_diff_load restates diff.dat reading (src/diffin.f:100-232) and the
+ * derived pass (src/diffin.f:328-405); pass path=NULL for constant-Lewis
+ * transport (NFMAVT=0, src/diffin.f:65). */
+int senga_chem_load(const char* path, senga_chem* out);
+int senga_diff_load(const char* path, const senga_chem* chem, senga_diff* out);
+
+/* ---- context: device-resident state for one box ---------------------------
+ * Replaces the reference's COMMON-resident registers xRUN/xRHS/xERR, TRUN and
+ * ITNDEX (src/com_senga2.h:576-679) with HBM-resident SoA fields. */
+int senga_ctx_create(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff,
+                     senga_ctx** out);
+int senga_ctx_destroy(senga_ctx* ctx);
+const char* senga_last_error(void);
+int senga_sync(senga_ctx* ctx);
+/* device pointer to the context's stream (cudaStream_t) */
+void* senga_stream(senga_ctx* ctx);
+
+/* Upload/download the conserved state (rho, rho u, rho v, rho w, rho E,
+ * rho Y_1..rho Y_n; nc = 5+nspec interior arrays, field slowest), the
+ * temperature seed TRUN and the thermo interval index ITNDEX. Upload sets both
+ * RK registers (xRUN = xRHS), as at the end of FINCOM (src/fincom.f:54-168)
+ * and after INDATA (src/indata.f:1540-1565). */
+int senga_upload_state_host(senga_ctx* ctx, const double* fields, const double* trun, const int32_t* itndex);
+int senga_download_state_host(senga_ctx* ctx, double* fields, double* trun, int32_t* itndex);
+
+/* One RK substage (irkstp = 1..5): BOUNDT, PARFER, RHSCAL, RHSVEL, BOUNDS and
+ * LINCOM (irkstp < 5) or FINCOM (irkstp = 5): src/senga2.f:113-159. */
+int senga_substage(senga_ctx* ctx, int irkstp);
+/* nsteps full RK steps (5 substages each, src/senga2.f:96-194; the filter
+ * call at src/senga2.f:178 is commented out in the reference and not run). */
+int senga_step(senga_ctx* ctx, int nsteps);
+/* Capture one full RK step as a CUDA graph and replay it nsteps times. */
+int senga_step_graph(senga_ctx* ctx, int nsteps);
+
+/* RHSCAL + RHSVEL on the current U register without the RK update:
+ * rhs (nc interior arrays) = R(U); optional trun/prun outputs after TEMPER.
+ * Host pointers. */
+int senga_rhs_host(senga_ctx* ctx, double* rhs, double* trun, double* prun);
+
+/* One RK step (5 substages) with CUDA events around every kernel launch on
+ * the context's stream; ms[4] receives the summed time of the four kernel
+ * families (thermo, flow, species_a, species_b+RK), *launches their count.
+ * Advances the state like senga_step(ctx, 1). */
+int senga_profile_step(senga_ctx* ctx, double* ms, int* launches);
+
+/* Status word of the last steps: bit 0 = TEMPER non-convergence. */
+int senga_get_status(senga_ctx* ctx, int* status);
+
+/* ---- operator-level entry points (unit parity) -----------------------------
+ * DFBYDX/DFBYDY/DFBYDZ(FUNCTN, FDERIV): src/dfbydx.f:36-37,53-238
+ * D2FDX2/D2FDY2/D2FDZ2: src/d2fdx2.f:54-270
+ * D2FDXY/D2FDXZ/D2FDYZ: src/d2fdxy.f:55-1937
+ * kind: 0 dx, 1 dy, 2 dz, 3 dxx, 4 dyy, 5 dzz, 6 dxy, 7 dxz, 8 dyz.
+ * f and out are interior arrays (device pointers); periodic directions are
+ * wrapped in place of the reference's halo copy. */
+int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
+int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
+
+/* TEMPER (src/temper.f:58-219) on the current U register; host outputs of
+ * T and p (either may be NULL). CHRATE (src/chrate.f:146-741) on the current U
+ * register and T: host output of RATE (nspec interior arrays). */
+int senga_temper_host(senga_ctx* ctx, double* trun, double* prun);
+int senga_chrate_host(senga_ctx* ctx, double* rate);
+
+/* Integrate FUNCTN over [argmin,argmax] by successive Simpson refinement
+ * (INTEGF, src/integf.f:57-96): host-side helper used by initial-condition
+ * generation (init only, never per substage). */
+typedef double (*senga_integrand)(double x, void* user);
+int senga_integf(senga_integrand f, void* user, double argmin, double argmax, double* answer);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SENGA_GPU_H */

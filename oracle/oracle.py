@@ -1,0 +1,140 @@
+"""ORACLE — TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper of liboracle.so, the CPU restatement of the reference's
+RHSCAL/RHSVEL/TEMPER/CHRATE/derivatives/LINCOM path (senga_oracle.cpp).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
+it, and only as the checker or the timed CPU baseline, never as the product.
+Parity status: the reference is Fortran and no Fortran compiler exists in
+this build environment, so the oracle is pinned by its own known-answer
+tests (tests/test_oracle_kat.py) rather than by outputs of the reference.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+def build():
+    subprocess.run(["make", "-C", HERE, "-s"], check=True)
+
+
+class _Cfg(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("xgdlen", C.c_double), ("ygdlen", C.c_double), ("zgdlen", C.c_double),
+                ("nend", C.c_int * 6), ("flmavt", C.c_int), ("tstep", C.c_double),
+                ("chem_path", C.c_char_p), ("diff_path", C.c_char_p)]
+
+
+_lib = None
+
+
+def _get():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = C.CDLL(LIB)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int32)
+        lib.oracle_create.restype = C.c_void_p
+        lib.oracle_create.argtypes = [C.POINTER(_Cfg)]
+        lib.oracle_destroy.argtypes = [C.c_void_p]
+        lib.oracle_nspec.argtypes = [C.c_void_p]
+        lib.oracle_last_error.restype = C.c_char_p
+        lib.oracle_set_state.argtypes = [C.c_void_p, dp, dp, ip]
+        lib.oracle_get_state.argtypes = [C.c_void_p, dp, dp, ip]
+        lib.oracle_step.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle_rhs.argtypes = [C.c_void_p, dp, dp, dp]
+        lib.oracle_deriv.argtypes = [C.c_void_p, C.c_int, dp, dp]
+        lib.oracle_chrate.argtypes = [C.c_void_p, dp]
+        lib.oracle_chem_scalar.argtypes = [C.c_void_p, C.c_char_p, dp]
+        _lib = lib
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """CPU restatement of one rank of the reference, same interface as Box."""
+
+    def __init__(self, shape, lengths, chem_path, diff_path, tstep, nend=(2,) * 6):
+        lib = _get()
+        nx, ny, nz = shape
+        self.shape = (nz, ny, nx)
+        cfg = _Cfg()
+        cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
+        cfg.xgdlen, cfg.ygdlen, cfg.zgdlen = lengths
+        for i, v in enumerate(nend):
+            cfg.nend[i] = v
+        cfg.flmavt = 1 if diff_path else 0
+        cfg.tstep = tstep
+        self._chem = chem_path.encode()
+        self._diff = diff_path.encode() if diff_path else None
+        cfg.chem_path = self._chem
+        cfg.diff_path = self._diff
+        h = lib.oracle_create(C.byref(cfg))
+        if not h:
+            raise RuntimeError("oracle_create: " + lib.oracle_last_error().decode())
+        self.h = h
+        self.nspec = lib.oracle_nspec(h)
+        self.nc = 5 + self.nspec
+
+    def close(self):
+        if self.h:
+            _get().oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, fields, trun, itndex):
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        t = np.ascontiguousarray(trun, dtype=np.float64)
+        it = np.ascontiguousarray(itndex, dtype=np.int32)
+        _get().oracle_set_state(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)))
+
+    def download(self):
+        f = np.empty((self.nc,) + self.shape)
+        t = np.empty(self.shape)
+        it = np.empty(self.shape, dtype=np.int32)
+        _get().oracle_get_state(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)))
+        return f, t, it
+
+    def step(self, nsteps=1):
+        if _get().oracle_step(self.h, nsteps) != 0:
+            raise RuntimeError("oracle_step: " + _get().oracle_last_error().decode())
+
+    def rhs(self):
+        r = np.empty((self.nc,) + self.shape)
+        t = np.empty(self.shape)
+        p = np.empty(self.shape)
+        if _get().oracle_rhs(self.h, _dp(r), _dp(t), _dp(p)) != 0:
+            raise RuntimeError("oracle_rhs: " + _get().oracle_last_error().decode())
+        return r, t, p
+
+    def chrate(self):
+        r = np.empty((self.nspec,) + self.shape)
+        if _get().oracle_chrate(self.h, _dp(r)) != 0:
+            raise RuntimeError("oracle_chrate: " + _get().oracle_last_error().decode())
+        return r
+
+    def deriv(self, kind, f):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.empty_like(a)
+        if _get().oracle_deriv(self.h, kind, _dp(a), _dp(out)) != 0:
+            raise RuntimeError("oracle_deriv: " + _get().oracle_last_error().decode())
+        return out
+
+    def scalar(self, name):
+        v = C.c_double()
+        _get().oracle_chem_scalar(self.h, name.encode(), C.byref(v))
+        return v.value

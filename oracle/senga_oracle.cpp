@@ -1,0 +1,1256 @@
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// A serial/OpenMP CPU restatement of the reference's per-substage right-hand
+// side and low-storage Runge-Kutta advance. It exists to check the CUDA path:
+// only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+// The product library never links or calls it.
+//
+// Loop order, expression association and array conventions follow the
+// Fortran (column-major, halo of 5, 1-based indices). Compile with
+// -ffp-contract=off so that, like gfortran's x86-64 default, no FMA is formed.
+//
+// Restated routines (file:line within the reference project):
+//   src/dfinit.f:42-482     FD coefficients, spacing L/(N-1)
+//   src/dfbydx.f:53-238     first derivative (+dfbydy.f, dfbydz.f)
+//   src/d2fdx2.f:54-270     second derivative (+d2fdy2.f, d2fdz2.f)
+//   src/d2fdxy.f:55-141,1925-1937  mixed derivative interior (+xz, yz)
+//   src/temper.f:58-219     temperature Newton inversion, cp, p
+//   src/chrate.f:146-741    multistep chemistry
+//   src/rhscal.f:58-3938    scalar RHS (energy, species), configs' branches
+//   src/rhsvel.f:48-2318    momentum/continuity RHS, pressure and viscous work
+//   src/lincom.f:53-169, src/fincom.f:54-168  2N-storage RK update
+//   src/dtinit.f:76-209     RK4(3)5[2R+]C coefficients
+//   src/parfer.f:840-873, src/cxhalo.f:49-72  single-rank periodic halo copy
+#include <omp.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <memory>
+
+#include "oracle_tables.hpp"
+
+namespace orc {
+
+constexpr int NHALO = 5;
+constexpr int NOBC = 0, NBOUND = 1, NPERI = 2;
+
+// Big array with halo: indices 1-NHALO .. n+NHALO in each direction.
+struct Field {
+  int nx = 0, ny = 0, nz = 0, bx = 0, by = 0, bz = 0;
+  std::vector<double> v;
+  void init(int nx_, int ny_, int nz_) {
+    nx = nx_; ny = ny_; nz = nz_;
+    bx = nx + 2 * NHALO; by = ny + 2 * NHALO; bz = nz + 2 * NHALO;
+    v.assign((size_t)bx * by * bz, 0.0);
+  }
+  inline double& operator()(int i, int j, int k) {
+    return v[(size_t)(i - 1 + NHALO) + (size_t)bx * ((size_t)(j - 1 + NHALO) + (size_t)by * (size_t)(k - 1 + NHALO))];
+  }
+  inline double operator()(int i, int j, int k) const {
+    return v[(size_t)(i - 1 + NHALO) + (size_t)bx * ((size_t)(j - 1 + NHALO) + (size_t)by * (size_t)(k - 1 + NHALO))];
+  }
+};
+
+struct IField {
+  int bx = 0, by = 0;
+  std::vector<int32_t> v;
+  void init(int nx, int ny, int nz) {
+    bx = nx + 2 * NHALO; by = ny + 2 * NHALO;
+    v.assign((size_t)bx * by * (nz + 2 * NHALO), 0);
+  }
+  inline int32_t& operator()(int i, int j, int k) {
+    return v[(size_t)(i - 1 + NHALO) + (size_t)bx * ((size_t)(j - 1 + NHALO) + (size_t)by * (size_t)(k - 1 + NHALO))];
+  }
+};
+
+// FD coefficients, src/dfinit.f:42-482 (interior, closures, mixed).
+struct FD {
+  double acoffx, bcoffx, ccoffx, dcoffx, ecoffx;  // same for y,z
+  double acof1, bcof1, ccof1, dcof1, acof2, bcof2, ccof2, dcof2;
+  double acof3, bcof3, acof4, bcof4, ccof4, acof5, bcof5, ccof5, dcof5;
+  double acofs, bcofs, ccofs, dcofs, ecofs;
+  double acfs1, bcfs1, ccfs1, dcfs1, ecfs1, acfs2, bcfs2, ccfs2, dcfs2, ecfs2;
+  double acfs3, bcfs3, acfs4, bcfs4, ccfs4, acfs5, bcfs5, ccfs5, dcfs5;
+  double acofxy, bcofxy, ccofxy, dcofxy, ecofxy;
+  double ovdelx, ovdely, ovdelz, ovdlx2, ovdly2, ovdlz2, deltax, deltay, deltaz;
+  void init(double xl, double yl, double zl, int nxg, int nyg, int nzg) {
+    deltax = xl / (double)(float)(nxg - 1);
+    ovdelx = 1.0 / deltax; ovdlx2 = ovdelx * ovdelx;
+    deltay = yl / (double)(float)(nyg - 1);
+    ovdely = 1.0 / deltay; ovdly2 = ovdely * ovdely;
+    deltaz = zl / (double)(float)(nzg - 1);
+    ovdelz = 1.0 / deltaz; ovdlz2 = ovdelz * ovdelz;
+    double a = 5.0 / 3.0, b = -2.0e1 / 2.1e1, c = 5.0 / 1.4e1, d = -5.0 / 6.3e1, e = 1.0 / 1.26e2;
+    acoffx = a / 2.0; bcoffx = b / 4.0; ccoffx = c / 6.0; dcoffx = d / 8.0; ecoffx = e / 1.0e1;
+    acof1 = 4.0; bcof1 = -3.0; ccof1 = 4.0 / 3.0; dcof1 = -1.0 / 4.0;
+    acof2 = -1.0 / 4.0; bcof2 = 3.0 / 2.0; ccof2 = -1.0 / 2.0; dcof2 = 1.0 / 1.2e1;
+    double a3 = 4.0 / 3.0, b3 = -1.0 / 3.0;
+    acof3 = a3 / 2.0; bcof3 = b3 / 4.0;
+    double a4 = 3.0 / 2.0, b4 = -3.0 / 5.0, c4 = 1.0 / 1.0e1;
+    acof4 = a4 / 2.0; bcof4 = b4 / 4.0; ccof4 = c4 / 6.0;
+    double a5 = 8.0 / 5.0, b5 = -4.0 / 5.0, c5 = 8.0 / 3.5e1, d5 = -1.0 / 3.5e1;
+    acof5 = a5 / 2.0; bcof5 = b5 / 4.0; ccof5 = c5 / 6.0; dcof5 = d5 / 8.0;
+    acofs = a; bcofs = b / 4.0; ccofs = c / 9.0; dcofs = d / 1.6e1; ecofs = e / 2.5e1;
+    acfs1 = -7.7e1 / 6.0; bcfs1 = 1.07e2 / 6.0; ccfs1 = -1.3e1; dcfs1 = 6.1e1 / 1.2e1; ecfs1 = -5.0 / 6.0;
+    acfs2 = 5.0 / 6.0; bcfs2 = -1.0 / 3.0; ccfs2 = 7.0 / 6.0; dcfs2 = -1.0 / 2.0; ecfs2 = 1.0 / 1.2e1;
+    acfs3 = a3; bcfs3 = b3 / 4.0;
+    acfs4 = a4; bcfs4 = b4 / 4.0; ccfs4 = c4 / 9.0;
+    acfs5 = a5; bcfs5 = b5 / 4.0; ccfs5 = c5 / 9.0; dcfs5 = d5 / 1.6e1;
+    acofxy = a / 4.0; bcofxy = b / 4.0 / 4.0; ccofxy = c / 4.0 / 9.0; dcofxy = d / 4.0 / 1.6e1;
+    ecofxy = e / 4.0 / 2.5e1;
+  }
+};
+
+struct Config {
+  int nx, ny, nz;
+  double xgdlen, ygdlen, zgdlen;
+  int nend[6];  // NENDXL, NENDXR, NENDYL, NENDYR, NENDZL, NENDZR
+  int flmavt;   // mixture-averaged transport on/off (cont.dat switch)
+  double tstep;
+};
+
+struct Oracle {
+  Config cf{};
+  Chem ch;
+  Diff df;
+  FD fd{};
+  int nspec = 0;
+  int nx, ny, nz;
+  int istal, istol, jstal, jstol, kstal, kstol;
+  int istab, istob, jstab, jstob, kstab, kstob;
+  int istalt, istolt, jstalt, jstolt, kstalt, kstolt;
+  int nendxl, nendxr, nendyl, nendyr, nendzl, nendzr;
+  // BC zeroing flags (all false for the periodic cases handled here)
+  bool fxlcon = false, fxrcon = false, fylcon = false, fyrcon = false, fzlcon = false, fzrcon = false;
+  bool fxldif = false, fxrdif = false, fyldif = false, fyrdif = false, fzldif = false, fzrdif = false;
+  bool fxladb = false, fxradb = false, fyladb = false, fyradb = false, fzladb = false, fzradb = false;
+  bool fxlvsn = false, fxrvsn = false, fylvsn = false, fyrvsn = false, fzlvsn = false, fzrvsn = false;
+  bool fxlvst = false, fxrvst = false, fylvst = false, fyrvst = false, fzlvst = false, fzrvst = false;
+  // RK
+  double rklhs[5], rkrhs[5], rkerr[5];
+  // state
+  Field drun, urun, vrun, wrun, erun;
+  std::vector<Field> yrun;
+  Field drhs, urhs, vrhs, wrhs, erhs;
+  std::vector<Field> yrhs;
+  Field derr, uerr, verr, werr, eerr;
+  std::vector<Field> yerr;
+  // work
+  Field store1, store2, store3, store4, store5, store6, store7, divm;
+  std::vector<Field> rate, rrte;
+  Field ucor, vcor, wcor, utmp, vtmp, wtmp, prun, trun, transp;
+  Field wmomix, difmix;
+  IField itndex;
+  Field wk1, wk2, wk3, wk4;  // chrate STORE1..4 counterparts
+
+  void init(const Config& c, const std::string& chem, const std::string& diff) {
+    cf = c;
+    read_chem(chem, ch);
+    nspec = ch.nspec;
+    if (c.flmavt) read_diff(diff, ch, df);
+    nx = c.nx; ny = c.ny; nz = c.nz;
+    istal = 1; istol = nx; jstal = 1; jstol = ny; kstal = 1; kstol = nz;
+    istab = 1 - NHALO; istob = nx + NHALO; jstab = 1 - NHALO; jstob = ny + NHALO;
+    kstab = 1 - NHALO; kstob = nz + NHALO;
+    nendxl = c.nend[0]; nendxr = c.nend[1]; nendyl = c.nend[2]; nendyr = c.nend[3];
+    nendzl = c.nend[4]; nendzr = c.nend[5];
+    istalt = nendxl == NPERI ? istal - NHALO : istal;
+    istolt = nendxr == NPERI ? istol + NHALO : istol;
+    jstalt = nendyl == NPERI ? jstal - NHALO : jstal;
+    jstolt = nendyr == NPERI ? jstol + NHALO : jstol;
+    kstalt = nendzl == NPERI ? kstal - NHALO : kstal;
+    kstolt = nendzr == NPERI ? kstol + NHALO : kstol;
+    fd.init(c.xgdlen, c.ygdlen, c.zgdlen, nx, ny, nz);
+    Field* all[] = {&drun, &urun, &vrun, &wrun, &erun, &drhs, &urhs, &vrhs, &wrhs, &erhs,
+                    &derr, &uerr, &verr, &werr, &eerr, &store1, &store2, &store3, &store4,
+                    &store5, &store6, &store7, &divm, &ucor, &vcor, &wcor, &utmp, &vtmp,
+                    &wtmp, &prun, &trun, &transp, &wmomix, &difmix, &wk1, &wk2, &wk3, &wk4};
+    for (Field* f : all) f->init(nx, ny, nz);
+    auto mk = [&](std::vector<Field>& v) {
+      v.resize(nspec);
+      for (auto& f : v) f.init(nx, ny, nz);
+    };
+    mk(yrun); mk(yrhs); mk(yerr); mk(rate); mk(rrte);
+    itndex.init(nx, ny, nz);
+    dtinit(c.tstep);
+  }
+
+  // ---- RK coefficients: src/dtinit.f:76-209 ----
+  void dtinit(double tstep) {
+    const double a[5] = {970286171893.0 / 4311952581923.0, 6584761158862.0 / 12103376702013.0,
+                         2251764453980.0 / 15575788980749.0, 26877169314380.0 / 34165994151039.0, 0.0};
+    const double b[5] = {1153189308089.0 / 22510343858157.0, 1772645290293.0 / 4653164025191.0,
+                         -1672844663538.0 / 4480602732383.0, 2114624349019.0 / 3568978502595.0,
+                         5198255086312.0 / 14908931495163.0};
+    const double bh[5] = {1016888040809.0 / 7410784769900.0, 11231460423587.0 / 58533540763752.0,
+                          -1563879915014.0 / 6823010717585.0, 606302364029.0 / 971179775848.0,
+                          1097981568119.0 / 3980877426909.0};
+    for (int i = 0; i < 5; ++i) {
+      rklhs[i] = b[i] * tstep;
+      rkrhs[i] = a[i] * tstep;
+      rkerr[i] = (b[i] - bh[i]) * tstep;
+    }
+  }
+
+  // ---------------------------------------------------------------------
+  // Derivatives. FUNCTN is a big array; FDERIV interior.
+  // src/dfbydx.f:53-238 (first), d2fdx2.f:54-270 (second).
+  // The three directions are the same scheme along a different axis; `dir`
+  // selects it. The closure formulas follow the x routines line by line.
+  template <int dir>
+  inline double& at(Field& f, int a, int j, int k) {
+    if (dir == 0) return f(a, j, k);
+    if (dir == 1) return f(j, a, k);
+    return f(j, k, a);
+  }
+  template <int dir>
+  void d1(Field& F, Field& D) {
+    int nl = dir == 0 ? nendxl : dir == 1 ? nendyl : nendzl;
+    int nr = dir == 0 ? nendxr : dir == 1 ? nendyr : nendzr;
+    int n = dir == 0 ? nx : dir == 1 ? ny : nz;
+    int n1 = dir == 0 ? ny : nx, n2 = dir == 0 ? nz : dir == 1 ? nz : ny;
+    double ovd = dir == 0 ? fd.ovdelx : dir == 1 ? fd.ovdely : fd.ovdelz;
+    int ist = 1, ifn = n;
+    if (nl == NBOUND) ist = 6;
+    if (nr == NBOUND) ifn = n - 5;
+    const FD& c = fd;
+#pragma omp parallel for schedule(static)
+    for (int q = 1; q <= n2; ++q)
+      for (int p = 1; p <= n1; ++p) {
+        auto f = [&](int a) { return at<dir>(F, a, p, q); };
+        for (int ic = ist; ic <= ifn; ++ic) {
+          double fa = f(ic + 1) - f(ic - 1), fb = f(ic + 2) - f(ic - 2), fc = f(ic + 3) - f(ic - 3);
+          double fdd = f(ic + 4) - f(ic - 4), fe = f(ic + 5) - f(ic - 5);
+          at<dir>(D, ic, p, q) = c.acoffx * fa + c.bcoffx * fb + c.ccoffx * fc + c.dcoffx * fdd + c.ecoffx * fe;
+        }
+        if (nl == NBOUND) {
+          double fa, fb, fc, fdd;
+          fa = f(2) - f(1); fb = f(3) - f(1); fc = f(4) - f(1); fdd = f(5) - f(1);
+          at<dir>(D, 1, p, q) = c.acof1 * fa + c.bcof1 * fb + c.ccof1 * fc + c.dcof1 * fdd;
+          fa = f(1) - f(2); fb = f(3) - f(2); fc = f(4) - f(2); fdd = f(5) - f(2);
+          at<dir>(D, 2, p, q) = c.acof2 * fa + c.bcof2 * fb + c.ccof2 * fc + c.dcof2 * fdd;
+          fa = f(4) - f(2); fb = f(5) - f(1);
+          at<dir>(D, 3, p, q) = c.acof3 * fa + c.bcof3 * fb;
+          fa = f(5) - f(3); fb = f(6) - f(2); fc = f(7) - f(1);
+          at<dir>(D, 4, p, q) = c.acof4 * fa + c.bcof4 * fb + c.ccof4 * fc;
+          fa = f(6) - f(4); fb = f(7) - f(3); fc = f(8) - f(2); fdd = f(9) - f(1);
+          at<dir>(D, 5, p, q) = c.acof5 * fa + c.bcof5 * fb + c.ccof5 * fc + c.dcof5 * fdd;
+        }
+        if (nr == NBOUND) {
+          double fa, fb, fc, fdd;
+          const int L = n;
+          fa = f(L - 3) - f(L - 5); fb = f(L - 2) - f(L - 6); fc = f(L - 1) - f(L - 7); fdd = f(L) - f(L - 8);
+          at<dir>(D, L - 4, p, q) = c.acof5 * fa + c.bcof5 * fb + c.ccof5 * fc + c.dcof5 * fdd;
+          fa = f(L - 2) - f(L - 4); fb = f(L - 1) - f(L - 5); fc = f(L) - f(L - 6);
+          at<dir>(D, L - 3, p, q) = c.acof4 * fa + c.bcof4 * fb + c.ccof4 * fc;
+          fa = f(L - 1) - f(L - 3); fb = f(L) - f(L - 4);
+          at<dir>(D, L - 2, p, q) = c.acof3 * fa + c.bcof3 * fb;
+          fa = f(L - 1) - f(L); fb = f(L - 1) - f(L - 2); fc = f(L - 1) - f(L - 3); fdd = f(L - 1) - f(L - 4);
+          at<dir>(D, L - 1, p, q) = c.acof2 * fa + c.bcof2 * fb + c.ccof2 * fc + c.dcof2 * fdd;
+          fa = f(L) - f(L - 1); fb = f(L) - f(L - 2); fc = f(L) - f(L - 3); fdd = f(L) - f(L - 4);
+          at<dir>(D, L, p, q) = c.acof1 * fa + c.bcof1 * fb + c.ccof1 * fc + c.dcof1 * fdd;
+        }
+        for (int ic = 1; ic <= n; ++ic) at<dir>(D, ic, p, q) = at<dir>(D, ic, p, q) * ovd;
+      }
+  }
+  template <int dir>
+  void d2(Field& F, Field& D) {
+    int nl = dir == 0 ? nendxl : dir == 1 ? nendyl : nendzl;
+    int nr = dir == 0 ? nendxr : dir == 1 ? nendyr : nendzr;
+    int n = dir == 0 ? nx : dir == 1 ? ny : nz;
+    int n1 = dir == 0 ? ny : nx, n2 = dir == 0 ? nz : dir == 1 ? nz : ny;
+    double ovd2 = dir == 0 ? fd.ovdlx2 : dir == 1 ? fd.ovdly2 : fd.ovdlz2;
+    int ist = 1, ifn = n;
+    if (nl == NBOUND) ist = 6;
+    if (nr == NBOUND) ifn = n - 5;
+    const FD& c = fd;
+#pragma omp parallel for schedule(static)
+    for (int q = 1; q <= n2; ++q)
+      for (int p = 1; p <= n1; ++p) {
+        auto f = [&](int a) { return at<dir>(F, a, p, q); };
+        for (int ic = ist; ic <= ifn; ++ic) {
+          double fc0 = f(ic);
+          double ap = f(ic + 1) - fc0, am = fc0 - f(ic - 1);
+          double bp = f(ic + 2) - fc0, bm = fc0 - f(ic - 2);
+          double cp = f(ic + 3) - fc0, cm = fc0 - f(ic - 3);
+          double dp = f(ic + 4) - fc0, dm = fc0 - f(ic - 4);
+          double ep = f(ic + 5) - fc0, em = fc0 - f(ic - 5);
+          at<dir>(D, ic, p, q) = c.acofs * (ap - am) + c.bcofs * (bp - bm) + c.ccofs * (cp - cm) +
+                                 c.dcofs * (dp - dm) + c.ecofs * (ep - em);
+        }
+        if (nl == NBOUND) {
+          double ap, am, bp, bm, cp, cm, dp, dm, ep;
+          ap = f(2) - f(1); bp = f(3) - f(1); cp = f(4) - f(1); dp = f(5) - f(1); ep = f(6) - f(1);
+          at<dir>(D, 1, p, q) = c.acfs1 * ap + c.bcfs1 * bp + c.ccfs1 * cp + c.dcfs1 * dp + c.ecfs1 * ep;
+          ap = f(1) - f(2); bp = f(3) - f(2); cp = f(4) - f(2); dp = f(5) - f(2); ep = f(6) - f(2);
+          at<dir>(D, 2, p, q) = c.acfs2 * ap + c.bcfs2 * bp + c.ccfs2 * cp + c.dcfs2 * dp + c.ecfs2 * ep;
+          ap = f(4) - f(3); am = f(3) - f(2); bp = f(5) - f(3); bm = f(3) - f(1);
+          at<dir>(D, 3, p, q) = c.acfs3 * (ap - am) + c.bcfs3 * (bp - bm);
+          ap = f(5) - f(4); am = f(4) - f(3); bp = f(6) - f(4); bm = f(4) - f(2); cp = f(7) - f(4);
+          cm = f(4) - f(1);
+          at<dir>(D, 4, p, q) = c.acfs4 * (ap - am) + c.bcfs4 * (bp - bm) + c.ccfs4 * (cp - cm);
+          ap = f(6) - f(5); am = f(5) - f(4); bp = f(7) - f(5); bm = f(5) - f(3); cp = f(8) - f(5);
+          cm = f(5) - f(2); dp = f(9) - f(5); dm = f(5) - f(1);
+          at<dir>(D, 5, p, q) =
+              c.acfs5 * (ap - am) + c.bcfs5 * (bp - bm) + c.ccfs5 * (cp - cm) + c.dcfs5 * (dp - dm);
+        }
+        if (nr == NBOUND) {
+          const int L = n;
+          double ap, am, bp, bm, cp, cm, dp, dm, ep;
+          ap = f(L - 3) - f(L - 4); am = f(L - 4) - f(L - 5); bp = f(L - 2) - f(L - 4);
+          bm = f(L - 4) - f(L - 6); cp = f(L - 1) - f(L - 4); cm = f(L - 4) - f(L - 7);
+          dp = f(L) - f(L - 4); dm = f(L - 4) - f(L - 8);
+          at<dir>(D, L - 4, p, q) =
+              c.acfs5 * (ap - am) + c.bcfs5 * (bp - bm) + c.ccfs5 * (cp - cm) + c.dcfs5 * (dp - dm);
+          ap = f(L - 2) - f(L - 3); am = f(L - 3) - f(L - 4); bp = f(L - 1) - f(L - 3);
+          bm = f(L - 3) - f(L - 5); cp = f(L) - f(L - 3); cm = f(L - 3) - f(L - 6);
+          at<dir>(D, L - 3, p, q) = c.acfs4 * (ap - am) + c.bcfs4 * (bp - bm) + c.ccfs4 * (cp - cm);
+          ap = f(L - 1) - f(L - 2); am = f(L - 2) - f(L - 3); bp = f(L) - f(L - 2); bm = f(L - 2) - f(L - 4);
+          at<dir>(D, L - 2, p, q) = c.acfs3 * (ap - am) + c.bcfs3 * (bp - bm);
+          ap = f(L) - f(L - 1); bp = f(L - 2) - f(L - 1); cp = f(L - 3) - f(L - 1); dp = f(L - 4) - f(L - 1);
+          ep = f(L - 5) - f(L - 1);
+          at<dir>(D, L - 1, p, q) = c.acfs2 * ap + c.bcfs2 * bp + c.ccfs2 * cp + c.dcfs2 * dp + c.ecfs2 * ep;
+          ap = f(L - 1) - f(L); bp = f(L - 2) - f(L); cp = f(L - 3) - f(L); dp = f(L - 4) - f(L);
+          ep = f(L - 5) - f(L);
+          at<dir>(D, L, p, q) = c.acfs1 * ap + c.bcfs1 * bp + c.ccfs1 * cp + c.dcfs1 * dp + c.ecfs1 * ep;
+        }
+        for (int ic = 1; ic <= n; ++ic) at<dir>(D, ic, p, q) = at<dir>(D, ic, p, q) * ovd2;
+      }
+  }
+  // Mixed derivative, interior scheme (src/d2fdxy.f:67-141; scaling :1925-1937).
+  // plane 0: xy, 1: xz, 2: yz. Both directions must be periodic here; the
+  // one-sided edge/corner closures are not restated in this oracle.
+  template <int plane>
+  void dmix(Field& F, Field& D) {
+    double s1 = plane == 2 ? fd.ovdely : fd.ovdelx;
+    double s2 = plane == 0 ? fd.ovdely : fd.ovdelz;
+    int na = plane == 2 ? ny : nx, nb = plane == 0 ? ny : nz, nc = plane == 0 ? nz : plane == 1 ? ny : nx;
+    bool bnd = plane == 0 ? (nendxl == NBOUND || nendxr == NBOUND || nendyl == NBOUND || nendyr == NBOUND)
+               : plane == 1 ? (nendxl == NBOUND || nendxr == NBOUND || nendzl == NBOUND || nendzr == NBOUND)
+                            : (nendyl == NBOUND || nendyr == NBOUND || nendzl == NBOUND || nendzr == NBOUND);
+    if (bnd) throw std::runtime_error("oracle: mixed-derivative closures not restated");
+    const FD& c = fd;
+#pragma omp parallel for schedule(static)
+    for (int r = 1; r <= nc; ++r)
+      for (int b = 1; b <= nb; ++b)
+        for (int a = 1; a <= na; ++a) {
+          auto f = [&](int da, int db) -> double {
+            if (plane == 0) return F(a + da, b + db, r);
+            if (plane == 1) return F(a + da, r, b + db);
+            return F(r, a + da, b + db);
+          };
+          double fa = f(1, 1) - f(1, -1) - f(-1, 1) + f(-1, -1);
+          double fb = f(2, 2) - f(2, -2) - f(-2, 2) + f(-2, -2);
+          double fc = f(3, 3) - f(3, -3) - f(-3, 3) + f(-3, -3);
+          double fdd = f(4, 4) - f(4, -4) - f(-4, 4) + f(-4, -4);
+          double fe = f(5, 5) - f(5, -5) - f(-5, 5) + f(-5, -5);
+          double v = c.acofxy * fa + c.bcofxy * fb + c.ccofxy * fc + c.dcofxy * fdd + c.ecofxy * fe;
+          double& out = plane == 0 ? D(a, b, r) : plane == 1 ? D(a, r, b) : D(r, a, b);
+          out = v * s1 * s2;
+        }
+  }
+  void dfbydx(Field& F, Field& D) { d1<0>(F, D); }
+  void dfbydy(Field& F, Field& D) { d1<1>(F, D); }
+  void dfbydz(Field& F, Field& D) { d1<2>(F, D); }
+  void d2fdx2(Field& F, Field& D) { d2<0>(F, D); }
+  void d2fdy2(Field& F, Field& D) { d2<1>(F, D); }
+  void d2fdz2(Field& F, Field& D) { d2<2>(F, D); }
+  void d2fdxy(Field& F, Field& D) { dmix<0>(F, D); }
+  void d2fdxz(Field& F, Field& D) { dmix<1>(F, D); }
+  void d2fdyz(Field& F, Field& D) { dmix<2>(F, D); }
+
+  // ZEROxx: zero an end plane of an interior derivative array (src/zeroxl.f).
+  void zero_plane(Field& D, int dir, bool right) {
+    if (dir == 0) { int i = right ? istol : istal; for (int k = 1; k <= nz; ++k) for (int j = 1; j <= ny; ++j) D(i, j, k) = 0.0; }
+    if (dir == 1) { int j = right ? jstol : jstal; for (int k = 1; k <= nz; ++k) for (int i = 1; i <= nx; ++i) D(i, j, k) = 0.0; }
+    if (dir == 2) { int k = right ? kstol : kstal; for (int j = 1; j <= ny; ++j) for (int i = 1; i <= nx; ++i) D(i, j, k) = 0.0; }
+  }
+  void zx(bool l, bool r, Field& D) { if (l) zero_plane(D, 0, false); if (r) zero_plane(D, 0, true); }
+  void zy(bool l, bool r, Field& D) { if (l) zero_plane(D, 1, false); if (r) zero_plane(D, 1, true); }
+  void zz(bool l, bool r, Field& D) { if (l) zero_plane(D, 2, false); if (r) zero_plane(D, 2, true); }
+
+  // ---- periodic halo copy: src/parfer.f:840-873, src/cxhalo.f:49-72 ----
+  void halo_periodic(Field& f) {
+    if (nendxl == NPERI)
+      for (int k = kstal; k <= kstol; ++k)
+        for (int j = jstal; j <= jstol; ++j)
+          for (int h = 1; h <= NHALO; ++h) {
+            f(nx + h, j, k) = f(h, j, k);
+            f(1 - h, j, k) = f(nx + 1 - h, j, k);
+          }
+    if (nendyl == NPERI)
+      for (int k = kstal; k <= kstol; ++k)
+        for (int h = 1; h <= NHALO; ++h)
+          for (int i = istab; i <= istob; ++i) {
+            f(i, ny + h, k) = f(i, h, k);
+            f(i, 1 - h, k) = f(i, ny + 1 - h, k);
+          }
+    if (nendzl == NPERI)
+      for (int h = 1; h <= NHALO; ++h)
+        for (int j = jstab; j <= jstob; ++j)
+          for (int i = istab; i <= istob; ++i) {
+            f(i, j, nz + h) = f(i, j, h);
+            f(i, j, 1 - h) = f(i, j, nz + 1 - h);
+          }
+  }
+  void parfer() {
+    halo_periodic(drhs); halo_periodic(urhs); halo_periodic(vrhs); halo_periodic(wrhs);
+    halo_periodic(erhs);
+    for (auto& y : yrhs) halo_periodic(y);
+  }
+
+  // ---- TEMPER: src/temper.f:58-219 ----
+  void temper() {
+    const double toltmp = (double)1.0e-10f;  // single-precision literal in the reference
+    const int ntitrs = 100;
+    int failed = 0;
+#pragma omp parallel for schedule(static) reduction(+ : failed)
+    for (int kc = kstalt; kc <= kstolt; ++kc)
+      for (int jc = jstalt; jc <= jstolt; ++jc)
+        for (int ic = istalt; ic <= istolt; ++ic) {
+          double tcoeff[NCTMAX + 1], tderiv[NCTMAX + 1];
+          double ukuk = (urhs(ic, jc, kc) * urhs(ic, jc, kc) + vrhs(ic, jc, kc) * vrhs(ic, jc, kc) +
+                         wrhs(ic, jc, kc) * wrhs(ic, jc, kc)) / drhs(ic, jc, kc);
+          tcoeff[0] = 0.5 * ukuk - erhs(ic, jc, kc);
+          for (int icp = 1; icp <= NCTMAX; ++icp) { tcoeff[icp] = 0.0; tderiv[icp] = 0.0; }
+          double st7 = 0.0;
+          int itn = itndex(ic, jc, kc);
+          for (int is = 1; is <= nspec; ++is) {
+            int ipower = is - 1;
+            int icoef2 = 1;
+            for (int q = 0; q < ipower; ++q) icoef2 *= NTBASE;
+            int icoef1 = icoef2 * NTBASE;
+            int itint = 1 + (itn % icoef1) / icoef2;
+            double y = yrhs[is - 1](ic, jc, kc);
+            int k2 = Chem::c2(itint, is);
+            tcoeff[0] = tcoeff[0] + y * ch.amascp[Chem::c3(ch.ncenth[k2], itint, is)];
+            tcoeff[1] = tcoeff[1] + y * ch.amasct[Chem::c3(1, itint, is)];
+            tderiv[1] = tcoeff[1];
+            for (int icp = 2; icp <= ch.ncpoly[k2]; ++icp) {
+              tcoeff[icp] = tcoeff[icp] + y * ch.amasct[Chem::c3(icp, itint, is)];
+              tderiv[icp] = tderiv[icp] + y * ch.amascp[Chem::c3(icp, itint, is)];
+            }
+            st7 = st7 + y * ch.rgspec[is - 1];
+          }
+          double tempor = trun(ic, jc, kc);
+          int itrs = 1;
+          for (;;) {
+            double tf = tcoeff[NCTMAX], tdp = tderiv[NCTMAX];
+            for (int icp = NCTMAX - 1; icp >= 1; --icp) {
+              tf = tcoeff[icp] + tf * tempor;
+              tdp = tderiv[icp] + tdp * tempor;
+            }
+            tf = tcoeff[0] + tf * tempor;
+            double del = -tf / tdp;
+            if (std::fabs(del) > toltmp) {
+              if (itrs < ntitrs) { tempor = tempor + del; ++itrs; continue; }
+              ++failed;
+            }
+            break;
+          }
+          trun(ic, jc, kc) = tempor;
+          int itnew = 0;
+          double tr = 0.0;
+          for (int is = 1; is <= nspec; ++is) {
+            int itint = 1;
+            while (trun(ic, jc, kc) > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
+            int p = 1;
+            for (int q = 0; q < is - 1; ++q) p *= NTBASE;
+            itnew = itnew + (itint - 1) * p;
+            int k2 = Chem::c2(itint, is);
+            double cpf = ch.amascp[Chem::c3(ch.ncpoly[k2], itint, is)];
+            for (int icp = ch.ncpom1[k2]; icp >= 1; --icp)
+              cpf = cpf * trun(ic, jc, kc) + ch.amascp[Chem::c3(icp, itint, is)];
+            tr = tr + yrhs[is - 1](ic, jc, kc) * cpf;
+          }
+          itndex(ic, jc, kc) = itnew;
+          transp(ic, jc, kc) = tr / drhs(ic, jc, kc);
+          store7(ic, jc, kc) = st7;
+          prun(ic, jc, kc) = trun(ic, jc, kc) * store7(ic, jc, kc);
+        }
+    if (failed) throw std::runtime_error("oracle TEMPER: Newton iteration failed to converge");
+  }
+
+  // ---- CHRATE: src/chrate.f:146-741 (per point; same operation order) ----
+  void chrate_point(int ic, int jc, int kc) {
+    const double YSMALL = 1.0e-30, YDENOM = 1.0e-15, CLNTEN = std::log(10.0);
+    double T = trun(ic, jc, kc);
+    int itn = itndex(ic, jc, kc);
+    for (int is = 1; is <= nspec; ++is) rate[is - 1](ic, jc, kc) = 0.0;
+    // STORE3 keeps the last third-body concentration across steps, as in the
+    // reference (a falloff step without its own third body would reuse it).
+    double s3 = 0.0;
+    for (int ist = 1; ist <= ch.nstep; ++ist) {
+      bool flthrd = true;
+      if (ch.mblist[ist - 1] != 0) {
+        int ib = ch.mblist[ist - 1];
+        s3 = 0.0;
+        for (int is = 1; is <= nspec; ++is) {
+          double ovwmas = ch.ovwmol[is - 1] * ch.effy3b[(ib - 1) * NSPCMX + (is - 1)];
+          s3 = s3 + yrhs[is - 1](ic, jc, kc) * ovwmas;
+        }
+      }
+      double racnst = ch.rparam[(ist - 1) * 3 + 0], rncnst = ch.rparam[(ist - 1) * 3 + 1],
+             reovrr = ch.rparam[(ist - 1) * 3 + 2];
+      double s2 = racnst + rncnst * std::log(T) - reovrr / T;
+      double s1 = std::exp(s2);
+      if (ch.mllist[ist - 1] != 0) {
+        const double* rl = &ch.rclind[(ch.mllist[ist - 1] - 1) * 4];
+        float flcnst = (float)rl[3];  // implicitly typed REAL in the reference
+        double s4 = rl[0] + rl[1] * std::log(T) - rl[2] / T;
+        s4 = std::exp(s4);
+        double preduc = s3 * s4 / s1;
+        double fornow = (double)flcnst * preduc / (1.0 + preduc);
+        s1 = s1 * fornow;
+        s2 = std::log(s1);
+        flthrd = false;
+      }
+      if (ch.mtlist[ist - 1] != 0) {
+        const double* rt = &ch.rctroe[(ch.mtlist[ist - 1] - 1) * 12];
+        float talpha = (float)rt[3];
+        double ovtst1 = rt[4], tstar2 = rt[5], ovtst3 = rt[6];
+        float cfcst1 = (float)rt[7], cfcst2 = (float)rt[8], encst1 = (float)rt[9], encst2 = (float)rt[10],
+              dtcnst = (float)rt[11];
+        double omalph = 1.0 - (double)talpha;
+        double s4 = rt[0] + rt[1] * std::log(T) - rt[2] / T;
+        s4 = std::exp(s4);
+        double preduc = s3 * s4 / s1;
+        double trats1 = T * ovtst1, trats2 = -tstar2 / T, trats3 = T * ovtst3;
+        double ftcent = omalph * std::exp(trats3) + (double)talpha * std::exp(trats1) + std::exp(trats2);
+        ftcent = std::log10(ftcent);
+        double cfactr = (double)cfcst1 + (double)cfcst2 * ftcent;
+        double enfact = (double)encst1 + (double)encst2 * ftcent;
+        double fornow = std::log10(preduc) + cfactr;
+        fornow = fornow / (enfact - (double)dtcnst * fornow);
+        fornow = 1.0 + fornow * fornow;
+        double fbroad = ftcent / fornow;
+        fbroad = std::exp(fbroad * CLNTEN);
+        fornow = fbroad * preduc / (1.0 + preduc);
+        s1 = s1 * fornow;
+        s2 = std::log(s1);
+        flthrd = false;
+      }
+      if (ch.mslist[ist - 1] != 0) {
+        const double* rs = &ch.rcsrif[(ch.mslist[ist - 1] - 1) * 8];
+        double s4 = rs[0] + rs[1] * std::log(T) - rs[2] / T;
+        s4 = std::exp(s4);
+        double preduc = s3 * s4 / s1;
+        double fornow = rs[4] / T;
+        double fbroad = rs[3] * std::exp(fornow);
+        fornow = T * rs[5];
+        fbroad = fbroad + std::exp(fornow);
+        fornow = std::log10(preduc);
+        fornow = 1.0 / (1.0 + std::log10(fornow));
+        fbroad = rs[6] * std::exp(fornow * std::log(fbroad));
+        fornow = fbroad * std::exp(rs[7] * std::log(T));
+        fornow = fbroad * preduc / (1.0 + preduc);
+        s1 = s1 * fornow;
+        s2 = std::log(s1);
+        flthrd = false;
+      }
+      for (int isl = 1; isl <= ch.nrslen[ist - 1]; ++isl) {
+        int is = ch.nrspec[Chem::ss(isl, ist)];
+        double fornow = std::max(yrhs[is - 1](ic, jc, kc) * ch.ovwmol[is - 1], 0.0);
+        s1 = s1 * fornow;
+      }
+      for (int isl = 1; isl <= ch.nrclen[ist - 1]; ++isl) {
+        int is = ch.nrcpec[Chem::ss(isl, ist)];
+        double scoef = ch.crspec[Chem::ss(isl, ist)];
+        double fornow = yrhs[is - 1](ic, jc, kc) * ch.ovwmol[is - 1];
+        fornow = std::max(fornow, YSMALL);
+        fornow = std::exp(scoef * std::log(fornow));
+        fornow = fornow / (1.0 + YDENOM * fornow);
+        s1 = s1 * fornow;
+      }
+      if (ch.mglist[ist - 1] != 0) {
+        for (int isl = 1; isl <= ch.nsslen[ist - 1]; ++isl) {
+          int is = ch.nsspec[Chem::ss(isl, ist)];
+          int p = 1;
+          for (int q = 0; q < is - 1; ++q) p *= NTBASE;
+          int itint = 1 + (itn % (p * NTBASE)) / p;
+          int k2 = Chem::c2(itint, is);
+          double g = ch.amolgb[Chem::c3(ch.ncpoly[k2], itint, is)];
+          for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) g = ch.amolgb[Chem::c3(icp, itint, is)] + g * T;
+          g = ch.amolgb[Chem::c3(ch.ncenth[k2], itint, is)] / T -
+              ch.amolgb[Chem::c3(ch.ncenpy[k2], itint, is)] * std::log(T) - g;
+          s2 = s2 + ch.diffmu[Chem::ss(isl, ist)] * g;
+        }
+        s2 = std::exp(s2);
+        for (int isl = 1; isl <= ch.npslen[ist - 1]; ++isl) {
+          int is = ch.npspec[Chem::ss(isl, ist)];
+          double fornow = std::max(yrhs[is - 1](ic, jc, kc) * ch.ovwmol[is - 1], 0.0);
+          s2 = s2 * fornow;
+        }
+        for (int isl = 1; isl <= ch.npclen[ist - 1]; ++isl) {
+          int is = ch.npcpec[Chem::ss(isl, ist)];
+          double scoef = ch.cpspec[Chem::ss(isl, ist)];
+          double fornow = yrhs[is - 1](ic, jc, kc) * ch.ovwmol[is - 1];
+          fornow = std::max(fornow, YSMALL);
+          fornow = std::exp(scoef * std::log(fornow));
+          fornow = fornow / (1.0 + YDENOM * fornow);
+          s2 = s2 * fornow;
+        }
+        s1 = s1 - s2;
+      }
+      if (ch.mblist[ist - 1] != 0 && flthrd) s1 = s1 * s3;
+      for (int isl = 1; isl <= ch.nsslen[ist - 1]; ++isl) {
+        int is = ch.nsspec[Chem::ss(isl, ist)];
+        rate[is - 1](ic, jc, kc) = rate[is - 1](ic, jc, kc) + s1 * ch.diffmw[Chem::ss(isl, ist)];
+      }
+    }
+  }
+  void chrate() {
+#pragma omp parallel for schedule(static)
+    for (int kc = kstal; kc <= kstol; ++kc)
+      for (int jc = jstal; jc <= jstol; ++jc)
+        for (int ic = istal; ic <= istol; ++ic) chrate_point(ic, jc, kc);
+  }
+
+#define STD3 _Pragma("omp parallel for schedule(static)") for (int kc = kstal; kc <= kstol; ++kc) for (int jc = jstal; jc <= jstol; ++jc) for (int ic = istal; ic <= istol; ++ic)
+#define BIG3 _Pragma("omp parallel for schedule(static)") for (int kc = kstab; kc <= kstob; ++kc) for (int jc = jstab; jc <= jstob; ++jc) for (int ic = istab; ic <= istob; ++ic)
+#define TRG3 _Pragma("omp parallel for schedule(static)") for (int kc = kstalt; kc <= kstolt; ++kc) for (int jc = jstalt; jc <= jstolt; ++jc) for (int ic = istalt; ic <= istolt; ++ic)
+
+  // ---- RHSCAL: src/rhscal.f (branches used by the periodic cases) ----
+  void rhscal() {
+    temper();
+    dfbydx(urhs, store1); dfbydy(vrhs, store2); dfbydz(wrhs, store3);
+    STD3 divm(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc);
+    TRG3 erhs(ic, jc, kc) = erhs(ic, jc, kc) / drhs(ic, jc, kc);
+    STD3 store4(ic, jc, kc) = erhs(ic, jc, kc) * divm(ic, jc, kc);
+    BIG3 store7(ic, jc, kc) = erhs(ic, jc, kc) * urhs(ic, jc, kc);
+    dfbydx(store7, store1);
+    BIG3 store7(ic, jc, kc) = erhs(ic, jc, kc) * vrhs(ic, jc, kc);
+    dfbydy(store7, store2);
+    BIG3 store7(ic, jc, kc) = erhs(ic, jc, kc) * wrhs(ic, jc, kc);
+    dfbydz(store7, store3);
+    STD3 store4(ic, jc, kc) = store4(ic, jc, kc) + store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc);
+    dfbydx(erhs, store1); dfbydy(erhs, store2); dfbydz(erhs, store3);
+    STD3 erhs(ic, jc, kc) = -0.5 * (store4(ic, jc, kc) + store1(ic, jc, kc) * urhs(ic, jc, kc) +
+                                     store2(ic, jc, kc) * vrhs(ic, jc, kc) + store3(ic, jc, kc) * wrhs(ic, jc, kc));
+    // heat flux
+    dfbydx(trun, store1); dfbydy(trun, store2); dfbydz(trun, store3);
+    BIG3 {
+      double fornow = ch.alamda * std::exp(RLAMDA * std::log(trun(ic, jc, kc)));
+      store7(ic, jc, kc) = fornow * transp(ic, jc, kc);
+      transp(ic, jc, kc) = fornow;
+    }
+    if (df.flmavt) {
+      BIG3 {
+        double ctrans[NSPCMX];
+        transp(ic, jc, kc) = std::log(trun(ic, jc, kc) / df.tdifgb);
+        for (int is = 1; is <= nspec; ++is) {
+          double f = df.condco[Diff::v2(df.nccon, is)];
+          for (int icp = df.nccon - 1; icp >= 1; --icp) f = f * transp(ic, jc, kc) + df.condco[Diff::v2(icp, is)];
+          ctrans[is - 1] = std::exp(f);
+        }
+        double c1 = 0.0, c2 = 0.0, c3 = 0.0;
+        for (int is = 1; is <= nspec; ++is) {
+          double f = yrhs[is - 1](ic, jc, kc) * ch.ovwmol[is - 1];
+          c1 = c1 + f * ctrans[is - 1];
+          c2 = c2 + f / ctrans[is - 1];
+          c3 = c3 + f;
+        }
+        c3 = 1.0 / c3;
+        c1 = c1 * c3;
+        c2 = c2 * c3;
+        store7(ic, jc, kc) = 0.5 * (c1 + 1.0 / c2);
+        wmomix(ic, jc, kc) = drhs(ic, jc, kc) * c3;
+      }
+    }
+    dfbydx(store7, store4); dfbydy(store7, store5); dfbydz(store7, store6);
+    zx(fxlcon, fxrcon, store4); zy(fylcon, fyrcon, store5); zz(fzlcon, fzrcon, store6);
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + (store4(ic, jc, kc) * store1(ic, jc, kc) +
+                                               store5(ic, jc, kc) * store2(ic, jc, kc) +
+                                               store6(ic, jc, kc) * store3(ic, jc, kc));
+    d2fdx2(trun, store1); d2fdy2(trun, store2); d2fdz2(trun, store3);
+    zx(fxlcon, fxrcon, store1); zy(fylcon, fyrcon, store2); zz(fzlcon, fzrcon, store3);
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc)) *
+                                                   store7(ic, jc, kc);
+    // species
+    chrate();
+    STD3 for (int is = 0; is < nspec; ++is) rrte[is](ic, jc, kc) = rate[is](ic, jc, kc);
+    STD3 { ucor(ic, jc, kc) = 0.0; vcor(ic, jc, kc) = 0.0; wcor(ic, jc, kc) = 0.0; vtmp(ic, jc, kc) = 0.0; }
+    BIG3 wtmp(ic, jc, kc) = 0.0;
+    for (int is = 0; is < nspec; ++is) {
+      Field& y = yrhs[is];
+      TRG3 y(ic, jc, kc) = y(ic, jc, kc) / drhs(ic, jc, kc);
+    }
+    for (int is = 1; is <= nspec; ++is) {
+      Field& y = yrhs[is - 1];
+      Field& rt = rate[is - 1];
+      STD3 rt(ic, jc, kc) = rt(ic, jc, kc) - 0.5 * y(ic, jc, kc) * divm(ic, jc, kc);
+      BIG3 store7(ic, jc, kc) = y(ic, jc, kc) * urhs(ic, jc, kc);
+      dfbydx(store7, store1);
+      BIG3 store7(ic, jc, kc) = y(ic, jc, kc) * vrhs(ic, jc, kc);
+      dfbydy(store7, store2);
+      BIG3 store7(ic, jc, kc) = y(ic, jc, kc) * wrhs(ic, jc, kc);
+      dfbydz(store7, store3);
+      STD3 rt(ic, jc, kc) = rt(ic, jc, kc) - 0.5 * (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc));
+      BIG3 store7(ic, jc, kc) = y(ic, jc, kc);
+      dfbydx(store7, store1); dfbydy(store7, store2); dfbydz(store7, store3);
+      STD3 rt(ic, jc, kc) = rt(ic, jc, kc) - 0.5 * (store1(ic, jc, kc) * urhs(ic, jc, kc) +
+                                                    store2(ic, jc, kc) * vrhs(ic, jc, kc) +
+                                                    store3(ic, jc, kc) * wrhs(ic, jc, kc));
+      BIG3 store7(ic, jc, kc) = transp(ic, jc, kc) * ch.olewis[is - 1];
+      if (df.flmavt) {
+        BIG3 {
+          double ctrans[NSPCMX];
+          for (int js = 1; js <= nspec; ++js) {
+            double f = df.diffco[Diff::d3(df.ncodif, js, is)];
+            for (int icp = df.ncodif - 1; icp >= 1; --icp)
+              f = f * transp(ic, jc, kc) + df.diffco[Diff::d3(icp, js, is)];
+            ctrans[js - 1] = std::exp(f) * df.pdifgb / prun(ic, jc, kc);
+          }
+          double c1 = 0.0, c2 = 0.0;
+          for (int js = 1; js <= nspec; ++js) {
+            double f = yrhs[js - 1](ic, jc, kc) + DFCTOL;
+            c1 = c1 + f;
+            c2 = c2 + f * ch.ovwmol[js - 1] / ctrans[js - 1];
+          }
+          double f = y(ic, jc, kc) + DFCTOL;
+          c1 = c1 - f;
+          c2 = c2 - f * ch.ovwmol[is - 1] / ctrans[is - 1];
+          c2 = c2 * wmomix(ic, jc, kc);
+          difmix(ic, jc, kc) = drhs(ic, jc, kc) * c1 / c2;
+          store7(ic, jc, kc) = difmix(ic, jc, kc);
+        }
+      }
+      STD3 {
+        ucor(ic, jc, kc) = ucor(ic, jc, kc) + store7(ic, jc, kc) * store1(ic, jc, kc);
+        vcor(ic, jc, kc) = vcor(ic, jc, kc) + store7(ic, jc, kc) * store2(ic, jc, kc);
+        wcor(ic, jc, kc) = wcor(ic, jc, kc) + store7(ic, jc, kc) * store3(ic, jc, kc);
+      }
+      {
+        int p = 1;
+        for (int q = 0; q < is - 1; ++q) p *= NTBASE;
+        const int icoef2 = p, icoef1 = p * NTBASE;
+        BIG3 {
+          int itint = 1 + (itndex(ic, jc, kc) % icoef1) / icoef2;
+          int k2 = Chem::c2(itint, is);
+          double f = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
+          for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) f = f * trun(ic, jc, kc) + ch.amasch[Chem::c3(icp, itint, is)];
+          utmp(ic, jc, kc) = ch.amasch[Chem::c3(ch.ncenth[k2], itint, is)] + f * trun(ic, jc, kc);
+          wtmp(ic, jc, kc) = wtmp(ic, jc, kc) + utmp(ic, jc, kc) * y(ic, jc, kc);
+        }
+      }
+      dfbydx(store7, store4); dfbydy(store7, store5); dfbydz(store7, store6);
+      zx(fxldif, fxrdif, store4); zy(fyldif, fyrdif, store5); zz(fzldif, fzrdif, store6);
+      STD3 {
+        double f = store4(ic, jc, kc) * store1(ic, jc, kc) + store5(ic, jc, kc) * store2(ic, jc, kc) +
+                   store6(ic, jc, kc) * store3(ic, jc, kc);
+        rt(ic, jc, kc) = rt(ic, jc, kc) + f;
+        vtmp(ic, jc, kc) = vtmp(ic, jc, kc) + f;
+      }
+      zx(fxladb, fxradb, store4); zy(fyladb, fyradb, store5); zz(fzladb, fzradb, store6);
+      STD3 {
+        double f = store4(ic, jc, kc) * store1(ic, jc, kc) + store5(ic, jc, kc) * store2(ic, jc, kc) +
+                   store6(ic, jc, kc) * store3(ic, jc, kc);
+        erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * utmp(ic, jc, kc);
+      }
+      dfbydx(utmp, store4); dfbydy(utmp, store5); dfbydz(utmp, store6);
+      zx(fxldif, fxrdif, store4); zy(fyldif, fyrdif, store5); zz(fzldif, fzrdif, store6);
+      zx(fxladb, fxradb, store4); zy(fyladb, fyradb, store5); zz(fzladb, fzradb, store6);
+      STD3 {
+        double f = store4(ic, jc, kc) * store1(ic, jc, kc) + store5(ic, jc, kc) * store2(ic, jc, kc) +
+                   store6(ic, jc, kc) * store3(ic, jc, kc);
+        erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * store7(ic, jc, kc);
+      }
+      STD3 store4(ic, jc, kc) = store7(ic, jc, kc);
+      BIG3 store7(ic, jc, kc) = y(ic, jc, kc);
+      d2fdx2(store7, store1); d2fdy2(store7, store2); d2fdz2(store7, store3);
+      zx(fxldif, fxrdif, store1); zy(fyldif, fyrdif, store2); zz(fzldif, fzrdif, store3);
+      STD3 {
+        double f = (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc)) * store4(ic, jc, kc);
+        rt(ic, jc, kc) = rt(ic, jc, kc) + f;
+        vtmp(ic, jc, kc) = vtmp(ic, jc, kc) + f;
+      }
+      zx(fxladb, fxradb, store1); zy(fyladb, fyradb, store2); zz(fzladb, fzradb, store3);
+      STD3 {
+        double f = (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc)) * store4(ic, jc, kc);
+        erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * utmp(ic, jc, kc);
+      }
+    }
+    dfbydx(wtmp, store1); dfbydy(wtmp, store2); dfbydz(wtmp, store3);
+    zx(fxldif, fxrdif, store1); zy(fyldif, fyrdif, store2); zz(fzldif, fzrdif, store3);
+    zx(fxladb, fxradb, store1); zy(fyladb, fyradb, store2); zz(fzladb, fzradb, store3);
+    STD3 store4(ic, jc, kc) = vtmp(ic, jc, kc);
+    zx(fxladb, fxradb, store4); zy(fyladb, fyradb, store4); zz(fzladb, fzradb, store4);
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) - wtmp(ic, jc, kc) * store4(ic, jc, kc) -
+                            store1(ic, jc, kc) * ucor(ic, jc, kc) - store2(ic, jc, kc) * vcor(ic, jc, kc) -
+                            store3(ic, jc, kc) * wcor(ic, jc, kc);
+    if (df.flmavt) {
+      BIG3 {
+        double ctrans[NSPCMX];
+        for (int is = 1; is <= nspec; ++is) {
+          double f = df.viscco[Diff::v2(df.ncovis, is)];
+          for (int icp = df.ncovis - 1; icp >= 1; --icp) f = f * transp(ic, jc, kc) + df.viscco[Diff::v2(icp, is)];
+          ctrans[is - 1] = std::exp(f);
+        }
+        double c1 = 0.0;
+        for (int is = 1; is <= nspec; ++is) {
+          double c2 = 0.0;
+          for (int js = 1; js <= nspec; ++js) {
+            double f = std::sqrt(ctrans[is - 1] / ctrans[js - 1]);
+            f = 1.0 + f * df.wilko2[Diff::d2(js, is)];
+            f = df.wilko1[Diff::d2(js, is)] * f * f;
+            c2 = c2 + yrhs[js - 1](ic, jc, kc) * ch.ovwmol[js - 1] * f;
+          }
+          double f = ctrans[is - 1] / c2;
+          c1 = c1 + yrhs[is - 1](ic, jc, kc) * ch.ovwmol[is - 1] * f;
+        }
+        difmix(ic, jc, kc) = c1;
+      }
+    }
+    for (int is = 1; is <= nspec; ++is) {
+      Field& y = yrhs[is - 1];
+      BIG3 store7(ic, jc, kc) = y(ic, jc, kc);
+      dfbydx(store7, store1); dfbydy(store7, store2); dfbydz(store7, store3);
+      zx(fxldif, fxrdif, store1); zy(fyldif, fyrdif, store2); zz(fzldif, fzrdif, store3);
+      Field& rt = rate[is - 1];
+      STD3 y(ic, jc, kc) = rt(ic, jc, kc) - y(ic, jc, kc) * vtmp(ic, jc, kc) - store1(ic, jc, kc) * ucor(ic, jc, kc) -
+                           store2(ic, jc, kc) * vcor(ic, jc, kc) - store3(ic, jc, kc) * wcor(ic, jc, kc);
+    }
+  }
+
+  // ---- RHSVEL: src/rhsvel.f:48-2318 ----
+  void rhsvel() {
+    BIG3 {
+      utmp(ic, jc, kc) = urhs(ic, jc, kc) / drhs(ic, jc, kc);
+      vtmp(ic, jc, kc) = vrhs(ic, jc, kc) / drhs(ic, jc, kc);
+      wtmp(ic, jc, kc) = wrhs(ic, jc, kc) / drhs(ic, jc, kc);
+    }
+    // (the 18 boundary-only transverse derivatives of rhsvel.f:66-335 feed
+    //  only NSCBC face arrays and are not needed for periodic boxes)
+    BIG3 store7(ic, jc, kc) = urhs(ic, jc, kc) * utmp(ic, jc, kc);
+    dfbydx(store7, store4);
+    BIG3 store7(ic, jc, kc) = urhs(ic, jc, kc) * vtmp(ic, jc, kc);
+    dfbydy(store7, store1); dfbydx(store7, store5);
+    STD3 store4(ic, jc, kc) = store4(ic, jc, kc) + store1(ic, jc, kc);
+    BIG3 store7(ic, jc, kc) = urhs(ic, jc, kc) * wtmp(ic, jc, kc);
+    dfbydz(store7, store1); dfbydx(store7, store6);
+    STD3 store4(ic, jc, kc) = store4(ic, jc, kc) + store1(ic, jc, kc);
+    BIG3 store7(ic, jc, kc) = vrhs(ic, jc, kc) * vtmp(ic, jc, kc);
+    dfbydy(store7, store1);
+    STD3 store5(ic, jc, kc) = store5(ic, jc, kc) + store1(ic, jc, kc);
+    BIG3 store7(ic, jc, kc) = vrhs(ic, jc, kc) * wtmp(ic, jc, kc);
+    dfbydz(store7, store1); dfbydy(store7, store2);
+    STD3 {
+      store5(ic, jc, kc) = store5(ic, jc, kc) + store1(ic, jc, kc);
+      store6(ic, jc, kc) = store6(ic, jc, kc) + store2(ic, jc, kc);
+    }
+    BIG3 store7(ic, jc, kc) = wrhs(ic, jc, kc) * wtmp(ic, jc, kc);
+    dfbydz(store7, store1);
+    STD3 store6(ic, jc, kc) = store6(ic, jc, kc) + store1(ic, jc, kc);
+    dfbydx(utmp, store1); dfbydy(vtmp, store2); dfbydz(wtmp, store3);
+    STD3 store7(ic, jc, kc) = store4(ic, jc, kc) + utmp(ic, jc, kc) * divm(ic, jc, kc);
+    STD3 store4(ic, jc, kc) = urhs(ic, jc, kc) * store1(ic, jc, kc);
+    STD3 urhs(ic, jc, kc) = -0.5 * (store4(ic, jc, kc) + store7(ic, jc, kc));
+    STD3 store7(ic, jc, kc) = store5(ic, jc, kc) + vtmp(ic, jc, kc) * divm(ic, jc, kc);
+    STD3 store5(ic, jc, kc) = vrhs(ic, jc, kc) * store2(ic, jc, kc);
+    STD3 vrhs(ic, jc, kc) = -0.5 * (store5(ic, jc, kc) + store7(ic, jc, kc));
+    STD3 store7(ic, jc, kc) = store6(ic, jc, kc) + wtmp(ic, jc, kc) * divm(ic, jc, kc);
+    STD3 store6(ic, jc, kc) = wrhs(ic, jc, kc) * store3(ic, jc, kc);
+    STD3 wrhs(ic, jc, kc) = -0.5 * (store6(ic, jc, kc) + store7(ic, jc, kc));
+    double prefer = prun(1, 1, 1);
+    BIG3 store7(ic, jc, kc) = prun(ic, jc, kc) - prefer;
+    dfbydx(store7, store4); dfbydy(store7, store5); dfbydz(store7, store6);
+    STD3 {
+      urhs(ic, jc, kc) = urhs(ic, jc, kc) - store4(ic, jc, kc);
+      vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - store5(ic, jc, kc);
+      wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - store6(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) - utmp(ic, jc, kc) * store4(ic, jc, kc) -
+                         vtmp(ic, jc, kc) * store5(ic, jc, kc) - wtmp(ic, jc, kc) * store6(ic, jc, kc);
+    }
+    STD3 erhs(ic, jc, kc) =
+        erhs(ic, jc, kc) - prun(ic, jc, kc) * (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc));
+    BIG3 transp(ic, jc, kc) = transp(ic, jc, kc) * PRANTL;
+    if (df.flmavt) { BIG3 transp(ic, jc, kc) = difmix(ic, jc, kc); }
+    const double THRD = 1.0 / 3.0, TTHD = 2.0 * THRD, FTHD = 2.0 * TTHD;
+    // TAUXX b,e,f
+    STD3 store6(ic, jc, kc) = store2(ic, jc, kc) + store3(ic, jc, kc);
+    STD3 store6(ic, jc, kc) = FTHD * store1(ic, jc, kc) - TTHD * store6(ic, jc, kc);
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + transp(ic, jc, kc) * store6(ic, jc, kc) * store1(ic, jc, kc);
+    dfbydx(transp, store4);
+    STD3 store6(ic, jc, kc) = store6(ic, jc, kc) * store4(ic, jc, kc);
+    zx(fxlvsn, fxrvsn, store6);
+    STD3 {
+      urhs(ic, jc, kc) = urhs(ic, jc, kc) + store6(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + utmp(ic, jc, kc) * store6(ic, jc, kc);
+    }
+    // TAUYY b,e,f
+    STD3 store6(ic, jc, kc) = store1(ic, jc, kc) + store3(ic, jc, kc);
+    STD3 store6(ic, jc, kc) = FTHD * store2(ic, jc, kc) - TTHD * store6(ic, jc, kc);
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + transp(ic, jc, kc) * store6(ic, jc, kc) * store2(ic, jc, kc);
+    dfbydy(transp, store5);
+    STD3 store6(ic, jc, kc) = store6(ic, jc, kc) * store5(ic, jc, kc);
+    zy(fylvsn, fyrvsn, store6);
+    STD3 {
+      vrhs(ic, jc, kc) = vrhs(ic, jc, kc) + store6(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + vtmp(ic, jc, kc) * store6(ic, jc, kc);
+    }
+    // TAUZZ b,e,f
+    STD3 store1(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc);
+    STD3 store1(ic, jc, kc) = FTHD * store3(ic, jc, kc) - TTHD * store1(ic, jc, kc);
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + transp(ic, jc, kc) * store1(ic, jc, kc) * store3(ic, jc, kc);
+    dfbydz(transp, store6);
+    STD3 store1(ic, jc, kc) = store1(ic, jc, kc) * store6(ic, jc, kc);
+    zz(fzlvsn, fzrvsn, store1);
+    STD3 {
+      wrhs(ic, jc, kc) = wrhs(ic, jc, kc) + store1(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + wtmp(ic, jc, kc) * store1(ic, jc, kc);
+    }
+    // ---- xy cross terms ----
+    dfbydy(utmp, store1);
+    STD3 urhs(ic, jc, kc) = urhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * vtmp(ic, jc, kc) * store1(ic, jc, kc);
+    dfbydx(vtmp, store2);
+    STD3 vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * utmp(ic, jc, kc) * store2(ic, jc, kc);
+    STD3 store7(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc);
+    d2fdxy(utmp, store1); d2fdxy(vtmp, store2);
+    cross_terms(urhs, utmp, vrhs, vtmp, fxlvsn, fxrvsn, 0, fylvsn, fyrvsn, 1);
+    d2fdy2(utmp, store3);
+    STD3 store3(ic, jc, kc) = store3(ic, jc, kc) + store2(ic, jc, kc);
+    STD3 store3(ic, jc, kc) = transp(ic, jc, kc) * store3(ic, jc, kc) + store7(ic, jc, kc) * store5(ic, jc, kc);
+    zy(fylvst, fyrvst, store3);
+    STD3 {
+      urhs(ic, jc, kc) = urhs(ic, jc, kc) + store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + utmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+    d2fdx2(vtmp, store3);
+    STD3 store3(ic, jc, kc) = store3(ic, jc, kc) + store1(ic, jc, kc);
+    STD3 store3(ic, jc, kc) = transp(ic, jc, kc) * store3(ic, jc, kc) + store7(ic, jc, kc) * store4(ic, jc, kc);
+    zx(fxlvst, fxrvst, store3);
+    STD3 {
+      vrhs(ic, jc, kc) = vrhs(ic, jc, kc) + store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + vtmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + transp(ic, jc, kc) * store7(ic, jc, kc) * store7(ic, jc, kc);
+    // ---- xz cross terms ----
+    dfbydz(utmp, store1);
+    STD3 urhs(ic, jc, kc) = urhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * wtmp(ic, jc, kc) * store1(ic, jc, kc);
+    dfbydx(wtmp, store2);
+    STD3 wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * utmp(ic, jc, kc) * store2(ic, jc, kc);
+    STD3 store7(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc);
+    d2fdxz(utmp, store1); d2fdxz(wtmp, store2);
+    cross_terms(urhs, utmp, wrhs, wtmp, fxlvsn, fxrvsn, 0, fzlvsn, fzrvsn, 2);
+    d2fdz2(utmp, store3);
+    STD3 store3(ic, jc, kc) = store3(ic, jc, kc) + store2(ic, jc, kc);
+    STD3 store3(ic, jc, kc) = transp(ic, jc, kc) * store3(ic, jc, kc) + store7(ic, jc, kc) * store6(ic, jc, kc);
+    zz(fzlvst, fzrvst, store3);
+    STD3 {
+      urhs(ic, jc, kc) = urhs(ic, jc, kc) + store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + utmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+    d2fdx2(wtmp, store3);
+    STD3 store3(ic, jc, kc) = store3(ic, jc, kc) + store1(ic, jc, kc);
+    STD3 store3(ic, jc, kc) = transp(ic, jc, kc) * store3(ic, jc, kc) + store7(ic, jc, kc) * store4(ic, jc, kc);
+    zx(fxlvst, fxrvst, store3);
+    STD3 {
+      wrhs(ic, jc, kc) = wrhs(ic, jc, kc) + store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + wtmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + transp(ic, jc, kc) * store7(ic, jc, kc) * store7(ic, jc, kc);
+    // ---- yz cross terms ----
+    dfbydz(vtmp, store1);
+    STD3 vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * wtmp(ic, jc, kc) * store1(ic, jc, kc);
+    dfbydy(wtmp, store2);
+    STD3 wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * vtmp(ic, jc, kc) * store2(ic, jc, kc);
+    STD3 store7(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc);
+    d2fdyz(vtmp, store1); d2fdyz(wtmp, store2);
+    cross_terms(vrhs, vtmp, wrhs, wtmp, fylvsn, fyrvsn, 1, fzlvsn, fzrvsn, 2);
+    d2fdz2(vtmp, store3);
+    STD3 store3(ic, jc, kc) = store3(ic, jc, kc) + store2(ic, jc, kc);
+    STD3 store3(ic, jc, kc) = transp(ic, jc, kc) * store3(ic, jc, kc) + store7(ic, jc, kc) * store6(ic, jc, kc);
+    zz(fzlvst, fzrvst, store3);
+    STD3 {
+      vrhs(ic, jc, kc) = vrhs(ic, jc, kc) + store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + vtmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+    d2fdy2(wtmp, store3);
+    STD3 store3(ic, jc, kc) = store3(ic, jc, kc) + store1(ic, jc, kc);
+    STD3 store3(ic, jc, kc) = transp(ic, jc, kc) * store3(ic, jc, kc) + store7(ic, jc, kc) * store5(ic, jc, kc);
+    zy(fylvst, fyrvst, store3);
+    STD3 {
+      wrhs(ic, jc, kc) = wrhs(ic, jc, kc) + store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + wtmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+    STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + transp(ic, jc, kc) * store7(ic, jc, kc) * store7(ic, jc, kc);
+    // ---- normal second derivatives ----
+    d2fdx2(utmp, store1); d2fdy2(vtmp, store2); d2fdz2(wtmp, store3);
+    zx(fxlvsn, fxrvsn, store1); zy(fylvsn, fyrvsn, store2); zz(fzlvsn, fzrvsn, store3);
+    STD3 {
+      double f = transp(ic, jc, kc) * FTHD * store1(ic, jc, kc);
+      urhs(ic, jc, kc) = urhs(ic, jc, kc) + f;
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * utmp(ic, jc, kc);
+    }
+    STD3 {
+      double f = transp(ic, jc, kc) * FTHD * store2(ic, jc, kc);
+      vrhs(ic, jc, kc) = vrhs(ic, jc, kc) + f;
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * vtmp(ic, jc, kc);
+    }
+    STD3 {
+      double f = transp(ic, jc, kc) * FTHD * store3(ic, jc, kc);
+      wrhs(ic, jc, kc) = wrhs(ic, jc, kc) + f;
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * wtmp(ic, jc, kc);
+    }
+    STD3 drhs(ic, jc, kc) = -divm(ic, jc, kc);
+  }
+  // TAUaa,a c / TAUbb,b c pair with the mixed derivatives in store1/store2
+  // (rhsvel.f:1340-1395 pattern): a-eq gets -2/3 mu d2(b)/da db, b-eq gets
+  // -2/3 mu d2(a)/da db.
+  void cross_terms(Field& arhs, Field& atmp, Field& brhs, Field& btmp, bool zal, bool zar, int da, bool zbl,
+                   bool zbr, int db) {
+    const double THRD = 1.0 / 3.0, TTHD = 2.0 * THRD;
+    STD3 store3(ic, jc, kc) = TTHD * transp(ic, jc, kc) * store2(ic, jc, kc);
+    if (zal) zero_plane(store3, da, false);
+    if (zar) zero_plane(store3, da, true);
+    STD3 {
+      arhs(ic, jc, kc) = arhs(ic, jc, kc) - store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) - atmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+    STD3 store3(ic, jc, kc) = TTHD * transp(ic, jc, kc) * store1(ic, jc, kc);
+    if (zbl) zero_plane(store3, db, false);
+    if (zbr) zero_plane(store3, db, true);
+    STD3 {
+      brhs(ic, jc, kc) = brhs(ic, jc, kc) - store3(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) - btmp(ic, jc, kc) * store3(ic, jc, kc);
+    }
+  }
+
+  // ---- LINCOM / FINCOM: src/lincom.f:53-169, src/fincom.f:54-168 ----
+  void rkupdate(Field& run, Field& rhs, Field& err, int irk, bool last) {
+    STD3 {
+      err(ic, jc, kc) = err(ic, jc, kc) + rkerr[irk - 1] * rhs(ic, jc, kc);
+      if (!last) {
+        double f = run(ic, jc, kc);
+        run(ic, jc, kc) = f + rklhs[irk - 1] * rhs(ic, jc, kc);
+        rhs(ic, jc, kc) = f + rkrhs[irk - 1] * rhs(ic, jc, kc);
+      } else {
+        run(ic, jc, kc) = run(ic, jc, kc) + rklhs[irk - 1] * rhs(ic, jc, kc);
+        rhs(ic, jc, kc) = run(ic, jc, kc);
+      }
+    }
+  }
+  void lincom(int irk, bool last) {
+    rkupdate(drun, drhs, derr, irk, last);
+    rkupdate(urun, urhs, uerr, irk, last);
+    rkupdate(vrun, vrhs, verr, irk, last);
+    rkupdate(wrun, wrhs, werr, irk, last);
+    rkupdate(erun, erhs, eerr, irk, last);
+    for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last);
+  }
+
+  void rhs() {
+    parfer();
+    rhscal();
+    rhsvel();
+  }
+  // One time step: senga2.f:106-159 (periodic: BOUNDT/BOUNDS/BOUNTT are
+  // no-ops; FLTREM is commented out at senga2.f:178; fixed dt, ADAPTT idle).
+  void step() {
+    for (int irk = 1; irk <= 5; ++irk) {
+      rhs();
+      lincom(irk, irk == 5);
+    }
+  }
+};
+
+}  // namespace orc
+
+// ===========================================================================
+// C interface used by the Python test harness (ctypes).
+extern "C" {
+
+struct oracle_config {
+  int nx, ny, nz;
+  double xgdlen, ygdlen, zgdlen;
+  int nend[6];
+  int flmavt;
+  double tstep;
+  const char* chem_path;
+  const char* diff_path;
+};
+
+static thread_local std::string g_err;
+
+const char* oracle_last_error() { return g_err.c_str(); }
+
+void* oracle_create(const oracle_config* c) {
+  try {
+    auto* o = new orc::Oracle();
+    orc::Config cf{};
+    cf.nx = c->nx; cf.ny = c->ny; cf.nz = c->nz;
+    cf.xgdlen = c->xgdlen; cf.ygdlen = c->ygdlen; cf.zgdlen = c->zgdlen;
+    for (int i = 0; i < 6; ++i) cf.nend[i] = c->nend[i];
+    cf.flmavt = c->flmavt;
+    cf.tstep = c->tstep;
+    o->init(cf, c->chem_path, c->diff_path ? c->diff_path : "");
+    return o;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+
+void oracle_destroy(void* h) { delete static_cast<orc::Oracle*>(h); }
+
+int oracle_nspec(void* h) { return static_cast<orc::Oracle*>(h)->nspec; }
+
+// Interior arrays, Fortran order (x fastest). fields = [rho, rhou, rhov, rhow,
+// rhoE, rhoY_1..rhoY_n], each nx*ny*nz. Both registers (xRUN and xRHS) are
+// set to the given conserved state, as at the start of a time step.
+int oracle_set_state(void* h, const double* fields, const double* t, const int32_t* itn) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  const size_t n = (size_t)o->nx * o->ny * o->nz;
+  std::vector<orc::Field*> run = {&o->drun, &o->urun, &o->vrun, &o->wrun, &o->erun};
+  std::vector<orc::Field*> rhs = {&o->drhs, &o->urhs, &o->vrhs, &o->wrhs, &o->erhs};
+  for (int s = 0; s < o->nspec; ++s) { run.push_back(&o->yrun[s]); rhs.push_back(&o->yrhs[s]); }
+  for (size_t f = 0; f < run.size(); ++f) {
+    const double* src = fields + f * n;
+    for (int k = 1; k <= o->nz; ++k)
+      for (int j = 1; j <= o->ny; ++j)
+        for (int i = 1; i <= o->nx; ++i) {
+          double v = src[(size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1))];
+          (*run[f])(i, j, k) = v;
+          (*rhs[f])(i, j, k) = v;
+        }
+  }
+  // T and the interval index live on the halo-extended range; fill the halo
+  // with the periodic image (what the reference's own initialisation yields).
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j)
+      for (int i = 1; i <= o->nx; ++i) {
+        size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
+        o->trun(i, j, k) = t[q];
+        o->itndex(i, j, k) = itn[q];
+      }
+  auto wrap = [&](int a, int n_) { return ((a - 1) % n_ + n_) % n_ + 1; };
+  for (int k = o->kstab; k <= o->kstob; ++k)
+    for (int j = o->jstab; j <= o->jstob; ++j)
+      for (int i = o->istab; i <= o->istob; ++i) {
+        int ii = wrap(i, o->nx), jj = wrap(j, o->ny), kk = wrap(k, o->nz);
+        o->trun(i, j, k) = o->trun(ii, jj, kk);
+        o->itndex(i, j, k) = o->itndex(ii, jj, kk);
+      }
+  return 0;
+}
+
+int oracle_get_state(void* h, double* fields, double* t, int32_t* itn) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  const size_t n = (size_t)o->nx * o->ny * o->nz;
+  std::vector<orc::Field*> run = {&o->drun, &o->urun, &o->vrun, &o->wrun, &o->erun};
+  for (int s = 0; s < o->nspec; ++s) run.push_back(&o->yrun[s]);
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j)
+      for (int i = 1; i <= o->nx; ++i) {
+        size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
+        for (size_t f = 0; f < run.size(); ++f) fields[f * n + q] = (*run[f])(i, j, k);
+        if (t) t[q] = o->trun(i, j, k);
+        if (itn) itn[q] = o->itndex(i, j, k);
+      }
+  return 0;
+}
+
+int oracle_step(void* h, int nsteps) {
+  try {
+    auto* o = static_cast<orc::Oracle*>(h);
+    for (int s = 0; s < nsteps; ++s) o->step();
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// One RHS evaluation of the U register (PARFER, RHSCAL, RHSVEL) without the
+// RK update; writes R(U) for the Nc fields plus T and p after TEMPER.
+int oracle_rhs(void* h, double* rhs_out, double* t_out, double* p_out) {
+  try {
+    auto* o = static_cast<orc::Oracle*>(h);
+    o->rhs();
+    const size_t n = (size_t)o->nx * o->ny * o->nz;
+    std::vector<orc::Field*> rf = {&o->drhs, &o->urhs, &o->vrhs, &o->wrhs, &o->erhs};
+    for (int s = 0; s < o->nspec; ++s) rf.push_back(&o->yrhs[s]);
+    for (int k = 1; k <= o->nz; ++k)
+      for (int j = 1; j <= o->ny; ++j)
+        for (int i = 1; i <= o->nx; ++i) {
+          size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
+          for (size_t f = 0; f < rf.size(); ++f) rhs_out[f * n + q] = (*rf[f])(i, j, k);
+          if (t_out) t_out[q] = o->trun(i, j, k);
+          if (p_out) p_out[q] = o->prun(i, j, k);
+        }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// Derivative of an interior field (periodic directions wrapped by the halo
+// copy). kind: 0 dx 1 dy 2 dz 3 dxx 4 dyy 5 dzz 6 dxy 7 dxz 8 dyz.
+int oracle_deriv(void* h, int kind, const double* f, double* out) {
+  try {
+    auto* o = static_cast<orc::Oracle*>(h);
+    orc::Field& F = o->store7;
+    for (int k = 1; k <= o->nz; ++k)
+      for (int j = 1; j <= o->ny; ++j)
+        for (int i = 1; i <= o->nx; ++i)
+          F(i, j, k) = f[(size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1))];
+    o->halo_periodic(F);
+    orc::Field& D = o->store1;
+    switch (kind) {
+      case 0: o->dfbydx(F, D); break;
+      case 1: o->dfbydy(F, D); break;
+      case 2: o->dfbydz(F, D); break;
+      case 3: o->d2fdx2(F, D); break;
+      case 4: o->d2fdy2(F, D); break;
+      case 5: o->d2fdz2(F, D); break;
+      case 6: o->d2fdxy(F, D); break;
+      case 7: o->d2fdxz(F, D); break;
+      case 8: o->d2fdyz(F, D); break;
+      default: return 2;
+    }
+    for (int k = 1; k <= o->nz; ++k)
+      for (int j = 1; j <= o->ny; ++j)
+        for (int i = 1; i <= o->nx; ++i)
+          out[(size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1))] = D(i, j, k);
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// TEMPER then CHRATE on the current U register (src/rhscal.f:61,822): RATE
+// for nspec interior arrays, with rho*Y in YRHS as in the reference.
+int oracle_chrate(void* h, double* rate_out) {
+  try {
+    auto* o = static_cast<orc::Oracle*>(h);
+    o->parfer();
+    o->temper();
+    o->chrate();
+    const size_t n = (size_t)o->nx * o->ny * o->nz;
+    for (int k = 1; k <= o->nz; ++k)
+      for (int j = 1; j <= o->ny; ++j)
+        for (int i = 1; i <= o->nx; ++i) {
+          size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
+          for (int s = 0; s < o->nspec; ++s) rate_out[s * n + q] = o->rate[s](i, j, k);
+        }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// Table access for the parity tests of the host-side table builder.
+int oracle_chem_scalar(void* h, const char* name, double* out) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  std::string n(name);
+  if (n == "alamda") *out = o->ch.alamda;
+  else if (n == "prefgb") *out = o->ch.prefgb;
+  else if (n == "deltax") *out = o->fd.deltax;
+  else return 1;
+  return 0;
+}
+
+}  // extern "C"

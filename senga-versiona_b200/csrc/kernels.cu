@@ -1,0 +1,639 @@
+// Per-substage kernels of the B200 RHS + RK path.
+//
+//   k_thermo      pointwise: TEMPER (src/temper.f:58-219), transport
+//                 properties (src/rhscal.f:515-571, 1292-1340, 3854-3885;
+//                 src/rhsvel.f:933-952), species enthalpy (rhscal.f:1444-1466)
+//                 and CHRATE (src/chrate.f:146-741), fused per grid point.
+//   k_flow        stencil: continuity, momentum, energy convection, heat
+//                 conduction, pressure and viscous work (rhscal.f:141-793,
+//                 rhsvel.f:48-2318).
+//   k_species_a   stencil: species convection/diffusion and the enthalpy
+//                 flux terms of the energy equation (rhscal.f:1030-1955).
+//   k_species_b   stencil: diffusion-correction terms (rhscal.f:3782-3938)
+//                 fused with the 2N-storage RK update (src/lincom.f:53-169,
+//                 src/fincom.f:54-168).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "senga_internal.h"
+#include "stencil.cuh"
+
+namespace senga {
+
+namespace {
+constexpr double kPrantl = 7.0e-1;  // src/com_senga2.h:115
+constexpr double kRlamda = 7.0e-1;  // :113
+constexpr double kThrd = 1.0 / 3.0, kTthd = 2.0 * kThrd, kFthd = 2.0 * kTthd;
+constexpr double kYsmall = 1.0e-30, kYdenom = 1.0e-15;  // src/chrate.f:40
+constexpr double kDfctol = 1.0e-12;                     // src/com_senga2.h:187
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ int tint_of(int32_t itn, int s) { return (itn >> (2 * s)) & 3; }
+
+// Select-by-index update of a register array (keeps the array in registers
+// when the index comes from a table).
+template <int NSM>
+__device__ __forceinline__ void add_at(double (&a)[NSM], int k, double v) {
+#pragma unroll
+  for (int s = 0; s < NSM; ++s)
+    if (s == k) a[s] += v;
+}
+template <int NSM>
+__device__ __forceinline__ double get_at(const double (&a)[NSM], int k) {
+  double r = 0.0;
+#pragma unroll
+  for (int s = 0; s < NSM; ++s)
+    if (s == k) r = a[s];
+  return r;
+}
+
+// -------------------------------------------------------------------------
+// CHRATE for one point. ry: rho*Y_k, T, itn (updated interval index).
+// Gibbs functions and log T are hoisted out of the step loop: the reference
+// evaluates the same expressions per step, so the values are identical.
+template <int NSM>
+__device__ void chrate_point(const senga_chem* __restrict__ C, int nspec, const double (&ry)[NSM], double T,
+                             int32_t itn, double (&rate)[NSM]) {
+  const double lnT = log(T);
+  const double ovT = 1.0 / T;
+  double gib[NSM];
+#pragma unroll
+  for (int s = 0; s < NSM; ++s) {
+    rate[s] = 0.0;
+    gib[s] = 0.0;
+    if (s < nspec && C->ngibb > 0) {
+      const int it = tint_of(itn, s);
+      const int np = C->ncpoly[s][it];
+      const double* gb = C->amolgb[s][it];
+      double g = gb[np - 1];
+      for (int icp = np - 1; icp >= 1; --icp) g = gb[icp - 1] + g * T;
+      gib[s] = gb[C->ncenth[s][it] - 1] / T - gb[C->ncenpy[s][it] - 1] * lnT - g;
+    }
+  }
+  double s3 = 0.0;
+  for (int st = 0; st < C->nstep; ++st) {
+    bool flthrd = true;
+    const int ib = C->mblist[st];
+    if (ib != 0) {
+      s3 = 0.0;
+#pragma unroll
+      for (int s = 0; s < NSM; ++s)
+        if (s < nspec) s3 += ry[s] * (C->ovwmol[s] * C->effy3b[ib - 1][s]);
+    }
+    double s2 = C->rparam[st][0] + C->rparam[st][1] * lnT - C->rparam[st][2] * ovT;
+    double s1 = exp(s2);
+    if (C->mllist[st] != 0) {
+      const double* rl = C->rclind[C->mllist[st] - 1];
+      const double flcnst = (double)(float)rl[3];  // implicit REAL in the reference
+      const double s4 = exp(rl[0] + rl[1] * lnT - rl[2] * ovT);
+      const double pr = s3 * s4 / s1;
+      s1 = s1 * (flcnst * pr / (1.0 + pr));
+      s2 = log(s1);
+      flthrd = false;
+    }
+    if (C->mtlist[st] != 0) {
+      const double* rt = C->rctroe[C->mtlist[st] - 1];
+      const double talpha = (double)(float)rt[3];
+      const double cf1 = (double)(float)rt[7], cf2 = (double)(float)rt[8];
+      const double en1 = (double)(float)rt[9], en2 = (double)(float)rt[10], dtc = (double)(float)rt[11];
+      const double s4 = exp(rt[0] + rt[1] * lnT - rt[2] * ovT);
+      const double pr = s3 * s4 / s1;
+      double ftc = (1.0 - talpha) * exp(T * rt[6]) + talpha * exp(T * rt[4]) + exp(-rt[5] / T);
+      ftc = log10(ftc);
+      const double cfa = cf1 + cf2 * ftc, enf = en1 + en2 * ftc;
+      double fn = log10(pr) + cfa;
+      fn = fn / (enf - dtc * fn);
+      fn = 1.0 + fn * fn;
+      const double fbroad = exp((ftc / fn) * 2.302585092994046);
+      s1 = s1 * (fbroad * pr / (1.0 + pr));
+      s2 = log(s1);
+      flthrd = false;
+    }
+    if (C->mslist[st] != 0) {
+      const double* rs = C->rcsrif[C->mslist[st] - 1];
+      const double s4 = exp(rs[0] + rs[1] * lnT - rs[2] * ovT);
+      const double pr = s3 * s4 / s1;
+      double fb = rs[3] * exp(rs[4] / T) + exp(T * rs[5]);
+      const double fn = 1.0 / (1.0 + log10(log10(pr)));
+      fb = rs[6] * exp(fn * log(fb));
+      s1 = s1 * (fb * pr / (1.0 + pr));
+      s2 = log(s1);
+      flthrd = false;
+    }
+    for (int l = 0; l < C->nrslen[st]; ++l) {
+      const int s = C->nrspec[st][l] - 1;
+      s1 = s1 * fmax(get_at(ry, s) * C->ovwmol[s], 0.0);
+    }
+    for (int l = 0; l < C->nrclen[st]; ++l) {
+      const int s = C->nrcpec[st][l] - 1;
+      double fn = fmax(get_at(ry, s) * C->ovwmol[s], kYsmall);
+      fn = exp(C->crspec[st][l] * log(fn));
+      s1 = s1 * (fn / (1.0 + kYdenom * fn));
+    }
+    if (C->mglist[st] != 0) {
+      for (int l = 0; l < C->nsslen[st]; ++l) s2 = s2 + C->diffmu[st][l] * get_at(gib, C->nsspec[st][l] - 1);
+      s2 = exp(s2);
+      for (int l = 0; l < C->npslen[st]; ++l) {
+        const int s = C->npspec[st][l] - 1;
+        s2 = s2 * fmax(get_at(ry, s) * C->ovwmol[s], 0.0);
+      }
+      for (int l = 0; l < C->npclen[st]; ++l) {
+        const int s = C->npcpec[st][l] - 1;
+        double fn = fmax(get_at(ry, s) * C->ovwmol[s], kYsmall);
+        fn = exp(C->cpspec[st][l] * log(fn));
+        s2 = s2 * (fn / (1.0 + kYdenom * fn));
+      }
+      s1 = s1 - s2;
+    }
+    if (ib != 0 && flthrd) s1 = s1 * s3;
+    for (int l = 0; l < C->nsslen[st]; ++l) add_at(rate, C->nsspec[st][l] - 1, s1 * C->diffmw[st][l]);
+  }
+}
+
+// -------------------------------------------------------------------------
+template <int NSM, bool MAVT, bool CHEM>
+__global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, const senga_chem* __restrict__ C,
+                                                   const senga_diff* __restrict__ Dt, int nspec) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  const int64_t n = g.n;
+  const double* U = f.uin;
+  const double rho = U[q], ru = U[n + q], rv = U[2 * n + q], rw = U[3 * n + q], re = U[4 * n + q];
+  double ry[NSM];
+#pragma unroll
+  for (int s = 0; s < NSM; ++s) ry[s] = s < nspec ? U[(5 + s) * n + q] : 0.0;
+
+  // ---- TEMPER ----
+  const double ukuk = (ru * ru + rv * rv + rw * rw) / rho;
+  double tc[6], td[6];
+  tc[0] = 0.5 * ukuk - re;
+#pragma unroll
+  for (int i = 1; i < 6; ++i) tc[i] = td[i] = 0.0;
+  double rmix = 0.0;
+  const int32_t itn0 = f.itn[q];
+#pragma unroll
+  for (int s = 0; s < NSM; ++s) {
+    if (s >= nspec) continue;
+    const int it = tint_of(itn0, s);
+    const double y = ry[s];
+    const int np = C->ncpoly[s][it];
+    tc[0] = tc[0] + y * C->amascp[s][it][C->ncenth[s][it] - 1];
+    tc[1] = tc[1] + y * C->amasct[s][it][0];
+    td[1] = tc[1];
+#pragma unroll
+    for (int icp = 2; icp <= 5; ++icp)
+      if (icp <= np) {
+        tc[icp] = tc[icp] + y * C->amasct[s][it][icp - 1];
+        td[icp] = td[icp] + y * C->amascp[s][it][icp - 1];
+      }
+    rmix = rmix + y * C->rgspec[s];
+  }
+  const double toltmp = (double)1.0e-10f;  // TOLTMP is a single-precision literal
+  double T = f.t[q];
+  int iters = 1;
+  for (;;) {
+    double tf = tc[5], tdp = td[5];
+#pragma unroll
+    for (int icp = 4; icp >= 1; --icp) {
+      tf = tc[icp] + tf * T;
+      tdp = td[icp] + tdp * T;
+    }
+    tf = tc[0] + tf * T;
+    const double del = -tf / tdp;
+    if (fabs(del) > toltmp) {
+      if (iters < 100) {
+        T = T + del;
+        ++iters;
+        continue;
+      }
+      atomicOr(f.status, 1u);  // reported through senga_get_status
+    }
+    break;
+  }
+  int32_t itn = 0;
+  double cpm = 0.0;
+#pragma unroll
+  for (int s = 0; s < NSM; ++s) {
+    if (s >= nspec) continue;
+    int it = 0;
+    while (T > C->tinthi[s][it] && it + 1 < C->ntint[s]) ++it;
+    itn += it << (2 * s);
+    const int np = C->ncpoly[s][it];
+    const double* cp = C->amascp[s][it];
+    double c = cp[np - 1];
+    for (int icp = np - 1; icp >= 1; --icp) c = c * T + cp[icp - 1];
+    cpm = cpm + ry[s] * c;
+  }
+  cpm = cpm / rho;
+  const double p = T * rmix;
+  f.t[q] = T;
+  f.itn[q] = itn;
+  f.p[q] = p;
+
+  // ---- primitive variables ----
+  const double ovr = 1.0 / rho;
+  double y[NSM];
+#pragma unroll
+  for (int s = 0; s < NSM; ++s) {
+    y[s] = ry[s] / rho;
+    if (s < nspec) f.y[s * n + q] = y[s];
+  }
+  f.vel[q] = ru / rho;
+  f.vel[n + q] = rv / rho;
+  f.vel[2 * n + q] = rw / rho;
+  f.e[q] = re / rho;
+  (void)ovr;
+
+  // ---- transport properties ----
+  if (!MAVT) {
+    const double lcp = C->alamda * exp(kRlamda * log(T));
+    f.lam[q] = lcp * cpm;
+    f.lcp[q] = lcp;
+    f.mu[q] = lcp * kPrantl;
+#pragma unroll
+    for (int s = 0; s < NSM; ++s)
+      if (s < nspec) f.rd[s * n + q] = lcp * C->olewis[s];
+  } else {
+    const double lt = log(T / Dt->tdifgb);
+    // conductivity combination (rhscal.f:531-571), with rho*Y
+    double c1 = 0.0, c2 = 0.0, c3 = 0.0;
+#pragma unroll
+    for (int s = 0; s < NSM; ++s) {
+      if (s >= nspec) continue;
+      double fp = Dt->condco[s][Dt->ncocon - 1];
+      for (int icp = Dt->ncocon - 1; icp >= 1; --icp) fp = fp * lt + Dt->condco[s][icp - 1];
+      const double lk = exp(fp);
+      const double fm = ry[s] * C->ovwmol[s];
+      c1 = c1 + fm * lk;
+      c2 = c2 + fm / lk;
+      c3 = c3 + fm;
+    }
+    c3 = 1.0 / c3;
+    c1 = c1 * c3;
+    c2 = c2 * c3;
+    f.lam[q] = 0.5 * (c1 + 1.0 / c2);
+    const double wmix = rho * c3;
+    // mixture-averaged diffusivity (rhscal.f:1311-1340): each D_jk is
+    // evaluated once per unordered pair (DIFFCO is symmetric).
+    double sumy = 0.0;
+    double den[NSM];
+#pragma unroll
+    for (int s = 0; s < NSM; ++s) {
+      den[s] = 0.0;
+      if (s < nspec) sumy += y[s] + kDfctol;
+    }
+    const double povr = p / Dt->pdifgb;
+#pragma unroll
+    for (int s = 0; s < NSM; ++s) {
+#pragma unroll
+      for (int t = s + 1; t < NSM; ++t) {
+        if (t >= nspec) continue;
+        const double* dc = Dt->diffco[s][t];
+        double fp = dc[Dt->ncodif - 1];
+        for (int icp = Dt->ncodif - 1; icp >= 1; --icp) fp = fp * lt + dc[icp - 1];
+        const double inv = exp(-fp) * povr;  // 1/D_st
+        den[s] += (y[t] + kDfctol) * C->ovwmol[t] * inv;
+        den[t] += (y[s] + kDfctol) * C->ovwmol[s] * inv;
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < NSM; ++s)
+      if (s < nspec) f.rd[s * n + q] = rho * (sumy - (y[s] + kDfctol)) / (den[s] * wmix);
+    // Wilke viscosity (rhscal.f:3854-3885): sqrt(mu_i/mu_j) = sqrt(mu_i)/sqrt(mu_j)
+    double mk[NSM], sq[NSM], rq[NSM];
+#pragma unroll
+    for (int s = 0; s < NSM; ++s) {
+      mk[s] = 1.0;
+      if (s < nspec) {
+        double fp = Dt->viscco[s][Dt->ncovis - 1];
+        for (int icp = Dt->ncovis - 1; icp >= 1; --icp) fp = fp * lt + Dt->viscco[s][icp - 1];
+        mk[s] = exp(fp);
+      }
+      sq[s] = sqrt(mk[s]);
+      rq[s] = 1.0 / sq[s];
+    }
+    double mu = 0.0;
+#pragma unroll
+    for (int s = 0; s < NSM; ++s) {
+      if (s >= nspec) continue;
+      double cc = 0.0;
+#pragma unroll
+      for (int t = 0; t < NSM; ++t) {
+        if (t >= nspec) continue;
+        double fw = 1.0 + sq[s] * rq[t] * Dt->wilko2[s][t];
+        fw = Dt->wilko1[s][t] * fw * fw;
+        cc = cc + y[t] * C->ovwmol[t] * fw;
+      }
+      mu = mu + y[s] * C->ovwmol[s] * (mk[s] / cc);
+    }
+    f.mu[q] = mu;
+  }
+
+  // ---- species enthalpy and mixture enthalpy (new interval index) ----
+  double hm = 0.0;
+#pragma unroll
+  for (int s = 0; s < NSM; ++s) {
+    if (s >= nspec) continue;
+    const int it = tint_of(itn, s);
+    const int np = C->ncpoly[s][it];
+    const double* ch = C->amasch[s][it];
+    double h = ch[np - 1];
+    for (int icp = np - 1; icp >= 1; --icp) h = h * T + ch[icp - 1];
+    h = ch[C->ncenth[s][it] - 1] + h * T;
+    f.h[s * n + q] = h;
+    hm = hm + h * y[s];
+  }
+  f.hmix[q] = hm;
+
+  // ---- CHRATE ----
+  if (CHEM) {
+    double rate[NSM];
+    chrate_point<NSM>(C, nspec, ry, T, itn, rate);
+#pragma unroll
+    for (int s = 0; s < NSM; ++s)
+      if (s < nspec) f.wdot[s * n + q] = rate[s];
+  }
+}
+
+// -------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_flow(Geo g, Fields f) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  const Pt pt = point_of(g, q);
+  const int64_t n = g.n;
+  const double* U = f.uin;
+  const Ld rho{U}, ru{U + n}, rv{U + 2 * n}, rw{U + 3 * n};
+  const Ld u{f.vel}, v{f.vel + n}, w{f.vel + 2 * n}, E{f.e}, T{f.t}, lam{f.lam}, mu{f.mu};
+  const double ruq = ru(q), rvq = rv(q), rwq = rw(q), uq = u(q), vq = v(q), wq = w(q), rhq = rho(q);
+
+  // mass-flux divergence
+  const double divm = D1<0>(g, pt, ru) + D1<1>(g, pt, rv) + D1<2>(g, pt, rw);
+  // energy convection, skew-symmetric
+  double s4 = E(q) * divm + D1<0>(g, pt, LdMul{f.e, U + n}) + D1<1>(g, pt, LdMul{f.e, U + 2 * n}) +
+              D1<2>(g, pt, LdMul{f.e, U + 3 * n});
+  double rE = -0.5 * (s4 + D1<0>(g, pt, E) * ruq + D1<1>(g, pt, E) * rvq + D1<2>(g, pt, E) * rwq);
+  // heat conduction
+  {
+    const double tx = D1<0>(g, pt, T), ty = D1<1>(g, pt, T), tz = D1<2>(g, pt, T);
+    rE = rE + (D1<0>(g, pt, lam) * tx + D1<1>(g, pt, lam) * ty + D1<2>(g, pt, lam) * tz);
+    rE = rE + (D2<0>(g, pt, T) + D2<1>(g, pt, T) + D2<2>(g, pt, T)) * lam(q);
+  }
+  // momentum convection, skew-symmetric
+  const double S4 = D1<0>(g, pt, LdMul{U + n, f.vel}) + D1<1>(g, pt, LdMul{U + n, f.vel + n}) +
+                    D1<2>(g, pt, LdMul{U + n, f.vel + 2 * n});
+  const double S5 = D1<0>(g, pt, LdMul{U + n, f.vel + n}) + D1<1>(g, pt, LdMul{U + 2 * n, f.vel + n}) +
+                    D1<2>(g, pt, LdMul{U + 2 * n, f.vel + 2 * n});
+  const double S6 = D1<0>(g, pt, LdMul{U + n, f.vel + 2 * n}) + D1<1>(g, pt, LdMul{U + 2 * n, f.vel + 2 * n}) +
+                    D1<2>(g, pt, LdMul{U + 3 * n, f.vel + 2 * n});
+  const double ux = D1<0>(g, pt, u), vy = D1<1>(g, pt, v), wz = D1<2>(g, pt, w);
+  double rU = -0.5 * (ruq * ux + (S4 + uq * divm));
+  double rV = -0.5 * (rvq * vy + (S5 + vq * divm));
+  double rW = -0.5 * (rwq * wz + (S6 + wq * divm));
+  // pressure gradient and pressure work (gradient of p - p(1,1,1))
+  {
+    const LdSub pp{f.p, __ldg(f.p)};
+    const double px = D1<0>(g, pt, pp), py = D1<1>(g, pt, pp), pz = D1<2>(g, pt, pp);
+    rU -= px;
+    rV -= py;
+    rW -= pz;
+    rE = rE - uq * px - vq * py - wq * pz;
+    rE = rE - __ldg(f.p + q) * (ux + vy + wz);
+  }
+  // viscous normal-stress terms with viscosity gradients
+  const double muq = mu(q);
+  const double mux = D1<0>(g, pt, mu), muy = D1<1>(g, pt, mu), muz = D1<2>(g, pt, mu);
+  {
+    double t6 = kFthd * ux - kTthd * (vy + wz);
+    rE = rE + muq * t6 * ux;
+    t6 = t6 * mux;
+    rU += t6;
+    rE = rE + uq * t6;
+    t6 = kFthd * vy - kTthd * (ux + wz);
+    rE = rE + muq * t6 * vy;
+    t6 = t6 * muy;
+    rV += t6;
+    rE = rE + vq * t6;
+    t6 = kFthd * wz - kTthd * (ux + vy);
+    rE = rE + muq * t6 * wz;
+    t6 = t6 * muz;
+    rW += t6;
+    rE = rE + wq * t6;
+  }
+  // xy
+  {
+    const double uy = D1<1>(g, pt, u), vx = D1<0>(g, pt, v);
+    rU = rU - 0.5 * rhq * vq * uy;
+    rV = rV - 0.5 * rhq * uq * vx;
+    const double s7 = uy + vx;
+    const double uxy = DM<0, 1>(g, pt, u), vxy = DM<0, 1>(g, pt, v);
+    double s3 = kTthd * muq * vxy;
+    rU -= s3;
+    rE = rE - uq * s3;
+    s3 = kTthd * muq * uxy;
+    rV -= s3;
+    rE = rE - vq * s3;
+    s3 = muq * (D2<1>(g, pt, u) + vxy) + s7 * muy;
+    rU += s3;
+    rE = rE + uq * s3;
+    s3 = muq * (D2<0>(g, pt, v) + uxy) + s7 * mux;
+    rV += s3;
+    rE = rE + vq * s3;
+    rE = rE + muq * s7 * s7;
+  }
+  // xz
+  {
+    const double uz = D1<2>(g, pt, u), wx = D1<0>(g, pt, w);
+    rU = rU - 0.5 * rhq * wq * uz;
+    rW = rW - 0.5 * rhq * uq * wx;
+    const double s7 = uz + wx;
+    const double uxz = DM<0, 2>(g, pt, u), wxz = DM<0, 2>(g, pt, w);
+    double s3 = kTthd * muq * wxz;
+    rU -= s3;
+    rE = rE - uq * s3;
+    s3 = kTthd * muq * uxz;
+    rW -= s3;
+    rE = rE - wq * s3;
+    s3 = muq * (D2<2>(g, pt, u) + wxz) + s7 * muz;
+    rU += s3;
+    rE = rE + uq * s3;
+    s3 = muq * (D2<0>(g, pt, w) + uxz) + s7 * mux;
+    rW += s3;
+    rE = rE + wq * s3;
+    rE = rE + muq * s7 * s7;
+  }
+  // yz
+  {
+    const double vz = D1<2>(g, pt, v), wy = D1<1>(g, pt, w);
+    rV = rV - 0.5 * rhq * wq * vz;
+    rW = rW - 0.5 * rhq * vq * wy;
+    const double s7 = vz + wy;
+    const double vyz = DM<1, 2>(g, pt, v), wyz = DM<1, 2>(g, pt, w);
+    double s3 = kTthd * muq * wyz;
+    rV -= s3;
+    rE = rE - vq * s3;
+    s3 = kTthd * muq * vyz;
+    rW -= s3;
+    rE = rE - wq * s3;
+    s3 = muq * (D2<2>(g, pt, v) + wyz) + s7 * muz;
+    rV += s3;
+    rE = rE + vq * s3;
+    s3 = muq * (D2<1>(g, pt, w) + vyz) + s7 * muy;
+    rW += s3;
+    rE = rE + wq * s3;
+    rE = rE + muq * s7 * s7;
+  }
+  // normal second derivatives
+  {
+    double fn = muq * kFthd * D2<0>(g, pt, u);
+    rU += fn;
+    rE = rE + fn * uq;
+    fn = muq * kFthd * D2<1>(g, pt, v);
+    rV += fn;
+    rE = rE + fn * vq;
+    fn = muq * kFthd * D2<2>(g, pt, w);
+    rW += fn;
+    rE = rE + fn * wq;
+  }
+  f.rhs[q] = -divm;
+  f.rhs[n + q] = rU;
+  f.rhs[2 * n + q] = rV;
+  f.rhs[3 * n + q] = rW;
+  f.rhs[4 * n + q] = rE;
+  f.divm[q] = divm;
+}
+
+// -------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_species_a(Geo g, Fields f, int nspec) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  const Pt pt = point_of(g, q);
+  const int64_t n = g.n;
+  const double* U = f.uin;
+  const double ruq = __ldg(U + n + q), rvq = __ldg(U + 2 * n + q), rwq = __ldg(U + 3 * n + q);
+  const double divm = f.divm[q];
+  double rE = f.rhs[4 * n + q];
+  double vcx = 0.0, vcy = 0.0, vcz = 0.0, vt = 0.0;
+  for (int s = 0; s < nspec; ++s) {
+    const double* ys = f.y + s * n;
+    const Ld Y{ys}, RD{f.rd + s * n}, H{f.h + s * n};
+    const double yq = Y(q);
+    double rate = f.wdot[s * n + q];
+    rate = rate - 0.5 * yq * divm;
+    rate = rate - 0.5 * (D1<0>(g, pt, LdMul{ys, U + n}) + D1<1>(g, pt, LdMul{ys, U + 2 * n}) +
+                         D1<2>(g, pt, LdMul{ys, U + 3 * n}));
+    const double yx = D1<0>(g, pt, Y), yy = D1<1>(g, pt, Y), yz = D1<2>(g, pt, Y);
+    rate = rate - 0.5 * (yx * ruq + yy * rvq + yz * rwq);
+    const double rd = RD(q), hk = H(q);
+    vcx = vcx + rd * yx;
+    vcy = vcy + rd * yy;
+    vcz = vcz + rd * yz;
+    double fn = D1<0>(g, pt, RD) * yx + D1<1>(g, pt, RD) * yy + D1<2>(g, pt, RD) * yz;
+    rate = rate + fn;
+    vt = vt + fn;
+    rE = rE + fn * hk;
+    fn = D1<0>(g, pt, H) * yx + D1<1>(g, pt, H) * yy + D1<2>(g, pt, H) * yz;
+    rE = rE + fn * rd;
+    fn = (D2<0>(g, pt, Y) + D2<1>(g, pt, Y) + D2<2>(g, pt, Y)) * rd;
+    rate = rate + fn;
+    vt = vt + fn;
+    rE = rE + fn * hk;
+    f.wdot[s * n + q] = rate;
+  }
+  f.vc[q] = vcx;
+  f.vc[n + q] = vcy;
+  f.vc[2 * n + q] = vcz;
+  f.vtmp[q] = vt;
+  f.rhs[4 * n + q] = rE;
+}
+
+// -------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_species_b_rk(Geo g, Fields f, int nspec, RK rk) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  const Pt pt = point_of(g, q);
+  const int64_t n = g.n;
+  const double vcx = f.vc[q], vcy = f.vc[n + q], vcz = f.vc[2 * n + q], vt = f.vtmp[q];
+  const Ld HM{f.hmix};
+  const double rE = f.rhs[4 * n + q] - HM(q) * vt - D1<0>(g, pt, HM) * vcx - D1<1>(g, pt, HM) * vcy -
+                    D1<2>(g, pt, HM) * vcz;
+  auto advance = [&](int fld, double R) {
+    const int64_t o = (int64_t)fld * n + q;
+    if (rk.last < 0) {  // right-hand side only (no RK update)
+      f.rhs[o] = R;
+      return;
+    }
+    if (f.err) f.err[o] = f.err[o] + rk.err * R;
+    if (!rk.last) {
+      const double s = f.run[o];
+      f.run[o] = s + rk.lhs * R;
+      f.uout[o] = s + rk.rhs * R;
+    } else {
+      const double s = f.run[o] + rk.lhs * R;
+      f.run[o] = s;
+      f.uout[o] = s;
+    }
+  };
+#pragma unroll
+  for (int fl = 0; fl < 4; ++fl) advance(fl, f.rhs[fl * n + q]);
+  advance(4, rE);
+  for (int s = 0; s < nspec; ++s) {
+    const Ld Y{f.y + s * n};
+    const double R = f.wdot[s * n + q] - Y(q) * vt - D1<0>(g, pt, Y) * vcx - D1<1>(g, pt, Y) * vcy -
+                     D1<2>(g, pt, Y) * vcz;
+    advance(5 + s, R);
+  }
+}
+
+// -------------------------------------------------------------------------
+__global__ void k_deriv(Geo g, int kind, const double* __restrict__ in, double* __restrict__ out) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  const Pt pt = point_of(g, q);
+  const Ld F{in};
+  double r = 0.0;
+  switch (kind) {
+    case 0: r = D1<0>(g, pt, F); break;
+    case 1: r = D1<1>(g, pt, F); break;
+    case 2: r = D1<2>(g, pt, F); break;
+    case 3: r = D2<0>(g, pt, F); break;
+    case 4: r = D2<1>(g, pt, F); break;
+    case 5: r = D2<2>(g, pt, F); break;
+    case 6: r = DM<0, 1>(g, pt, F); break;
+    case 7: r = DM<0, 2>(g, pt, F); break;
+    default: r = DM<1, 2>(g, pt, F); break;
+  }
+  out[q] = r;
+}
+
+inline unsigned grid_of(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+}  // namespace
+
+void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const senga_diff* ddiff, int nspec,
+                   int flmavt, cudaStream_t s) {
+  const unsigned gr = grid_of(g.n);
+  if (nspec <= 2) {
+    if (flmavt) k_thermo<2, true, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
+    else k_thermo<2, false, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
+  } else {
+    if (flmavt) k_thermo<9, true, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
+    else k_thermo<9, false, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
+  }
+}
+
+void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s) { k_flow<<<grid_of(g.n), kBlock, 0, s>>>(g, f); }
+
+void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s) {
+  k_species_a<<<grid_of(g.n), kBlock, 0, s>>>(g, f, nspec);
+}
+
+void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s) {
+  k_species_b_rk<<<grid_of(g.n), kBlock, 0, s>>>(g, f, nspec, rk);
+}
+
+void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s) {
+  k_deriv<<<grid_of(g.n), kBlock, 0, s>>>(g, kind, in, out);
+}
+
+}  // namespace senga

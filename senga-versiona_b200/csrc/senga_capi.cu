@@ -1,0 +1,391 @@
+// C ABI: device-resident context, state transfer, substage driver.
+//
+// The reference keeps every field in COMMON and calls, per substage,
+// BOUNDT, PARFER, RHSCAL, RHSVEL, BOUNDS, LINCOM/FINCOM (src/senga2.f:113-159).
+// Here one context owns the HBM-resident registers and scratch of one box and
+// a substage is four kernels on the context's stream:
+//   thermo (TEMPER + transport + enthalpy + CHRATE, pointwise)
+//   flow   (continuity, momentum, energy convection/conduction/work)
+//   species_a, species_b+RK (species equations, correction velocity, LINCOM).
+// PARFER's single-rank periodic copy is replaced by index wrapping inside the
+// stencils, so no halo exchange runs.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "senga_gpu.h"
+#include "senga_internal.h"
+
+namespace senga {
+
+static thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      throw Error(e_ == cudaErrorMemoryAllocation ? SENGA_ERR_NOMEM : SENGA_ERR_CUDA,         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+  } while (0)
+
+// RK4(3)5[2R+]C of Kennedy, Carpenter & Lewis: src/dtinit.f:76-94.
+static const double kAcof[5] = {970286171893.0 / 4311952581923.0, 6584761158862.0 / 12103376702013.0,
+                                2251764453980.0 / 15575788980749.0, 26877169314380.0 / 34165994151039.0, 0.0};
+static const double kBcof[5] = {1153189308089.0 / 22510343858157.0, 1772645290293.0 / 4653164025191.0,
+                                -1672844663538.0 / 4480602732383.0, 2114624349019.0 / 3568978502595.0,
+                                5198255086312.0 / 14908931495163.0};
+static const double kBhat[5] = {1016888040809.0 / 7410784769900.0, 11231460423587.0 / 58533540763752.0,
+                                -1563879915014.0 / 6823010717585.0, 606302364029.0 / 971179775848.0,
+                                1097981568119.0 / 3980877426909.0};
+
+}  // namespace senga
+
+using namespace senga;
+
+struct senga_ctx {
+  senga_config cfg{};
+  senga_chem chem{};
+  senga_diff diff{};
+  Geo geo{};
+  int nspec = 0, nc = 0;
+  cudaStream_t stream = nullptr;
+  senga_chem* d_chem = nullptr;
+  senga_diff* d_diff = nullptr;
+  double* pool = nullptr;
+  unsigned int* d_status = nullptr;
+  Fields f{};
+  double rklhs[5], rkrhs[5], rkerr[5];
+  cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+void build_geo(const senga_config& c, Geo& g) {
+  g.nx = c.nx;
+  g.ny = c.ny;
+  g.nz = c.nz;
+  g.n = (int64_t)c.nx * c.ny * c.nz;
+  const int n3[3] = {c.nx, c.ny, c.nz};
+  const double len[3] = {c.xgdlen, c.ygdlen, c.zgdlen};
+  for (int d = 0; d < 3; ++d) {
+    g.per[d] = c.nend[2 * d] == SENGA_NPERI ? 1 : 0;
+    // DELTAX = XGDLEN/REAL(NXGLBL-1): spacing L/(N-1) also for periodic boxes
+    const double delta = len[d] / (double)(float)(n3[d] - 1);
+    g.ovd[d] = 1.0 / delta;
+    g.ovd2[d] = g.ovd[d] * g.ovd[d];
+  }
+}
+
+void check_config(const senga_config& c, int nspec) {
+  const int n3[3] = {c.nx, c.ny, c.nz};
+  for (int d = 0; d < 3; ++d) {
+    if (n3[d] < 11) throw Error(SENGA_ERR_ARG, "grid extent must be at least 11 points per direction");
+    const int l = c.nend[2 * d], r = c.nend[2 * d + 1];
+    if ((l == SENGA_NPERI) != (r == SENGA_NPERI))
+      throw Error(SENGA_ERR_ARG, "periodic end conditions must be set on both faces of a direction");
+    if (l != SENGA_NPERI)
+      throw Error(SENGA_ERR_UNSUPPORTED, "non-periodic boxes need the NSCBC face kernels (not built)");
+  }
+  if (c.tstep <= 0.0) throw Error(SENGA_ERR_ARG, "tstep must be positive");
+  if (nspec < 1 || nspec > SENGA_NSPCMX) throw Error(SENGA_ERR_ARG, "nspec out of range");
+}
+
+void set_rk(senga_ctx* c, double tstep) {
+  for (int i = 0; i < 5; ++i) {
+    c->rklhs[i] = kBcof[i] * tstep;
+    c->rkrhs[i] = kAcof[i] * tstep;
+    c->rkerr[i] = (kBcof[i] - kBhat[i]) * tstep;
+  }
+}
+
+void run_rhs(senga_ctx* c) {
+  launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+  launch_flow(c->geo, c->f, c->nspec, c->stream);
+  launch_species_a(c->geo, c->f, c->nspec, c->stream);
+}
+
+void run_substage(senga_ctx* c, int irk) {
+  run_rhs(c);
+  RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
+  launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+}
+
+template <class Fn>
+int guard(Fn&& fn) {
+  try {
+    fn();
+    return SENGA_OK;
+  } catch (const Error& e) {
+    return fail(e.code, e.what());
+  } catch (const std::exception& e) {
+    return fail(SENGA_ERR_CUDA, e.what());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* senga_last_error(void) { return g_last_error.c_str(); }
+
+int senga_ctx_create(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff, senga_ctx** out) {
+  if (!cfg || !chem || !out) return fail(SENGA_ERR_ARG, "senga_ctx_create: null argument");
+  *out = nullptr;
+  senga_ctx* c = new senga_ctx();
+  int rc = guard([&] {
+    c->cfg = *cfg;
+    c->chem = *chem;
+    if (diff) c->diff = *diff;
+    else std::memset(&c->diff, 0, sizeof(c->diff));
+    c->nspec = chem->nspec;
+    c->nc = 5 + c->nspec;
+    check_config(*cfg, c->nspec);
+    build_geo(*cfg, c->geo);
+    set_rk(c, cfg->tstep);
+    CK(cudaSetDevice(cfg->device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&c->d_chem, sizeof(senga_chem)));
+    CK(cudaMalloc(&c->d_diff, sizeof(senga_diff)));
+    CK(cudaMemcpy(c->d_chem, &c->chem, sizeof(senga_chem), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_diff, &c->diff, sizeof(senga_diff), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_status, sizeof(unsigned int)));
+    CK(cudaMemset(c->d_status, 0, sizeof(unsigned int)));
+    const int64_t n = c->geo.n;
+    const int S = c->nspec, nc = c->nc;
+    // pool layout (doubles): run nc | u nc | err nc? | t | p lam lcp mu | rd S | h S |
+    // hmix | wdot S | vel 3 | e | y S | rhs nc | divm | vc 3 | vtmp | itn (int32, n/2 doubles)
+    const int64_t per_point = (int64_t)nc * 2 + (cfg->adaptive ? nc : 0) + 1 + 4 + 3 * S + 1 + 3 + 1 + S + nc + 1 + 3 + 1;
+    const int64_t total = per_point * n + (n + 1) / 2 + 64;
+    CK(cudaMalloc(&c->pool, (size_t)total * sizeof(double)));
+    CK(cudaMemsetAsync(c->pool, 0, (size_t)total * sizeof(double), c->stream));
+    double* p = c->pool;
+    auto take = [&](int64_t k) {
+      double* r = p;
+      p += k * n;
+      return r;
+    };
+    Fields& f = c->f;
+    f.run = take(nc);
+    f.uin = take(nc);
+    f.uout = f.uin;  // the RK epilogue reads no neighbour of the U register
+    f.err = cfg->adaptive ? take(nc) : nullptr;
+    f.t = take(1);
+    f.p = take(1);
+    f.lam = take(1);
+    f.lcp = take(1);
+    f.mu = take(1);
+    f.rd = take(S);
+    f.h = take(S);
+    f.hmix = take(1);
+    f.wdot = take(S);
+    f.vel = take(3);
+    f.e = take(1);
+    f.y = take(S);
+    f.rhs = take(nc);
+    f.divm = take(1);
+    f.vc = take(3);
+    f.vtmp = take(1);
+    f.itn = reinterpret_cast<int32_t*>(p);
+    f.status = c->d_status;
+    CK(cudaStreamSynchronize(c->stream));
+  });
+  if (rc != SENGA_OK) {
+    senga_ctx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return SENGA_OK;
+}
+
+int senga_ctx_destroy(senga_ctx* c) {
+  if (!c) return SENGA_OK;
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->pool);
+  cudaFree(c->d_chem);
+  cudaFree(c->d_diff);
+  cudaFree(c->d_status);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return SENGA_OK;
+}
+
+int senga_sync(senga_ctx* c) {
+  if (!c) return fail(SENGA_ERR_ARG, "null context");
+  return guard([&] { CK(cudaStreamSynchronize(c->stream)); });
+}
+
+void* senga_stream(senga_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int senga_upload_state_host(senga_ctx* c, const double* fields, const double* trun, const int32_t* itn) {
+  if (!c || !fields || !trun || !itn) return fail(SENGA_ERR_ARG, "senga_upload_state_host: null argument");
+  return guard([&] {
+    const size_t bytes = (size_t)c->nc * c->geo.n * sizeof(double);
+    CK(cudaMemcpyAsync(c->f.run, fields, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.uin, c->f.run, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.t, trun, c->geo.n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.itn, itn, c->geo.n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    if (c->f.err) CK(cudaMemsetAsync(c->f.err, 0, bytes, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_download_state_host(senga_ctx* c, double* fields, double* trun, int32_t* itn) {
+  if (!c || !fields) return fail(SENGA_ERR_ARG, "senga_download_state_host: null argument");
+  return guard([&] {
+    const size_t bytes = (size_t)c->nc * c->geo.n * sizeof(double);
+    CK(cudaMemcpyAsync(fields, c->f.run, bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (trun) CK(cudaMemcpyAsync(trun, c->f.t, c->geo.n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (itn) CK(cudaMemcpyAsync(itn, c->f.itn, c->geo.n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_substage(senga_ctx* c, int irkstp) {
+  if (!c || irkstp < 1 || irkstp > 5) return fail(SENGA_ERR_ARG, "senga_substage: bad argument");
+  return guard([&] {
+    run_substage(c, irkstp);
+    CK(cudaGetLastError());
+  });
+}
+
+int senga_step(senga_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_step: bad argument");
+  return guard([&] {
+    for (int s = 0; s < nsteps; ++s)
+      for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
+    CK(cudaGetLastError());
+  });
+}
+
+int senga_step_graph(senga_ctx* c, int nsteps) {
+  if (!c || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_step_graph: bad argument");
+  return guard([&] {
+    if (!c->graph) {
+      cudaGraph_t gr;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
+      CK(cudaStreamEndCapture(c->stream, &gr));
+      CK(cudaGraphInstantiate(&c->graph, gr, 0));
+      CK(cudaGraphDestroy(gr));
+    }
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(c->graph, c->stream));
+    CK(cudaGetLastError());
+  });
+}
+
+int senga_rhs_host(senga_ctx* c, double* rhs, double* trun, double* prun) {
+  if (!c || !rhs) return fail(SENGA_ERR_ARG, "senga_rhs_host: null argument");
+  return guard([&] {
+    run_rhs(c);
+    RK rk{0.0, 0.0, 0.0, -1};  // last = -1: write R(U) into the rhs fields only
+    launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+    CK(cudaGetLastError());
+    const int64_t n = c->geo.n;
+    CK(cudaMemcpyAsync(rhs, c->f.rhs, (size_t)c->nc * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (trun) CK(cudaMemcpyAsync(trun, c->f.t, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (prun) CK(cudaMemcpyAsync(prun, c->f.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
+  if (!c || !ms) return fail(SENGA_ERR_ARG, "senga_profile_step: null argument");
+  return guard([&] {
+    cudaEvent_t ev[21];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int k = 0; k < 4; ++k) ms[k] = 0.0;
+    int nl = 0;
+    for (int irk = 1; irk <= 5; ++irk) {
+      const int b = (irk - 1) * 4;
+      CK(cudaEventRecord(ev[b], c->stream));
+      launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+      CK(cudaEventRecord(ev[b + 1], c->stream));
+      launch_flow(c->geo, c->f, c->nspec, c->stream);
+      CK(cudaEventRecord(ev[b + 2], c->stream));
+      launch_species_a(c->geo, c->f, c->nspec, c->stream);
+      CK(cudaEventRecord(ev[b + 3], c->stream));
+      RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
+      launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+      CK(cudaEventRecord(irk < 5 ? ev[b + 4] : ev[20], c->stream));
+      nl += 4;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    for (int irk = 1; irk <= 5; ++irk) {
+      const int b = (irk - 1) * 4;
+      for (int k = 0; k < 4; ++k) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, ev[b + k], (b + k + 1 < 20) ? ev[b + k + 1] : ev[20]));
+        ms[k] += t;
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (launches) *launches = nl;
+  });
+}
+
+int senga_get_status(senga_ctx* c, int* status) {
+  if (!c || !status) return fail(SENGA_ERR_ARG, "senga_get_status: null argument");
+  return guard([&] {
+    unsigned int s = 0;
+    CK(cudaMemcpyAsync(&s, c->d_status, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *status = (int)s;
+  });
+}
+
+int senga_deriv(senga_ctx* c, int kind, const double* f, double* out) {
+  if (!c || !f || !out || kind < 0 || kind > 8) return fail(SENGA_ERR_ARG, "senga_deriv: bad argument");
+  return guard([&] {
+    launch_deriv(c->geo, kind, f, out, c->stream);
+    CK(cudaGetLastError());
+  });
+}
+
+int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
+  if (!c || !f || !out || kind < 0 || kind > 8) return fail(SENGA_ERR_ARG, "senga_deriv_host: bad argument");
+  return guard([&] {
+    const size_t bytes = c->geo.n * sizeof(double);
+    // the context's rhs scratch holds the operand and the result
+    double* din = c->f.rhs;
+    double* dout = c->f.rhs + c->geo.n;
+    CK(cudaMemcpyAsync(din, f, bytes, cudaMemcpyHostToDevice, c->stream));
+    launch_deriv(c->geo, kind, din, dout, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_temper_host(senga_ctx* c, double* trun, double* prun) {
+  if (!c) return fail(SENGA_ERR_ARG, "null context");
+  return guard([&] {
+    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+    CK(cudaGetLastError());
+    const int64_t n = c->geo.n;
+    if (trun) CK(cudaMemcpyAsync(trun, c->f.t, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (prun) CK(cudaMemcpyAsync(prun, c->f.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_chrate_host(senga_ctx* c, double* rate) {
+  if (!c || !rate) return fail(SENGA_ERR_ARG, "senga_chrate_host: null argument");
+  return guard([&] {
+    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(rate, c->f.wdot, (size_t)c->nspec * c->geo.n * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+// Internal declarations shared by the host and device translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "senga_gpu.h"
+
+namespace senga {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Records the message as the thread's last error and returns the code.
+int fail(int code, const std::string& msg);
+
+// Field slots of the conserved register (reference: DRHS,URHS,VRHS,WRHS,ERHS,
+// YRHS(:,:,:,k)).
+enum : int { F_RHO = 0, F_RU = 1, F_RV = 2, F_RW = 3, F_RE = 4, F_Y0 = 5 };
+
+// Box geometry handed to every kernel.
+struct Geo {
+  int nx, ny, nz;
+  int64_t n;            // nx*ny*nz
+  int per[3];           // 1 = periodic, 0 = bounded (one-sided closures)
+  double ovd[3];        // 1/Delta   (OVDELX..)
+  double ovd2[3];       // 1/Delta^2 (OVDLX2..)
+};
+
+// Device pointers of one box's registers and per-substage scratch.
+struct Fields {
+  double* run;    // S register  [nc][n]   (xRUN)
+  double* uin;    // U register read this substage  [nc][n] (xRHS on entry)
+  double* uout;   // U register written by the RK update
+  double* err;    // error register [nc][n] or nullptr (fixed dt)
+  double* t;      // TRUN
+  int32_t* itn;   // ITNDEX (2 bits per species)
+  // scratch
+  double* p;      // PRUN
+  double* lam;    // thermal conductivity lambda
+  double* lcp;    // lambda/cp (constant-Lewis transport; TRANSP)
+  double* mu;     // viscosity
+  double* rd;     // rho*D_k [nspec][n]
+  double* h;      // species enthalpy h_k [nspec][n]
+  double* hmix;   // mixture enthalpy
+  double* wdot;   // CHRATE rate, then species RHS partial [nspec][n]
+  double* vel;    // u,v,w [3][n]
+  double* e;      // E = rho E / rho
+  double* y;      // Y_k [nspec][n]
+  double* rhs;    // R(U) [nc][n]
+  double* divm;   // DIVM
+  double* vc;     // diffusion correction velocity [3][n] (UCOR,VCOR,WCOR)
+  double* vtmp;   // divergence of correction flux (VTMP)
+  unsigned int* status;  // device status word
+};
+
+struct RK {
+  double lhs, rhs, err;  // RKLHS, RKRHS, RKERR of this substage (times dt)
+  int last;              // 1 on the final substage (FINCOM)
+};
+
+// Launchers (kernels.cu).
+void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const senga_diff* ddiff, int nspec,
+                   int flmavt, cudaStream_t s);
+void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
+void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
+void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s);
+void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s);
+void launch_chrate_only(const Geo& g, const Fields& f, const senga_chem* dchem, int nspec, cudaStream_t s);
+
+}  // namespace senga

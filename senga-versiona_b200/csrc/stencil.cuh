@@ -1,0 +1,179 @@
+// 10th-order explicit finite-difference operators on device.
+//
+// Coefficients: src/dfinit.f:61-171 (first), :191-301 (second), :326-336
+// (mixed). Interior first derivative src/dfbydx.f:67-105 with scaling :234-238;
+// one-sided 4th/4th/4th/6th/8th-order closures :116-223. Second derivative
+// src/d2fdx2.f:96-111, closures :127-263, scaling :270. Mixed derivative
+// interior src/d2fdxy.f:126-141, scaling :1937.
+//
+// Periodic directions wrap the index (the single-rank halo copy of
+// src/parfer.f:840-873 produces exactly those values); bounded directions use
+// the one-sided closures on the first/last five points.
+#pragma once
+#include <cstdint>
+
+#include "senga_internal.h"
+
+namespace senga {
+
+// ---- coefficients (constant-folded exactly as DFINIT computes them) ----
+namespace fdc {
+constexpr double A = 5.0 / 3.0, B = -2.0e1 / 2.1e1, C = 5.0 / 1.4e1, D = -5.0 / 6.3e1, E = 1.0 / 1.26e2;
+constexpr double a1 = A / 2.0, b1 = B / 4.0, c1 = C / 6.0, d1 = D / 8.0, e1 = E / 1.0e1;
+constexpr double a2 = A, b2 = B / 4.0, c2 = C / 9.0, d2 = D / 1.6e1, e2 = E / 2.5e1;
+constexpr double ax = A / 4.0, bx = B / 4.0 / 4.0, cx = C / 4.0 / 9.0, dx = D / 4.0 / 1.6e1, ex = E / 4.0 / 2.5e1;
+// first-derivative closures
+constexpr double p1a = 4.0, p1b = -3.0, p1c = 4.0 / 3.0, p1d = -1.0 / 4.0;
+constexpr double p2a = -1.0 / 4.0, p2b = 3.0 / 2.0, p2c = -1.0 / 2.0, p2d = 1.0 / 1.2e1;
+constexpr double p3a = (4.0 / 3.0) / 2.0, p3b = (-1.0 / 3.0) / 4.0;
+constexpr double p4a = (3.0 / 2.0) / 2.0, p4b = (-3.0 / 5.0) / 4.0, p4c = (1.0 / 1.0e1) / 6.0;
+constexpr double p5a = (8.0 / 5.0) / 2.0, p5b = (-4.0 / 5.0) / 4.0, p5c = (8.0 / 3.5e1) / 6.0, p5d = (-1.0 / 3.5e1) / 8.0;
+// second-derivative closures
+constexpr double s1a = -7.7e1 / 6.0, s1b = 1.07e2 / 6.0, s1c = -1.3e1, s1d = 6.1e1 / 1.2e1, s1e = -5.0 / 6.0;
+constexpr double s2a = 5.0 / 6.0, s2b = -1.0 / 3.0, s2c = 7.0 / 6.0, s2d = -1.0 / 2.0, s2e = 1.0 / 1.2e1;
+constexpr double s3a = 4.0 / 3.0, s3b = (-1.0 / 3.0) / 4.0;
+constexpr double s4a = 3.0 / 2.0, s4b = (-3.0 / 5.0) / 4.0, s4c = (1.0 / 1.0e1) / 9.0;
+constexpr double s5a = 8.0 / 5.0, s5b = (-4.0 / 5.0) / 4.0, s5c = (8.0 / 3.5e1) / 9.0, s5d = (-1.0 / 3.5e1) / 1.6e1;
+}  // namespace fdc
+
+struct Pt {
+  int i, j, k;
+  int64_t q;
+};
+
+template <int DIR>
+__device__ __forceinline__ int ext(const Geo& g) {
+  return DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
+}
+template <int DIR>
+__device__ __forceinline__ int64_t strd(const Geo& g) {
+  return DIR == 0 ? (int64_t)1 : DIR == 1 ? (int64_t)g.nx : (int64_t)g.nx * g.ny;
+}
+template <int DIR>
+__device__ __forceinline__ int crd(const Pt& p) {
+  return DIR == 0 ? p.i : DIR == 1 ? p.j : p.k;
+}
+// element offset of the point m steps along DIR (periodic wrap)
+template <int DIR>
+__device__ __forceinline__ int64_t woff(const Geo& g, int c, int m) {
+  const int n = ext<DIR>(g);
+  int cm = c + m;
+  cm = cm < 0 ? cm + n : (cm >= n ? cm - n : cm);
+  return (int64_t)(cm - c) * strd<DIR>(g);
+}
+
+// First derivative along DIR at p of the field given by accessor f(q).
+template <int DIR, class F>
+__device__ __forceinline__ double D1(const Geo& g, const Pt& p, const F& f) {
+  using namespace fdc;
+  const int n = ext<DIR>(g), c = crd<DIR>(p);
+  double r;
+  if (g.per[DIR] || (c >= 5 && c <= n - 6)) {
+    auto v = [&](int m) { return f(p.q + woff<DIR>(g, c, m)); };
+    r = a1 * (v(1) - v(-1)) + b1 * (v(2) - v(-2)) + c1 * (v(3) - v(-3)) + d1 * (v(4) - v(-4)) +
+        e1 * (v(5) - v(-5));
+  } else {
+    const int64_t s = strd<DIR>(g);
+    auto a = [&](int abs0) { return f(p.q + (int64_t)(abs0 - c) * s); };  // 0-based absolute index
+    if (c < 5) {
+      switch (c) {
+        case 0: r = p1a * (a(1) - a(0)) + p1b * (a(2) - a(0)) + p1c * (a(3) - a(0)) + p1d * (a(4) - a(0)); break;
+        case 1: r = p2a * (a(0) - a(1)) + p2b * (a(2) - a(1)) + p2c * (a(3) - a(1)) + p2d * (a(4) - a(1)); break;
+        case 2: r = p3a * (a(3) - a(1)) + p3b * (a(4) - a(0)); break;
+        case 3: r = p4a * (a(4) - a(2)) + p4b * (a(5) - a(1)) + p4c * (a(6) - a(0)); break;
+        default: r = p5a * (a(5) - a(3)) + p5b * (a(6) - a(2)) + p5c * (a(7) - a(1)) + p5d * (a(8) - a(0)); break;
+      }
+    } else {
+      const int L = n - 1;
+      switch (L - c) {
+        case 4: r = p5a * (a(L - 3) - a(L - 5)) + p5b * (a(L - 2) - a(L - 6)) + p5c * (a(L - 1) - a(L - 7)) + p5d * (a(L) - a(L - 8)); break;
+        case 3: r = p4a * (a(L - 2) - a(L - 4)) + p4b * (a(L - 1) - a(L - 5)) + p4c * (a(L) - a(L - 6)); break;
+        case 2: r = p3a * (a(L - 1) - a(L - 3)) + p3b * (a(L) - a(L - 4)); break;
+        case 1: r = p2a * (a(L - 1) - a(L)) + p2b * (a(L - 1) - a(L - 2)) + p2c * (a(L - 1) - a(L - 3)) + p2d * (a(L - 1) - a(L - 4)); break;
+        default: r = p1a * (a(L) - a(L - 1)) + p1b * (a(L) - a(L - 2)) + p1c * (a(L) - a(L - 3)) + p1d * (a(L) - a(L - 4)); break;
+      }
+    }
+  }
+  return r * g.ovd[DIR];
+}
+
+// Second derivative along DIR.
+template <int DIR, class F>
+__device__ __forceinline__ double D2(const Geo& g, const Pt& p, const F& f) {
+  using namespace fdc;
+  const int n = ext<DIR>(g), c = crd<DIR>(p);
+  double r;
+  if (g.per[DIR] || (c >= 5 && c <= n - 6)) {
+    auto v = [&](int m) { return f(p.q + woff<DIR>(g, c, m)); };
+    const double f0 = f(p.q);
+    r = a2 * ((v(1) - f0) - (f0 - v(-1))) + b2 * ((v(2) - f0) - (f0 - v(-2))) +
+        c2 * ((v(3) - f0) - (f0 - v(-3))) + d2 * ((v(4) - f0) - (f0 - v(-4))) +
+        e2 * ((v(5) - f0) - (f0 - v(-5)));
+  } else {
+    const int64_t s = strd<DIR>(g);
+    auto a = [&](int abs0) { return f(p.q + (int64_t)(abs0 - c) * s); };
+    if (c < 5) {
+      switch (c) {
+        case 0: r = s1a * (a(1) - a(0)) + s1b * (a(2) - a(0)) + s1c * (a(3) - a(0)) + s1d * (a(4) - a(0)) + s1e * (a(5) - a(0)); break;
+        case 1: r = s2a * (a(0) - a(1)) + s2b * (a(2) - a(1)) + s2c * (a(3) - a(1)) + s2d * (a(4) - a(1)) + s2e * (a(5) - a(1)); break;
+        case 2: r = s3a * ((a(3) - a(2)) - (a(2) - a(1))) + s3b * ((a(4) - a(2)) - (a(2) - a(0))); break;
+        case 3: r = s4a * ((a(4) - a(3)) - (a(3) - a(2))) + s4b * ((a(5) - a(3)) - (a(3) - a(1))) + s4c * ((a(6) - a(3)) - (a(3) - a(0))); break;
+        default: r = s5a * ((a(5) - a(4)) - (a(4) - a(3))) + s5b * ((a(6) - a(4)) - (a(4) - a(2))) + s5c * ((a(7) - a(4)) - (a(4) - a(1))) + s5d * ((a(8) - a(4)) - (a(4) - a(0))); break;
+      }
+    } else {
+      const int L = n - 1;
+      switch (L - c) {
+        case 4: r = s5a * ((a(L - 3) - a(L - 4)) - (a(L - 4) - a(L - 5))) + s5b * ((a(L - 2) - a(L - 4)) - (a(L - 4) - a(L - 6))) + s5c * ((a(L - 1) - a(L - 4)) - (a(L - 4) - a(L - 7))) + s5d * ((a(L) - a(L - 4)) - (a(L - 4) - a(L - 8))); break;
+        case 3: r = s4a * ((a(L - 2) - a(L - 3)) - (a(L - 3) - a(L - 4))) + s4b * ((a(L - 1) - a(L - 3)) - (a(L - 3) - a(L - 5))) + s4c * ((a(L) - a(L - 3)) - (a(L - 3) - a(L - 6))); break;
+        case 2: r = s3a * ((a(L - 1) - a(L - 2)) - (a(L - 2) - a(L - 3))) + s3b * ((a(L) - a(L - 2)) - (a(L - 2) - a(L - 4))); break;
+        case 1: r = s2a * (a(L) - a(L - 1)) + s2b * (a(L - 2) - a(L - 1)) + s2c * (a(L - 3) - a(L - 1)) + s2d * (a(L - 4) - a(L - 1)) + s2e * (a(L - 5) - a(L - 1)); break;
+        default: r = s1a * (a(L - 1) - a(L)) + s1b * (a(L - 2) - a(L)) + s1c * (a(L - 3) - a(L)) + s1d * (a(L - 4) - a(L)) + s1e * (a(L - 5) - a(L)); break;
+      }
+    }
+  }
+  return r * (DIR == 0 ? g.ovd2[0] : DIR == 1 ? g.ovd2[1] : g.ovd2[2]);
+}
+
+// Mixed derivative in the plane (D1DIR, D2DIR), interior diagonal scheme.
+// Both directions periodic (bounded edges/corners are rejected on the host).
+template <int DA, int DB, class F>
+__device__ __forceinline__ double DM(const Geo& g, const Pt& p, const F& f) {
+  using namespace fdc;
+  const int ca = crd<DA>(p), cb = crd<DB>(p);
+  auto v = [&](int ma, int mb) { return f(p.q + woff<DA>(g, ca, ma) + woff<DB>(g, cb, mb)); };
+  const double fa = v(1, 1) - v(1, -1) - v(-1, 1) + v(-1, -1);
+  const double fb = v(2, 2) - v(2, -2) - v(-2, 2) + v(-2, -2);
+  const double fc = v(3, 3) - v(3, -3) - v(-3, 3) + v(-3, -3);
+  const double fd = v(4, 4) - v(4, -4) - v(-4, 4) + v(-4, -4);
+  const double fe = v(5, 5) - v(5, -5) - v(-5, 5) + v(-5, -5);
+  return (ax * fa + bx * fb + cx * fc + dx * fd + ex * fe) * g.ovd[DA] * g.ovd[DB];
+}
+
+// ---- accessors ----
+struct Ld {
+  const double* __restrict__ a;
+  __device__ __forceinline__ double operator()(int64_t q) const { return __ldg(a + q); }
+};
+struct LdMul {
+  const double* __restrict__ a;
+  const double* __restrict__ b;
+  __device__ __forceinline__ double operator()(int64_t q) const { return __ldg(a + q) * __ldg(b + q); }
+};
+struct LdSub {
+  const double* __restrict__ a;
+  double c;
+  __device__ __forceinline__ double operator()(int64_t q) const { return __ldg(a + q) - c; }
+};
+
+__device__ __forceinline__ Pt point_of(const Geo& g, int64_t q) {
+  Pt p;
+  p.q = q;
+  const int64_t nxy = (int64_t)g.nx * g.ny;
+  p.k = (int)(q / nxy);
+  const int64_t r = q - (int64_t)p.k * nxy;
+  p.j = (int)(r / g.nx);
+  p.i = (int)(r - (int64_t)p.j * g.nx);
+  return p;
+}
+
+}  // namespace senga

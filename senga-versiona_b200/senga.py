@@ -1,0 +1,289 @@
+"""Host-side Python interface to libsenga_gpu.so (the B200 SENGA2 RHS/RK path).
+
+Mirrors the reference's call surfaces for this path:
+  * CHEMIN / DIFFIN table set-up            -> Chem.load / Diff.load
+  * the COMMON-resident state of one rank   -> Box (device-resident context)
+  * RHSCAL + RHSVEL                         -> Box.rhs()
+  * one substage / one RK step              -> Box.substage(irk) / Box.step(n)
+  * DFBYDX..D2FDYZ(FUNCTN, FDERIV)          -> Box.dfbydx(f) ... Box.d2fdyz(f)
+  * TEMPER, CHRATE                          -> Box.temper(), Box.chrate()
+
+Arrays are numpy float64 with shape (..., nz, ny, nx) in C order, which is
+the reference's Fortran (nx, ny, nz) column-major layout byte for byte.
+The CUDA library is required: importing this module fails loudly when
+libsenga_gpu.so is missing or cannot be loaded; there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsenga_gpu.so")
+DATA = os.path.join(HERE, "data")
+
+NSPCMX, NSTPMX, NTINMX, NCOFMX, NSSMAX, NBDYMX, NLLMAX, NDCFMX = 9, 21, 2, 7, 10, 10, 10, 4
+NOBC, NBOUND, NPERI = 0, 1, 2
+
+
+def _arr(t, *dims):
+    for d in reversed(dims):
+        t = t * d
+    return t
+
+
+class ChemT(C.Structure):
+    """senga_chem: COMMON/CHEMIC after CHEMIN (src/com_senga2.h:121-178)."""
+
+    _fields_ = [
+        ("nspec", C.c_int), ("nstep", C.c_int), ("nbody", C.c_int), ("ngibb", C.c_int),
+        ("nlind", C.c_int), ("ntroe", C.c_int), ("nsrif", C.c_int),
+        ("ntint", _arr(C.c_int, NSPCMX)),
+        ("ncofcp", _arr(C.c_int, NSPCMX, NTINMX)), ("ncpoly", _arr(C.c_int, NSPCMX, NTINMX)),
+        ("ncpom1", _arr(C.c_int, NSPCMX, NTINMX)), ("ncenth", _arr(C.c_int, NSPCMX, NTINMX)),
+        ("ncenpy", _arr(C.c_int, NSPCMX, NTINMX)),
+        ("nsslen", _arr(C.c_int, NSTPMX)), ("nrslen", _arr(C.c_int, NSTPMX)),
+        ("npslen", _arr(C.c_int, NSTPMX)), ("nrclen", _arr(C.c_int, NSTPMX)),
+        ("npclen", _arr(C.c_int, NSTPMX)),
+        ("nsspec", _arr(C.c_int, NSTPMX, NSSMAX)), ("nrspec", _arr(C.c_int, NSTPMX, NSSMAX)),
+        ("npspec", _arr(C.c_int, NSTPMX, NSSMAX)), ("nrcpec", _arr(C.c_int, NSTPMX, NSSMAX)),
+        ("npcpec", _arr(C.c_int, NSTPMX, NSSMAX)),
+        ("mblist", _arr(C.c_int, NSTPMX)), ("mglist", _arr(C.c_int, NSTPMX)),
+        ("mllist", _arr(C.c_int, NSTPMX)), ("mtlist", _arr(C.c_int, NSTPMX)),
+        ("mslist", _arr(C.c_int, NSTPMX)),
+        ("prefgb", C.c_double), ("alamda", C.c_double),
+        ("tintlo", _arr(C.c_double, NSPCMX, NTINMX)), ("tinthi", _arr(C.c_double, NSPCMX, NTINMX)),
+        ("amolcp", _arr(C.c_double, NSPCMX, NTINMX, NCOFMX)),
+        ("amolgb", _arr(C.c_double, NSPCMX, NTINMX, NCOFMX)),
+        ("amascp", _arr(C.c_double, NSPCMX, NTINMX, NCOFMX)),
+        ("amasct", _arr(C.c_double, NSPCMX, NTINMX, NCOFMX)),
+        ("amasch", _arr(C.c_double, NSPCMX, NTINMX, NCOFMX)),
+        ("amascs", _arr(C.c_double, NSPCMX, NTINMX, NCOFMX)),
+        ("rparam", _arr(C.c_double, NSTPMX, 3)),
+        ("rclind", _arr(C.c_double, NLLMAX, 4)), ("rctroe", _arr(C.c_double, NLLMAX, 12)),
+        ("rcsrif", _arr(C.c_double, NLLMAX, 8)),
+        ("diffmu", _arr(C.c_double, NSTPMX, NSSMAX)), ("diffmw", _arr(C.c_double, NSTPMX, NSSMAX)),
+        ("crspec", _arr(C.c_double, NSTPMX, NSSMAX)), ("cpspec", _arr(C.c_double, NSTPMX, NSSMAX)),
+        ("effy3b", _arr(C.c_double, NBDYMX, NSPCMX)),
+        ("wmolar", _arr(C.c_double, NSPCMX)), ("ovwmol", _arr(C.c_double, NSPCMX)),
+        ("rgspec", _arr(C.c_double, NSPCMX)), ("clewis", _arr(C.c_double, NSPCMX)),
+        ("olewis", _arr(C.c_double, NSPCMX)),
+    ]
+
+
+class DiffT(C.Structure):
+    """senga_diff: COMMON/DIFFUS after DIFFIN (src/com_senga2.h:189-214)."""
+
+    _fields_ = [
+        ("flmavt", C.c_int), ("ncodif", C.c_int), ("ncotdr", C.c_int), ("ncovis", C.c_int),
+        ("ncocon", C.c_int), ("pdifgb", C.c_double), ("tdifgb", C.c_double),
+        ("diffco", _arr(C.c_double, NSPCMX, NSPCMX, NDCFMX)),
+        ("tdrcco", _arr(C.c_double, NSPCMX, NSPCMX, NDCFMX)),
+        ("wilko1", _arr(C.c_double, NSPCMX, NSPCMX)), ("wilko2", _arr(C.c_double, NSPCMX, NSPCMX)),
+        ("viscco", _arr(C.c_double, NSPCMX, NDCFMX)), ("condco", _arr(C.c_double, NSPCMX, NDCFMX)),
+    ]
+
+
+class ConfigT(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("xgdlen", C.c_double), ("ygdlen", C.c_double), ("zgdlen", C.c_double),
+        ("nend", C.c_int * 6), ("tstep", C.c_double), ("adaptive", C.c_int), ("device", C.c_int),
+    ]
+
+
+class SengaError(RuntimeError):
+    pass
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise SengaError(f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+    lib = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
+    i32p = C.POINTER(C.c_int32)
+    sig = {
+        "senga_chem_load": (ip, [C.c_char_p, C.POINTER(ChemT)]),
+        "senga_diff_load": (ip, [C.c_char_p, C.POINTER(ChemT), C.POINTER(DiffT)]),
+        "senga_ctx_create": (ip, [C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), C.POINTER(vp)]),
+        "senga_ctx_destroy": (ip, [vp]),
+        "senga_last_error": (C.c_char_p, []),
+        "senga_sync": (ip, [vp]),
+        "senga_stream": (vp, [vp]),
+        "senga_upload_state_host": (ip, [vp, dp, dp, i32p]),
+        "senga_download_state_host": (ip, [vp, dp, dp, i32p]),
+        "senga_substage": (ip, [vp, ip]),
+        "senga_step": (ip, [vp, ip]),
+        "senga_step_graph": (ip, [vp, ip]),
+        "senga_rhs_host": (ip, [vp, dp, dp, dp]),
+        "senga_get_status": (ip, [vp, C.POINTER(C.c_int)]),
+        "senga_profile_step": (ip, [vp, dp, C.POINTER(C.c_int)]),
+        "senga_deriv": (ip, [vp, ip, vp, vp]),
+        "senga_deriv_host": (ip, [vp, ip, dp, dp]),
+        "senga_temper_host": (ip, [vp, dp, dp]),
+        "senga_chrate_host": (ip, [vp, dp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = lib.senga_last_error()
+        raise SengaError(f"{what} failed (status {rc}): {msg.decode() if msg else ''}")
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Chem:
+    """Chemistry tables (CHEMIN) loaded from a chem.dat file."""
+
+    def __init__(self, path):
+        self.path = path
+        self.t = ChemT()
+        _check(lib.senga_chem_load(path.encode(), C.byref(self.t)), "senga_chem_load")
+
+    @property
+    def nspec(self):
+        return self.t.nspec
+
+    def table(self, name):
+        return np.ctypeslib.as_array(getattr(self.t, name))
+
+
+class Diff:
+    """Transport tables (DIFFIN); path=None gives constant-Lewis transport."""
+
+    def __init__(self, path, chem):
+        self.path = path
+        self.t = DiffT()
+        _check(lib.senga_diff_load(path.encode() if path else None, C.byref(chem.t), C.byref(self.t)),
+               "senga_diff_load")
+
+    @property
+    def mixture_averaged(self):
+        return bool(self.t.flmavt)
+
+
+class Box:
+    """One box: HBM-resident state plus the per-substage RHS/RK path."""
+
+    def __init__(self, shape, lengths, chem, diff, tstep, nend=(NPERI,) * 6, adaptive=False, device=0):
+        nx, ny, nz = shape
+        self.shape = (nz, ny, nx)
+        self.chem, self.diff = chem, diff
+        self.nspec = chem.nspec
+        self.nc = 5 + self.nspec
+        cfg = ConfigT()
+        cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
+        cfg.xgdlen, cfg.ygdlen, cfg.zgdlen = lengths
+        for i, v in enumerate(nend):
+            cfg.nend[i] = v
+        cfg.tstep = tstep
+        cfg.adaptive = 1 if adaptive else 0
+        cfg.device = device
+        self.cfg = cfg
+        h = C.c_void_p()
+        _check(lib.senga_ctx_create(C.byref(cfg), C.byref(chem.t), C.byref(diff.t), C.byref(h)),
+               "senga_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.senga_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state ----
+    def upload(self, fields, trun, itndex):
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        t = np.ascontiguousarray(trun, dtype=np.float64)
+        it = np.ascontiguousarray(itndex, dtype=np.int32)
+        assert f.shape == (self.nc,) + self.shape and t.shape == self.shape and it.shape == self.shape
+        _check(lib.senga_upload_state_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
+               "upload")
+
+    def download(self):
+        f = np.empty((self.nc,) + self.shape)
+        t = np.empty(self.shape)
+        it = np.empty(self.shape, dtype=np.int32)
+        _check(lib.senga_download_state_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
+               "download")
+        return f, t, it
+
+    # ---- hot path ----
+    def substage(self, irk):
+        _check(lib.senga_substage(self.h, irk), "senga_substage")
+
+    def step(self, nsteps=1, graph=False):
+        _check((lib.senga_step_graph if graph else lib.senga_step)(self.h, nsteps), "senga_step")
+
+    def sync(self):
+        _check(lib.senga_sync(self.h), "senga_sync")
+
+    def status(self):
+        s = C.c_int()
+        _check(lib.senga_get_status(self.h, C.byref(s)), "senga_get_status")
+        return s.value
+
+    def profile_step(self):
+        """One RK step with per-kernel-family CUDA-event timing:
+        ({'thermo','flow','species_a','species_b_rk'} -> ms, launches)."""
+        ms = np.zeros(4)
+        nl = C.c_int()
+        _check(lib.senga_profile_step(self.h, _dp(ms), C.byref(nl)), "senga_profile_step")
+        return dict(zip(("thermo", "flow", "species_a", "species_b_rk"), ms.tolist())), nl.value
+
+    @property
+    def stream(self):
+        return lib.senga_stream(self.h)
+
+    def rhs(self):
+        """RHSCAL + RHSVEL of the current U register: (R(U), T, p)."""
+        r = np.empty((self.nc,) + self.shape)
+        t = np.empty(self.shape)
+        p = np.empty(self.shape)
+        _check(lib.senga_rhs_host(self.h, _dp(r), _dp(t), _dp(p)), "senga_rhs_host")
+        return r, t, p
+
+    def temper(self):
+        t = np.empty(self.shape)
+        p = np.empty(self.shape)
+        _check(lib.senga_temper_host(self.h, _dp(t), _dp(p)), "senga_temper_host")
+        return t, p
+
+    def chrate(self):
+        r = np.empty((self.nspec,) + self.shape)
+        _check(lib.senga_chrate_host(self.h, _dp(r)), "senga_chrate_host")
+        return r
+
+    # ---- derivative family (FUNCTN interior array -> FDERIV) ----
+    def deriv(self, kind, f):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        assert a.shape == self.shape
+        out = np.empty_like(a)
+        _check(lib.senga_deriv_host(self.h, kind, _dp(a), _dp(out)), "senga_deriv_host")
+        return out
+
+    def dfbydx(self, f): return self.deriv(0, f)
+    def dfbydy(self, f): return self.deriv(1, f)
+    def dfbydz(self, f): return self.deriv(2, f)
+    def d2fdx2(self, f): return self.deriv(3, f)
+    def d2fdy2(self, f): return self.deriv(4, f)
+    def d2fdz2(self, f): return self.deriv(5, f)
+    def d2fdxy(self, f): return self.deriv(6, f)
+    def d2fdxz(self, f): return self.deriv(7, f)
+    def d2fdyz(self, f): return self.deriv(8, f)

@@ -1,0 +1,168 @@
+"""CUDA path vs the oracle (CPU restatement of the reference), through the C ABI.
+
+Tolerance: field-normalised relative L-infinity, max|gpu-ref|/max|ref|,
+<= 1e-10 for state after N steps and for the right-hand side (the FP64 sums
+are reordered and contracted into FMAs on the GPU, so bit-exactness is not
+expected); derivative operators <= 1e-12.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_linf
+
+pytestmark = pytest.mark.gpu
+
+TOL_STATE = 1e-10
+TOL_DERIV = 1e-12
+
+
+def _pair(case):
+    import senga
+    from oracle import Oracle
+
+    chem = senga.Chem(case["chem"])
+    diff = senga.Diff(case["diff"], chem)
+    box = senga.Box(case["shape"], case["lengths"], chem, diff, case["dt"], nend=case["nend"])
+    ref = Oracle(case["shape"], case["lengths"], case["chem"], case["diff"], case["dt"], nend=case["nend"])
+    box.upload(case["fields"], case["T"], case["itn"])
+    ref.upload(case["fields"], case["T"], case["itn"])
+    return box, ref
+
+
+def _case(name, n, seed=7):
+    import cases
+
+    return cases.make_case(name, n=n, seed=seed)
+
+
+@pytest.mark.parametrize("kind", range(9))
+def test_derivative_family_noncubic(kind):
+    """DFBYDX..D2FDYZ on a non-cubic periodic box against the oracle."""
+    import senga
+    from oracle import Oracle
+
+    rng = np.random.default_rng(kind)
+    nx, ny, nz = 24, 20, 16
+    shape = (nz, ny, nx)
+    # smooth periodic field plus a little noise (exercises every stencil weight)
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    f = (np.sin(2 * np.pi * x / nx) * np.cos(4 * np.pi * y / ny) + np.sin(2 * np.pi * (z / nz + x / nx))
+         + 1e-3 * rng.standard_normal(shape))
+    c = _case("ignition32", 16)
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(None, chem)
+    lengths = (3.1e-3, 2.3e-3, 1.7e-3)
+    box = senga.Box((nx, ny, nz), lengths, chem, diff, 1e-8)
+    ref = Oracle((nx, ny, nz), lengths, c["chem"], None, 1e-8)
+    got = box.deriv(kind, f)
+    want = ref.deriv(kind, f)
+    assert rel_linf(got, want) <= TOL_DERIV
+
+
+@pytest.mark.parametrize("name,n", [("ignition32", 16), ("h2_kernels", 16)])
+def test_rhs_matches_oracle(name, n):
+    c = _case(name, n)
+    box, ref = _pair(c)
+    r_g, t_g, p_g = box.rhs()
+    r_o, t_o, p_o = ref.rhs()
+    assert rel_linf(t_g, t_o) <= TOL_STATE
+    assert rel_linf(p_g, p_o) <= TOL_STATE
+    for k in range(r_o.shape[0]):
+        assert rel_linf(r_g[k], r_o[k]) <= TOL_STATE, f"field {k}"
+
+
+@pytest.mark.parametrize("name", ["ignition32", "h2_kernels"])
+def test_chrate_matches_oracle(name):
+    c = _case(name, 12)
+    box, ref = _pair(c)
+    got = box.chrate()
+    want = ref.chrate()
+    for k in range(want.shape[0]):
+        if np.max(np.abs(want[k])) > 0:
+            assert rel_linf(got[k], want[k]) <= TOL_STATE, f"species {k}"
+
+
+def test_ignition32_ten_steps():
+    """The 32^3 one-step ignition workload: 10 RK steps, all fields."""
+    c = _case("ignition32", 32)
+    box, ref = _pair(c)
+    box.step(10)
+    ref.step(10)
+    g, tg, _ = box.download()
+    o, to, _ = ref.download()
+    for k in range(o.shape[0]):
+        assert rel_linf(g[k], o[k]) <= TOL_STATE, f"field {k}"
+    assert rel_linf(tg, to) <= TOL_STATE
+
+
+def test_h2_mixture_averaged_steps():
+    """H2 mechanism with mixture-averaged transport, 20^3, 3 RK steps."""
+    c = _case("h2_kernels", 20)
+    box, ref = _pair(c)
+    box.step(3)
+    ref.step(3)
+    g, tg, _ = box.download()
+    o, to, _ = ref.download()
+    for k in range(o.shape[0]):
+        assert rel_linf(g[k], o[k]) <= TOL_STATE, f"field {k}"
+    assert rel_linf(tg, to) <= TOL_STATE
+
+
+def test_noncubic_ensemble_box_steps():
+    """A non-cubic box of the batched ensemble (one-step chemistry)."""
+    import cases
+
+    c = cases.make_case("ensemble", seed=11)
+    c2 = dict(c)
+    box, ref = _pair(c2)
+    box.step(2)
+    ref.step(2)
+    g, _, _ = box.download()
+    o, _, _ = ref.download()
+    for k in range(o.shape[0]):
+        assert rel_linf(g[k], o[k]) <= TOL_STATE, f"field {k}"
+
+
+def test_graph_replay_is_bitwise_identical():
+    c = _case("ignition32", 16)
+    import senga
+
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(None, chem)
+    a = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"])
+    b = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"])
+    a.upload(c["fields"], c["T"], c["itn"])
+    b.upload(c["fields"], c["T"], c["itn"])
+    a.step(3)
+    b.step(3, graph=True)
+    fa, ta, _ = a.download()
+    fb, tb, _ = b.download()
+    assert np.array_equal(fa, fb) and np.array_equal(ta, tb)
+
+
+def test_mass_conservation_periodic():
+    """Periodic box: sum of the continuity RHS vanishes to round-off."""
+    c = _case("h2_kernels", 16)
+    box, _ = _pair(c)
+    r, _, _ = box.rhs()
+    assert abs(float(np.sum(r[0]))) <= 1e-9 * float(np.sum(np.abs(r[0])))
+
+
+def test_temper_failure_reports_status_without_fault():
+    """An impossible energy makes the Newton inversion fail: the status word
+    reports it and the context stays usable (no trap, no hang)."""
+    c = _case("ignition32", 16)
+    import senga
+
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(None, chem)
+    box = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"])
+    bad = c["fields"].copy()
+    bad[4, 3, 4, 5] = -1.0e12  # rho E far below any T > 0
+    box.upload(bad, c["T"], c["itn"])
+    box.temper()
+    assert box.status() & 1
+    box.upload(c["fields"], c["T"], c["itn"])
+    box.step(1)
+    f, _, _ = box.download()
+    assert np.isfinite(f).all()
