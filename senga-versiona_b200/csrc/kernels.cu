@@ -29,7 +29,9 @@ constexpr double kYsmall = 1.0e-30, kYdenom = 1.0e-15;  // src/chrate.f:40
 constexpr double kDfctol = 1.0e-12;                     // src/com_senga2.h:187
 constexpr int kBlock = 256;
 
-__device__ __forceinline__ int tint_of(int32_t itn, int s) { return (itn >> (2 * s)) & 3; }
+// Interval of species s packed in ITNDEX (2 bits per species). NTINMX = 2,
+// so only 0/1 are valid; the mask keeps a corrupt upload inside the tables.
+__device__ __forceinline__ int tint_of(int32_t itn, int s) { return (itn >> (2 * s)) & 1; }
 
 // Select-by-index update of a register array (keeps the array in registers
 // when the index comes from a table).

@@ -62,6 +62,11 @@ double rfield(const std::string& rec, size_t col, size_t width) {
   std::string s = field(rec, col, width);
   return s.empty() ? 0.0 : std::strtod(s.c_str(), nullptr);
 }
+// 0-based index of a record field, checked against the table extent.
+int at(int v, int extent, const char* what) {
+  if (v < 0 || v >= extent) throw senga::Error(SENGA_ERR_ARG, std::string("chem.dat: bad index in ") + what);
+  return v;
+}
 std::vector<double> free_format(const std::string& rec) {
   std::string s = rec;
   for (auto& ch : s) {
@@ -107,19 +112,19 @@ void load_chem(const char* path, senga_chem& c) {
   if (c.nstep < 1 || c.nstep > SENGA_NSTPMX) throw senga::Error(SENGA_ERR_ARG, "chem.dat: NSTEP out of range");
   for (int n = 0; n < c.nstep; ++n) {
     std::string rec = r.line();
-    int st = ifield(rec, 0, 5) - 1;
+    int st = at(ifield(rec, 0, 5) - 1, c.nstep, "step rate data");
     for (int q = 0; q < 3; ++q) c.rparam[st][q] = rfield(rec, 5 + 12 * q, 12);
   }
   auto step_list = [&](int* len, int (*lst)[SENGA_NSSMAX], double (*coef)[SENGA_NSSMAX]) {
     r.skip();
     for (int n = 0; n < c.nstep; ++n) {
       std::string rec = r.line();
-      int st = ifield(rec, 0, 5) - 1;
+      int st = at(ifield(rec, 0, 5) - 1, c.nstep, "step list");
       len[st] = ifield(rec, 5, 5);
       if (len[st] < 0 || len[st] > SENGA_NSSMAX) throw senga::Error(SENGA_ERR_ARG, "chem.dat: list length");
       for (int q = 0; q < len[st]; ++q) {
         std::string e = r.line();
-        int st2 = ifield(e, 0, 5) - 1, slot = ifield(e, 5, 5) - 1;
+        int st2 = at(ifield(e, 0, 5) - 1, c.nstep, "step list"), slot = at(ifield(e, 5, 5) - 1, SENGA_NSSMAX, "step list");
         lst[st2][slot] = ifield(e, 10, 8);
         if (coef) coef[st2][slot] = rfield(e, 18, 12);
       }
@@ -134,22 +139,25 @@ void load_chem(const char* path, senga_chem& c) {
   for (int st = 0; st < c.nstep; ++st)
     for (int q = 0; q < c.nsslen[st]; ++q) {
       std::string e = r.line();
-      c.diffmu[ifield(e, 0, 5) - 1][ifield(e, 5, 5) - 1] = rfield(e, 10, 5);
+      c.diffmu[at(ifield(e, 0, 5) - 1, c.nstep, "delta-list")][at(ifield(e, 5, 5) - 1, SENGA_NSSMAX, "delta-list")] =
+          rfield(e, 10, 5);
     }
   r.skip();
   c.nbody = ifield(r.line(), 0, 5);
+  if (c.nbody < 0 || c.nbody > SENGA_NBDYMX) throw senga::Error(SENGA_ERR_ARG, "chem.dat: NBODY out of range");
   r.skip(c.nbody);
   r.skip();
   if (c.nbody > 0)
     for (int n = 0; n < c.nstep; ++n) {
       std::string e = r.line();
-      c.mblist[ifield(e, 0, 5) - 1] = ifield(e, 5, 8);
+      c.mblist[at(ifield(e, 0, 5) - 1, c.nstep, "third-body step-list")] = ifield(e, 5, 8);
     }
   r.skip();
   for (int b = 0; b < c.nbody; ++b)
     for (int s = 0; s < c.nspec; ++s) {
       std::string e = r.line();
-      c.effy3b[ifield(e, 0, 5) - 1][ifield(e, 5, 5) - 1] = rfield(e, 10, 12);
+      c.effy3b[at(ifield(e, 0, 5) - 1, c.nbody, "efficiencies")][at(ifield(e, 5, 5) - 1, c.nspec, "efficiencies")] =
+          rfield(e, 10, 12);
     }
   auto flag_list = [&](int* count, int* lst) {
     r.skip();
@@ -157,7 +165,7 @@ void load_chem(const char* path, senga_chem& c) {
     if (*count > 0)
       for (int n = 0; n < c.nstep; ++n) {
         std::string e = r.line();
-        lst[ifield(e, 0, 5) - 1] = ifield(e, 5, 8);
+        lst[at(ifield(e, 0, 5) - 1, c.nstep, "step flag list")] = ifield(e, 5, 8);
       }
   };
   flag_list(&c.ngibb, c.mglist);
@@ -165,14 +173,14 @@ void load_chem(const char* path, senga_chem& c) {
   r.skip();
   for (int n = 0; n < c.nlind; ++n) {
     std::string e = r.line();
-    int il = ifield(e, 0, 5) - 1;
+    int il = at(ifield(e, 0, 5) - 1, SENGA_NLLMAX, "Lindemann data");
     for (int q = 0; q < 4; ++q) c.rclind[il][q] = rfield(e, 5 + 12 * q, 12);
   }
   flag_list(&c.ntroe, c.mtlist);
   r.skip();
   for (int n = 0; n < c.ntroe; ++n) {
     std::string e = r.line();
-    int it = ifield(e, 0, 5) - 1;
+    int it = at(ifield(e, 0, 5) - 1, SENGA_NLLMAX, "Troe data");
     for (int q = 0; q < 6; ++q) c.rctroe[it][q] = rfield(e, 5 + 12 * q, 12);
     e = r.line();
     for (int q = 0; q < 6; ++q) c.rctroe[it][6 + q] = rfield(e, 5 + 12 * q, 12);
@@ -181,11 +189,31 @@ void load_chem(const char* path, senga_chem& c) {
   r.skip();
   for (int n = 0; n < c.nsrif; ++n) {
     std::string e = r.line();
-    int is = ifield(e, 0, 5) - 1;
+    int is = at(ifield(e, 0, 5) - 1, SENGA_NLLMAX, "SRI data");
     for (int q = 0; q < 3; ++q) c.rcsrif[is][q] = rfield(e, 5 + 12 * q, 12);
     e = r.line();
     for (int q = 0; q < 5; ++q) c.rcsrif[is][3 + q] = rfield(e, 5 + 12 * q, 12);
   }
+
+  // every species/step index used by the device kernels must be in range
+  auto in_range = [](int v, int lo, int hi, const char* what) {
+    if (v < lo || v > hi) throw senga::Error(SENGA_ERR_ARG, std::string("chem.dat: index out of range in ") + what);
+  };
+  for (int st = 0; st < c.nstep; ++st) {
+    for (int q = 0; q < c.nsslen[st]; ++q) in_range(c.nsspec[st][q], 1, c.nspec, "species-list");
+    for (int q = 0; q < c.nrslen[st]; ++q) in_range(c.nrspec[st][q], 1, c.nspec, "reactant-list");
+    for (int q = 0; q < c.npslen[st]; ++q) in_range(c.npspec[st][q], 1, c.nspec, "product-list");
+    for (int q = 0; q < c.nrclen[st]; ++q) in_range(c.nrcpec[st][q], 1, c.nspec, "reactant coefficient-list");
+    for (int q = 0; q < c.npclen[st]; ++q) in_range(c.npcpec[st][q], 1, c.nspec, "product coefficient-list");
+    in_range(c.mblist[st], 0, c.nbody, "third-body step-list");
+    in_range(c.mllist[st], 0, c.nlind, "Lindemann step-list");
+    in_range(c.mtlist[st], 0, c.ntroe, "Troe step-list");
+    in_range(c.mslist[st], 0, c.nsrif, "SRI step-list");
+  }
+  in_range(c.nbody, 0, SENGA_NBDYMX, "third-body count");
+  in_range(c.nlind, 0, SENGA_NLLMAX, "Lindemann count");
+  in_range(c.ntroe, 0, SENGA_NLLMAX, "Troe count");
+  in_range(c.nsrif, 0, SENGA_NLLMAX, "SRI count");
 
   // ---- derived quantities (src/chemin.f:822-983) ----
   for (int st = 0; st < c.nstep; ++st) {
