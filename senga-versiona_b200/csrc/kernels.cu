@@ -1,17 +1,12 @@
-// Per-substage kernels of the B200 RHS + RK path.
+// Pointwise kernel of the B200 RHS + RK path and the operator-level stencils.
 //
 //   k_thermo      pointwise: TEMPER (src/temper.f:58-219), transport
 //                 properties (src/rhscal.f:515-571, 1292-1340, 3854-3885;
 //                 src/rhsvel.f:933-952), species enthalpy (rhscal.f:1444-1466)
 //                 and CHRATE (src/chrate.f:146-741), fused per grid point.
-//   k_flow        stencil: continuity, momentum, energy convection, heat
-//                 conduction, pressure and viscous work (rhscal.f:141-793,
-//                 rhsvel.f:48-2318).
-//   k_species_a   stencil: species convection/diffusion and the enthalpy
-//                 flux terms of the energy equation (rhscal.f:1030-1955).
-//   k_species_b   stencil: diffusion-correction terms (rhscal.f:3782-3938)
-//                 fused with the 2N-storage RK update (src/lincom.f:53-169,
-//                 src/fincom.f:54-168).
+//   k_deriv       operator-level derivative family (DFBYDX..D2FDYZ) reading
+//                 global memory, for the unit entry points.
+// The stencil kernels of the substage are in kernels_tiled.cu.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -359,235 +354,6 @@ __global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, const senga_
 }
 
 // -------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_flow(Geo g, Fields f) {
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= g.n) return;
-  const Pt pt = point_of(g, q);
-  const int64_t n = g.n;
-  const double* U = f.uin;
-  const Ld rho{U}, ru{U + n}, rv{U + 2 * n}, rw{U + 3 * n};
-  const Ld u{f.vel}, v{f.vel + n}, w{f.vel + 2 * n}, E{f.e}, T{f.t}, lam{f.lam}, mu{f.mu};
-  const double ruq = ru(q), rvq = rv(q), rwq = rw(q), uq = u(q), vq = v(q), wq = w(q), rhq = rho(q);
-
-  // mass-flux divergence
-  const double divm = D1<0>(g, pt, ru) + D1<1>(g, pt, rv) + D1<2>(g, pt, rw);
-  // energy convection, skew-symmetric
-  double s4 = E(q) * divm + D1<0>(g, pt, LdMul{f.e, U + n}) + D1<1>(g, pt, LdMul{f.e, U + 2 * n}) +
-              D1<2>(g, pt, LdMul{f.e, U + 3 * n});
-  double rE = -0.5 * (s4 + D1<0>(g, pt, E) * ruq + D1<1>(g, pt, E) * rvq + D1<2>(g, pt, E) * rwq);
-  // heat conduction
-  {
-    const double tx = D1<0>(g, pt, T), ty = D1<1>(g, pt, T), tz = D1<2>(g, pt, T);
-    rE = rE + (D1<0>(g, pt, lam) * tx + D1<1>(g, pt, lam) * ty + D1<2>(g, pt, lam) * tz);
-    rE = rE + (D2<0>(g, pt, T) + D2<1>(g, pt, T) + D2<2>(g, pt, T)) * lam(q);
-  }
-  // momentum convection, skew-symmetric
-  const double S4 = D1<0>(g, pt, LdMul{U + n, f.vel}) + D1<1>(g, pt, LdMul{U + n, f.vel + n}) +
-                    D1<2>(g, pt, LdMul{U + n, f.vel + 2 * n});
-  const double S5 = D1<0>(g, pt, LdMul{U + n, f.vel + n}) + D1<1>(g, pt, LdMul{U + 2 * n, f.vel + n}) +
-                    D1<2>(g, pt, LdMul{U + 2 * n, f.vel + 2 * n});
-  const double S6 = D1<0>(g, pt, LdMul{U + n, f.vel + 2 * n}) + D1<1>(g, pt, LdMul{U + 2 * n, f.vel + 2 * n}) +
-                    D1<2>(g, pt, LdMul{U + 3 * n, f.vel + 2 * n});
-  const double ux = D1<0>(g, pt, u), vy = D1<1>(g, pt, v), wz = D1<2>(g, pt, w);
-  double rU = -0.5 * (ruq * ux + (S4 + uq * divm));
-  double rV = -0.5 * (rvq * vy + (S5 + vq * divm));
-  double rW = -0.5 * (rwq * wz + (S6 + wq * divm));
-  // pressure gradient and pressure work (gradient of p - p(1,1,1))
-  {
-    const LdSub pp{f.p, __ldg(f.p)};
-    const double px = D1<0>(g, pt, pp), py = D1<1>(g, pt, pp), pz = D1<2>(g, pt, pp);
-    rU -= px;
-    rV -= py;
-    rW -= pz;
-    rE = rE - uq * px - vq * py - wq * pz;
-    rE = rE - __ldg(f.p + q) * (ux + vy + wz);
-  }
-  // viscous normal-stress terms with viscosity gradients
-  const double muq = mu(q);
-  const double mux = D1<0>(g, pt, mu), muy = D1<1>(g, pt, mu), muz = D1<2>(g, pt, mu);
-  {
-    double t6 = kFthd * ux - kTthd * (vy + wz);
-    rE = rE + muq * t6 * ux;
-    t6 = t6 * mux;
-    rU += t6;
-    rE = rE + uq * t6;
-    t6 = kFthd * vy - kTthd * (ux + wz);
-    rE = rE + muq * t6 * vy;
-    t6 = t6 * muy;
-    rV += t6;
-    rE = rE + vq * t6;
-    t6 = kFthd * wz - kTthd * (ux + vy);
-    rE = rE + muq * t6 * wz;
-    t6 = t6 * muz;
-    rW += t6;
-    rE = rE + wq * t6;
-  }
-  // xy
-  {
-    const double uy = D1<1>(g, pt, u), vx = D1<0>(g, pt, v);
-    rU = rU - 0.5 * rhq * vq * uy;
-    rV = rV - 0.5 * rhq * uq * vx;
-    const double s7 = uy + vx;
-    const double uxy = DM<0, 1>(g, pt, u), vxy = DM<0, 1>(g, pt, v);
-    double s3 = kTthd * muq * vxy;
-    rU -= s3;
-    rE = rE - uq * s3;
-    s3 = kTthd * muq * uxy;
-    rV -= s3;
-    rE = rE - vq * s3;
-    s3 = muq * (D2<1>(g, pt, u) + vxy) + s7 * muy;
-    rU += s3;
-    rE = rE + uq * s3;
-    s3 = muq * (D2<0>(g, pt, v) + uxy) + s7 * mux;
-    rV += s3;
-    rE = rE + vq * s3;
-    rE = rE + muq * s7 * s7;
-  }
-  // xz
-  {
-    const double uz = D1<2>(g, pt, u), wx = D1<0>(g, pt, w);
-    rU = rU - 0.5 * rhq * wq * uz;
-    rW = rW - 0.5 * rhq * uq * wx;
-    const double s7 = uz + wx;
-    const double uxz = DM<0, 2>(g, pt, u), wxz = DM<0, 2>(g, pt, w);
-    double s3 = kTthd * muq * wxz;
-    rU -= s3;
-    rE = rE - uq * s3;
-    s3 = kTthd * muq * uxz;
-    rW -= s3;
-    rE = rE - wq * s3;
-    s3 = muq * (D2<2>(g, pt, u) + wxz) + s7 * muz;
-    rU += s3;
-    rE = rE + uq * s3;
-    s3 = muq * (D2<0>(g, pt, w) + uxz) + s7 * mux;
-    rW += s3;
-    rE = rE + wq * s3;
-    rE = rE + muq * s7 * s7;
-  }
-  // yz
-  {
-    const double vz = D1<2>(g, pt, v), wy = D1<1>(g, pt, w);
-    rV = rV - 0.5 * rhq * wq * vz;
-    rW = rW - 0.5 * rhq * vq * wy;
-    const double s7 = vz + wy;
-    const double vyz = DM<1, 2>(g, pt, v), wyz = DM<1, 2>(g, pt, w);
-    double s3 = kTthd * muq * wyz;
-    rV -= s3;
-    rE = rE - vq * s3;
-    s3 = kTthd * muq * vyz;
-    rW -= s3;
-    rE = rE - wq * s3;
-    s3 = muq * (D2<2>(g, pt, v) + wyz) + s7 * muz;
-    rV += s3;
-    rE = rE + vq * s3;
-    s3 = muq * (D2<1>(g, pt, w) + vyz) + s7 * muy;
-    rW += s3;
-    rE = rE + wq * s3;
-    rE = rE + muq * s7 * s7;
-  }
-  // normal second derivatives
-  {
-    double fn = muq * kFthd * D2<0>(g, pt, u);
-    rU += fn;
-    rE = rE + fn * uq;
-    fn = muq * kFthd * D2<1>(g, pt, v);
-    rV += fn;
-    rE = rE + fn * vq;
-    fn = muq * kFthd * D2<2>(g, pt, w);
-    rW += fn;
-    rE = rE + fn * wq;
-  }
-  f.rhs[q] = -divm;
-  f.rhs[n + q] = rU;
-  f.rhs[2 * n + q] = rV;
-  f.rhs[3 * n + q] = rW;
-  f.rhs[4 * n + q] = rE;
-  f.divm[q] = divm;
-}
-
-// -------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_species_a(Geo g, Fields f, int nspec) {
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= g.n) return;
-  const Pt pt = point_of(g, q);
-  const int64_t n = g.n;
-  const double* U = f.uin;
-  const double ruq = __ldg(U + n + q), rvq = __ldg(U + 2 * n + q), rwq = __ldg(U + 3 * n + q);
-  const double divm = f.divm[q];
-  double rE = f.rhs[4 * n + q];
-  double vcx = 0.0, vcy = 0.0, vcz = 0.0, vt = 0.0;
-  for (int s = 0; s < nspec; ++s) {
-    const double* ys = f.y + s * n;
-    const Ld Y{ys}, RD{f.rd + s * n}, H{f.h + s * n};
-    const double yq = Y(q);
-    double rate = f.wdot[s * n + q];
-    rate = rate - 0.5 * yq * divm;
-    rate = rate - 0.5 * (D1<0>(g, pt, LdMul{ys, U + n}) + D1<1>(g, pt, LdMul{ys, U + 2 * n}) +
-                         D1<2>(g, pt, LdMul{ys, U + 3 * n}));
-    const double yx = D1<0>(g, pt, Y), yy = D1<1>(g, pt, Y), yz = D1<2>(g, pt, Y);
-    rate = rate - 0.5 * (yx * ruq + yy * rvq + yz * rwq);
-    const double rd = RD(q), hk = H(q);
-    vcx = vcx + rd * yx;
-    vcy = vcy + rd * yy;
-    vcz = vcz + rd * yz;
-    double fn = D1<0>(g, pt, RD) * yx + D1<1>(g, pt, RD) * yy + D1<2>(g, pt, RD) * yz;
-    rate = rate + fn;
-    vt = vt + fn;
-    rE = rE + fn * hk;
-    fn = D1<0>(g, pt, H) * yx + D1<1>(g, pt, H) * yy + D1<2>(g, pt, H) * yz;
-    rE = rE + fn * rd;
-    fn = (D2<0>(g, pt, Y) + D2<1>(g, pt, Y) + D2<2>(g, pt, Y)) * rd;
-    rate = rate + fn;
-    vt = vt + fn;
-    rE = rE + fn * hk;
-    f.wdot[s * n + q] = rate;
-  }
-  f.vc[q] = vcx;
-  f.vc[n + q] = vcy;
-  f.vc[2 * n + q] = vcz;
-  f.vtmp[q] = vt;
-  f.rhs[4 * n + q] = rE;
-}
-
-// -------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_species_b_rk(Geo g, Fields f, int nspec, RK rk) {
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= g.n) return;
-  const Pt pt = point_of(g, q);
-  const int64_t n = g.n;
-  const double vcx = f.vc[q], vcy = f.vc[n + q], vcz = f.vc[2 * n + q], vt = f.vtmp[q];
-  const Ld HM{f.hmix};
-  const double rE = f.rhs[4 * n + q] - HM(q) * vt - D1<0>(g, pt, HM) * vcx - D1<1>(g, pt, HM) * vcy -
-                    D1<2>(g, pt, HM) * vcz;
-  auto advance = [&](int fld, double R) {
-    const int64_t o = (int64_t)fld * n + q;
-    if (rk.last < 0) {  // right-hand side only (no RK update)
-      f.rhs[o] = R;
-      return;
-    }
-    if (f.err) f.err[o] = f.err[o] + rk.err * R;
-    if (!rk.last) {
-      const double s = f.run[o];
-      f.run[o] = s + rk.lhs * R;
-      f.uout[o] = s + rk.rhs * R;
-    } else {
-      const double s = f.run[o] + rk.lhs * R;
-      f.run[o] = s;
-      f.uout[o] = s;
-    }
-  };
-#pragma unroll
-  for (int fl = 0; fl < 4; ++fl) advance(fl, f.rhs[fl * n + q]);
-  advance(4, rE);
-  for (int s = 0; s < nspec; ++s) {
-    const Ld Y{f.y + s * n};
-    const double R = f.wdot[s * n + q] - Y(q) * vt - D1<0>(g, pt, Y) * vcx - D1<1>(g, pt, Y) * vcy -
-                     D1<2>(g, pt, Y) * vcz;
-    advance(5 + s, R);
-  }
-}
-
-// -------------------------------------------------------------------------
 __global__ void k_deriv(Geo g, int kind, const double* __restrict__ in, double* __restrict__ out) {
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= g.n) return;
@@ -622,16 +388,6 @@ void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const
     if (flmavt) k_thermo<9, true, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
     else k_thermo<9, false, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
   }
-}
-
-void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s) { k_flow<<<grid_of(g.n), kBlock, 0, s>>>(g, f); }
-
-void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s) {
-  k_species_a<<<grid_of(g.n), kBlock, 0, s>>>(g, f, nspec);
-}
-
-void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s) {
-  k_species_b_rk<<<grid_of(g.n), kBlock, 0, s>>>(g, f, nspec, rk);
 }
 
 void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s) {

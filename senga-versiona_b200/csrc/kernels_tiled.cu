@@ -1,0 +1,546 @@
+// Shared-memory-tiled stencil kernels of the substage (see tiles.cuh).
+//
+//   k_flow_t      continuity, momentum, energy convection, heat conduction,
+//                 pressure and viscous terms (src/rhscal.f:141-793,
+//                 src/rhsvel.f:48-2318) for a 32x8x2 tile; 7 staging phases.
+//   k_species_t   species convection/diffusion, correction velocity and the
+//                 species enthalpy fluxes of the energy equation
+//                 (src/rhscal.f:1030-1955) for a 32x8x4 tile, all species.
+//   k_species_rk_t diffusion-correction terms (src/rhscal.f:3782-3938) fused
+//                 with the 2N-storage RK update (src/lincom.f:53-169,
+//                 src/fincom.f:54-168).
+// The physics and the association of every product follow the reference
+// line by line within a term; terms are accumulated per grid point in a
+// different order (FP64 rounding differences only).
+#include <cuda_runtime.h>
+
+#include "senga_internal.h"
+#include "tiles.cuh"
+
+namespace senga {
+
+namespace {
+
+using namespace tile;
+
+constexpr double kThrd = 1.0 / 3.0, kTthd = 2.0 * kThrd, kFthd = 2.0 * kTthd;
+
+// flow tile
+constexpr int FX = 32, FY = 8, FZ = 2;
+constexpr int FNW = FX * FY / 32;
+// species tiles
+constexpr int SX_ = 32, SY_ = 8, SZ_ = 4;
+constexpr int SNW = SX_ * SY_ / 32;
+
+using FStar = Star<FX, FY, FZ>;
+using FBox = Box<FX, FY, FZ>;
+using FXRow = XRow<FX, FY, FZ>;
+using FYRow = YRow<FX, FY, FZ>;
+using FZCol = ZCol<FX, FY, FZ>;
+
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int kFlowSmem =
+    cmax(cmax(FXRow::SIZE + FYRow::SIZE + FZCol::SIZE + FStar::SIZE, 2 * FStar::SIZE),
+         cmax(cmax(FXRow::SIZE + 2 * FStar::SIZE, FYRow::SIZE + FStar::SIZE + FZCol::SIZE), FStar::SIZE + FBox::SIZE));
+
+using SStar = Star<SX_, SY_, SZ_>;
+using SXRow = XRow<SX_, SY_, SZ_>;
+using SYRow = YRow<SX_, SY_, SZ_>;
+using SZCol = ZCol<SX_, SY_, SZ_>;
+constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + SZCol::SIZE + SStar::SIZE;
+constexpr int kSpecRkSmem = SStar::SIZE;
+
+template <bool P>
+__global__ void __launch_bounds__(FX* FY, 2) k_flow_t(Geo g, Fields f) {
+  extern __shared__ double sm[];
+  const Origin o{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ};
+  const int tx = threadIdx.x % FX, ty = threadIdx.x / FX;
+  __shared__ Folds<FX, FY, FZ> fo;
+  fo.init(g, o);
+  __syncthreads();
+  TP tp[FZ];
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) tp[z] = make_tp(g, o, tx, ty, z);
+  const int64_t n = g.n;
+  const double* U = f.uin;
+  double divm[FZ], rU[FZ], rV[FZ], rW[FZ], rE[FZ];
+
+  // ---- phase 1: mass-flux divergence, energy convection ----
+  {
+    const FXRow bru{sm};
+    const FYRow brv{sm + FXRow::SIZE};
+    const FZCol brw{sm + FXRow::SIZE + FYRow::SIZE};
+    const FStar bE{sm + FXRow::SIZE + FYRow::SIZE + FZCol::SIZE};
+    bru.stage<FNW>(fo, Ld{U + n});
+    brv.stage<FNW>(fo, Ld{U + 2 * n});
+    brw.stage<FNW>(fo, Ld{U + 3 * n});
+    bE.stage<FNW>(fo, Ld{f.e});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) {
+      const TP& t = tp[z];
+      const double dv = d1<0, P>(g, t, bru) + d1<1, P>(g, t, brv) + d1<2, P>(g, t, brw);
+      divm[z] = dv;
+      const double s4 = bE.v(t.x, t.y, t.z) * dv + d1p<0, P>(g, t, bE, bru) + d1p<1, P>(g, t, bE, brv) +
+                        d1p<2, P>(g, t, bE, brw);
+      rE[z] = -0.5 * (s4 + d1<0, P>(g, t, bE) * bru.v(t.x, t.y, t.z) + d1<1, P>(g, t, bE) * brv.v(t.x, t.y, t.z) +
+                      d1<2, P>(g, t, bE) * brw.v(t.x, t.y, t.z));
+    }
+    __syncthreads();
+  }
+  // ---- phase 2: heat conduction ----
+  {
+    const FStar bT{sm}, bL{sm + FStar::SIZE};
+    bT.stage<FNW>(fo, Ld{f.t});
+    bL.stage<FNW>(fo, Ld{f.lam});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) {
+      const TP& t = tp[z];
+      rE[z] = rE[z] + (d1<0, P>(g, t, bL) * d1<0, P>(g, t, bT) + d1<1, P>(g, t, bL) * d1<1, P>(g, t, bT) +
+                       d1<2, P>(g, t, bL) * d1<2, P>(g, t, bT));
+      rE[z] = rE[z] + (d2<0, P>(g, t, bT) + d2<1, P>(g, t, bT) + d2<2, P>(g, t, bT)) * bL.v(t.x, t.y, t.z);
+    }
+    __syncthreads();
+  }
+  // ---- phase 3: pressure gradient (of p - p(1,1,1)) and pressure work ----
+  {
+    const FStar bP{sm};
+    bP.stage<FNW>(fo, LdSub{f.p, __ldg(f.p)});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) {
+      const TP& t = tp[z];
+      const double px = d1<0, P>(g, t, bP), py = d1<1, P>(g, t, bP), pz = d1<2, P>(g, t, bP);
+      rU[z] = -px;
+      rV[z] = -py;
+      rW[z] = -pz;
+      rE[z] = rE[z] - __ldg(f.vel + t.q) * px - __ldg(f.vel + n + t.q) * py - __ldg(f.vel + 2 * n + t.q) * pz;
+    }
+    __syncthreads();
+  }
+  // ---- phase 4: momentum fluxes d/dx_j (rho u_i u_j) ----
+  double S4[FZ], S5[FZ], S6[FZ];
+  {
+    const FXRow bA{sm};
+    const FStar bB{sm + FXRow::SIZE}, bC{sm + FXRow::SIZE + FStar::SIZE};
+    bA.stage<FNW>(fo, LdMul{U + n, f.vel});
+    bB.stage<FNW>(fo, LdMul{U + n, f.vel + n});
+    bC.stage<FNW>(fo, LdMul{U + n, f.vel + 2 * n});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) {
+      const TP& t = tp[z];
+      S4[z] = d1<0, P>(g, t, bA) + d1<1, P>(g, t, bB) + d1<2, P>(g, t, bC);
+      S5[z] = d1<0, P>(g, t, bB);
+      S6[z] = d1<0, P>(g, t, bC);
+    }
+    __syncthreads();
+  }
+  {
+    const FYRow bA{sm};
+    const FStar bB{sm + FYRow::SIZE};
+    const FZCol bC{sm + FYRow::SIZE + FStar::SIZE};
+    bA.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + n});
+    bB.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + 2 * n});
+    bC.stage<FNW>(fo, LdMul{U + 3 * n, f.vel + 2 * n});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) {
+      const TP& t = tp[z];
+      S5[z] = S5[z] + d1<1, P>(g, t, bA);
+      S5[z] = S5[z] + d1<2, P>(g, t, bB);
+      S6[z] = S6[z] + d1<1, P>(g, t, bB);
+      S6[z] = S6[z] + d1<2, P>(g, t, bC);
+    }
+    __syncthreads();
+  }
+  // ---- phase 5: velocity derivatives, viscous stresses and work ----
+  const FStar bM{sm};
+  const FBox bX{sm + FStar::SIZE};
+  bM.stage<FNW>(fo, Ld{f.mu});
+  double mux[FZ], muy[FZ], muz[FZ], ux[FZ], uy[FZ], uz[FZ], vx[FZ], vy[FZ], vz[FZ];
+  // 5a: u
+  bX.stage<FNW>(fo, Ld{f.vel});
+  __syncthreads();
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) {
+    const TP& t = tp[z];
+    const double mu = bM.v(t.x, t.y, t.z);
+    mux[z] = d1<0, P>(g, t, bM);
+    muy[z] = d1<1, P>(g, t, bM);
+    muz[z] = d1<2, P>(g, t, bM);
+    ux[z] = d1<0, P>(g, t, bX);
+    uy[z] = d1<1, P>(g, t, bX);
+    uz[z] = d1<2, P>(g, t, bX);
+    const double uq = bX.v(t.x, t.y, t.z);
+    const double vq = __ldg(f.vel + n + t.q), wq = __ldg(f.vel + 2 * n + t.q);
+    rU[z] = rU[z] + -0.5 * (__ldg(U + n + t.q) * ux[z] + (S4[z] + uq * divm[z]));
+    double fn = mu * kFthd * d2<0, P>(g, t, bX);
+    rU[z] += fn;
+    rE[z] = rE[z] + fn * uq;
+    fn = mu * d2<1, P>(g, t, bX);
+    rU[z] += fn;
+    rE[z] = rE[z] + uq * fn;
+    fn = mu * d2<2, P>(g, t, bX);
+    rU[z] += fn;
+    rE[z] = rE[z] + uq * fn;
+    const double uxy = dm<0, 1>(g, t, bX), uxz = dm<0, 2>(g, t, bX);
+    fn = kTthd * mu * uxy;
+    rV[z] -= fn;
+    rE[z] = rE[z] - vq * fn;
+    fn = mu * uxy;
+    rV[z] += fn;
+    rE[z] = rE[z] + vq * fn;
+    fn = kTthd * mu * uxz;
+    rW[z] -= fn;
+    rE[z] = rE[z] - wq * fn;
+    fn = mu * uxz;
+    rW[z] += fn;
+    rE[z] = rE[z] + wq * fn;
+  }
+  __syncthreads();
+  // 5b: v
+  bX.stage<FNW>(fo, Ld{f.vel + n});
+  __syncthreads();
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) {
+    const TP& t = tp[z];
+    const double mu = bM.v(t.x, t.y, t.z);
+    vx[z] = d1<0, P>(g, t, bX);
+    vy[z] = d1<1, P>(g, t, bX);
+    vz[z] = d1<2, P>(g, t, bX);
+    const double vq = bX.v(t.x, t.y, t.z);
+    const double uq = __ldg(f.vel + t.q), wq = __ldg(f.vel + 2 * n + t.q);
+    rV[z] = rV[z] + -0.5 * (__ldg(U + 2 * n + t.q) * vy[z] + (S5[z] + vq * divm[z]));
+    double fn = mu * kFthd * d2<1, P>(g, t, bX);
+    rV[z] += fn;
+    rE[z] = rE[z] + fn * vq;
+    fn = mu * d2<0, P>(g, t, bX);
+    rV[z] += fn;
+    rE[z] = rE[z] + vq * fn;
+    fn = mu * d2<2, P>(g, t, bX);
+    rV[z] += fn;
+    rE[z] = rE[z] + vq * fn;
+    const double vxy = dm<0, 1>(g, t, bX), vyz = dm<1, 2>(g, t, bX);
+    fn = kTthd * mu * vxy;
+    rU[z] -= fn;
+    rE[z] = rE[z] - uq * fn;
+    fn = mu * vxy;
+    rU[z] += fn;
+    rE[z] = rE[z] + uq * fn;
+    fn = kTthd * mu * vyz;
+    rW[z] -= fn;
+    rE[z] = rE[z] - wq * fn;
+    fn = mu * vyz;
+    rW[z] += fn;
+    rE[z] = rE[z] + wq * fn;
+  }
+  __syncthreads();
+  // 5c: w, then the first-derivative products
+  bX.stage<FNW>(fo, Ld{f.vel + 2 * n});
+  __syncthreads();
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) {
+    const TP& t = tp[z];
+    if (!t.valid) continue;
+    const double mu = bM.v(t.x, t.y, t.z);
+    const double wx = d1<0, P>(g, t, bX), wy = d1<1, P>(g, t, bX), wz = d1<2, P>(g, t, bX);
+    const double wq = bX.v(t.x, t.y, t.z);
+    const double uq = __ldg(f.vel + t.q), vq = __ldg(f.vel + n + t.q);
+    const double rho = __ldg(U + t.q);
+    rW[z] = rW[z] + -0.5 * (__ldg(U + 3 * n + t.q) * wz + (S6[z] + wq * divm[z]));
+    double fn = mu * kFthd * d2<2, P>(g, t, bX);
+    rW[z] += fn;
+    rE[z] = rE[z] + fn * wq;
+    fn = mu * d2<0, P>(g, t, bX);
+    rW[z] += fn;
+    rE[z] = rE[z] + wq * fn;
+    fn = mu * d2<1, P>(g, t, bX);
+    rW[z] += fn;
+    rE[z] = rE[z] + wq * fn;
+    const double wxz = dm<0, 2>(g, t, bX), wyz = dm<1, 2>(g, t, bX);
+    fn = kTthd * mu * wxz;
+    rU[z] -= fn;
+    rE[z] = rE[z] - uq * fn;
+    fn = mu * wxz;
+    rU[z] += fn;
+    rE[z] = rE[z] + uq * fn;
+    fn = kTthd * mu * wyz;
+    rV[z] -= fn;
+    rE[z] = rE[z] - vq * fn;
+    fn = mu * wyz;
+    rV[z] += fn;
+    rE[z] = rE[z] + vq * fn;
+    // pressure work p div u
+    rE[z] = rE[z] - __ldg(f.p + t.q) * (ux[z] + vy[z] + wz);
+    // normal stresses with viscosity gradients (TAUxx b,e,f)
+    double t6 = kFthd * ux[z] - kTthd * (vy[z] + wz);
+    rE[z] = rE[z] + mu * t6 * ux[z];
+    t6 = t6 * mux[z];
+    rU[z] += t6;
+    rE[z] = rE[z] + uq * t6;
+    t6 = kFthd * vy[z] - kTthd * (ux[z] + wz);
+    rE[z] = rE[z] + mu * t6 * vy[z];
+    t6 = t6 * muy[z];
+    rV[z] += t6;
+    rE[z] = rE[z] + vq * t6;
+    t6 = kFthd * wz - kTthd * (ux[z] + vy[z]);
+    rE[z] = rE[z] + mu * t6 * wz;
+    t6 = t6 * muz[z];
+    rW[z] += t6;
+    rE[z] = rE[z] + wq * t6;
+    // xy
+    rU[z] = rU[z] - 0.5 * rho * vq * uy[z];
+    rV[z] = rV[z] - 0.5 * rho * uq * vx[z];
+    double s7 = uy[z] + vx[z];
+    fn = s7 * muy[z];
+    rU[z] += fn;
+    rE[z] = rE[z] + uq * fn;
+    fn = s7 * mux[z];
+    rV[z] += fn;
+    rE[z] = rE[z] + vq * fn;
+    rE[z] = rE[z] + mu * s7 * s7;
+    // xz
+    rU[z] = rU[z] - 0.5 * rho * wq * uz[z];
+    rW[z] = rW[z] - 0.5 * rho * uq * wx;
+    s7 = uz[z] + wx;
+    fn = s7 * muz[z];
+    rU[z] += fn;
+    rE[z] = rE[z] + uq * fn;
+    fn = s7 * mux[z];
+    rW[z] += fn;
+    rE[z] = rE[z] + wq * fn;
+    rE[z] = rE[z] + mu * s7 * s7;
+    // yz
+    rV[z] = rV[z] - 0.5 * rho * wq * vz[z];
+    rW[z] = rW[z] - 0.5 * rho * vq * wy;
+    s7 = vz[z] + wy;
+    fn = s7 * muz[z];
+    rV[z] += fn;
+    rE[z] = rE[z] + vq * fn;
+    fn = s7 * muy[z];
+    rW[z] += fn;
+    rE[z] = rE[z] + wq * fn;
+    rE[z] = rE[z] + mu * s7 * s7;
+
+    f.rhs[t.q] = -divm[z];
+    f.rhs[n + t.q] = rU[z];
+    f.rhs[2 * n + t.q] = rV[z];
+    f.rhs[3 * n + t.q] = rW[z];
+    f.rhs[4 * n + t.q] = rE[z];
+    f.divm[t.q] = divm[z];
+  }
+}
+
+// -------------------------------------------------------------------------
+template <bool P>
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int nspec) {
+  extern __shared__ double sm[];
+  const Origin o{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_};
+  const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
+  __shared__ Folds<SX_, SY_, SZ_> fo;
+  fo.init(g, o);
+  __syncthreads();
+  TP tp[SZ_];
+#pragma unroll
+  for (int z = 0; z < SZ_; ++z) tp[z] = make_tp(g, o, tx, ty, z);
+  const int64_t n = g.n;
+  const double* U = f.uin;
+  const SXRow bru{sm};
+  const SYRow brv{sm + SXRow::SIZE};
+  const SZCol brw{sm + SXRow::SIZE + SYRow::SIZE};
+  const SStar bS{sm + SXRow::SIZE + SYRow::SIZE + SZCol::SIZE};
+  bru.stage<SNW>(fo, Ld{U + n});
+  brv.stage<SNW>(fo, Ld{U + 2 * n});
+  brw.stage<SNW>(fo, Ld{U + 3 * n});
+  double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
+#pragma unroll
+  for (int z = 0; z < SZ_; ++z) {
+    vcx[z] = vcy[z] = vcz[z] = vt[z] = 0.0;
+    rE[z] = tp[z].valid ? f.rhs[4 * n + tp[z].q] : 0.0;
+    dvm[z] = tp[z].valid ? f.divm[tp[z].q] : 0.0;
+  }
+  for (int s = 0; s < nspec; ++s) {
+    double rate[SZ_], yx[SZ_], yy[SZ_], yz[SZ_], lap[SZ_], fn1[SZ_], fn3[SZ_], rd[SZ_];
+    // Y_k: convection, gradient, Laplacian
+    bS.stage<SNW>(fo, Ld{f.y + s * n});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < SZ_; ++z) {
+      const TP& t = tp[z];
+      const double yq = bS.v(t.x, t.y, t.z);
+      double r = f.wdot[s * n + t.q];
+      r = r - 0.5 * yq * dvm[z];
+      r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1p<2, P>(g, t, bS, brw));
+      yx[z] = d1<0, P>(g, t, bS);
+      yy[z] = d1<1, P>(g, t, bS);
+      yz[z] = d1<2, P>(g, t, bS);
+      r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * brw.v(t.x, t.y, t.z));
+      rate[z] = r;
+      lap[z] = d2<0, P>(g, t, bS) + d2<1, P>(g, t, bS) + d2<2, P>(g, t, bS);
+    }
+    __syncthreads();
+    // rho D_k: correction velocity, diffusive flux divergence
+    bS.stage<SNW>(fo, Ld{f.rd + s * n});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < SZ_; ++z) {
+      const TP& t = tp[z];
+      rd[z] = bS.v(t.x, t.y, t.z);
+      vcx[z] = vcx[z] + rd[z] * yx[z];
+      vcy[z] = vcy[z] + rd[z] * yy[z];
+      vcz[z] = vcz[z] + rd[z] * yz[z];
+      const double fn = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1<2, P>(g, t, bS) * yz[z];
+      rate[z] = rate[z] + fn;
+      vt[z] = vt[z] + fn;
+      fn1[z] = fn;
+      const double f3 = lap[z] * rd[z];
+      rate[z] = rate[z] + f3;
+      vt[z] = vt[z] + f3;
+      fn3[z] = f3;
+    }
+    __syncthreads();
+    // h_k: enthalpy fluxes of the energy equation
+    bS.stage<SNW>(fo, Ld{f.h + s * n});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < SZ_; ++z) {
+      const TP& t = tp[z];
+      const double hk = bS.v(t.x, t.y, t.z);
+      rE[z] = rE[z] + fn1[z] * hk;
+      const double fn2 = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1<2, P>(g, t, bS) * yz[z];
+      rE[z] = rE[z] + fn2 * rd[z];
+      rE[z] = rE[z] + fn3[z] * hk;
+      if (t.valid) f.wdot[s * n + t.q] = rate[z];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int z = 0; z < SZ_; ++z) {
+    const TP& t = tp[z];
+    if (!t.valid) continue;
+    f.vc[t.q] = vcx[z];
+    f.vc[n + t.q] = vcy[z];
+    f.vc[2 * n + t.q] = vcz[z];
+    f.vtmp[t.q] = vt[z];
+    f.rhs[4 * n + t.q] = rE[z];
+  }
+}
+
+// -------------------------------------------------------------------------
+template <bool P>
+__global__ void __launch_bounds__(SX_* SY_) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
+  extern __shared__ double sm[];
+  const Origin o{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_};
+  const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
+  __shared__ Folds<SX_, SY_, SZ_> fo;
+  fo.init(g, o);
+  __syncthreads();
+  TP tp[SZ_];
+#pragma unroll
+  for (int z = 0; z < SZ_; ++z) tp[z] = make_tp(g, o, tx, ty, z);
+  const int64_t n = g.n;
+  const SStar bS{sm};
+  auto advance = [&](int fld, int64_t q, double R) {
+    const int64_t idx = (int64_t)fld * n + q;
+    if (rk.last < 0) {  // right-hand side only
+      f.rhs[idx] = R;
+      return;
+    }
+    if (f.err) f.err[idx] = f.err[idx] + rk.err * R;
+    if (!rk.last) {
+      const double s = f.run[idx];
+      f.run[idx] = s + rk.lhs * R;
+      f.uout[idx] = s + rk.rhs * R;
+    } else {
+      const double s = f.run[idx] + rk.lhs * R;
+      f.run[idx] = s;
+      f.uout[idx] = s;
+    }
+  };
+  double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_];
+#pragma unroll
+  for (int z = 0; z < SZ_; ++z) {
+    const int64_t q = tp[z].q;
+    vcx[z] = f.vc[q];
+    vcy[z] = f.vc[n + q];
+    vcz[z] = f.vc[2 * n + q];
+    vt[z] = f.vtmp[q];
+  }
+  bS.stage<SNW>(fo, Ld{f.hmix});
+  __syncthreads();
+#pragma unroll
+  for (int z = 0; z < SZ_; ++z) {
+    const TP& t = tp[z];
+    if (!t.valid) continue;
+    const double rE = f.rhs[4 * n + t.q] - bS.v(t.x, t.y, t.z) * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
+                      d1<1, P>(g, t, bS) * vcy[z] - d1<2, P>(g, t, bS) * vcz[z];
+#pragma unroll
+    for (int fl = 0; fl < 4; ++fl) advance(fl, t.q, f.rhs[fl * n + t.q]);
+    advance(4, t.q, rE);
+  }
+  for (int s = 0; s < nspec; ++s) {
+    __syncthreads();
+    bS.stage<SNW>(fo, Ld{f.y + s * n});
+    __syncthreads();
+#pragma unroll
+    for (int z = 0; z < SZ_; ++z) {
+      const TP& t = tp[z];
+      if (!t.valid) continue;
+      const double R = f.wdot[s * n + t.q] - bS.v(t.x, t.y, t.z) * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
+                       d1<1, P>(g, t, bS) * vcy[z] - d1<2, P>(g, t, bS) * vcz[z];
+      advance(5 + s, t.q, R);
+    }
+  }
+}
+
+dim3 tiles(const Geo& g, int tx, int ty, int tz) {
+  return dim3((unsigned)((g.nx + tx - 1) / tx), (unsigned)((g.ny + ty - 1) / ty), (unsigned)((g.nz + tz - 1) / tz));
+}
+
+template <bool P>
+void set_attrs() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(k_flow_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
+  cudaFuncSetAttribute(k_species_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
+  cudaFuncSetAttribute(k_species_rk_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
+  done = true;
+}
+
+bool all_periodic(const Geo& g) { return g.per[0] && g.per[1] && g.per[2]; }
+
+}  // namespace
+
+void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s) {
+  if (all_periodic(g)) {
+    set_attrs<true>();
+    k_flow_t<true><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f);
+  } else {
+    set_attrs<false>();
+    k_flow_t<false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f);
+  }
+}
+
+void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s) {
+  if (all_periodic(g)) {
+    set_attrs<true>();
+    k_species_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec);
+  } else {
+    set_attrs<false>();
+    k_species_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec);
+  }
+}
+
+void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s) {
+  if (all_periodic(g)) {
+    set_attrs<true>();
+    k_species_rk_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk);
+  } else {
+    set_attrs<false>();
+    k_species_rk_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk);
+  }
+}
+
+}  // namespace senga

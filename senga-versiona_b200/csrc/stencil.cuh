@@ -62,91 +62,98 @@ __device__ __forceinline__ int64_t woff(const Geo& g, int c, int m) {
   return (int64_t)(cm - c) * strd<DIR>(g);
 }
 
-// First derivative along DIR at p of the field given by accessor f(q).
-template <int DIR, class F>
-__device__ __forceinline__ double D1(const Geo& g, const Pt& p, const F& f) {
+// ---- scheme cores -----------------------------------------------------------
+// v(m) returns the field m points along the direction from the evaluation
+// point; c is the point's coordinate in that direction, n the extent, per the
+// periodic flag. Results are unscaled (the caller multiplies by 1/Delta^k).
+template <class V>
+__device__ __forceinline__ double d1core(const V& v, int c, int n, int per) {
   using namespace fdc;
-  const int n = ext<DIR>(g), c = crd<DIR>(p);
-  double r;
-  if (g.per[DIR] || (c >= 5 && c <= n - 6)) {
-    auto v = [&](int m) { return f(p.q + woff<DIR>(g, c, m)); };
-    r = a1 * (v(1) - v(-1)) + b1 * (v(2) - v(-2)) + c1 * (v(3) - v(-3)) + d1 * (v(4) - v(-4)) +
-        e1 * (v(5) - v(-5));
-  } else {
-    const int64_t s = strd<DIR>(g);
-    auto a = [&](int abs0) { return f(p.q + (int64_t)(abs0 - c) * s); };  // 0-based absolute index
-    if (c < 5) {
-      switch (c) {
-        case 0: r = p1a * (a(1) - a(0)) + p1b * (a(2) - a(0)) + p1c * (a(3) - a(0)) + p1d * (a(4) - a(0)); break;
-        case 1: r = p2a * (a(0) - a(1)) + p2b * (a(2) - a(1)) + p2c * (a(3) - a(1)) + p2d * (a(4) - a(1)); break;
-        case 2: r = p3a * (a(3) - a(1)) + p3b * (a(4) - a(0)); break;
-        case 3: r = p4a * (a(4) - a(2)) + p4b * (a(5) - a(1)) + p4c * (a(6) - a(0)); break;
-        default: r = p5a * (a(5) - a(3)) + p5b * (a(6) - a(2)) + p5c * (a(7) - a(1)) + p5d * (a(8) - a(0)); break;
-      }
-    } else {
-      const int L = n - 1;
-      switch (L - c) {
-        case 4: r = p5a * (a(L - 3) - a(L - 5)) + p5b * (a(L - 2) - a(L - 6)) + p5c * (a(L - 1) - a(L - 7)) + p5d * (a(L) - a(L - 8)); break;
-        case 3: r = p4a * (a(L - 2) - a(L - 4)) + p4b * (a(L - 1) - a(L - 5)) + p4c * (a(L) - a(L - 6)); break;
-        case 2: r = p3a * (a(L - 1) - a(L - 3)) + p3b * (a(L) - a(L - 4)); break;
-        case 1: r = p2a * (a(L - 1) - a(L)) + p2b * (a(L - 1) - a(L - 2)) + p2c * (a(L - 1) - a(L - 3)) + p2d * (a(L - 1) - a(L - 4)); break;
-        default: r = p1a * (a(L) - a(L - 1)) + p1b * (a(L) - a(L - 2)) + p1c * (a(L) - a(L - 3)) + p1d * (a(L) - a(L - 4)); break;
-      }
+  if (per || (c >= 5 && c <= n - 6))
+    return a1 * (v(1) - v(-1)) + b1 * (v(2) - v(-2)) + c1 * (v(3) - v(-3)) + d1 * (v(4) - v(-4)) +
+           e1 * (v(5) - v(-5));
+  auto a = [&](int abs0) { return v(abs0 - c); };  // 0-based absolute index
+  if (c < 5) {
+    switch (c) {
+      case 0: return p1a * (a(1) - a(0)) + p1b * (a(2) - a(0)) + p1c * (a(3) - a(0)) + p1d * (a(4) - a(0));
+      case 1: return p2a * (a(0) - a(1)) + p2b * (a(2) - a(1)) + p2c * (a(3) - a(1)) + p2d * (a(4) - a(1));
+      case 2: return p3a * (a(3) - a(1)) + p3b * (a(4) - a(0));
+      case 3: return p4a * (a(4) - a(2)) + p4b * (a(5) - a(1)) + p4c * (a(6) - a(0));
+      default: return p5a * (a(5) - a(3)) + p5b * (a(6) - a(2)) + p5c * (a(7) - a(1)) + p5d * (a(8) - a(0));
     }
   }
-  return r * g.ovd[DIR];
+  const int L = n - 1;
+  switch (L - c) {
+    case 4: return p5a * (a(L - 3) - a(L - 5)) + p5b * (a(L - 2) - a(L - 6)) + p5c * (a(L - 1) - a(L - 7)) + p5d * (a(L) - a(L - 8));
+    case 3: return p4a * (a(L - 2) - a(L - 4)) + p4b * (a(L - 1) - a(L - 5)) + p4c * (a(L) - a(L - 6));
+    case 2: return p3a * (a(L - 1) - a(L - 3)) + p3b * (a(L) - a(L - 4));
+    case 1: return p2a * (a(L - 1) - a(L)) + p2b * (a(L - 1) - a(L - 2)) + p2c * (a(L - 1) - a(L - 3)) + p2d * (a(L - 1) - a(L - 4));
+    default: return p1a * (a(L) - a(L - 1)) + p1b * (a(L) - a(L - 2)) + p1c * (a(L) - a(L - 3)) + p1d * (a(L) - a(L - 4));
+  }
 }
 
-// Second derivative along DIR.
-template <int DIR, class F>
-__device__ __forceinline__ double D2(const Geo& g, const Pt& p, const F& f) {
+template <class V>
+__device__ __forceinline__ double d2core(const V& v, int c, int n, int per) {
   using namespace fdc;
-  const int n = ext<DIR>(g), c = crd<DIR>(p);
-  double r;
-  if (g.per[DIR] || (c >= 5 && c <= n - 6)) {
-    auto v = [&](int m) { return f(p.q + woff<DIR>(g, c, m)); };
-    const double f0 = f(p.q);
-    r = a2 * ((v(1) - f0) - (f0 - v(-1))) + b2 * ((v(2) - f0) - (f0 - v(-2))) +
-        c2 * ((v(3) - f0) - (f0 - v(-3))) + d2 * ((v(4) - f0) - (f0 - v(-4))) +
-        e2 * ((v(5) - f0) - (f0 - v(-5)));
-  } else {
-    const int64_t s = strd<DIR>(g);
-    auto a = [&](int abs0) { return f(p.q + (int64_t)(abs0 - c) * s); };
-    if (c < 5) {
-      switch (c) {
-        case 0: r = s1a * (a(1) - a(0)) + s1b * (a(2) - a(0)) + s1c * (a(3) - a(0)) + s1d * (a(4) - a(0)) + s1e * (a(5) - a(0)); break;
-        case 1: r = s2a * (a(0) - a(1)) + s2b * (a(2) - a(1)) + s2c * (a(3) - a(1)) + s2d * (a(4) - a(1)) + s2e * (a(5) - a(1)); break;
-        case 2: r = s3a * ((a(3) - a(2)) - (a(2) - a(1))) + s3b * ((a(4) - a(2)) - (a(2) - a(0))); break;
-        case 3: r = s4a * ((a(4) - a(3)) - (a(3) - a(2))) + s4b * ((a(5) - a(3)) - (a(3) - a(1))) + s4c * ((a(6) - a(3)) - (a(3) - a(0))); break;
-        default: r = s5a * ((a(5) - a(4)) - (a(4) - a(3))) + s5b * ((a(6) - a(4)) - (a(4) - a(2))) + s5c * ((a(7) - a(4)) - (a(4) - a(1))) + s5d * ((a(8) - a(4)) - (a(4) - a(0))); break;
-      }
-    } else {
-      const int L = n - 1;
-      switch (L - c) {
-        case 4: r = s5a * ((a(L - 3) - a(L - 4)) - (a(L - 4) - a(L - 5))) + s5b * ((a(L - 2) - a(L - 4)) - (a(L - 4) - a(L - 6))) + s5c * ((a(L - 1) - a(L - 4)) - (a(L - 4) - a(L - 7))) + s5d * ((a(L) - a(L - 4)) - (a(L - 4) - a(L - 8))); break;
-        case 3: r = s4a * ((a(L - 2) - a(L - 3)) - (a(L - 3) - a(L - 4))) + s4b * ((a(L - 1) - a(L - 3)) - (a(L - 3) - a(L - 5))) + s4c * ((a(L) - a(L - 3)) - (a(L - 3) - a(L - 6))); break;
-        case 2: r = s3a * ((a(L - 1) - a(L - 2)) - (a(L - 2) - a(L - 3))) + s3b * ((a(L) - a(L - 2)) - (a(L - 2) - a(L - 4))); break;
-        case 1: r = s2a * (a(L) - a(L - 1)) + s2b * (a(L - 2) - a(L - 1)) + s2c * (a(L - 3) - a(L - 1)) + s2d * (a(L - 4) - a(L - 1)) + s2e * (a(L - 5) - a(L - 1)); break;
-        default: r = s1a * (a(L - 1) - a(L)) + s1b * (a(L - 2) - a(L)) + s1c * (a(L - 3) - a(L)) + s1d * (a(L - 4) - a(L)) + s1e * (a(L - 5) - a(L)); break;
-      }
+  if (per || (c >= 5 && c <= n - 6)) {
+    const double f0 = v(0);
+    return a2 * ((v(1) - f0) - (f0 - v(-1))) + b2 * ((v(2) - f0) - (f0 - v(-2))) +
+           c2 * ((v(3) - f0) - (f0 - v(-3))) + d2 * ((v(4) - f0) - (f0 - v(-4))) +
+           e2 * ((v(5) - f0) - (f0 - v(-5)));
+  }
+  auto a = [&](int abs0) { return v(abs0 - c); };
+  if (c < 5) {
+    switch (c) {
+      case 0: return s1a * (a(1) - a(0)) + s1b * (a(2) - a(0)) + s1c * (a(3) - a(0)) + s1d * (a(4) - a(0)) + s1e * (a(5) - a(0));
+      case 1: return s2a * (a(0) - a(1)) + s2b * (a(2) - a(1)) + s2c * (a(3) - a(1)) + s2d * (a(4) - a(1)) + s2e * (a(5) - a(1));
+      case 2: return s3a * ((a(3) - a(2)) - (a(2) - a(1))) + s3b * ((a(4) - a(2)) - (a(2) - a(0)));
+      case 3: return s4a * ((a(4) - a(3)) - (a(3) - a(2))) + s4b * ((a(5) - a(3)) - (a(3) - a(1))) + s4c * ((a(6) - a(3)) - (a(3) - a(0)));
+      default: return s5a * ((a(5) - a(4)) - (a(4) - a(3))) + s5b * ((a(6) - a(4)) - (a(4) - a(2))) + s5c * ((a(7) - a(4)) - (a(4) - a(1))) + s5d * ((a(8) - a(4)) - (a(4) - a(0)));
     }
   }
-  return r * (DIR == 0 ? g.ovd2[0] : DIR == 1 ? g.ovd2[1] : g.ovd2[2]);
+  const int L = n - 1;
+  switch (L - c) {
+    case 4: return s5a * ((a(L - 3) - a(L - 4)) - (a(L - 4) - a(L - 5))) + s5b * ((a(L - 2) - a(L - 4)) - (a(L - 4) - a(L - 6))) + s5c * ((a(L - 1) - a(L - 4)) - (a(L - 4) - a(L - 7))) + s5d * ((a(L) - a(L - 4)) - (a(L - 4) - a(L - 8)));
+    case 3: return s4a * ((a(L - 2) - a(L - 3)) - (a(L - 3) - a(L - 4))) + s4b * ((a(L - 1) - a(L - 3)) - (a(L - 3) - a(L - 5))) + s4c * ((a(L) - a(L - 3)) - (a(L - 3) - a(L - 6)));
+    case 2: return s3a * ((a(L - 1) - a(L - 2)) - (a(L - 2) - a(L - 3))) + s3b * ((a(L) - a(L - 2)) - (a(L - 2) - a(L - 4)));
+    case 1: return s2a * (a(L) - a(L - 1)) + s2b * (a(L - 2) - a(L - 1)) + s2c * (a(L - 3) - a(L - 1)) + s2d * (a(L - 4) - a(L - 1)) + s2e * (a(L - 5) - a(L - 1));
+    default: return s1a * (a(L - 1) - a(L)) + s1b * (a(L - 2) - a(L)) + s1c * (a(L - 3) - a(L)) + s1d * (a(L - 4) - a(L)) + s1e * (a(L - 5) - a(L));
+  }
 }
 
-// Mixed derivative in the plane (D1DIR, D2DIR), interior diagonal scheme.
-// Both directions periodic (bounded edges/corners are rejected on the host).
-template <int DA, int DB, class F>
-__device__ __forceinline__ double DM(const Geo& g, const Pt& p, const F& f) {
+// Mixed derivative, interior diagonal scheme; v(ma, mb) is the value ma, mb
+// points away along the two directions.
+template <class V2>
+__device__ __forceinline__ double dmcore(const V2& v) {
   using namespace fdc;
-  const int ca = crd<DA>(p), cb = crd<DB>(p);
-  auto v = [&](int ma, int mb) { return f(p.q + woff<DA>(g, ca, ma) + woff<DB>(g, cb, mb)); };
   const double fa = v(1, 1) - v(1, -1) - v(-1, 1) + v(-1, -1);
   const double fb = v(2, 2) - v(2, -2) - v(-2, 2) + v(-2, -2);
   const double fc = v(3, 3) - v(3, -3) - v(-3, 3) + v(-3, -3);
   const double fd = v(4, 4) - v(4, -4) - v(-4, 4) + v(-4, -4);
   const double fe = v(5, 5) - v(5, -5) - v(-5, 5) + v(-5, -5);
-  return (ax * fa + bx * fb + cx * fc + dx * fd + ex * fe) * g.ovd[DA] * g.ovd[DB];
+  return ax * fa + bx * fb + cx * fc + dx * fd + ex * fe;
+}
+
+// ---- global-memory forms (operator-level entry points) ----------------------
+// Periodic directions wrap the index; bounded ones never leave the domain
+// because the closures only read inward.
+template <int DIR, class F>
+__device__ __forceinline__ double D1(const Geo& g, const Pt& p, const F& f) {
+  const int n = ext<DIR>(g), c = crd<DIR>(p);
+  auto v = [&](int m) { return f(p.q + woff<DIR>(g, c, m)); };
+  return d1core(v, c, n, g.per[DIR]) * g.ovd[DIR];
+}
+template <int DIR, class F>
+__device__ __forceinline__ double D2(const Geo& g, const Pt& p, const F& f) {
+  const int n = ext<DIR>(g), c = crd<DIR>(p);
+  auto v = [&](int m) { return f(p.q + woff<DIR>(g, c, m)); };
+  return d2core(v, c, n, g.per[DIR]) * g.ovd2[DIR];
+}
+template <int DA, int DB, class F>
+__device__ __forceinline__ double DM(const Geo& g, const Pt& p, const F& f) {
+  const int ca = crd<DA>(p), cb = crd<DB>(p);
+  auto v = [&](int ma, int mb) { return f(p.q + woff<DA>(g, ca, ma) + woff<DB>(g, cb, mb)); };
+  return dmcore(v) * g.ovd[DA] * g.ovd[DB];
 }
 
 // ---- accessors ----

@@ -1,0 +1,266 @@
+// Shared-memory tiles for the fused stencil kernels.
+//
+// A CTA owns a TX x TY x TZ block of grid points; thread (tx, ty) owns the TZ
+// points of one z-column. Every field a kernel differentiates is staged once
+// per tile into shared memory with exactly the halo its derivatives need (5
+// points, the half-width of the 11-point stencils), then all derivatives of
+// that field at the tile's points are read from shared memory. Halo points of
+// periodic directions are wrapped into the domain (the single-rank halo copy
+// of src/parfer.f:840-873); in a bounded direction they are clamped and never
+// read, because the one-sided closures only look inward.
+//
+// Buffer layouts (doubles):
+//   Star : slab[TZ][TY+2H][TX+2H] + zhalo[2H][TY][TX]   first/second derivatives
+//          in x, y, z (+ xy corners for the xy mixed derivative when loaded)
+//   Box  : [TZ+2H][TY+2H][TX+2H]                         all mixed derivatives
+//   XRow : [TZ][TY][TX+2H]    YRow : [TZ][TY+2H][TX]    ZCol : [TZ+2H][TY][TX]
+#pragma once
+#include <cstdint>
+
+#include "stencil.cuh"
+
+namespace senga {
+namespace tile {
+
+constexpr int H = 5;
+
+struct Origin {
+  int x0, y0, z0;
+};
+
+// Fold a coordinate into the domain: periodic wrap, or clamp (bounded
+// directions: the clamped halo values are never read by the closures).
+__device__ __forceinline__ int fold(int c, int n, int per) {
+  if (per) {
+    while (c < 0) c += n;
+    while (c >= n) c -= n;
+    return c;
+  }
+  return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+// Element offsets of the tile's (halo-extended) x, y and z coordinates,
+// folded into the domain once per CTA: ox[x+H], oy[y+H]*nx, oz[z+H]*nx*ny.
+template <int TX, int TY, int TZ>
+struct Folds {
+  static constexpr int NX = TX + 2 * H, NY = TY + 2 * H, NZ = TZ + 2 * H;
+  int64_t ox[NX], oy[NY], oz[NZ];
+  __device__ void init(const Geo& g, const Origin& o) {
+    for (int e = threadIdx.x; e < NX + NY + NZ; e += blockDim.x) {
+      if (e < NX) ox[e] = fold(o.x0 + e - H, g.nx, g.per[0]);
+      else if (e < NX + NY) oy[e - NX] = (int64_t)fold(o.y0 + (e - NX) - H, g.ny, g.per[1]) * g.nx;
+      else oz[e - NX - NY] = (int64_t)fold(o.z0 + (e - NX - NY) - H, g.nz, g.per[2]) * ((int64_t)g.nx * g.ny);
+    }
+  }
+};
+
+// Stage NR rows of a region (NW warps per CTA). Row r covers tile-local x in
+// [XLO, XLO+XL) at tile-local (y, z) and lands at dst[d*DS + (x - XLO)], where
+// rowyz(r, y, z, d) gives y, z and the destination row d. Warps take rows,
+// lanes take x; rows are processed four at a time so that every thread keeps
+// several global loads in flight before it writes shared memory.
+template <int XL, int XLO, int NR, int NW, class FO, class RowYZ, class F>
+__device__ __forceinline__ void stage_rows(double* dst, int DS, const FO& fo, const RowYZ& rowyz, const F& f) {
+  constexpr int NK = (XL + 31) / 32;
+  constexpr int ITER = (NR + NW - 1) / NW;
+  constexpr int UB = 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t gx[NK];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) gx[k] = (lane + 32 * k < XL) ? fo.ox[XLO + H + lane + 32 * k] : 0;
+#pragma unroll 1
+  for (int i0 = 0; i0 < ITER; i0 += UB) {
+    double val[UB][NK];
+    int drow[UB];
+#pragma unroll
+    for (int u = 0; u < UB; ++u) {
+      const int r = warp + (i0 + u) * NW;
+      drow[u] = -1;
+      if (i0 + u < ITER && r < NR) {
+        int y, z;
+        rowyz(r, y, z, drow[u]);
+        const int64_t base = fo.oy[y + H] + fo.oz[z + H];
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (lane + 32 * k < XL) val[u][k] = f(base + gx[k]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UB; ++u)
+      if (drow[u] >= 0) {
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (lane + 32 * k < XL) dst[drow[u] * DS + lane + 32 * k] = val[u][k];
+      }
+  }
+}
+
+template <int TX, int TY, int TZ>
+struct Star {
+  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H;
+  static constexpr int SLAB = TZ * SY * SX;
+  static constexpr int SIZE = SLAB + 2 * H * TY * TX;
+  double* p;
+  __device__ __forceinline__ double v(int x, int y, int z) const {
+    if (z >= 0 && z < TZ) return p[(z * SY + (y + H)) * SX + (x + H)];
+    const int zz = z < 0 ? z + H : z - TZ + H;
+    return p[SLAB + (zz * TY + y) * TX + x];
+  }
+  // XYC: also load the xy corners (only the xy mixed derivative reads them)
+  template <int NW, bool XYC = false, class F>
+  __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
+    // in-tile rows of every in-tile plane, with the x halos
+    stage_rows<SX, -H, TY * TZ, NW>(p, SX, fo,
+                                    [](int r, int& y, int& z, int& d) {
+                                      y = r % TY;
+                                      z = r / TY;
+                                      d = z * SY + y + H;
+                                    },
+                                    f);
+    // the y-halo rows of every in-tile plane (with or without the corners)
+    auto yh = [](int r, int& y, int& z, int& d) {
+      const int k = r % (2 * H);
+      y = k < H ? k - H : TY + k - H;
+      z = r / (2 * H);
+      d = z * SY + y + H;
+    };
+    if (XYC) stage_rows<SX, -H, 2 * H * TZ, NW>(p, SX, fo, yh, f);
+    else stage_rows<TX, 0, 2 * H * TZ, NW>(p + H, SX, fo, yh, f);
+    // z halos: in-tile rows of the 2H planes below and above the tile
+    stage_rows<TX, 0, 2 * H * TY, NW>(p + SLAB, TX, fo,
+                                      [](int r, int& y, int& z, int& d) {
+                                        y = r % TY;
+                                        const int zz = r / TY;
+                                        z = zz < H ? zz - H : TZ + zz - H;
+                                        d = r;
+                                      },
+                                      f);
+  }
+};
+
+template <int TX, int TY, int TZ>
+struct Box {
+  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H, SZ = TZ + 2 * H;
+  static constexpr int SIZE = SX * SY * SZ;
+  double* p;
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[((z + H) * SY + (y + H)) * SX + (x + H)]; }
+  template <int NW, class F>
+  __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
+    stage_rows<SX, -H, SY * SZ, NW>(p, SX, fo,
+                                    [](int r, int& y, int& z, int& d) {
+                                      y = r % SY - H;
+                                      z = r / SY - H;
+                                      d = r;
+                                    },
+                                    f);
+  }
+};
+
+// One-direction halo buffers (for fluxes differentiated along one axis only)
+template <int TX, int TY, int TZ>
+struct XRow {
+  static constexpr int SX = TX + 2 * H, SIZE = TZ * TY * SX;
+  double* p;
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[(z * TY + y) * SX + (x + H)]; }
+  template <int NW, class F>
+  __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
+    stage_rows<SX, -H, TY * TZ, NW>(p, SX, fo,
+                                    [](int r, int& y, int& z, int& d) {
+                                      y = r % TY;
+                                      z = r / TY;
+                                      d = r;
+                                    },
+                                    f);
+  }
+};
+template <int TX, int TY, int TZ>
+struct YRow {
+  static constexpr int SY = TY + 2 * H, SIZE = TZ * SY * TX;
+  double* p;
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[(z * SY + (y + H)) * TX + x]; }
+  template <int NW, class F>
+  __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
+    stage_rows<TX, 0, SY * TZ, NW>(p, TX, fo,
+                                   [](int r, int& y, int& z, int& d) {
+                                     y = r % SY - H;
+                                     z = r / SY;
+                                     d = r;
+                                   },
+                                   f);
+  }
+};
+template <int TX, int TY, int TZ>
+struct ZCol {
+  static constexpr int SZ = TZ + 2 * H, SIZE = SZ * TY * TX;
+  double* p;
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[((z + H) * TY + y) * TX + x]; }
+  template <int NW, class F>
+  __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
+    stage_rows<TX, 0, TY * SZ, NW>(p, TX, fo,
+                                   [](int r, int& y, int& z, int& d) {
+                                     y = r % TY;
+                                     z = r / TY - H;
+                                     d = r;
+                                   },
+                                   f);
+  }
+};
+
+// A grid point of the tile as seen by one thread.
+struct TP {
+  int x, y, z;      // tile-local
+  int gx, gy, gz;   // global
+  int64_t q;        // global linear index
+  bool valid;       // inside the domain (partial edge tiles)
+};
+
+__device__ __forceinline__ TP make_tp(const Geo& g, const Origin& o, int x, int y, int z) {
+  TP t;
+  t.x = x;
+  t.y = y;
+  t.z = z;
+  t.gx = o.x0 + x;
+  t.gy = o.y0 + y;
+  t.gz = o.z0 + z;
+  t.valid = t.gx < g.nx && t.gy < g.ny && t.gz < g.nz;
+  t.q = t.valid ? (int64_t)t.gx + (int64_t)g.nx * ((int64_t)t.gy + (int64_t)g.ny * t.gz) : 0;
+  return t;
+}
+
+// ---- derivatives of staged fields (scaled) ----
+// P = true: every direction is periodic (known at compile time, no closure
+// branch); P = false: the box's per-direction flags select the closures.
+template <int DIR, bool P, class B>
+__device__ __forceinline__ double d1(const Geo& g, const TP& t, const B& b) {
+  if (DIR == 0) return d1core([&](int m) { return b.v(t.x + m, t.y, t.z); }, t.gx, g.nx, P ? 1 : g.per[0]) * g.ovd[0];
+  if (DIR == 1) return d1core([&](int m) { return b.v(t.x, t.y + m, t.z); }, t.gy, g.ny, P ? 1 : g.per[1]) * g.ovd[1];
+  return d1core([&](int m) { return b.v(t.x, t.y, t.z + m); }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd[2];
+}
+// derivative of the pointwise product of two staged fields
+template <int DIR, bool P, class A, class B>
+__device__ __forceinline__ double d1p(const Geo& g, const TP& t, const A& a, const B& b) {
+  if (DIR == 0)
+    return d1core([&](int m) { return a.v(t.x + m, t.y, t.z) * b.v(t.x + m, t.y, t.z); }, t.gx, g.nx, P ? 1 : g.per[0]) * g.ovd[0];
+  if (DIR == 1)
+    return d1core([&](int m) { return a.v(t.x, t.y + m, t.z) * b.v(t.x, t.y + m, t.z); }, t.gy, g.ny, P ? 1 : g.per[1]) * g.ovd[1];
+  return d1core([&](int m) { return a.v(t.x, t.y, t.z + m) * b.v(t.x, t.y, t.z + m); }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd[2];
+}
+template <int DIR, bool P, class B>
+__device__ __forceinline__ double d2(const Geo& g, const TP& t, const B& b) {
+  if (DIR == 0) return d2core([&](int m) { return b.v(t.x + m, t.y, t.z); }, t.gx, g.nx, P ? 1 : g.per[0]) * g.ovd2[0];
+  if (DIR == 1) return d2core([&](int m) { return b.v(t.x, t.y + m, t.z); }, t.gy, g.ny, P ? 1 : g.per[1]) * g.ovd2[1];
+  return d2core([&](int m) { return b.v(t.x, t.y, t.z + m); }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd2[2];
+}
+template <int DA, int DB, class B>
+__device__ __forceinline__ double dm(const Geo& g, const TP& t, const B& b) {
+  auto v = [&](int ma, int mb) {
+    const int dx = (DA == 0 ? ma : 0) + (DB == 0 ? mb : 0);
+    const int dy = (DA == 1 ? ma : 0) + (DB == 1 ? mb : 0);
+    const int dz = (DA == 2 ? ma : 0) + (DB == 2 ? mb : 0);
+    return b.v(t.x + dx, t.y + dy, t.z + dz);
+  };
+  return dmcore(v) * g.ovd[DA] * g.ovd[DB];
+}
+
+}  // namespace tile
+}  // namespace senga
