@@ -179,6 +179,29 @@ int senga_chrate_host(senga_ctx* ctx, double* rate);
 typedef double (*senga_integrand)(double x, void* user);
 int senga_integf(senga_integrand f, void* user, double argmin, double argmax, double* answer);
 
+/* ---- allocation-free right-hand side ----------------------------------------
+ * No counterpart in the reference. RHSCAL + RHSVEL of one periodic box, like
+ * senga_rhs_host, for callers that cannot allocate device memory when they
+ * call (a host that reserves all device memory at start-up, or one that runs
+ * inside another framework's memory pool): all arrays are caller-owned
+ * device pointers and the intermediate fields live in a fixed file-scope
+ * device array of SENGA_NOALLOC_SCRATCH_BYTES, held by every GPU that loads
+ * the library until exit. No cudaMalloc/cudaFree is called.
+ *   state  : nc = 5+nspec conserved interior arrays (read)
+ *   trun   : T seed in, T after TEMPER out;  itndex: interval index in/out
+ *   rhs    : nc interior arrays, R(U) out
+ *   status : optional device word, bit 0 set on TEMPER non-convergence
+ *            (cleared by the call); NULL uses an internal word
+ *   stream : cudaStream_t to run on (NULL = default stream); asynchronous.
+ * A box needs (14 + 4*nspec)*8 bytes of scratch per grid point; larger boxes
+ * are rejected with SENGA_ERR_ARG. Every call reuses the same array, so calls
+ * that overlap on the GPU race. The first call on a device (with it current)
+ * looks up the array's device address; make it before any stream capture. */
+#define SENGA_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff,
+                      const double* state, double* trun, int32_t* itndex, double* rhs,
+                      unsigned int* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,163 @@
+// Allocation-free right-hand side: senga_rhs_noalloc.
+//
+// Some callers of this library cannot allocate device memory when they call
+// it: a Fortran driver that reserves all device memory once at start-up and
+// forbids allocation afterwards, or a host that embeds this library inside
+// another framework's memory pool. For them this entry point evaluates
+// RHSCAL + RHSVEL of one box from caller-owned device buffers and keeps every
+// intermediate field in a fixed, file-scope device array instead of a
+// context-owned pool. It calls no cudaMalloc, cudaFree or allocating library
+// routine.
+//
+// Limits and sharing:
+//   * the scratch array holds SENGA_NOALLOC_SCRATCH_BYTES (16 MiB) on every
+//     GPU that loads the library, until the process exits; a box needs
+//     (14 + 4*nspec) doubles of scratch per grid point, so e.g. 41,943 points
+//     for the 9-species mechanism and 95,325 for the 2-species one; larger
+//     boxes are rejected with SENGA_ERR_ARG;
+//   * every call shares the array and leaves its contents behind; the status
+//     word is cleared at the start of each call and all other scratch fields
+//     are written before they are read; calls whose work overlaps on the GPU
+//     (different streams, or different host threads) race on the array;
+//   * the first call on a device, with that device current, looks up the
+//     device addresses of the file-scope arrays (cudaGetSymbolAddress); make
+//     that first call before any stream capture.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "senga_gpu.h"
+#include "senga_internal.h"
+
+namespace {
+
+constexpr size_t kScratchBytes = SENGA_NOALLOC_SCRATCH_BYTES;
+constexpr size_t kScratchDoubles = kScratchBytes / sizeof(double);
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+static __device__ __align__(256) senga_chem g_noalloc_chem;
+static __device__ __align__(256) senga_diff g_noalloc_diff;
+static __device__ __align__(256) unsigned int g_noalloc_status;
+
+struct DevicePtrs {
+  bool ready = false;
+  double* scratch = nullptr;
+  senga_chem* chem = nullptr;
+  senga_diff* diff = nullptr;
+  unsigned int* status = nullptr;
+};
+DevicePtrs g_ptrs[kMaxDevices];
+std::mutex g_mutex;
+
+// RK4(3)5[2R+]C coefficients are not needed: the RK epilogue runs in
+// "right-hand side only" mode (RK::last = -1).
+
+int setup(int dev, DevicePtrs& out) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  DevicePtrs& p = g_ptrs[dev];
+  if (!p.ready) {
+    cudaError_t e = cudaGetSymbolAddress((void**)&p.scratch, g_noalloc_scratch);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p.chem, g_noalloc_chem);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p.diff, g_noalloc_diff);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p.status, g_noalloc_status);
+    if (e != cudaSuccess)
+      return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: cudaGetSymbolAddress: ") +
+                                             cudaGetErrorString(e));
+    p.ready = true;
+  }
+  out = p;
+  return SENGA_OK;
+}
+
+}  // namespace
+
+extern "C" int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff,
+                                 const double* state, double* trun, int32_t* itndex, double* rhs,
+                                 unsigned int* status, void* stream) {
+  if (!cfg || !chem || !state || !trun || !itndex || !rhs)
+    return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: null argument");
+  const int nspec = chem->nspec;
+  if (nspec < 1 || nspec > SENGA_NSPCMX) return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: nspec out of range");
+  const int n3[3] = {cfg->nx, cfg->ny, cfg->nz};
+  const double len[3] = {cfg->xgdlen, cfg->ygdlen, cfg->zgdlen};
+  senga::Geo g{};
+  for (int d = 0; d < 3; ++d) {
+    if (n3[d] < 11) return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: grid extent must be at least 11 points");
+    if (cfg->nend[2 * d] != SENGA_NPERI || cfg->nend[2 * d + 1] != SENGA_NPERI)
+      return senga::fail(SENGA_ERR_UNSUPPORTED, "senga_rhs_noalloc: periodic boxes only");
+    g.per[d] = 1;
+    const double delta = len[d] / (double)(float)(n3[d] - 1);
+    g.ovd[d] = 1.0 / delta;
+    g.ovd2[d] = g.ovd[d] * g.ovd[d];
+  }
+  g.nx = cfg->nx;
+  g.ny = cfg->ny;
+  g.nz = cfg->nz;
+  g.n = (int64_t)cfg->nx * cfg->ny * cfg->nz;
+  const int64_t per_point = 14 + 4 * (int64_t)nspec;
+  if (g.n * per_point > (int64_t)kScratchDoubles)
+    return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: box of " + std::to_string(g.n) + " points needs " +
+                                          std::to_string(g.n * per_point * 8) + " bytes of scratch, limit " +
+                                          std::to_string(kScratchBytes));
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: device ordinal too large");
+  DevicePtrs ptr;
+  int rc = setup(dev, ptr);
+  if (rc != SENGA_OK) return rc;
+
+  cudaStream_t s = (cudaStream_t)stream;
+  senga_diff dz;
+  if (!diff) std::memset(&dz, 0, sizeof(dz));
+  e = cudaMemcpyAsync(ptr.chem, chem, sizeof(senga_chem), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ptr.diff, diff ? diff : &dz, sizeof(senga_diff), cudaMemcpyHostToDevice, s);
+  unsigned int* st = status ? status : ptr.status;
+  if (e == cudaSuccess) e = cudaMemsetAsync(st, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess) return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: ") + cudaGetErrorString(e));
+
+  // carve the scratch fields; the caller's rhs buffer is the accumulator
+  const int64_t n = g.n;
+  double* q = ptr.scratch;
+  auto take = [&](int64_t k) {
+    double* r = q;
+    q += k * n;
+    return r;
+  };
+  senga::Fields f{};
+  f.uin = const_cast<double*>(state);
+  f.uout = nullptr;
+  f.run = nullptr;
+  f.err = nullptr;
+  f.t = trun;
+  f.itn = itndex;
+  f.p = take(1);
+  f.lam = take(1);
+  f.lcp = take(1);
+  f.mu = take(1);
+  f.rd = take(nspec);
+  f.h = take(nspec);
+  f.hmix = take(1);
+  f.wdot = take(nspec);
+  f.vel = take(3);
+  f.e = take(1);
+  f.y = take(nspec);
+  f.divm = take(1);
+  f.vc = take(3);
+  f.vtmp = take(1);
+  f.rhs = rhs;
+  f.status = st;
+
+  const int flmavt = diff ? diff->flmavt : 0;
+  senga::launch_thermo(g, f, ptr.chem, ptr.diff, nspec, flmavt, s);
+  senga::launch_flow(g, f, nspec, s);
+  senga::launch_species_a(g, f, nspec, s);
+  senga::RK rk{0.0, 0.0, 0.0, -1};
+  senga::launch_species_b_rk(g, f, nspec, rk, s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: ") + cudaGetErrorString(e));
+  return SENGA_OK;
+}

@@ -122,6 +122,8 @@ def _load():
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
         "senga_temper_host": (ip, [vp, dp, dp]),
         "senga_chrate_host": (ip, [vp, dp]),
+        "senga_rhs_noalloc": (ip, [C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), vp, vp, vp, vp, vp,
+                                   vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
