@@ -180,6 +180,7 @@ def main():
     box = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"], device=local)
     box.upload(c["fields"], c["T"], c["itn"])
     npts = c["shape"][0] * c["shape"][1] * c["shape"][2]
+    workload["thermochemistry_kernel"] = {0: "table-driven", 1: "generated 1-step", 2: "generated H2"}[box.info()["mech"]]
 
     def barrier():
         if world > 1:

@@ -154,6 +154,11 @@ int senga_rhs_host(senga_ctx* ctx, double* rhs, double* trun, double* prun);
  * Advances the state like senga_step(ctx, 1). */
 int senga_profile_step(senga_ctx* ctx, double* ms, int* launches);
 
+/* Context facts: *mech = thermochemistry kernel in use (0 table-driven, 1 the
+ * generated one-step R->P kernel, 2 the generated H2/air kernel), and the
+ * device bytes the context holds. */
+int senga_ctx_info(senga_ctx* ctx, int* mech, int64_t* device_bytes);
+
 /* Status word of the last steps: bit 0 = TEMPER non-convergence. */
 int senga_get_status(senga_ctx* ctx, int* status);
 

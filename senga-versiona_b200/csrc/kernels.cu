@@ -11,6 +11,10 @@
 
 #include <cstdint>
 
+#include <cstdlib>
+#include <cstring>
+
+#include "mech_gen.cuh"
 #include "senga_internal.h"
 #include "stencil.cuh"
 
@@ -149,43 +153,173 @@ __device__ void chrate_point(const senga_chem* __restrict__ C, int nspec, const 
 }
 
 // -------------------------------------------------------------------------
-template <int NSM, bool MAVT, bool CHEM>
-__global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, const senga_chem* __restrict__ C,
-                                                   const senga_diff* __restrict__ Dt, int nspec) {
+// Mechanism policies. A policy supplies the per-point thermochemistry of one
+// mechanism: TEMPER's e(T) polynomial (src/temper.f:84-122), interval
+// location and mixture cp (:168-209), transport properties (src/rhscal.f:
+// 515-571, 1292-1340, 3854-3885; src/rhsvel.f:933-952), species enthalpy
+// (src/rhscal.f:1444-1466) and CHRATE. MechTables reads the tables of any
+// chem.dat/diff.dat; generated policies (mech_gen.cuh) hard-code one
+// mechanism and are selected only when the loaded tables match them exactly.
+template <int NSM, bool MAVT_>
+struct MechTables {
+  static constexpr int NS = NSM;
+  static constexpr bool MAVT = MAVT_;
+  const senga_chem* __restrict__ C;
+  const senga_diff* __restrict__ Dt;
+  int nspec;
+
+  __device__ __forceinline__ bool has(int s) const { return s < nspec; }
+
+  __device__ __forceinline__ void temper_coeffs(const double (&ry)[NS], int32_t itn0, double (&tc)[6], double (&td)[6],
+                                                double& rmix) const {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      if (s >= nspec) continue;
+      const int it = tint_of(itn0, s);
+      const double y = ry[s];
+      const int np = C->ncpoly[s][it];
+      tc[0] = tc[0] + y * C->amascp[s][it][C->ncenth[s][it] - 1];
+      tc[1] = tc[1] + y * C->amasct[s][it][0];
+      td[1] = tc[1];
+#pragma unroll
+      for (int icp = 2; icp <= 5; ++icp)
+        if (icp <= np) {
+          tc[icp] = tc[icp] + y * C->amasct[s][it][icp - 1];
+          td[icp] = td[icp] + y * C->amascp[s][it][icp - 1];
+        }
+      rmix = rmix + y * C->rgspec[s];
+    }
+  }
+  // new interval index and sum_k rho Y_k cp_k (divided by rho by the caller)
+  __device__ __forceinline__ void locate(double T, const double (&ry)[NS], int32_t& itn, double& cpsum) const {
+    itn = 0;
+    cpsum = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      if (s >= nspec) continue;
+      int it = 0;
+      while (T > C->tinthi[s][it] && it + 1 < C->ntint[s]) ++it;
+      itn += it << (2 * s);
+      const int np = C->ncpoly[s][it];
+      const double* cp = C->amascp[s][it];
+      double c = cp[np - 1];
+      for (int icp = np - 1; icp >= 1; --icp) c = c * T + cp[icp - 1];
+      cpsum = cpsum + ry[s] * c;
+    }
+  }
+  __device__ __forceinline__ double alamda() const { return C->alamda; }
+  __device__ __forceinline__ double olewis(int s) const { return C->olewis[s]; }
+  // mixture-averaged transport: lambda, rho*D_k, mu
+  __device__ __forceinline__ void mixture(double T, double p, double rho, const double (&ry)[NS], const double (&y)[NS],
+                                          double& lam, double (&rd)[NS], double& mu) const {
+    const double lt = log(T / Dt->tdifgb);
+    double c1 = 0.0, c2 = 0.0, c3 = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      if (s >= nspec) continue;
+      double fp = Dt->condco[s][Dt->ncocon - 1];
+      for (int icp = Dt->ncocon - 1; icp >= 1; --icp) fp = fp * lt + Dt->condco[s][icp - 1];
+      const double lk = exp(fp);
+      const double fm = ry[s] * C->ovwmol[s];
+      c1 = c1 + fm * lk;
+      c2 = c2 + fm / lk;
+      c3 = c3 + fm;
+    }
+    c3 = 1.0 / c3;
+    c1 = c1 * c3;
+    c2 = c2 * c3;
+    lam = 0.5 * (c1 + 1.0 / c2);
+    const double wmix = rho * c3;
+    double sumy = 0.0;
+    double den[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      den[s] = 0.0;
+      if (s < nspec) sumy += y[s] + kDfctol;
+    }
+    const double povr = p / Dt->pdifgb;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+#pragma unroll
+      for (int t = s + 1; t < NS; ++t) {
+        if (t >= nspec) continue;
+        const double* dc = Dt->diffco[s][t];
+        double fp = dc[Dt->ncodif - 1];
+        for (int icp = Dt->ncodif - 1; icp >= 1; --icp) fp = fp * lt + dc[icp - 1];
+        const double inv = exp(-fp) * povr;  // 1/D_st (DIFFCO is symmetric: one exp per pair)
+        den[s] += (y[t] + kDfctol) * C->ovwmol[t] * inv;
+        den[t] += (y[s] + kDfctol) * C->ovwmol[s] * inv;
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+      if (s < nspec) rd[s] = rho * (sumy - (y[s] + kDfctol)) / (den[s] * wmix);
+    double mk[NS], sq[NS], rq[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      mk[s] = 1.0;
+      if (s < nspec) {
+        double fp = Dt->viscco[s][Dt->ncovis - 1];
+        for (int icp = Dt->ncovis - 1; icp >= 1; --icp) fp = fp * lt + Dt->viscco[s][icp - 1];
+        mk[s] = exp(fp);
+      }
+      sq[s] = sqrt(mk[s]);  // sqrt(mu_i/mu_j) evaluated as sqrt(mu_i)/sqrt(mu_j)
+      rq[s] = 1.0 / sq[s];
+    }
+    mu = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      if (s >= nspec) continue;
+      double cc = 0.0;
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        if (t >= nspec) continue;
+        double fw = 1.0 + sq[s] * rq[t] * Dt->wilko2[s][t];
+        fw = Dt->wilko1[s][t] * fw * fw;
+        cc = cc + y[t] * C->ovwmol[t] * fw;
+      }
+      mu = mu + y[s] * C->ovwmol[s] * (mk[s] / cc);
+    }
+  }
+  __device__ __forceinline__ void enthalpy(double T, int32_t itn, double (&h)[NS]) const {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      h[s] = 0.0;
+      if (s >= nspec) continue;
+      const int it = tint_of(itn, s);
+      const int np = C->ncpoly[s][it];
+      const double* ch = C->amasch[s][it];
+      double v = ch[np - 1];
+      for (int icp = np - 1; icp >= 1; --icp) v = v * T + ch[icp - 1];
+      h[s] = ch[C->ncenth[s][it] - 1] + v * T;
+    }
+  }
+  __device__ __forceinline__ void chrate(double T, int32_t itn, const double (&ry)[NS], double (&rate)[NS]) const {
+    chrate_point<NS>(C, nspec, ry, T, itn, rate);
+  }
+};
+
+// -------------------------------------------------------------------------
+template <class M>
+__global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, M m) {
+  constexpr int NS = M::NS;
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= g.n) return;
   const int64_t n = g.n;
   const double* U = f.uin;
   const double rho = U[q], ru = U[n + q], rv = U[2 * n + q], rw = U[3 * n + q], re = U[4 * n + q];
-  double ry[NSM];
+  double ry[NS];
 #pragma unroll
-  for (int s = 0; s < NSM; ++s) ry[s] = s < nspec ? U[(5 + s) * n + q] : 0.0;
+  for (int s = 0; s < NS; ++s) ry[s] = m.has(s) ? U[(5 + s) * n + q] : 0.0;
 
-  // ---- TEMPER ----
+  // ---- TEMPER: Newton inversion of e(T) from the previous T ----
   const double ukuk = (ru * ru + rv * rv + rw * rw) / rho;
   double tc[6], td[6];
   tc[0] = 0.5 * ukuk - re;
 #pragma unroll
   for (int i = 1; i < 6; ++i) tc[i] = td[i] = 0.0;
   double rmix = 0.0;
-  const int32_t itn0 = f.itn[q];
-#pragma unroll
-  for (int s = 0; s < NSM; ++s) {
-    if (s >= nspec) continue;
-    const int it = tint_of(itn0, s);
-    const double y = ry[s];
-    const int np = C->ncpoly[s][it];
-    tc[0] = tc[0] + y * C->amascp[s][it][C->ncenth[s][it] - 1];
-    tc[1] = tc[1] + y * C->amasct[s][it][0];
-    td[1] = tc[1];
-#pragma unroll
-    for (int icp = 2; icp <= 5; ++icp)
-      if (icp <= np) {
-        tc[icp] = tc[icp] + y * C->amasct[s][it][icp - 1];
-        td[icp] = td[icp] + y * C->amascp[s][it][icp - 1];
-      }
-    rmix = rmix + y * C->rgspec[s];
-  }
+  m.temper_coeffs(ry, f.itn[q], tc, td, rmix);
   const double toltmp = (double)1.0e-10f;  // TOLTMP is a single-precision literal
   double T = f.t[q];
   int iters = 1;
@@ -208,20 +342,9 @@ __global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, const senga_
     }
     break;
   }
-  int32_t itn = 0;
-  double cpm = 0.0;
-#pragma unroll
-  for (int s = 0; s < NSM; ++s) {
-    if (s >= nspec) continue;
-    int it = 0;
-    while (T > C->tinthi[s][it] && it + 1 < C->ntint[s]) ++it;
-    itn += it << (2 * s);
-    const int np = C->ncpoly[s][it];
-    const double* cp = C->amascp[s][it];
-    double c = cp[np - 1];
-    for (int icp = np - 1; icp >= 1; --icp) c = c * T + cp[icp - 1];
-    cpm = cpm + ry[s] * c;
-  }
+  int32_t itn;
+  double cpm;
+  m.locate(T, ry, itn, cpm);
   cpm = cpm / rho;
   const double p = T * rmix;
   f.t[q] = T;
@@ -229,127 +352,57 @@ __global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, const senga_
   f.p[q] = p;
 
   // ---- primitive variables ----
-  const double ovr = 1.0 / rho;
-  double y[NSM];
+  double y[NS];
 #pragma unroll
-  for (int s = 0; s < NSM; ++s) {
+  for (int s = 0; s < NS; ++s) {
     y[s] = ry[s] / rho;
-    if (s < nspec) f.y[s * n + q] = y[s];
+    if (m.has(s)) f.y[s * n + q] = y[s];
   }
   f.vel[q] = ru / rho;
   f.vel[n + q] = rv / rho;
   f.vel[2 * n + q] = rw / rho;
   f.e[q] = re / rho;
-  (void)ovr;
 
   // ---- transport properties ----
-  if (!MAVT) {
-    const double lcp = C->alamda * exp(kRlamda * log(T));
+  if (!M::MAVT) {
+    const double lcp = m.alamda() * exp(kRlamda * log(T));
     f.lam[q] = lcp * cpm;
     f.lcp[q] = lcp;
     f.mu[q] = lcp * kPrantl;
 #pragma unroll
-    for (int s = 0; s < NSM; ++s)
-      if (s < nspec) f.rd[s * n + q] = lcp * C->olewis[s];
+    for (int s = 0; s < NS; ++s)
+      if (m.has(s)) f.rd[s * n + q] = lcp * m.olewis(s);
   } else {
-    const double lt = log(T / Dt->tdifgb);
-    // conductivity combination (rhscal.f:531-571), with rho*Y
-    double c1 = 0.0, c2 = 0.0, c3 = 0.0;
-#pragma unroll
-    for (int s = 0; s < NSM; ++s) {
-      if (s >= nspec) continue;
-      double fp = Dt->condco[s][Dt->ncocon - 1];
-      for (int icp = Dt->ncocon - 1; icp >= 1; --icp) fp = fp * lt + Dt->condco[s][icp - 1];
-      const double lk = exp(fp);
-      const double fm = ry[s] * C->ovwmol[s];
-      c1 = c1 + fm * lk;
-      c2 = c2 + fm / lk;
-      c3 = c3 + fm;
-    }
-    c3 = 1.0 / c3;
-    c1 = c1 * c3;
-    c2 = c2 * c3;
-    f.lam[q] = 0.5 * (c1 + 1.0 / c2);
-    const double wmix = rho * c3;
-    // mixture-averaged diffusivity (rhscal.f:1311-1340): each D_jk is
-    // evaluated once per unordered pair (DIFFCO is symmetric).
-    double sumy = 0.0;
-    double den[NSM];
-#pragma unroll
-    for (int s = 0; s < NSM; ++s) {
-      den[s] = 0.0;
-      if (s < nspec) sumy += y[s] + kDfctol;
-    }
-    const double povr = p / Dt->pdifgb;
-#pragma unroll
-    for (int s = 0; s < NSM; ++s) {
-#pragma unroll
-      for (int t = s + 1; t < NSM; ++t) {
-        if (t >= nspec) continue;
-        const double* dc = Dt->diffco[s][t];
-        double fp = dc[Dt->ncodif - 1];
-        for (int icp = Dt->ncodif - 1; icp >= 1; --icp) fp = fp * lt + dc[icp - 1];
-        const double inv = exp(-fp) * povr;  // 1/D_st
-        den[s] += (y[t] + kDfctol) * C->ovwmol[t] * inv;
-        den[t] += (y[s] + kDfctol) * C->ovwmol[s] * inv;
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < NSM; ++s)
-      if (s < nspec) f.rd[s * n + q] = rho * (sumy - (y[s] + kDfctol)) / (den[s] * wmix);
-    // Wilke viscosity (rhscal.f:3854-3885): sqrt(mu_i/mu_j) = sqrt(mu_i)/sqrt(mu_j)
-    double mk[NSM], sq[NSM], rq[NSM];
-#pragma unroll
-    for (int s = 0; s < NSM; ++s) {
-      mk[s] = 1.0;
-      if (s < nspec) {
-        double fp = Dt->viscco[s][Dt->ncovis - 1];
-        for (int icp = Dt->ncovis - 1; icp >= 1; --icp) fp = fp * lt + Dt->viscco[s][icp - 1];
-        mk[s] = exp(fp);
-      }
-      sq[s] = sqrt(mk[s]);
-      rq[s] = 1.0 / sq[s];
-    }
-    double mu = 0.0;
-#pragma unroll
-    for (int s = 0; s < NSM; ++s) {
-      if (s >= nspec) continue;
-      double cc = 0.0;
-#pragma unroll
-      for (int t = 0; t < NSM; ++t) {
-        if (t >= nspec) continue;
-        double fw = 1.0 + sq[s] * rq[t] * Dt->wilko2[s][t];
-        fw = Dt->wilko1[s][t] * fw * fw;
-        cc = cc + y[t] * C->ovwmol[t] * fw;
-      }
-      mu = mu + y[s] * C->ovwmol[s] * (mk[s] / cc);
-    }
+    double lam, mu, rd[NS];
+    m.mixture(T, p, rho, ry, y, lam, rd, mu);
+    f.lam[q] = lam;
     f.mu[q] = mu;
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+      if (m.has(s)) f.rd[s * n + q] = rd[s];
   }
 
   // ---- species enthalpy and mixture enthalpy (new interval index) ----
-  double hm = 0.0;
+  {
+    double h[NS];
+    m.enthalpy(T, itn, h);
+    double hm = 0.0;
 #pragma unroll
-  for (int s = 0; s < NSM; ++s) {
-    if (s >= nspec) continue;
-    const int it = tint_of(itn, s);
-    const int np = C->ncpoly[s][it];
-    const double* ch = C->amasch[s][it];
-    double h = ch[np - 1];
-    for (int icp = np - 1; icp >= 1; --icp) h = h * T + ch[icp - 1];
-    h = ch[C->ncenth[s][it] - 1] + h * T;
-    f.h[s * n + q] = h;
-    hm = hm + h * y[s];
+    for (int s = 0; s < NS; ++s) {
+      if (!m.has(s)) continue;
+      f.h[s * n + q] = h[s];
+      hm = hm + h[s] * y[s];
+    }
+    f.hmix[q] = hm;
   }
-  f.hmix[q] = hm;
 
   // ---- CHRATE ----
-  if (CHEM) {
-    double rate[NSM];
-    chrate_point<NSM>(C, nspec, ry, T, itn, rate);
+  {
+    double rate[NS];
+    m.chrate(T, itn, ry, rate);
 #pragma unroll
-    for (int s = 0; s < NSM; ++s)
-      if (s < nspec) f.wdot[s * n + q] = rate[s];
+    for (int s = 0; s < NS; ++s)
+      if (m.has(s)) f.wdot[s * n + q] = rate[s];
   }
 }
 
@@ -378,15 +431,27 @@ inline unsigned grid_of(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock
 
 }  // namespace
 
+int select_mech(const senga_chem& chem, const senga_diff& diff) {
+  const char* env = std::getenv("SENGA_MECH");
+  if (env && std::strcmp(env, "generic") == 0) return 0;
+  if (gen::Mech_onestep::matches(chem, diff)) return 1;
+  if (gen::Mech_h2::matches(chem, diff)) return 2;
+  return 0;
+}
+
 void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const senga_diff* ddiff, int nspec,
-                   int flmavt, cudaStream_t s) {
+                   int flmavt, int mech, cudaStream_t s) {
   const unsigned gr = grid_of(g.n);
-  if (nspec <= 2) {
-    if (flmavt) k_thermo<2, true, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
-    else k_thermo<2, false, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
+  if (mech == 1) {
+    k_thermo<<<gr, kBlock, 0, s>>>(g, f, gen::Mech_onestep{});
+  } else if (mech == 2) {
+    k_thermo<<<gr, kBlock, 0, s>>>(g, f, gen::Mech_h2{});
+  } else if (nspec <= 2) {
+    if (flmavt) k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<2, true>{dchem, ddiff, nspec});
+    else k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<2, false>{dchem, ddiff, nspec});
   } else {
-    if (flmavt) k_thermo<9, true, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
-    else k_thermo<9, false, true><<<gr, kBlock, 0, s>>>(g, f, dchem, ddiff, nspec);
+    if (flmavt) k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<9, true>{dchem, ddiff, nspec});
+    else k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<9, false>{dchem, ddiff, nspec});
   }
 }
 

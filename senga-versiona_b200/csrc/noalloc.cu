@@ -152,7 +152,7 @@ extern "C" int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem
   f.status = st;
 
   const int flmavt = diff ? diff->flmavt : 0;
-  senga::launch_thermo(g, f, ptr.chem, ptr.diff, nspec, flmavt, s);
+  senga::launch_thermo(g, f, ptr.chem, ptr.diff, nspec, flmavt, senga::select_mech(*chem, diff ? *diff : dz), s);
   senga::launch_flow(g, f, nspec, s);
   senga::launch_species_a(g, f, nspec, s);
   senga::RK rk{0.0, 0.0, 0.0, -1};

@@ -64,6 +64,7 @@ struct senga_ctx {
   Fields f{};
   double rklhs[5], rkrhs[5], rkerr[5];
   cudaGraphExec_t graph = nullptr;
+  int mech = 0;  // thermochemistry policy (select_mech)
 };
 
 namespace {
@@ -107,7 +108,7 @@ void set_rk(senga_ctx* c, double tstep) {
 }
 
 void run_rhs(senga_ctx* c) {
-  launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+  launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
   launch_flow(c->geo, c->f, c->nspec, c->stream);
   launch_species_a(c->geo, c->f, c->nspec, c->stream);
 }
@@ -150,6 +151,7 @@ int senga_ctx_create(const senga_config* cfg, const senga_chem* chem, const seng
     check_config(*cfg, c->nspec);
     build_geo(*cfg, c->geo);
     set_rk(c, cfg->tstep);
+    c->mech = select_mech(c->chem, c->diff);
     CK(cudaSetDevice(cfg->device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaMalloc(&c->d_chem, sizeof(senga_chem)));
@@ -307,7 +309,7 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
     for (int irk = 1; irk <= 5; ++irk) {
       const int b = (irk - 1) * 4;
       CK(cudaEventRecord(ev[b], c->stream));
-      launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+      launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
       CK(cudaEventRecord(ev[b + 1], c->stream));
       launch_flow(c->geo, c->f, c->nspec, c->stream);
       CK(cudaEventRecord(ev[b + 2], c->stream));
@@ -330,6 +332,21 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
     for (auto& e : ev) cudaEventDestroy(e);
     if (launches) *launches = nl;
   });
+}
+
+int senga_ctx_info(senga_ctx* c, int* mech, int64_t* device_bytes) {
+  if (!c) return fail(SENGA_ERR_ARG, "senga_ctx_info: null context");
+  if (mech) *mech = c->mech;
+  if (device_bytes) {
+    size_t bytes = 0;
+    cudaPointerAttributes a;
+    (void)a;
+    const int64_t n = c->geo.n;
+    const int S = c->nspec, nc = c->nc;
+    bytes = (size_t)((int64_t)(3 * nc + 4 * S + 15 + (c->cfg.adaptive ? nc : 0)) * n + (n + 1) / 2 + 64) * sizeof(double);
+    *device_bytes = (int64_t)bytes;
+  }
+  return SENGA_OK;
 }
 
 int senga_get_status(senga_ctx* c, int* status) {
@@ -368,7 +385,7 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
 int senga_temper_host(senga_ctx* c, double* trun, double* prun) {
   if (!c) return fail(SENGA_ERR_ARG, "null context");
   return guard([&] {
-    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
     CK(cudaGetLastError());
     const int64_t n = c->geo.n;
     if (trun) CK(cudaMemcpyAsync(trun, c->f.t, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -380,7 +397,7 @@ int senga_temper_host(senga_ctx* c, double* trun, double* prun) {
 int senga_chrate_host(senga_ctx* c, double* rate) {
   if (!c || !rate) return fail(SENGA_ERR_ARG, "senga_chrate_host: null argument");
   return guard([&] {
-    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->stream);
+    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(rate, c->f.wdot, (size_t)c->nspec * c->geo.n * sizeof(double), cudaMemcpyDeviceToHost,
                        c->stream));

@@ -64,8 +64,13 @@ struct RK {
 };
 
 // Launchers (kernels.cu).
+// Mechanism-specialised thermochemistry: 0 = table-driven (any chem.dat),
+// otherwise the id of a generated policy whose constants equal the loaded
+// tables bit for bit (select_mech). SENGA_MECH=generic in the environment
+// forces the table-driven kernel.
+int select_mech(const senga_chem& chem, const senga_diff& diff);
 void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const senga_diff* ddiff, int nspec,
-                   int flmavt, cudaStream_t s);
+                   int flmavt, int mech, cudaStream_t s);
 void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s);

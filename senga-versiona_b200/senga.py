@@ -118,6 +118,7 @@ def _load():
         "senga_rhs_host": (ip, [vp, dp, dp, dp]),
         "senga_get_status": (ip, [vp, C.POINTER(C.c_int)]),
         "senga_profile_step": (ip, [vp, dp, C.POINTER(C.c_int)]),
+        "senga_ctx_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
         "senga_temper_host": (ip, [vp, dp, dp]),
@@ -248,6 +249,13 @@ class Box:
         nl = C.c_int()
         _check(lib.senga_profile_step(self.h, _dp(ms), C.byref(nl)), "senga_profile_step")
         return dict(zip(("thermo", "flow", "species_a", "species_b_rk"), ms.tolist())), nl.value
+
+    def info(self):
+        """{'mech': thermochemistry kernel id, 'device_bytes': bytes held}."""
+        m = C.c_int()
+        b = C.c_int64()
+        _check(lib.senga_ctx_info(self.h, C.byref(m), C.byref(b)), "senga_ctx_info")
+        return {"mech": m.value, "device_bytes": b.value}
 
     @property
     def stream(self):

@@ -166,3 +166,22 @@ def test_temper_failure_reports_status_without_fault():
     box.step(1)
     f, _, _ = box.download()
     assert np.isfinite(f).all()
+
+
+@pytest.mark.parametrize("name", ["ignition32", "h2_kernels"])
+def test_generated_and_table_driven_thermochemistry_agree(name, monkeypatch):
+    """The shipped mechanisms run the generated straight-line kernel; the
+    table-driven kernel (any chem.dat) gives the same right-hand side, and
+    both match the oracle."""
+    c = _case(name, 12)
+    box, ref = _pair(c)
+    assert box.info()["mech"] in (1, 2)
+    r_gen, _, _ = box.rhs()
+    monkeypatch.setenv("SENGA_MECH", "generic")
+    box2, _ = _pair(c)
+    assert box2.info()["mech"] == 0
+    r_tab, _, _ = box2.rhs()
+    r_o, _, _ = ref.rhs()
+    for k in range(r_o.shape[0]):
+        assert rel_linf(r_gen[k], r_tab[k]) <= 1e-12, f"field {k}"
+        assert rel_linf(r_tab[k], r_o[k]) <= TOL_STATE, f"field {k}"
