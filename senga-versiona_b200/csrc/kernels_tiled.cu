@@ -29,7 +29,7 @@ constexpr double kThrd = 1.0 / 3.0, kTthd = 2.0 * kThrd, kFthd = 2.0 * kTthd;
 constexpr int FX = 32, FY = 8, FZ = 2;
 constexpr int FNW = FX * FY / 32;
 // species tiles
-constexpr int SX_ = 32, SY_ = 8, SZ_ = 4;
+constexpr int SX_ = 32, SY_ = 8, SZ_ = 2;
 constexpr int SNW = SX_ * SY_ / 32;
 
 using FStar = Star<FX, FY, FZ>;
@@ -43,12 +43,12 @@ constexpr int kFlowSmem =
     cmax(cmax(FXRow::SIZE + FYRow::SIZE + FZCol::SIZE + FStar::SIZE, 2 * FStar::SIZE),
          cmax(cmax(FXRow::SIZE + 2 * FStar::SIZE, FYRow::SIZE + FStar::SIZE + FZCol::SIZE), FStar::SIZE + FBox::SIZE));
 
-using SStar = Star<SX_, SY_, SZ_>;
+using SSlab = Slab<SX_, SY_, SZ_>;
 using SXRow = XRow<SX_, SY_, SZ_>;
 using SYRow = YRow<SX_, SY_, SZ_>;
-using SZCol = ZCol<SX_, SY_, SZ_>;
-constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + SZCol::SIZE + SStar::SIZE;
-constexpr int kSpecRkSmem = SStar::SIZE;
+using SCol = Column<SZ_>;
+constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + SSlab::SIZE;
+constexpr int kSpecRkSmem = SSlab::SIZE;
 
 template <bool P>
 __global__ void __launch_bounds__(FX* FY, 2) k_flow_t(Geo g, Fields f) {
@@ -349,11 +349,11 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int 
   const double* U = f.uin;
   const SXRow bru{sm};
   const SYRow brv{sm + SXRow::SIZE};
-  const SZCol brw{sm + SXRow::SIZE + SYRow::SIZE};
-  const SStar bS{sm + SXRow::SIZE + SYRow::SIZE + SZCol::SIZE};
+  const SSlab bS{sm + SXRow::SIZE + SYRow::SIZE};
   bru.stage<SNW>(fo, Ld{U + n});
   brv.stage<SNW>(fo, Ld{U + 2 * n});
-  brw.stage<SNW>(fo, Ld{U + 3 * n});
+  SCol rw;
+  rw.load(fo, tx, ty, Ld{U + 3 * n});
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) {
@@ -362,59 +362,71 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int 
     dvm[z] = tp[z].valid ? f.divm[tp[z].q] : 0.0;
   }
   for (int s = 0; s < nspec; ++s) {
-    double rate[SZ_], yx[SZ_], yy[SZ_], yz[SZ_], lap[SZ_], fn1[SZ_], fn3[SZ_], rd[SZ_];
+    double rate[SZ_], yx[SZ_], yy[SZ_], yz[SZ_], fn1[SZ_], fn3[SZ_], rd[SZ_];
     // Y_k: convection, gradient, Laplacian
-    bS.stage<SNW>(fo, Ld{f.y + s * n});
-    __syncthreads();
+    {
+      SCol cy;
+      cy.load(fo, tx, ty, Ld{f.y + s * n});
+      bS.stage<SNW>(fo, Ld{f.y + s * n});
+      __syncthreads();
 #pragma unroll
-    for (int z = 0; z < SZ_; ++z) {
-      const TP& t = tp[z];
-      const double yq = bS.v(t.x, t.y, t.z);
-      double r = f.wdot[s * n + t.q];
-      r = r - 0.5 * yq * dvm[z];
-      r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1p<2, P>(g, t, bS, brw));
-      yx[z] = d1<0, P>(g, t, bS);
-      yy[z] = d1<1, P>(g, t, bS);
-      yz[z] = d1<2, P>(g, t, bS);
-      r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * brw.v(t.x, t.y, t.z));
-      rate[z] = r;
-      lap[z] = d2<0, P>(g, t, bS) + d2<1, P>(g, t, bS) + d2<2, P>(g, t, bS);
+      for (int z = 0; z < SZ_; ++z) {
+        const TP& t = tp[z];
+        const double yq = cy.c[z + H];
+        double r = f.wdot[s * n + t.q];
+        r = r - 0.5 * yq * dvm[z];
+        r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1zp<P>(g, t, cy, rw));
+        yx[z] = d1<0, P>(g, t, bS);
+        yy[z] = d1<1, P>(g, t, bS);
+        yz[z] = d1z<P>(g, t, cy);
+        r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * rw.c[z + H]);
+        rate[z] = r;
+        fn3[z] = d2<0, P>(g, t, bS) + d2<1, P>(g, t, bS) + d2z<P>(g, t, cy);  // Laplacian for now
+      }
+      __syncthreads();
     }
-    __syncthreads();
     // rho D_k: correction velocity, diffusive flux divergence
-    bS.stage<SNW>(fo, Ld{f.rd + s * n});
-    __syncthreads();
+    {
+      SCol cd;
+      cd.load(fo, tx, ty, Ld{f.rd + s * n});
+      bS.stage<SNW>(fo, Ld{f.rd + s * n});
+      __syncthreads();
 #pragma unroll
-    for (int z = 0; z < SZ_; ++z) {
-      const TP& t = tp[z];
-      rd[z] = bS.v(t.x, t.y, t.z);
-      vcx[z] = vcx[z] + rd[z] * yx[z];
-      vcy[z] = vcy[z] + rd[z] * yy[z];
-      vcz[z] = vcz[z] + rd[z] * yz[z];
-      const double fn = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1<2, P>(g, t, bS) * yz[z];
-      rate[z] = rate[z] + fn;
-      vt[z] = vt[z] + fn;
-      fn1[z] = fn;
-      const double f3 = lap[z] * rd[z];
-      rate[z] = rate[z] + f3;
-      vt[z] = vt[z] + f3;
-      fn3[z] = f3;
+      for (int z = 0; z < SZ_; ++z) {
+        const TP& t = tp[z];
+        rd[z] = cd.c[z + H];
+        vcx[z] = vcx[z] + rd[z] * yx[z];
+        vcy[z] = vcy[z] + rd[z] * yy[z];
+        vcz[z] = vcz[z] + rd[z] * yz[z];
+        const double fn = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1z<P>(g, t, cd) * yz[z];
+        rate[z] = rate[z] + fn;
+        vt[z] = vt[z] + fn;
+        fn1[z] = fn;
+        const double f3 = fn3[z] * rd[z];
+        rate[z] = rate[z] + f3;
+        vt[z] = vt[z] + f3;
+        fn3[z] = f3;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     // h_k: enthalpy fluxes of the energy equation
-    bS.stage<SNW>(fo, Ld{f.h + s * n});
-    __syncthreads();
+    {
+      SCol ch;
+      ch.load(fo, tx, ty, Ld{f.h + s * n});
+      bS.stage<SNW>(fo, Ld{f.h + s * n});
+      __syncthreads();
 #pragma unroll
-    for (int z = 0; z < SZ_; ++z) {
-      const TP& t = tp[z];
-      const double hk = bS.v(t.x, t.y, t.z);
-      rE[z] = rE[z] + fn1[z] * hk;
-      const double fn2 = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1<2, P>(g, t, bS) * yz[z];
-      rE[z] = rE[z] + fn2 * rd[z];
-      rE[z] = rE[z] + fn3[z] * hk;
-      if (t.valid) f.wdot[s * n + t.q] = rate[z];
+      for (int z = 0; z < SZ_; ++z) {
+        const TP& t = tp[z];
+        const double hk = ch.c[z + H];
+        rE[z] = rE[z] + fn1[z] * hk;
+        const double fn2 = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1z<P>(g, t, ch) * yz[z];
+        rE[z] = rE[z] + fn2 * rd[z];
+        rE[z] = rE[z] + fn3[z] * hk;
+        if (t.valid) f.wdot[s * n + t.q] = rate[z];
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) {
@@ -430,7 +442,7 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int 
 
 // -------------------------------------------------------------------------
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
   extern __shared__ double sm[];
   const Origin o{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_};
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
@@ -441,7 +453,7 @@ __global__ void __launch_bounds__(SX_* SY_) k_species_rk_t(Geo g, Fields f, int 
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) tp[z] = make_tp(g, o, tx, ty, z);
   const int64_t n = g.n;
-  const SStar bS{sm};
+  const SSlab bS{sm};
   auto advance = [&](int fld, int64_t q, double R) {
     const int64_t idx = (int64_t)fld * n + q;
     if (rk.last < 0) {  // right-hand side only
@@ -468,28 +480,34 @@ __global__ void __launch_bounds__(SX_* SY_) k_species_rk_t(Geo g, Fields f, int 
     vcz[z] = f.vc[2 * n + q];
     vt[z] = f.vtmp[q];
   }
-  bS.stage<SNW>(fo, Ld{f.hmix});
-  __syncthreads();
+  {
+    SCol cm;
+    cm.load(fo, tx, ty, Ld{f.hmix});
+    bS.stage<SNW>(fo, Ld{f.hmix});
+    __syncthreads();
 #pragma unroll
-  for (int z = 0; z < SZ_; ++z) {
-    const TP& t = tp[z];
-    if (!t.valid) continue;
-    const double rE = f.rhs[4 * n + t.q] - bS.v(t.x, t.y, t.z) * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
-                      d1<1, P>(g, t, bS) * vcy[z] - d1<2, P>(g, t, bS) * vcz[z];
+    for (int z = 0; z < SZ_; ++z) {
+      const TP& t = tp[z];
+      if (!t.valid) continue;
+      const double rE = f.rhs[4 * n + t.q] - cm.c[z + H] * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
+                        d1<1, P>(g, t, bS) * vcy[z] - d1z<P>(g, t, cm) * vcz[z];
 #pragma unroll
-    for (int fl = 0; fl < 4; ++fl) advance(fl, t.q, f.rhs[fl * n + t.q]);
-    advance(4, t.q, rE);
+      for (int fl = 0; fl < 4; ++fl) advance(fl, t.q, f.rhs[fl * n + t.q]);
+      advance(4, t.q, rE);
+    }
   }
   for (int s = 0; s < nspec; ++s) {
     __syncthreads();
+    SCol cy;
+    cy.load(fo, tx, ty, Ld{f.y + s * n});
     bS.stage<SNW>(fo, Ld{f.y + s * n});
     __syncthreads();
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
       if (!t.valid) continue;
-      const double R = f.wdot[s * n + t.q] - bS.v(t.x, t.y, t.z) * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
-                       d1<1, P>(g, t, bS) * vcy[z] - d1<2, P>(g, t, bS) * vcz[z];
+      const double R = f.wdot[s * n + t.q] - cy.c[z + H] * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
+                       d1<1, P>(g, t, bS) * vcy[z] - d1z<P>(g, t, cy) * vcz[z];
       advance(5 + s, t.q, R);
     }
   }

@@ -206,6 +206,49 @@ struct ZCol {
   }
 };
 
+// Slab: the in-tile planes with x and y halos only, [TZ][TY+2H][TX+2H]. Used
+// with a per-thread register column for the z direction (Column below): the
+// z-halo values of a column are only read by the thread that owns it.
+template <int TX, int TY, int TZ>
+struct Slab {
+  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H;
+  static constexpr int SIZE = TZ * SY * SX;
+  double* p;
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[(z * SY + (y + H)) * SX + (x + H)]; }
+  template <int NW, bool XYC = false, class F>
+  __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
+    stage_rows<SX, -H, TY * TZ, NW>(p, SX, fo,
+                                    [](int r, int& y, int& z, int& d) {
+                                      y = r % TY;
+                                      z = r / TY;
+                                      d = z * SY + y + H;
+                                    },
+                                    f);
+    auto yh = [](int r, int& y, int& z, int& d) {
+      const int k = r % (2 * H);
+      y = k < H ? k - H : TY + k - H;
+      z = r / (2 * H);
+      d = z * SY + y + H;
+    };
+    if (XYC) stage_rows<SX, -H, 2 * H * TZ, NW>(p, SX, fo, yh, f);
+    else stage_rows<TX, 0, 2 * H * TZ, NW>(p + H, SX, fo, yh, f);
+  }
+};
+
+// The thread's own z-column of a field, tile-local z in [-H, TZ+H), held in
+// registers: c[z + H]. load() reads it straight from global memory (a warp
+// reads 32 consecutive x per row: coalesced).
+template <int TZ>
+struct Column {
+  double c[TZ + 2 * H];
+  template <int TX, int TY, class F>
+  __device__ __forceinline__ void load(const Folds<TX, TY, TZ>& fo, int tx, int ty, const F& f) {
+    const int64_t b = fo.ox[tx + H] + fo.oy[ty + H];
+#pragma unroll
+    for (int k = 0; k < TZ + 2 * H; ++k) c[k] = f(b + fo.oz[k]);
+  }
+};
+
 // A grid point of the tile as seen by one thread.
 struct TP {
   int x, y, z;      // tile-local
@@ -260,6 +303,20 @@ __device__ __forceinline__ double dm(const Geo& g, const TP& t, const B& b) {
     return b.v(t.x + dx, t.y + dy, t.z + dz);
   };
   return dmcore(v) * g.ovd[DA] * g.ovd[DB];
+}
+
+// z derivatives from a register column (z in-tile, compile-time after unrolling)
+template <bool P, int TZ>
+__device__ __forceinline__ double d1z(const Geo& g, const TP& t, const Column<TZ>& col) {
+  return d1core([&](int m) { return col.c[t.z + H + m]; }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd[2];
+}
+template <bool P, int TZ>
+__device__ __forceinline__ double d2z(const Geo& g, const TP& t, const Column<TZ>& col) {
+  return d2core([&](int m) { return col.c[t.z + H + m]; }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd2[2];
+}
+template <bool P, int TZ>
+__device__ __forceinline__ double d1zp(const Geo& g, const TP& t, const Column<TZ>& a, const Column<TZ>& b) {
+  return d1core([&](int m) { return a.c[t.z + H + m] * b.c[t.z + H + m]; }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd[2];
 }
 
 }  // namespace tile
