@@ -184,6 +184,44 @@ int senga_chrate_host(senga_ctx* ctx, double* rate);
 typedef double (*senga_integrand)(double x, void* user);
 int senga_integf(senga_integrand f, void* user, double argmin, double argmax, double* answer);
 
+/* ---- batched ensembles --------------------------------------------------------
+ * No counterpart in the reference (it runs one box per MPI job). Many
+ * independent periodic boxes of uneven sizes, one mechanism, each with its own
+ * dt (cfgs[i].tstep): one persistent launch per kernel family per substage
+ * over a device work-list of (box, tile) items; the RK step is captured once
+ * as a CUDA graph. senga_batch_autotune times candidate persistent grid sizes
+ * on the uploaded state (saved and restored) and keeps the fastest. */
+typedef struct senga_batch senga_batch;
+int senga_batch_create(int nbox, const senga_config* cfgs, const senga_chem* chem, const senga_diff* diff,
+                       int device, senga_batch** out);
+int senga_batch_destroy(senga_batch* b);
+int senga_batch_upload_host(senga_batch* b, int ibox, const double* fields, const double* trun,
+                            const int32_t* itndex);
+int senga_batch_download_host(senga_batch* b, int ibox, double* fields, double* trun, int32_t* itndex);
+int senga_batch_step(senga_batch* b, int nsteps);
+int senga_batch_autotune(senga_batch* b, int* grid_stencil, int* grid_thermo);
+int senga_batch_sync(senga_batch* b);
+void* senga_batch_stream(senga_batch* b);
+int senga_batch_status(senga_batch* b, int* status);
+
+/* ---- serving loop ---------------------------------------------------------------
+ * No counterpart in the reference. Continuous batching of DNS requests: a
+ * request (one periodic box, its initial state and a number of RK steps) is
+ * admitted, first come first served, as soon as the device arena of
+ * arena_bytes has room for its fields; all admitted requests advance one RK
+ * step per senga_server_tick in one batched graph; finished requests are
+ * copied back and their memory freed. Times are seconds since creation. */
+typedef struct senga_server senga_server;
+int senga_server_create(size_t arena_bytes, const senga_chem* chem, const senga_diff* diff, int device,
+                        senga_server** out);
+int senga_server_destroy(senga_server* s);
+int senga_server_submit(senga_server* s, const senga_config* cfg, const double* fields, const double* trun,
+                        const int32_t* itndex, int nsteps, int* request_id);
+int senga_server_tick(senga_server* s, int* finished);
+int senga_server_result(senga_server* s, int request_id, double* fields, double* trun, int32_t* itndex,
+                        double* times);
+int senga_server_stats(senga_server* s, int* active, int* pending, int64_t* gpsu, int64_t* free_bytes);
+
 /* ---- allocation-free right-hand side ----------------------------------------
  * No counterpart in the reference. RHSCAL + RHSVEL of one periodic box, like
  * senga_rhs_host, for callers that cannot allocate device memory when they

@@ -301,10 +301,8 @@ struct MechTables {
 
 // -------------------------------------------------------------------------
 template <class M>
-__global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, M m) {
+__device__ __forceinline__ void thermo_point(const Geo& g, const Fields& f, const M& m, const int64_t q) {
   constexpr int NS = M::NS;
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= g.n) return;
   const int64_t n = g.n;
   const double* U = f.uin;
   const double rho = U[q], ru = U[n + q], rv = U[2 * n + q], rw = U[3 * n + q], re = U[4 * n + q];
@@ -406,6 +404,32 @@ __global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, M m) {
   }
 }
 
+template <class M>
+__global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, M m) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  thermo_point(g, f, m, q);
+}
+
+// Batched: CTAs stride over (box, 256-point chunk) items.
+template <class M>
+__global__ void __launch_bounds__(kBlock) k_thermo_b(const BoxDesc* __restrict__ boxes,
+                                                     const WorkItem* __restrict__ chunks, int nchunks, M m) {
+  __shared__ BoxDesc sd;
+  for (int it = blockIdx.x; it < nchunks; it += gridDim.x) {
+    const WorkItem w = chunks[it];
+    __syncthreads();
+    {
+      const double* src = reinterpret_cast<const double*>(boxes + w.box);
+      double* dst = reinterpret_cast<double*>(&sd);
+      for (int e = threadIdx.x; e < (int)(sizeof(BoxDesc) / sizeof(double)); e += blockDim.x) dst[e] = src[e];
+    }
+    __syncthreads();
+    const int64_t q = (int64_t)w.x0 * kBlock + threadIdx.x;
+    if (q < sd.g.n) thermo_point(sd.g, sd.f, m, q);
+  }
+}
+
 // -------------------------------------------------------------------------
 __global__ void k_deriv(Geo g, int kind, const double* __restrict__ in, double* __restrict__ out) {
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -454,6 +478,23 @@ void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const
     else k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<9, false>{dchem, ddiff, nspec});
   }
 }
+
+void launch_batch_thermo(const BoxDesc* boxes, const WorkItem* chunks, int nchunks, int grid, int mech,
+                         const senga_chem* dchem, const senga_diff* ddiff, int nspec, int flmavt, cudaStream_t s) {
+  if (mech == 1) {
+    k_thermo_b<<<grid, kBlock, 0, s>>>(boxes, chunks, nchunks, gen::Mech_onestep{});
+  } else if (mech == 2) {
+    k_thermo_b<<<grid, kBlock, 0, s>>>(boxes, chunks, nchunks, gen::Mech_h2{});
+  } else if (nspec <= 2) {
+    if (flmavt) k_thermo_b<<<grid, kBlock, 0, s>>>(boxes, chunks, nchunks, MechTables<2, true>{dchem, ddiff, nspec});
+    else k_thermo_b<<<grid, kBlock, 0, s>>>(boxes, chunks, nchunks, MechTables<2, false>{dchem, ddiff, nspec});
+  } else {
+    if (flmavt) k_thermo_b<<<grid, kBlock, 0, s>>>(boxes, chunks, nchunks, MechTables<9, true>{dchem, ddiff, nspec});
+    else k_thermo_b<<<grid, kBlock, 0, s>>>(boxes, chunks, nchunks, MechTables<9, false>{dchem, ddiff, nspec});
+  }
+}
+
+int thermo_block() { return kBlock; }
 
 void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s) {
   k_deriv<<<grid_of(g.n), kBlock, 0, s>>>(g, kind, in, out);

@@ -51,11 +51,9 @@ constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + SSlab::SIZE;
 constexpr int kSpecRkSmem = SSlab::SIZE;
 
 template <bool P>
-__global__ void __launch_bounds__(FX* FY, 2) k_flow_t(Geo g, Fields f) {
-  extern __shared__ double sm[];
-  const Origin o{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ};
+__device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const Origin o, double* sm,
+                                          Folds<FX, FY, FZ>& fo) {
   const int tx = threadIdx.x % FX, ty = threadIdx.x / FX;
-  __shared__ Folds<FX, FY, FZ> fo;
   fo.init(g, o);
   __syncthreads();
   TP tp[FZ];
@@ -335,11 +333,9 @@ __global__ void __launch_bounds__(FX* FY, 2) k_flow_t(Geo g, Fields f) {
 
 // -------------------------------------------------------------------------
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int nspec) {
-  extern __shared__ double sm[];
-  const Origin o{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_};
+__device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int nspec, const Origin o, double* sm,
+                                             Folds<SX_, SY_, SZ_>& fo) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
-  __shared__ Folds<SX_, SY_, SZ_> fo;
   fo.init(g, o);
   __syncthreads();
   TP tp[SZ_];
@@ -442,11 +438,9 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int 
 
 // -------------------------------------------------------------------------
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
-  extern __shared__ double sm[];
-  const Origin o{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_};
+__device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, int nspec, const RK& rk,
+                                                const Origin o, double* sm, Folds<SX_, SY_, SZ_>& fo) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
-  __shared__ Folds<SX_, SY_, SZ_> fo;
   fo.init(g, o);
   __syncthreads();
   TP tp[SZ_];
@@ -513,6 +507,77 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_t(Geo g, Fields f, i
   }
 }
 
+// ---- single-box launches: one CTA per tile ----
+template <bool P>
+__global__ void __launch_bounds__(FX* FY, 2) k_flow_t(Geo g, Fields f) {
+  extern __shared__ double sm[];
+  __shared__ Folds<FX, FY, FZ> fo;
+  flow_tile<P>(g, f, Origin{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ}, sm, fo);
+}
+template <bool P>
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int nspec) {
+  extern __shared__ double sm[];
+  __shared__ Folds<SX_, SY_, SZ_> fo;
+  species_tile<P>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm, fo);
+}
+template <bool P>
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
+  extern __shared__ double sm[];
+  __shared__ Folds<SX_, SY_, SZ_> fo;
+  species_rk_tile<P>(g, f, nspec, rk, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_},
+                     sm, fo);
+}
+
+// ---- batched persistent launches: CTAs stride over a (box, tile) work list;
+// the box's descriptor is copied to shared memory per work item ----
+__device__ __forceinline__ void load_desc(const BoxDesc* __restrict__ boxes, int b, BoxDesc& sd) {
+  const double* src = reinterpret_cast<const double*>(boxes + b);
+  double* dst = reinterpret_cast<double*>(&sd);
+  for (int e = threadIdx.x; e < (int)(sizeof(BoxDesc) / sizeof(double)); e += blockDim.x) dst[e] = src[e];
+}
+template <bool P>
+__global__ void __launch_bounds__(FX* FY, 2) k_flow_b(const BoxDesc* __restrict__ boxes, const WorkItem* __restrict__ items,
+                                                      int nitems) {
+  extern __shared__ double sm[];
+  __shared__ Folds<FX, FY, FZ> fo;
+  __shared__ BoxDesc sd;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const WorkItem w = items[it];
+    __syncthreads();
+    load_desc(boxes, w.box, sd);
+    __syncthreads();
+    flow_tile<P>(sd.g, sd.f, Origin{w.x0, w.y0, w.z0}, sm, fo);
+  }
+}
+template <bool P>
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_b(const BoxDesc* __restrict__ boxes,
+                                                           const WorkItem* __restrict__ items, int nitems) {
+  extern __shared__ double sm[];
+  __shared__ Folds<SX_, SY_, SZ_> fo;
+  __shared__ BoxDesc sd;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const WorkItem w = items[it];
+    __syncthreads();
+    load_desc(boxes, w.box, sd);
+    __syncthreads();
+    species_tile<P>(sd.g, sd.f, sd.nspec, Origin{w.x0, w.y0, w.z0}, sm, fo);
+  }
+}
+template <bool P>
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_b(const BoxDesc* __restrict__ boxes,
+                                                              const WorkItem* __restrict__ items, int nitems, int irk) {
+  extern __shared__ double sm[];
+  __shared__ Folds<SX_, SY_, SZ_> fo;
+  __shared__ BoxDesc sd;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const WorkItem w = items[it];
+    __syncthreads();
+    load_desc(boxes, w.box, sd);
+    __syncthreads();
+    species_rk_tile<P>(sd.g, sd.f, sd.nspec, sd.rk[irk], Origin{w.x0, w.y0, w.z0}, sm, fo);
+  }
+}
+
 dim3 tiles(const Geo& g, int tx, int ty, int tz) {
   return dim3((unsigned)((g.nx + tx - 1) / tx), (unsigned)((g.ny + ty - 1) / ty), (unsigned)((g.nz + tz - 1) / tz));
 }
@@ -524,6 +589,9 @@ void set_attrs() {
   cudaFuncSetAttribute(k_flow_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
   cudaFuncSetAttribute(k_species_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
   cudaFuncSetAttribute(k_species_rk_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
+  cudaFuncSetAttribute(k_flow_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
+  cudaFuncSetAttribute(k_species_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
+  cudaFuncSetAttribute(k_species_rk_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
   done = true;
 }
 
@@ -559,6 +627,21 @@ void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk,
     set_attrs<false>();
     k_species_rk_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk);
   }
+}
+
+void tile_shape(int* tx, int* ty, int* tz) {
+  static_assert(FX == SX_ && FY == SY_ && FZ == SZ_, "batched work lists assume one tile shape");
+  *tx = FX;
+  *ty = FY;
+  *tz = FZ;
+}
+
+void launch_batch_stencils(const BoxDesc* boxes, const WorkItem* items, int nitems, int grid, int irk,
+                           cudaStream_t s) {
+  set_attrs<true>();
+  k_flow_b<true><<<grid, FX * FY, kFlowSmem * 8, s>>>(boxes, items, nitems);
+  k_species_b<true><<<grid, SX_ * SY_, kSpecSmem * 8, s>>>(boxes, items, nitems);
+  k_species_rk_b<true><<<grid, SX_ * SY_, kSpecRkSmem * 8, s>>>(boxes, items, nitems, irk);
 }
 
 }  // namespace senga

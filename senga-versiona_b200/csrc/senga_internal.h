@@ -63,6 +63,19 @@ struct RK {
   int last;              // 1 on the final substage (FINCOM)
 };
 
+// One box of a batched ensemble, as the batched kernels see it.
+struct BoxDesc {
+  Geo g;
+  Fields f;
+  RK rk[5];   // RKLHS/RKRHS/RKERR of the five substages (box's own dt)
+  int nspec;
+  int pad;
+};
+// One tile of one box (stencil kernels) or one 256-point chunk (pointwise).
+struct WorkItem {
+  int box, x0, y0, z0;
+};
+
 // Launchers (kernels.cu).
 // Mechanism-specialised thermochemistry: 0 = table-driven (any chem.dat),
 // otherwise the id of a generated policy whose constants equal the loaded
@@ -75,6 +88,14 @@ void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s);
 void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s);
+// Batched ensemble (kernels.cu, kernels_tiled.cu): all boxes periodic, one
+// mechanism; grid = persistent CTA count.
+void tile_shape(int* tx, int* ty, int* tz);
+int thermo_block();
+void launch_batch_thermo(const BoxDesc* boxes, const WorkItem* chunks, int nchunks, int grid, int mech,
+                         const senga_chem* dchem, const senga_diff* ddiff, int nspec, int flmavt, cudaStream_t s);
+void launch_batch_stencils(const BoxDesc* boxes, const WorkItem* items, int nitems, int grid, int irk,
+                           cudaStream_t s);
 void launch_chrate_only(const Geo& g, const Fields& f, const senga_chem* dchem, int nspec, cudaStream_t s);
 
 }  // namespace senga

@@ -123,6 +123,22 @@ def _load():
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
         "senga_temper_host": (ip, [vp, dp, dp]),
         "senga_chrate_host": (ip, [vp, dp]),
+        "senga_batch_create": (ip, [ip, C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), ip, C.POINTER(vp)]),
+        "senga_batch_destroy": (ip, [vp]),
+        "senga_batch_upload_host": (ip, [vp, ip, dp, dp, i32p]),
+        "senga_batch_download_host": (ip, [vp, ip, dp, dp, i32p]),
+        "senga_batch_step": (ip, [vp, ip]),
+        "senga_batch_autotune": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "senga_batch_sync": (ip, [vp]),
+        "senga_batch_stream": (vp, [vp]),
+        "senga_batch_status": (ip, [vp, C.POINTER(C.c_int)]),
+        "senga_server_create": (ip, [C.c_size_t, C.POINTER(ChemT), C.POINTER(DiffT), ip, C.POINTER(vp)]),
+        "senga_server_destroy": (ip, [vp]),
+        "senga_server_submit": (ip, [vp, C.POINTER(ConfigT), dp, dp, i32p, ip, C.POINTER(C.c_int)]),
+        "senga_server_tick": (ip, [vp, C.POINTER(C.c_int)]),
+        "senga_server_result": (ip, [vp, ip, dp, dp, i32p, dp]),
+        "senga_server_stats": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64)]),
         "senga_rhs_noalloc": (ip, [C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), vp, vp, vp, vp, vp,
                                    vp]),
     }
@@ -297,3 +313,134 @@ class Box:
     def d2fdxy(self, f): return self.deriv(6, f)
     def d2fdxz(self, f): return self.deriv(7, f)
     def d2fdyz(self, f): return self.deriv(8, f)
+
+
+def make_config(shape, lengths, tstep, nend=(NPERI,) * 6, adaptive=False, device=0):
+    cfg = ConfigT()
+    cfg.nx, cfg.ny, cfg.nz = shape
+    cfg.xgdlen, cfg.ygdlen, cfg.zgdlen = lengths
+    for i, v in enumerate(nend):
+        cfg.nend[i] = v
+    cfg.tstep = tstep
+    cfg.adaptive = 1 if adaptive else 0
+    cfg.device = device
+    return cfg
+
+
+class Batch:
+    """Ensemble of independent periodic boxes advanced together (one persistent
+    launch per kernel family per substage, RK step as one CUDA graph)."""
+
+    def __init__(self, boxes, chem, diff, device=0):
+        """boxes: list of (shape_xyz, lengths, tstep)."""
+        self.chem, self.diff = chem, diff
+        self.nc = 5 + chem.nspec
+        self.shapes = [(s[2], s[1], s[0]) for s, _, _ in boxes]
+        arr = (ConfigT * len(boxes))(*[make_config(s, l, dt, device=device) for s, l, dt in boxes])
+        h = C.c_void_p()
+        _check(lib.senga_batch_create(len(boxes), arr, C.byref(chem.t), C.byref(diff.t), device, C.byref(h)),
+               "senga_batch_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.senga_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, i, fields, trun, itndex):
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        t = np.ascontiguousarray(trun, dtype=np.float64)
+        it = np.ascontiguousarray(itndex, dtype=np.int32)
+        assert f.shape == (self.nc,) + self.shapes[i]
+        _check(lib.senga_batch_upload_host(self.h, i, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
+               "senga_batch_upload_host")
+
+    def download(self, i):
+        f = np.empty((self.nc,) + self.shapes[i])
+        t = np.empty(self.shapes[i])
+        it = np.empty(self.shapes[i], dtype=np.int32)
+        _check(lib.senga_batch_download_host(self.h, i, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
+               "senga_batch_download_host")
+        return f, t, it
+
+    def step(self, nsteps=1):
+        _check(lib.senga_batch_step(self.h, nsteps), "senga_batch_step")
+
+    def sync(self):
+        _check(lib.senga_batch_sync(self.h), "senga_batch_sync")
+
+    def autotune(self):
+        a, b = C.c_int(), C.c_int()
+        _check(lib.senga_batch_autotune(self.h, C.byref(a), C.byref(b)), "senga_batch_autotune")
+        return {"grid_stencil": a.value, "grid_thermo": b.value}
+
+    @property
+    def stream(self):
+        return lib.senga_batch_stream(self.h)
+
+    def status(self):
+        s = C.c_int()
+        _check(lib.senga_batch_status(self.h, C.byref(s)), "senga_batch_status")
+        return s.value
+
+
+class Server:
+    """Continuous-batching request loop (admission by HBM footprint)."""
+
+    def __init__(self, arena_bytes, chem, diff, device=0):
+        self.chem, self.diff = chem, diff
+        self.nc = 5 + chem.nspec
+        self.shapes = {}
+        h = C.c_void_p()
+        _check(lib.senga_server_create(arena_bytes, C.byref(chem.t), C.byref(diff.t), device, C.byref(h)),
+               "senga_server_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.senga_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, shape, lengths, tstep, fields, trun, itndex, nsteps):
+        cfg = make_config(shape, lengths, tstep)
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        t = np.ascontiguousarray(trun, dtype=np.float64)
+        it = np.ascontiguousarray(itndex, dtype=np.int32)
+        rid = C.c_int()
+        _check(lib.senga_server_submit(self.h, C.byref(cfg), _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       nsteps, C.byref(rid)), "senga_server_submit")
+        self.shapes[rid.value] = (shape[2], shape[1], shape[0])
+        return rid.value
+
+    def tick(self):
+        n = C.c_int()
+        _check(lib.senga_server_tick(self.h, C.byref(n)), "senga_server_tick")
+        return n.value
+
+    def result(self, rid):
+        shp = self.shapes[rid]
+        f = np.empty((self.nc,) + shp)
+        t = np.empty(shp)
+        it = np.empty(shp, dtype=np.int32)
+        tm = np.empty(3)
+        _check(lib.senga_server_result(self.h, rid, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)), _dp(tm)),
+               "senga_server_result")
+        return f, t, it, tm
+
+    def stats(self):
+        a, p = C.c_int(), C.c_int()
+        g, fb = C.c_int64(), C.c_int64()
+        _check(lib.senga_server_stats(self.h, C.byref(a), C.byref(p), C.byref(g), C.byref(fb)), "senga_server_stats")
+        return {"active": a.value, "pending": p.value, "gpsu": g.value, "free_bytes": fb.value}
