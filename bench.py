@@ -135,7 +135,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="grid extent (cubic); 256 is the named workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="h2_kernels", choices=["h2_kernels", "ensemble", "serve"],
+                    help="h2_kernels: the 256^3 headline; ensemble: 64 batched boxes vs one at a time; "
+                         "serve: Poisson request stream through the serving loop")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests")
+    ap.add_argument("--boxes", type=int, default=64, help="ensemble: number of boxes")
     args = ap.parse_args()
+    if args.workload != "h2_kernels":
+        return workload_main(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -284,6 +291,47 @@ def main():
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def workload_main(args):
+    """Ensemble and serving workloads (single GPU)."""
+    import torch
+
+    import workloads
+
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            v, info = cpu_reference_sample(1, 0, n=48)
+            print(json.dumps({"impl": "reference", "metric": "grid-point substage updates/s", "value": v,
+                              "unit": "GPSU/s", "n_gpus": 1, "higher_is_better": True,
+                              "config": {"workload": args.workload},
+                              "cpu_baseline": {"value": v, "unit": "GPSU/s", "cores": info["cores"], "kind": "port",
+                                               "sample": info["sample"]},
+                              "e2e": {"value": v, "unit": "GPSU/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if args.workload == "ensemble":
+        steps = args.steps if args.steps != 5 else 50
+        r = workloads.run_ensemble(steps=steps, warmup=max(3, args.warmup), nbox=args.boxes)
+        line = {"metric": "grid-point substage updates/s", "value": r["batched_gpsu_s"], "unit": "GPSU/s",
+                "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup),
+                "ms_per_step": 1e3 * r["t_batched_s"] / steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "ensemble_64_boxes_{32,48,64,96}^3_1step", "boxes": r["boxes"],
+                           "points": r["points"], "autotune": r["autotune"]},
+                "sequential_value": r["sequential_gpsu_s"], "batched_vs_sequential": r["speedup"],
+                "status_word": r["status_word"]}
+    else:
+        r = workloads.run_serve(nreq=args.requests)
+        line = {"metric": "grid-point substage updates/s", "value": r["served_gpsu_s"], "unit": "GPSU/s",
+                "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"serve_poisson_{r['requests']}req_20per_s", "arena_bytes": r["arena_bytes"]},
+                "p50_s": r["p50_s"], "p99_s": r["p99_s"], "mean_latency_s": r["mean_latency_s"], "wall_s": r["wall_s"],
+                "gpsu": r["gpsu"], "sequential_value": r["sequential_gpsu_s"],
+                "served_vs_sequential": r["served_gpsu_s"] / r["sequential_gpsu_s"],
+                "busy_value": r["busy_gpsu_s"]}
+    print(json.dumps(line))
 
 
 if __name__ == "__main__":

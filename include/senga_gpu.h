@@ -187,10 +187,13 @@ int senga_integf(senga_integrand f, void* user, double argmin, double argmax, do
 /* ---- batched ensembles --------------------------------------------------------
  * No counterpart in the reference (it runs one box per MPI job). Many
  * independent periodic boxes of uneven sizes, one mechanism, each with its own
- * dt (cfgs[i].tstep): one persistent launch per kernel family per substage
- * over a device work-list of (box, tile) items; the RK step is captured once
- * as a CUDA graph. senga_batch_autotune times candidate persistent grid sizes
- * on the uploaded state (saved and restored) and keeps the fastest. */
+ * dt (cfgs[i].tstep): per substage, one launch per kernel family for every 64
+ * boxes, over a device work-list of (box, tile) items (stencil kernels: one
+ * CTA per item; pointwise kernel: a persistent grid striding over 256-point
+ * chunks); the RK step is captured once as a CUDA graph.
+ * senga_batch_autotune times candidate persistent grid sizes of the pointwise
+ * kernel on the uploaded state (saved and restored) and keeps the fastest;
+ * it reports that grid and the number of stencil CTAs per launch. */
 typedef struct senga_batch senga_batch;
 int senga_batch_create(int nbox, const senga_config* cfgs, const senga_chem* chem, const senga_diff* diff,
                        int device, senga_batch** out);

@@ -156,6 +156,30 @@ def stable_dt(chem, fields, T, lengths, shape, cfl=0.5):
     return cfl * dmin / umax
 
 
+def ignition_box(shape_xyz, seed, uprime, tpeak, chem_path=CHEM_1STEP):
+    """One ignition-kernel box of the batched/served workloads: one-step
+    chemistry, premixed reactant at 300 K and 101325 Pa, a centred Gaussian
+    kernel of radius 1 mm and peak tpeak, Passot-Pouquet turbulence of rms
+    uprime and integral scale 1 mm; grid spacing that of the 32^3 case."""
+    from senga import Chem
+
+    nx, ny, nz = shape_xyz
+    dx = 2.0 * math.pi * 1.0e-3 / 31.0
+    lengths = (dx * (nx - 1), dx * (ny - 1), dx * (nz - 1))
+    chem = Chem(chem_path)
+    shp = (nz, ny, nx)
+    centre = (lengths[0] / 2, lengths[1] / 2, lengths[2] / 2)
+    T = hot_kernels(shp, lengths, [centre], 1.0e-3, 300.0, tpeak)
+    Y = np.zeros((2,) + shp)
+    Y[0] = 1.0
+    u, v, w = passot_pouquet(shp, lengths, uprime, 1.0e-3, seed)
+    p = np.full(shp, 101325.0)
+    fields, itn = conserved(chem, p, T, u, v, w, Y)
+    dt = stable_dt(chem, fields, T, lengths, shp)
+    return dict(name="ensemble", shape=tuple(shape_xyz), lengths=lengths, chem=chem_path, diff=None,
+                fields=fields, T=T, itn=itn, dt=dt, nend=(NPERI,) * 6)
+
+
 def make_case(name, n=None, seed=1234, scale_n=None):
     """Named workloads. Returns dict with shape (nx,ny,nz), lengths, chem/diff
     paths, fields (nc,nz,ny,nx), T, itn and a CFL-0.5 dt.
@@ -206,20 +230,9 @@ def make_case(name, n=None, seed=1234, scale_n=None):
     elif name == "ensemble":
         sizes = (32, 48, 64, 96)
         shape_xyz = tuple(int(rng.choice(sizes)) for _ in range(3)) if n is None else (n, n, n)
-        nx, ny, nz = shape_xyz
-        dx = 2.0 * math.pi * 1.0e-3 / 31.0  # the 32^3 case's spacing
-        lengths = (dx * (nx - 1), dx * (ny - 1), dx * (nz - 1))
-        chem_path, diff_path = CHEM_1STEP, None
-        chem = Chem(chem_path)
-        shp = (nz, ny, nx)
         up = float(rng.uniform(0.5, 3.0))
         tpk = float(rng.uniform(1400.0, 2000.0))
-        centre = (lengths[0] / 2, lengths[1] / 2, lengths[2] / 2)
-        T = hot_kernels(shp, lengths, [centre], 1.0e-3, 300.0, tpk)
-        Y = np.zeros((2,) + shp)
-        Y[0] = 1.0
-        u, v, w = passot_pouquet(shp, lengths, up, 1.0e-3, seed)
-        p = np.full(shp, 101325.0)
+        return ignition_box(shape_xyz, seed, up, tpk)
     else:
         raise ValueError(f"unknown case {name}")
     fields, itn = conserved(chem, p, T, u, v, w, Y)

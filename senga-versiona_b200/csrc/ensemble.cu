@@ -23,6 +23,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -175,13 +176,11 @@ class Ensemble {
     int sms = 0;
     CKE(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     sms_ = sms;
-    grid_stencil = 2 * sms;
     grid_thermo = 4 * sms;
   }
   void destroy() {
     drop_graph();
     if (stream) cudaStreamSynchronize(stream);
-    cudaFree(d_desc_);
     cudaFree(d_items_);
     cudaFree(d_chunks_);
     cudaFree(d_chem);
@@ -270,36 +269,51 @@ class Ensemble {
     if (itn) CKE(cudaMemcpyAsync(itn, m.desc.f.itn, n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
   }
 
-  // rebuild descriptors and work lists of the active members
+  // rebuild descriptors and work lists of the active members: boxes go into
+  // tables of kTableBoxes, each with its contiguous run of tiles and chunks
   void rebuild() {
     drop_graph();
-    std::vector<BoxDesc> desc;
+    groups_.clear();
+    grid_stencil = 0;
     std::vector<WorkItem> items, chunks;
     int tx, ty, tz;
     tile_shape(&tx, &ty, &tz);
     const int tb = thermo_block();
     for (size_t k = 0; k < active.size(); ++k) {
+      const int local = (int)(k % kTableBoxes);
+      if (local == 0) {
+        groups_.emplace_back();
+        Group& gr = groups_.back();
+        gr.table.reset(new BoxTable());
+        std::memset(gr.table.get(), 0, sizeof(BoxTable));
+        gr.item0 = (int)items.size();
+        gr.chunk0 = (int)chunks.size();
+      }
+      Group& gr = groups_.back();
       const BoxDesc& b = active[k]->desc;
-      desc.push_back(b);
+      gr.table->d[local] = b;
       const int bx = (b.g.nx + tx - 1) / tx, by = (b.g.ny + ty - 1) / ty, bz = (b.g.nz + tz - 1) / tz;
       for (int z = 0; z < bz; ++z)
         for (int y = 0; y < by; ++y)
-          for (int x = 0; x < bx; ++x) items.push_back(WorkItem{(int)k, x * tx, y * ty, z * tz});
+          for (int x = 0; x < bx; ++x) items.push_back(WorkItem{local, x * tx, y * ty, z * tz});
       const int64_t nch = (b.g.n + tb - 1) / tb;
-      for (int64_t c = 0; c < nch; ++c) chunks.push_back(WorkItem{(int)k, (int)c, 0, 0});
+      for (int64_t c = 0; c < nch; ++c) chunks.push_back(WorkItem{local, (int)c, 0, 0});
+      gr.nitems = (int)items.size() - gr.item0;
+      grid_stencil = (int)items.size();
+      gr.nchunks = (int)chunks.size() - gr.chunk0;
     }
-    nitems_ = (int)items.size();
-    nchunks_ = (int)chunks.size();
-    upload_vec(desc, &d_desc_, &cap_desc_);
     upload_vec(items, &d_items_, &cap_items_);
     upload_vec(chunks, &d_chunks_, &cap_chunks_);
     CKE(cudaStreamSynchronize(stream));
   }
   void substage(int irk) {
     if (active.empty()) return;
-    launch_batch_thermo(d_desc_, d_chunks_, nchunks_, std::min(grid_thermo, nchunks_), mech, d_chem, d_diff, nspec,
-                        diff.flmavt, stream);
-    launch_batch_stencils(d_desc_, d_items_, nitems_, std::min(grid_stencil, nitems_), irk - 1, stream);
+    for (const Group& gr : groups_)
+      launch_batch_thermo(*gr.table, d_chunks_ + gr.chunk0, gr.nchunks, std::min(grid_thermo, gr.nchunks), mech,
+                          d_chem, d_diff, nspec, diff.flmavt, stream);
+    for (int phase = 0; phase < 3; ++phase)
+      for (const Group& gr : groups_)
+        launch_batch_stencil(*gr.table, d_items_ + gr.item0, gr.nitems, irk - 1, phase, stream);
   }
   void step_graph(int nsteps) {
     if (active.empty()) return;
@@ -314,8 +328,9 @@ class Ensemble {
     for (int s = 0; s < nsteps; ++s) CKE(cudaGraphLaunch(graph_, stream));
     CKE(cudaGetLastError());
   }
-  // Times one RK step per candidate persistent-grid configuration on the
-  // live ensemble (state saved and restored) and keeps the fastest.
+  // Times one RK step per candidate persistent grid of the pointwise kernel
+  // on the live ensemble (state saved and restored) and keeps the fastest.
+  // The stencil kernels launch one CTA per tile and have nothing to tune.
   void autotune() {
     if (active.empty()) return;
     // save registers, T and ITNDEX of every member
@@ -335,28 +350,23 @@ class Ensemble {
     cudaEvent_t e0, e1;
     CKE(cudaEventCreate(&e0));
     CKE(cudaEventCreate(&e1));
-    const int st_opts[] = {1, 2, 3, 4, 8};
-    const int th_opts[] = {2, 4, 8, 16};
+    const int th_opts[] = {2, 4, 8, 16, 32};
     float best = 1e30f;
-    int bst = grid_stencil, bth = grid_thermo;
-    for (int a : st_opts)
-      for (int t : th_opts) {
-        grid_stencil = a * sms_;
-        grid_thermo = t * sms_;
-        for (int irk = 1; irk <= 5; ++irk) substage(irk);  // warm
-        CKE(cudaEventRecord(e0, stream));
-        for (int irk = 1; irk <= 5; ++irk) substage(irk);
-        CKE(cudaEventRecord(e1, stream));
-        CKE(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CKE(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) {
-          best = ms;
-          bst = grid_stencil;
-          bth = grid_thermo;
-        }
+    int bth = grid_thermo;
+    for (int t : th_opts) {
+      grid_thermo = t * sms_;
+      for (int irk = 1; irk <= 5; ++irk) substage(irk);  // warm
+      CKE(cudaEventRecord(e0, stream));
+      for (int irk = 1; irk <= 5; ++irk) substage(irk);
+      CKE(cudaEventRecord(e1, stream));
+      CKE(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CKE(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        bth = grid_thermo;
       }
-    grid_stencil = bst;
+    }
     grid_thermo = bth;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -391,11 +401,14 @@ class Ensemble {
     CKE(cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
   }
   int sms_ = 148;
-  BoxDesc* d_desc_ = nullptr;
+  struct Group {
+    std::unique_ptr<BoxTable> table;
+    int item0 = 0, nitems = 0, chunk0 = 0, nchunks = 0;
+  };
+  std::vector<Group> groups_;
   WorkItem* d_items_ = nullptr;
   WorkItem* d_chunks_ = nullptr;
-  size_t cap_desc_ = 0, cap_items_ = 0, cap_chunks_ = 0;
-  int nitems_ = 0, nchunks_ = 0;
+  size_t cap_items_ = 0, cap_chunks_ = 0;
   cudaGraphExec_t graph_ = nullptr;
 };
 

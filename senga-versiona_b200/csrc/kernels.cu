@@ -413,18 +413,11 @@ __global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, M m) {
 
 // Batched: CTAs stride over (box, 256-point chunk) items.
 template <class M>
-__global__ void __launch_bounds__(kBlock) k_thermo_b(const BoxDesc* __restrict__ boxes,
+__global__ void __launch_bounds__(kBlock) k_thermo_b(const __grid_constant__ BoxTable t,
                                                      const WorkItem* __restrict__ chunks, int nchunks, M m) {
-  __shared__ BoxDesc sd;
   for (int it = blockIdx.x; it < nchunks; it += gridDim.x) {
     const WorkItem w = chunks[it];
-    __syncthreads();
-    {
-      const double* src = reinterpret_cast<const double*>(boxes + w.box);
-      double* dst = reinterpret_cast<double*>(&sd);
-      for (int e = threadIdx.x; e < (int)(sizeof(BoxDesc) / sizeof(double)); e += blockDim.x) dst[e] = src[e];
-    }
-    __syncthreads();
+    const BoxDesc& sd = t.d[w.box];
     const int64_t q = (int64_t)w.x0 * kBlock + threadIdx.x;
     if (q < sd.g.n) thermo_point(sd.g, sd.f, m, q);
   }
@@ -479,7 +472,7 @@ void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const
   }
 }
 
-void launch_batch_thermo(const BoxDesc* boxes, const WorkItem* chunks, int nchunks, int grid, int mech,
+void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchunks, int grid, int mech,
                          const senga_chem* dchem, const senga_diff* ddiff, int nspec, int flmavt, cudaStream_t s) {
   if (mech == 1) {
     k_thermo_b<<<grid, kBlock, 0, s>>>(boxes, chunks, nchunks, gen::Mech_onestep{});

@@ -528,54 +528,36 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_t(Geo g, Fields f, i
                      sm, fo);
 }
 
-// ---- batched persistent launches: CTAs stride over a (box, tile) work list;
-// the box's descriptor is copied to shared memory per work item ----
-__device__ __forceinline__ void load_desc(const BoxDesc* __restrict__ boxes, int b, BoxDesc& sd) {
-  const double* src = reinterpret_cast<const double*>(boxes + b);
-  double* dst = reinterpret_cast<double*>(&sd);
-  for (int e = threadIdx.x; e < (int)(sizeof(BoxDesc) / sizeof(double)); e += blockDim.x) dst[e] = src[e];
-}
+// ---- batched launches: one CTA per (box, tile) work item; box descriptors
+// come from the launch's parameter table. (A persistent form that strides
+// over the items keeps per-tile state live across iterations and spills
+// ~2 KB per thread in the flow kernel; one CTA per item does not.) ----
 template <bool P>
-__global__ void __launch_bounds__(FX* FY, 2) k_flow_b(const BoxDesc* __restrict__ boxes, const WorkItem* __restrict__ items,
-                                                      int nitems) {
+__global__ void __launch_bounds__(FX* FY, 2) k_flow_b(const __grid_constant__ BoxTable t,
+                                                      const WorkItem* __restrict__ items) {
   extern __shared__ double sm[];
   __shared__ Folds<FX, FY, FZ> fo;
-  __shared__ BoxDesc sd;
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const WorkItem w = items[it];
-    __syncthreads();
-    load_desc(boxes, w.box, sd);
-    __syncthreads();
-    flow_tile<P>(sd.g, sd.f, Origin{w.x0, w.y0, w.z0}, sm, fo);
-  }
+  const WorkItem w = items[blockIdx.x];
+  const BoxDesc& sd = t.d[w.box];
+  flow_tile<P>(sd.g, sd.f, Origin{w.x0, w.y0, w.z0}, sm, fo);
 }
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, 2) k_species_b(const BoxDesc* __restrict__ boxes,
-                                                           const WorkItem* __restrict__ items, int nitems) {
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_b(const __grid_constant__ BoxTable t,
+                                                           const WorkItem* __restrict__ items) {
   extern __shared__ double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
-  __shared__ BoxDesc sd;
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const WorkItem w = items[it];
-    __syncthreads();
-    load_desc(boxes, w.box, sd);
-    __syncthreads();
-    species_tile<P>(sd.g, sd.f, sd.nspec, Origin{w.x0, w.y0, w.z0}, sm, fo);
-  }
+  const WorkItem w = items[blockIdx.x];
+  const BoxDesc& sd = t.d[w.box];
+  species_tile<P>(sd.g, sd.f, sd.nspec, Origin{w.x0, w.y0, w.z0}, sm, fo);
 }
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_b(const BoxDesc* __restrict__ boxes,
-                                                              const WorkItem* __restrict__ items, int nitems, int irk) {
+__global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_b(const __grid_constant__ BoxTable t,
+                                                              const WorkItem* __restrict__ items, int irk) {
   extern __shared__ double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
-  __shared__ BoxDesc sd;
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const WorkItem w = items[it];
-    __syncthreads();
-    load_desc(boxes, w.box, sd);
-    __syncthreads();
-    species_rk_tile<P>(sd.g, sd.f, sd.nspec, sd.rk[irk], Origin{w.x0, w.y0, w.z0}, sm, fo);
-  }
+  const WorkItem w = items[blockIdx.x];
+  const BoxDesc& sd = t.d[w.box];
+  species_rk_tile<P>(sd.g, sd.f, sd.nspec, sd.rk[irk], Origin{w.x0, w.y0, w.z0}, sm, fo);
 }
 
 dim3 tiles(const Geo& g, int tx, int ty, int tz) {
@@ -636,12 +618,13 @@ void tile_shape(int* tx, int* ty, int* tz) {
   *tz = FZ;
 }
 
-void launch_batch_stencils(const BoxDesc* boxes, const WorkItem* items, int nitems, int grid, int irk,
-                           cudaStream_t s) {
+void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
+                          cudaStream_t s) {
   set_attrs<true>();
-  k_flow_b<true><<<grid, FX * FY, kFlowSmem * 8, s>>>(boxes, items, nitems);
-  k_species_b<true><<<grid, SX_ * SY_, kSpecSmem * 8, s>>>(boxes, items, nitems);
-  k_species_rk_b<true><<<grid, SX_ * SY_, kSpecRkSmem * 8, s>>>(boxes, items, nitems, irk);
+  if (nitems <= 0) return;
+  if (phase < 0 || phase == 0) k_flow_b<true><<<nitems, FX * FY, kFlowSmem * 8, s>>>(boxes, items);
+  if (phase < 0 || phase == 1) k_species_b<true><<<nitems, SX_ * SY_, kSpecSmem * 8, s>>>(boxes, items);
+  if (phase < 0 || phase == 2) k_species_rk_b<true><<<nitems, SX_ * SY_, kSpecRkSmem * 8, s>>>(boxes, items, irk);
 }
 
 }  // namespace senga

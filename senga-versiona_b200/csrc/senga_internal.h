@@ -71,10 +71,21 @@ struct BoxDesc {
   int nspec;
   int pad;
 };
-// One tile of one box (stencil kernels) or one 256-point chunk (pointwise).
+// One tile of one box (stencil kernels) or one 256-point chunk (pointwise);
+// `box` indexes the BoxTable of the launch.
 struct WorkItem {
   int box, x0, y0, z0;
 };
+// The descriptors of up to kTableBoxes boxes, handed to a batched launch by
+// value. Kernel parameters live in a read-only constant bank: a tile function
+// reads any descriptor field as an operand (or reloads it) instead of holding
+// it in a register, as it does for a single-box launch. Larger batches are
+// launched as several tables.
+constexpr int kTableBoxes = 64;
+struct BoxTable {
+  BoxDesc d[kTableBoxes];
+};
+static_assert(sizeof(BoxTable) + 256 <= 32764, "a kernel's parameters are limited to 32764 bytes");
 
 // Launchers (kernels.cu).
 // Mechanism-specialised thermochemistry: 0 = table-driven (any chem.dat),
@@ -92,10 +103,12 @@ void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStr
 // mechanism; grid = persistent CTA count.
 void tile_shape(int* tx, int* ty, int* tz);
 int thermo_block();
-void launch_batch_thermo(const BoxDesc* boxes, const WorkItem* chunks, int nchunks, int grid, int mech,
+void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchunks, int grid, int mech,
                          const senga_chem* dchem, const senga_diff* ddiff, int nspec, int flmavt, cudaStream_t s);
-void launch_batch_stencils(const BoxDesc* boxes, const WorkItem* items, int nitems, int grid, int irk,
-                           cudaStream_t s);
+// Flow, species and species+RK phases of substage irk (0-based), one CTA per
+// work item; `phase` selects one of them (0, 1, 2) or all three (-1).
+void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
+                          cudaStream_t s);
 void launch_chrate_only(const Geo& g, const Fields& f, const senga_chem* dchem, int nspec, cudaStream_t s);
 
 }  // namespace senga
