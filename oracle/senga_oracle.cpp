@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <map>
 #include <memory>
 
 #include "oracle_tables.hpp"
@@ -1246,9 +1247,30 @@ int oracle_chrate(void* h, double* rate_out) {
 int oracle_chem_scalar(void* h, const char* name, double* out) {
   auto* o = static_cast<orc::Oracle*>(h);
   std::string n(name);
+  const orc::FD& f = o->fd;
+  const std::map<std::string, double> fd = {
+      {"acoffx", f.acoffx}, {"bcoffx", f.bcoffx}, {"ccoffx", f.ccoffx}, {"dcoffx", f.dcoffx}, {"ecoffx", f.ecoffx},
+      {"acof1", f.acof1},   {"bcof1", f.bcof1},   {"ccof1", f.ccof1},   {"dcof1", f.dcof1},   {"acof2", f.acof2},
+      {"bcof2", f.bcof2},   {"ccof2", f.ccof2},   {"dcof2", f.dcof2},   {"acof3", f.acof3},   {"bcof3", f.bcof3},
+      {"acof4", f.acof4},   {"bcof4", f.bcof4},   {"ccof4", f.ccof4},   {"acof5", f.acof5},   {"bcof5", f.bcof5},
+      {"ccof5", f.ccof5},   {"dcof5", f.dcof5},   {"acofs", f.acofs},   {"bcofs", f.bcofs},   {"ccofs", f.ccofs},
+      {"dcofs", f.dcofs},   {"ecofs", f.ecofs},   {"acfs1", f.acfs1},   {"bcfs1", f.bcfs1},   {"ccfs1", f.ccfs1},
+      {"dcfs1", f.dcfs1},   {"ecfs1", f.ecfs1},   {"acfs2", f.acfs2},   {"bcfs2", f.bcfs2},   {"ccfs2", f.ccfs2},
+      {"dcfs2", f.dcfs2},   {"ecfs2", f.ecfs2},   {"acfs3", f.acfs3},   {"bcfs3", f.bcfs3},   {"acfs4", f.acfs4},
+      {"bcfs4", f.bcfs4},   {"ccfs4", f.ccfs4},   {"acfs5", f.acfs5},   {"bcfs5", f.bcfs5},   {"ccfs5", f.ccfs5},
+      {"dcfs5", f.dcfs5},   {"acofxy", f.acofxy}, {"bcofxy", f.bcofxy}, {"ccofxy", f.ccofxy},
+      {"dcofxy", f.dcofxy}, {"ecofxy", f.ecofxy}, {"deltax", f.deltax}, {"deltay", f.deltay}, {"deltaz", f.deltaz}};
+  // RK registers per unit dt: rk.lhs<i> = BCOFRK(i), rk.rhs<i> = ACOFRK(i),
+  // rk.err<i> = BCOFRK(i)-BHATRK(i), i = 1..5.
   if (n == "alamda") *out = o->ch.alamda;
   else if (n == "prefgb") *out = o->ch.prefgb;
-  else if (n == "deltax") *out = o->fd.deltax;
+  else if (fd.count(n)) *out = fd.at(n);
+  else if (n.size() == 7 && n.compare(0, 6, "rk.lhs") == 0 && n[6] >= '1' && n[6] <= '5')
+    *out = o->rklhs[n[6] - '1'] / o->cf.tstep;
+  else if (n.size() == 7 && n.compare(0, 6, "rk.rhs") == 0 && n[6] >= '1' && n[6] <= '5')
+    *out = o->rkrhs[n[6] - '1'] / o->cf.tstep;
+  else if (n.size() == 7 && n.compare(0, 6, "rk.err") == 0 && n[6] >= '1' && n[6] <= '5')
+    *out = o->rkerr[n[6] - '1'] / o->cf.tstep;
   else return 1;
   return 0;
 }

@@ -185,3 +185,31 @@ def test_generated_and_table_driven_thermochemistry_agree(name, monkeypatch):
     for k in range(r_o.shape[0]):
         assert rel_linf(r_gen[k], r_tab[k]) <= 1e-12, f"field {k}"
         assert rel_linf(r_tab[k], r_o[k]) <= TOL_STATE, f"field {k}"
+
+
+@pytest.mark.parametrize("key", ["h2_mavt", "onestep"])
+def test_golden_fixture_rhs_and_two_steps(key):
+    """The committed oracle fixtures (tests/golden/oracle_*.npz, non-cubic
+    12x10x8): right-hand side and the state after two RK steps."""
+    import os
+
+    import cases
+    import senga
+
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"oracle_{key}.npz"))
+    shape = tuple(int(v) for v in g["shape"])
+    chem = senga.Chem(os.path.join(cases.DATA, str(g["chem"])))
+    diff = senga.Diff(os.path.join(cases.DATA, str(g["diff"])) if str(g["diff"]) else None, chem)
+    box = senga.Box(shape, tuple(g["lengths"]), chem, diff, float(g["dt"]))
+    box.upload(g["fields"], g["T"], g["itn"])
+    r, t, p = box.rhs()
+    for k in range(r.shape[0]):
+        assert rel_linf(r[k], g["rhs"][k]) <= TOL_STATE, f"rhs field {k}"
+    assert rel_linf(t, g["T_rhs"]) <= TOL_STATE
+    assert rel_linf(p, g["p_rhs"]) <= TOL_STATE
+    box.upload(g["fields"], g["T"], g["itn"])
+    box.step(2)
+    f2, t2, _ = box.download()
+    for k in range(f2.shape[0]):
+        assert rel_linf(f2[k], g["fields_2"][k]) <= TOL_STATE, f"field {k}"
+    assert rel_linf(t2, g["T_2"]) <= TOL_STATE
