@@ -40,6 +40,17 @@ def peaks():
         return FALLBACK_HBM, "fallback"
 
 
+def dram_traffic_per_point():
+    """DRAM bytes per point of each kernel from the committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one capture, per point;
+    the traffic grows in proportion to the point count)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic_h2_kernels.json")) as fh:
+            return json.load(fh)["dram_bytes_per_point"]
+    except Exception:
+        return {}
+
+
 def compulsory_bytes_per_gpsu(nspec):
     # read+write of the S and U registers and of T (Newton seed): 8*(4*Nc+2)
     return 8 * (4 * (5 + nspec) + 2)
@@ -255,6 +266,7 @@ def main():
         return
 
     hbm, peak_kind = peaks()
+    fp64 = senga.fp64_peak(local)  # FP64 FMA probe: denominator of the thermochemistry kernel's FP64 figure
     kb = kernel_bytes_per_point(chem.nspec)
     kern = {}
     tot = sum(prof.values())
@@ -266,6 +278,8 @@ def main():
     stencil = max(("flow", "species_a", "species_b_rk"), key=lambda k: prof[k])
     dom = max(prof, key=prof.get)
     rk = kern[stencil]
+    tpp = dram_traffic_per_point().get(stencil)
+    traffic = tpp * npts if tpp else None
     step_ms = ms / args.steps
     whole = gpsu / world * compulsory_bytes_per_gpsu(chem.nspec) / 1e9
     cpu = None
@@ -277,10 +291,12 @@ def main():
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload,
         "roofline": {"bound": "hbm", "kernel": stencil, "achieved": rk["achieved_gbs"], "peak": hbm,
-                     "unit": "GB/s", "frac": rk["frac_hbm"], "traffic": None, "peak_kind": peak_kind},
+                     "unit": "GB/s", "frac": rk["frac_hbm"], "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic_source": "profiles/dram_traffic_h2_kernels.json (128^3 capture, per point x points)"},
         "dominant_kernel": dom,
         "kernels": kern,
         "whole_step_hbm_frac": whole / hbm,
+        "fp64_peak_tflops_measured": fp64,
         "compulsory_bytes_per_gpsu": compulsory_bytes_per_gpsu(chem.nspec),
         "cpu_baseline": cpu,
         "e2e": e2e,

@@ -159,6 +159,11 @@ int senga_profile_step(senga_ctx* ctx, double* ms, int* launches);
  * device bytes the context holds. */
 int senga_ctx_info(senga_ctx* ctx, int* mech, int64_t* device_bytes);
 
+/* Measured FP64 FMA throughput of the device in TFLOP/s (independent FMA
+ * chains on every SM): the denominator of the FP64-pipe roofline of the
+ * pointwise thermochemistry kernel. No counterpart in the reference. */
+int senga_fp64_peak(int device, double* tflops);
+
 /* Status word of the last steps: bit 0 = TEMPER non-convergence. */
 int senga_get_status(senga_ctx* ctx, int* status);
 

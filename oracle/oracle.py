@@ -4,9 +4,11 @@ ctypes wrapper of liboracle.so, the CPU restatement of the reference's
 RHSCAL/RHSVEL/TEMPER/CHRATE/derivatives/LINCOM path (senga_oracle.cpp).
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
 it, and only as the checker or the timed CPU baseline, never as the product.
-Parity status: the reference is Fortran and no Fortran compiler exists in
-this build environment, so the oracle is pinned by its own known-answer
-tests (tests/test_oracle_kat.py) rather than by outputs of the reference.
+Parity unpinned against outputs of the reference: it is Fortran and no
+Fortran compiler exists in this build environment, and the reference ships
+no tests. The oracle is pinned by known-answer tests instead
+(tests/test_oracle_kat.py: constants read from the reference sources,
+closed-form answers, RK order, conservation, committed fixtures).
 """
 import ctypes as C
 import os

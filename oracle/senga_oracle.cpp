@@ -5,6 +5,11 @@
 // only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
 // The product library never links or calls it.
 //
+// Parity unpinned against outputs of the reference: it is Fortran and cannot
+// be compiled in this environment, and it ships no tests. The restatement is
+// pinned by known-answer tests instead (constants read from the reference
+// sources, closed-form stencil/rate/TEMPER answers, RK order, conservation).
+//
 // Loop order, expression association and array conventions follow the
 // Fortran (column-major, halo of 5, 1-based indices). Compile with
 // -ffp-contract=off so that, like gfortran's x86-64 default, no FMA is formed.

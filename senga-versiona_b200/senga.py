@@ -119,6 +119,7 @@ def _load():
         "senga_get_status": (ip, [vp, C.POINTER(C.c_int)]),
         "senga_profile_step": (ip, [vp, dp, C.POINTER(C.c_int)]),
         "senga_ctx_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+        "senga_fp64_peak": (ip, [ip, dp]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
         "senga_temper_host": (ip, [vp, dp, dp]),
@@ -150,6 +151,13 @@ def _load():
 
 
 lib = _load()
+
+
+def fp64_peak(device=0):
+    """Measured FP64 FMA throughput of the device, TFLOP/s."""
+    v = C.c_double()
+    _check(lib.senga_fp64_peak(device, C.byref(v)), "senga_fp64_peak")
+    return v.value
 
 
 def _check(rc, what):
