@@ -177,6 +177,19 @@ int senga_get_status(senga_ctx* ctx, int* status);
 int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
 
+/* Explicit filter FLTREM (src/fltrem.f:43-90) of the U register (xRHS):
+ * FILTRX -> FILTRY -> FILTRZ (src/filtrx.f:56-295) on every conserved field,
+ * 12th-order interior, 6th..11th-order one-sided rows on bounded faces,
+ * coefficients of FLINIT (src/flinit.f:42-…). The reference never calls it
+ * (src/senga2.f:178 is commented out); a host calls this after a step, e.g.
+ * every 10 steps. mode bit 0: flip the sign of TWFACT (the coded sign
+ * amplifies the grid-scale mode; flipped, the filter damps it); bit 1: also
+ * filter the S register (xRUN), which the reference leaves unfiltered.
+ * Periodic neighbours at +-6 are reached by index wrap. */
+int senga_filter(senga_ctx* ctx, int mode);
+/* The three-pass filter of one interior field (host pointers). */
+int senga_filter_field_host(senga_ctx* ctx, int mode, const double* f, double* out);
+
 /* TEMPER (src/temper.f:58-219) on the current U register; host outputs of
  * T and p (either may be NULL). CHRATE (src/chrate.f:146-741) on the current U
  * register and T: host output of RATE (nspec interior arrays). */

@@ -54,6 +54,8 @@ def _get():
         lib.oracle_deriv.argtypes = [C.c_void_p, C.c_int, dp, dp]
         lib.oracle_chrate.argtypes = [C.c_void_p, dp]
         lib.oracle_chem_scalar.argtypes = [C.c_void_p, C.c_char_p, dp]
+        lib.oracle_filter.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle_filter_field.argtypes = [C.c_void_p, C.c_int, dp, dp]
         _lib = lib
     return _lib
 
@@ -134,6 +136,18 @@ class Oracle:
         out = np.empty_like(a)
         if _get().oracle_deriv(self.h, kind, _dp(a), _dp(out)) != 0:
             raise RuntimeError("oracle_deriv: " + _get().oracle_last_error().decode())
+        return out
+
+    def filter(self, mode=0):
+        """FLTREM on the registers; mode bit 0 flips TWFACT, bit 1 also filters S."""
+        if _get().oracle_filter(self.h, mode) != 0:
+            raise RuntimeError("oracle_filter: " + _get().oracle_last_error().decode())
+
+    def filter_field(self, f, mode=0):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.empty_like(a)
+        if _get().oracle_filter_field(self.h, mode, _dp(a), _dp(out)) != 0:
+            raise RuntimeError("oracle_filter_field: " + _get().oracle_last_error().decode())
         return out
 
     def scalar(self, name):

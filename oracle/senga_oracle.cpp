@@ -1045,6 +1045,99 @@ struct Oracle {
     for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last);
   }
 
+  // ---- explicit filter: src/flinit.f:42-…, src/filtrx.f:56-295 (+y, z),
+  // src/fltrem.f:43-90 ----
+  // 12th-order interior F = c0 f_i + sum_m c_m (f_{i+m} + f_{i-m}), m=1..6,
+  // and 6th..11th-order one-sided rows on the first/last six points of a
+  // bounded direction. Coefficients are TWFACT times integers (flinit.f) with
+  // TWFACT = -EXP(-12 LOG 2) as coded, or +EXP(-12 LOG 2) (sign flipped:
+  // the dissipative filter) when `flip`.
+  // Deviations from the coded routine, on purpose: periodic neighbours at
+  // +-6 are taken by index wrap (the reference reads +-6 from a 5-deep halo,
+  // outside the array), and each directional pass sees the current values
+  // of the previous pass (the reference's halo is not refreshed between
+  // FILTRX/Y/Z). The filter is called nowhere in the reference
+  // (src/senga2.f:178 is commented out).
+  struct FilterCoef {
+    double in[7];       // c1..c6, c0
+    double bnd[6][12];  // rows 1..6 (row r uses r+6 entries)
+  };
+  FilterCoef filter_coef(bool flip) const {
+    FilterCoef c{};
+    const double tw0 = -std::exp(-1.2e1 * std::log(2.0));
+    const double tw = flip ? -tw0 : tw0;
+    const double ints[6] = {7.92e2, -4.95e2, 2.20e2, -6.60e1, 1.20e1, -1.00};
+    for (int m = 0; m < 6; ++m) c.in[m] = ints[m] * tw;
+    c.in[6] = 1.0 + (-9.24e2 * tw);
+    const double rows[6][12] = {
+        {-1, 6, -15, 20, -15, 6, -1},
+        {6, -37, 96, -135, 110, -51, 12, -1},
+        {-15, 96, -262, 396, -360, 200, -66, 12, -1},
+        {20, -135, 396, -662, 696, -480, 220, -66, 12, -1},
+        {-15, 110, -360, 696, -887, 786, -495, 220, -66, 12, -1},
+        {6, -51, 200, -480, 786, -923, 792, -495, 220, -66, 12, -1}};
+    for (int r = 0; r < 6; ++r) {
+      for (int e = 0; e < r + 7; ++e) c.bnd[r][e] = rows[r][e] * tw;
+      c.bnd[r][r] = 1.0 + c.bnd[r][r];  // the diagonal entry carries the 1
+    }
+    return c;
+  }
+  template <int dir>
+  void filter_dir(Field& F, const FilterCoef& c) {
+    const int n = dir == 0 ? nx : dir == 1 ? ny : nz;
+    const int nl = dir == 0 ? nendxl : dir == 1 ? nendyl : nendzl;
+    const int nr = dir == 0 ? nendxr : dir == 1 ? nendyr : nendzr;
+    const int n1 = dir == 0 ? ny : nx, n2 = dir == 0 ? nz : dir == 1 ? nz : ny;
+    const bool per = nl == NPERI;
+    Field out;
+    out.init(nx, ny, nz);
+    for (int q = 1; q <= n2; ++q)
+      for (int p = 1; p <= n1; ++p) {
+        auto f = [&](int a) {
+          if (per) a = ((a - 1) % n + n) % n + 1;
+          return at<dir>(F, a, p, q);
+        };
+        const int ist = nl == NBOUND ? 7 : 1, ifn = nr == NBOUND ? n - 6 : n;
+        for (int ic = ist; ic <= ifn; ++ic) {
+          const double fa = f(ic + 1) + f(ic - 1), fb = f(ic + 2) + f(ic - 2), fc = f(ic + 3) + f(ic - 3);
+          const double fd = f(ic + 4) + f(ic - 4), fe = f(ic + 5) + f(ic - 5), ff = f(ic + 6) + f(ic - 6);
+          at<dir>(out, ic, p, q) = c.in[0] * fa + c.in[1] * fb + c.in[2] * fc + c.in[3] * fd + c.in[4] * fe +
+                                   c.in[5] * ff + c.in[6] * f(ic);
+        }
+        if (nl == NBOUND)
+          for (int r = 0; r < 6; ++r) {
+            double v = c.bnd[r][0] * f(1);
+            for (int e = 1; e < r + 7; ++e) v = v + c.bnd[r][e] * f(1 + e);
+            at<dir>(out, 1 + r, p, q) = v;
+          }
+        if (nr == NBOUND)
+          for (int r = 0; r < 6; ++r) {
+            double v = c.bnd[r][0] * f(n);
+            for (int e = 1; e < r + 7; ++e) v = v + c.bnd[r][e] * f(n - e);
+            at<dir>(out, n - r, p, q) = v;
+          }
+      }
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) F(i, j, k) = out(i, j, k);
+  }
+  void filter_field(Field& F, const FilterCoef& c) {
+    filter_dir<0>(F, c);
+    filter_dir<1>(F, c);
+    filter_dir<2>(F, c);
+  }
+  // FLTREM: every U-register field (xRHS) in the order D, U, V, W, E, Y_k;
+  // with `also_run` the S register too (the reference filters xRHS only).
+  void fltrem(bool flip, bool also_run) {
+    const FilterCoef c = filter_coef(flip);
+    for (Field* f : {&drhs, &urhs, &vrhs, &wrhs, &erhs}) filter_field(*f, c);
+    for (auto& y : yrhs) filter_field(y, c);
+    if (also_run) {
+      for (Field* f : {&drun, &urun, &vrun, &wrun, &erun}) filter_field(*f, c);
+      for (auto& y : yrun) filter_field(y, c);
+    }
+  }
+
   void rhs() {
     parfer();
     rhscal();
@@ -1184,6 +1277,39 @@ int oracle_rhs(void* h, double* rhs_out, double* t_out, double* p_out) {
           if (t_out) t_out[q] = o->trun(i, j, k);
           if (p_out) p_out[q] = o->prun(i, j, k);
         }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// Explicit filter (FLTREM) of the registers: mode bit 0 flips the sign of
+// TWFACT (dissipative filter), bit 1 also filters the S register.
+int oracle_filter(void* h, int mode) {
+  try {
+    static_cast<orc::Oracle*>(h)->fltrem(mode & 1, mode & 2);
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// The three-pass filter of one interior field.
+int oracle_filter_field(void* h, int mode, const double* f, double* out) {
+  try {
+    auto* o = static_cast<orc::Oracle*>(h);
+    orc::Field& F = o->store7;
+    for (int k = 1; k <= o->nz; ++k)
+      for (int j = 1; j <= o->ny; ++j)
+        for (int i = 1; i <= o->nx; ++i)
+          F(i, j, k) = f[(size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1))];
+    o->filter_field(F, o->filter_coef(mode & 1));
+    for (int k = 1; k <= o->nz; ++k)
+      for (int j = 1; j <= o->ny; ++j)
+        for (int i = 1; i <= o->nx; ++i)
+          out[(size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1))] = F(i, j, k);
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

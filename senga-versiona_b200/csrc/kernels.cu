@@ -404,8 +404,20 @@ __device__ __forceinline__ void thermo_point(const Geo& g, const Fields& f, cons
   }
 }
 
+// Resident blocks per SM asked of the compiler for a policy (register cap
+// 65536 / (256 * blocks)): more warps hide the FP64 dependency chains of the
+// long straight-line mechanisms.
 template <class M>
-__global__ void __launch_bounds__(kBlock) k_thermo(Geo g, Fields f, M m) {
+struct ThermoOcc {
+  static constexpr int blocks = 1;
+};
+template <>
+struct ThermoOcc<gen::Mech_h2> {
+  static constexpr int blocks = 2;
+};
+
+template <class M>
+__global__ void __launch_bounds__(kBlock, ThermoOcc<M>::blocks) k_thermo(Geo g, Fields f, M m) {
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= g.n) return;
   thermo_point(g, f, m, q);

@@ -382,6 +382,37 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
   });
 }
 
+int senga_filter(senga_ctx* c, int mode) {
+  if (!c || mode < 0 || mode > 3) return fail(SENGA_ERR_ARG, "senga_filter: bad argument");
+  return guard([&] {
+    const FilterCoef cf = filter_coef(mode & 1);
+    const int64_t n = c->geo.n;
+    double* t1 = c->f.rhs;  // free between steps
+    double* t2 = c->f.rhs + n;
+    for (int fl = 0; fl < c->nc; ++fl) launch_filter_field(c->geo, c->f.uin + fl * n, c->f.uin + fl * n, t1, t2, cf, c->stream);
+    if (mode & 2)
+      for (int fl = 0; fl < c->nc; ++fl)
+        launch_filter_field(c->geo, c->f.run + fl * n, c->f.run + fl * n, t1, t2, cf, c->stream);
+    CK(cudaGetLastError());
+  });
+}
+
+int senga_filter_field_host(senga_ctx* c, int mode, const double* f, double* out) {
+  if (!c || !f || !out || mode < 0 || mode > 3) return fail(SENGA_ERR_ARG, "senga_filter_field_host: bad argument");
+  return guard([&] {
+    const int64_t n = c->geo.n;
+    const size_t bytes = n * sizeof(double);
+    double* a = c->f.rhs;
+    double* t1 = c->f.rhs + n;
+    double* t2 = c->f.rhs + 2 * n;
+    CK(cudaMemcpyAsync(a, f, bytes, cudaMemcpyHostToDevice, c->stream));
+    launch_filter_field(c->geo, a, a, t1, t2, filter_coef(mode & 1), c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, a, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
 int senga_temper_host(senga_ctx* c, double* trun, double* prun) {
   if (!c) return fail(SENGA_ERR_ARG, "null context");
   return guard([&] {

@@ -109,6 +109,16 @@ void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchu
 // work item; `phase` selects one of them (0, 1, 2) or all three (-1).
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
+// Explicit filter (filter.cu): coefficient table of FLINIT, sign-flipped
+// when flip (dissipative), and the three-pass filter of one interior field
+// (in -> t1 -> t2 -> out; out may alias in).
+struct FilterCoef {
+  double in[7];       // c1..c6 of the +-m pairs, then c0
+  double bnd[6][12];  // one-sided rows of the first/last six points
+};
+FilterCoef filter_coef(bool flip);
+void launch_filter_field(const Geo& g, const double* in, double* out, double* t1, double* t2, const FilterCoef& c,
+                         cudaStream_t s);
 void launch_chrate_only(const Geo& g, const Fields& f, const senga_chem* dchem, int nspec, cudaStream_t s);
 
 }  // namespace senga

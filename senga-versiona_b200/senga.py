@@ -120,6 +120,8 @@ def _load():
         "senga_profile_step": (ip, [vp, dp, C.POINTER(C.c_int)]),
         "senga_ctx_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
         "senga_fp64_peak": (ip, [ip, dp]),
+        "senga_filter": (ip, [vp, ip]),
+        "senga_filter_field_host": (ip, [vp, ip, dp, dp]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
         "senga_temper_host": (ip, [vp, dp, dp]),
@@ -310,6 +312,18 @@ class Box:
         assert a.shape == self.shape
         out = np.empty_like(a)
         _check(lib.senga_deriv_host(self.h, kind, _dp(a), _dp(out)), "senga_deriv_host")
+        return out
+
+    def filter(self, mode=0):
+        """FLTREM on the U register (mode bit 0: flip TWFACT's sign; bit 1:
+        also filter the S register)."""
+        _check(lib.senga_filter(self.h, mode), "senga_filter")
+
+    def filter_field(self, f, mode=0):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        assert a.shape == self.shape
+        out = np.empty_like(a)
+        _check(lib.senga_filter_field_host(self.h, mode, _dp(a), _dp(out)), "senga_filter_field_host")
         return out
 
     def dfbydx(self, f): return self.deriv(0, f)

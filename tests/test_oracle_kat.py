@@ -325,3 +325,42 @@ def test_oracle_reproduces_golden_fixture(key):
     for k in range(f2.shape[0]):
         assert rel_linf(f2[k], g["fields_2"][k]) <= 1e-13, k
     assert np.array_equal(itn2, g["itn_2"])
+
+
+# ------------------------------------------------------------ explicit filter
+def _tw():
+    return math.exp(-12.0 * math.log(2.0))
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+@pytest.mark.parametrize("flip", [0, 1])
+def test_filter_transfer_function(axis, flip):
+    """Interior 12th-order filter (src/filtrx.f:67-104, coefficients
+    src/flinit.f): a mode exp(i theta j) is multiplied by
+    1 + sin^12(theta/2) with the coded TWFACT = -2^-12 (grid-scale modes
+    are amplified) and by 1 - sin^12(theta/2) with the sign flipped."""
+    o = _oracle(SHAPE, LEN)
+    for mode in (1, 3, SHAPE[axis] // 2):
+        th, ph = _grid_phase(axis, mode)
+        f = np.cos(ph)
+        T = 1.0 + (-1.0 if flip else 1.0) * math.sin(th / 2) ** 12
+        assert rel_linf(o.filter_field(f, mode=flip), T * f) <= 1e-13
+
+
+def test_filter_one_sided_rows_keep_quintics():
+    """The boundary rows (6th..11th order, src/flinit.f FACF1X..FLCF6X) and
+    the interior leave polynomials of degree <= 5 unchanged."""
+    nend = (1, 1, 1, 1, 1, 1)
+    o = _oracle(SHAPE, LEN, nend=nend)
+    nx, ny, nz = SHAPE
+    z, y, x = np.meshgrid(np.arange(nz) / nz, np.arange(ny) / ny, np.arange(nx) / nx, indexing="ij")
+    f = 0.4 + x - 2 * y ** 2 + 3 * z ** 3 - x ** 4 * y + 0.5 * x ** 2 * y * z ** 2 + 0.7 * x ** 5
+    assert rel_linf(o.filter_field(f), f) <= 1e-12
+
+
+def test_filter_rows_sum_to_one():
+    """Every row of the filter conserves a constant: c0 + 2 sum c_m = 1 and
+    each one-sided row sums to 1."""
+    o = _oracle(SHAPE, LEN, nend=(1, 1, 2, 2, 2, 2))
+    f = np.full((SHAPE[2], SHAPE[1], SHAPE[0]), 3.25)
+    assert float(np.max(np.abs(o.filter_field(f) - 3.25))) <= 1e-13
