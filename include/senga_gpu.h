@@ -177,6 +177,15 @@ int senga_get_status(senga_ctx* ctx, int* status);
 int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
 
+/* Adaptive time step (cfg.adaptive = 1, the reference's NSTPSW = 1):
+ * ADAPTT (src/adaptt.f:53-330) runs after every step of senga_step /
+ * senga_step_graph (the latter then launches kernels per step, since dt
+ * changes): per-field maxima of |ERR|/(|RUN|+norm) on the device, the PID
+ * controller of DTINIT (src/dtinit.f:99-175) on the host, RK coefficients
+ * rescaled, error register zeroed. This returns the current TSTEP, the last
+ * ERRMAX and INDERR (-4 rho, -1..-3 momentum, 0 energy, k species). */
+int senga_get_tstep(senga_ctx* ctx, double* tstep, double* errmax, int* inderr);
+
 /* Explicit filter FLTREM (src/fltrem.f:43-90) of the U register (xRHS):
  * FILTRX -> FILTRY -> FILTRZ (src/filtrx.f:56-295) on every conserved field,
  * 12th-order interior, 6th..11th-order one-sided rows on bounded faces,

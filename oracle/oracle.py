@@ -55,6 +55,8 @@ def _get():
         lib.oracle_chrate.argtypes = [C.c_void_p, dp]
         lib.oracle_chem_scalar.argtypes = [C.c_void_p, C.c_char_p, dp]
         lib.oracle_filter.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle_set_adaptive.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle_tstep.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int)]
         lib.oracle_filter_field.argtypes = [C.c_void_p, C.c_int, dp, dp]
         _lib = lib
     return _lib
@@ -137,6 +139,14 @@ class Oracle:
         if _get().oracle_deriv(self.h, kind, _dp(a), _dp(out)) != 0:
             raise RuntimeError("oracle_deriv: " + _get().oracle_last_error().decode())
         return out
+
+    def set_adaptive(self, on=True):
+        _get().oracle_set_adaptive(self.h, 1 if on else 0)
+
+    def tstep(self):
+        t, e, i = C.c_double(), C.c_double(), C.c_int()
+        _get().oracle_tstep(self.h, C.byref(t), C.byref(e), C.byref(i))
+        return t.value, e.value, i.value
 
     def filter(self, mode=0):
         """FLTREM on the registers; mode bit 0 flips TWFACT, bit 1 also filters S."""

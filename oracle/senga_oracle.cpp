@@ -179,6 +179,7 @@ struct Oracle {
     mk(yrun); mk(yrhs); mk(yerr); mk(rate); mk(rrte);
     itndex.init(nx, ny, nz);
     dtinit(c.tstep);
+    tstep_now = c.tstep;
   }
 
   // ---- RK coefficients: src/dtinit.f:76-209 ----
@@ -1143,13 +1144,73 @@ struct Oracle {
     rhscal();
     rhsvel();
   }
+  // ---- ADAPTT: src/adaptt.f:53-330 with the controller constants and error
+  // norms DTINIT leaves in force (src/dtinit.f:99-175: ERRTOL 1e-4, ERRLOW
+  // 1e-30, TRMAX 1.01, TRMIN 1e-2, TSMAX 1, TSMIN 1e-15; norms D 0, u/v/w 1e-6,
+  // E 1e-2, Y 1e-10; PID CTMULT 0.9, CTALPH 0.49/3, CTBETA 0.34/3, CTGAMA
+  // 0.1/3; ERROLD = ERRLDR = ERRTOL on a cold start) ----
+  bool fladpt = false;
+  double tstep_now = 0.0, errold = 1.0e-4, errldr = 1.0e-4, errmax_last = 0.0;
+  int inderr = 0;
+  static double field_errmax(const Field& err, const Field& run, double nrm, int nx_, int ny_, int nz_) {
+    double tot = 0.0;
+    for (int k = 1; k <= nz_; ++k)
+      for (int j = 1; j <= ny_; ++j)
+        for (int i = 1; i <= nx_; ++i) {
+          const double fornow = std::fabs(err(i, j, k)) / (std::fabs(run(i, j, k)) + nrm);
+          if (fornow > tot) tot = fornow;
+        }
+    return tot;
+  }
+  void adaptt() {
+    const double errtol = 1.0e-4, errlow = 1.0e-30, trmax = 1.01, trmin = 1.0e-2, tsmax = 1.0, tsmin = 1.0e-15;
+    const double ctmult = 9.0e-1, ctalph = 4.9e-1 / 3.0, ctbeta = 3.4e-1 / 3.0, ctgama = 1.0e-1 / 3.0;
+    const double ed = field_errmax(derr, drun, 0.0, nx, ny, nz);
+    const double eu = field_errmax(uerr, urun, 1.0e-6, nx, ny, nz);
+    const double ev = field_errmax(verr, vrun, 1.0e-6, nx, ny, nz);
+    const double ew = field_errmax(werr, wrun, 1.0e-6, nx, ny, nz);
+    const double ee = field_errmax(eerr, erun, 1.0e-2, nx, ny, nz);
+    double errmax = 0.0;
+    if (ed > errmax) { errmax = ed; inderr = -4; }
+    if (eu > errmax) { errmax = eu; inderr = -1; }
+    if (ev > errmax) { errmax = ev; inderr = -2; }
+    if (ew > errmax) { errmax = ew; inderr = -3; }
+    if (ee > errmax) { errmax = ee; inderr = 0; }
+    for (int is = 0; is < nspec; ++is) {
+      const double ey = field_errmax(yerr[is], yrun[is], 1.0e-10, nx, ny, nz);
+      if (ey > errmax) { errmax = ey; inderr = is + 1; }
+    }
+    if (errmax < errlow) errmax = errlow;
+    errmax_last = errmax;
+    double tratio = ctmult * std::exp(ctalph * std::log(errtol / errmax) + ctbeta * std::log(errold / errtol) +
+                                      ctgama * std::log(errtol / errldr));
+    errldr = errold;
+    errold = errmax;
+    if (tratio > trmax) tratio = trmax;
+    if (tratio < trmin) tratio = trmin;
+    const double tstold = tstep_now;
+    tstep_now = tstep_now * tratio;
+    if (tstep_now > tsmax) tstep_now = tsmax;
+    if (tstep_now < tsmin) tstep_now = tsmin;
+    tratio = tstep_now / tstold;
+    for (int i = 0; i < 5; ++i) {
+      rklhs[i] = rklhs[i] * tratio;
+      rkrhs[i] = rkrhs[i] * tratio;
+      rkerr[i] = rkerr[i] * tratio;
+    }
+    for (Field* f : {&derr, &uerr, &verr, &werr, &eerr}) std::fill(f->v.begin(), f->v.end(), 0.0);
+    for (auto& y : yerr) std::fill(y.v.begin(), y.v.end(), 0.0);
+  }
+
   // One time step: senga2.f:106-159 (periodic: BOUNDT/BOUNDS/BOUNTT are
-  // no-ops; FLTREM is commented out at senga2.f:178; fixed dt, ADAPTT idle).
+  // no-ops; FLTREM is commented out at senga2.f:178; ADAPTT runs when the
+  // step switch asks for adaptive steps, src/dtinit.f:174-175).
   void step() {
     for (int irk = 1; irk <= 5; ++irk) {
       rhs();
       lincom(irk, irk == 5);
     }
+    if (fladpt) adaptt();
   }
 };
 
@@ -1282,6 +1343,21 @@ int oracle_rhs(void* h, double* rhs_out, double* t_out, double* p_out) {
     g_err = e.what();
     return 1;
   }
+}
+
+// Adaptive time stepping (ADAPTT after every step) on or off.
+int oracle_set_adaptive(void* h, int on) {
+  static_cast<orc::Oracle*>(h)->fladpt = on != 0;
+  return 0;
+}
+
+// Current TSTEP, last ERRMAX and INDERR of the controller.
+int oracle_tstep(void* h, double* tstep, double* errmax, int* inderr) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  if (tstep) *tstep = o->tstep_now;
+  if (errmax) *errmax = o->errmax_last;
+  if (inderr) *inderr = o->inderr;
+  return 0;
 }
 
 // Explicit filter (FLTREM) of the registers: mode bit 0 flips the sign of

@@ -11,6 +11,7 @@
 // stencils, so no halo exchange runs.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -65,6 +66,10 @@ struct senga_ctx {
   double rklhs[5], rkrhs[5], rkerr[5];
   cudaGraphExec_t graph = nullptr;
   int mech = 0;  // thermochemistry policy (select_mech)
+  // ADAPTT state (cfg.adaptive): current TSTEP, ERROLD/ERRLDR, last ERRMAX
+  double tstep = 0.0, errold = 1.0e-4, errldr = 1.0e-4, errmax = 0.0;
+  int inderr = 0, sms = 148;
+  unsigned long long* d_errmax = nullptr;
 };
 
 namespace {
@@ -119,6 +124,52 @@ void run_substage(senga_ctx* c, int irk) {
   launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
 }
 
+// ADAPTT (src/adaptt.f:53-330) after a step: error maxima on the device, the
+// PID controller on the host with the constants DTINIT leaves in force
+// (src/dtinit.f:99-175), RK coefficients rescaled by TRATIO as the reference
+// does (cumulatively), error register zeroed.
+void adaptt(senga_ctx* c) {
+  const int nc = c->nc;
+  ErrNorms nrm{};
+  const double base[5] = {0.0, 1.0e-6, 1.0e-6, 1.0e-6, 1.0e-2};
+  for (int fl = 0; fl < nc; ++fl) nrm.v[fl] = fl < 5 ? base[fl] : 1.0e-10;
+  launch_errmax(c->geo.n, nc, c->f.err, c->f.run, nrm, c->d_errmax, c->sms, c->stream);
+  unsigned long long bits[5 + SENGA_NSPCMX];
+  CK(cudaMemcpyAsync(bits, c->d_errmax, nc * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemsetAsync(c->f.err, 0, (size_t)nc * c->geo.n * sizeof(double), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double tot[5 + SENGA_NSPCMX];
+  std::memcpy(tot, bits, nc * sizeof(double));
+  const double errtol = 1.0e-4, errlow = 1.0e-30, trmax = 1.01, trmin = 1.0e-2, tsmax = 1.0, tsmin = 1.0e-15;
+  const double ctmult = 9.0e-1, ctalph = 4.9e-1 / 3.0, ctbeta = 3.4e-1 / 3.0, ctgama = 1.0e-1 / 3.0;
+  // field order and strict comparisons of adaptt.f: D(-4), U(-1), V(-2), W(-3), E(0), Y_k(k)
+  const int code[5] = {-4, -1, -2, -3, 0};
+  double errmax = 0.0;
+  for (int fl = 0; fl < nc; ++fl)
+    if (tot[fl] > errmax) {
+      errmax = tot[fl];
+      c->inderr = fl < 5 ? code[fl] : fl - 4;
+    }
+  if (errmax < errlow) errmax = errlow;
+  c->errmax = errmax;
+  double tratio = ctmult * std::exp(ctalph * std::log(errtol / errmax) + ctbeta * std::log(c->errold / errtol) +
+                                    ctgama * std::log(errtol / c->errldr));
+  c->errldr = c->errold;
+  c->errold = errmax;
+  if (tratio > trmax) tratio = trmax;
+  if (tratio < trmin) tratio = trmin;
+  const double tstold = c->tstep;
+  c->tstep = c->tstep * tratio;
+  if (c->tstep > tsmax) c->tstep = tsmax;
+  if (c->tstep < tsmin) c->tstep = tsmin;
+  tratio = c->tstep / tstold;
+  for (int i = 0; i < 5; ++i) {
+    c->rklhs[i] = c->rklhs[i] * tratio;
+    c->rkrhs[i] = c->rkrhs[i] * tratio;
+    c->rkerr[i] = c->rkerr[i] * tratio;
+  }
+}
+
 template <class Fn>
 int guard(Fn&& fn) {
   try {
@@ -159,6 +210,9 @@ int senga_ctx_create(const senga_config* cfg, const senga_chem* chem, const seng
     CK(cudaMemcpy(c->d_chem, &c->chem, sizeof(senga_chem), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->d_diff, &c->diff, sizeof(senga_diff), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_status, sizeof(unsigned int)));
+    CK(cudaMalloc(&c->d_errmax, (5 + SENGA_NSPCMX) * sizeof(unsigned long long)));
+    CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, cfg->device));
+    c->tstep = cfg->tstep;
     CK(cudaMemset(c->d_status, 0, sizeof(unsigned int)));
     const int64_t n = c->geo.n;
     const int S = c->nspec, nc = c->nc;
@@ -215,6 +269,7 @@ int senga_ctx_destroy(senga_ctx* c) {
   cudaFree(c->d_chem);
   cudaFree(c->d_diff);
   cudaFree(c->d_status);
+  cudaFree(c->d_errmax);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SENGA_OK;
@@ -262,14 +317,17 @@ int senga_substage(senga_ctx* c, int irkstp) {
 int senga_step(senga_ctx* c, int nsteps) {
   if (!c || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_step: bad argument");
   return guard([&] {
-    for (int s = 0; s < nsteps; ++s)
+    for (int s = 0; s < nsteps; ++s) {
       for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
+      if (c->cfg.adaptive) adaptt(c);
+    }
     CK(cudaGetLastError());
   });
 }
 
 int senga_step_graph(senga_ctx* c, int nsteps) {
   if (!c || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_step_graph: bad argument");
+  if (c->cfg.adaptive) return senga_step(c, nsteps);  // dt changes every step: no fixed graph
   return guard([&] {
     if (!c->graph) {
       cudaGraph_t gr;
@@ -380,6 +438,14 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
     CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });
+}
+
+int senga_get_tstep(senga_ctx* c, double* tstep, double* errmax, int* inderr) {
+  if (!c) return fail(SENGA_ERR_ARG, "senga_get_tstep: null context");
+  if (tstep) *tstep = c->tstep;
+  if (errmax) *errmax = c->errmax;
+  if (inderr) *inderr = c->inderr;
+  return SENGA_OK;
 }
 
 int senga_filter(senga_ctx* c, int mode) {

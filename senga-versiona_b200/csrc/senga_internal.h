@@ -109,6 +109,14 @@ void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchu
 // work item; `phase` selects one of them (0, 1, 2) or all three (-1).
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
+// ADAPTT error maxima (adapt.cu): out[fl] = max |err|/(|run| + nrm.v[fl])
+// as the bit pattern of a non-negative double, per conserved field.
+struct ErrNorms {
+  double v[5 + SENGA_NSPCMX];
+};
+void launch_errmax(int64_t n, int nc, const double* err, const double* run, const ErrNorms& nrm,
+                   unsigned long long* out, int sms, cudaStream_t s);
+
 // Explicit filter (filter.cu): coefficient table of FLINIT, sign-flipped
 // when flip (dissipative), and the three-pass filter of one interior field
 // (in -> t1 -> t2 -> out; out may alias in).

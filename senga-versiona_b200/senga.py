@@ -121,6 +121,7 @@ def _load():
         "senga_ctx_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
         "senga_fp64_peak": (ip, [ip, dp]),
         "senga_filter": (ip, [vp, ip]),
+        "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
         "senga_filter_field_host": (ip, [vp, ip, dp, dp]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
@@ -313,6 +314,12 @@ class Box:
         out = np.empty_like(a)
         _check(lib.senga_deriv_host(self.h, kind, _dp(a), _dp(out)), "senga_deriv_host")
         return out
+
+    def tstep(self):
+        """(TSTEP, last ERRMAX, INDERR) of the adaptive controller."""
+        t, e, i = C.c_double(), C.c_double(), C.c_int()
+        _check(lib.senga_get_tstep(self.h, C.byref(t), C.byref(e), C.byref(i)), "senga_get_tstep")
+        return t.value, e.value, i.value
 
     def filter(self, mode=0):
         """FLTREM on the U register (mode bit 0: flip TWFACT's sign; bit 1:

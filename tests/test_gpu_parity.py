@@ -250,3 +250,30 @@ def test_filter_then_steps_match_oracle(mode):
     for k in range(o.shape[0]):
         assert rel_linf(g[k], o[k]) <= TOL_STATE, f"field {k}"
     assert rel_linf(tg, to) <= TOL_STATE
+
+
+def test_adaptive_steps_match_oracle():
+    """ADAPTT after every step: dt sequence, ERRMAX, INDERR and the state."""
+    import senga
+    from oracle import Oracle
+
+    c = _case("h2_kernels", 16)
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(c["diff"], chem)
+    box = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"], adaptive=True)
+    ref = Oracle(c["shape"], c["lengths"], c["chem"], c["diff"], c["dt"])
+    ref.set_adaptive(True)
+    box.upload(c["fields"], c["T"], c["itn"])
+    ref.upload(c["fields"], c["T"], c["itn"])
+    for _ in range(3):
+        box.step(1)
+        ref.step(1)
+        tg, eg, ig = box.tstep()
+        to, eo, io = ref.tstep()
+        assert abs(tg - to) <= 1e-9 * to
+        assert abs(eg - eo) <= 1e-6 * eo
+        assert ig == io
+    g, _, _ = box.download()
+    o, _, _ = ref.download()
+    for k in range(o.shape[0]):
+        assert rel_linf(g[k], o[k]) <= TOL_STATE, f"field {k}"

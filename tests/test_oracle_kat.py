@@ -364,3 +364,28 @@ def test_filter_rows_sum_to_one():
     o = _oracle(SHAPE, LEN, nend=(1, 1, 2, 2, 2, 2))
     f = np.full((SHAPE[2], SHAPE[1], SHAPE[0]), 3.25)
     assert float(np.max(np.abs(o.filter_field(f) - 3.25))) <= 1e-13
+
+
+# ------------------------------------------------------------ ADAPTT
+def test_adaptt_pid_controller_first_steps():
+    """ADAPTT (src/adaptt.f) with DTINIT's PID constants: on a cold start
+    ERROLD = ERRLDR = ERRTOL = 1e-4, so the first ratio is
+    0.9 (ERRTOL/ERRMAX)^(0.49/3), clipped to [0.01, 1.01]; the second uses
+    ERROLD = first ERRMAX."""
+    import cases
+
+    c = cases.make_case("ignition32", n=12, seed=8)
+    o = _oracle(c["shape"], c["lengths"], chem=c["chem"], dt=c["dt"])
+    o.upload(c["fields"], c["T"], c["itn"])
+    o.set_adaptive(True)
+    o.step(1)
+    t1, e1, i1 = o.tstep()
+    r = min(1.01, max(0.01, 0.9 * math.exp((0.49 / 3) * math.log(1e-4 / e1))))
+    assert math.isclose(t1, c["dt"] * r, rel_tol=1e-14)
+    assert e1 > 0 and i1 in (-4, -3, -2, -1, 0, 1, 2)
+    o.step(1)
+    t2, e2, _ = o.tstep()
+    r2 = 0.9 * math.exp((0.49 / 3) * math.log(1e-4 / e2) + (0.34 / 3) * math.log(e1 / 1e-4)
+                        + (0.1 / 3) * math.log(1e-4 / 1e-4))
+    r2 = min(1.01, max(0.01, r2))
+    assert math.isclose(t2, t1 * r2, rel_tol=1e-13)
