@@ -93,8 +93,11 @@ void build_geo(const senga_config& c, Geo& g) {
 void check_config(const senga_config& c, int nspec) {
   const int n3[3] = {c.nx, c.ny, c.nz};
   for (int d = 0; d < 3; ++d) {
-    if (n3[d] < 11) throw Error(SENGA_ERR_ARG, "grid extent must be at least 11 points per direction");
     const int l = c.nend[2 * d], r = c.nend[2 * d + 1];
+    // periodic: the 13-point filter wraps once (6 points); bounded: the
+    // filter's one-sided rows read 12 points, the derivative closures 11
+    if (n3[d] < (l == SENGA_NPERI ? 6 : 12))
+      throw Error(SENGA_ERR_ARG, "grid extent must be at least 6 points per periodic and 12 per bounded direction");
     if ((l == SENGA_NPERI) != (r == SENGA_NPERI))
       throw Error(SENGA_ERR_ARG, "periodic end conditions must be set on both faces of a direction");
     if (l != SENGA_NPERI)
