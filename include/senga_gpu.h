@@ -177,6 +177,31 @@ int senga_get_status(senga_ctx* ctx, int* status);
 int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
 
+/* NSCBC x faces (config: bounded x, NBOUND on both x faces; y, z periodic).
+ * xl = 13: I3 subsonic inflow at x-left with constant velocity (NXLPRM(1)=1):
+ *   u = u_in, v = w = 0, density rho_in (DRIN), mass fractions y_in (YRIN)
+ *   imposed on the inflow plane (BOUNDT src/boundt.f:177-200, BOUNTT
+ *   src/bountt.f:203-252, RK ranges src/bcinit.f), energy by the wave
+ *   amplitudes of BOUNDS src/bounds.f:610-675.
+ * xr = 21: O1 partially non-reflecting outflow at x-right: pressure relaxed
+ *   to p_inf with COBCXR = sigma (1 - eta) / (2 XGDLEN) (RXRPRM(1..3)), pio =
+ *   NXRPRM(1) (inflow-through-outlet switch), bet_local = NXRPRM(2) (local
+ *   Mach number in place of BET = 0.05 on the transverse terms), BOUNDS
+ *   src/bounds.f:1198-1450; viscous shear, conduction and diffusion zeroed on
+ *   the plane (FXRVST, FXRCON, FXRDIF, FXRADB).
+ * Face data and wave amplitudes are computed after the thermochemistry
+ * kernel and added to the face planes' right-hand side in the RK epilogue.
+ * Other face kinds return SENGA_ERR_UNSUPPORTED. Stepping a box with a
+ * bounded x direction needs this call first. */
+typedef struct senga_nscbc {
+  int xl, xr;
+  double u_in, rho_in;
+  double y_in[SENGA_NSPCMX];
+  double p_inf, sigma, eta;
+  int pio, bet_local;
+} senga_nscbc;
+int senga_set_nscbc(senga_ctx* ctx, const senga_nscbc* bc);
+
 /* Adaptive time step (cfg.adaptive = 1, the reference's NSTPSW = 1):
  * ADAPTT (src/adaptt.f:53-330) runs after every step of senga_step /
  * senga_step_graph (the latter then launches kernels per step, since dt

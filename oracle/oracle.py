@@ -24,6 +24,12 @@ def build():
     subprocess.run(["make", "-C", HERE, "-s"], check=True)
 
 
+class _Bc(C.Structure):
+    _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
+                ("y_in", C.c_double * 9), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
+                ("pio", C.c_int), ("bet_local", C.c_int)]
+
+
 class _Cfg(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("xgdlen", C.c_double), ("ygdlen", C.c_double), ("zgdlen", C.c_double),
@@ -56,6 +62,7 @@ def _get():
         lib.oracle_chem_scalar.argtypes = [C.c_void_p, C.c_char_p, dp]
         lib.oracle_filter.argtypes = [C.c_void_p, C.c_int]
         lib.oracle_set_adaptive.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle_set_bc.argtypes = [C.c_void_p, C.POINTER(_Bc)]
         lib.oracle_tstep.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int)]
         lib.oracle_filter_field.argtypes = [C.c_void_p, C.c_int, dp, dp]
         _lib = lib
@@ -139,6 +146,19 @@ class Oracle:
         if _get().oracle_deriv(self.h, kind, _dp(a), _dp(out)) != 0:
             raise RuntimeError("oracle_deriv: " + _get().oracle_last_error().decode())
         return out
+
+    def set_bc(self, bc):
+        """NSCBC x faces: bc = dict(xl=13|0, xr=21|0, u_in, rho_in, y_in, p_inf,
+        sigma, eta, pio=0, bet_local=0)."""
+        b = _Bc()
+        b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
+        b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
+        for i, v in enumerate(bc.get("y_in", ())):
+            b.y_in[i] = v
+        b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
+        b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
+        if _get().oracle_set_bc(self.h, C.byref(b)) != 0:
+            raise RuntimeError("oracle_set_bc: " + _get().oracle_last_error().decode())
 
     def set_adaptive(self, on=True):
         _get().oracle_set_adaptive(self.h, 1 if on else 0)

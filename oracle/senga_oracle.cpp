@@ -324,37 +324,86 @@ struct Oracle {
         for (int ic = 1; ic <= n; ++ic) at<dir>(D, ic, p, q) = at<dir>(D, ic, p, q) * ovd2;
       }
   }
-  // Mixed derivative, interior scheme (src/d2fdxy.f:67-141; scaling :1925-1937).
-  // plane 0: xy, 1: xz, 2: yz. Both directions must be periodic here; the
-  // one-sided edge/corner closures are not restated in this oracle.
+  // Mixed derivative (src/d2fdxy.f:55-1937, d2fdxz.f, d2fdyz.f): 10th-order
+  // diagonal interior scheme (:67-141); with a bounded x direction the x-left
+  // and x-right inner points (:151-392) use the 4th/4th/4th/6th/8th closures:
+  // the first two points apply the one-sided first-derivative rows in x to a
+  // 4th-order centred difference in the other direction (ACOFY1, BCOFY1),
+  // points 3-5 diagonal 4th/6th/8th-order schemes. Scaling :1925-1937.
+  // plane 0: xy, 1: xz, 2: yz. Only the x-bounded edges are restated (the
+  // other direction periodic); other bounded combinations throw.
   template <int plane>
   void dmix(Field& F, Field& D) {
     double s1 = plane == 2 ? fd.ovdely : fd.ovdelx;
     double s2 = plane == 0 ? fd.ovdely : fd.ovdelz;
     int na = plane == 2 ? ny : nx, nb = plane == 0 ? ny : nz, nc = plane == 0 ? nz : plane == 1 ? ny : nx;
-    bool bnd = plane == 0 ? (nendxl == NBOUND || nendxr == NBOUND || nendyl == NBOUND || nendyr == NBOUND)
-               : plane == 1 ? (nendxl == NBOUND || nendxr == NBOUND || nendzl == NBOUND || nendzr == NBOUND)
-                            : (nendyl == NBOUND || nendyr == NBOUND || nendzl == NBOUND || nendzr == NBOUND);
-    if (bnd) throw std::runtime_error("oracle: mixed-derivative closures not restated");
+    const bool xb = nendxl == NBOUND || nendxr == NBOUND;
+    const bool yb = nendyl == NBOUND || nendyr == NBOUND;
+    const bool zb = nendzl == NBOUND || nendzr == NBOUND;
+    const bool bnd_a = plane == 2 ? yb : xb;
+    const bool bnd_b = plane == 0 ? yb : (plane == 1 ? zb : zb);
+    if (bnd_b || (plane == 2 && bnd_a))
+      throw std::runtime_error("oracle: mixed-derivative closures restated for bounded x only");
     const FD& c = fd;
+    const double ay = 4.0 / 3.0 / 2.0, by = -1.0 / 3.0 / 4.0;  // ACOFY1, BCOFY1 (= ACOFZ1, BCOFZ1)
+    const double c3a = (4.0 / 3.0) / 4.0, c3b = (-1.0 / 3.0) / 4.0 / 4.0;
+    const double c4a = (3.0 / 2.0) / 4.0, c4b = (-3.0 / 5.0) / 4.0 / 4.0, c4c = (1.0 / 1.0e1) / 4.0 / 9.0;
+    const double c5a = (8.0 / 5.0) / 4.0, c5b = (-4.0 / 5.0) / 4.0 / 4.0, c5c = (8.0 / 3.5e1) / 4.0 / 9.0,
+                 c5d = (-1.0 / 3.5e1) / 4.0 / 1.6e1;
+    const int ist = (bnd_a && nendxl == NBOUND) ? 6 : 1, ifn = (bnd_a && nendxr == NBOUND) ? na - 5 : na;
 #pragma omp parallel for schedule(static)
     for (int r = 1; r <= nc; ++r)
-      for (int b = 1; b <= nb; ++b)
-        for (int a = 1; a <= na; ++a) {
-          auto f = [&](int da, int db) -> double {
-            if (plane == 0) return F(a + da, b + db, r);
-            if (plane == 1) return F(a + da, r, b + db);
-            return F(r, a + da, b + db);
-          };
-          double fa = f(1, 1) - f(1, -1) - f(-1, 1) + f(-1, -1);
-          double fb = f(2, 2) - f(2, -2) - f(-2, 2) + f(-2, -2);
-          double fc = f(3, 3) - f(3, -3) - f(-3, 3) + f(-3, -3);
-          double fdd = f(4, 4) - f(4, -4) - f(-4, 4) + f(-4, -4);
-          double fe = f(5, 5) - f(5, -5) - f(-5, 5) + f(-5, -5);
-          double v = c.acofxy * fa + c.bcofxy * fb + c.ccofxy * fc + c.dcofxy * fdd + c.ecofxy * fe;
-          double& out = plane == 0 ? D(a, b, r) : plane == 1 ? D(a, r, b) : D(r, a, b);
-          out = v * s1 * s2;
+      for (int b = 1; b <= nb; ++b) {
+        auto f = [&](int a, int db) -> double {
+          if (plane == 0) return F(a, b + db, r);
+          if (plane == 1) return F(a, r, b + db);
+          return F(r, a, b + db);
+        };
+        auto out = [&](int a) -> double& { return plane == 0 ? D(a, b, r) : plane == 1 ? D(a, r, b) : D(r, a, b); };
+        auto dg = [&](int a, int m) {  // diagonal difference at distance m around a
+          return f(a + m, m) - f(a + m, -m) - f(a - m, m) + f(a - m, -m);
+        };
+        for (int a = ist; a <= ifn; ++a) {
+          double fa = dg(a, 1), fb = dg(a, 2), fc = dg(a, 3), fdd = dg(a, 4), fe = dg(a, 5);
+          out(a) = (c.acofxy * fa + c.bcofxy * fb + c.ccofxy * fc + c.dcofxy * fdd + c.ecofxy * fe) * s1 * s2;
         }
+        // 4th-order centred difference in the second direction along x-row a
+        auto g = [&](int a, int a0) {  // (f(a) - f(a0)) pairs, as the Fortran groups them
+          return ay * (f(a, 1) - f(a, -1) - f(a0, 1) + f(a0, -1)) + by * (f(a, 2) - f(a, -2) - f(a0, 2) + f(a0, -2));
+        };
+        if (bnd_a && nendxl == NBOUND) {
+          out(1) = (c.acof1 * g(2, 1) + c.bcof1 * g(3, 1) + c.ccof1 * g(4, 1) + c.dcof1 * g(5, 1)) * s1 * s2;
+          out(2) = (c.acof2 * g(1, 2) + c.bcof2 * g(3, 2) + c.ccof2 * g(4, 2) + c.dcof2 * g(5, 2)) * s1 * s2;
+          out(3) = (c3a * (f(4, 1) - f(4, -1) - f(2, 1) + f(2, -1)) + c3b * (f(5, 2) - f(5, -2) - f(1, 2) + f(1, -2))) *
+                   s1 * s2;
+          out(4) = (c4a * (f(5, 1) - f(5, -1) - f(3, 1) + f(3, -1)) + c4b * (f(6, 2) - f(6, -2) - f(2, 2) + f(2, -2)) +
+                    c4c * (f(7, 3) - f(7, -3) - f(1, 3) + f(1, -3))) *
+                   s1 * s2;
+          out(5) = (c5a * (f(6, 1) - f(6, -1) - f(4, 1) + f(4, -1)) + c5b * (f(7, 2) - f(7, -2) - f(3, 2) + f(3, -2)) +
+                    c5c * (f(8, 3) - f(8, -3) - f(2, 3) + f(2, -3)) + c5d * (f(9, 4) - f(9, -4) - f(1, 4) + f(1, -4))) *
+                   s1 * s2;
+        }
+        if (bnd_a && nendxr == NBOUND) {
+          const int L = na;
+          out(L - 4) = (c5a * (f(L - 3, 1) - f(L - 3, -1) - f(L - 5, 1) + f(L - 5, -1)) +
+                        c5b * (f(L - 2, 2) - f(L - 2, -2) - f(L - 6, 2) + f(L - 6, -2)) +
+                        c5c * (f(L - 1, 3) - f(L - 1, -3) - f(L - 7, 3) + f(L - 7, -3)) +
+                        c5d * (f(L, 4) - f(L, -4) - f(L - 8, 4) + f(L - 8, -4))) *
+                       s1 * s2;
+          out(L - 3) = (c4a * (f(L - 2, 1) - f(L - 2, -1) - f(L - 4, 1) + f(L - 4, -1)) +
+                        c4b * (f(L - 1, 2) - f(L - 1, -2) - f(L - 5, 2) + f(L - 5, -2)) +
+                        c4c * (f(L, 3) - f(L, -3) - f(L - 6, 3) + f(L - 6, -3))) *
+                       s1 * s2;
+          out(L - 2) = (c3a * (f(L - 1, 1) - f(L - 1, -1) - f(L - 3, 1) + f(L - 3, -1)) +
+                        c3b * (f(L, 2) - f(L, -2) - f(L - 4, 2) + f(L - 4, -2))) *
+                       s1 * s2;
+          out(L - 1) = (c.acof2 * g(L - 1, L) + c.bcof2 * g(L - 1, L - 2) + c.ccof2 * g(L - 1, L - 3) +
+                        c.dcof2 * g(L - 1, L - 4)) *
+                       s1 * s2;
+          out(L) = (c.acof1 * g(L, L - 1) + c.bcof1 * g(L, L - 2) + c.ccof1 * g(L, L - 3) + c.dcof1 * g(L, L - 4)) *
+                   s1 * s2;
+        }
+      }
   }
   void dfbydx(Field& F, Field& D) { d1<0>(F, D); }
   void dfbydy(Field& F, Field& D) { d1<1>(F, D); }
@@ -375,6 +424,228 @@ struct Oracle {
   void zx(bool l, bool r, Field& D) { if (l) zero_plane(D, 0, false); if (r) zero_plane(D, 0, true); }
   void zy(bool l, bool r, Field& D) { if (l) zero_plane(D, 1, false); if (r) zero_plane(D, 1, true); }
   void zz(bool l, bool r, Field& D) { if (l) zero_plane(D, 2, false); if (r) zero_plane(D, 2, true); }
+
+  // ---- NSCBC x faces: BCINIT flags and ranges (src/bcinit.f:287-600), face
+  // data gathered inside RHSCAL/RHSVEL, BOUNDT (src/boundt.f:58-211), BOUNDS
+  // (src/bounds.f:115-372, 610-675, 1198-1450), BOUNTT (src/bountt.f:61-260).
+  // Restated: I3 inflow at x-left (NXLPRM(1)=1: constant u, v=w=0, density
+  // DRIN, mass fractions YRIN) and O1 partially non-reflecting outflow at
+  // x-right; y and z periodic.
+  static constexpr int BC_NONE = 0, BC_I3 = 13, BC_O1 = 21;
+  int bcxl = BC_NONE, bcxr = BC_NONE;
+  double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0;
+  int pio_xr = 0, betloc_xr = 0;
+  bool fxlcnv = false, fxrcnv = false;
+  int istald = 1, istalu = 1, istalv = 1, istalw = 1, istale = 1, istaly = 1;
+  struct Face {
+    std::vector<double> d, u, v, w, p, t, r, g, e, bcl1, bcl2, bcl3, bcl4, bcl5, t1b, t2b, t3b, t4b, t51b, t52b;
+    std::vector<double> y, h, rate, bcly, t6b;  // [nspec][ny*nz]
+    void init(int m, int ns) {
+      for (auto* a : {&d, &u, &v, &w, &p, &t, &r, &g, &e, &bcl1, &bcl2, &bcl3, &bcl4, &bcl5, &t1b, &t2b, &t3b, &t4b,
+                      &t51b, &t52b})
+        a->assign(m, 0.0);
+      for (auto* a : {&y, &h, &rate, &bcly, &t6b}) a->assign((size_t)m * ns, 0.0);
+    }
+  } fxl, fxr;
+  inline int fj(int jc, int kc) const { return (jc - 1) + ny * (kc - 1); }
+  inline int fs(int is, int jc, int kc) const { return is * ny * nz + (jc - 1) + ny * (kc - 1); }
+  // visit both active x faces: fn(face, ic)
+  template <class Fn>
+  void faces(Fn&& fn) {
+    if (fxlcnv) fn(fxl, istal);
+    if (fxrcnv) fn(fxr, istol);
+  }
+  template <class Fn>
+  void face_pts(Fn&& fn) {
+    faces([&](Face& F, int ic) {
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) fn(F, ic, jc, kc, fj(jc, kc));
+    });
+  }
+  void set_bc(int xl, int xr, double u_in, double rho_in, const double* y_in, double p_inf, double sigma,
+              double eta, int pio, int betloc) {
+    if ((xl != BC_NONE && xl != BC_I3) || (xr != BC_NONE && xr != BC_O1))
+      throw std::runtime_error("oracle: NSCBC restated for I3 at x-left and O1 at x-right");
+    if ((xl != BC_NONE && nendxl != NBOUND) || (xr != BC_NONE && nendxr != NBOUND))
+      throw std::runtime_error("oracle: NSCBC faces need NBOUND end conditions");
+    bcxl = xl;
+    bcxr = xr;
+    uin = u_in;
+    rhoin = rho_in;
+    for (int is = 0; is < nspec; ++is) yin[is] = y_in[is];
+    pinfxr = p_inf;
+    cobcxr = sigma * (1.0 - eta) / (2.0 * cf.xgdlen);  // COBCXR, src/bcinit.f
+    pio_xr = pio;
+    betloc_xr = betloc;
+    fxlcnv = xl != BC_NONE;
+    fxrcnv = xr != BC_NONE;
+    if (xl == BC_I3) {  // src/bcinit.f: FXLCNV, FXLVSN; D,U,V,W,Y ranges start at ISTAP1
+      fxlvsn = true;
+      istald = istalu = istalv = istalw = istaly = istal + 1;
+    }
+    if (xr == BC_O1) {  // FXRCNV, FXRVST, FXRCON, FXRADB, FXRDIF
+      fxrvst = fxrcon = fxradb = fxrdif = true;
+    }
+    fxl.init(ny * nz, nspec);
+    fxr.init(ny * nz, nspec);
+  }
+  // BOUNDT, I3 at x-left: impose the inflow state on the U register (DRHS..YRHS
+  // at ISTAL; src/boundt.f:177-200 with BCDTXL, BCUTXL NXLPRM(1)=1, BCYTXL)
+  void boundt() {
+    if (bcxl != BC_I3) return;
+    for (int kc = kstal; kc <= kstol; ++kc)
+      for (int jc = jstal; jc <= jstol; ++jc) {
+        drhs(istal, jc, kc) = rhoin;
+        urhs(istal, jc, kc) = rhoin * uin;
+        vrhs(istal, jc, kc) = rhoin * 0.0;
+        wrhs(istal, jc, kc) = rhoin * 0.0;
+        for (int is = 0; is < nspec; ++is) yrhs[is](istal, jc, kc) = rhoin * yin[is];
+      }
+  }
+  // BOUNTT, I3 at x-left: both registers at ISTAL set to the inflow state, its
+  // error zeroed (src/bountt.f:203-252)
+  void bountt() {
+    if (bcxl != BC_I3) return;
+    for (int kc = kstal; kc <= kstol; ++kc)
+      for (int jc = jstal; jc <= jstol; ++jc) {
+        drhs(istal, jc, kc) = rhoin;
+        urhs(istal, jc, kc) = rhoin * uin;
+        vrhs(istal, jc, kc) = rhoin * 0.0;
+        wrhs(istal, jc, kc) = rhoin * 0.0;
+        drun(istal, jc, kc) = drhs(istal, jc, kc);
+        urun(istal, jc, kc) = urhs(istal, jc, kc);
+        vrun(istal, jc, kc) = vrhs(istal, jc, kc);
+        wrun(istal, jc, kc) = wrhs(istal, jc, kc);
+        derr(istal, jc, kc) = 0.0;
+        uerr(istal, jc, kc) = 0.0;
+        verr(istal, jc, kc) = 0.0;
+        werr(istal, jc, kc) = 0.0;
+        for (int is = 0; is < nspec; ++is) {
+          yrhs[is](istal, jc, kc) = rhoin * yin[is];
+          yrun[is](istal, jc, kc) = yrhs[is](istal, jc, kc);
+          yerr[is](istal, jc, kc) = 0.0;
+        }
+      }
+  }
+  // BOUNDS: wave amplitudes and their corrections of the boundary-plane RHS.
+  void bounds() {
+    const double bet_global = 0.050;
+    auto prelim = [&](Face& F, std::vector<double>& gam1, std::vector<double>& ovgm, std::vector<double>& acou,
+                      std::vector<double>& ova2, std::vector<double>& tt1, std::vector<double>& tt5) {
+      const int m = ny * nz;
+      for (int is = 0; is < nspec; ++is)
+        for (int q = 0; q < m; ++q)
+          F.h[is * m + q] = F.h[is * m + q] - F.g[q] * F.t[q] * ch.rgspec[is] / F.r[q];
+      for (int q = 0; q < m; ++q) {
+        gam1[q] = F.g[q] - F.r[q];
+        F.e[q] = F.e[q] - gam1[q] * F.t[q];
+        gam1[q] = F.r[q] / gam1[q];
+        ovgm[q] = 1.0 / gam1[q];
+      }
+      for (int q = 0; q < m; ++q) {
+        const double fornow = F.g[q] * gam1[q] * F.t[q];
+        acou[q] = std::sqrt(fornow);
+        ova2[q] = 1.0 / fornow;
+        // TT1 = T51B + T52B (gamma-1+1) - rho c T2B ; TT5 the same with +
+        tt1[q] = F.t51b[q] + F.t52b[q] * (gam1[q] + 1.0) - F.d[q] * acou[q] * F.t2b[q];
+        tt5[q] = F.t51b[q] + F.t52b[q] * (gam1[q] + 1.0) + F.d[q] * acou[q] * F.t2b[q];
+      }
+    };
+    const int m = ny * nz;
+    std::vector<double> gam1(m), ovgm(m), acou(m), ova2(m), tt1(m), tt5(m);
+    if (bcxl == BC_I3) {
+      Face& F = fxl;
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      // inflow velocity and density are constant: DUDT = DVDT = DWDT = DDDT = 0,
+      // DYDT = 0 (BCUTXL NXLPRM(1)=1, BCDTXL, BCYTXL)
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          double fornow = F.d[q] * acou[q] * F.bcl1[q];
+          double bcl1 = 0.5 * (F.u[q] - acou[q]) * (F.bcl5[q] - fornow);
+          double bcl2 = F.u[q] * (F.bcl2[q] - F.bcl5[q] * ova2[q]);
+          double bcl3 = F.u[q] * F.bcl3[q];
+          double bcl4 = F.u[q] * F.bcl4[q];
+          double bcl5 = 0.5 * (F.u[q] + acou[q]) * (F.bcl5[q] + fornow);
+          fornow = bcl1 - F.d[q] * acou[q] * 0.0;
+          bcl2 = -0.0 - ova2[q] * (bcl1 + fornow) - bcl2;
+          bcl3 = -0.0 - bcl3;
+          bcl4 = -0.0 - bcl4;
+          bcl5 = fornow - bcl5;
+          double& er = erhs(istal, jc, kc);
+          er = er - bcl2 * F.e[q] - bcl3 * F.d[q] * F.v[q] - bcl4 * F.d[q] * F.w[q] -
+               bcl5 * (ova2[q] * F.e[q] + F.u[q] / acou[q] + ovgm[q]);
+        }
+      for (int is = 0; is < nspec; ++is)
+        for (int kc = kstal; kc <= kstol; ++kc)
+          for (int jc = jstal; jc <= jstol; ++jc) {
+            const int q = fj(jc, kc), qs = is * m + q;
+            const double bcly = F.rate[qs] / F.d[q] - 0.0 - F.u[q] * F.bcly[qs];
+            erhs(istal, jc, kc) = erhs(istal, jc, kc) - bcly * F.d[q] * F.h[qs];
+          }
+    }
+    if (bcxr == BC_O1) {
+      Face& F = fxr;
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      std::vector<double> sorp(m, 0.0), b1(m), b2(m), b3(m), b4(m);
+      for (int is = 0; is < nspec; ++is)
+        for (int q = 0; q < m; ++q) sorp[q] = sorp[q] + F.h[is * m + q] * F.rate[is * m + q];
+      for (int q = 0; q < m; ++q) sorp[q] = -sorp[q] * gam1[q];
+      for (int q = 0; q < m; ++q) {
+        double bet = bet_global;
+        b2[q] = F.u[q] * (F.bcl2[q] - ova2[q] * F.bcl5[q]);
+        b3[q] = F.u[q] * F.bcl3[q];
+        b4[q] = F.u[q] * F.bcl4[q];
+        b1[q] = 0.5 * (F.u[q] - acou[q]) * (F.bcl5[q] - F.d[q] * acou[q] * F.bcl1[q]);
+        if (betloc_xr == 1) {
+          bet = F.u[q] * F.u[q] + F.v[q] * F.v[q] + F.w[q] * F.w[q];
+          bet = std::sqrt(bet) / acou[q];
+        }
+        if (F.u[q] < 0.0 && pio_xr == 1) {
+          b2[q] = -ova2[q] * sorp[q] - b2[q];
+          b3[q] = (double)0.1f * (F.v[q] - 0.0) - b3[q];
+          b4[q] = (double)0.1f * (F.w[q] - 0.0) - b4[q];
+          b1[q] = 0.5 * sorp[q] + cobcxr * acou[q] * (F.p[q] - pinfxr) + 0.5 * (1.0 - bet) * tt1[q] - b1[q] -
+                  100.0 * F.d[q] * (1.0 / cf.xgdlen) * (std::pow(acou[q], 2.0) - std::pow(F.u[q], 2.0)) *
+                      (F.u[q] - 0.0);
+        } else {
+          b1[q] = 0.5 * sorp[q] + cobcxr * acou[q] * (F.p[q] - pinfxr) + 0.5 * (1.0 - bet) * tt1[q] - b1[q];
+        }
+      }
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          const int ic = istol;
+          if (F.u[q] < 0.0 && pio_xr == 1) {
+            drhs(ic, jc, kc) = drhs(ic, jc, kc) - b1[q] * ova2[q] - b2[q];
+            urhs(ic, jc, kc) = urhs(ic, jc, kc) - b1[q] * ova2[q] * (F.u[q] - acou[q]) - b2[q] * F.u[q];
+            vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - b1[q] * ova2[q] * F.v[q] - b2[q] * F.v[q] - b3[q] * F.d[q];
+            wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - b1[q] * ova2[q] * F.w[q] - b2[q] * F.w[q] - b4[q] * F.d[q];
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - b1[q] * (ova2[q] * F.e[q] - F.u[q] / acou[q] + ovgm[q]) -
+                               b2[q] * F.e[q] - b3[q] * F.d[q] * F.v[q] - b4[q] * F.d[q] * F.w[q];
+          } else {
+            drhs(ic, jc, kc) = drhs(ic, jc, kc) - b1[q] * ova2[q];
+            urhs(ic, jc, kc) = urhs(ic, jc, kc) - b1[q] * ova2[q] * (F.u[q] - acou[q]);
+            vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - b1[q] * ova2[q] * F.v[q];
+            wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - b1[q] * ova2[q] * F.w[q];
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - b1[q] * (ova2[q] * F.e[q] - F.u[q] / acou[q] + ovgm[q]);
+          }
+        }
+      for (int is = 0; is < nspec; ++is)
+        for (int kc = kstal; kc <= kstol; ++kc)
+          for (int jc = jstal; jc <= jstol; ++jc) {
+            const int q = fj(jc, kc), qs = is * m + q;
+            double& yr = yrhs[is](istol, jc, kc);
+            if (F.u[q] < 0.0 && pio_xr == 1) {
+              const double fornow = F.bcly[qs] * F.d[q];
+              erhs(istol, jc, kc) = erhs(istol, jc, kc) - fornow * F.h[qs];
+              yr = yr - (b2[q] + b1[q] * ova2[q]) * F.y[qs] - fornow;
+            } else {
+              yr = yr - b1[q] * ova2[q] * F.y[qs];
+            }
+          }
+    }
+  }
 
   // ---- periodic halo copy: src/parfer.f:840-873, src/cxhalo.f:49-72 ----
   void halo_periodic(Field& f) {
@@ -620,9 +891,17 @@ struct Oracle {
   // ---- RHSCAL: src/rhscal.f (branches used by the periodic cases) ----
   void rhscal() {
     temper();
+    // rhscal.f:70-90: cp_mix and R_mix on the faces
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) {
+      F.g[q] = transp(ic, jc, kc);
+      F.r[q] = store7(ic, jc, kc) / drhs(ic, jc, kc);
+    });
     dfbydx(urhs, store1); dfbydy(vrhs, store2); dfbydz(wrhs, store3);
     STD3 divm(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc);
+    // rhscal.f:159-180: transverse mass-flux divergence
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.t1b[q] = -(store2(ic, jc, kc) + store3(ic, jc, kc)); });
     TRG3 erhs(ic, jc, kc) = erhs(ic, jc, kc) / drhs(ic, jc, kc);
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.e[q] = erhs(ic, jc, kc); });  // rhscal.f:257-275
     STD3 store4(ic, jc, kc) = erhs(ic, jc, kc) * divm(ic, jc, kc);
     BIG3 store7(ic, jc, kc) = erhs(ic, jc, kc) * urhs(ic, jc, kc);
     dfbydx(store7, store1);
@@ -636,6 +915,7 @@ struct Oracle {
                                      store2(ic, jc, kc) * vrhs(ic, jc, kc) + store3(ic, jc, kc) * wrhs(ic, jc, kc));
     // heat flux
     dfbydx(trun, store1); dfbydy(trun, store2); dfbydz(trun, store3);
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.t[q] = trun(ic, jc, kc); });  // rhscal.f:438-456
     BIG3 {
       double fornow = ch.alamda * std::exp(RLAMDA * std::log(trun(ic, jc, kc)));
       store7(ic, jc, kc) = fornow * transp(ic, jc, kc);
@@ -676,6 +956,9 @@ struct Oracle {
     // species
     chrate();
     STD3 for (int is = 0; is < nspec; ++is) rrte[is](ic, jc, kc) = rate[is](ic, jc, kc);
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) {  // rhscal.f:841-862
+      for (int is = 0; is < nspec; ++is) F.rate[fs(is, jc, kc)] = rate[is](ic, jc, kc);
+    });
     STD3 { ucor(ic, jc, kc) = 0.0; vcor(ic, jc, kc) = 0.0; wcor(ic, jc, kc) = 0.0; vtmp(ic, jc, kc) = 0.0; }
     BIG3 wtmp(ic, jc, kc) = 0.0;
     for (int is = 0; is < nspec; ++is) {
@@ -695,6 +978,13 @@ struct Oracle {
       STD3 rt(ic, jc, kc) = rt(ic, jc, kc) - 0.5 * (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc));
       BIG3 store7(ic, jc, kc) = y(ic, jc, kc);
       dfbydx(store7, store1); dfbydy(store7, store2); dfbydz(store7, store3);
+      face_pts([&](Face& F, int ic, int jc, int kc, int q) {  // rhscal.f:1140-1180
+        const int qs = fs(is - 1, jc, kc);
+        F.y[qs] = y(ic, jc, kc);
+        F.bcly[qs] = store1(ic, jc, kc);
+        F.t6b[qs] = -store2(ic, jc, kc) * vrhs(ic, jc, kc) / drhs(ic, jc, kc) -
+                    store3(ic, jc, kc) * wrhs(ic, jc, kc) / drhs(ic, jc, kc);
+      });
       STD3 rt(ic, jc, kc) = rt(ic, jc, kc) - 0.5 * (store1(ic, jc, kc) * urhs(ic, jc, kc) +
                                                     store2(ic, jc, kc) * vrhs(ic, jc, kc) +
                                                     store3(ic, jc, kc) * wrhs(ic, jc, kc));
@@ -740,6 +1030,7 @@ struct Oracle {
           wtmp(ic, jc, kc) = wtmp(ic, jc, kc) + utmp(ic, jc, kc) * y(ic, jc, kc);
         }
       }
+      face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.h[fs(is - 1, jc, kc)] = utmp(ic, jc, kc); });
       dfbydx(store7, store4); dfbydy(store7, store5); dfbydz(store7, store6);
       zx(fxldif, fxrdif, store4); zy(fyldif, fyrdif, store5); zz(fzldif, fzrdif, store6);
       STD3 {
@@ -817,6 +1108,13 @@ struct Oracle {
       STD3 y(ic, jc, kc) = rt(ic, jc, kc) - y(ic, jc, kc) * vtmp(ic, jc, kc) - store1(ic, jc, kc) * ucor(ic, jc, kc) -
                            store2(ic, jc, kc) * vcor(ic, jc, kc) - store3(ic, jc, kc) * wcor(ic, jc, kc);
     }
+    if (fxlcnv || fxrcnv) {  // rhscal.f:3966-3990: density and its x-gradient
+      dfbydx(drhs, store1);
+      face_pts([&](Face& F, int ic, int jc, int kc, int q) {
+        F.d[q] = drhs(ic, jc, kc);
+        F.bcl2[q] = store1(ic, jc, kc);
+      });
+    }
   }
 
   // ---- RHSVEL: src/rhsvel.f:48-2318 ----
@@ -826,8 +1124,24 @@ struct Oracle {
       vtmp(ic, jc, kc) = vrhs(ic, jc, kc) / drhs(ic, jc, kc);
       wtmp(ic, jc, kc) = wrhs(ic, jc, kc) / drhs(ic, jc, kc);
     }
-    // (the 18 boundary-only transverse derivatives of rhsvel.f:66-335 feed
-    //  only NSCBC face arrays and are not needed for periodic boxes)
+    // rhsvel.f:62-200: velocities and transverse convection terms on the faces
+    if (fxlcnv || fxrcnv) {
+      dfbydy(utmp, store1); dfbydz(utmp, store2);
+      face_pts([&](Face& F, int ic, int jc, int kc, int q) {
+        F.u[q] = utmp(ic, jc, kc);
+        F.v[q] = vtmp(ic, jc, kc);
+        F.w[q] = wtmp(ic, jc, kc);
+        F.t2b[q] = -vtmp(ic, jc, kc) * store1(ic, jc, kc) - wtmp(ic, jc, kc) * store2(ic, jc, kc);
+      });
+      dfbydy(vtmp, store1); dfbydz(vtmp, store2);
+      face_pts([&](Face& F, int ic, int jc, int kc, int q) {
+        F.t3b[q] = -vtmp(ic, jc, kc) * store1(ic, jc, kc) - wtmp(ic, jc, kc) * store2(ic, jc, kc);
+      });
+      dfbydy(wtmp, store1); dfbydz(wtmp, store2);
+      face_pts([&](Face& F, int ic, int jc, int kc, int q) {
+        F.t4b[q] = -vtmp(ic, jc, kc) * store1(ic, jc, kc) - wtmp(ic, jc, kc) * store2(ic, jc, kc);
+      });
+    }
     BIG3 store7(ic, jc, kc) = urhs(ic, jc, kc) * utmp(ic, jc, kc);
     dfbydx(store7, store4);
     BIG3 store7(ic, jc, kc) = urhs(ic, jc, kc) * vtmp(ic, jc, kc);
@@ -849,6 +1163,7 @@ struct Oracle {
     dfbydz(store7, store1);
     STD3 store6(ic, jc, kc) = store6(ic, jc, kc) + store1(ic, jc, kc);
     dfbydx(utmp, store1); dfbydy(vtmp, store2); dfbydz(wtmp, store3);
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.bcl1[q] = store1(ic, jc, kc); });  // rhsvel.f:558-570
     STD3 store7(ic, jc, kc) = store4(ic, jc, kc) + utmp(ic, jc, kc) * divm(ic, jc, kc);
     STD3 store4(ic, jc, kc) = urhs(ic, jc, kc) * store1(ic, jc, kc);
     STD3 urhs(ic, jc, kc) = -0.5 * (store4(ic, jc, kc) + store7(ic, jc, kc));
@@ -861,6 +1176,14 @@ struct Oracle {
     double prefer = prun(1, 1, 1);
     BIG3 store7(ic, jc, kc) = prun(ic, jc, kc) - prefer;
     dfbydx(store7, store4); dfbydy(store7, store5); dfbydz(store7, store6);
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) {  // rhsvel.f:764-800
+      F.p[q] = prun(ic, jc, kc);
+      F.bcl5[q] = store4(ic, jc, kc);
+      F.t3b[q] = F.t3b[q] - store5(ic, jc, kc) / drhs(ic, jc, kc);
+      F.t4b[q] = F.t4b[q] - store6(ic, jc, kc) / drhs(ic, jc, kc);
+      F.t51b[q] = -vtmp(ic, jc, kc) * store5(ic, jc, kc) - wtmp(ic, jc, kc) * store6(ic, jc, kc);
+      F.t52b[q] = -prun(ic, jc, kc) * (store2(ic, jc, kc) + store3(ic, jc, kc));
+    });
     STD3 {
       urhs(ic, jc, kc) = urhs(ic, jc, kc) - store4(ic, jc, kc);
       vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - store5(ic, jc, kc);
@@ -910,6 +1233,7 @@ struct Oracle {
     dfbydy(utmp, store1);
     STD3 urhs(ic, jc, kc) = urhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * vtmp(ic, jc, kc) * store1(ic, jc, kc);
     dfbydx(vtmp, store2);
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.bcl3[q] = store2(ic, jc, kc); });  // rhsvel.f:1310-1325
     STD3 vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * utmp(ic, jc, kc) * store2(ic, jc, kc);
     STD3 store7(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc);
     d2fdxy(utmp, store1); d2fdxy(vtmp, store2);
@@ -935,6 +1259,7 @@ struct Oracle {
     dfbydz(utmp, store1);
     STD3 urhs(ic, jc, kc) = urhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * wtmp(ic, jc, kc) * store1(ic, jc, kc);
     dfbydx(wtmp, store2);
+    face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.bcl4[q] = store2(ic, jc, kc); });  // rhsvel.f:1630-1650
     STD3 wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - 0.5 * drhs(ic, jc, kc) * utmp(ic, jc, kc) * store2(ic, jc, kc);
     STD3 store7(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc);
     d2fdxz(utmp, store1); d2fdxz(wtmp, store2);
@@ -1024,8 +1349,9 @@ struct Oracle {
   }
 
   // ---- LINCOM / FINCOM: src/lincom.f:53-169, src/fincom.f:54-168 ----
-  void rkupdate(Field& run, Field& rhs, Field& err, int irk, bool last) {
-    STD3 {
+  void rkupdate(Field& run, Field& rhs, Field& err, int irk, bool last, int ista = 1) {
+#pragma omp parallel for schedule(static)
+    for (int kc = kstal; kc <= kstol; ++kc) for (int jc = jstal; jc <= jstol; ++jc) for (int ic = ista; ic <= istol; ++ic) {
       err(ic, jc, kc) = err(ic, jc, kc) + rkerr[irk - 1] * rhs(ic, jc, kc);
       if (!last) {
         double f = run(ic, jc, kc);
@@ -1038,12 +1364,14 @@ struct Oracle {
     }
   }
   void lincom(int irk, bool last) {
-    rkupdate(drun, drhs, derr, irk, last);
-    rkupdate(urun, urhs, uerr, irk, last);
-    rkupdate(vrun, vrhs, verr, irk, last);
-    rkupdate(wrun, wrhs, werr, irk, last);
-    rkupdate(erun, erhs, eerr, irk, last);
-    for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last);
+    // per-field ranges ISTALD..ISTALY (src/bcinit.f: the I3 inflow plane is
+    // imposed, not integrated, for D, U, V, W, Y)
+    rkupdate(drun, drhs, derr, irk, last, istald);
+    rkupdate(urun, urhs, uerr, irk, last, istalu);
+    rkupdate(vrun, vrhs, verr, irk, last, istalv);
+    rkupdate(wrun, wrhs, werr, irk, last, istalw);
+    rkupdate(erun, erhs, eerr, irk, last, istale);
+    for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last, istaly);
   }
 
   // ---- explicit filter: src/flinit.f:42-…, src/filtrx.f:56-295 (+y, z),
@@ -1207,9 +1535,12 @@ struct Oracle {
   // step switch asks for adaptive steps, src/dtinit.f:174-175).
   void step() {
     for (int irk = 1; irk <= 5; ++irk) {
+      boundt();
       rhs();
+      bounds();
       lincom(irk, irk == 5);
     }
+    bountt();
     if (fladpt) adaptt();
   }
 };
@@ -1326,7 +1657,9 @@ int oracle_step(void* h, int nsteps) {
 int oracle_rhs(void* h, double* rhs_out, double* t_out, double* p_out) {
   try {
     auto* o = static_cast<orc::Oracle*>(h);
+    o->boundt();
     o->rhs();
+    o->bounds();
     const size_t n = (size_t)o->nx * o->ny * o->nz;
     std::vector<orc::Field*> rf = {&o->drhs, &o->urhs, &o->vrhs, &o->wrhs, &o->erhs};
     for (int s = 0; s < o->nspec; ++s) rf.push_back(&o->yrhs[s]);
@@ -1338,6 +1671,25 @@ int oracle_rhs(void* h, double* rhs_out, double* t_out, double* p_out) {
           if (t_out) t_out[q] = o->trun(i, j, k);
           if (p_out) p_out[q] = o->prun(i, j, k);
         }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// NSCBC x faces (I3 inflow at x-left, O1 outflow at x-right; 0 = none).
+struct oracle_bc {
+  int xl, xr;
+  double u_in, rho_in;
+  double y_in[9];
+  double p_inf, sigma, eta;
+  int pio, bet_local;
+};
+int oracle_set_bc(void* h, const oracle_bc* b) {
+  try {
+    static_cast<orc::Oracle*>(h)->set_bc(b->xl, b->xr, b->u_in, b->rho_in, b->y_in, b->p_inf, b->sigma, b->eta, b->pio,
+                                         b->bet_local);
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

@@ -192,6 +192,15 @@ def make_case(name, n=None, seed=1234, scale_n=None):
                   l=1.5 mm (the integral scale of the 128^3 flame case).
     ensemble    : one box of the batched ensemble (sizes from {32,48,64,96},
                   seeded u' in U[0.5,3] m/s, peak T in U[1400,2000] K), 1-step.
+    flame_inout : 128^3, 10 mm, H2/air mixture-averaged; NSCBC I3 inflow at
+                  x-left (u = 1.25 m/s, v = w = 0, unburnt density and
+                  composition) and O1 outflow at x-right (p_inf = 1e5 Pa,
+                  sigma = 0.287, eta = 1e-3); y, z periodic. A planar lean
+                  (Y_H2 = 0.0116) premixed flame: tanh progress profile of
+                  thickness 0.5 mm at x = 3 mm from 300 K to 1350 K, burnt
+                  composition of complete H2 -> H2O conversion; mean flow
+                  1.25 m/s plus Passot-Pouquet turbulence u' = 2 m/s,
+                  l = 1.5 mm. The result carries "bc" for the face setup.
     `n` overrides the grid extent (cubic) for smaller test instances.
     """
     from senga import Chem  # noqa: local import keeps this module numpy-only
@@ -227,6 +236,38 @@ def make_case(name, n=None, seed=1234, scale_n=None):
         Y[0], Y[1], Y[8] = yv[0], yv[1], yv[2]
         u, v, w = passot_pouquet(shp, lengths, 4.0, 1.5e-3, seed)
         p = np.full(shp, 101325.0)
+    elif name == "flame_inout":
+        nn = n or 128
+        shape_xyz = (nn, nn, nn)
+        L = 1.0e-2
+        lengths = (L, L, L)
+        chem_path, diff_path = CHEM_H2, DIFF_H2
+        chem = Chem(chem_path)
+        shp = (nn, nn, nn)
+        wm = chem.table("wmolar")
+        yu = np.zeros(9)
+        yu[0], yu[1], yu[8] = 1.1606960e-2, 2.30295282e-1, 7.58097758e-1  # input/cont.dat defaults
+        yb = yu.copy()
+        nh2 = yu[0] / wm[0]
+        yb[0] = 0.0
+        yb[1] = yu[1] - 0.5 * nh2 * wm[1]
+        yb[2] = nh2 * wm[2]
+        x = np.arange(nn) * (L / (nn - 1))
+        prog = 0.5 * (1.0 + np.tanh((x - 3.0e-3) / 0.5e-3))
+        prog3 = np.broadcast_to(prog, shp)
+        T = 300.0 + (1350.0 - 300.0) * prog3
+        Y = np.array([yu[k] + (yb[k] - yu[k]) * prog3 for k in range(9)])
+        u, v, w = passot_pouquet(shp, lengths, 2.0, 1.5e-3, seed)
+        u = u + 1.25
+        p = np.full(shp, 1.0e5)
+        fields, itn = conserved(chem, p, T, u, v, w, Y)
+        rg = chem.table("rgspec")
+        rho_in = 1.0e5 / (300.0 * float(sum(rg[k] * yu[k] for k in range(9))))
+        bc = dict(xl=13, xr=21, u_in=1.25, rho_in=rho_in, y_in=tuple(float(v_) for v_ in yu), p_inf=1.0e5,
+                  sigma=0.287, eta=1.0e-3, pio=0, bet_local=0)
+        dt = stable_dt(chem, fields, T, lengths, shp)
+        return dict(name=name, shape=shape_xyz, lengths=lengths, chem=chem_path, diff=diff_path, fields=fields, T=T,
+                    itn=itn, dt=dt, nend=(1, 1, NPERI, NPERI, NPERI, NPERI), bc=bc)
     elif name == "ensemble":
         sizes = (32, 48, 64, 96)
         shape_xyz = tuple(int(rng.choice(sizes)) for _ in range(3)) if n is None else (n, n, n)

@@ -348,6 +348,10 @@ __device__ __forceinline__ void thermo_point(const Geo& g, const Fields& f, cons
   f.t[q] = T;
   f.itn[q] = itn;
   f.p[q] = p;
+  if (f.cp) {  // NSCBC face data (cp_mix, rho R_mix of TEMPER)
+    f.cp[q] = cpm;
+    f.rmix[q] = rmix;
+  }
 
   // ---- primitive variables ----
   double y[NS];
@@ -411,9 +415,12 @@ template <class M>
 struct ThermoOcc {
   static constexpr int blocks = 1;
 };
+#ifndef SENGA_THERMO_H2_MINB
+#define SENGA_THERMO_H2_MINB 2
+#endif
 template <>
 struct ThermoOcc<gen::Mech_h2> {
-  static constexpr int blocks = 2;
+  static constexpr int blocks = SENGA_THERMO_H2_MINB;
 };
 
 template <class M>

@@ -95,9 +95,11 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
-      rE[z] = rE[z] + (d1<0, P>(g, t, bL) * d1<0, P>(g, t, bT) + d1<1, P>(g, t, bL) * d1<1, P>(g, t, bT) +
+      // FxxCON: the x conduction terms vanish on the face plane (rhscal.f:582,774)
+      const bool con = !P && (face_bits(g, t.gx) & BF_CON);
+      rE[z] = rE[z] + ((con ? 0.0 : d1<0, P>(g, t, bL) * d1<0, P>(g, t, bT)) + d1<1, P>(g, t, bL) * d1<1, P>(g, t, bT) +
                        d1<2, P>(g, t, bL) * d1<2, P>(g, t, bT));
-      rE[z] = rE[z] + (d2<0, P>(g, t, bT) + d2<1, P>(g, t, bT) + d2<2, P>(g, t, bT)) * bL.v(t.x, t.y, t.z);
+      rE[z] = rE[z] + ((con ? 0.0 : d2<0, P>(g, t, bT)) + d2<1, P>(g, t, bT) + d2<2, P>(g, t, bT)) * bL.v(t.x, t.y, t.z);
     }
     __syncthreads();
   }
@@ -173,8 +175,11 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     uz[z] = d1<2, P>(g, t, bX);
     const double uq = bX.v(t.x, t.y, t.z);
     const double vq = __ldg(f.vel + n + t.q), wq = __ldg(f.vel + 2 * n + t.q);
+    // x-face viscous flags (rhsvel.f: FxxVSN normal, FxxVST shear terms zeroed on the plane)
+    const int bf = P ? 0 : face_bits(g, t.gx);
+    const double vsn = (bf & BF_VSN) ? 0.0 : 1.0, vst = (bf & BF_VST) ? 0.0 : 1.0;
     rU[z] = rU[z] + -0.5 * (__ldg(U + n + t.q) * ux[z] + (S4[z] + uq * divm[z]));
-    double fn = mu * kFthd * d2<0, P>(g, t, bX);
+    double fn = vsn * (mu * kFthd * d2<0, P>(g, t, bX));
     rU[z] += fn;
     rE[z] = rE[z] + fn * uq;
     fn = mu * d2<1, P>(g, t, bX);
@@ -183,17 +188,17 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     fn = mu * d2<2, P>(g, t, bX);
     rU[z] += fn;
     rE[z] = rE[z] + uq * fn;
-    const double uxy = dm<0, 1>(g, t, bX), uxz = dm<0, 2>(g, t, bX);
+    const double uxy = dm<0, 1, P>(g, t, bX), uxz = dm<0, 2, P>(g, t, bX);
     fn = kTthd * mu * uxy;
     rV[z] -= fn;
     rE[z] = rE[z] - vq * fn;
-    fn = mu * uxy;
+    fn = vst * (mu * uxy);
     rV[z] += fn;
     rE[z] = rE[z] + vq * fn;
     fn = kTthd * mu * uxz;
     rW[z] -= fn;
     rE[z] = rE[z] - wq * fn;
-    fn = mu * uxz;
+    fn = vst * (mu * uxz);
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
   }
@@ -210,18 +215,20 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     vz[z] = d1<2, P>(g, t, bX);
     const double vq = bX.v(t.x, t.y, t.z);
     const double uq = __ldg(f.vel + t.q), wq = __ldg(f.vel + 2 * n + t.q);
+    const int bf = P ? 0 : face_bits(g, t.gx);
+    const double vsn = (bf & BF_VSN) ? 0.0 : 1.0, vst = (bf & BF_VST) ? 0.0 : 1.0;
     rV[z] = rV[z] + -0.5 * (__ldg(U + 2 * n + t.q) * vy[z] + (S5[z] + vq * divm[z]));
     double fn = mu * kFthd * d2<1, P>(g, t, bX);
     rV[z] += fn;
     rE[z] = rE[z] + fn * vq;
-    fn = mu * d2<0, P>(g, t, bX);
+    fn = vst * (mu * d2<0, P>(g, t, bX));
     rV[z] += fn;
     rE[z] = rE[z] + vq * fn;
     fn = mu * d2<2, P>(g, t, bX);
     rV[z] += fn;
     rE[z] = rE[z] + vq * fn;
-    const double vxy = dm<0, 1>(g, t, bX), vyz = dm<1, 2>(g, t, bX);
-    fn = kTthd * mu * vxy;
+    const double vxy = dm<0, 1, P>(g, t, bX), vyz = dm<1, 2, P>(g, t, bX);
+    fn = vsn * (kTthd * mu * vxy);
     rU[z] -= fn;
     rE[z] = rE[z] - uq * fn;
     fn = mu * vxy;
@@ -247,18 +254,20 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     const double wq = bX.v(t.x, t.y, t.z);
     const double uq = __ldg(f.vel + t.q), vq = __ldg(f.vel + n + t.q);
     const double rho = __ldg(U + t.q);
+    const int bf = P ? 0 : face_bits(g, t.gx);
+    const double vsn = (bf & BF_VSN) ? 0.0 : 1.0, vst = (bf & BF_VST) ? 0.0 : 1.0;
     rW[z] = rW[z] + -0.5 * (__ldg(U + 3 * n + t.q) * wz + (S6[z] + wq * divm[z]));
     double fn = mu * kFthd * d2<2, P>(g, t, bX);
     rW[z] += fn;
     rE[z] = rE[z] + fn * wq;
-    fn = mu * d2<0, P>(g, t, bX);
+    fn = vst * (mu * d2<0, P>(g, t, bX));
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
     fn = mu * d2<1, P>(g, t, bX);
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
-    const double wxz = dm<0, 2>(g, t, bX), wyz = dm<1, 2>(g, t, bX);
-    fn = kTthd * mu * wxz;
+    const double wxz = dm<0, 2, P>(g, t, bX), wyz = dm<1, 2, P>(g, t, bX);
+    fn = vsn * (kTthd * mu * wxz);
     rU[z] -= fn;
     rE[z] = rE[z] - uq * fn;
     fn = mu * wxz;
@@ -275,7 +284,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     // normal stresses with viscosity gradients (TAUxx b,e,f)
     double t6 = kFthd * ux[z] - kTthd * (vy[z] + wz);
     rE[z] = rE[z] + mu * t6 * ux[z];
-    t6 = t6 * mux[z];
+    t6 = vsn * (t6 * mux[z]);
     rU[z] += t6;
     rE[z] = rE[z] + uq * t6;
     t6 = kFthd * vy[z] - kTthd * (ux[z] + wz);
@@ -295,7 +304,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     fn = s7 * muy[z];
     rU[z] += fn;
     rE[z] = rE[z] + uq * fn;
-    fn = s7 * mux[z];
+    fn = vst * (s7 * mux[z]);
     rV[z] += fn;
     rE[z] = rE[z] + vq * fn;
     rE[z] = rE[z] + mu * s7 * s7;
@@ -306,7 +315,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     fn = s7 * muz[z];
     rU[z] += fn;
     rE[z] = rE[z] + uq * fn;
-    fn = s7 * mux[z];
+    fn = vst * (s7 * mux[z]);
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
     rE[z] = rE[z] + mu * s7 * s7;
@@ -377,7 +386,9 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         yz[z] = d1z<P>(g, t, cy);
         r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * rw.c[z + H]);
         rate[z] = r;
-        fn3[z] = d2<0, P>(g, t, bS) + d2<1, P>(g, t, bS) + d2z<P>(g, t, cy);  // Laplacian for now
+        // FxxDIF/FxxADB zero the x diffusive terms on the face plane (rhscal.f:1581-1955)
+        const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
+        fn3[z] = (dif ? 0.0 : d2<0, P>(g, t, bS)) + d2<1, P>(g, t, bS) + d2z<P>(g, t, cy);  // Laplacian for now
       }
       __syncthreads();
     }
@@ -394,7 +405,9 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         vcx[z] = vcx[z] + rd[z] * yx[z];
         vcy[z] = vcy[z] + rd[z] * yy[z];
         vcz[z] = vcz[z] + rd[z] * yz[z];
-        const double fn = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1z<P>(g, t, cd) * yz[z];
+        const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
+        const double fn = (dif ? 0.0 : d1<0, P>(g, t, bS) * yx[z]) + d1<1, P>(g, t, bS) * yy[z] +
+                          d1z<P>(g, t, cd) * yz[z];
         rate[z] = rate[z] + fn;
         vt[z] = vt[z] + fn;
         fn1[z] = fn;
@@ -416,7 +429,9 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         const TP& t = tp[z];
         const double hk = ch.c[z + H];
         rE[z] = rE[z] + fn1[z] * hk;
-        const double fn2 = d1<0, P>(g, t, bS) * yx[z] + d1<1, P>(g, t, bS) * yy[z] + d1z<P>(g, t, ch) * yz[z];
+        const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
+        const double fn2 = (dif ? 0.0 : d1<0, P>(g, t, bS) * yx[z]) + d1<1, P>(g, t, bS) * yy[z] +
+                           d1z<P>(g, t, ch) * yz[z];
         rE[z] = rE[z] + fn2 * rd[z];
         rE[z] = rE[z] + fn3[z] * hk;
         if (t.valid) f.wdot[s * n + t.q] = rate[z];
@@ -448,12 +463,22 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
   for (int z = 0; z < SZ_; ++z) tp[z] = make_tp(g, o, tx, ty, z);
   const int64_t n = g.n;
   const SSlab bS{sm};
-  auto advance = [&](int fld, int64_t q, double R) {
+  const int nc = 5 + nspec;
+  // bf: x-face bits of the point; NSCBC planes add the BOUNDS correction
+  // (precomputed per face point) and an I3 inflow plane integrates only E
+  // (src/bcinit.f ranges ISTALD..ISTALY start at ISTAP1)
+  auto advance = [&](int fld, const TP& t, int bf, double R) {
+    const int64_t q = t.q;
     const int64_t idx = (int64_t)fld * n + q;
+    if (!P && (bf & BF_NSCBC)) {
+      const int side = t.gx == 0 ? 0 : 1;
+      R = R + f.face[((int64_t)side * nc + fld) * ((int64_t)g.ny * g.nz) + t.gy + (int64_t)g.ny * t.gz];
+    }
     if (rk.last < 0) {  // right-hand side only
       f.rhs[idx] = R;
       return;
     }
+    if (!P && (bf & BF_IMPOSED) && fld != 4) return;
     if (f.err) f.err[idx] = f.err[idx] + rk.err * R;
     if (!rk.last) {
       const double s = f.run[idx];
@@ -483,11 +508,15 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
       if (!t.valid) continue;
-      const double rE = f.rhs[4 * n + t.q] - cm.c[z + H] * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
-                        d1<1, P>(g, t, bS) * vcy[z] - d1z<P>(g, t, cm) * vcz[z];
+      const int bf = P ? 0 : face_bits(g, t.gx);
+      // FxxDIF/FxxADB: x gradient term and VTMP vanish on the face (rhscal.f:3782-3839)
+      const bool dif = bf & BF_DIF;
+      const double rE = f.rhs[4 * n + t.q] - cm.c[z + H] * (dif ? 0.0 : vt[z]) -
+                        (dif ? 0.0 : d1<0, P>(g, t, bS) * vcx[z]) - d1<1, P>(g, t, bS) * vcy[z] -
+                        d1z<P>(g, t, cm) * vcz[z];
 #pragma unroll
-      for (int fl = 0; fl < 4; ++fl) advance(fl, t.q, f.rhs[fl * n + t.q]);
-      advance(4, t.q, rE);
+      for (int fl = 0; fl < 4; ++fl) advance(fl, t, bf, f.rhs[fl * n + t.q]);
+      advance(4, t, bf, rE);
     }
   }
   for (int s = 0; s < nspec; ++s) {
@@ -500,28 +529,41 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
       if (!t.valid) continue;
-      const double R = f.wdot[s * n + t.q] - cy.c[z + H] * vt[z] - d1<0, P>(g, t, bS) * vcx[z] -
+      const int bf = P ? 0 : face_bits(g, t.gx);
+      const bool dif = bf & BF_DIF;  // rhscal.f:3919: x gradient of Y zeroed on the face
+      const double R = f.wdot[s * n + t.q] - cy.c[z + H] * vt[z] - (dif ? 0.0 : d1<0, P>(g, t, bS) * vcx[z]) -
                        d1<1, P>(g, t, bS) * vcy[z] - d1z<P>(g, t, cy) * vcz[z];
-      advance(5 + s, t.q, R);
+      advance(5 + s, t, bf, R);
     }
   }
 }
 
+// Resident CTAs per SM asked of the compiler (register cap 65536/(256*n)).
+#ifndef SENGA_FLOW_MINB
+#define SENGA_FLOW_MINB 2
+#endif
+#ifndef SENGA_SPEC_MINB
+#define SENGA_SPEC_MINB 2
+#endif
+#ifndef SENGA_SPECRK_MINB
+#define SENGA_SPECRK_MINB 3
+#endif
+
 // ---- single-box launches: one CTA per tile ----
 template <bool P>
-__global__ void __launch_bounds__(FX* FY, 2) k_flow_t(Geo g, Fields f) {
+__global__ void __launch_bounds__(FX* FY, SENGA_FLOW_MINB) k_flow_t(Geo g, Fields f) {
   extern __shared__ double sm[];
   __shared__ Folds<FX, FY, FZ> fo;
   flow_tile<P>(g, f, Origin{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ}, sm, fo);
 }
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, 2) k_species_t(Geo g, Fields f, int nspec) {
+__global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB) k_species_t(Geo g, Fields f, int nspec) {
   extern __shared__ double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
   species_tile<P>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm, fo);
 }
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
+__global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
   extern __shared__ double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
   species_rk_tile<P>(g, f, nspec, rk, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_},

@@ -70,6 +70,10 @@ struct senga_ctx {
   double tstep = 0.0, errold = 1.0e-4, errldr = 1.0e-4, errmax = 0.0;
   int inderr = 0, sms = 148;
   unsigned long long* d_errmax = nullptr;
+  // NSCBC x faces (senga_set_nscbc)
+  bool nscbc = false;
+  NscbcParams bc{};
+  double* nscbc_pool = nullptr;
 };
 
 namespace {
@@ -100,8 +104,8 @@ void check_config(const senga_config& c, int nspec) {
       throw Error(SENGA_ERR_ARG, "grid extent must be at least 6 points per periodic and 12 per bounded direction");
     if ((l == SENGA_NPERI) != (r == SENGA_NPERI))
       throw Error(SENGA_ERR_ARG, "periodic end conditions must be set on both faces of a direction");
-    if (l != SENGA_NPERI)
-      throw Error(SENGA_ERR_UNSUPPORTED, "non-periodic boxes need the NSCBC face kernels (not built)");
+    if (l != SENGA_NPERI && (d != 0 || l != SENGA_NBOUND || r != SENGA_NBOUND))
+      throw Error(SENGA_ERR_UNSUPPORTED, "bounded boxes: only x may be bounded (NBOUND on both x faces)");
   }
   if (c.tstep <= 0.0) throw Error(SENGA_ERR_ARG, "tstep must be positive");
   if (nspec < 1 || nspec > SENGA_NSPCMX) throw Error(SENGA_ERR_ARG, "nspec out of range");
@@ -116,7 +120,11 @@ void set_rk(senga_ctx* c, double tstep) {
 }
 
 void run_rhs(senga_ctx* c) {
+  if (!c->geo.per[0] && !c->nscbc)
+    throw Error(SENGA_ERR_UNSUPPORTED, "a bounded x direction needs its face conditions (senga_set_nscbc)");
+  if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->stream);  // BOUNDT
   launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+  if (c->nscbc) launch_face(c->geo, c->f, c->bc, c->nspec, c->d_chem, c->stream);  // face data + BOUNDS
   launch_flow(c->geo, c->f, c->nspec, c->stream);
   launch_species_a(c->geo, c->f, c->nspec, c->stream);
 }
@@ -273,6 +281,7 @@ int senga_ctx_destroy(senga_ctx* c) {
   cudaFree(c->d_diff);
   cudaFree(c->d_status);
   cudaFree(c->d_errmax);
+  cudaFree(c->nscbc_pool);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SENGA_OK;
@@ -322,6 +331,7 @@ int senga_step(senga_ctx* c, int nsteps) {
   return guard([&] {
     for (int s = 0; s < nsteps; ++s) {
       for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
+      if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->stream);  // BOUNTT
       if (c->cfg.adaptive) adaptt(c);
     }
     CK(cudaGetLastError());
@@ -336,6 +346,7 @@ int senga_step_graph(senga_ctx* c, int nsteps) {
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
+      if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->stream);  // BOUNTT
       CK(cudaStreamEndCapture(c->stream, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       CK(cudaGraphDestroy(gr));
@@ -439,6 +450,48 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
     launch_deriv(c->geo, kind, din, dout, c->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
+  if (!c || !b) return fail(SENGA_ERR_ARG, "senga_set_nscbc: null argument");
+  if ((b->xl != 0 && b->xl != 13) || (b->xr != 0 && b->xr != 21))
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I3 (13) at x-left and O1 (21) at x-right");
+  if (c->geo.per[0] || b->xl == 0 || b->xr == 0)
+    return fail(SENGA_ERR_ARG, "senga_set_nscbc: needs a bounded x direction and a kind on both x faces");
+  if (b->rho_in <= 0.0 || b->p_inf <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: rho_in and p_inf must be > 0");
+  return guard([&] {
+    NscbcParams& p = c->bc;
+    p = NscbcParams{};
+    p.xl = b->xl;
+    p.xr = b->xr;
+    p.u_in = b->u_in;
+    p.rho_in = b->rho_in;
+    for (int s = 0; s < c->nspec; ++s) p.y_in[s] = b->y_in[s];
+    p.p_inf = b->p_inf;
+    p.cobc = b->sigma * (1.0 - b->eta) / (2.0 * c->cfg.xgdlen);  // COBCXR, src/bcinit.f
+    p.bet = 0.050;                                               // BET default, src/bounds.f:103
+    p.xlen = c->cfg.xgdlen;
+    p.pio = b->pio;
+    p.betloc = b->bet_local;
+    // face-plane flags of src/bcinit.f: I3 -> FXLCNV, FXLVSN, inflow ranges;
+    // O1 -> FXRCNV, FXRVST, FXRCON, FXRADB, FXRDIF
+    c->geo.bxl = BF_VSN | BF_NSCBC | BF_IMPOSED;
+    c->geo.bxr = BF_VST | BF_CON | BF_DIF | BF_NSCBC;
+    if (!c->nscbc_pool) {
+      const int64_t n = c->geo.n, nyz = (int64_t)c->geo.ny * c->geo.nz;
+      CK(cudaMalloc(&c->nscbc_pool, (size_t)(2 * n + 2 * c->nc * nyz) * sizeof(double)));
+      CK(cudaMemsetAsync(c->nscbc_pool, 0, (size_t)(2 * n + 2 * c->nc * nyz) * sizeof(double), c->stream));
+      c->f.cp = c->nscbc_pool;
+      c->f.rmix = c->nscbc_pool + n;
+      c->f.face = c->nscbc_pool + 2 * n;
+    }
+    c->nscbc = true;
+    if (c->graph) {
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
     CK(cudaStreamSynchronize(c->stream));
   });
 }

@@ -29,7 +29,23 @@ struct Geo {
   int per[3];           // 1 = periodic, 0 = bounded (one-sided closures)
   double ovd[3];        // 1/Delta   (OVDELX..)
   double ovd2[3];       // 1/Delta^2 (OVDLX2..)
+  int bxl, bxr;         // x-face treatment bits (BF_*), 0 for periodic x
 };
+
+// Boundary-plane treatment of a bounded x face (src/bcinit.f:287-600 flags):
+// which flux derivatives are zeroed on the face plane inside the RHS, and
+// whether the NSCBC correction and the imposed-inflow update apply there.
+enum : int {
+  BF_VSN = 1,       // FxxVSN: normal viscous stress terms (TAUxx,x)
+  BF_VST = 2,       // FxxVST: shear viscous stress terms
+  BF_CON = 4,       // FxxCON: heat conduction
+  BF_DIF = 8,       // FxxDIF and FxxADB: species diffusion and its enthalpy flux
+  BF_NSCBC = 16,    // BOUNDS corrections are added to the plane's RHS
+  BF_IMPOSED = 32,  // I3 inflow: D, U, V, W, Y are imposed, not integrated
+};
+__host__ __device__ __forceinline__ int face_bits(const Geo& g, int gx) {
+  return gx == 0 ? g.bxl : (gx == g.nx - 1 ? g.bxr : 0);
+}
 
 // Device pointers of one box's registers and per-substage scratch.
 struct Fields {
@@ -56,6 +72,10 @@ struct Fields {
   double* vc;     // diffusion correction velocity [3][n] (UCOR,VCOR,WCOR)
   double* vtmp;   // divergence of correction flux (VTMP)
   unsigned int* status;  // device status word
+  // NSCBC boxes only (nullptr otherwise)
+  double* cp;     // cp_mix after TEMPER (STRGxx source)
+  double* rmix;   // rho R_mix after TEMPER (STORE7)
+  double* face;   // per-face RHS corrections of BOUNDS [2][nc][ny*nz]
 };
 
 struct RK {
@@ -109,6 +129,20 @@ void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchu
 // work item; `phase` selects one of them (0, 1, 2) or all three (-1).
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
+// NSCBC x faces (nscbc.cu): face kinds 0 (none), 13 (I3 inflow, x-left),
+// 21 (O1 outflow, x-right) and their parameters.
+struct NscbcParams {
+  int xl, xr;
+  double u_in, rho_in, y_in[SENGA_NSPCMX];  // I3: RXLPRM(1), DRIN, YRIN
+  double p_inf, cobc, bet, xlen;            // O1: PINFXR, COBCXR, BET, XGDLEN
+  int pio, betloc;                          // O1: NXRPRM(1), NXRPRM(2)
+};
+// BOUNDT (both = false) or BOUNTT (both = true: U and S registers, error zeroed)
+void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both, cudaStream_t s);
+// face data + BOUNDS corrections into f.face, after the thermochemistry kernel
+void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,
+                 cudaStream_t s);
+
 // ADAPTT error maxima (adapt.cu): out[fl] = max |err|/(|run| + nrm.v[fl])
 // as the bit pattern of a non-negative double, per conserved field.
 struct ErrNorms {

@@ -69,6 +69,9 @@ __device__ __forceinline__ int64_t woff(const Geo& g, int c, int m) {
 template <class V>
 __device__ __forceinline__ double d1core(const V& v, int c, int n, int per) {
   using namespace fdc;
+  // points past the end of a partial tile (never stored) evaluate as the
+  // last point, so a closure never reaches outside the staged halo
+  if (!per && c > n - 1) c = n - 1;
   if (per || (c >= 5 && c <= n - 6))
     return a1 * (v(1) - v(-1)) + b1 * (v(2) - v(-2)) + c1 * (v(3) - v(-3)) + d1 * (v(4) - v(-4)) +
            e1 * (v(5) - v(-5));
@@ -95,6 +98,7 @@ __device__ __forceinline__ double d1core(const V& v, int c, int n, int per) {
 template <class V>
 __device__ __forceinline__ double d2core(const V& v, int c, int n, int per) {
   using namespace fdc;
+  if (!per && c > n - 1) c = n - 1;  // see d1core
   if (per || (c >= 5 && c <= n - 6)) {
     const double f0 = v(0);
     return a2 * ((v(1) - f0) - (f0 - v(-1))) + b2 * ((v(2) - f0) - (f0 - v(-2))) +
@@ -134,6 +138,44 @@ __device__ __forceinline__ double dmcore(const V2& v) {
   return ax * fa + bx * fb + cx * fc + dx * fd + ex * fe;
 }
 
+// Mixed derivative with a bounded first direction and a periodic second one
+// (src/d2fdxy.f:151-392, d2fdxz.f likewise): on the first two points the
+// one-sided first-derivative rows act on a 4th-order centred difference in
+// the second direction (ACOFY1, BCOFY1); points 3-5 from each end use the
+// diagonal 4th/6th/8th-order schemes (ACF3XY..DCF5XY); the rest the
+// 10th-order interior scheme. c is the point's coordinate along the bounded
+// direction, n its extent; v(ma, mb) as for dmcore.
+namespace fdc {
+constexpr double my1 = (4.0 / 3.0) / 2.0, my2 = (-1.0 / 3.0) / 4.0;
+constexpr double m3a = (4.0 / 3.0) / 4.0, m3b = (-1.0 / 3.0) / 4.0 / 4.0;
+constexpr double m4a = (3.0 / 2.0) / 4.0, m4b = (-3.0 / 5.0) / 4.0 / 4.0, m4c = (1.0 / 1.0e1) / 4.0 / 9.0;
+constexpr double m5a = (8.0 / 5.0) / 4.0, m5b = (-4.0 / 5.0) / 4.0 / 4.0, m5c = (8.0 / 3.5e1) / 4.0 / 9.0,
+                 m5d = (-1.0 / 3.5e1) / 4.0 / 1.6e1;
+}  // namespace fdc
+template <class V2>
+__device__ __forceinline__ double dmcore_b(const V2& v, int c, int n) {
+  using namespace fdc;
+  if (c > n - 1) c = n - 1;  // see d1core
+  if (c >= 5 && c <= n - 6) return dmcore(v);
+  auto dg = [&](int m) { return v(m, m) - v(m, -m) - v(-m, m) + v(-m, -m); };
+  auto g2 = [&](int a, int a0) {  // absolute indices along the bounded direction
+    const int da = a - c, d0 = a0 - c;
+    return my1 * (v(da, 1) - v(da, -1) - v(d0, 1) + v(d0, -1)) + my2 * (v(da, 2) - v(da, -2) - v(d0, 2) + v(d0, -2));
+  };
+  const int L = n - 1;
+  const int e = c < 5 ? c : L - c;  // distance from the nearer end
+  switch (e) {
+    case 2: return m3a * dg(1) + m3b * dg(2);
+    case 3: return m4a * dg(1) + m4b * dg(2) + m4c * dg(3);
+    case 4: return m5a * dg(1) + m5b * dg(2) + m5c * dg(3) + m5d * dg(4);
+    default: break;
+  }
+  if (c == 0) return p1a * g2(1, 0) + p1b * g2(2, 0) + p1c * g2(3, 0) + p1d * g2(4, 0);
+  if (c == 1) return p2a * g2(0, 1) + p2b * g2(2, 1) + p2c * g2(3, 1) + p2d * g2(4, 1);
+  if (c == L) return p1a * g2(L, L - 1) + p1b * g2(L, L - 2) + p1c * g2(L, L - 3) + p1d * g2(L, L - 4);
+  return p2a * g2(L - 1, L) + p2b * g2(L - 1, L - 2) + p2c * g2(L - 1, L - 3) + p2d * g2(L - 1, L - 4);
+}
+
 // ---- global-memory forms (operator-level entry points) ----------------------
 // Periodic directions wrap the index; bounded ones never leave the domain
 // because the closures only read inward.
@@ -153,6 +195,7 @@ template <int DA, int DB, class F>
 __device__ __forceinline__ double DM(const Geo& g, const Pt& p, const F& f) {
   const int ca = crd<DA>(p), cb = crd<DB>(p);
   auto v = [&](int ma, int mb) { return f(p.q + woff<DA>(g, ca, ma) + woff<DB>(g, cb, mb)); };
+  if (!g.per[DA]) return dmcore_b(v, ca, ext<DA>(g)) * g.ovd[DA] * g.ovd[DB];
   return dmcore(v) * g.ovd[DA] * g.ovd[DB];
 }
 

@@ -294,7 +294,7 @@ __device__ __forceinline__ double d2(const Geo& g, const TP& t, const B& b) {
   if (DIR == 1) return d2core([&](int m) { return b.v(t.x, t.y + m, t.z); }, t.gy, g.ny, P ? 1 : g.per[1]) * g.ovd2[1];
   return d2core([&](int m) { return b.v(t.x, t.y, t.z + m); }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd2[2];
 }
-template <int DA, int DB, class B>
+template <int DA, int DB, bool P, class B>
 __device__ __forceinline__ double dm(const Geo& g, const TP& t, const B& b) {
   auto v = [&](int ma, int mb) {
     const int dx = (DA == 0 ? ma : 0) + (DB == 0 ? mb : 0);
@@ -302,6 +302,11 @@ __device__ __forceinline__ double dm(const Geo& g, const TP& t, const B& b) {
     const int dz = (DA == 2 ? ma : 0) + (DB == 2 ? mb : 0);
     return b.v(t.x + dx, t.y + dy, t.z + dz);
   };
+  if (!P && !g.per[DA]) {
+    const int c = DA == 0 ? t.gx : DA == 1 ? t.gy : t.gz;
+    const int n = DA == 0 ? g.nx : DA == 1 ? g.ny : g.nz;
+    return dmcore_b(v, c, n) * g.ovd[DA] * g.ovd[DB];
+  }
   return dmcore(v) * g.ovd[DA] * g.ovd[DB];
 }
 

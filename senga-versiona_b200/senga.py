@@ -92,6 +92,14 @@ class ConfigT(C.Structure):
     ]
 
 
+class NscbcT(C.Structure):
+    """senga_nscbc: I3 inflow (x-left) / O1 outflow (x-right) parameters."""
+
+    _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
+                ("y_in", C.c_double * NSPCMX), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
+                ("pio", C.c_int), ("bet_local", C.c_int)]
+
+
 class SengaError(RuntimeError):
     pass
 
@@ -122,6 +130,7 @@ def _load():
         "senga_fp64_peak": (ip, [ip, dp]),
         "senga_filter": (ip, [vp, ip]),
         "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
+        "senga_set_nscbc": (ip, [vp, C.POINTER(NscbcT)]),
         "senga_filter_field_host": (ip, [vp, ip, dp, dp]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
@@ -314,6 +323,18 @@ class Box:
         out = np.empty_like(a)
         _check(lib.senga_deriv_host(self.h, kind, _dp(a), _dp(out)), "senga_deriv_host")
         return out
+
+    def set_nscbc(self, bc):
+        """NSCBC x faces from a dict (xl=13, xr=21, u_in, rho_in, y_in, p_inf,
+        sigma, eta, pio, bet_local)."""
+        b = NscbcT()
+        b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
+        b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
+        for i, v in enumerate(bc.get("y_in", ())):
+            b.y_in[i] = v
+        b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
+        b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
+        _check(lib.senga_set_nscbc(self.h, C.byref(b)), "senga_set_nscbc")
 
     def tstep(self):
         """(TSTEP, last ERRMAX, INDERR) of the adaptive controller."""

@@ -389,3 +389,95 @@ def test_adaptt_pid_controller_first_steps():
                         + (0.1 / 3) * math.log(1e-4 / 1e-4))
     r2 = min(1.01, max(0.01, r2))
     assert math.isclose(t2, t1 * r2, rel_tol=1e-13)
+
+
+# ------------------------------------------------------------ bounded x: mixed closures, NSCBC
+@pytest.mark.parametrize("plane", [0, 1])
+def test_mixed_closures_on_x_linear_fields(plane):
+    """d2fdxy/d2fdxz with x bounded (src/d2fdxy.f:151-392): for f = x sin(theta s)
+    (s = y or z, periodic) the first two rows from each x end give the
+    4th-order centred s-derivative (ACOFY1, BCOFY1), rows 3-5 the diagonal
+    4th/6th/8th-order schemes, the rest the 10th-order interior one."""
+    nend = (1, 1, 2, 2, 2, 2)
+    o = _oracle(SHAPE, LEN, nend=nend)
+    nx, ny, nz = SHAPE
+    a2 = 1 + plane
+    ns = SHAPE[a2]
+    dx = LEN[0] / (nx - 1)
+    ds = LEN[a2] / (ns - 1)
+    th = 2 * np.pi * 2 / ns
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    s = (y, z)[plane]
+    f = x * dx * np.sin(th * s)
+    got = o.deriv(6 + plane, f)
+    my = (_fd("ACOFY1"), _fd("BCOFY1"))
+    four = (2 * my[0] * math.sin(th) + 2 * my[1] * math.sin(2 * th)) / ds
+    rows = {2: ("ACF3XY", "BCF3XY"), 3: ("ACF4XY", "BCF4XY", "CCF4XY"), 4: ("ACF5XY", "BCF5XY", "CCF5XY", "DCF5XY")}
+    inner = ("ACOFXY", "BCOFXY", "CCOFXY", "DCOFXY", "ECOFXY")
+
+    def diag(names):
+        return sum(_fd(nm) * 4 * (m + 1) * math.sin((m + 1) * th) for m, nm in enumerate(names)) / ds
+
+    for i in range(nx):
+        e = min(i, nx - 1 - i)
+        k = four if e < 2 else diag(rows[e]) if e < 5 else diag(inner)
+        want = k * np.cos(th * s[..., i])
+        assert rel_linf(got[..., i], want) <= 1e-11, (i, e)
+
+
+def _uniform_inflow_state(c, p=1.0e5, n=16):
+    import senga
+
+    chem = senga.Chem(c["chem"])
+    shp = (n, n, n)
+    bc = c["bc"]
+    T = np.full(shp, 300.0)
+    Y = np.array([np.full(shp, y) for y in bc["y_in"]])
+    u = np.full(shp, bc["u_in"])
+    z = np.zeros(shp)
+    import cases
+
+    f, itn = cases.conserved(chem, np.full(shp, p), T, u, z, z, Y)
+    return f, T, itn
+
+
+def test_nscbc_uniform_inflow_state_is_steady():
+    """I3 inflow + O1 outflow box holding the inflow state at p = p_inf: every
+    wave amplitude vanishes and the state does not move."""
+    import cases
+
+    c = cases.make_case("flame_inout", n=16, seed=5)
+    f, T, itn = _uniform_inflow_state(c)
+    o = _oracle(c["shape"], c["lengths"], chem=c["chem"], diff=c["diff"], dt=c["dt"], nend=c["nend"])
+    o.set_bc(c["bc"])
+    o.upload(f, T, itn)
+    o.step(3)
+    g, _, _ = o.download()
+    for k in range(5):
+        assert rel_linf(g[k], f[k]) <= 1e-12, k
+    assert float(np.max(np.abs(g[5:] - f[5:]))) <= 1e-12
+
+
+def test_nscbc_outflow_relaxes_pressure_and_inflow_is_imposed():
+    """p above p_inf: the O1 plane loses mass (dRHO/dt < 0 there, sigma > 0);
+    after steps the I3 plane still holds rho_in, rho_in u_in and rho_in Y_in."""
+    import cases
+
+    c = cases.make_case("flame_inout", n=16, seed=5)
+    f, T, itn = _uniform_inflow_state(c, p=1.02e5)
+    o = _oracle(c["shape"], c["lengths"], chem=c["chem"], diff=c["diff"], dt=c["dt"], nend=c["nend"])
+    o.set_bc(c["bc"])
+    o.upload(f, T, itn)
+    r, _, _ = o.rhs()
+    assert float(np.max(r[0][..., -1])) < 0.0
+    # away from both faces (the imposed inflow density differs from the box's
+    # near x = 0) the uniform state has no mass flux divergence
+    assert float(np.max(np.abs(r[0][..., 6:-1]))) <= 1e-9 * float(np.max(np.abs(r[0][..., -1])))
+    o.upload(f, T, itn)
+    o.step(2)
+    g, _, _ = o.download()
+    bc = c["bc"]
+    assert np.all(g[0][..., 0] == bc["rho_in"])
+    assert np.all(g[1][..., 0] == bc["rho_in"] * bc["u_in"])
+    for s_ in range(9):
+        assert np.all(g[5 + s_][..., 0] == bc["rho_in"] * bc["y_in"][s_])
