@@ -146,9 +146,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="grid extent (cubic); 256 is the named workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="h2_kernels", choices=["h2_kernels", "ensemble", "serve"],
+    ap.add_argument("--workload", default="h2_kernels", choices=["h2_kernels", "ensemble", "serve", "flame"],
                     help="h2_kernels: the 256^3 headline; ensemble: 64 batched boxes vs one at a time; "
-                         "serve: Poisson request stream through the serving loop")
+                         "serve: Poisson request stream through the serving loop; "
+                         "flame: 128^3 NSCBC inflow/outflow flame, filter every 10 steps")
     ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests")
     ap.add_argument("--boxes", type=int, default=64, help="ensemble: number of boxes")
     args = ap.parse_args()
@@ -338,6 +339,16 @@ def workload_main(args):
                            "points": r["points"], "autotune": r["autotune"]},
                 "sequential_value": r["sequential_gpsu_s"], "batched_vs_sequential": r["speedup"],
                 "status_word": r["status_word"]}
+    elif args.workload == "flame":
+        steps = args.steps if args.steps != 5 else 20
+        r = workloads.run_flame(steps=steps, warmup=max(3, args.warmup))
+        line = {"metric": "grid-point substage updates/s", "value": r["gpsu_s"], "unit": "GPSU/s", "n_gpus": 1,
+                "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": 1e3 * r["seconds"] / steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": "flame_inout_128^3_H2_nscbc_I3_O1", "filter": "every 10 steps, coded TWFACT "
+                           "sign, U register only", "points": r["points"]},
+                "finite": r["finite"], "T_range": [r["t_min"], r["t_max"]], "status_word": r["status_word"]}
     else:
         r = workloads.run_serve(nreq=args.requests)
         line = {"metric": "grid-point substage updates/s", "value": r["served_gpsu_s"], "unit": "GPSU/s",
