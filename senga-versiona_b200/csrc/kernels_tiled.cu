@@ -55,7 +55,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
                                           Folds<FX, FY, FZ>& fo) {
   const int tx = threadIdx.x % FX, ty = threadIdx.x / FX;
   fo.init(g, o);
-  __syncthreads();
+  tile_sync();
   TP tp[FZ];
 #pragma unroll
   for (int z = 0; z < FZ; ++z) tp[z] = make_tp(g, o, tx, ty, z);
@@ -73,7 +73,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     brv.stage<FNW>(fo, Ld{U + 2 * n});
     brw.stage<FNW>(fo, Ld{U + 3 * n});
     bE.stage<FNW>(fo, Ld{f.e});
-    __syncthreads();
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
@@ -84,14 +84,14 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
       rE[z] = -0.5 * (s4 + d1<0, P>(g, t, bE) * bru.v(t.x, t.y, t.z) + d1<1, P>(g, t, bE) * brv.v(t.x, t.y, t.z) +
                       d1<2, P>(g, t, bE) * brw.v(t.x, t.y, t.z));
     }
-    __syncthreads();
+    tile_sync();
   }
   // ---- phase 2: heat conduction ----
   {
     const FStar bT{sm}, bL{sm + FStar::SIZE};
     bT.stage<FNW>(fo, Ld{f.t});
     bL.stage<FNW>(fo, Ld{f.lam});
-    __syncthreads();
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
@@ -101,13 +101,13 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
                        d1<2, P>(g, t, bL) * d1<2, P>(g, t, bT));
       rE[z] = rE[z] + ((con ? 0.0 : d2<0, P>(g, t, bT)) + d2<1, P>(g, t, bT) + d2<2, P>(g, t, bT)) * bL.v(t.x, t.y, t.z);
     }
-    __syncthreads();
+    tile_sync();
   }
   // ---- phase 3: pressure gradient (of p - p(1,1,1)) and pressure work ----
   {
     const FStar bP{sm};
     bP.stage<FNW>(fo, LdSub{f.p, __ldg(f.p)});
-    __syncthreads();
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
@@ -117,7 +117,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
       rW[z] = -pz;
       rE[z] = rE[z] - __ldg(f.vel + t.q) * px - __ldg(f.vel + n + t.q) * py - __ldg(f.vel + 2 * n + t.q) * pz;
     }
-    __syncthreads();
+    tile_sync();
   }
   // ---- phase 4: momentum fluxes d/dx_j (rho u_i u_j) ----
   double S4[FZ], S5[FZ], S6[FZ];
@@ -127,7 +127,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     bA.stage<FNW>(fo, LdMul{U + n, f.vel});
     bB.stage<FNW>(fo, LdMul{U + n, f.vel + n});
     bC.stage<FNW>(fo, LdMul{U + n, f.vel + 2 * n});
-    __syncthreads();
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
@@ -135,7 +135,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
       S5[z] = d1<0, P>(g, t, bB);
       S6[z] = d1<0, P>(g, t, bC);
     }
-    __syncthreads();
+    tile_sync();
   }
   {
     const FYRow bA{sm};
@@ -144,7 +144,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     bA.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + n});
     bB.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + 2 * n});
     bC.stage<FNW>(fo, LdMul{U + 3 * n, f.vel + 2 * n});
-    __syncthreads();
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
@@ -153,7 +153,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
       S6[z] = S6[z] + d1<1, P>(g, t, bB);
       S6[z] = S6[z] + d1<2, P>(g, t, bC);
     }
-    __syncthreads();
+    tile_sync();
   }
   // ---- phase 5: velocity derivatives, viscous stresses and work ----
   const FStar bM{sm};
@@ -162,7 +162,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
   double mux[FZ], muy[FZ], muz[FZ], ux[FZ], uy[FZ], uz[FZ], vx[FZ], vy[FZ], vz[FZ];
   // 5a: u
   bX.stage<FNW>(fo, Ld{f.vel});
-  __syncthreads();
+  tile_sync();
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
     const TP& t = tp[z];
@@ -202,10 +202,10 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
   }
-  __syncthreads();
+  tile_sync();
   // 5b: v
   bX.stage<FNW>(fo, Ld{f.vel + n});
-  __syncthreads();
+  tile_sync();
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
     const TP& t = tp[z];
@@ -241,10 +241,10 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
   }
-  __syncthreads();
+  tile_sync();
   // 5c: w, then the first-derivative products
   bX.stage<FNW>(fo, Ld{f.vel + 2 * n});
-  __syncthreads();
+  tile_sync();
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
     const TP& t = tp[z];
@@ -346,7 +346,7 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
                                              Folds<SX_, SY_, SZ_>& fo) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
   fo.init(g, o);
-  __syncthreads();
+  tile_sync();
   TP tp[SZ_];
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) tp[z] = make_tp(g, o, tx, ty, z);
@@ -373,7 +373,7 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       SCol cy;
       cy.load(fo, tx, ty, Ld{f.y + s * n});
       bS.stage<SNW>(fo, Ld{f.y + s * n});
-      __syncthreads();
+      tile_sync();
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -390,14 +390,14 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
         fn3[z] = (dif ? 0.0 : d2<0, P>(g, t, bS)) + d2<1, P>(g, t, bS) + d2z<P>(g, t, cy);  // Laplacian for now
       }
-      __syncthreads();
+      tile_sync();
     }
     // rho D_k: correction velocity, diffusive flux divergence
     {
       SCol cd;
       cd.load(fo, tx, ty, Ld{f.rd + s * n});
       bS.stage<SNW>(fo, Ld{f.rd + s * n});
-      __syncthreads();
+      tile_sync();
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -416,14 +416,14 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         vt[z] = vt[z] + f3;
         fn3[z] = f3;
       }
-      __syncthreads();
+      tile_sync();
     }
     // h_k: enthalpy fluxes of the energy equation
     {
       SCol ch;
       ch.load(fo, tx, ty, Ld{f.h + s * n});
       bS.stage<SNW>(fo, Ld{f.h + s * n});
-      __syncthreads();
+      tile_sync();
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -436,7 +436,7 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         rE[z] = rE[z] + fn3[z] * hk;
         if (t.valid) f.wdot[s * n + t.q] = rate[z];
       }
-      __syncthreads();
+      tile_sync();
     }
   }
 #pragma unroll
@@ -457,7 +457,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
                                                 const Origin o, double* sm, Folds<SX_, SY_, SZ_>& fo) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
   fo.init(g, o);
-  __syncthreads();
+  tile_sync();
   TP tp[SZ_];
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) tp[z] = make_tp(g, o, tx, ty, z);
@@ -503,7 +503,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     SCol cm;
     cm.load(fo, tx, ty, Ld{f.hmix});
     bS.stage<SNW>(fo, Ld{f.hmix});
-    __syncthreads();
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
@@ -520,11 +520,11 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     }
   }
   for (int s = 0; s < nspec; ++s) {
-    __syncthreads();
+    tile_sync();
     SCol cy;
     cy.load(fo, tx, ty, Ld{f.y + s * n});
     bS.stage<SNW>(fo, Ld{f.y + s * n});
-    __syncthreads();
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];

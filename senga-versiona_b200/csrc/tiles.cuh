@@ -59,6 +59,27 @@ struct Folds {
 // rowyz(r, y, z, d) gives y, z and the destination row d. Warps take rows,
 // lanes take x; rows are processed four at a time so that every thread keeps
 // several global loads in flight before it writes shared memory.
+// Asynchronous global -> shared copies (cp.async, 8 bytes each): a plain
+// field (Ld) is staged without passing through registers, every row of a
+// buffer in flight at once; tile_sync() waits for the copies of this thread
+// and then for the block.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void tile_sync() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+}
+template <class F>
+struct PlainLoad {
+  static constexpr bool value = false;
+};
+template <>
+struct PlainLoad<Ld> {
+  static constexpr bool value = true;
+};
+
 template <int XL, int XLO, int NR, int NW, class FO, class RowYZ, class F>
 __device__ __forceinline__ void stage_rows(double* dst, int DS, const FO& fo, const RowYZ& rowyz, const F& f) {
   constexpr int NK = (XL + 31) / 32;
@@ -68,6 +89,22 @@ __device__ __forceinline__ void stage_rows(double* dst, int DS, const FO& fo, co
   int64_t gx[NK];
 #pragma unroll
   for (int k = 0; k < NK; ++k) gx[k] = (lane + 32 * k < XL) ? fo.ox[XLO + H + lane + 32 * k] : 0;
+  if constexpr (PlainLoad<F>::value) {
+#pragma unroll 2
+    for (int i = 0; i < ITER; ++i) {
+      const int r = warp + i * NW;
+      if (r < NR) {
+        int y, z, d;
+        rowyz(r, y, z, d);
+        const int64_t base = fo.oy[y + H] + fo.oz[z + H];
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (lane + 32 * k < XL) cp_async8(dst + d * DS + lane + 32 * k, f.a + base + gx[k]);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    return;
+  }
 #pragma unroll 1
   for (int i0 = 0; i0 < ITER; i0 += UB) {
     double val[UB][NK];
