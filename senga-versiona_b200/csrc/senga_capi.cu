@@ -381,7 +381,7 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
     for (int irk = 1; irk <= 5; ++irk) {
       const int b = (irk - 1) * 4;
       CK(cudaEventRecord(ev[b], c->stream));
-      launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+      const int nth = launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
       CK(cudaEventRecord(ev[b + 1], c->stream));
       launch_flow(c->geo, c->f, c->nspec, c->stream);
       CK(cudaEventRecord(ev[b + 2], c->stream));
@@ -390,7 +390,7 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
       RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
       launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
       CK(cudaEventRecord(irk < 5 ? ev[b + 4] : ev[20], c->stream));
-      nl += 4;
+      nl += 3 + nth;
     }
     CK(cudaStreamSynchronize(c->stream));
     for (int irk = 1; irk <= 5; ++irk) {

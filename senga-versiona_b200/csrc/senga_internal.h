@@ -113,8 +113,9 @@ static_assert(sizeof(BoxTable) + 256 <= 32764, "a kernel's parameters are limite
 // tables bit for bit (select_mech). SENGA_MECH=generic in the environment
 // forces the table-driven kernel.
 int select_mech(const senga_chem& chem, const senga_diff& diff);
-void launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const senga_diff* ddiff, int nspec,
-                   int flmavt, int mech, cudaStream_t s);
+// Returns the number of kernels it launched (the long mechanisms run as two).
+int launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const senga_diff* ddiff, int nspec,
+                  int flmavt, int mech, cudaStream_t s);
 void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s);
