@@ -226,13 +226,11 @@ def main():
     torch.cuda.synchronize()
     clocks = clk.stop()
     barrier()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    import replicas
+
+    ms = replicas.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
     status = box.status()
-    gpsu = npts * 5 * args.steps * world / (ms / 1e3)
+    gpsu = replicas.job_rate(npts, 5 * args.steps, world, ms / 1e3)
 
     # end-to-end through the host C ABI: per step, upload the state from pinned
     # host memory, advance one RK step, download the state.
@@ -251,13 +249,9 @@ def main():
         box.upload(pin_f, pin_t, pin_i)
         box.step(1, graph=True)
         f1, t1_, i1 = box.download()
-    t_e = time.perf_counter() - t_e0
-    if world > 1:
-        t = torch.tensor([t_e], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_e = float(t.item())
+    t_e = replicas.max_over_ranks(time.perf_counter() - t_e0, device="cuda")
     state_bytes = nc * npts * 8 + npts * 8 + npts * 4
-    e2e = {"value": npts * 5 * e2e_steps * world / t_e, "unit": unit, "h2d_bytes_per_step": state_bytes,
+    e2e = {"value": replicas.job_rate(npts, 5 * e2e_steps, world, t_e), "unit": unit, "h2d_bytes_per_step": state_bytes,
            "d2h_bytes_per_step": state_bytes,
            "call": "senga_upload_state_host + senga_step_graph(1) + senga_download_state_host per step"}
 
