@@ -347,7 +347,8 @@ def workload_main(args):
         r = workloads.run_serve(nreq=args.requests)
         line = {"metric": "grid-point substage updates/s", "value": r["served_gpsu_s"], "unit": "GPSU/s",
                 "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": f"serve_poisson_{r['requests']}req_20per_s", "arena_bytes": r["arena_bytes"]},
+                "config": {"workload": f"serve_poisson_{r['requests']}req_20per_s", "arena_bytes": r["arena_bytes"],
+                           "max_points_per_tick": r["max_points_per_tick"]},
                 "p50_s": r["p50_s"], "p99_s": r["p99_s"], "mean_latency_s": r["mean_latency_s"], "wall_s": r["wall_s"],
                 "gpsu": r["gpsu"], "sequential_value": r["sequential_gpsu_s"],
                 "served_vs_sequential": r["served_gpsu_s"] / r["sequential_gpsu_s"],

@@ -276,6 +276,12 @@ int senga_server_tick(senga_server* s, int* finished);
 int senga_server_result(senga_server* s, int request_id, double* fields, double* trun, int32_t* itndex,
                         double* times);
 int senga_server_stats(senga_server* s, int* active, int* pending, int64_t* gpsu, int64_t* free_bytes);
+/* Caps the grid points advanced per tick (admission stops once the active
+ * requests hold that many points; a lone request is always admitted). 0
+ * (the default) admits while the arena has room. With a cap, requests run
+ * nearly in arrival order instead of all sharing one long tick, which
+ * lowers the median time to completion under overload. */
+int senga_server_set_max_points(senga_server* s, int64_t max_points);
 
 /* ---- allocation-free right-hand side ----------------------------------------
  * No counterpart in the reference. RHSCAL + RHSVEL of one periodic box, like

@@ -538,6 +538,7 @@ struct senga_server {
   int next_id = 0;
   int64_t gpsu_done = 0;
   double t0 = 0.0;
+  int64_t max_points = 0;  // admission cap on the grid points advanced per tick (0: arena only)
 };
 
 extern "C" {
@@ -557,6 +558,12 @@ int senga_server_create(size_t arena_bytes, const senga_chem* chem, const senga_
     return rc;
   }
   *out = s;
+  return SENGA_OK;
+}
+
+int senga_server_set_max_points(senga_server* s, int64_t max_points) {
+  if (!s || max_points < 0) return fail(SENGA_ERR_ARG, "senga_server_set_max_points: bad argument");
+  s->max_points = max_points;
   return SENGA_OK;
 }
 
@@ -599,9 +606,16 @@ int senga_server_tick(senga_server* s, int* finished) {
   return guard2([&] {
     Ensemble& E = s->ens;
     bool changed = false;
+    int64_t active_points = 0;
+    for (const Member* a : E.active) active_points += a->desc.g.n;
     while (!s->pending.empty()) {
       Member* m = s->pending.front();
+      const int64_t n = (int64_t)m->cfg.nx * m->cfg.ny * m->cfg.nz;
+      // the cap keeps a tick short, so requests run to completion in arrival
+      // order instead of all sharing a slow tick; one request always fits
+      if (s->max_points > 0 && !E.active.empty() && active_points + n > s->max_points) break;
       if (!E.place(*m)) break;  // admission by HBM footprint, first come first served
+      active_points += n;
       E.upload(*m, m->h_fields.data(), m->h_t.data(), m->h_itn.data());
       m->t_admit = now_s() - s->t0;
       E.active.push_back(m);

@@ -131,6 +131,7 @@ def _load():
         "senga_filter": (ip, [vp, ip]),
         "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
         "senga_set_nscbc": (ip, [vp, C.POINTER(NscbcT)]),
+        "senga_server_set_max_points": (ip, [vp, C.c_int64]),
         "senga_filter_field_host": (ip, [vp, ip, dp, dp]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
@@ -462,6 +463,10 @@ class Server:
             self.close()
         except Exception:
             pass
+
+    def set_max_points(self, max_points):
+        """Cap on the grid points advanced per tick (0: arena only)."""
+        _check(lib.senga_server_set_max_points(self.h, int(max_points)), "senga_server_set_max_points")
 
     def submit(self, shape, lengths, tstep, fields, trun, itndex, nsteps):
         cfg = make_config(shape, lengths, tstep)

@@ -152,7 +152,7 @@ def _instance(cache, r):
     return c, f
 
 
-def run_serve(nreq=2000, rate=20.0, seed=2024, device=0, arena_frac=0.6):
+def run_serve(nreq=2000, rate=20.0, seed=2024, device=0, arena_frac=0.6, max_points=32 * 1024 * 1024):
     import torch
 
     reqs = serve_requests(nreq, rate, seed)
@@ -164,6 +164,9 @@ def run_serve(nreq=2000, rate=20.0, seed=2024, device=0, arena_frac=0.6):
     free, _ = torch.cuda.mem_get_info(device)
     arena = int(min(arena_frac * free, 120e9))
     srv = senga.Server(arena, chem, diff, device=device)
+    # about 32 M points per tick (~0.1 s): requests run close to arrival
+    # order instead of all sharing one long tick
+    srv.set_max_points(max_points)
     t0 = time.perf_counter()
     ids = {}
     i = 0
@@ -214,4 +217,4 @@ def run_serve(nreq=2000, rate=20.0, seed=2024, device=0, arena_frac=0.6):
     return {"requests": nreq, "rate_per_s": rate, "wall_s": wall, "gpsu": int(gpsu), "served_gpsu_s": gpsu / wall,
             "busy_gpsu_s": gpsu / max(1e-9, wall - reqs[0]["t"]), "sequential_gpsu_s": gpsu / t_seq,
             "sequential_s": t_seq, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "mean_latency_s": float(lat.mean()), "arena_bytes": arena}
+            "mean_latency_s": float(lat.mean()), "arena_bytes": arena, "max_points_per_tick": max_points}

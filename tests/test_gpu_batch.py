@@ -89,3 +89,35 @@ def test_server_results_equal_alone_and_in_the_mix():
         for k in range(want.shape[0]):
             assert rel_linf(got[k], want[k]) <= TOL, f"request {rid} field {k}"
         assert rel_linf(tg, tw) <= TOL
+
+
+def test_server_point_cap_admits_in_order_and_results_match():
+    """With a per-tick point cap of two small boxes, later requests wait for
+    earlier ones to finish (not for arena room); results equal runs alone."""
+    import senga
+    import cases
+
+    reqs = []
+    for seed, nsteps in ((41, 2), (42, 1), (43, 3), (44, 1)):
+        c = cases.make_case("ensemble", n=16, seed=seed)
+        reqs.append((c, nsteps))
+    chem = senga.Chem(reqs[0][0]["chem"])
+    diff = senga.Diff(None, chem)
+    srv = senga.Server(256 * 1024 * 1024, chem, diff)
+    srv.set_max_points(2 * 16 ** 3)
+    ids = [srv.submit(c["shape"], c["lengths"], c["dt"], c["fields"], c["T"], c["itn"], ns) for c, ns in reqs]
+    done = 0
+    for _ in range(100):
+        done += srv.tick()
+        if done == len(reqs):
+            break
+    assert done == len(reqs)
+    times = [srv.result(rid)[3] for rid in ids]  # [submit, admit, done] each
+    # the third request was admitted only once the second had finished
+    assert times[2][1] >= times[1][2]
+    assert times[3][1] >= times[0][2]
+    for rid, (c, ns) in zip(ids, reqs):
+        got, tg, _, _ = srv.result(rid)
+        want, tw, _ = _alone(c, chem, diff, ns)
+        for k in range(want.shape[0]):
+            assert rel_linf(got[k], want[k]) <= TOL, f"request {rid} field {k}"
