@@ -546,7 +546,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
 #define SENGA_SPEC_MINB 2
 #endif
 #ifndef SENGA_SPECRK_MINB
-#define SENGA_SPECRK_MINB 3
+#define SENGA_SPECRK_MINB 4
 #endif
 
 // ---- single-box launches: one CTA per tile ----
