@@ -236,6 +236,23 @@ int senga_chrate_host(senga_ctx* ctx, double* rate);
 typedef double (*senga_integrand)(double x, void* user);
 int senga_integf(senga_integrand f, void* user, double argmin, double argmax, double* answer);
 
+/* ---- restart dumps ---------------------------------------------------------
+ * The reference's dump file of one rank, written by src/output.f:296-322 and
+ * read back by src/indata.f:1405-1436: NXNODE, NYNODE, NZNODE, NSPEC, then
+ * DRUN, URUN, VRUN, WRUN, ERUN, YRUN (the whole YRUN(..., NSPCMX) array of
+ * COMMON, so nspcmx is the reference build's NSPCMX), then ETIME, TSTEP,
+ * ERROLD, ERRLDR. formatted = 0: one sequential unformatted record (4-byte
+ * length markers, sub-records beyond 2 GB; NDOFMT/NDIFMT = 0); formatted = 1:
+ * list-directed text, one line per point (NDOFMT/NDIFMT = 1).
+ * fields: (5 + nspec) interior arrays, x fastest, field slowest (the layout
+ * of senga_upload_state_host); scalars[4] = ETIME, TSTEP, ERROLD, ERRLDR.
+ * senga_dump_read with fields = NULL only returns dims[4] (nx, ny, nz,
+ * nspec); capacity is the number of doubles fields can hold. */
+int senga_dump_write(const char* path, int formatted, int nx, int ny, int nz, int nspec, int nspcmx,
+                     const double* fields, const double* scalars);
+int senga_dump_read(const char* path, int formatted, int nspcmx, int* dims, double* fields, int64_t capacity,
+                    double* scalars);
+
 /* ---- batched ensembles --------------------------------------------------------
  * No counterpart in the reference (it runs one box per MPI job). Many
  * independent periodic boxes of uneven sizes, one mechanism, each with its own

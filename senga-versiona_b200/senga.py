@@ -132,6 +132,8 @@ def _load():
         "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
         "senga_set_nscbc": (ip, [vp, C.POINTER(NscbcT)]),
         "senga_server_set_max_points": (ip, [vp, C.c_int64]),
+        "senga_dump_write": (ip, [C.c_char_p, ip, ip, ip, ip, ip, ip, dp, dp]),
+        "senga_dump_read": (ip, [C.c_char_p, ip, ip, C.POINTER(C.c_int), dp, C.c_int64, dp]),
         "senga_filter_field_host": (ip, [vp, ip, dp, dp]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
@@ -164,6 +166,32 @@ def _load():
 
 
 lib = _load()
+
+
+def dump_write(path, fields, etime=0.0, tstep=0.0, errold=1.0e-4, errldr=1.0e-4, formatted=False, nspcmx=None):
+    """Write a restart dump in the reference's layout. fields: (5+nspec, nz,
+    ny, nx) conserved state (rho, rho u, rho v, rho w, rho E, rho Y_k)."""
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    nc, nz, ny, nx = f.shape
+    nspec = nc - 5
+    sc = np.array([etime, tstep, errold, errldr], dtype=np.float64)
+    _check(lib.senga_dump_write(os.fsencode(path), 1 if formatted else 0, nx, ny, nz, nspec, nspcmx or nspec,
+                                _dp(f), _dp(sc)), "senga_dump_write")
+
+
+def dump_read(path, formatted=False, nspcmx=None):
+    """Read a restart dump; returns (fields (5+nspec, nz, ny, nx), dict of
+    etime, tstep, errold, errldr). nspcmx: the writing build's NSPCMX
+    (unformatted files store that many species slots; default nspec)."""
+    dims = (C.c_int * 4)()
+    _check(lib.senga_dump_read(os.fsencode(path), 1 if formatted else 0, nspcmx or 99, dims, None, 0, None),
+           "senga_dump_read")
+    nx, ny, nz, nspec = list(dims)
+    f = np.empty((5 + nspec, nz, ny, nx))
+    sc = np.empty(4)
+    _check(lib.senga_dump_read(os.fsencode(path), 1 if formatted else 0, nspcmx or nspec, dims, _dp(f), f.size,
+                               _dp(sc)), "senga_dump_read")
+    return f, dict(etime=sc[0], tstep=sc[1], errold=sc[2], errldr=sc[3])
 
 
 def fp64_peak(device=0):

@@ -167,7 +167,18 @@ def oracle_fixtures():
         print("wrote", key)
 
 
+def casefile_dump():
+    """The reference's formatted restart input of its 1-step case
+    (src/casefiles/1step/dmpi0000000.dat, 1001 x 1 x 1 points, 2 species),
+    copied as a parser fixture."""
+    import shutil
+
+    shutil.copyfile(os.path.join(REF, "casefiles", "1step", "dmpi0000000.dat"),
+                    os.path.join(HERE, "dmpi_1step_1001.dat"))
+
+
 def main():
+    casefile_dump()
     coeffs = {"rk": rk_coefficients(), "fd": fd_coefficients()}
     with open(os.path.join(HERE, "coefficients.json"), "w") as f:
         json.dump(coeffs, f, indent=1, sort_keys=True)

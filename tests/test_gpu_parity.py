@@ -280,3 +280,30 @@ def test_adaptive_steps_match_oracle():
     o, _, _ = ref.download()
     for k in range(o.shape[0]):
         assert rel_linf(g[k], o[k]) <= TOL_STATE, f"field {k}"
+
+
+def test_checkpoint_resume_through_a_restart_dump(tmp_path):
+    """Two steps, dump (reference unformatted layout), resume in a fresh
+    context from the dump, two more steps: equal to four steps in one go.
+    (A dump holds the conserved state only, as the reference's does; the
+    temperature seed is re-sent with the state.)"""
+    import senga
+
+    c = _case("h2_kernels", 16)
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(c["diff"], chem)
+    a = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"])
+    a.upload(c["fields"], c["T"], c["itn"])
+    a.step(2)
+    f2, t2, i2 = a.download()
+    p = str(tmp_path / "dmpi.bin")
+    senga.dump_write(p, f2, etime=2 * c["dt"], tstep=c["dt"], nspcmx=9)
+    a.step(2)
+    fa, _, _ = a.download()
+    g, sc = senga.dump_read(p, nspcmx=9)
+    assert sc["tstep"] == c["dt"]
+    b = senga.Box(c["shape"], c["lengths"], chem, diff, sc["tstep"])
+    b.upload(g, t2, i2)
+    b.step(2)
+    fb, _, _ = b.download()
+    assert np.array_equal(fa, fb)
