@@ -284,10 +284,18 @@ class Box:
         _check(lib.senga_upload_state_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
                "upload")
 
-    def download(self):
-        f = np.empty((self.nc,) + self.shape)
-        t = np.empty(self.shape)
-        it = np.empty(self.shape, dtype=np.int32)
+    def download(self, out=None):
+        """State, T and ITNDEX as host arrays; out=(fields, T, itn) reuses
+        caller arrays (e.g. page-locked ones, for full-speed copies)."""
+        if out is None:
+            f = np.empty((self.nc,) + self.shape)
+            t = np.empty(self.shape)
+            it = np.empty(self.shape, dtype=np.int32)
+        else:
+            f, t, it = out
+            assert f.shape == (self.nc,) + self.shape and f.dtype == np.float64 and f.flags.c_contiguous
+            assert t.shape == self.shape and t.dtype == np.float64 and t.flags.c_contiguous
+            assert it.shape == self.shape and it.dtype == np.int32 and it.flags.c_contiguous
         _check(lib.senga_download_state_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
                "download")
         return f, t, it
