@@ -34,6 +34,7 @@ extern "C" {
 #define SENGA_NBDYMX 10
 #define SENGA_NLLMAX 10
 #define SENGA_NDCFMX 4
+#define SENGA_NCFRMX 6
 
 /* End conditions per face: src/com_senga2.h (NOBC/NBOUND/NPERI) */
 #define SENGA_NOBC 0
@@ -176,6 +177,23 @@ int senga_get_status(senga_ctx* ctx, int* status);
  * wrapped in place of the reference's halo copy. */
 int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
+
+/* Optically thin radiation heat loss, RADCAL (src/radcal.f:45-119), run when
+ * the cont.dat radiation switch is on (src/rhscal.f:810):
+ * ERHS -= 4 STEFBO sum_j a_j(T) rho Y_j R_j T (T^4 - TREFRN^4), with the
+ * Planck-mean absorption polynomials a_j of the radiating species read from
+ * radn.dat by senga_radn_load (RADCIN, src/radcin.f:57-200; species indices
+ * 1-based as in the file) and trefrn the cont.dat reference temperature.
+ * senga_set_radiation(ctx, NULL) turns it off (the default). */
+typedef struct senga_radn {
+  int nsprad;                                   /* radiating species (NSPRAD) */
+  int nsprid[SENGA_NSPCMX];                     /* their species indices, 1-based */
+  int nkprad[SENGA_NSPCMX];                     /* coefficients per polynomial */
+  double akprad[SENGA_NSPCMX][SENGA_NCFRMX];    /* AKPRAD(icoeff, j) as [j][icoeff] */
+  double trefrn;                                /* TREFRN [K] */
+} senga_radn;
+int senga_radn_load(const char* path, const senga_chem* chem, double trefrn, senga_radn* out);
+int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
 
 /* NSCBC x faces (config: bounded x, NBOUND on both x faces; y, z periodic).
  * xl = 13: I3 subsonic inflow at x-left with constant velocity (NXLPRM(1)=1):

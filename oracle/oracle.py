@@ -62,6 +62,7 @@ def _get():
         lib.oracle_chem_scalar.argtypes = [C.c_void_p, C.c_char_p, dp]
         lib.oracle_filter.argtypes = [C.c_void_p, C.c_int]
         lib.oracle_set_adaptive.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle_set_radiation.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
         lib.oracle_set_bc.argtypes = [C.c_void_p, C.POINTER(_Bc)]
         lib.oracle_tstep.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int)]
         lib.oracle_filter_field.argtypes = [C.c_void_p, C.c_int, dp, dp]
@@ -159,6 +160,12 @@ class Oracle:
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
         if _get().oracle_set_bc(self.h, C.byref(b)) != 0:
             raise RuntimeError("oracle_set_bc: " + _get().oracle_last_error().decode())
+
+    def set_radiation(self, radn_path, trefrn=300.0):
+        """RADCAL on (radn.dat path, TREFRN) or off (radn_path None)."""
+        p = None if radn_path is None else str(radn_path).encode()
+        if _get().oracle_set_radiation(self.h, p, float(trefrn)) != 0:
+            raise RuntimeError("oracle_set_radiation: " + _get().oracle_last_error().decode())
 
     def set_adaptive(self, on=True):
         _get().oracle_set_adaptive(self.h, 1 if on else 0)

@@ -406,4 +406,41 @@ inline void read_diff(const std::string& path, const Chem& c, Diff& d) {
   d.flmavt = true;
 }
 
+// radn.dat reader: src/radcin.f:80-113 (records) and :210-220 (derived).
+// Five header records, the "Species list:" record, NRDSPC '(I5)', NSPEC
+// species records, a comment record, NSPRAD, then per radiating species a
+// record "JSPEC NKPRAD" and the NKPRAD coefficients read list-directed (the
+// read continues onto following records until it has them all).
+constexpr int NCFRMX = 6;
+struct Radn {
+  int nsprad = 0;
+  int nsprid[NSPCMX] = {};
+  int nkprad[NSPCMX] = {};
+  double akprad[NSPCMX][NCFRMX] = {};
+  double foursb = 0.0, trfrth = 0.0;
+};
+inline void read_radn(const std::string& path, const Chem& c, double trefrn, Radn& r) {
+  LineReader rd(path);
+  for (int i = 0; i < 6; ++i) rd.next();
+  rd.next();  // NRDSPC: only compared with NSPEC
+  for (int j = 0; j < c.nspec; ++j) rd.next();
+  rd.next();  // "Planck mean absorption coefficient data"
+  std::istringstream n0(rd.next());
+  if (!(n0 >> r.nsprad) || r.nsprad < 0 || r.nsprad > NSPCMX) throw std::runtime_error("NSPRAD out of range");
+  for (int j = 0; j < r.nsprad; ++j) {
+    std::istringstream h(rd.next());
+    if (!(h >> r.nsprid[j] >> r.nkprad[j]) || r.nsprid[j] < 1 || r.nsprid[j] > c.nspec || r.nkprad[j] < 1 ||
+        r.nkprad[j] > NCFRMX)
+      throw std::runtime_error("bad radiating species record");
+    int got = 0;
+    while (got < r.nkprad[j]) {
+      std::istringstream v(rd.next());
+      std::string tok;
+      while (got < r.nkprad[j] && v >> tok) r.akprad[j][got++] = freal(tok);
+    }
+  }
+  r.foursb = 4.0 * 5.67037321e-08;  // FOUR*STEFBO; STEFBO from src/com_senga2.h:222
+  r.trfrth = trefrn * trefrn * trefrn * trefrn;
+}
+
 }  // namespace orc

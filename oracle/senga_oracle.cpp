@@ -26,6 +26,7 @@
 //   src/lincom.f:53-169, src/fincom.f:54-168  2N-storage RK update
 //   src/dtinit.f:76-209     RK4(3)5[2R+]C coefficients
 //   src/parfer.f:840-873, src/cxhalo.f:49-72  single-rank periodic halo copy
+//   src/radcal.f:45-119, src/radcin.f:80-220  optically thin radiation loss
 #include <omp.h>
 
 #include <algorithm>
@@ -888,6 +889,34 @@ struct Oracle {
 #define BIG3 _Pragma("omp parallel for schedule(static)") for (int kc = kstab; kc <= kstob; ++kc) for (int jc = jstab; jc <= jstob; ++jc) for (int ic = istab; ic <= istob; ++ic)
 #define TRG3 _Pragma("omp parallel for schedule(static)") for (int kc = kstalt; kc <= kstolt; ++kc) for (int jc = jstalt; jc <= jstolt; ++jc) for (int ic = istalt; ic <= istolt; ++ic)
 
+  // ---- RADCAL: src/radcal.f:45-119. Planck-mean absorption of each
+  // radiating species (Horner in T), times its partial pressure
+  // YRHS*RGSPEC*T (YRHS is still rho*Y here), summed; ERHS loses
+  // FOURSB*sum*(T^4 - TREFRN^4). ----
+  bool flradn = false;
+  Radn rad;
+  void radcal() {
+    STD3 store1(ic, jc, kc) = 0.0;
+    for (int js = 0; js < rad.nsprad; ++js) {
+      STD3 {
+        const double fornow = trun(ic, jc, kc);
+        double plspec = rad.akprad[js][rad.nkprad[js] - 1];
+        for (int icp = rad.nkprad[js] - 1; icp >= 1; --icp) plspec = plspec * fornow + rad.akprad[js][icp - 1];
+        store2(ic, jc, kc) = plspec;
+      }
+      const int is = rad.nsprid[js] - 1;
+      STD3 {
+        const double fornow = yrhs[is](ic, jc, kc) * ch.rgspec[is] * trun(ic, jc, kc);
+        store1(ic, jc, kc) = store1(ic, jc, kc) + store2(ic, jc, kc) * fornow;
+      }
+    }
+    STD3 {
+      double fornow = trun(ic, jc, kc);
+      fornow = fornow * fornow * fornow * fornow;
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) - rad.foursb * store1(ic, jc, kc) * (fornow - rad.trfrth);
+    }
+  }
+
   // ---- RHSCAL: src/rhscal.f (branches used by the periodic cases) ----
   void rhscal() {
     temper();
@@ -953,6 +982,8 @@ struct Oracle {
     zx(fxlcon, fxrcon, store1); zy(fylcon, fyrcon, store2); zz(fzlcon, fzrcon, store3);
     STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc)) *
                                                    store7(ic, jc, kc);
+    // rhscal.f:810: radiation heat loss
+    if (flradn) radcal();
     // species
     chrate();
     STD3 for (int is = 0; is < nspec; ++is) rrte[is](ic, jc, kc) = rate[is](ic, jc, kc);
@@ -1690,6 +1721,26 @@ int oracle_set_bc(void* h, const oracle_bc* b) {
   try {
     static_cast<orc::Oracle*>(h)->set_bc(b->xl, b->xr, b->u_in, b->rho_in, b->y_in, b->p_inf, b->sigma, b->eta, b->pio,
                                          b->bet_local);
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// Optically thin radiation (RADCAL) from a radn.dat file and the reference
+// temperature TREFRN; a null path turns it off.
+int oracle_set_radiation(void* h, const char* radn_path, double trefrn) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  try {
+    if (!radn_path) {
+      o->flradn = false;
+      return 0;
+    }
+    orc::Radn r;
+    orc::read_radn(radn_path, o->ch, trefrn, r);
+    o->rad = r;
+    o->flradn = true;
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

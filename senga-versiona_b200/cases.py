@@ -22,6 +22,7 @@ DATA = os.path.join(HERE, "data")
 CHEM_1STEP = os.path.join(DATA, "chem_1step.dat")
 CHEM_H2 = os.path.join(DATA, "chem_h2.dat")
 DIFF_H2 = os.path.join(DATA, "diff_h2.dat")
+RADN_H2 = os.path.join(DATA, "radn_h2.dat")  # Planck-mean absorption of H2O
 
 NPERI = 2
 

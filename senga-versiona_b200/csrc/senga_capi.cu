@@ -70,6 +70,9 @@ struct senga_ctx {
   double tstep = 0.0, errold = 1.0e-4, errldr = 1.0e-4, errmax = 0.0;
   int inderr = 0, sms = 148;
   unsigned long long* d_errmax = nullptr;
+  // radiation heat loss (senga_set_radiation)
+  bool rad = false;
+  RadParams rp{};
   // NSCBC x faces (senga_set_nscbc)
   bool nscbc = false;
   NscbcParams bc{};
@@ -126,6 +129,7 @@ void run_rhs(senga_ctx* c) {
   launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
   if (c->nscbc) launch_face(c->geo, c->f, c->bc, c->nspec, c->d_chem, c->stream);  // face data + BOUNDS
   launch_flow(c->geo, c->f, c->nspec, c->stream);
+  if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);  // RADCAL
   launch_species_a(c->geo, c->f, c->nspec, c->stream);
 }
 
@@ -384,13 +388,14 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
       const int nth = launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
       CK(cudaEventRecord(ev[b + 1], c->stream));
       launch_flow(c->geo, c->f, c->nspec, c->stream);
+      if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);
       CK(cudaEventRecord(ev[b + 2], c->stream));
       launch_species_a(c->geo, c->f, c->nspec, c->stream);
       CK(cudaEventRecord(ev[b + 3], c->stream));
       RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
       launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
       CK(cudaEventRecord(irk < 5 ? ev[b + 4] : ev[20], c->stream));
-      nl += 3 + nth;
+      nl += 3 + nth + (c->rad ? 1 : 0);
     }
     CK(cudaStreamSynchronize(c->stream));
     for (int irk = 1; irk <= 5; ++irk) {
@@ -452,6 +457,34 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
     CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });
+}
+
+int senga_set_radiation(senga_ctx* c, const senga_radn* r) {
+  if (!c) return fail(SENGA_ERR_ARG, "senga_set_radiation: null context");
+  if (!r) {
+    c->rad = false;
+  } else {
+    if (r->nsprad < 0 || r->nsprad > SENGA_NSPCMX) return fail(SENGA_ERR_ARG, "senga_set_radiation: bad nsprad");
+    RadParams p{};
+    p.nsprad = r->nsprad;
+    for (int j = 0; j < r->nsprad; ++j) {
+      if (r->nsprid[j] < 1 || r->nsprid[j] > c->nspec || r->nkprad[j] < 1 || r->nkprad[j] > SENGA_NCFRMX)
+        return fail(SENGA_ERR_ARG, "senga_set_radiation: bad radiating species record");
+      p.id[j] = r->nsprid[j] - 1;
+      p.nk[j] = r->nkprad[j];
+      for (int k = 0; k < r->nkprad[j]; ++k) p.ak[j][k] = r->akprad[j][k];
+      p.rg[j] = c->chem.rgspec[p.id[j]];
+    }
+    p.foursb = 4.0 * 5.67037321e-08;  // FOUR*STEFBO, src/radcin.f; STEFBO of src/com_senga2.h:222
+    p.trfrth = r->trefrn * r->trefrn * r->trefrn * r->trefrn;
+    c->rp = p;
+    c->rad = true;
+  }
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return SENGA_OK;
 }
 
 int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {

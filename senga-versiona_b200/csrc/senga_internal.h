@@ -144,6 +144,16 @@ void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nsp
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,
                  cudaStream_t s);
 
+// RADCAL (radiation.cu): radiating species (0-based), their polynomials,
+// gas constants, 4 STEFBO and TREFRN^4.
+struct RadParams {
+  int nsprad;
+  int id[SENGA_NSPCMX], nk[SENGA_NSPCMX];
+  double ak[SENGA_NSPCMX][SENGA_NCFRMX], rg[SENGA_NSPCMX];
+  double foursb, trfrth;
+};
+void launch_radcal(const Geo& g, const Fields& f, const RadParams& r, cudaStream_t s);
+
 // ADAPTT error maxima (adapt.cu): out[fl] = max |err|/(|run| + nrm.v[fl])
 // as the bit pattern of a non-negative double, per conserved field.
 struct ErrNorms {

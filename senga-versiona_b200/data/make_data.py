@@ -3,6 +3,9 @@
 * chem_h2.dat / diff_h2.dat: the reference project's own input/chem.dat and
   input/diff.dat (H2/air, 9 species, 21 steps; ppchem/ppdiff output), copied
   verbatim because the 128^3 and 256^3 workloads are defined on them.
+* radn_h2.dat: the reference project's input/radn.dat (Planck-mean
+  absorption polynomial of H2O for the same 9-species list), copied verbatim
+  for the radiation tests.
 * chem_1step.dat: the single-step irreversible R -> P mechanism of the 32^3
   and batched workloads, written in the same chem.dat record layout
   (src/chemin.f:146-344): A = 1e9 1/s, Ea/R = 15000 K, equal molar mass 29
@@ -57,7 +60,8 @@ def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     with open(os.path.join(HERE, "chem_1step.dat"), "w") as fh:
         fh.write(one_step_chem())
-    for src, dst in (("input/chem.dat", "chem_h2.dat"), ("input/diff.dat", "diff_h2.dat")):
+    for src, dst in (("input/chem.dat", "chem_h2.dat"), ("input/diff.dat", "diff_h2.dat"),
+                     ("input/radn.dat", "radn_h2.dat")):
         path = os.path.join(ref, src)
         if os.path.exists(path):
             shutil.copyfile(path, os.path.join(HERE, dst))

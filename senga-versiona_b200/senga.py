@@ -100,6 +100,16 @@ class NscbcT(C.Structure):
                 ("pio", C.c_int), ("bet_local", C.c_int)]
 
 
+NCFRMX = 6
+
+
+class RadnT(C.Structure):
+    """senga_radn: Planck-mean absorption data of the radiating species."""
+
+    _fields_ = [("nsprad", C.c_int), ("nsprid", C.c_int * NSPCMX), ("nkprad", C.c_int * NSPCMX),
+                ("akprad", (C.c_double * NCFRMX) * NSPCMX), ("trefrn", C.c_double)]
+
+
 class SengaError(RuntimeError):
     pass
 
@@ -131,6 +141,8 @@ def _load():
         "senga_filter": (ip, [vp, ip]),
         "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
         "senga_set_nscbc": (ip, [vp, C.POINTER(NscbcT)]),
+        "senga_radn_load": (ip, [C.c_char_p, C.POINTER(ChemT), C.c_double, C.POINTER(RadnT)]),
+        "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
         "senga_server_set_max_points": (ip, [vp, C.c_int64]),
         "senga_dump_write": (ip, [C.c_char_p, ip, ip, ip, ip, ip, ip, dp, dp]),
         "senga_dump_read": (ip, [C.c_char_p, ip, ip, C.POINTER(C.c_int), dp, C.c_int64, dp]),
@@ -239,6 +251,25 @@ class Diff:
     @property
     def mixture_averaged(self):
         return bool(self.t.flmavt)
+
+
+class Radn:
+    """Radiation data (RADCIN) from a radn.dat file and the reference
+    ambient temperature TREFRN [K] of the cont.dat radiation line."""
+
+    def __init__(self, path, chem, trefrn=300.0):
+        self.path = path
+        self.t = RadnT()
+        _check(lib.senga_radn_load(path.encode(), C.byref(chem.t), float(trefrn), C.byref(self.t)),
+               "senga_radn_load")
+
+    @property
+    def species(self):
+        """1-based indices of the radiating species."""
+        return [self.t.nsprid[j] for j in range(self.t.nsprad)]
+
+    def coefficients(self, j):
+        return [self.t.akprad[j][k] for k in range(self.t.nkprad[j])]
 
 
 class Box:
@@ -372,6 +403,11 @@ class Box:
         b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
         _check(lib.senga_set_nscbc(self.h, C.byref(b)), "senga_set_nscbc")
+
+    def set_radiation(self, radn):
+        """Optically thin radiation loss (RADCAL) on with a Radn, off with None."""
+        _check(lib.senga_set_radiation(self.h, C.byref(radn.t) if radn is not None else None),
+               "senga_set_radiation")
 
     def tstep(self):
         """(TSTEP, last ERRMAX, INDERR) of the adaptive controller."""
