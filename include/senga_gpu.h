@@ -178,6 +178,14 @@ int senga_get_status(senga_ctx* ctx, int* status);
 int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
 
+/* Mixture-averaged transport switches of cont.dat's transport line
+ * (NFMIXW, NFMIXP, NFMSOR, NFMDUF, WMLTDR; src/contin.f:205): molar-mass
+ * (src/rhscal.f:1966-2357), pressure (:2361-2757) diffusion, Soret
+ * (:2760-3765) and Dufour (:1552-1564) terms; the last two for the species
+ * with W_k <= WMLTDR + 1e-3 (src/diffin.f:384-406). Needs a diff.dat
+ * (flmavt). All zero turns them off (the default). */
+int senga_set_transport(senga_ctx* ctx, int mixw, int mixp, int soret, int dufour, double wmltdr);
+
 /* Optically thin radiation heat loss, RADCAL (src/radcal.f:45-119), run when
  * the cont.dat radiation switch is on (src/rhscal.f:810):
  * ERHS -= 4 STEFBO sum_j a_j(T) rho Y_j R_j T (T^4 - TREFRN^4), with the

@@ -27,6 +27,8 @@
 //   src/dtinit.f:76-209     RK4(3)5[2R+]C coefficients
 //   src/parfer.f:840-873, src/cxhalo.f:49-72  single-rank periodic halo copy
 //   src/radcal.f:45-119, src/radcin.f:80-220  optically thin radiation loss
+//   src/rhscal.f:946-1003,1352-1403,1552-1564,1966-3765  molar-mass, pressure,
+//                           Soret and Dufour terms of mixture-averaged transport
 #include <omp.h>
 
 #include <algorithm>
@@ -147,6 +149,11 @@ struct Oracle {
   std::vector<Field> rate, rrte;
   Field ucor, vcor, wcor, utmp, vtmp, wtmp, prun, trun, transp;
   Field wmomix, difmix;
+  // mixture-averaged transport extras: first/second derivatives of ln W_mix,
+  // ln p and ln(T/TDIFGB); thermal diffusion ratio of the current species
+  Field wd1x, wd1y, wd1z, wd2x, wd2y, wd2z, pd1x, pd1y, pd1z, pd2x, pd2y, pd2z;
+  Field td1x, td1y, td1z, td2x, td2y, td2z, tdrmix;
+  bool flmsor[NSPCMX] = {}, flmduf[NSPCMX] = {}, flmtdr[NSPCMX] = {};
   IField itndex;
   Field wk1, wk2, wk3, wk4;  // chrate STORE1..4 counterparts
 
@@ -171,7 +178,9 @@ struct Oracle {
     Field* all[] = {&drun, &urun, &vrun, &wrun, &erun, &drhs, &urhs, &vrhs, &wrhs, &erhs,
                     &derr, &uerr, &verr, &werr, &eerr, &store1, &store2, &store3, &store4,
                     &store5, &store6, &store7, &divm, &ucor, &vcor, &wcor, &utmp, &vtmp,
-                    &wtmp, &prun, &trun, &transp, &wmomix, &difmix, &wk1, &wk2, &wk3, &wk4};
+                    &wtmp, &prun, &trun, &transp, &wmomix, &difmix, &wk1, &wk2, &wk3, &wk4,
+                    &wd1x, &wd1y, &wd1z, &wd2x, &wd2y, &wd2z, &pd1x, &pd1y, &pd1z, &pd2x, &pd2y, &pd2z,
+                    &td1x, &td1y, &td1z, &td2x, &td2y, &td2z, &tdrmix};
     for (Field* f : all) f->init(nx, ny, nz);
     auto mk = [&](std::vector<Field>& v) {
       v.resize(nspec);
@@ -917,6 +926,76 @@ struct Oracle {
     }
   }
 
+  // One molar-mass or pressure branch of the species loop (rhscal.f:1966-2357
+  // and 2361-2757 have the same statements on WD* and PD*), STORE7 holding
+  // the driving diffusivity. The wall terms (FxxDFW) are not restated: no
+  // wall boundary is built.
+  void gradient_branch(Field& rt, Field& g1x, Field& g1y, Field& g1z, Field& g2x, Field& g2y, Field& g2z) {
+    STD3 {
+      ucor(ic, jc, kc) = ucor(ic, jc, kc) + store7(ic, jc, kc) * g1x(ic, jc, kc);
+      vcor(ic, jc, kc) = vcor(ic, jc, kc) + store7(ic, jc, kc) * g1y(ic, jc, kc);
+      wcor(ic, jc, kc) = wcor(ic, jc, kc) + store7(ic, jc, kc) * g1z(ic, jc, kc);
+    }
+    dfbydx(store7, store1); dfbydy(store7, store2); dfbydz(store7, store3);
+    zx(fxldif, fxrdif, store1); zy(fyldif, fyrdif, store2); zz(fzldif, fzrdif, store3);
+    STD3 {
+      double f = store1(ic, jc, kc) * g1x(ic, jc, kc) + store2(ic, jc, kc) * g1y(ic, jc, kc) +
+                 store3(ic, jc, kc) * g1z(ic, jc, kc);
+      rt(ic, jc, kc) = rt(ic, jc, kc) + f;
+      vtmp(ic, jc, kc) = vtmp(ic, jc, kc) + f;
+    }
+    zx(fxladb, fxradb, store1); zy(fyladb, fyradb, store2); zz(fzladb, fzradb, store3);
+    STD3 {
+      double f = store1(ic, jc, kc) * g1x(ic, jc, kc) + store2(ic, jc, kc) * g1y(ic, jc, kc) +
+                 store3(ic, jc, kc) * g1z(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * utmp(ic, jc, kc);
+    }
+    zx(fxldif, fxrdif, store4); zy(fyldif, fyrdif, store5); zz(fzldif, fzrdif, store6);
+    zx(fxladb, fxradb, store4); zy(fyladb, fyradb, store5); zz(fzladb, fzradb, store6);
+    STD3 {
+      double f = store4(ic, jc, kc) * g1x(ic, jc, kc) + store5(ic, jc, kc) * g1y(ic, jc, kc) +
+                 store6(ic, jc, kc) * g1z(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * store7(ic, jc, kc);
+    }
+    second_derivative_terms(rt, g2x, g2y, g2z);
+  }
+  // the second-derivative part of each branch; the zeroing acts on the
+  // stored second derivatives themselves, as in the reference
+  void second_derivative_terms(Field& rt, Field& g2x, Field& g2y, Field& g2z) {
+    zx(fxldif, fxrdif, g2x); zy(fyldif, fyrdif, g2y); zz(fzldif, fzrdif, g2z);
+    STD3 {
+      double f = (g2x(ic, jc, kc) + g2y(ic, jc, kc) + g2z(ic, jc, kc)) * store7(ic, jc, kc);
+      rt(ic, jc, kc) = rt(ic, jc, kc) + f;
+      vtmp(ic, jc, kc) = vtmp(ic, jc, kc) + f;
+    }
+    zx(fxladb, fxradb, g2x); zy(fyladb, fyradb, g2y); zz(fzladb, fzradb, g2z);
+    STD3 {
+      double f = (g2x(ic, jc, kc) + g2y(ic, jc, kc) + g2z(ic, jc, kc)) * store7(ic, jc, kc);
+      erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * utmp(ic, jc, kc);
+    }
+  }
+
+  // Switches of the cont.dat transport line (molar mass, pressure, Soret,
+  // Dufour, molar-mass limit): src/diffin.f:384-406, WMLTOL 1e-3 (:34).
+  void set_transport(bool mixw, bool mixp, bool soret, bool dufour, double wmltdr) {
+    if (!df.flmavt) throw std::runtime_error("transport switches need mixture-averaged transport");
+    df.flmixw = mixw;
+    df.flmixp = mixp;
+    df.flmixt = false;
+    for (int is = 0; is < NSPCMX; ++is) flmsor[is] = flmduf[is] = flmtdr[is] = false;
+    const double wmltol = 1.0e-3;
+    if (soret) {
+      df.flmixt = true;
+      for (int is = 0; is < nspec; ++is)
+        if (ch.wmolar[is] <= wmltdr + wmltol) flmsor[is] = flmtdr[is] = true;
+    }
+    if (dufour) {
+      df.flmixt = true;
+      for (int is = 0; is < nspec; ++is)
+        if (ch.wmolar[is] <= wmltdr + wmltol) flmduf[is] = flmtdr[is] = true;
+    }
+  }
+
   // ---- RHSCAL: src/rhscal.f (branches used by the periodic cases) ----
   void rhscal() {
     temper();
@@ -992,6 +1071,22 @@ struct Oracle {
     });
     STD3 { ucor(ic, jc, kc) = 0.0; vcor(ic, jc, kc) = 0.0; wcor(ic, jc, kc) = 0.0; vtmp(ic, jc, kc) = 0.0; }
     BIG3 wtmp(ic, jc, kc) = 0.0;
+    // rhscal.f:946-1003: ln(W_mix), ln(p) and ln(T/TDIFGB) (TRANSP holds the
+    // last) with their first and second derivatives
+    if (df.flmixw) {
+      BIG3 store7(ic, jc, kc) = std::log(wmomix(ic, jc, kc));
+      dfbydx(store7, wd1x); dfbydy(store7, wd1y); dfbydz(store7, wd1z);
+      d2fdx2(store7, wd2x); d2fdy2(store7, wd2y); d2fdz2(store7, wd2z);
+    }
+    if (df.flmixp) {
+      BIG3 store7(ic, jc, kc) = std::log(prun(ic, jc, kc));
+      dfbydx(store7, pd1x); dfbydy(store7, pd1y); dfbydz(store7, pd1z);
+      d2fdx2(store7, pd2x); d2fdy2(store7, pd2y); d2fdz2(store7, pd2z);
+    }
+    if (df.flmixt) {
+      dfbydx(transp, td1x); dfbydy(transp, td1y); dfbydz(transp, td1z);
+      d2fdx2(transp, td2x); d2fdy2(transp, td2y); d2fdz2(transp, td2z);
+    }
     for (int is = 0; is < nspec; ++is) {
       Field& y = yrhs[is];
       TRG3 y(ic, jc, kc) = y(ic, jc, kc) / drhs(ic, jc, kc);
@@ -1043,6 +1138,22 @@ struct Oracle {
           store7(ic, jc, kc) = difmix(ic, jc, kc);
         }
       }
+      // rhscal.f:1352-1403: thermal diffusion ratio of this species against
+      // the other light species, times its mole fraction
+      if (flmtdr[is - 1]) {
+        BIG3 tdrmix(ic, jc, kc) = 0.0;
+        for (int js = 1; js <= nspec; ++js) {
+          if (!flmtdr[js - 1] || js == is) continue;
+          BIG3 {
+            const double combo2 = trun(ic, jc, kc) / df.tdifgb;
+            double f = df.tdrcco[Diff::d3(df.ncotdr, js, is)];
+            for (int icp = df.ncotdr - 1; icp >= 1; --icp) f = f * combo2 + df.tdrcco[Diff::d3(icp, js, is)];
+            const double fornow = yrhs[js - 1](ic, jc, kc) * ch.ovwmol[js - 1];
+            tdrmix(ic, jc, kc) = tdrmix(ic, jc, kc) + fornow * wmomix(ic, jc, kc) * f;
+          }
+        }
+        BIG3 tdrmix(ic, jc, kc) = tdrmix(ic, jc, kc) * y(ic, jc, kc) * wmomix(ic, jc, kc) * ch.ovwmol[is - 1];
+      }
       STD3 {
         ucor(ic, jc, kc) = ucor(ic, jc, kc) + store7(ic, jc, kc) * store1(ic, jc, kc);
         vcor(ic, jc, kc) = vcor(ic, jc, kc) + store7(ic, jc, kc) * store2(ic, jc, kc);
@@ -1062,6 +1173,8 @@ struct Oracle {
         }
       }
       face_pts([&](Face& F, int ic, int jc, int kc, int q) { F.h[fs(is - 1, jc, kc)] = utmp(ic, jc, kc); });
+      // rhscal.f:1552-1564: Dufour term added to the species enthalpy
+      if (flmduf[is - 1]) BIG3 utmp(ic, jc, kc) = utmp(ic, jc, kc) + ch.rgspec[is - 1] * trun(ic, jc, kc) * tdrmix(ic, jc, kc);
       dfbydx(store7, store4); dfbydy(store7, store5); dfbydz(store7, store6);
       zx(fxldif, fxrdif, store4); zy(fyldif, fyrdif, store5); zz(fzldif, fzrdif, store6);
       STD3 {
@@ -1097,6 +1210,52 @@ struct Oracle {
       STD3 {
         double f = (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc)) * store4(ic, jc, kc);
         erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * utmp(ic, jc, kc);
+      }
+      // rhscal.f:1966-2357 (molar mass), 2361-2757 (pressure): STORE7 is the
+      // driving diffusivity; STORE4..6 still hold what the code above left
+      // there (STORE4 = DIFMIX, STORE5/6 = y/z enthalpy gradients)
+      if (df.flmixw) {
+        BIG3 store7(ic, jc, kc) = difmix(ic, jc, kc) * y(ic, jc, kc);
+        gradient_branch(rt, wd1x, wd1y, wd1z, wd2x, wd2y, wd2z);
+      }
+      if (df.flmixp) {
+        BIG3 store7(ic, jc, kc) = difmix(ic, jc, kc) * y(ic, jc, kc) * (1.0 - ch.wmolar[is - 1] / wmomix(ic, jc, kc));
+        gradient_branch(rt, pd1x, pd1y, pd1z, pd2x, pd2y, pd2z);
+      }
+      // rhscal.f:2760-3765: Soret term, with the Dufour part taken out of the
+      // species enthalpy again and its gradients recomputed
+      if (flmsor[is - 1]) {
+        BIG3 store7(ic, jc, kc) = difmix(ic, jc, kc) * y(ic, jc, kc) * tdrmix(ic, jc, kc);
+        STD3 {
+          ucor(ic, jc, kc) = ucor(ic, jc, kc) + store7(ic, jc, kc) * td1x(ic, jc, kc);
+          vcor(ic, jc, kc) = vcor(ic, jc, kc) + store7(ic, jc, kc) * td1y(ic, jc, kc);
+          wcor(ic, jc, kc) = wcor(ic, jc, kc) + store7(ic, jc, kc) * td1z(ic, jc, kc);
+        }
+        dfbydx(store7, store1); dfbydy(store7, store2); dfbydz(store7, store3);
+        zx(fxldif, fxrdif, store1); zy(fyldif, fyrdif, store2); zz(fzldif, fzrdif, store3);
+        STD3 {
+          double f = store1(ic, jc, kc) * td1x(ic, jc, kc) + store2(ic, jc, kc) * td1y(ic, jc, kc) +
+                     store3(ic, jc, kc) * td1z(ic, jc, kc);
+          rt(ic, jc, kc) = rt(ic, jc, kc) + f;
+          vtmp(ic, jc, kc) = vtmp(ic, jc, kc) + f;
+        }
+        if (flmduf[is - 1])
+          BIG3 utmp(ic, jc, kc) = utmp(ic, jc, kc) - ch.rgspec[is - 1] * trun(ic, jc, kc) * tdrmix(ic, jc, kc);
+        zx(fxladb, fxradb, store1); zy(fyladb, fyradb, store2); zz(fzladb, fzradb, store3);
+        STD3 {
+          double f = store1(ic, jc, kc) * td1x(ic, jc, kc) + store2(ic, jc, kc) * td1y(ic, jc, kc) +
+                     store3(ic, jc, kc) * td1z(ic, jc, kc);
+          erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * utmp(ic, jc, kc);
+        }
+        dfbydx(utmp, store4); dfbydy(utmp, store5); dfbydz(utmp, store6);
+        zx(fxldif, fxrdif, store4); zy(fyldif, fyrdif, store5); zz(fzldif, fzrdif, store6);
+        zx(fxladb, fxradb, store4); zy(fyladb, fyradb, store5); zz(fzladb, fzradb, store6);
+        STD3 {
+          double f = store4(ic, jc, kc) * td1x(ic, jc, kc) + store5(ic, jc, kc) * td1y(ic, jc, kc) +
+                     store6(ic, jc, kc) * td1z(ic, jc, kc);
+          erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * store7(ic, jc, kc);
+        }
+        second_derivative_terms(rt, td2x, td2y, td2z);
       }
     }
     dfbydx(wtmp, store1); dfbydy(wtmp, store2); dfbydz(wtmp, store3);
@@ -1721,6 +1880,17 @@ int oracle_set_bc(void* h, const oracle_bc* b) {
   try {
     static_cast<orc::Oracle*>(h)->set_bc(b->xl, b->xr, b->u_in, b->rho_in, b->y_in, b->p_inf, b->sigma, b->eta, b->pio,
                                          b->bet_local);
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// Transport switches of cont.dat (NFMIXW, NFMIXP, NFMSOR, NFMDUF, WMLTDR).
+int oracle_set_transport(void* h, int mixw, int mixp, int soret, int dufour, double wmltdr) {
+  try {
+    static_cast<orc::Oracle*>(h)->set_transport(mixw != 0, mixp != 0, soret != 0, dufour != 0, wmltdr);
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

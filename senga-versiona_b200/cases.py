@@ -202,6 +202,13 @@ def make_case(name, n=None, seed=1234, scale_n=None):
                   composition of complete H2 -> H2O conversion; mean flow
                   1.25 m/s plus Passot-Pouquet turbulence u' = 2 m/s,
                   l = 1.5 mm. The result carries "bc" for the face setup.
+    h2_pool     : 32^3 periodic, 10 mm, H2/air mixture-averaged with a
+                  radical pool: the h2_kernels layout (4 seeded kernels
+                  r = 1 mm, 800 K -> 1600 K) with the kernels' composition
+                  moving from stoichiometric unburnt towards a partially
+                  burnt mixture holding H, O, OH, HO2, H2O2, and a 5%
+                  sinusoidal pressure modulation, so that the molar-mass,
+                  pressure, Soret and Dufour terms are all active.
     `n` overrides the grid extent (cubic) for smaller test instances.
     """
     from senga import Chem  # noqa: local import keeps this module numpy-only
@@ -269,6 +276,27 @@ def make_case(name, n=None, seed=1234, scale_n=None):
         dt = stable_dt(chem, fields, T, lengths, shp)
         return dict(name=name, shape=shape_xyz, lengths=lengths, chem=chem_path, diff=diff_path, fields=fields, T=T,
                     itn=itn, dt=dt, nend=(1, 1, NPERI, NPERI, NPERI, NPERI), bc=bc)
+    elif name == "h2_pool":
+        nn = n or 32
+        shape_xyz = (nn, nn, nn)
+        L = 1.0e-2
+        lengths = (L, L, L)
+        chem_path, diff_path = CHEM_H2, DIFF_H2
+        chem = Chem(chem_path)
+        shp = (nn, nn, nn)
+        centres = [tuple(rng.uniform(0.0, L, size=3)) for _ in range(4)]
+        T = hot_kernels(shp, lengths, centres, 1.0e-3, 800.0, 1600.0)
+        prog = (T - 800.0) / 800.0
+        wm = chem.table("wmolar")
+        mass = np.array([2 * wm[0], wm[1], 3.76 * wm[8]])
+        yu = np.zeros(9)
+        yu[0], yu[1], yu[8] = mass / mass.sum()
+        yb = np.array([0.01, 0.12, 0.14, 0.004, 0.012, 0.002, 0.0005, 0.0002, 0.0])
+        yb[8] = 1.0 - yb[:8].sum()
+        Y = np.array([yu[k] + (yb[k] - yu[k]) * prog for k in range(9)])
+        u, v, w = passot_pouquet(shp, lengths, 2.0, 1.5e-3, seed)
+        z_, y_, x_ = np.meshgrid(*(np.arange(m) * (L / (m - 1)) for m in shp), indexing="ij")
+        p = 101325.0 * (1.0 + 0.05 * np.sin(2 * math.pi * x_ / L) * np.sin(2 * math.pi * y_ / L))
     elif name == "ensemble":
         sizes = (32, 48, 64, 96)
         shape_xyz = tuple(int(rng.choice(sizes)) for _ in range(3)) if n is None else (n, n, n)

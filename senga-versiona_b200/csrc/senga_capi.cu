@@ -70,6 +70,10 @@ struct senga_ctx {
   double tstep = 0.0, errold = 1.0e-4, errldr = 1.0e-4, errmax = 0.0;
   int inderr = 0, sms = 148;
   unsigned long long* d_errmax = nullptr;
+  // molar-mass / pressure / Soret / Dufour transport terms (senga_set_transport)
+  bool mixt = false;
+  MixtParams mx{};
+  double* mixt_pool = nullptr;
   // radiation heat loss (senga_set_radiation)
   bool rad = false;
   RadParams rp{};
@@ -131,6 +135,7 @@ void run_rhs(senga_ctx* c) {
   launch_flow(c->geo, c->f, c->nspec, c->stream);
   if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);  // RADCAL
   launch_species_a(c->geo, c->f, c->nspec, c->stream);
+  if (c->mixt) launch_mixt(c->geo, c->f, c->mx, c->d_chem, c->d_diff, c->nspec, c->stream);
 }
 
 void run_substage(senga_ctx* c, int irk) {
@@ -286,6 +291,7 @@ int senga_ctx_destroy(senga_ctx* c) {
   cudaFree(c->d_status);
   cudaFree(c->d_errmax);
   cudaFree(c->nscbc_pool);
+  cudaFree(c->mixt_pool);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SENGA_OK;
@@ -391,11 +397,12 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
       if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);
       CK(cudaEventRecord(ev[b + 2], c->stream));
       launch_species_a(c->geo, c->f, c->nspec, c->stream);
+      const int nmx = c->mixt ? launch_mixt(c->geo, c->f, c->mx, c->d_chem, c->d_diff, c->nspec, c->stream) : 0;
       CK(cudaEventRecord(ev[b + 3], c->stream));
       RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
       launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
       CK(cudaEventRecord(irk < 5 ? ev[b + 4] : ev[20], c->stream));
-      nl += 3 + nth + (c->rad ? 1 : 0);
+      nl += 3 + nth + (c->rad ? 1 : 0) + nmx;
     }
     CK(cudaStreamSynchronize(c->stream));
     for (int irk = 1; irk <= 5; ++irk) {
@@ -456,6 +463,53 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_set_transport(senga_ctx* c, int mixw, int mixp, int soret, int dufour, double wmltdr) {
+  if (!c) return fail(SENGA_ERR_ARG, "senga_set_transport: null context");
+  return guard([&] {
+    if ((mixw || mixp || soret || dufour) && !c->diff.flmavt)
+      throw Error(SENGA_ERR_ARG, "senga_set_transport: the switches need mixture-averaged transport (diff.dat)");
+    CK(cudaStreamSynchronize(c->stream));
+    cudaFree(c->mixt_pool);
+    c->mixt_pool = nullptr;
+    c->mx = MixtParams{};
+    c->mixt = false;
+    if (c->graph) {
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
+    if (!(mixw || mixp || soret || dufour)) return;
+    MixtParams m{};
+    m.w = mixw ? 1 : 0;
+    m.p = mixp ? 1 : 0;
+    m.t = (soret || dufour) ? 1 : 0;
+    // light species: W_k <= WMLTDR + WMLTOL, WMLTOL = 1e-3 (src/diffin.f:34,390-405)
+    for (int k = 0; k < c->nspec; ++k) {
+      if (c->chem.wmolar[k] > wmltdr + 1.0e-3) continue;
+      if (soret) m.sor |= 1u << k;
+      if (dufour) m.duf |= 1u << k;
+      if (soret || dufour) m.tdr |= 1u << k;
+    }
+    const int64_t n = c->geo.n;
+    const int nb = m.w + m.p + m.t;
+    const int64_t fields = 1 + 5 * (int64_t)nb + (m.tdr ? c->nspec : 0);
+    CK(cudaMalloc(&c->mixt_pool, (size_t)(fields * n) * sizeof(double)));
+    double* p = c->mixt_pool;
+    m.wmix = p;
+    p += n;
+    const int on[3] = {m.w, m.p, m.t};
+    for (int b = 0; b < 3; ++b) {
+      if (!on[b]) continue;
+      m.lng[b] = p;
+      m.g1[b] = p + n;
+      m.g2[b] = p + 4 * n;
+      p += 5 * n;
+    }
+    if (m.tdr) m.tdrmix = p;
+    c->mx = m;
+    c->mixt = true;
   });
 }
 

@@ -154,6 +154,21 @@ struct RadParams {
 };
 void launch_radcal(const Geo& g, const Fields& f, const RadParams& r, cudaStream_t s);
 
+// Mixture-averaged transport extras (transport.cu): switches, per-species
+// bit masks (FLMSOR, FLMDUF, FLMTDR) and scratch. lng/g1/g2 index 0 molar
+// mass, 1 pressure, 2 temperature.
+struct MixtParams {
+  int w, p, t;
+  unsigned sor, duf, tdr;
+  double* wmix;      // [n]
+  double* lng[3];    // [n] each, nullptr when off
+  double* g1[3];     // [3][n] first derivatives
+  double* g2[3];     // [n] sum of second derivatives (x part zeroed on diffusion-flux faces)
+  double* tdrmix;    // [nspec][n], nullptr without Soret/Dufour
+};
+int launch_mixt(const Geo& g, const Fields& f, const MixtParams& m, const senga_chem* dchem, const senga_diff* ddiff,
+                int nspec, cudaStream_t s);
+
 // ADAPTT error maxima (adapt.cu): out[fl] = max |err|/(|run| + nrm.v[fl])
 // as the bit pattern of a non-negative double, per conserved field.
 struct ErrNorms {

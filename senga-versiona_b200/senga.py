@@ -143,6 +143,7 @@ def _load():
         "senga_set_nscbc": (ip, [vp, C.POINTER(NscbcT)]),
         "senga_radn_load": (ip, [C.c_char_p, C.POINTER(ChemT), C.c_double, C.POINTER(RadnT)]),
         "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
+        "senga_set_transport": (ip, [vp, ip, ip, ip, ip, C.c_double]),
         "senga_server_set_max_points": (ip, [vp, C.c_int64]),
         "senga_dump_write": (ip, [C.c_char_p, ip, ip, ip, ip, ip, ip, dp, dp]),
         "senga_dump_read": (ip, [C.c_char_p, ip, ip, C.POINTER(C.c_int), dp, C.c_int64, dp]),
@@ -403,6 +404,12 @@ class Box:
         b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
         _check(lib.senga_set_nscbc(self.h, C.byref(b)), "senga_set_nscbc")
+
+    def set_transport(self, mixw=False, mixp=False, soret=False, dufour=False, wmltdr=5.0):
+        """cont.dat transport switches: molar-mass and pressure diffusion,
+        Soret and Dufour for species lighter than wmltdr (+1e-3)."""
+        _check(lib.senga_set_transport(self.h, int(mixw), int(mixp), int(soret), int(dufour), float(wmltdr)),
+               "senga_set_transport")
 
     def set_radiation(self, radn):
         """Optically thin radiation loss (RADCAL) on with a Radn, off with None."""
