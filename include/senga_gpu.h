@@ -279,6 +279,22 @@ int senga_dump_write(const char* path, int formatted, int nx, int ny, int nz, in
 int senga_dump_read(const char* path, int formatted, int nspcmx, int* dims, double* fields, int64_t capacity,
                     double* scalars);
 
+/* ---- post-processing output ------------------------------------------------
+ * The record written every NTDUMP steps for post-processing
+ * (src/output.f:240-265, file output/out<IDDUMP:5><IPROC:4>.res): DRUN,
+ * URUN/DRUN, VRUN/DRUN, WRUN/DRUN, ERUN/DRUN, TRUN, PRUN, YRUN/DRUN (NSPEC
+ * fields), RRTE (NSPCMX fields) and ETIME, one unformatted record.
+ * senga_keep_rates(ctx, 1) makes every substage keep its CHRATE rates
+ * (RRTE, src/rhscal.f:828); senga_post_fields_host then fills post with
+ * (7 + 2 nspec) interior arrays (the primitives formed on the device, then
+ * RRTE_1..RRTE_nspec); senga_post_write / senga_post_read write and read the
+ * file (no size header: the sizes are the caller's). */
+int senga_keep_rates(senga_ctx* ctx, int on);
+int senga_post_fields_host(senga_ctx* ctx, double* post);
+int senga_post_write(const char* path, int nx, int ny, int nz, int nspec, int nspcmx, const double* post,
+                     double etime);
+int senga_post_read(const char* path, int nx, int ny, int nz, int nspec, int nspcmx, double* post, double* etime);
+
 /* ---- batched ensembles --------------------------------------------------------
  * No counterpart in the reference (it runs one box per MPI job). Many
  * independent periodic boxes of uneven sizes, one mechanism, each with its own

@@ -63,6 +63,7 @@ def _get():
         lib.oracle_filter.argtypes = [C.c_void_p, C.c_int]
         lib.oracle_set_adaptive.argtypes = [C.c_void_p, C.c_int]
         lib.oracle_set_radiation.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
+        lib.oracle_post.argtypes = [C.c_void_p, dp]
         lib.oracle_set_transport.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
         lib.oracle_set_bc.argtypes = [C.c_void_p, C.POINTER(_Bc)]
         lib.oracle_tstep.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int)]
@@ -167,6 +168,12 @@ class Oracle:
         p = None if radn_path is None else str(radn_path).encode()
         if _get().oracle_set_radiation(self.h, p, float(trefrn)) != 0:
             raise RuntimeError("oracle_set_radiation: " + _get().oracle_last_error().decode())
+
+    def post(self):
+        """Post-processing record fields (7 + 2 nspec, nz, ny, nx)."""
+        out = np.empty((7 + 2 * self.nspec,) + self.shape)
+        _get().oracle_post(self.h, _dp(out))
+        return out
 
     def set_transport(self, mixw=False, mixp=False, soret=False, dufour=False, wmltdr=5.0):
         """cont.dat transport switches (molar mass, pressure, Soret, Dufour;

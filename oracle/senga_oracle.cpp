@@ -1887,6 +1887,32 @@ int oracle_set_bc(void* h, const oracle_bc* b) {
   }
 }
 
+// The post-processing record's fields (src/output.f:240-265): DRUN,
+// URUN/DRUN, VRUN/DRUN, WRUN/DRUN, ERUN/DRUN, TRUN, PRUN, YRUN/DRUN, RRTE.
+int oracle_post(void* h, double* out) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  const int ns = o->nspec;
+  const size_t n = (size_t)o->nx * o->ny * o->nz;
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j)
+      for (int i = 1; i <= o->nx; ++i) {
+        const size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
+        const double d = o->drun(i, j, k);
+        out[q] = d;
+        out[n + q] = o->urun(i, j, k) / d;
+        out[2 * n + q] = o->vrun(i, j, k) / d;
+        out[3 * n + q] = o->wrun(i, j, k) / d;
+        out[4 * n + q] = o->erun(i, j, k) / d;
+        out[5 * n + q] = o->trun(i, j, k);
+        out[6 * n + q] = o->prun(i, j, k);
+        for (int s = 0; s < ns; ++s) {
+          out[(7 + s) * n + q] = o->yrun[s](i, j, k) / d;
+          out[(7 + ns + s) * n + q] = o->rrte[s](i, j, k);
+        }
+      }
+  return 0;
+}
+
 // Transport switches of cont.dat (NFMIXW, NFMIXP, NFMSOR, NFMDUF, WMLTDR).
 int oracle_set_transport(void* h, int mixw, int mixp, int soret, int dufour, double wmltdr) {
   try {

@@ -1,4 +1,5 @@
-// Restart dump files in the reference's two layouts (host code).
+// Restart dump files in the reference's two layouts, and the
+// post-processing record (host code).
 //
 // Writer: src/output.f:296-322 (NDOFMT = 0 unformatted, 1 formatted);
 // reader: src/indata.f:1405-1436 (NDIFMT likewise). One record / one file
@@ -148,6 +149,35 @@ extern "C" int senga_dump_write(const char* path, int formatted, int nx, int ny,
   }
   std::fprintf(fp, " %25.17E %25.17E %25.17E %25.17E\n", scalars[0], scalars[1], scalars[2], scalars[3]);
   if (std::fclose(fp) != 0) return fail(SENGA_ERR_IO, std::string("senga_dump_write: cannot write ") + path);
+  return SENGA_OK;
+}
+
+// Post-processing record (src/output.f:240-265): D, u, v, w, E, T, p,
+// Y_1..Y_NSPEC, RRTE(..., 1..NSPCMX) (slots past NSPEC zero), ETIME; one
+// sequential unformatted record, no size header.
+extern "C" int senga_post_write(const char* path, int nx, int ny, int nz, int nspec, int nspcmx, const double* post,
+                                double etime) {
+  if (!path || !post || nx < 1 || ny < 1 || nz < 1 || nspec < 1 || nspcmx < nspec)
+    return fail(SENGA_ERR_ARG, "senga_post_write: bad argument");
+  const int64_t n = (int64_t)nx * ny * nz;
+  std::vector<char> rec((size_t)((7 + nspec + nspcmx) * n + 1) * 8, 0);
+  std::memcpy(rec.data(), post, (size_t)(7 + 2 * nspec) * n * 8);
+  std::memcpy(rec.data() + (size_t)(7 + nspec + nspcmx) * n * 8, &etime, 8);
+  if (!write_unformatted(path, rec)) return fail(SENGA_ERR_IO, std::string("senga_post_write: cannot write ") + path);
+  return SENGA_OK;
+}
+
+extern "C" int senga_post_read(const char* path, int nx, int ny, int nz, int nspec, int nspcmx, double* post,
+                               double* etime) {
+  if (!path || !post || nx < 1 || ny < 1 || nz < 1 || nspec < 1 || nspcmx < nspec)
+    return fail(SENGA_ERR_ARG, "senga_post_read: bad argument");
+  std::vector<char> rec;
+  if (!read_unformatted(path, rec)) return fail(SENGA_ERR_IO, std::string("senga_post_read: cannot read ") + path);
+  const int64_t n = (int64_t)nx * ny * nz;
+  if ((int64_t)rec.size() != ((7 + nspec + nspcmx) * n + 1) * 8)
+    return fail(SENGA_ERR_IO, "senga_post_read: record size does not match the sizes given");
+  std::memcpy(post, rec.data(), (size_t)(7 + 2 * nspec) * n * 8);
+  if (etime) std::memcpy(etime, rec.data() + (size_t)(7 + nspec + nspcmx) * n * 8, 8);
   return SENGA_OK;
 }
 

@@ -74,6 +74,8 @@ struct senga_ctx {
   bool mixt = false;
   MixtParams mx{};
   double* mixt_pool = nullptr;
+  // CHRATE rates of the last RHS evaluation (RRTE), kept on request
+  double* rrte = nullptr;
   // radiation heat loss (senga_set_radiation)
   bool rad = false;
   RadParams rp{};
@@ -131,6 +133,9 @@ void run_rhs(senga_ctx* c) {
     throw Error(SENGA_ERR_UNSUPPORTED, "a bounded x direction needs its face conditions (senga_set_nscbc)");
   if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->stream);  // BOUNDT
   launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+  if (c->rrte)  // RRTE = RATE (src/rhscal.f:828)
+    CK(cudaMemcpyAsync(c->rrte, c->f.wdot, (size_t)c->nspec * c->geo.n * sizeof(double), cudaMemcpyDeviceToDevice,
+                       c->stream));
   if (c->nscbc) launch_face(c->geo, c->f, c->bc, c->nspec, c->d_chem, c->stream);  // face data + BOUNDS
   launch_flow(c->geo, c->f, c->nspec, c->stream);
   if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);  // RADCAL
@@ -292,6 +297,7 @@ int senga_ctx_destroy(senga_ctx* c) {
   cudaFree(c->d_errmax);
   cudaFree(c->nscbc_pool);
   cudaFree(c->mixt_pool);
+  cudaFree(c->rrte);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SENGA_OK;
@@ -463,6 +469,43 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int senga_keep_rates(senga_ctx* c, int on) {
+  if (!c) return fail(SENGA_ERR_ARG, "senga_keep_rates: null context");
+  return guard([&] {
+    CK(cudaStreamSynchronize(c->stream));
+    if (on && !c->rrte) {
+      CK(cudaMalloc(&c->rrte, (size_t)c->nspec * c->geo.n * sizeof(double)));
+      CK(cudaMemset(c->rrte, 0, (size_t)c->nspec * c->geo.n * sizeof(double)));
+    } else if (!on && c->rrte) {
+      cudaFree(c->rrte);
+      c->rrte = nullptr;
+    }
+    if (c->graph) {
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
+  });
+}
+
+int senga_post_fields_host(senga_ctx* c, double* out) {
+  if (!c || !out) return fail(SENGA_ERR_ARG, "senga_post_fields_host: null argument");
+  if (!c->rrte) return fail(SENGA_ERR_ARG, "senga_post_fields_host: RRTE needs senga_keep_rates(ctx, 1) before the step");
+  return guard([&] {
+    const int64_t n = c->geo.n;
+    const size_t prim = (size_t)(7 + c->nspec) * n;
+    double* d = nullptr;
+    CK(cudaMalloc(&d, prim * sizeof(double)));
+    launch_post(n, c->nspec, c->f.run, c->f.t, c->f.p, d, c->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, prim * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out + prim, c->rrte, (size_t)c->nspec * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d);
+    CK(e);
   });
 }
 

@@ -169,6 +169,10 @@ struct MixtParams {
 int launch_mixt(const Geo& g, const Fields& f, const MixtParams& m, const senga_chem* dchem, const senga_diff* ddiff,
                 int nspec, cudaStream_t s);
 
+// Post-processing record fields (post.cu): D, u, v, w, E, T, p, Y_k.
+void launch_post(int64_t n, int nspec, const double* run, const double* t, const double* p, double* out,
+                 cudaStream_t s);
+
 // ADAPTT error maxima (adapt.cu): out[fl] = max |err|/(|run| + nrm.v[fl])
 // as the bit pattern of a non-negative double, per conserved field.
 struct ErrNorms {

@@ -144,6 +144,10 @@ def _load():
         "senga_radn_load": (ip, [C.c_char_p, C.POINTER(ChemT), C.c_double, C.POINTER(RadnT)]),
         "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
         "senga_set_transport": (ip, [vp, ip, ip, ip, ip, C.c_double]),
+        "senga_keep_rates": (ip, [vp, ip]),
+        "senga_post_fields_host": (ip, [vp, dp]),
+        "senga_post_write": (ip, [C.c_char_p, ip, ip, ip, ip, ip, dp, C.c_double]),
+        "senga_post_read": (ip, [C.c_char_p, ip, ip, ip, ip, ip, dp, dp]),
         "senga_server_set_max_points": (ip, [vp, C.c_int64]),
         "senga_dump_write": (ip, [C.c_char_p, ip, ip, ip, ip, ip, ip, dp, dp]),
         "senga_dump_read": (ip, [C.c_char_p, ip, ip, C.POINTER(C.c_int), dp, C.c_int64, dp]),
@@ -205,6 +209,31 @@ def dump_read(path, formatted=False, nspcmx=None):
     _check(lib.senga_dump_read(os.fsencode(path), 1 if formatted else 0, nspcmx or nspec, dims, _dp(f), f.size,
                                _dp(sc)), "senga_dump_read")
     return f, dict(etime=sc[0], tstep=sc[1], errold=sc[2], errldr=sc[3])
+
+
+def post_name(iddump, iproc=0):
+    """File name of a post-processing record: out<IDDUMP:5><IPROC:4>.res."""
+    return f"out{iddump:05d}{iproc:04d}.res"
+
+
+def post_write(path, post, etime=0.0, nspcmx=None):
+    """Write a post-processing record; post: (7 + 2 nspec, nz, ny, nx) as
+    Box.post_fields returns it."""
+    a = np.ascontiguousarray(post, dtype=np.float64)
+    nf, nz, ny, nx = a.shape
+    nspec = (nf - 7) // 2
+    _check(lib.senga_post_write(os.fsencode(path), nx, ny, nz, nspec, nspcmx or nspec, _dp(a), float(etime)),
+           "senga_post_write")
+
+
+def post_read(path, shape, nspec, nspcmx=None):
+    """Read a post-processing record of a (nx, ny, nz) box: (post, etime)."""
+    nx, ny, nz = shape
+    a = np.empty((7 + 2 * nspec, nz, ny, nx))
+    e = C.c_double()
+    _check(lib.senga_post_read(os.fsencode(path), nx, ny, nz, nspec, nspcmx or nspec, _dp(a), C.byref(e)),
+           "senga_post_read")
+    return a, e.value
 
 
 def fp64_peak(device=0):
@@ -410,6 +439,17 @@ class Box:
         Soret and Dufour for species lighter than wmltdr (+1e-3)."""
         _check(lib.senga_set_transport(self.h, int(mixw), int(mixp), int(soret), int(dufour), float(wmltdr)),
                "senga_set_transport")
+
+    def keep_rates(self, on=True):
+        """Keep each substage's CHRATE rates (RRTE) for post_fields."""
+        _check(lib.senga_keep_rates(self.h, 1 if on else 0), "senga_keep_rates")
+
+    def post_fields(self):
+        """Post-processing record fields (7 + 2 nspec, nz, ny, nx): rho, u, v,
+        w, E, T, p, Y_k, RRTE_k (needs keep_rates before the step)."""
+        out = np.empty((7 + 2 * self.nspec,) + self.shape)
+        _check(lib.senga_post_fields_host(self.h, _dp(out)), "senga_post_fields_host")
+        return out
 
     def set_radiation(self, radn):
         """Optically thin radiation loss (RADCAL) on with a Radn, off with None."""
