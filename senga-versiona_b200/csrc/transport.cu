@@ -15,13 +15,14 @@
 //   k_mixt_grad     first derivatives of each logarithm and the sum of its
 //                   second derivatives (x part zeroed on diffusion-flux
 //                   faces, as ZEROXL/XR do to WD2X/PD2X/TD2X);
-//   k_mixt_species  per point, all species: the branch terms, and the
-//                   Dufour part of the main heat-flux terms (the species
-//                   kernel formed those with the plain enthalpy h_k; the
-//                   reference uses h_k + R_k T TDRMIX_k, so the difference,
-//                   linear in the enthalpy, is added here).
-// Neighbour values come from global memory through the read-only cache:
-// these passes are off by default and sit outside the headline step.
+//   k_mixt_species  one launch per kind of term (molar mass, pressure,
+//                   Soret, and the Dufour part of the main heat-flux terms:
+//                   the species kernel formed those with the plain enthalpy
+//                   h_k; the reference uses h_k + R_k T TDRMIX_k, so the
+//                   difference, linear in the enthalpy, is added here), each
+//                   looping over the species of the point.
+// The per-species terms use the tile machinery of the species kernels
+// (shared-memory slabs for x/y, register columns for z).
 //
 // Kept as coded: in the molar-mass and pressure branches the x component of
 // the "species enthalpy gradient" is STORE4, which the code before them
@@ -32,6 +33,7 @@
 #include "senga_gpu.h"
 #include "senga_internal.h"
 #include "stencil.cuh"
+#include "tiles.cuh"
 
 namespace senga {
 namespace {
@@ -89,128 +91,169 @@ __global__ void __launch_bounds__(kMixBlock) k_mixt_grad(Geo g, MixtParams m) {
   }
 }
 
-// value of a pointwise function of the fields at a neighbour, for D1
-template <class Fn>
-struct At {
-  Fn fn;
-  __device__ __forceinline__ double operator()(int64_t q) const { return fn(q); }
-};
-template <class Fn>
-__device__ __forceinline__ At<Fn> at(Fn fn) {
-  return At<Fn>{fn};
-}
+// ---- per-species terms: one tile kernel per kind of term ----------------
+// Tiles of 32 x 8 x 2 points as in the species kernels (tiles.cuh): each
+// field a term differentiates is staged once per tile and species into a
+// shared-memory slab (x, y halos) plus a register column per thread (z
+// halo), the driving diffusivities as products formed while staging.
+constexpr int MX = 32, MY = 8, MZ = 2, MNW = MX * MY / 32;
+using MSlab = tile::Slab<MX, MY, MZ>;
+using MCol = tile::Column<MZ>;
+constexpr int kMixSmem = 3 * MSlab::SIZE;
 
-template <class F>
-__device__ __forceinline__ void grad(const Geo& g, const Pt& pt, const F& acc, bool zero_x, double d[3]) {
-  d[0] = zero_x ? 0.0 : D1<0>(g, pt, acc);
-  d[1] = D1<1>(g, pt, acc);
-  d[2] = D1<2>(g, pt, acc);
-}
-__device__ __forceinline__ double dot(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+enum { kBrW = 0, kBrP = 1, kBrT = 2, kBrDufour = 3 };
 
-__global__ void __launch_bounds__(kMixBlock) k_mixt_species(Geo g, Fields f, MixtParams m, const senga_chem* __restrict__ ch,
-                                                            int nspec) {
-  const int64_t q = (int64_t)blockIdx.x * kMixBlock + threadIdx.x;
-  if (q >= g.n) return;
-  const int64_t n = g.n;
-  const Pt pt = point_of(g, q);
-  const bool dif = !g.per[0] && (face_bits(g, pt.i) & BF_DIF);
-  const double* __restrict__ T = f.t;
-  const double* __restrict__ wm = m.wmix;
-  double gW[3] = {0, 0, 0}, gP[3] = {0, 0, 0}, gT[3] = {0, 0, 0};
-  double lW = 0.0, lP = 0.0, lT = 0.0;
-  for (int d = 0; d < 3; ++d) {
-    if (m.w) gW[d] = m.g1[0][d * n + q];
-    if (m.p) gP[d] = m.g1[1][d * n + q];
-    if (m.t) gT[d] = m.g1[2][d * n + q];
+// DIFMIX * Y_k times a branch factor: 1 (molar mass), 1 - W_k/W_mix
+// (pressure), TDRMIX_k (Soret)
+template <int BR>
+struct DrivingF {
+  const double* __restrict__ rd;
+  const double* __restrict__ y;
+  const double* __restrict__ x;  // W_mix or TDRMIX_k
+  double wk;
+  __device__ __forceinline__ double operator()(int64_t q) const {
+    if (BR == kBrW) return rd[q] * y[q];
+    if (BR == kBrP) return rd[q] * y[q] * (1.0 - wk / x[q]);
+    return rd[q] * y[q] * x[q];
   }
-  if (m.w) lW = m.g2[0][q];
-  if (m.p) lP = m.g2[1][q];
-  if (m.t) lT = m.g2[2][q];
-  double vc[3] = {0.0, 0.0, 0.0}, vt = 0.0, eacc = 0.0;
+};
+// UTMP as the reference holds it: h_k, + R_k T TDRMIX_k with Dufour
+// (mode 1), and that with the Dufour term taken out again (mode 2)
+struct EnthF {
+  const double* __restrict__ h;
+  const double* __restrict__ t;
+  const double* __restrict__ tk;
+  double rg;
+  int mode;
+  __device__ __forceinline__ double operator()(int64_t q) const {
+    if (mode == 0) return h[q];
+    const double dl = rg * t[q] * tk[q];
+    return mode == 1 ? h[q] + dl : (h[q] + dl) - dl;
+  }
+};
+// the Dufour enthalpy increment R_k T TDRMIX_k
+struct DufF {
+  const double* __restrict__ t;
+  const double* __restrict__ tk;
+  double rg;
+  __device__ __forceinline__ double operator()(int64_t q) const { return rg * t[q] * tk[q]; }
+};
+
+template <int BR, bool P>
+__global__ void __launch_bounds__(MX* MY, 2) k_mixt_species(Geo g, Fields f, MixtParams m,
+                                                            const senga_chem* __restrict__ ch, int nspec) {
+  using namespace tile;
+  extern __shared__ double sm[];
+  __shared__ Folds<MX, MY, MZ> fo;
+  const Origin o{(int)blockIdx.x * MX, (int)blockIdx.y * MY, (int)blockIdx.z * MZ};
+  const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
+  fo.init(g, o);
+  tile_sync();
+  TP tp[MZ];
+#pragma unroll
+  for (int z = 0; z < MZ; ++z) tp[z] = make_tp(g, o, tx, ty, z);
+  const int64_t n = g.n;
+  const MSlab bA{sm}, bB{sm + MSlab::SIZE}, bC{sm + 2 * MSlab::SIZE};
+  const int b = BR == kBrW ? 0 : BR == kBrP ? 1 : 2;
+  double gG[MZ][3], lG[MZ], vc[MZ][3], vt[MZ], ea[MZ];
+#pragma unroll
+  for (int z = 0; z < MZ; ++z) {
+    const int64_t q = tp[z].q;
+    for (int d = 0; d < 3; ++d) {
+      gG[z][d] = BR == kBrDufour ? 0.0 : m.g1[b][d * n + q];
+      vc[z][d] = 0.0;
+    }
+    lG[z] = BR == kBrDufour ? 0.0 : m.g2[b][q];
+    vt[z] = 0.0;
+    ea[z] = 0.0;
+  }
+#pragma unroll 1
   for (int k = 0; k < nspec; ++k) {
+    const bool duf = (m.duf >> k) & 1u, sor = (m.sor >> k) & 1u;
+    if (BR == kBrDufour && !duf) continue;
+    if (BR == kBrT && !sor) continue;
     const double* __restrict__ rdk = f.rd + k * n;
     const double* __restrict__ yk = f.y + k * n;
     const double* __restrict__ hk = f.h + k * n;
     const double* __restrict__ tk = m.tdrmix ? m.tdrmix + k * n : nullptr;
-    const bool duf = (m.duf >> k) & 1u, sor = (m.sor >> k) & 1u;
-    const double rg = ch->rgspec[k], wk = ch->wmolar[k];
-    const double rd = rdk[q], y = yk[q], h = hk[q];
-    const double delta = duf ? rg * T[q] * tk[q] : 0.0;
-    const double hp = duf ? h + delta : h;  // UTMP with the Dufour term
-    double src = 0.0;                       // added to RATE
-    double dY[3];
-    if (duf) {
+    const double rg = ch->rgspec[k];
+    tile_sync();
+    if (BR == kBrDufour) {
       // the Dufour part of the main heat-flux terms: (grad rhoD . grad Y) dh,
       // (grad dh . grad Y) rhoD, (rhoD lap Y) dh, dh = R_k T TDRMIX_k
-      grad(g, pt, Ld{yk}, false, dY);
-      double dRD[3], dDl[3];
-      grad(g, pt, Ld{rdk}, dif, dRD);
-      grad(g, pt, at([=](int64_t r) { return rg * T[r] * tk[r]; }), dif, dDl);
-      const Ld Y{yk};
-      const double lapY = (dif ? 0.0 : D2<0>(g, pt, Y)) + D2<1>(g, pt, Y) + D2<2>(g, pt, Y);
-      eacc = eacc + dot(dRD, dY) * delta + dot(dDl, dY) * rd + lapY * rd * delta;
-    }
-    // molar-mass and pressure branches share the enthalpy gradient: x part
-    // DIFMIX (see the file comment), y/z parts those of h_k + Dufour term
-    double hy = 0.0, hz = 0.0;
-    if (m.w || m.p) {
-      if (duf) {
-        const auto hpa = at([=](int64_t r) { return hk[r] + rg * T[r] * tk[r]; });
-        hy = D1<1>(g, pt, hpa);
-        hz = D1<2>(g, pt, hpa);
-      } else {
-        hy = D1<1>(g, pt, Ld{hk});
-        hz = D1<2>(g, pt, Ld{hk});
+      const DufF dl{f.t, tk, rg};
+      MCol cY, cR, cD;
+      cY.load(fo, tx, ty, Ld{yk});
+      cR.load(fo, tx, ty, Ld{rdk});
+      cD.load(fo, tx, ty, dl);
+      bA.stage<MNW>(fo, Ld{yk});
+      bB.stage<MNW>(fo, Ld{rdk});
+      bC.stage<MNW>(fo, dl);
+      tile_sync();
+#pragma unroll
+      for (int z = 0; z < MZ; ++z) {
+        const TP& t = tp[z];
+        const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
+        const double dY[3] = {d1<0, P>(g, t, bA), d1<1, P>(g, t, bA), d1z<P>(g, t, cY)};
+        const double dRD[3] = {dif ? 0.0 : d1<0, P>(g, t, bB), d1<1, P>(g, t, bB), d1z<P>(g, t, cR)};
+        const double dDl[3] = {dif ? 0.0 : d1<0, P>(g, t, bC), d1<1, P>(g, t, bC), d1z<P>(g, t, cD)};
+        const double lapY = (dif ? 0.0 : d2<0, P>(g, t, bA)) + d2<1, P>(g, t, bA) + d2z<P>(g, t, cY);
+        const double rd = cR.c[z + H], delta = cD.c[z + H];
+        ea[z] = ea[z] + (dRD[0] * dY[0] + dRD[1] * dY[1] + dRD[2] * dY[2]) * delta +
+                (dDl[0] * dY[0] + dDl[1] * dY[1] + dDl[2] * dY[2]) * rd + lapY * rd * delta;
       }
+      continue;
     }
-    const double hx = dif ? 0.0 : rd;
-    auto branch = [&](double s7, const double dS[3], const double gG[3], double lG) {
-      for (int d = 0; d < 3; ++d) vc[d] = vc[d] + s7 * gG[d];
-      const double f1 = dot(dS, gG);
-      const double f2 = lG * s7;
-      src = src + f1 + f2;
-      vt = vt + f1 + f2;
-      eacc = eacc + f1 * hp + (hx * gG[0] + hy * gG[1] + hz * gG[2]) * s7 + f2 * hp;
-    };
-    if (m.w) {
-      double dS[3];
-      grad(g, pt, LdMul{rdk, yk}, dif, dS);
-      branch(rd * y, dS, gW, lW);
+    const DrivingF<BR> drv{rdk, yk, BR == kBrP ? m.wmix : tk, ch->wmolar[k]};
+    // W, P: UTMP with the Dufour term; Soret: with it taken out again
+    const EnthF en{hk, f.t, tk, rg, duf ? (BR == kBrT ? 2 : 1) : 0};
+    MCol cA, cB;
+    cA.load(fo, tx, ty, drv);
+    cB.load(fo, tx, ty, en);
+    bA.stage<MNW>(fo, drv);
+    bB.stage<MNW>(fo, en);
+    tile_sync();
+#pragma unroll
+    for (int z = 0; z < MZ; ++z) {
+      const TP& t = tp[z];
+      const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
+      const double s7 = cA.c[z + H], u = cB.c[z + H];
+      const double dS[3] = {dif ? 0.0 : d1<0, P>(g, t, bA), d1<1, P>(g, t, bA), d1z<P>(g, t, cA)};
+      // molar-mass and pressure branches: the x part of the "enthalpy
+      // gradient" is DIFMIX (see the file comment)
+      double dHx;
+      if (BR == kBrT) dHx = dif ? 0.0 : d1<0, P>(g, t, bB);
+      else dHx = dif ? 0.0 : rdk[t.q];
+      const double dH[3] = {dHx, d1<1, P>(g, t, bB), d1z<P>(g, t, cB)};
+      for (int d = 0; d < 3; ++d) vc[z][d] = vc[z][d] + s7 * gG[z][d];
+      const double f1 = dS[0] * gG[z][0] + dS[1] * gG[z][1] + dS[2] * gG[z][2];
+      const double f2 = lG[z] * s7;
+      vt[z] = vt[z] + f1 + f2;
+      ea[z] = ea[z] + f1 * u + (dH[0] * gG[z][0] + dH[1] * gG[z][1] + dH[2] * gG[z][2]) * s7 + f2 * u;
+      if (t.valid) f.wdot[k * n + t.q] += f1 + f2;
     }
-    if (m.p) {
-      double dS[3];
-      grad(g, pt, at([=](int64_t r) { return rdk[r] * yk[r] * (1.0 - wk / wm[r]); }), dif, dS);
-      branch(rd * y * (1.0 - wk / wm[q]), dS, gP, lP);
-    }
-    if (sor) {
-      const double s7 = rd * y * tk[q];
-      double dS[3], dU[3];
-      grad(g, pt, at([=](int64_t r) { return rdk[r] * yk[r] * tk[r]; }), dif, dS);
-      // UTMP with the Dufour term taken out again, and its gradient
-      const double u = duf ? hp - delta : h;
-      if (duf)
-        grad(g, pt, at([=](int64_t r) {
-               const double dl = rg * T[r] * tk[r];
-               return (hk[r] + dl) - dl;
-             }),
-             dif, dU);
-      else
-        grad(g, pt, Ld{hk}, dif, dU);
-      for (int d = 0; d < 3; ++d) vc[d] = vc[d] + s7 * gT[d];
-      const double f1 = dot(dS, gT);
-      const double f2 = lT * s7;
-      src = src + f1 + f2;
-      vt = vt + f1 + f2;
-      eacc = eacc + f1 * u + dot(dU, gT) * s7 + f2 * u;
-    }
-    if (src != 0.0) f.wdot[k * n + q] += src;
   }
-  f.vc[q] += vc[0];
-  f.vc[n + q] += vc[1];
-  f.vc[2 * n + q] += vc[2];
-  f.vtmp[q] += vt;
-  f.rhs[4 * n + q] += eacc;
+#pragma unroll
+  for (int z = 0; z < MZ; ++z) {
+    const TP& t = tp[z];
+    if (!t.valid) continue;
+    if (BR != kBrDufour) {
+      f.vc[t.q] += vc[z][0];
+      f.vc[n + t.q] += vc[z][1];
+      f.vc[2 * n + t.q] += vc[z][2];
+      f.vtmp[t.q] += vt[z];
+    }
+    f.rhs[4 * n + t.q] += ea[z];
+  }
+}
+
+template <int BR>
+void launch_branch(const Geo& g, const Fields& f, const MixtParams& m, const senga_chem* dchem, int nspec,
+                   cudaStream_t s) {
+  const dim3 grid((unsigned)((g.nx + MX - 1) / MX), (unsigned)((g.ny + MY - 1) / MY), (unsigned)((g.nz + MZ - 1) / MZ));
+  const bool per = g.per[0] && g.per[1] && g.per[2];
+  if (per) k_mixt_species<BR, true><<<grid, MX * MY, kMixSmem * 8, s>>>(g, f, m, dchem, nspec);
+  else k_mixt_species<BR, false><<<grid, MX * MY, kMixSmem * 8, s>>>(g, f, m, dchem, nspec);
 }
 
 inline unsigned grid_of(int64_t n) { return (unsigned)((n + kMixBlock - 1) / kMixBlock); }
@@ -226,8 +269,11 @@ int launch_mixt(const Geo& g, const Fields& f, const MixtParams& m, const senga_
     k_mixt_grad<<<gr, kMixBlock, 0, s>>>(g, m);
     ++nl;
   }
-  k_mixt_species<<<gr, kMixBlock, 0, s>>>(g, f, m, dchem, nspec);
-  return nl + 1;
+  if (m.duf) launch_branch<kBrDufour>(g, f, m, dchem, nspec, s), ++nl;
+  if (m.w) launch_branch<kBrW>(g, f, m, dchem, nspec, s), ++nl;
+  if (m.p) launch_branch<kBrP>(g, f, m, dchem, nspec, s), ++nl;
+  if (m.sor) launch_branch<kBrT>(g, f, m, dchem, nspec, s), ++nl;
+  return nl;
 }
 
 }  // namespace senga
