@@ -134,6 +134,14 @@ void* senga_stream(senga_ctx* ctx);
  * and after INDATA (src/indata.f:1540-1565). */
 int senga_upload_state_host(senga_ctx* ctx, const double* fields, const double* trun, const int32_t* itndex);
 int senga_download_state_host(senga_ctx* ctx, double* fields, double* trun, int32_t* itndex);
+/* Stream-ordered forms of the two copies: they return at once, queued on the
+ * context's stream before/after whatever is launched next (senga_step_graph
+ * also returns without waiting). With page-locked host buffers the copies
+ * then run on the copy engines while other contexts compute, so a caller
+ * with a queue of independent boxes keeps the link and the SMs busy at the
+ * same time. The host buffers must stay untouched until senga_sync(ctx). */
+int senga_upload_state_async(senga_ctx* ctx, const double* fields, const double* trun, const int32_t* itndex);
+int senga_download_state_async(senga_ctx* ctx, double* fields, double* trun, int32_t* itndex);
 
 /* One RK substage (irkstp = 1..5): BOUNDT, PARFER, RHSCAL, RHSVEL, BOUNDS and
  * LINCOM (irkstp < 5) or FINCOM (irkstp = 5): src/senga2.f:113-159. */

@@ -323,6 +323,28 @@ int senga_upload_state_host(senga_ctx* c, const double* fields, const double* tr
   });
 }
 
+int senga_upload_state_async(senga_ctx* c, const double* fields, const double* trun, const int32_t* itn) {
+  if (!c || !fields || !trun || !itn) return fail(SENGA_ERR_ARG, "senga_upload_state_async: null argument");
+  return guard([&] {
+    const size_t bytes = (size_t)c->nc * c->geo.n * sizeof(double);
+    CK(cudaMemcpyAsync(c->f.run, fields, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.uin, c->f.run, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.t, trun, c->geo.n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.itn, itn, c->geo.n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    if (c->f.err) CK(cudaMemsetAsync(c->f.err, 0, bytes, c->stream));
+  });
+}
+
+int senga_download_state_async(senga_ctx* c, double* fields, double* trun, int32_t* itn) {
+  if (!c || !fields) return fail(SENGA_ERR_ARG, "senga_download_state_async: null argument");
+  return guard([&] {
+    const size_t bytes = (size_t)c->nc * c->geo.n * sizeof(double);
+    CK(cudaMemcpyAsync(fields, c->f.run, bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (trun) CK(cudaMemcpyAsync(trun, c->f.t, c->geo.n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (itn) CK(cudaMemcpyAsync(itn, c->f.itn, c->geo.n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  });
+}
+
 int senga_download_state_host(senga_ctx* c, double* fields, double* trun, int32_t* itn) {
   if (!c || !fields) return fail(SENGA_ERR_ARG, "senga_download_state_host: null argument");
   return guard([&] {

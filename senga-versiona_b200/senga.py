@@ -145,6 +145,8 @@ def _load():
         "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
         "senga_set_transport": (ip, [vp, ip, ip, ip, ip, C.c_double]),
         "senga_keep_rates": (ip, [vp, ip]),
+        "senga_upload_state_async": (ip, [vp, dp, dp, i32p]),
+        "senga_download_state_async": (ip, [vp, dp, dp, i32p]),
         "senga_post_fields_host": (ip, [vp, dp]),
         "senga_post_write": (ip, [C.c_char_p, ip, ip, ip, ip, ip, dp, C.c_double]),
         "senga_post_read": (ip, [C.c_char_p, ip, ip, ip, ip, ip, dp, dp]),
@@ -439,6 +441,25 @@ class Box:
         Soret and Dufour for species lighter than wmltdr (+1e-3)."""
         _check(lib.senga_set_transport(self.h, int(mixw), int(mixp), int(soret), int(dufour), float(wmltdr)),
                "senga_set_transport")
+
+    def upload_async(self, fields, trun, itndex):
+        """Queue the upload on the box's stream and return; the arrays (C
+        contiguous, ideally page-locked) must stay alive and unchanged until
+        sync()."""
+        for a, dt in ((fields, np.float64), (trun, np.float64), (itndex, np.int32)):
+            assert a.dtype == dt and a.flags.c_contiguous
+        assert fields.shape == (self.nc,) + self.shape and trun.shape == self.shape and itndex.shape == self.shape
+        _check(lib.senga_upload_state_async(self.h, _dp(fields), _dp(trun),
+                                            itndex.ctypes.data_as(C.POINTER(C.c_int32))), "senga_upload_state_async")
+
+    def download_async(self, fields, trun, itndex):
+        """Queue the download into caller arrays and return; read them after
+        sync()."""
+        for a, dt in ((fields, np.float64), (trun, np.float64), (itndex, np.int32)):
+            assert a.dtype == dt and a.flags.c_contiguous and a.flags.writeable
+        assert fields.shape == (self.nc,) + self.shape and trun.shape == self.shape and itndex.shape == self.shape
+        _check(lib.senga_download_state_async(self.h, _dp(fields), _dp(trun),
+                                              itndex.ctypes.data_as(C.POINTER(C.c_int32))), "senga_download_state_async")
 
     def keep_rates(self, on=True):
         """Keep each substage's CHRATE rates (RRTE) for post_fields."""
