@@ -181,7 +181,7 @@ def ignition_box(shape_xyz, seed, uprime, tpeak, chem_path=CHEM_1STEP):
                 fields=fields, T=T, itn=itn, dt=dt, nend=(NPERI,) * 6)
 
 
-def make_case(name, n=None, seed=1234, scale_n=None):
+def make_case(name, n=None, seed=1234, scale_n=None, shape=None):
     """Named workloads. Returns dict with shape (nx,ny,nz), lengths, chem/diff
     paths, fields (nc,nz,ny,nx), T, itn and a CFL-0.5 dt.
 
@@ -209,7 +209,8 @@ def make_case(name, n=None, seed=1234, scale_n=None):
                   burnt mixture holding H, O, OH, HO2, H2O2, and a 5%
                   sinusoidal pressure modulation, so that the molar-mass,
                   pressure, Soret and Dufour terms are all active.
-    `n` overrides the grid extent (cubic) for smaller test instances.
+    `n` overrides the grid extent (cubic) for smaller test instances;
+    `shape` = (nx, ny, nz) gives h2_pool and flame_inout a non-cubic grid.
     """
     from senga import Chem  # noqa: local import keeps this module numpy-only
     rng = np.random.default_rng(seed)
@@ -246,12 +247,12 @@ def make_case(name, n=None, seed=1234, scale_n=None):
         p = np.full(shp, 101325.0)
     elif name == "flame_inout":
         nn = n or 128
-        shape_xyz = (nn, nn, nn)
+        shape_xyz = tuple(shape) if shape else (nn, nn, nn)
         L = 1.0e-2
         lengths = (L, L, L)
         chem_path, diff_path = CHEM_H2, DIFF_H2
         chem = Chem(chem_path)
-        shp = (nn, nn, nn)
+        shp = shape_xyz[::-1]
         wm = chem.table("wmolar")
         yu = np.zeros(9)
         yu[0], yu[1], yu[8] = 1.1606960e-2, 2.30295282e-1, 7.58097758e-1  # input/cont.dat defaults
@@ -260,7 +261,7 @@ def make_case(name, n=None, seed=1234, scale_n=None):
         yb[0] = 0.0
         yb[1] = yu[1] - 0.5 * nh2 * wm[1]
         yb[2] = nh2 * wm[2]
-        x = np.arange(nn) * (L / (nn - 1))
+        x = np.arange(shape_xyz[0]) * (L / (shape_xyz[0] - 1))
         prog = 0.5 * (1.0 + np.tanh((x - 3.0e-3) / 0.5e-3))
         prog3 = np.broadcast_to(prog, shp)
         T = 300.0 + (1350.0 - 300.0) * prog3
@@ -278,12 +279,12 @@ def make_case(name, n=None, seed=1234, scale_n=None):
                     itn=itn, dt=dt, nend=(1, 1, NPERI, NPERI, NPERI, NPERI), bc=bc)
     elif name == "h2_pool":
         nn = n or 32
-        shape_xyz = (nn, nn, nn)
+        shape_xyz = tuple(shape) if shape else (nn, nn, nn)
         L = 1.0e-2
         lengths = (L, L, L)
         chem_path, diff_path = CHEM_H2, DIFF_H2
         chem = Chem(chem_path)
-        shp = (nn, nn, nn)
+        shp = shape_xyz[::-1]
         centres = [tuple(rng.uniform(0.0, L, size=3)) for _ in range(4)]
         T = hot_kernels(shp, lengths, centres, 1.0e-3, 800.0, 1600.0)
         prog = (T - 800.0) / 800.0
