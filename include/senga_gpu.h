@@ -287,6 +287,18 @@ int senga_dump_write(const char* path, int formatted, int nx, int ny, int nz, in
 int senga_dump_read(const char* path, int formatted, int nspcmx, int* dims, double* fields, int64_t capacity,
                     double* scalars);
 
+/* ---- initial turbulence ---------------------------------------------------
+ * TURBIN (src/turbin.f:76-362, with TURBFT/FFTSYM and ESPECT/ESPINI) for one
+ * box on the current device: a solenoidal velocity field built in
+ * wavenumber space (Rogallo) from the RANINI/RANUNI stream seeded with
+ * inseed, spectrum E(k) = const0/ck0 (k/ck0)^4 exp(-2 (k/ck0)^2) in integer
+ * wavenumbers (SPARAM(1), SPARAM(2) of cont.dat), then transformed to
+ * physical space. uvw receives 3 arrays (u, v, w; x fastest) of
+ * nx*ny*nz doubles, the field TURBIN leaves in URUN/VRUN/WRUN before INDATA
+ * adds the mean velocity (src/indata.f:1111-1141); imag_max (optional) the
+ * largest imaginary part left by the transform. Extents 2..1024. */
+int senga_turbin_host(int nx, int ny, int nz, int inseed, double const0, double ck0, double* uvw, double* imag_max);
+
 /* ---- post-processing output ------------------------------------------------
  * The record written every NTDUMP steps for post-processing
  * (src/output.f:240-265, file output/out<IDDUMP:5><IPROC:4>.res): DRUN,

@@ -64,6 +64,8 @@ def _get():
         lib.oracle_set_adaptive.argtypes = [C.c_void_p, C.c_int]
         lib.oracle_set_radiation.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
         lib.oracle_post.argtypes = [C.c_void_p, dp]
+        lib.oracle_turbin.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dp, dp]
+        lib.oracle_ranuni.argtypes = [C.c_int, C.c_int64, dp]
         lib.oracle_set_transport.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
         lib.oracle_set_bc.argtypes = [C.c_void_p, C.POINTER(_Bc)]
         lib.oracle_tstep.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int)]
@@ -205,3 +207,21 @@ class Oracle:
         v = C.c_double()
         _get().oracle_chem_scalar(self.h, name.encode(), C.byref(v))
         return v.value
+
+
+def turbin(shape, inseed, const0, ck0):
+    """TURBIN's velocity field for an (nx, ny, nz) box: (uvw (3, nz, ny, nx),
+    imaginary parts left by the transform)."""
+    nx, ny, nz = shape
+    uvw = np.empty((3, nz, ny, nx))
+    im = np.empty((3, nz, ny, nx))
+    _get().oracle_turbin(nx, ny, nz, int(inseed), float(const0), float(ck0), _dp(uvw), _dp(im))
+    return uvw, im
+
+
+def ranuni(iseed, n):
+    """The first n draws of RANUNI after RANINI(iseed)."""
+    out = np.empty(n)
+    _get().oracle_ranuni(int(iseed), int(n), _dp(out))
+    return out
+

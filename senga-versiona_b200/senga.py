@@ -145,6 +145,7 @@ def _load():
         "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
         "senga_set_transport": (ip, [vp, ip, ip, ip, ip, C.c_double]),
         "senga_keep_rates": (ip, [vp, ip]),
+        "senga_turbin_host": (ip, [ip, ip, ip, ip, C.c_double, C.c_double, dp, dp]),
         "senga_upload_state_async": (ip, [vp, dp, dp, i32p]),
         "senga_download_state_async": (ip, [vp, dp, dp, i32p]),
         "senga_post_fields_host": (ip, [vp, dp]),
@@ -211,6 +212,17 @@ def dump_read(path, formatted=False, nspcmx=None):
     _check(lib.senga_dump_read(os.fsencode(path), 1 if formatted else 0, nspcmx or nspec, dims, _dp(f), f.size,
                                _dp(sc)), "senga_dump_read")
     return f, dict(etime=sc[0], tstep=sc[1], errold=sc[2], errldr=sc[3])
+
+
+def turbin(shape, inseed=1, const0=8.51064, ck0=5.0):
+    """Initial turbulence of TURBIN on the device for an (nx, ny, nz) box:
+    ((3, nz, ny, nx) velocity, largest imaginary part left)."""
+    nx, ny, nz = shape
+    uvw = np.empty((3, nz, ny, nx))
+    im = C.c_double()
+    _check(lib.senga_turbin_host(nx, ny, nz, int(inseed), float(const0), float(ck0), _dp(uvw), C.byref(im)),
+           "senga_turbin_host")
+    return uvw, im.value
 
 
 def post_name(iddump, iproc=0):
