@@ -380,15 +380,51 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         const double yq = cy.c[z + H];
         double r = f.wdot[s * n + t.q];
         r = r - 0.5 * yq * dvm[z];
-        r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1zp<P>(g, t, cy, rw));
-        yx[z] = d1<0, P>(g, t, bS);
-        yy[z] = d1<1, P>(g, t, bS);
-        yz[z] = d1z<P>(g, t, cy);
-        r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * rw.c[z + H]);
-        rate[z] = r;
-        // FxxDIF/FxxADB zero the x diffusive terms on the face plane (rhscal.f:1581-1955)
-        const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
-        fn3[z] = (dif ? 0.0 : d2<0, P>(g, t, bS)) + d2<1, P>(g, t, bS) + d2z<P>(g, t, cy);  // Laplacian for now
+        if constexpr (P) {
+          // all periodic: each staged neighbour of Y, rho u, rho v read once
+          // into registers and shared by the flux, first and second
+          // derivatives (same arithmetic as the generic path)
+          double d1px, d1py, d2x, d2y, uc, vc;
+          {
+            double yv[2 * H + 1], fv[2 * H + 1];
+#pragma unroll
+            for (int m = 0; m <= 2 * H; ++m) {
+              yv[m] = bS.v(t.x + m - H, t.y, t.z);
+              fv[m] = bru.v(t.x + m - H, t.y, t.z);
+            }
+            d1px = d1core([&](int m) { return yv[m + H] * fv[m + H]; }, t.gx, g.nx, 1) * g.ovd[0];
+            yx[z] = d1core([&](int m) { return yv[m + H]; }, t.gx, g.nx, 1) * g.ovd[0];
+            d2x = d2core([&](int m) { return yv[m + H]; }, t.gx, g.nx, 1) * g.ovd2[0];
+            uc = fv[H];
+          }
+          {
+            double yv[2 * H + 1], fv[2 * H + 1];
+#pragma unroll
+            for (int m = 0; m <= 2 * H; ++m) {
+              yv[m] = bS.v(t.x, t.y + m - H, t.z);
+              fv[m] = brv.v(t.x, t.y + m - H, t.z);
+            }
+            d1py = d1core([&](int m) { return yv[m + H] * fv[m + H]; }, t.gy, g.ny, 1) * g.ovd[1];
+            yy[z] = d1core([&](int m) { return yv[m + H]; }, t.gy, g.ny, 1) * g.ovd[1];
+            d2y = d2core([&](int m) { return yv[m + H]; }, t.gy, g.ny, 1) * g.ovd2[1];
+            vc = fv[H];
+          }
+          r = r - 0.5 * (d1px + d1py + d1zp<P>(g, t, cy, rw));
+          yz[z] = d1z<P>(g, t, cy);
+          r = r - 0.5 * (yx[z] * uc + yy[z] * vc + yz[z] * rw.c[z + H]);
+          rate[z] = r;
+          fn3[z] = d2x + d2y + d2z<P>(g, t, cy);  // Laplacian for now
+        } else {
+          r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1zp<P>(g, t, cy, rw));
+          yx[z] = d1<0, P>(g, t, bS);
+          yy[z] = d1<1, P>(g, t, bS);
+          yz[z] = d1z<P>(g, t, cy);
+          r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * rw.c[z + H]);
+          rate[z] = r;
+          // FxxDIF/FxxADB zero the x diffusive terms on the face plane (rhscal.f:1581-1955)
+          const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
+          fn3[z] = (dif ? 0.0 : d2<0, P>(g, t, bS)) + d2<1, P>(g, t, bS) + d2z<P>(g, t, cy);  // Laplacian for now
+        }
       }
       tile_sync();
     }
