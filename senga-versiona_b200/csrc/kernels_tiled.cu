@@ -47,7 +47,7 @@ using SSlab = Slab<SX_, SY_, SZ_>;
 using SXRow = XRow<SX_, SY_, SZ_>;
 using SYRow = YRow<SX_, SY_, SZ_>;
 using SCol = Column<SZ_>;
-constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + SSlab::SIZE;
+constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 2 * SSlab::SIZE;
 constexpr int kSpecRkSmem = SSlab::SIZE;
 
 template <bool P>
@@ -355,6 +355,7 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
   const SXRow bru{sm};
   const SYRow brv{sm + SXRow::SIZE};
   const SSlab bS{sm + SXRow::SIZE + SYRow::SIZE};
+  const SSlab bH{sm + SXRow::SIZE + SYRow::SIZE + SSlab::SIZE};
   bru.stage<SNW>(fo, Ld{U + n});
   brv.stage<SNW>(fo, Ld{U + 2 * n});
   SCol rw;
@@ -428,11 +429,15 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       }
       tile_sync();
     }
-    // rho D_k: correction velocity, diffusive flux divergence
+    // rho D_k and h_k staged together (one barrier pair): correction
+    // velocity, diffusive flux divergence, enthalpy fluxes of the energy
+    // equation
     {
-      SCol cd;
+      SCol cd, ch;
       cd.load(fo, tx, ty, Ld{f.rd + s * n});
+      ch.load(fo, tx, ty, Ld{f.h + s * n});
       bS.stage<SNW>(fo, Ld{f.rd + s * n});
+      bH.stage<SNW>(fo, Ld{f.h + s * n});
       tile_sync();
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
@@ -451,22 +456,9 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         rate[z] = rate[z] + f3;
         vt[z] = vt[z] + f3;
         fn3[z] = f3;
-      }
-      tile_sync();
-    }
-    // h_k: enthalpy fluxes of the energy equation
-    {
-      SCol ch;
-      ch.load(fo, tx, ty, Ld{f.h + s * n});
-      bS.stage<SNW>(fo, Ld{f.h + s * n});
-      tile_sync();
-#pragma unroll
-      for (int z = 0; z < SZ_; ++z) {
-        const TP& t = tp[z];
         const double hk = ch.c[z + H];
         rE[z] = rE[z] + fn1[z] * hk;
-        const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
-        const double fn2 = (dif ? 0.0 : d1<0, P>(g, t, bS) * yx[z]) + d1<1, P>(g, t, bS) * yy[z] +
+        const double fn2 = (dif ? 0.0 : d1<0, P>(g, t, bH) * yx[z]) + d1<1, P>(g, t, bH) * yy[z] +
                            d1z<P>(g, t, ch) * yz[z];
         rE[z] = rE[z] + fn2 * rd[z];
         rE[z] = rE[z] + fn3[z] * hk;
