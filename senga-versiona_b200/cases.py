@@ -82,6 +82,33 @@ def conserved(chem, p, T, u, v, w, Y):
     return fields, itn
 
 
+def temperature_from_state(chem, fields, tlo=200.0, thi=4000.0, iters=60):
+    """T and ITNDEX of a conserved state by bisection on
+    E(T) = sum_k Y_k h_k(T) - R_mix T + |u|^2 / 2 (the robust inversion
+    TEMPIN performs at start-up, src/tempin.f), for restart dumps, which
+    carry no temperature."""
+    rho = fields[0]
+    Y = fields[5:5 + chem.nspec] / rho
+    ke = 0.5 * (fields[1] ** 2 + fields[2] ** 2 + fields[3] ** 2) / (rho * rho)
+    e = fields[4] / rho - ke
+    rg = chem.table("rgspec")
+    rmix = sum(rg[s] * Y[s] for s in range(chem.nspec))
+
+    def energy(T):
+        itn = interval_index(chem, T)
+        return sum(species_enthalpy(chem, s, T, itn) * Y[s] for s in range(chem.nspec)) - rmix * T
+
+    lo = np.full(rho.shape, tlo)
+    hi = np.full(rho.shape, thi)
+    for _ in range(iters):
+        mid = 0.5 * (lo + hi)
+        up = energy(mid) < e
+        lo = np.where(up, mid, lo)
+        hi = np.where(up, hi, mid)
+    T = 0.5 * (lo + hi)
+    return T, interval_index(chem, T)
+
+
 def passot_pouquet(shape, lengths, uprime, lint, seed):
     """Solenoidal random-phase velocity (u, v, w) with a Passot-Pouquet
     spectrum, rms per component = uprime, integral scale lint [m]."""

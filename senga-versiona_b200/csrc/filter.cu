@@ -59,7 +59,10 @@ __global__ void __launch_bounds__(kFiltBlock) k_filter(Geo g, const double* __re
   const int64_t st = DIR == 0 ? 1 : DIR == 1 ? (int64_t)g.nx : (int64_t)g.nx * g.ny;
   const double* base = in + (q - (int64_t)cc * st);  // the line through q
   auto f = [&](int a) {  // a = 0-based coordinate along DIR
-    if (g.per[DIR]) a = a < 0 ? a + n : (a >= n ? a - n : a);
+    if (g.per[DIR]) {  // any extent, one-point directions included
+      a %= n;
+      if (a < 0) a += n;
+    }
     return base[(int64_t)a * st];
   };
   double v;

@@ -107,10 +107,11 @@ void check_config(const senga_config& c, int nspec) {
   const int n3[3] = {c.nx, c.ny, c.nz};
   for (int d = 0; d < 3; ++d) {
     const int l = c.nend[2 * d], r = c.nend[2 * d + 1];
-    // periodic: the 13-point filter wraps once (6 points); bounded: the
-    // filter's one-sided rows read 12 points, the derivative closures 11
-    if (n3[d] < (l == SENGA_NPERI ? 6 : 12))
-      throw Error(SENGA_ERR_ARG, "grid extent must be at least 6 points per periodic and 12 per bounded direction");
+    // periodic: any extent (one point for the unused directions of 1D and
+    // 2D runs: every derivative there is zero, the filter the identity);
+    // bounded: the filter's one-sided rows read 12 points, the closures 11
+    if (n3[d] < (l == SENGA_NPERI ? 1 : 12))
+      throw Error(SENGA_ERR_ARG, "grid extent must be at least 12 points per bounded direction");
     if ((l == SENGA_NPERI) != (r == SENGA_NPERI))
       throw Error(SENGA_ERR_ARG, "periodic end conditions must be set on both faces of a direction");
     if (l != SENGA_NPERI && (d != 0 || l != SENGA_NBOUND || r != SENGA_NBOUND))

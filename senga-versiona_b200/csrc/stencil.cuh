@@ -58,7 +58,12 @@ template <int DIR>
 __device__ __forceinline__ int64_t woff(const Geo& g, int c, int m) {
   const int n = ext<DIR>(g);
   int cm = c + m;
-  cm = cm < 0 ? cm + n : (cm >= n ? cm - n : cm);
+  if (n > 5) {
+    cm = cm < 0 ? cm + n : (cm >= n ? cm - n : cm);
+  } else {  // short periodic extents (a one-point direction of a 1D or 2D box)
+    cm %= n;
+    if (cm < 0) cm += n;
+  }
   return (int64_t)(cm - c) * strd<DIR>(g);
 }
 

@@ -168,13 +168,18 @@ def oracle_fixtures():
 
 
 def casefile_dump():
-    """The reference's formatted restart input of its 1-step case
+    """The reference's formatted restart inputs: its 1-step case
     (src/casefiles/1step/dmpi0000000.dat, 1001 x 1 x 1 points, 2 species),
-    copied as a parser fixture."""
+    copied as a parser fixture, and its 21-step H2/air case
+    (src/casefiles/21step/dmpi0000000.dat, the same grid, 9 species: a
+    freely propagating 1D flame that the case restarts from with inflow at
+    2.05 m/s, NSCBC I3/O1 x faces and every transport switch on)."""
     import shutil
 
     shutil.copyfile(os.path.join(REF, "casefiles", "1step", "dmpi0000000.dat"),
                     os.path.join(HERE, "dmpi_1step_1001.dat"))
+    shutil.copyfile(os.path.join(REF, "casefiles", "21step", "dmpi0000000.dat"),
+                    os.path.join(HERE, "dmpi_21step_1001.dat"))
 
 
 def main():

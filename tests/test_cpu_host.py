@@ -75,8 +75,8 @@ def test_bad_inputs_return_status_not_abort():
     diff = senga.Diff(None, chem)
     with pytest.raises(senga.SengaError, match="status 5"):
         senga.Box((16, 16, 16), (1e-3,) * 3, chem, diff, 1e-8, nend=(2, 2, 1, 1, 2, 2))
-    with pytest.raises(senga.SengaError, match="status 1"):
-        senga.Box((16, 16, 5), (1e-3,) * 3, chem, diff, 1e-8)
+    with pytest.raises(senga.SengaError, match="status 1"):  # bounded x needs 12 points
+        senga.Box((11, 16, 16), (1e-3,) * 3, chem, diff, 1e-8, nend=(1, 1, 2, 2, 2, 2))
 
 
 def test_integf_spectrum_moment():
