@@ -173,13 +173,18 @@ def casefile_dump():
     copied as a parser fixture, and its 21-step H2/air case
     (src/casefiles/21step/dmpi0000000.dat, the same grid, 9 species: a
     freely propagating 1D flame that the case restarts from with inflow at
-    2.05 m/s, NSCBC I3/O1 x faces and every transport switch on)."""
+    2.05 m/s, NSCBC I3/O1 x faces and every transport switch on), and the
+    1-step and 4-step cases' mechanisms (with the 4-step restart state)."""
     import shutil
 
     shutil.copyfile(os.path.join(REF, "casefiles", "1step", "dmpi0000000.dat"),
                     os.path.join(HERE, "dmpi_1step_1001.dat"))
     shutil.copyfile(os.path.join(REF, "casefiles", "21step", "dmpi0000000.dat"),
                     os.path.join(HERE, "dmpi_21step_1001.dat"))
+    # the 1-step and 4-step cases' own mechanisms and the 4-step restart state
+    for src, dst in (("1step/chem.dat", "casefile_1step_chem.dat"), ("4step/chem.dat", "casefile_4step_chem.dat"),
+                     ("4step/diff.dat", "casefile_4step_diff.dat"), ("4step/dmpi0000000.dat", "dmpi_4step_1001.dat")):
+        shutil.copyfile(os.path.join(REF, "casefiles", src), os.path.join(HERE, dst))
 
 
 def main():
