@@ -48,7 +48,7 @@ using SXRow = XRow<SX_, SY_, SZ_>;
 using SYRow = YRow<SX_, SY_, SZ_>;
 using SCol = Column<SZ_>;
 constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 2 * SSlab::SIZE;
-constexpr int kSpecRkSmem = SSlab::SIZE;
+constexpr int kSpecRkSmem = 2 * SSlab::SIZE;
 
 template <bool P>
 __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const Origin o, double* sm,
@@ -527,11 +527,15 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     vcz[z] = f.vc[2 * n + q];
     vt[z] = f.vtmp[q];
   }
+  // two slabs in turn: while one species' Y is differentiated, the next
+  // one's copy (cp.async) is in flight into the other
+  auto slab = [&](int i) { return SSlab{(i & 1) ? sm : sm + SSlab::SIZE}; };
   {
     SCol cm;
     cm.load(fo, tx, ty, Ld{f.hmix});
     bS.stage<SNW>(fo, Ld{f.hmix});
     tile_sync();
+    if (nspec > 0) slab(0).stage<SNW>(fo, Ld{f.y});
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
@@ -548,19 +552,20 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     }
   }
   for (int s = 0; s < nspec; ++s) {
-    tile_sync();
     SCol cy;
     cy.load(fo, tx, ty, Ld{f.y + s * n});
-    bS.stage<SNW>(fo, Ld{f.y + s * n});
+    // Y_s has landed in slab(s); every thread is done with the other slab
     tile_sync();
+    if (s + 1 < nspec) slab(s + 1).stage<SNW>(fo, Ld{f.y + (s + 1) * n});
+    const SSlab bY = slab(s);
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
       if (!t.valid) continue;
       const int bf = P ? 0 : face_bits(g, t.gx);
       const bool dif = bf & BF_DIF;  // rhscal.f:3919: x gradient of Y zeroed on the face
-      const double R = f.wdot[s * n + t.q] - cy.c[z + H] * vt[z] - (dif ? 0.0 : d1<0, P>(g, t, bS) * vcx[z]) -
-                       d1<1, P>(g, t, bS) * vcy[z] - d1z<P>(g, t, cy) * vcz[z];
+      const double R = f.wdot[s * n + t.q] - cy.c[z + H] * vt[z] - (dif ? 0.0 : d1<0, P>(g, t, bY) * vcx[z]) -
+                       d1<1, P>(g, t, bY) * vcy[z] - d1z<P>(g, t, cy) * vcz[z];
       advance(5 + s, t, bf, R);
     }
   }
