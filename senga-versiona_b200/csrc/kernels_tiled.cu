@@ -47,7 +47,7 @@ using SSlab = Slab<SX_, SY_, SZ_>;
 using SXRow = XRow<SX_, SY_, SZ_>;
 using SYRow = YRow<SX_, SY_, SZ_>;
 using SCol = Column<SZ_>;
-constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 2 * SSlab::SIZE;
+constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 3 * SSlab::SIZE;
 constexpr int kSpecRkSmem = 2 * SSlab::SIZE;
 
 template <bool P>
@@ -356,8 +356,12 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
   const SYRow brv{sm + SXRow::SIZE};
   const SSlab bS{sm + SXRow::SIZE + SYRow::SIZE};
   const SSlab bH{sm + SXRow::SIZE + SYRow::SIZE + SSlab::SIZE};
+  const SSlab bR{sm + SXRow::SIZE + SYRow::SIZE + 2 * SSlab::SIZE};
   bru.stage<SNW>(fo, Ld{U + n});
   brv.stage<SNW>(fo, Ld{U + 2 * n});
+  // copies run one stage ahead: Y_s while the previous species' rho D and
+  // h are used, rho D and h of species s while Y_s is used
+  if (nspec > 0) bS.stage<SNW>(fo, Ld{f.y});
   SCol rw;
   rw.load(fo, tx, ty, Ld{U + 3 * n});
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
@@ -373,8 +377,9 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
     {
       SCol cy;
       cy.load(fo, tx, ty, Ld{f.y + s * n});
-      bS.stage<SNW>(fo, Ld{f.y + s * n});
-      tile_sync();
+      tile_sync();  // Y_s has landed in bS; the rho D and h slabs are free
+      bR.stage<SNW>(fo, Ld{f.rd + s * n});
+      bH.stage<SNW>(fo, Ld{f.h + s * n});
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -427,7 +432,6 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
           fn3[z] = (dif ? 0.0 : d2<0, P>(g, t, bS)) + d2<1, P>(g, t, bS) + d2z<P>(g, t, cy);  // Laplacian for now
         }
       }
-      tile_sync();
     }
     // rho D_k and h_k staged together (one barrier pair): correction
     // velocity, diffusive flux divergence, enthalpy fluxes of the energy
@@ -436,9 +440,8 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       SCol cd, ch;
       cd.load(fo, tx, ty, Ld{f.rd + s * n});
       ch.load(fo, tx, ty, Ld{f.h + s * n});
-      bS.stage<SNW>(fo, Ld{f.rd + s * n});
-      bH.stage<SNW>(fo, Ld{f.h + s * n});
-      tile_sync();
+      tile_sync();  // rho D_s, h_s have landed; every thread is done with Y_s
+      if (s + 1 < nspec) bS.stage<SNW>(fo, Ld{f.y + (s + 1) * n});
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -447,7 +450,7 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         vcy[z] = vcy[z] + rd[z] * yy[z];
         vcz[z] = vcz[z] + rd[z] * yz[z];
         const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
-        const double fn = (dif ? 0.0 : d1<0, P>(g, t, bS) * yx[z]) + d1<1, P>(g, t, bS) * yy[z] +
+        const double fn = (dif ? 0.0 : d1<0, P>(g, t, bR) * yx[z]) + d1<1, P>(g, t, bR) * yy[z] +
                           d1z<P>(g, t, cd) * yz[z];
         rate[z] = rate[z] + fn;
         vt[z] = vt[z] + fn;
@@ -464,7 +467,6 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
         rE[z] = rE[z] + fn3[z] * hk;
         if (t.valid) f.wdot[s * n + t.q] = rate[z];
       }
-      tile_sync();
     }
   }
 #pragma unroll
