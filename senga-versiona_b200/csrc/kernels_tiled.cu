@@ -641,17 +641,21 @@ dim3 tiles(const Geo& g, int tx, int ty, int tz) {
   return dim3((unsigned)((g.nx + tx - 1) / tx), (unsigned)((g.ny + ty - 1) / ty), (unsigned)((g.nz + tz - 1) / tz));
 }
 
+// Shared-memory opt-in per kernel, once per device (the attribute belongs
+// to the current device's context).
 template <bool P>
 void set_attrs() {
-  static bool done = false;
-  if (done) return;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  if (done[dev]) return;
   cudaFuncSetAttribute(k_flow_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
   cudaFuncSetAttribute(k_species_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
   cudaFuncSetAttribute(k_species_rk_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
   cudaFuncSetAttribute(k_flow_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
   cudaFuncSetAttribute(k_species_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
   cudaFuncSetAttribute(k_species_rk_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
-  done = true;
+  done[dev] = true;
 }
 
 bool all_periodic(const Geo& g) { return g.per[0] && g.per[1] && g.per[2]; }
