@@ -181,6 +181,9 @@ def casefile_dump():
                     os.path.join(HERE, "dmpi_1step_1001.dat"))
     shutil.copyfile(os.path.join(REF, "casefiles", "21step", "dmpi0000000.dat"),
                     os.path.join(HERE, "dmpi_21step_1001.dat"))
+    # the same case's constant-Lewis-number flame (dmpi0000000_cle.dat)
+    shutil.copyfile(os.path.join(REF, "casefiles", "21step", "dmpi0000000_cle.dat"),
+                    os.path.join(HERE, "dmpi_21step_cle_1001.dat"))
     # the 1-step and 4-step cases' own mechanisms and the 4-step restart state
     for src, dst in (("1step/chem.dat", "casefile_1step_chem.dat"), ("4step/chem.dat", "casefile_4step_chem.dat"),
                      ("4step/diff.dat", "casefile_4step_diff.dat"), ("4step/dmpi0000000.dat", "dmpi_4step_1001.dat")):
