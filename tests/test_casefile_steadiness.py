@@ -11,7 +11,8 @@ equations finds it a small fraction of the inflow velocity (the flame
 stands still in the frame where the reference converged it), while the
 other transport model moves it by 15-25% of the inflow speed. This pins the
 oracle (chemistry, transport, NSCBC faces, derivative closures) against
-outputs of the reference itself, at the level of the flame speed."""
+outputs of the reference itself, at the level of the flame speed; the GPU
+test repeats the check through the product's C ABI."""
 import os
 
 import numpy as np
@@ -21,7 +22,7 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 ALL = dict(mixw=True, mixp=True, soret=True, dufour=True, wmltdr=5.0)
 
 
-def _front_velocity(chem_p, diff_p, dump, u_in, yin, switches):
+def _front_velocity(chem_p, diff_p, dump, u_in, yin, switches, device=False):
     import cases
     import senga
     from oracle import Oracle
@@ -36,8 +37,13 @@ def _front_velocity(chem_p, diff_p, dump, u_in, yin, switches):
         y[k] = v
     bc = dict(xl=13, xr=21, u_in=u_in, rho_in=1.0e5 / (300.0 * float((rg * y).sum())), y_in=tuple(y),
               p_inf=1.0e5, sigma=0.287, eta=1.0e-3, pio=0, bet_local=0)
-    o = Oracle((1001, 1, 1), (1.0e-2, 1.0e-3, 1.0e-3), chem_p, diff_p, 1.0e-8, nend=(1, 1, 2, 2, 2, 2))
-    o.set_bc(bc)
+    if device:  # the product path through the C ABI
+        o = senga.Box((1001, 1, 1), (1.0e-2, 1.0e-3, 1.0e-3), chem, senga.Diff(diff_p, chem), 1.0e-8,
+                      nend=(1, 1, 2, 2, 2, 2))
+        o.set_nscbc(bc)
+    else:
+        o = Oracle((1001, 1, 1), (1.0e-2, 1.0e-3, 1.0e-3), chem_p, diff_p, 1.0e-8, nend=(1, 1, 2, 2, 2, 2))
+        o.set_bc(bc)
     if switches:
         o.set_transport(**switches)
     o.upload(f, T, itn)
@@ -77,3 +83,15 @@ def test_one_step_flame_stands_still():
     v = _front_velocity(os.path.join(GOLD, "casefile_1step_chem.dat"), None, "dmpi_1step_1001.dat", 0.39, {0: 1.0},
                         None)
     assert abs(v) < 0.01 * 0.39, v
+
+
+@pytest.mark.gpu
+def test_device_holds_the_reference_flames_still():
+    import cases
+
+    v = _front_velocity(cases.CHEM_H2, cases.DIFF_H2, "dmpi_21step_1001.dat", 2.05, H2_IN, ALL, device=True)
+    assert abs(v) < 0.05 * 2.05, v
+    v = _front_velocity(os.path.join(GOLD, "casefile_1step_chem.dat"), None, "dmpi_1step_1001.dat", 0.39, {0: 1.0},
+                        None, device=True)
+    assert abs(v) < 0.01 * 0.39, v
+
