@@ -287,6 +287,25 @@ int senga_dump_write(const char* path, int formatted, int nx, int ny, int nz, in
 int senga_dump_read(const char* path, int formatted, int nspcmx, int* dims, double* fields, int64_t capacity,
                     double* scalars);
 
+/* ---- one box split along z over several contexts --------------------------
+ * No counterpart call in the reference, whose MPI decomposition (PARFER halo
+ * exchange, src/parfer.f) it replaces: nslabs contexts (devices[r], or
+ * cfg->device for all when devices is NULL) each own nz/nslabs planes of one
+ * periodic box; the stencil kernels read each tile's z halo directly from the
+ * slab that owns those planes (peer loads between GPUs, with peer access
+ * enabled at creation), and the slabs' streams wait on one another's events
+ * between the phases of every substage. Fully periodic boxes with a fixed
+ * time step; fields/trun/itn are the whole box in the senga_upload_state_host
+ * layout. */
+typedef struct senga_zgroup senga_zgroup;
+int senga_zgroup_create(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff, int nslabs,
+                        const int* devices, senga_zgroup** out);
+int senga_zgroup_upload_host(senga_zgroup* g, const double* fields, const double* trun, const int32_t* itndex);
+int senga_zgroup_step(senga_zgroup* g, int nsteps);
+int senga_zgroup_sync(senga_zgroup* g);
+int senga_zgroup_download_host(senga_zgroup* g, double* fields, double* trun, int32_t* itndex);
+int senga_zgroup_destroy(senga_zgroup* g);
+
 /* ---- initial turbulence ---------------------------------------------------
  * TURBIN (src/turbin.f:76-362, with TURBFT/FFTSYM and ESPECT/ESPINI) for one
  * box on the current device: a solenoidal velocity field built in

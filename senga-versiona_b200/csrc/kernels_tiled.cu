@@ -52,9 +52,9 @@ constexpr int kSpecRkSmem = 2 * SSlab::SIZE;
 
 template <bool P>
 __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const Origin o, double* sm,
-                                          Folds<FX, FY, FZ>& fo) {
+                                          Folds<FX, FY, FZ>& fo, const ZDec& zd) {
   const int tx = threadIdx.x % FX, ty = threadIdx.x / FX;
-  fo.init(g, o);
+  fo.init(g, o, zd);
   tile_sync();
   TP tp[FZ];
 #pragma unroll
@@ -106,7 +106,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
   // ---- phase 3: pressure gradient (of p - p(1,1,1)) and pressure work ----
   {
     const FStar bP{sm};
-    bP.stage<FNW>(fo, LdSub{f.p, __ldg(f.p)});
+    bP.stage<FNW>(fo, LdSub{f.p, __ldg(f.p + zd.base[0])});  // p(1,1,1) lives in slab 0
     tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
@@ -343,9 +343,9 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
 // -------------------------------------------------------------------------
 template <bool P>
 __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int nspec, const Origin o, double* sm,
-                                             Folds<SX_, SY_, SZ_>& fo) {
+                                             Folds<SX_, SY_, SZ_>& fo, const ZDec& zd) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
-  fo.init(g, o);
+  fo.init(g, o, zd);
   tile_sync();
   TP tp[SZ_];
 #pragma unroll
@@ -484,9 +484,10 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
 // -------------------------------------------------------------------------
 template <bool P>
 __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, int nspec, const RK& rk,
-                                                const Origin o, double* sm, Folds<SX_, SY_, SZ_>& fo) {
+                                                const Origin o, double* sm, Folds<SX_, SY_, SZ_>& fo,
+                                                const ZDec& zd) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
-  fo.init(g, o);
+  fo.init(g, o, zd);
   tile_sync();
   TP tp[SZ_];
 #pragma unroll
@@ -586,23 +587,24 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
 
 // ---- single-box launches: one CTA per tile ----
 template <bool P>
-__global__ void __launch_bounds__(FX* FY, SENGA_FLOW_MINB) k_flow_t(Geo g, Fields f) {
+__global__ void __launch_bounds__(FX* FY, SENGA_FLOW_MINB) k_flow_t(Geo g, Fields f, ZDec zd) {
   extern __shared__ double sm[];
   __shared__ Folds<FX, FY, FZ> fo;
-  flow_tile<P>(g, f, Origin{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ}, sm, fo);
+  flow_tile<P>(g, f, Origin{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ}, sm, fo, zd);
 }
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB) k_species_t(Geo g, Fields f, int nspec) {
+__global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB) k_species_t(Geo g, Fields f, int nspec, ZDec zd) {
   extern __shared__ double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
-  species_tile<P>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm, fo);
+  species_tile<P>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm, fo,
+                  zd);
 }
 template <bool P>
-__global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB) k_species_rk_t(Geo g, Fields f, int nspec, RK rk) {
+__global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB) k_species_rk_t(Geo g, Fields f, int nspec, RK rk, ZDec zd) {
   extern __shared__ double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
   species_rk_tile<P>(g, f, nspec, rk, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_},
-                     sm, fo);
+                     sm, fo, zd);
 }
 
 // ---- batched launches: one CTA per (box, tile) work item; box descriptors
@@ -616,7 +618,7 @@ __global__ void __launch_bounds__(FX* FY, 2) k_flow_b(const __grid_constant__ Bo
   __shared__ Folds<FX, FY, FZ> fo;
   const WorkItem w = items[blockIdx.x];
   const BoxDesc& sd = t.d[w.box];
-  flow_tile<P>(sd.g, sd.f, Origin{w.x0, w.y0, w.z0}, sm, fo);
+  flow_tile<P>(sd.g, sd.f, Origin{w.x0, w.y0, w.z0}, sm, fo, ZDec{});
 }
 template <bool P>
 __global__ void __launch_bounds__(SX_* SY_, 2) k_species_b(const __grid_constant__ BoxTable t,
@@ -625,7 +627,7 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_b(const __grid_constant
   __shared__ Folds<SX_, SY_, SZ_> fo;
   const WorkItem w = items[blockIdx.x];
   const BoxDesc& sd = t.d[w.box];
-  species_tile<P>(sd.g, sd.f, sd.nspec, Origin{w.x0, w.y0, w.z0}, sm, fo);
+  species_tile<P>(sd.g, sd.f, sd.nspec, Origin{w.x0, w.y0, w.z0}, sm, fo, ZDec{});
 }
 template <bool P>
 __global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_b(const __grid_constant__ BoxTable t,
@@ -634,7 +636,7 @@ __global__ void __launch_bounds__(SX_* SY_, 2) k_species_rk_b(const __grid_const
   __shared__ Folds<SX_, SY_, SZ_> fo;
   const WorkItem w = items[blockIdx.x];
   const BoxDesc& sd = t.d[w.box];
-  species_rk_tile<P>(sd.g, sd.f, sd.nspec, sd.rk[irk], Origin{w.x0, w.y0, w.z0}, sm, fo);
+  species_rk_tile<P>(sd.g, sd.f, sd.nspec, sd.rk[irk], Origin{w.x0, w.y0, w.z0}, sm, fo, ZDec{});
 }
 
 dim3 tiles(const Geo& g, int tx, int ty, int tz) {
@@ -662,33 +664,33 @@ bool all_periodic(const Geo& g) { return g.per[0] && g.per[1] && g.per[2]; }
 
 }  // namespace
 
-void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s) {
+void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    k_flow_t<true><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f);
+    k_flow_t<true><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
   } else {
     set_attrs<false>();
-    k_flow_t<false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f);
+    k_flow_t<false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
   }
 }
 
-void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s) {
+void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    k_species_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec);
+    k_species_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
   } else {
     set_attrs<false>();
-    k_species_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec);
+    k_species_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
   }
 }
 
-void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s) {
+void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    k_species_rk_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk);
+    k_species_rk_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
   } else {
     set_attrs<false>();
-    k_species_rk_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk);
+    k_species_rk_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
   }
 }
 

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -712,3 +713,184 @@ int senga_chrate_host(senga_ctx* c, double* rate) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// A box split along z into slabs, one context each (one GPU each, or several
+// on one GPU). The stencil kernels of a slab read their z halo straight from
+// the neighbouring slabs' registers (peer loads over NVLink between GPUs);
+// between the phases that write what the others read, every slab's stream
+// waits for the others' events: after TEMPER/CHRATE (T, p, Y, transport read
+// in halos), after the species kernel (the flow and species kernels read the
+// U register that the RK update then overwrites in place), and after the RK
+// update (the next substage reads it).
+struct senga_zgroup {
+  int nr = 0, nx = 0, ny = 0, nzg = 0, nzl = 0, nc = 0;
+  senga_ctx* ctx[kMaxZRanks] = {};
+  ZDec zd[kMaxZRanks];
+  cudaEvent_t ev[kMaxZRanks] = {};
+};
+
+namespace {
+
+void zgroup_barrier(senga_zgroup* g) {
+  for (int r = 0; r < g->nr; ++r) {
+    CK(cudaSetDevice(g->ctx[r]->cfg.device));
+    CK(cudaEventRecord(g->ev[r], g->ctx[r]->stream));
+  }
+  for (int r = 0; r < g->nr; ++r) {
+    CK(cudaSetDevice(g->ctx[r]->cfg.device));
+    for (int q = 0; q < g->nr; ++q)
+      if (q != r) CK(cudaStreamWaitEvent(g->ctx[r]->stream, g->ev[q], 0));
+  }
+}
+
+void zgroup_destroy(senga_zgroup* g) {
+  for (int r = 0; r < g->nr; ++r) {
+    if (g->ev[r]) cudaEventDestroy(g->ev[r]);
+    senga_ctx_destroy(g->ctx[r]);
+  }
+  delete g;
+}
+
+}  // namespace
+
+int senga_zgroup_create(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff, int nslabs,
+                        const int* devices, senga_zgroup** out) {
+  if (!cfg || !chem || !diff || !out || nslabs < 1 || nslabs > kMaxZRanks)
+    return fail(SENGA_ERR_ARG, "senga_zgroup_create: bad argument (1..16 slabs)");
+  for (int k = 0; k < 6; ++k)
+    if (cfg->nend[k] != SENGA_NPERI)
+      return fail(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: z-split boxes must be periodic in every direction");
+  if (cfg->adaptive) return fail(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: fixed time step only");
+  if (cfg->nz % nslabs != 0) return fail(SENGA_ERR_ARG, "senga_zgroup_create: nz must divide into equal slabs");
+  *out = nullptr;
+  senga_zgroup* g = new senga_zgroup;
+  g->nr = nslabs;
+  g->nx = cfg->nx;
+  g->ny = cfg->ny;
+  g->nzg = cfg->nz;
+  g->nzl = cfg->nz / nslabs;
+  g->nc = 5 + chem->nspec;
+  const int rc = guard([&] {
+    for (int r = 0; r < nslabs; ++r) {
+      senga_config c = *cfg;
+      c.nz = g->nzl;
+      c.device = devices ? devices[r] : cfg->device;
+      if (senga_ctx_create(&c, chem, diff, &g->ctx[r]) != SENGA_OK) throw Error(SENGA_ERR_CUDA, senga_last_error());
+      // z spacing of the whole box, DELTAZ = ZGDLEN/REAL(NZGLBL-1)
+      const double delta = cfg->zgdlen / (double)(float)(cfg->nz - 1);
+      g->ctx[r]->geo.ovd[2] = 1.0 / delta;
+      g->ctx[r]->geo.ovd2[2] = g->ctx[r]->geo.ovd[2] * g->ctx[r]->geo.ovd[2];
+      CK(cudaEventCreateWithFlags(&g->ev[r], cudaEventDisableTiming));
+    }
+    for (int r = 0; r < nslabs; ++r) {  // peer access between distinct GPUs
+      const int dr = g->ctx[r]->cfg.device;
+      CK(cudaSetDevice(dr));
+      for (int q = 0; q < nslabs; ++q) {
+        const int dq = g->ctx[q]->cfg.device;
+        if (dq == dr) continue;
+        int can = 0;
+        CK(cudaDeviceCanAccessPeer(&can, dr, dq));
+        if (!can) throw Error(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: no peer access between the GPUs");
+        const cudaError_t e = cudaDeviceEnablePeerAccess(dq, 0);
+        if (e != cudaSuccess && e != cudaErrorPeerAccessAlreadyEnabled) CK(e);
+        (void)cudaGetLastError();
+      }
+    }
+    for (int r = 0; r < nslabs; ++r) {
+      ZDec& z = g->zd[r];
+      z.nr = nslabs;
+      z.rank = r;
+      z.nzg = cfg->nz;
+      for (int q = 0; q < nslabs; ++q) {
+        const std::ptrdiff_t d =
+            reinterpret_cast<const char*>(g->ctx[q]->pool) - reinterpret_cast<const char*>(g->ctx[r]->pool);
+        if (d % (std::ptrdiff_t)sizeof(double) != 0) throw Error(SENGA_ERR_CUDA, "senga_zgroup_create: pool alignment");
+        z.base[q] = (int64_t)(d / (std::ptrdiff_t)sizeof(double));
+      }
+    }
+  });
+  if (rc != SENGA_OK) {
+    zgroup_destroy(g);
+    return rc;
+  }
+  *out = g;
+  return SENGA_OK;
+}
+
+int senga_zgroup_destroy(senga_zgroup* g) {
+  if (g) zgroup_destroy(g);
+  return SENGA_OK;
+}
+
+int senga_zgroup_upload_host(senga_zgroup* g, const double* fields, const double* trun, const int32_t* itn) {
+  if (!g || !fields || !trun || !itn) return fail(SENGA_ERR_ARG, "senga_zgroup_upload_host: null argument");
+  return guard([&] {
+    const int64_t nl = (int64_t)g->nx * g->ny * g->nzl, ng = nl * g->nr;
+    for (int r = 0; r < g->nr; ++r) {
+      senga_ctx* c = g->ctx[r];
+      CK(cudaSetDevice(c->cfg.device));
+      for (int fl = 0; fl < g->nc; ++fl)
+        CK(cudaMemcpyAsync(c->f.run + fl * nl, fields + fl * ng + r * nl, nl * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
+      CK(cudaMemcpyAsync(c->f.uin, c->f.run, (size_t)g->nc * nl * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->f.t, trun + r * nl, nl * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->f.itn, itn + r * nl, nl * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    }
+    for (int r = 0; r < g->nr; ++r) CK(cudaStreamSynchronize(g->ctx[r]->stream));
+  });
+}
+
+int senga_zgroup_download_host(senga_zgroup* g, double* fields, double* trun, int32_t* itn) {
+  if (!g || !fields) return fail(SENGA_ERR_ARG, "senga_zgroup_download_host: null argument");
+  return guard([&] {
+    const int64_t nl = (int64_t)g->nx * g->ny * g->nzl, ng = nl * g->nr;
+    for (int r = 0; r < g->nr; ++r) {
+      senga_ctx* c = g->ctx[r];
+      CK(cudaSetDevice(c->cfg.device));
+      for (int fl = 0; fl < g->nc; ++fl)
+        CK(cudaMemcpyAsync(fields + fl * ng + r * nl, c->f.run + fl * nl, nl * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+      if (trun) CK(cudaMemcpyAsync(trun + r * nl, c->f.t, nl * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      if (itn) CK(cudaMemcpyAsync(itn + r * nl, c->f.itn, nl * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    }
+    for (int r = 0; r < g->nr; ++r) CK(cudaStreamSynchronize(g->ctx[r]->stream));
+  });
+}
+
+int senga_zgroup_step(senga_zgroup* g, int nsteps) {
+  if (!g || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_zgroup_step: bad argument");
+  return guard([&] {
+    for (int s = 0; s < nsteps; ++s)
+      for (int irk = 1; irk <= 5; ++irk) {
+        for (int r = 0; r < g->nr; ++r) {
+          senga_ctx* c = g->ctx[r];
+          CK(cudaSetDevice(c->cfg.device));
+          launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+        }
+        zgroup_barrier(g);
+        for (int r = 0; r < g->nr; ++r) {
+          senga_ctx* c = g->ctx[r];
+          CK(cudaSetDevice(c->cfg.device));
+          launch_flow(c->geo, c->f, c->nspec, c->stream, g->zd[r]);
+          launch_species_a(c->geo, c->f, c->nspec, c->stream, g->zd[r]);
+        }
+        zgroup_barrier(g);
+        for (int r = 0; r < g->nr; ++r) {
+          senga_ctx* c = g->ctx[r];
+          CK(cudaSetDevice(c->cfg.device));
+          RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
+          launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream, g->zd[r]);
+        }
+        zgroup_barrier(g);
+      }
+    CK(cudaGetLastError());
+  });
+}
+
+int senga_zgroup_sync(senga_zgroup* g) {
+  if (!g) return fail(SENGA_ERR_ARG, "senga_zgroup_sync: null group");
+  return guard([&] {
+    for (int r = 0; r < g->nr; ++r) CK(cudaStreamSynchronize(g->ctx[r]->stream));
+  });
+}

@@ -32,6 +32,20 @@ struct Geo {
   int bxl, bxr;         // x-face treatment bits (BF_*), 0 for periodic x
 };
 
+// A box split along z into nr slabs of equal extent, one context each
+// (senga_zgroup_*): this slab is `rank`; g.nz is the slab's extent, nzg the
+// whole box's. The stencil kernels read the z halo of a tile from whichever
+// slab owns those planes: base[r] is the element offset from this slab's
+// register pool to slab r's (identical layouts), so a halo plane of slab r
+// is addressed as base[r] + its local plane offset. nr = 1: one box.
+constexpr int kMaxZRanks = 16;
+struct ZDec {
+  int nr = 1;
+  int rank = 0;
+  int nzg = 0;
+  int64_t base[kMaxZRanks] = {};
+};
+
 // Boundary-plane treatment of a bounded x face (src/bcinit.f:287-600 flags):
 // which flux derivatives are zeroed on the face plane inside the RHS, and
 // whether the NSCBC correction and the imposed-inflow update apply there.
@@ -116,9 +130,10 @@ int select_mech(const senga_chem& chem, const senga_diff& diff);
 // Returns the number of kernels it launched (the long mechanisms run as two).
 int launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const senga_diff* ddiff, int nspec,
                   int flmavt, int mech, cudaStream_t s);
-void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
-void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
-void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s);
+void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd = ZDec{});
+void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd = ZDec{});
+void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s,
+                         const ZDec& zd = ZDec{});
 void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s);
 // Batched ensemble (kernels.cu, kernels_tiled.cu): all boxes periodic, one
 // mechanism; grid = persistent CTA count.

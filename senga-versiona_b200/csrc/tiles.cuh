@@ -45,12 +45,22 @@ template <int TX, int TY, int TZ>
 struct Folds {
   static constexpr int NX = TX + 2 * H, NY = TY + 2 * H, NZ = TZ + 2 * H;
   int64_t ox[NX], oy[NY], oz[NZ];
-  __device__ void init(const Geo& g, const Origin& o) {
+  __device__ void init(const Geo& g, const Origin& o, const ZDec& zd = ZDec{}) {
     for (int e = threadIdx.x; e < NX + NY + NZ; e += blockDim.x) {
       if (e < NX) ox[e] = fold(o.x0 + e - H, g.nx, g.per[0]);
       else if (e < NX + NY) oy[e - NX] = (int64_t)fold(o.y0 + (e - NX) - H, g.ny, g.per[1]) * g.nx;
-      else oz[e - NX - NY] = (int64_t)fold(o.z0 + (e - NX - NY) - H, g.nz, g.per[2]) * ((int64_t)g.nx * g.ny);
+      else oz[e - NX - NY] = zplane(g, zd, o.z0 + (e - NX - NY) - H);
     }
+  }
+  // element offset of local plane z: folded in this box, or for a z-split
+  // box the plane of the owning slab (the whole box is periodic in z)
+  __device__ static int64_t zplane(const Geo& g, const ZDec& zd, int z) {
+    const int64_t plane = (int64_t)g.nx * g.ny;
+    if (zd.nr <= 1) return (int64_t)fold(z, g.nz, g.per[2]) * plane;
+    int zg = (zd.rank * g.nz + z) % zd.nzg;
+    if (zg < 0) zg += zd.nzg;
+    const int r = zg / g.nz;
+    return zd.base[r] + (int64_t)(zg - r * g.nz) * plane;
   }
 };
 

@@ -145,6 +145,13 @@ def _load():
         "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
         "senga_set_transport": (ip, [vp, ip, ip, ip, ip, C.c_double]),
         "senga_keep_rates": (ip, [vp, ip]),
+        "senga_zgroup_create": (ip, [C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), ip, C.POINTER(ip),
+                                     C.POINTER(vp)]),
+        "senga_zgroup_upload_host": (ip, [vp, dp, dp, i32p]),
+        "senga_zgroup_download_host": (ip, [vp, dp, dp, i32p]),
+        "senga_zgroup_step": (ip, [vp, ip]),
+        "senga_zgroup_sync": (ip, [vp]),
+        "senga_zgroup_destroy": (ip, [vp]),
         "senga_turbin_host": (ip, [ip, ip, ip, ip, C.c_double, C.c_double, dp, dp]),
         "senga_upload_state_async": (ip, [vp, dp, dp, i32p]),
         "senga_download_state_async": (ip, [vp, dp, dp, i32p]),
@@ -295,6 +302,64 @@ class Diff:
     @property
     def mixture_averaged(self):
         return bool(self.t.flmavt)
+
+
+class ZGroup:
+    """One periodic box split along z into `nslabs` contexts (on `devices`,
+    default all on `device`); the stencils read z halos from the neighbouring
+    slabs directly."""
+
+    def __init__(self, shape, lengths, chem, diff, tstep, nslabs, devices=None, device=0):
+        nx, ny, nz = shape
+        self.shape = (nz, ny, nx)
+        self.nspec = chem.nspec
+        self.nc = 5 + self.nspec
+        cfg = ConfigT()
+        cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
+        cfg.xgdlen, cfg.ygdlen, cfg.zgdlen = lengths
+        for i in range(6):
+            cfg.nend[i] = NPERI
+        cfg.tstep = tstep
+        cfg.adaptive = 0
+        cfg.device = device
+        devs = (C.c_int * nslabs)(*devices) if devices is not None else None
+        h = C.c_void_p()
+        _check(lib.senga_zgroup_create(C.byref(cfg), C.byref(chem.t), C.byref(diff.t), nslabs, devs, C.byref(h)),
+               "senga_zgroup_create")
+        self.h = h
+
+    def upload(self, fields, trun, itndex):
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        t = np.ascontiguousarray(trun, dtype=np.float64)
+        it = np.ascontiguousarray(itndex, dtype=np.int32)
+        assert f.shape == (self.nc,) + self.shape and t.shape == self.shape and it.shape == self.shape
+        _check(lib.senga_zgroup_upload_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
+               "senga_zgroup_upload_host")
+
+    def step(self, nsteps=1):
+        _check(lib.senga_zgroup_step(self.h, nsteps), "senga_zgroup_step")
+
+    def sync(self):
+        _check(lib.senga_zgroup_sync(self.h), "senga_zgroup_sync")
+
+    def download(self):
+        f = np.empty((self.nc,) + self.shape)
+        t = np.empty(self.shape)
+        it = np.empty(self.shape, dtype=np.int32)
+        _check(lib.senga_zgroup_download_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
+               "senga_zgroup_download_host")
+        return f, t, it
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.senga_zgroup_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Radn:
