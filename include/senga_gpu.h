@@ -211,18 +211,21 @@ typedef struct senga_radn {
 int senga_radn_load(const char* path, const senga_chem* chem, double trefrn, senga_radn* out);
 int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
 
-/* NSCBC x faces (config: bounded x, NBOUND on both x faces; y, z periodic).
- * xl = 13: I3 subsonic inflow at x-left with constant velocity (NXLPRM(1)=1):
- *   u = u_in, v = w = 0, density rho_in (DRIN), mass fractions y_in (YRIN)
- *   imposed on the inflow plane (BOUNDT src/boundt.f:177-200, BOUNTT
- *   src/bountt.f:203-252, RK ranges src/bcinit.f), energy by the wave
- *   amplitudes of BOUNDS src/bounds.f:610-675.
- * xr = 21: O1 partially non-reflecting outflow at x-right: pressure relaxed
- *   to p_inf with COBCXR = sigma (1 - eta) / (2 XGDLEN) (RXRPRM(1..3)), pio =
- *   NXRPRM(1) (inflow-through-outlet switch), bet_local = NXRPRM(2) (local
- *   Mach number in place of BET = 0.05 on the transverse terms), BOUNDS
- *   src/bounds.f:1198-1450; viscous shear, conduction and diffusion zeroed on
- *   the plane (FXRVST, FXRCON, FXRDIF, FXRADB).
+/* NSCBC x faces (bounded x, NBOUND on both x faces; y, z periodic). xl and
+ * xr each take one of the built kinds; inflow on one face at most.
+ * 13: I3 subsonic inflow with constant velocity (NXxPRM(1)=1): u = u_in
+ *   (negative for inflow through x-right), v = w = 0, density rho_in (DRIN),
+ *   mass fractions y_in (YRIN) imposed on the inflow plane (BOUNDT
+ *   src/boundt.f:177-200 left, 591- right; BOUNTT src/bountt.f:203-252 left,
+ *   709- right; RK ranges src/bcinit.f:560-586), energy by the wave
+ *   amplitudes of BOUNDS (src/bounds.f:610-675 left, 1688- right).
+ * 21: O1 partially non-reflecting outflow: pressure relaxed to p_inf with
+ *   COBC = sigma (1 - eta) / (2 XGDLEN) (RXxPRM(1..3)), pio = NXxPRM(1)
+ *   (inflow-through-outlet switch), bet_local = NXxPRM(2) (local Mach number
+ *   in place of BET = 0.05 on the transverse terms), BOUNDS
+ *   src/bounds.f:213-372 left, 1296-1450 right; viscous shear, conduction
+ *   and diffusion zeroed on the plane (FxxVST, FxxCON, FxxDIF, FxxADB). Two
+ *   O1 faces share these parameters.
  * Face data and wave amplitudes are computed after the thermochemistry
  * kernel and added to the face planes' right-hand side in the RK epilogue.
  * Other face kinds return SENGA_ERR_UNSUPPORTED. Stepping a box with a

@@ -153,7 +153,7 @@ class Oracle:
         return out
 
     def set_bc(self, bc):
-        """NSCBC x faces: bc = dict(xl=13|0, xr=21|0, u_in, rho_in, y_in, p_inf,
+        """NSCBC x faces: bc = dict(xl, xr in {0, 13, 21}, u_in, rho_in, y_in, p_inf,
         sigma, eta, pio=0, bet_local=0)."""
         b = _Bc()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)

@@ -167,6 +167,7 @@ struct Oracle {
     if (c.flmavt) read_diff(diff, ch, df);
     nx = c.nx; ny = c.ny; nz = c.nz;
     istal = 1; istol = nx; jstal = 1; jstol = ny; kstal = 1; kstol = nz;
+    istold = istolu = istolv = istolw = istole = istoly = istol;
     istab = 1 - NHALO; istob = nx + NHALO; jstab = 1 - NHALO; jstob = ny + NHALO;
     kstab = 1 - NHALO; kstob = nz + NHALO;
     nendxl = c.nend[0]; nendxr = c.nend[1]; nendyl = c.nend[2]; nendyr = c.nend[3];
@@ -441,15 +442,18 @@ struct Oracle {
   // ---- NSCBC x faces: BCINIT flags and ranges (src/bcinit.f:287-600), face
   // data gathered inside RHSCAL/RHSVEL, BOUNDT (src/boundt.f:58-211), BOUNDS
   // (src/bounds.f:115-372, 610-675, 1198-1450), BOUNTT (src/bountt.f:61-260).
-  // Restated: I3 inflow at x-left (NXLPRM(1)=1: constant u, v=w=0, density
-  // DRIN, mass fractions YRIN) and O1 partially non-reflecting outflow at
-  // x-right; y and z periodic.
+  // Restated: I3 inflow (NXxPRM(1)=1: constant u, v=w=0, density DRIN, mass
+  // fractions YRIN) and O1 partially non-reflecting outflow, on either x face
+  // (bounds.f:213-372 O1 left, 610-675 I3 left, 1296-1450 O1 right, 1688-
+  // I3 right; boundt.f:177, 591; bountt.f:203, 709); y and z periodic. Both
+  // O1 faces take the same outflow parameters.
   static constexpr int BC_NONE = 0, BC_I3 = 13, BC_O1 = 21;
   int bcxl = BC_NONE, bcxr = BC_NONE;
   double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0;
   int pio_xr = 0, betloc_xr = 0;
   bool fxlcnv = false, fxrcnv = false;
   int istald = 1, istalu = 1, istalv = 1, istalw = 1, istale = 1, istaly = 1;
+  int istold = 0, istolu = 0, istolv = 0, istolw = 0, istole = 0, istoly = 0;
   struct Face {
     std::vector<double> d, u, v, w, p, t, r, g, e, bcl1, bcl2, bcl3, bcl4, bcl5, t1b, t2b, t3b, t4b, t51b, t52b;
     std::vector<double> y, h, rate, bcly, t6b;  // [nspec][ny*nz]
@@ -477,8 +481,9 @@ struct Oracle {
   }
   void set_bc(int xl, int xr, double u_in, double rho_in, const double* y_in, double p_inf, double sigma,
               double eta, int pio, int betloc) {
-    if ((xl != BC_NONE && xl != BC_I3) || (xr != BC_NONE && xr != BC_O1))
-      throw std::runtime_error("oracle: NSCBC restated for I3 at x-left and O1 at x-right");
+    auto ok = [](int k) { return k == BC_NONE || k == BC_I3 || k == BC_O1; };
+    if (!ok(xl) || !ok(xr) || (xl == BC_I3 && xr == BC_I3))
+      throw std::runtime_error("oracle: NSCBC restated for I3 and O1 x faces (not inflow on both)");
     if ((xl != BC_NONE && nendxl != NBOUND) || (xr != BC_NONE && nendxr != NBOUND))
       throw std::runtime_error("oracle: NSCBC faces need NBOUND end conditions");
     bcxl = xl;
@@ -487,16 +492,22 @@ struct Oracle {
     rhoin = rho_in;
     for (int is = 0; is < nspec; ++is) yin[is] = y_in[is];
     pinfxr = p_inf;
-    cobcxr = sigma * (1.0 - eta) / (2.0 * cf.xgdlen);  // COBCXR, src/bcinit.f
+    cobcxr = sigma * (1.0 - eta) / (2.0 * cf.xgdlen);  // COBCXL/COBCXR, src/bcinit.f:309,324
     pio_xr = pio;
     betloc_xr = betloc;
     fxlcnv = xl != BC_NONE;
     fxrcnv = xr != BC_NONE;
-    if (xl == BC_I3) {  // src/bcinit.f: FXLCNV, FXLVSN; D,U,V,W,Y ranges start at ISTAP1
+    istold = istolu = istolv = istolw = istole = istoly = istol;
+    if (xl == BC_I3) {  // src/bcinit.f:560-571: FXLCNV, FXLVSN; D,U,V,W,Y ranges start at ISTAP1
       fxlvsn = true;
       istald = istalu = istalv = istalw = istaly = istal + 1;
     }
-    if (xr == BC_O1) {  // FXRCNV, FXRVST, FXRCON, FXRADB, FXRDIF
+    if (xr == BC_I3) {  // src/bcinit.f:575-586: FXRCNV, FXRVSN; D,U,V,W,Y ranges end at ISTOM1
+      fxrvsn = true;
+      istold = istolu = istolv = istolw = istoly = istol - 1;
+    }
+    if (xl == BC_O1) fxlvst = fxlcon = fxladb = fxldif = true;  // src/bcinit.f:299-311
+    if (xr == BC_O1) {  // FXRCNV, FXRVST, FXRCON, FXRADB, FXRDIF (src/bcinit.f:314-326)
       fxrvst = fxrcon = fxradb = fxrdif = true;
     }
     fxl.init(ny * nz, nspec);
@@ -505,38 +516,40 @@ struct Oracle {
   // BOUNDT, I3 at x-left: impose the inflow state on the U register (DRHS..YRHS
   // at ISTAL; src/boundt.f:177-200 with BCDTXL, BCUTXL NXLPRM(1)=1, BCYTXL)
   void boundt() {
-    if (bcxl != BC_I3) return;
+    if (bcxl != BC_I3 && bcxr != BC_I3) return;
+    const int ic = bcxl == BC_I3 ? istal : istol;  // boundt.f:177 (x-left), 591 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
       for (int jc = jstal; jc <= jstol; ++jc) {
-        drhs(istal, jc, kc) = rhoin;
-        urhs(istal, jc, kc) = rhoin * uin;
-        vrhs(istal, jc, kc) = rhoin * 0.0;
-        wrhs(istal, jc, kc) = rhoin * 0.0;
-        for (int is = 0; is < nspec; ++is) yrhs[is](istal, jc, kc) = rhoin * yin[is];
+        drhs(ic, jc, kc) = rhoin;
+        urhs(ic, jc, kc) = rhoin * uin;
+        vrhs(ic, jc, kc) = rhoin * 0.0;
+        wrhs(ic, jc, kc) = rhoin * 0.0;
+        for (int is = 0; is < nspec; ++is) yrhs[is](ic, jc, kc) = rhoin * yin[is];
       }
   }
   // BOUNTT, I3 at x-left: both registers at ISTAL set to the inflow state, its
   // error zeroed (src/bountt.f:203-252)
   void bountt() {
-    if (bcxl != BC_I3) return;
+    if (bcxl != BC_I3 && bcxr != BC_I3) return;
+    const int ic = bcxl == BC_I3 ? istal : istol;  // bountt.f:203 (x-left), 709 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
       for (int jc = jstal; jc <= jstol; ++jc) {
-        drhs(istal, jc, kc) = rhoin;
-        urhs(istal, jc, kc) = rhoin * uin;
-        vrhs(istal, jc, kc) = rhoin * 0.0;
-        wrhs(istal, jc, kc) = rhoin * 0.0;
-        drun(istal, jc, kc) = drhs(istal, jc, kc);
-        urun(istal, jc, kc) = urhs(istal, jc, kc);
-        vrun(istal, jc, kc) = vrhs(istal, jc, kc);
-        wrun(istal, jc, kc) = wrhs(istal, jc, kc);
-        derr(istal, jc, kc) = 0.0;
-        uerr(istal, jc, kc) = 0.0;
-        verr(istal, jc, kc) = 0.0;
-        werr(istal, jc, kc) = 0.0;
+        drhs(ic, jc, kc) = rhoin;
+        urhs(ic, jc, kc) = rhoin * uin;
+        vrhs(ic, jc, kc) = rhoin * 0.0;
+        wrhs(ic, jc, kc) = rhoin * 0.0;
+        drun(ic, jc, kc) = drhs(ic, jc, kc);
+        urun(ic, jc, kc) = urhs(ic, jc, kc);
+        vrun(ic, jc, kc) = vrhs(ic, jc, kc);
+        wrun(ic, jc, kc) = wrhs(ic, jc, kc);
+        derr(ic, jc, kc) = 0.0;
+        uerr(ic, jc, kc) = 0.0;
+        verr(ic, jc, kc) = 0.0;
+        werr(ic, jc, kc) = 0.0;
         for (int is = 0; is < nspec; ++is) {
-          yrhs[is](istal, jc, kc) = rhoin * yin[is];
-          yrun[is](istal, jc, kc) = yrhs[is](istal, jc, kc);
-          yerr[is](istal, jc, kc) = 0.0;
+          yrhs[is](ic, jc, kc) = rhoin * yin[is];
+          yrun[is](ic, jc, kc) = yrhs[is](ic, jc, kc);
+          yerr[is](ic, jc, kc) = 0.0;
         }
       }
   }
@@ -595,6 +608,96 @@ struct Oracle {
             const int q = fj(jc, kc), qs = is * m + q;
             const double bcly = F.rate[qs] / F.d[q] - 0.0 - F.u[q] * F.bcly[qs];
             erhs(istal, jc, kc) = erhs(istal, jc, kc) - bcly * F.d[q] * F.h[qs];
+          }
+    }
+    if (bcxl == BC_O1) {  // bounds.f:213-372: L5 (entering from the left) relaxed
+      Face& F = fxl;
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      std::vector<double> sorp(m, 0.0), b2(m), b3(m), b4(m), b5(m);
+      for (int is = 0; is < nspec; ++is)
+        for (int q = 0; q < m; ++q) sorp[q] = sorp[q] + F.h[is * m + q] * F.rate[is * m + q];
+      for (int q = 0; q < m; ++q) sorp[q] = -sorp[q] * gam1[q];
+      for (int q = 0; q < m; ++q) {
+        double bet = bet_global;
+        b2[q] = F.u[q] * (F.bcl2[q] - F.bcl5[q] * ova2[q]);
+        b3[q] = F.u[q] * F.bcl3[q];
+        b4[q] = F.u[q] * F.bcl4[q];
+        b5[q] = 0.5 * (F.u[q] + acou[q]) * (F.bcl5[q] + F.d[q] * acou[q] * F.bcl1[q]);
+        if (betloc_xr == 1) {
+          bet = F.u[q] * F.u[q] + F.v[q] * F.v[q] + F.w[q] * F.w[q];
+          bet = std::sqrt(bet) / acou[q];
+        }
+        if (F.u[q] > 0.0 && pio_xr == 1) {
+          b2[q] = -b2[q] - ova2[q] * sorp[q];
+          b3[q] = (double)0.1f * (F.v[q] - 0.0) - b3[q];
+          b4[q] = (double)0.1f * (F.w[q] - 0.0) - b4[q];
+          b5[q] = 0.5 * sorp[q] + cobcxr * acou[q] * (F.p[q] - pinfxr) + 0.5 * (1.0 - bet) * tt5[q] - b5[q] +
+                  100.0 * F.d[q] * (1.0 / cf.xgdlen) * (std::pow(acou[q], 2.0) - std::pow(F.u[q], 2.0)) *
+                      (F.u[q] - 0.0);
+        } else {
+          b5[q] = 0.5 * sorp[q] + cobcxr * acou[q] * (F.p[q] - pinfxr) + 0.5 * (1.0 - bet) * tt5[q] - b5[q];
+        }
+      }
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          const int ic = istal;
+          if (F.u[q] > 0.0 && pio_xr == 1) {
+            drhs(ic, jc, kc) = drhs(ic, jc, kc) - b2[q] - b5[q] * ova2[q];
+            urhs(ic, jc, kc) = urhs(ic, jc, kc) - b2[q] * F.u[q] - b5[q] * ova2[q] * (F.u[q] + acou[q]);
+            vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - b2[q] * F.v[q] - b3[q] * F.d[q] - b5[q] * ova2[q] * F.v[q];
+            wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - b2[q] * F.w[q] - b4[q] * F.d[q] - b5[q] * ova2[q] * F.w[q];
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - b2[q] * F.e[q] - b3[q] * F.d[q] * F.v[q] -
+                               b4[q] * F.d[q] * F.w[q] - b5[q] * (ova2[q] * F.e[q] + F.u[q] / acou[q] + ovgm[q]);
+          } else {
+            drhs(ic, jc, kc) = drhs(ic, jc, kc) - b5[q] * ova2[q];
+            urhs(ic, jc, kc) = urhs(ic, jc, kc) - b5[q] * ova2[q] * (F.u[q] + acou[q]);
+            vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - b5[q] * ova2[q] * F.v[q];
+            wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - b5[q] * ova2[q] * F.w[q];
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - b5[q] * (ova2[q] * F.e[q] + F.u[q] / acou[q] + ovgm[q]);
+          }
+        }
+      for (int is = 0; is < nspec; ++is)
+        for (int kc = kstal; kc <= kstol; ++kc)
+          for (int jc = jstal; jc <= jstol; ++jc) {
+            const int q = fj(jc, kc), qs = is * m + q;
+            double& yr = yrhs[is](istal, jc, kc);
+            if (F.u[q] > 0.0 && pio_xr == 1) {
+              const double fornow = F.bcly[qs] * F.d[q];
+              erhs(istal, jc, kc) = erhs(istal, jc, kc) - fornow * F.h[qs];
+              yr = yr - (b2[q] + b5[q] * ova2[q]) * F.y[qs] - fornow;
+            } else {
+              yr = yr - b5[q] * ova2[q] * F.y[qs];
+            }
+          }
+    }
+    if (bcxr == BC_I3) {  // bounds.f:1688-: L1 (entering from the right) from the imposed state
+      Face& F = fxr;
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          double fornow = F.d[q] * acou[q] * F.bcl1[q];
+          double bcl1 = 0.5 * (F.u[q] - acou[q]) * (F.bcl5[q] - fornow);
+          double bcl2 = F.u[q] * (F.bcl2[q] - F.bcl5[q] * ova2[q]);
+          double bcl3 = F.u[q] * F.bcl3[q];
+          double bcl4 = F.u[q] * F.bcl4[q];
+          double bcl5 = 0.5 * (F.u[q] + acou[q]) * (F.bcl5[q] + fornow);
+          fornow = bcl5 + F.d[q] * acou[q] * 0.0;
+          bcl1 = fornow - bcl1;
+          bcl2 = -0.0 - ova2[q] * (bcl5 + fornow) - bcl2;
+          bcl3 = -0.0 - bcl3;
+          bcl4 = -0.0 - bcl4;
+          double& er = erhs(istol, jc, kc);
+          er = er - bcl1 * (ova2[q] * F.e[q] - F.u[q] / acou[q] + ovgm[q]) - bcl2 * F.e[q] -
+               bcl3 * F.d[q] * F.v[q] - bcl4 * F.d[q] * F.w[q];
+        }
+      for (int is = 0; is < nspec; ++is)
+        for (int kc = kstal; kc <= kstol; ++kc)
+          for (int jc = jstal; jc <= jstol; ++jc) {
+            const int q = fj(jc, kc), qs = is * m + q;
+            const double bcly = F.rate[qs] / F.d[q] - 0.0 - F.u[q] * F.bcly[qs];
+            erhs(istol, jc, kc) = erhs(istol, jc, kc) - bcly * F.d[q] * F.h[qs];
           }
     }
     if (bcxr == BC_O1) {
@@ -1542,9 +1645,9 @@ struct Oracle {
   }
 
   // ---- LINCOM / FINCOM: src/lincom.f:53-169, src/fincom.f:54-168 ----
-  void rkupdate(Field& run, Field& rhs, Field& err, int irk, bool last, int ista = 1) {
+  void rkupdate(Field& run, Field& rhs, Field& err, int irk, bool last, int ista, int isto) {
 #pragma omp parallel for schedule(static)
-    for (int kc = kstal; kc <= kstol; ++kc) for (int jc = jstal; jc <= jstol; ++jc) for (int ic = ista; ic <= istol; ++ic) {
+    for (int kc = kstal; kc <= kstol; ++kc) for (int jc = jstal; jc <= jstol; ++jc) for (int ic = ista; ic <= isto; ++ic) {
       err(ic, jc, kc) = err(ic, jc, kc) + rkerr[irk - 1] * rhs(ic, jc, kc);
       if (!last) {
         double f = run(ic, jc, kc);
@@ -1559,12 +1662,12 @@ struct Oracle {
   void lincom(int irk, bool last) {
     // per-field ranges ISTALD..ISTALY (src/bcinit.f: the I3 inflow plane is
     // imposed, not integrated, for D, U, V, W, Y)
-    rkupdate(drun, drhs, derr, irk, last, istald);
-    rkupdate(urun, urhs, uerr, irk, last, istalu);
-    rkupdate(vrun, vrhs, verr, irk, last, istalv);
-    rkupdate(wrun, wrhs, werr, irk, last, istalw);
-    rkupdate(erun, erhs, eerr, irk, last, istale);
-    for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last, istaly);
+    rkupdate(drun, drhs, derr, irk, last, istald, istold);
+    rkupdate(urun, urhs, uerr, irk, last, istalu, istolu);
+    rkupdate(vrun, vrhs, verr, irk, last, istalv, istolv);
+    rkupdate(wrun, wrhs, werr, irk, last, istalw, istolw);
+    rkupdate(erun, erhs, eerr, irk, last, istale, istole);
+    for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last, istaly, istoly);
   }
 
   // ---- explicit filter: src/flinit.f:42-…, src/filtrx.f:56-295 (+y, z),

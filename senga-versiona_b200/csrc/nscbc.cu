@@ -1,14 +1,18 @@
 // Navier-Stokes characteristic boundary conditions on the x faces.
 //
-// Restated from the reference (I3 subsonic inflow at x-left with constant
-// velocity, NXLPRM(1)=1; O1 partially non-reflecting outflow at x-right):
-//   BOUNDT  src/boundt.f:177-200   impose the inflow state on the U register
+// Restated from the reference (I3 subsonic inflow with constant velocity,
+// NXxPRM(1)=1, and O1 partially non-reflecting outflow, on either x face;
+// inflow on one face at most; both O1 faces take the same parameters):
+//   BOUNDT  src/boundt.f:177-200 (x-left), 591- (x-right)   impose the
+//           inflow state on the U register
 //   face data gathered inside RHSCAL/RHSVEL (src/rhscal.f:70-90,159-180,
 //           257-275,438-456,841-862,1140-1180,1483-1500,3966-3990;
 //           src/rhsvel.f:62-200,558-570,764-800,1310-1325,1630-1650)
-//   BOUNDS  src/bounds.f:115-157 (x-left preliminaries), 610-675 (I3),
-//           1198-1240 (x-right preliminaries), 1296-1450 (O1)
-//   BOUNTT  src/bountt.f:203-252   both registers of the inflow plane reset
+//   BOUNDS  src/bounds.f:115-157 (x-left preliminaries), 213-372 (O1 left),
+//           610-675 (I3 left), 1198-1240 (x-right preliminaries), 1296-1450
+//           (O1 right), 1688- (I3 right)
+//   BOUNTT  src/bountt.f:203-252 (x-left), 709- (x-right)   both registers
+//           of the inflow plane reset
 // Every face quantity is a pointwise value or a derivative at the face plane,
 // so one thread per face point computes them from the thermochemistry
 // kernel's outputs and the U register right after that kernel (before the
@@ -53,7 +57,8 @@ __global__ void __launch_bounds__(kFaceBlock) k_boundt(Geo g, Fields f, NscbcPar
   const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
   if (jk >= g.ny * g.nz) return;
   const int64_t n = g.n;
-  const int64_t q = (int64_t)g.nx * jk;  // i = 0
+  const int i = bc.xl == 13 ? 0 : g.nx - 1;  // the inflow plane
+  const int64_t q = (int64_t)i + (int64_t)g.nx * jk;
   const double r = bc.rho_in;
   double* regs[2] = {f.uin, f.run};
   for (int w = 0; w < (both ? 2 : 1); ++w) {
@@ -106,7 +111,63 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
   double* corr = f.face + (int64_t)side * nc * nyz + jk;
   for (int fl = 0; fl < nc; ++fl) corr[(int64_t)fl * nyz] = 0.0;
   auto hprime = [&](int s) { return f.h[s * n + q] - cp * t * chem->rgspec[s] / rr; };
-  if (kind == 13) {  // I3 inflow, constant u, rho and Y (DUDT = DDDT = DYDT = 0)
+  if (kind == 13 && side == 1) {  // I3 inflow at x-right (bounds.f:1688-): L1 enters
+    double fornow = d * acou * bcl1;
+    double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
+    double b2 = u * (bcl2 - bcl5 * ova2);
+    double b3 = u * bcl3;
+    double b4 = u * bcl4;
+    const double b5 = 0.5 * (u + acou) * (bcl5 + fornow);
+    fornow = b5 + d * acou * 0.0;
+    b1 = fornow - b1;
+    b2 = -0.0 - ova2 * (b5 + fornow) - b2;
+    b3 = -0.0 - b3;
+    b4 = -0.0 - b4;
+    double ce = -b1 * (ova2 * e - u / acou + ovgm) - b2 * e - b3 * d * v - b4 * d * w;
+    for (int s = 0; s < nspec; ++s) {
+      const double bcly = f.wdot[s * n + q] / d - 0.0 - u * dd<0>(g, f.y + s * n, i, j, k);
+      ce = ce - bcly * d * hprime(s);
+    }
+    corr[4 * (int64_t)nyz] = ce;
+  } else if (kind == 21 && side == 0) {  // O1 outflow at x-left (bounds.f:213-372): L5 relaxed
+    double sorp = 0.0;
+    for (int s = 0; s < nspec; ++s) sorp = sorp + hprime(s) * f.wdot[s * n + q];
+    sorp = -sorp * gam1;
+    const double tt5 = t51b + t52b * (gam1 + 1.0) + d * acou * t2b;
+    double b2 = u * (bcl2 - bcl5 * ova2);
+    double b3 = u * bcl3;
+    double b4 = u * bcl4;
+    double b5 = 0.5 * (u + acou) * (bcl5 + d * acou * bcl1);
+    double bet = bc.bet;
+    if (bc.betloc == 1) bet = sqrt(u * u + v * v + w * w) / acou;
+    const bool pio = u > 0.0 && bc.pio == 1;
+    if (pio) {
+      b2 = -b2 - ova2 * sorp;
+      b3 = (double)0.1f * (v - 0.0) - b3;
+      b4 = (double)0.1f * (w - 0.0) - b4;
+      b5 = 0.5 * sorp + bc.cobc * acou * (p - bc.p_inf) + 0.5 * (1.0 - bet) * tt5 - b5 +
+           100.0 * d * (1.0 / bc.xlen) * (pow(acou, 2.0) - pow(u, 2.0)) * (u - 0.0);
+      corr[0] = -b2 - b5 * ova2;
+      corr[(int64_t)nyz] = -b2 * u - b5 * ova2 * (u + acou);
+      corr[2 * (int64_t)nyz] = -b2 * v - b3 * d - b5 * ova2 * v;
+      corr[3 * (int64_t)nyz] = -b2 * w - b4 * d - b5 * ova2 * w;
+      double ce = -b2 * e - b3 * d * v - b4 * d * w - b5 * (ova2 * e + u / acou + ovgm);
+      for (int s = 0; s < nspec; ++s) {
+        const double fn = dd<0>(g, f.y + s * n, i, j, k) * d;
+        ce = ce - fn * hprime(s);
+        corr[(int64_t)(5 + s) * nyz] = -(b2 + b5 * ova2) * f.y[s * n + q] - fn;
+      }
+      corr[4 * (int64_t)nyz] = ce;
+    } else {
+      b5 = 0.5 * sorp + bc.cobc * acou * (p - bc.p_inf) + 0.5 * (1.0 - bet) * tt5 - b5;
+      corr[0] = -b5 * ova2;
+      corr[(int64_t)nyz] = -b5 * ova2 * (u + acou);
+      corr[2 * (int64_t)nyz] = -b5 * ova2 * v;
+      corr[3 * (int64_t)nyz] = -b5 * ova2 * w;
+      corr[4 * (int64_t)nyz] = -b5 * (ova2 * e + u / acou + ovgm);
+      for (int s = 0; s < nspec; ++s) corr[(int64_t)(5 + s) * nyz] = -b5 * ova2 * f.y[s * n + q];
+    }
+  } else if (kind == 13) {  // I3 inflow at x-left, constant u, rho and Y (DUDT = DDDT = DYDT = 0)
     double fornow = d * acou * bcl1;
     const double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
     double b2 = u * (bcl2 - bcl5 * ova2);
@@ -124,7 +185,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
       ce = ce - bcly * d * hprime(s);
     }
     corr[4 * (int64_t)nyz] = ce;
-  } else {  // O1 outflow
+  } else {  // O1 outflow at x-right
     double sorp = 0.0;
     for (int s = 0; s < nspec; ++s) sorp = sorp + hprime(s) * f.wdot[s * n + q];
     sorp = -sorp * gam1;
@@ -168,7 +229,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
 }  // namespace
 
 void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both, cudaStream_t s) {
-  if (bc.xl != 13) return;
+  if (bc.xl != 13 && bc.xr != 13) return;
   const int nyz = g.ny * g.nz;
   k_boundt<<<(nyz + kFaceBlock - 1) / kFaceBlock, kFaceBlock, 0, s>>>(g, f, bc, nspec, both ? 1 : 0);
 }

@@ -610,8 +610,10 @@ int senga_set_radiation(senga_ctx* c, const senga_radn* r) {
 
 int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
   if (!c || !b) return fail(SENGA_ERR_ARG, "senga_set_nscbc: null argument");
-  if ((b->xl != 0 && b->xl != 13) || (b->xr != 0 && b->xr != 21))
-    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I3 (13) at x-left and O1 (21) at x-right");
+  auto kind_ok = [](int k) { return k == 13 || k == 21; };
+  if (!kind_ok(b->xl) || !kind_ok(b->xr) || (b->xl == 13 && b->xr == 13))
+    return fail(SENGA_ERR_UNSUPPORTED,
+                "senga_set_nscbc: built face kinds are I3 (13) and O1 (21) on either x face, inflow on one at most");
   if (c->geo.per[0] || b->xl == 0 || b->xr == 0)
     return fail(SENGA_ERR_ARG, "senga_set_nscbc: needs a bounded x direction and a kind on both x faces");
   if (b->rho_in <= 0.0 || b->p_inf <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: rho_in and p_inf must be > 0");
@@ -624,15 +626,18 @@ int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
     p.rho_in = b->rho_in;
     for (int s = 0; s < c->nspec; ++s) p.y_in[s] = b->y_in[s];
     p.p_inf = b->p_inf;
-    p.cobc = b->sigma * (1.0 - b->eta) / (2.0 * c->cfg.xgdlen);  // COBCXR, src/bcinit.f
+    p.cobc = b->sigma * (1.0 - b->eta) / (2.0 * c->cfg.xgdlen);  // COBCXL/COBCXR, src/bcinit.f:309,324
     p.bet = 0.050;                                               // BET default, src/bounds.f:103
     p.xlen = c->cfg.xgdlen;
     p.pio = b->pio;
     p.betloc = b->bet_local;
-    // face-plane flags of src/bcinit.f: I3 -> FXLCNV, FXLVSN, inflow ranges;
-    // O1 -> FXRCNV, FXRVST, FXRCON, FXRADB, FXRDIF
-    c->geo.bxl = BF_VSN | BF_NSCBC | BF_IMPOSED;
-    c->geo.bxr = BF_VST | BF_CON | BF_DIF | BF_NSCBC;
+    // face-plane flags of src/bcinit.f:299-326,560-586: I3 -> FxxCNV,
+    // FxxVSN, the plane imposed; O1 -> FxxCNV, FxxVST, FxxCON, FxxADB, FxxDIF
+    auto bits = [](int kind) {
+      return kind == 13 ? (BF_VSN | BF_NSCBC | BF_IMPOSED) : (BF_VST | BF_CON | BF_DIF | BF_NSCBC);
+    };
+    c->geo.bxl = bits(b->xl);
+    c->geo.bxr = bits(b->xr);
     if (!c->nscbc_pool) {
       const int64_t n = c->geo.n, nyz = (int64_t)c->geo.ny * c->geo.nz;
       CK(cudaMalloc(&c->nscbc_pool, (size_t)(2 * n + 2 * c->nc * nyz) * sizeof(double)));

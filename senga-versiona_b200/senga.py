@@ -502,7 +502,7 @@ class Box:
         return out
 
     def set_nscbc(self, bc):
-        """NSCBC x faces from a dict (xl=13, xr=21, u_in, rho_in, y_in, p_inf,
+        """NSCBC x faces from a dict (xl, xr in {13, 21}, u_in, rho_in, y_in, p_inf,
         sigma, eta, pio, bet_local)."""
         b = NscbcT()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
