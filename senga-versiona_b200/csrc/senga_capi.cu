@@ -737,6 +737,17 @@ struct senga_zgroup {
 
 namespace {
 
+// restores the caller's current device when a group call returns
+struct DeviceGuard {
+  int dev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  }
+  ~DeviceGuard() {
+    if (dev >= 0) cudaSetDevice(dev);
+  }
+};
+
 void zgroup_barrier(senga_zgroup* g) {
   for (int r = 0; r < g->nr; ++r) {
     CK(cudaSetDevice(g->ctx[r]->cfg.device));
@@ -769,6 +780,7 @@ int senga_zgroup_create(const senga_config* cfg, const senga_chem* chem, const s
   if (cfg->adaptive) return fail(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: fixed time step only");
   if (cfg->nz % nslabs != 0) return fail(SENGA_ERR_ARG, "senga_zgroup_create: nz must divide into equal slabs");
   *out = nullptr;
+  DeviceGuard dg;
   senga_zgroup* g = new senga_zgroup;
   g->nr = nslabs;
   g->nx = cfg->nx;
@@ -830,6 +842,7 @@ int senga_zgroup_destroy(senga_zgroup* g) {
 
 int senga_zgroup_upload_host(senga_zgroup* g, const double* fields, const double* trun, const int32_t* itn) {
   if (!g || !fields || !trun || !itn) return fail(SENGA_ERR_ARG, "senga_zgroup_upload_host: null argument");
+  DeviceGuard dg;
   return guard([&] {
     const int64_t nl = (int64_t)g->nx * g->ny * g->nzl, ng = nl * g->nr;
     for (int r = 0; r < g->nr; ++r) {
@@ -848,6 +861,7 @@ int senga_zgroup_upload_host(senga_zgroup* g, const double* fields, const double
 
 int senga_zgroup_download_host(senga_zgroup* g, double* fields, double* trun, int32_t* itn) {
   if (!g || !fields) return fail(SENGA_ERR_ARG, "senga_zgroup_download_host: null argument");
+  DeviceGuard dg;
   return guard([&] {
     const int64_t nl = (int64_t)g->nx * g->ny * g->nzl, ng = nl * g->nr;
     for (int r = 0; r < g->nr; ++r) {
@@ -865,6 +879,7 @@ int senga_zgroup_download_host(senga_zgroup* g, double* fields, double* trun, in
 
 int senga_zgroup_step(senga_zgroup* g, int nsteps) {
   if (!g || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_zgroup_step: bad argument");
+  DeviceGuard dg;
   return guard([&] {
     for (int s = 0; s < nsteps; ++s)
       for (int irk = 1; irk <= 5; ++irk) {
