@@ -182,7 +182,12 @@ int senga_get_status(senga_ctx* ctx, int* status);
  * D2FDXY/D2FDXZ/D2FDYZ: src/d2fdxy.f:55-1937
  * kind: 0 dx, 1 dy, 2 dz, 3 dxx, 4 dyy, 5 dzz, 6 dxy, 7 dxz, 8 dyz.
  * f and out are interior arrays (device pointers); periodic directions are
- * wrapped in place of the reference's halo copy. */
+ * wrapped in place of the reference's halo copy. Any direction may be
+ * bounded (NBOUND on both faces): one-sided closures, and for the mixed
+ * derivatives the end rows of either direction and the corner schemes
+ * where both are bounded. A context bounded in y or z runs these operators
+ * and the filter only (the RHS entry points return SENGA_ERR_UNSUPPORTED:
+ * no y/z face conditions are built). */
 int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
 

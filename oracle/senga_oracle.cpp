@@ -84,6 +84,7 @@ struct FD {
   double acfs1, bcfs1, ccfs1, dcfs1, ecfs1, acfs2, bcfs2, ccfs2, dcfs2, ecfs2;
   double acfs3, bcfs3, acfs4, bcfs4, ccfs4, acfs5, bcfs5, ccfs5, dcfs5;
   double acofxy, bcofxy, ccofxy, dcofxy, ecofxy;
+  double acc1xy, bcc1xy, ccc1xy, dcc1xy, acc2xy, bcc2xy, ccc2xy, dcc2xy;  // corner points (same for xz, yz)
   double ovdelx, ovdely, ovdelz, ovdlx2, ovdly2, ovdlz2, deltax, deltay, deltaz;
   void init(double xl, double yl, double zl, int nxg, int nyg, int nzg) {
     deltax = xl / (double)(float)(nxg - 1);
@@ -110,6 +111,12 @@ struct FD {
     acfs5 = a5; bcfs5 = b5 / 4.0; ccfs5 = c5 / 9.0; dcfs5 = d5 / 1.6e1;
     acofxy = a / 4.0; bcofxy = b / 4.0 / 4.0; ccofxy = c / 4.0 / 9.0; dcofxy = d / 4.0 / 1.6e1;
     ecofxy = e / 4.0 / 2.5e1;
+    // corner point schemes, dfinit.f:434-467 (ACOFC1..DCOFC2 from the
+    // first- and second-point first-derivative coefficients)
+    const double acofc1 = acof1, bcofc1 = bcof1 * 2.0, ccofc1 = ccof1 * 3.0, dcofc1 = dcof1 * 4.0;
+    acc1xy = acofc1; bcc1xy = bcofc1 / 4.0; ccc1xy = ccofc1 / 9.0; dcc1xy = dcofc1 / 1.6e1;
+    const double acofc2 = -acof2, bcofc2 = bcof2, ccofc2 = ccof2 * 2.0, dcofc2 = dcof2 * 3.0;
+    acc2xy = acofc2; bcc2xy = bcofc2; ccc2xy = ccofc2 / 4.0; dcc2xy = dcofc2 / 9.0;
   }
 };
 
@@ -344,8 +351,8 @@ struct Oracle {
   // the first two points apply the one-sided first-derivative rows in x to a
   // 4th-order centred difference in the other direction (ACOFY1, BCOFY1),
   // points 3-5 diagonal 4th/6th/8th-order schemes. Scaling :1925-1937.
-  // plane 0: xy, 1: xz, 2: yz. Only the x-bounded edges are restated (the
-  // other direction periodic); other bounded combinations throw.
+  // plane 0: xy, 1: xz, 2: yz. A bounded second direction (and y bounded
+  // in yz) goes to dmix_ends, which covers every combination point by point.
   template <int plane>
   void dmix(Field& F, Field& D) {
     double s1 = plane == 2 ? fd.ovdely : fd.ovdelx;
@@ -356,8 +363,7 @@ struct Oracle {
     const bool zb = nendzl == NBOUND || nendzr == NBOUND;
     const bool bnd_a = plane == 2 ? yb : xb;
     const bool bnd_b = plane == 0 ? yb : (plane == 1 ? zb : zb);
-    if (bnd_b || (plane == 2 && bnd_a))
-      throw std::runtime_error("oracle: mixed-derivative closures restated for bounded x only");
+    if (bnd_b || (plane == 2 && bnd_a)) return dmix_ends<plane>(F, D);
     const FD& c = fd;
     const double ay = 4.0 / 3.0 / 2.0, by = -1.0 / 3.0 / 4.0;  // ACOFY1, BCOFY1 (= ACOFZ1, BCOFZ1)
     const double c3a = (4.0 / 3.0) / 4.0, c3b = (-1.0 / 3.0) / 4.0 / 4.0;
@@ -418,6 +424,118 @@ struct Oracle {
                    s1 * s2;
         }
       }
+  }
+  // Mixed derivative with the second direction bounded, or both
+  // (src/d2fdxy.f:393-1924; d2fdxz.f and d2fdyz.f repeat it for their
+  // planes). Per point, with ea, eb its distances from the nearer bounded end
+  // of each direction (a periodic direction has none):
+  //   ea, eb >= 5: the 10th-order interior scheme (:126-141);
+  //   ea, eb >= 2: the diagonal 4th/6th/8th-order scheme of min(ea, eb)
+  //     (the end sections' third to fifth rows, e.g. :232-266, and the
+  //     corners' inner blocks :752-835);
+  //   ea <= 1 < eb: the one-sided first-derivative rows along a applied to
+  //     the 4th-order centred difference along b (ACOFY1, BCOFY1; :151-230,
+  //     and at the corners :690-750);
+  //   eb <= 1 < ea: the same with a and b exchanged (ACOFX1, BCOFX1;
+  //     :399-480, :628-688);
+  //   ea, eb <= 1: the corner point (one-sided/one-sided, ACC1XY, :516-528),
+  //     its diagonal neighbour (ACC2XY, :530-542) and the two edge points,
+  //     first-point rows (ACF1XY) of second-point differences (ACF2XY)
+  //     (:544-626).
+  // Each right end is the mirror image of the left one: offsets are taken
+  // inward and a one-sided result changes sign once per mirrored direction
+  // (which reorders the four terms of a difference against the source, a
+  // rounding-level change).
+  template <int plane>
+  void dmix_ends(Field& F, Field& D) {
+    const FD& c = fd;
+    const double s1 = plane == 2 ? fd.ovdely : fd.ovdelx;
+    const double s2 = plane == 0 ? fd.ovdely : fd.ovdelz;
+    const int na = plane == 2 ? ny : nx, nb = plane == 0 ? ny : nz, nc = plane == 0 ? nz : plane == 1 ? ny : nx;
+    const bool bal = (plane == 2 ? nendyl : nendxl) == NBOUND, bar = (plane == 2 ? nendyr : nendxr) == NBOUND;
+    const bool bbl = (plane == 0 ? nendyl : nendzl) == NBOUND, bbr = (plane == 0 ? nendyr : nendzr) == NBOUND;
+    const double my1 = 4.0 / 3.0 / 2.0, my2 = -1.0 / 3.0 / 4.0;  // ACOFX1/ACOFY1, BCOFX1/BCOFY1
+    const double c3[2] = {(4.0 / 3.0) / 4.0, (-1.0 / 3.0) / 4.0 / 4.0};
+    const double c4[3] = {(3.0 / 2.0) / 4.0, (-3.0 / 5.0) / 4.0 / 4.0, (1.0 / 1.0e1) / 4.0 / 9.0};
+    const double c5[4] = {(8.0 / 5.0) / 4.0, (-4.0 / 5.0) / 4.0 / 4.0, (8.0 / 3.5e1) / 4.0 / 9.0,
+                          (-1.0 / 3.5e1) / 4.0 / 1.6e1};
+    const double w0[4] = {c.acof1, c.bcof1, c.ccof1, c.dcof1};  // ACF1XY..: offsets +1..+4
+    const double w1[4] = {c.acof2, c.bcof2, c.ccof2, c.dcof2};  // ACF2XY..: offsets -1, +1, +2, +3
+    const int o1[4] = {-1, 1, 2, 3};
+    const double k1[4] = {c.acc1xy, c.bcc1xy, c.ccc1xy, c.dcc1xy};
+    const double k2[4] = {c.acc2xy, c.bcc2xy, c.ccc2xy, c.dcc2xy};
+    const int far = 1 << 20;
+#pragma omp parallel for schedule(static)
+    for (int r = 1; r <= nc; ++r)
+      for (int b = 1; b <= nb; ++b)
+        for (int a = 1; a <= na; ++a) {
+          const int la = bal ? a - 1 : far, ra = bar ? na - a : far;
+          const int lb = bbl ? b - 1 : far, rb = bbr ? nb - b : far;
+          const int ea = la < ra ? la : ra, eb = lb < rb ? lb : rb;
+          const int sa = (ea <= 1 && ra < la) ? -1 : 1, sb = (eb <= 1 && rb < lb) ? -1 : 1;
+          auto w = [&](int ia, int ib) -> double {  // ia, ib points inward from (a, b)
+            const int aa = a + sa * ia, bb = b + sb * ib;
+            if (plane == 0) return F(aa, bb, r);
+            if (plane == 1) return F(aa, r, bb);
+            return F(r, aa, bb);
+          };
+          auto dg = [&](int m) { return w(m, m) - w(m, -m) - w(-m, m) + w(-m, -m); };
+          double v;
+          if (ea >= 5 && eb >= 5) {
+            v = c.acofxy * dg(1) + c.bcofxy * dg(2) + c.ccofxy * dg(3) + c.dcofxy * dg(4) + c.ecofxy * dg(5);
+          } else if (ea >= 2 && eb >= 2) {
+            const int m = ea < eb ? ea : eb;
+            if (m == 2) v = c3[0] * dg(1) + c3[1] * dg(2);
+            else if (m == 3) v = c4[0] * dg(1) + c4[1] * dg(2) + c4[2] * dg(3);
+            else v = c5[0] * dg(1) + c5[1] * dg(2) + c5[2] * dg(3) + c5[3] * dg(4);
+          } else if (eb >= 2) {  // one-sided along a, centred along b
+            auto g = [&](int i1, int i0) {
+              return my1 * (w(i1, 1) - w(i1, -1) - w(i0, 1) + w(i0, -1)) +
+                     my2 * (w(i1, 2) - w(i1, -2) - w(i0, 2) + w(i0, -2));
+            };
+            v = 0.0;
+            for (int m = 0; m < 4; ++m) v += ea == 0 ? w0[m] * g(m + 1, 0) : w1[m] * g(o1[m], 0);
+            v *= sa;
+          } else if (ea >= 2) {  // one-sided along b, centred along a
+            auto g = [&](int i1, int i0) {
+              return my1 * (w(1, i1) - w(-1, i1) - w(1, i0) + w(-1, i0)) +
+                     my2 * (w(2, i1) - w(-2, i1) - w(2, i0) + w(-2, i0));
+            };
+            v = 0.0;
+            for (int m = 0; m < 4; ++m) v += eb == 0 ? w0[m] * g(m + 1, 0) : w1[m] * g(o1[m], 0);
+            v *= sb;
+          } else {
+            v = 0.0;
+            if (ea == 0 && eb == 0) {
+              for (int m = 0; m < 4; ++m) {
+                const int d = m + 1;
+                v += k1[m] * (w(d, d) - w(d, 0) - w(0, d) + w(0, 0));
+              }
+            } else if (ea == 1 && eb == 1) {
+              for (int m = 0; m < 4; ++m) {
+                const int d = o1[m];
+                v += k2[m] * (w(d, d) - w(d, 0) - w(0, d) + w(0, 0));
+              }
+            } else if (ea == 0) {  // eb == 1: first-point rows along a
+              for (int m = 0; m < 4; ++m) {
+                double t = 0.0;
+                for (int j = 0; j < 4; ++j)
+                  t += w1[j] * (w(m + 1, o1[j]) - w(m + 1, 0) - w(0, o1[j]) + w(0, 0));
+                v += w0[m] * t;
+              }
+            } else {  // ea == 1, eb == 0: first-point rows along b
+              for (int m = 0; m < 4; ++m) {
+                double t = 0.0;
+                for (int j = 0; j < 4; ++j)
+                  t += w1[j] * (w(o1[j], m + 1) - w(0, m + 1) - w(o1[j], 0) + w(0, 0));
+                v += w0[m] * t;
+              }
+            }
+            v *= sa * sb;
+          }
+          double& out = plane == 0 ? D(a, b, r) : plane == 1 ? D(a, r, b) : D(r, a, b);
+          out = v * s1 * s2;
+        }
   }
   void dfbydx(Field& F, Field& D) { d1<0>(F, D); }
   void dfbydy(Field& F, Field& D) { d1<1>(F, D); }
@@ -2171,6 +2289,8 @@ int oracle_chem_scalar(void* h, const char* name, double* out) {
       {"dcfs2", f.dcfs2},   {"ecfs2", f.ecfs2},   {"acfs3", f.acfs3},   {"bcfs3", f.bcfs3},   {"acfs4", f.acfs4},
       {"bcfs4", f.bcfs4},   {"ccfs4", f.ccfs4},   {"acfs5", f.acfs5},   {"bcfs5", f.bcfs5},   {"ccfs5", f.ccfs5},
       {"dcfs5", f.dcfs5},   {"acofxy", f.acofxy}, {"bcofxy", f.bcofxy}, {"ccofxy", f.ccofxy},
+      {"acc1xy", f.acc1xy}, {"bcc1xy", f.bcc1xy}, {"ccc1xy", f.ccc1xy}, {"dcc1xy", f.dcc1xy},
+      {"acc2xy", f.acc2xy}, {"bcc2xy", f.bcc2xy}, {"ccc2xy", f.ccc2xy}, {"dcc2xy", f.dcc2xy},
       {"dcofxy", f.dcofxy}, {"ecofxy", f.ecofxy}, {"deltax", f.deltax}, {"deltay", f.deltay}, {"deltaz", f.deltaz}};
   // RK registers per unit dt: rk.lhs<i> = BCOFRK(i), rk.rhs<i> = ACOFRK(i),
   // rk.err<i> = BCOFRK(i)-BHATRK(i), i = 1..5.

@@ -115,8 +115,8 @@ void check_config(const senga_config& c, int nspec) {
       throw Error(SENGA_ERR_ARG, "grid extent must be at least 12 points per bounded direction");
     if ((l == SENGA_NPERI) != (r == SENGA_NPERI))
       throw Error(SENGA_ERR_ARG, "periodic end conditions must be set on both faces of a direction");
-    if (l != SENGA_NPERI && (d != 0 || l != SENGA_NBOUND || r != SENGA_NBOUND))
-      throw Error(SENGA_ERR_UNSUPPORTED, "bounded boxes: only x may be bounded (NBOUND on both x faces)");
+    if (l != SENGA_NPERI && (l != SENGA_NBOUND || r != SENGA_NBOUND))
+      throw Error(SENGA_ERR_UNSUPPORTED, "a bounded direction takes NBOUND on both of its faces");
   }
   if (c.tstep <= 0.0) throw Error(SENGA_ERR_ARG, "tstep must be positive");
   if (nspec < 1 || nspec > SENGA_NSPCMX) throw Error(SENGA_ERR_ARG, "nspec out of range");
@@ -130,9 +130,19 @@ void set_rk(senga_ctx* c, double tstep) {
   }
 }
 
-void run_rhs(senga_ctx* c) {
+// The right-hand side needs conditions on every bounded face: the x faces
+// take NSCBC (senga_set_nscbc); no y or z face conditions are built, so a box
+// bounded in y or z serves the operator-level derivatives and the filter only.
+void require_rhs(const senga_ctx* c) {
+  if (!c->geo.per[1] || !c->geo.per[2])
+    throw Error(SENGA_ERR_UNSUPPORTED,
+                "bounded y or z direction: only senga_deriv and the filter run on this box (no y/z face conditions)");
   if (!c->geo.per[0] && !c->nscbc)
     throw Error(SENGA_ERR_UNSUPPORTED, "a bounded x direction needs its face conditions (senga_set_nscbc)");
+}
+
+void run_rhs(senga_ctx* c) {
+  require_rhs(c);
   if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->stream);  // BOUNDT
   launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
   if (c->rrte)  // RRTE = RATE (src/rhscal.f:828)
@@ -383,6 +393,7 @@ int senga_step_graph(senga_ctx* c, int nsteps) {
   if (c->cfg.adaptive) return senga_step(c, nsteps);  // dt changes every step: no fixed graph
   return guard([&] {
     if (!c->graph) {
+      require_rhs(c);  // before the capture, so a refusal leaves the stream uncaptured
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
@@ -414,6 +425,7 @@ int senga_rhs_host(senga_ctx* c, double* rhs, double* trun, double* prun) {
 int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
   if (!c || !ms) return fail(SENGA_ERR_ARG, "senga_profile_step: null argument");
   return guard([&] {
+    require_rhs(c);
     cudaEvent_t ev[21];
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (int k = 0; k < 4; ++k) ms[k] = 0.0;

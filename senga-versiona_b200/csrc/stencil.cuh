@@ -181,6 +181,72 @@ __device__ __forceinline__ double dmcore_b(const V2& v, int c, int n) {
   return p2a * g2(L - 1, L) + p2b * g2(L - 1, L - 2) + p2c * g2(L - 1, L - 3) + p2d * g2(L - 1, L - 4);
 }
 
+// Mixed derivative with the second direction bounded, or both
+// (src/d2fdxy.f:393-1924; d2fdxz.f and d2fdyz.f likewise). ea, eb are the
+// point's distances from the nearer bounded end of each direction (a large
+// number for a periodic one), ra_a / ra_b whether that end is the right one.
+// Classification per point:
+//   ea, eb >= 5: interior scheme;
+//   ea, eb >= 2: diagonal 4th/6th/8th-order scheme of min(ea, eb) (end
+//     sections' third to fifth rows and the corners' inner blocks);
+//   ea <= 1 < eb (or the reverse): one-sided first-derivative rows along the
+//     near direction on the 4th-order centred difference along the other;
+//   ea, eb <= 1: corner point (ACC1XY, :516-528), its diagonal neighbour
+//     (ACC2XY, :530-542), the two edge points (first-point rows of
+//     second-point differences, :544-626).
+// A right end is the mirror image of the left: offsets are taken inward and
+// a one-sided result changes sign per mirrored direction. v(ma, mb) as for
+// dmcore.
+namespace fdc {
+constexpr double k1a = p1a, k1b = p1b * 2.0 / 4.0, k1c = p1c * 3.0 / 9.0, k1d = p1d * 4.0 / 1.6e1;  // ACC1XY..
+constexpr double k2a = -p2a, k2b = p2b, k2c = p2c * 2.0 / 4.0, k2d = p2d * 3.0 / 9.0;                // ACC2XY..
+}  // namespace fdc
+template <class V2>
+__device__ __forceinline__ double dmcore_ends(const V2& v, int ea, bool ra_a, int eb, bool ra_b) {
+  using namespace fdc;
+  if (ea >= 5 && eb >= 5) return dmcore(v);
+  const int sa = (ea <= 1 && ra_a) ? -1 : 1, sb = (eb <= 1 && ra_b) ? -1 : 1;
+  auto w = [&](int ia, int ib) { return v(sa * ia, sb * ib); };
+  auto dg = [&](int m) { return w(m, m) - w(m, -m) - w(-m, m) + w(-m, -m); };
+  if (ea >= 2 && eb >= 2) {
+    switch (ea < eb ? ea : eb) {
+      case 2: return m3a * dg(1) + m3b * dg(2);
+      case 3: return m4a * dg(1) + m4b * dg(2) + m4c * dg(3);
+      default: return m5a * dg(1) + m5b * dg(2) + m5c * dg(3) + m5d * dg(4);
+    }
+  }
+  if (eb >= 2) {  // one-sided along a, centred along b
+    auto g = [&](int i1, int i0) {
+      return my1 * (w(i1, 1) - w(i1, -1) - w(i0, 1) + w(i0, -1)) + my2 * (w(i1, 2) - w(i1, -2) - w(i0, 2) + w(i0, -2));
+    };
+    const double r = ea == 0 ? p1a * g(1, 0) + p1b * g(2, 0) + p1c * g(3, 0) + p1d * g(4, 0)
+                             : p2a * g(-1, 0) + p2b * g(1, 0) + p2c * g(2, 0) + p2d * g(3, 0);
+    return r * sa;
+  }
+  if (ea >= 2) {  // one-sided along b, centred along a
+    auto g = [&](int i1, int i0) {
+      return my1 * (w(1, i1) - w(-1, i1) - w(1, i0) + w(-1, i0)) + my2 * (w(2, i1) - w(-2, i1) - w(2, i0) + w(-2, i0));
+    };
+    const double r = eb == 0 ? p1a * g(1, 0) + p1b * g(2, 0) + p1c * g(3, 0) + p1d * g(4, 0)
+                             : p2a * g(-1, 0) + p2b * g(1, 0) + p2c * g(2, 0) + p2d * g(3, 0);
+    return r * sb;
+  }
+  auto q = [&](int ia, int ib) { return w(ia, ib) - w(ia, 0) - w(0, ib) + w(0, 0); };
+  double r;
+  if (ea == 0 && eb == 0) {
+    r = k1a * q(1, 1) + k1b * q(2, 2) + k1c * q(3, 3) + k1d * q(4, 4);
+  } else if (ea == 1 && eb == 1) {
+    r = k2a * q(-1, -1) + k2b * q(1, 1) + k2c * q(2, 2) + k2d * q(3, 3);
+  } else if (ea == 0) {  // eb == 1: first-point rows along a of second-point differences along b
+    auto t = [&](int m) { return p2a * q(m, -1) + p2b * q(m, 1) + p2c * q(m, 2) + p2d * q(m, 3); };
+    r = p1a * t(1) + p1b * t(2) + p1c * t(3) + p1d * t(4);
+  } else {  // ea == 1, eb == 0
+    auto t = [&](int m) { return p2a * q(-1, m) + p2b * q(1, m) + p2c * q(2, m) + p2d * q(3, m); };
+    r = p1a * t(1) + p1b * t(2) + p1c * t(3) + p1d * t(4);
+  }
+  return r * (sa * sb);
+}
+
 // ---- global-memory forms (operator-level entry points) ----------------------
 // Periodic directions wrap the index; bounded ones never leave the domain
 // because the closures only read inward.
@@ -200,6 +266,12 @@ template <int DA, int DB, class F>
 __device__ __forceinline__ double DM(const Geo& g, const Pt& p, const F& f) {
   const int ca = crd<DA>(p), cb = crd<DB>(p);
   auto v = [&](int ma, int mb) { return f(p.q + woff<DA>(g, ca, ma) + woff<DB>(g, cb, mb)); };
+  if (!g.per[DB]) {
+    constexpr int kFar = 1 << 20;
+    const int la = g.per[DA] ? kFar : ca, ra = g.per[DA] ? kFar : ext<DA>(g) - 1 - ca;
+    const int lb = cb, rb = ext<DB>(g) - 1 - cb;
+    return dmcore_ends(v, la < ra ? la : ra, ra < la, lb < rb ? lb : rb, rb < lb) * g.ovd[DA] * g.ovd[DB];
+  }
   if (!g.per[DA]) return dmcore_b(v, ca, ext<DA>(g)) * g.ovd[DA] * g.ovd[DB];
   return dmcore(v) * g.ovd[DA] * g.ovd[DB];
 }

@@ -73,8 +73,8 @@ def test_bad_inputs_return_status_not_abort():
 
     chem = senga.Chem(cases.CHEM_1STEP)
     diff = senga.Diff(None, chem)
-    with pytest.raises(senga.SengaError, match="status 5"):
-        senga.Box((16, 16, 16), (1e-3,) * 3, chem, diff, 1e-8, nend=(2, 2, 1, 1, 2, 2))
+    with pytest.raises(senga.SengaError, match="status 5"):  # a bounded direction takes NBOUND on both faces
+        senga.Box((16, 16, 16), (1e-3,) * 3, chem, diff, 1e-8, nend=(2, 2, 1, 3, 2, 2))
     with pytest.raises(senga.SengaError, match="status 1"):  # bounded x needs 12 points
         senga.Box((11, 16, 16), (1e-3,) * 3, chem, diff, 1e-8, nend=(1, 1, 2, 2, 2, 2))
 
