@@ -173,7 +173,10 @@ int senga_ctx_info(senga_ctx* ctx, int* mech, int64_t* device_bytes);
  * pointwise thermochemistry kernel. No counterpart in the reference. */
 int senga_fp64_peak(int device, double* tflops);
 
-/* Status word of the last steps: bit 0 = TEMPER non-convergence. */
+/* Status word of the last steps: bit 0 = TEMPER non-convergence; bit 1 =
+ * TEMPIN found no sign change of the energy residual in [200, 3000] K (the
+ * reference stops there); bit 2 = TEMPIN still unconverged after 200
+ * bisections (the reference bisects without limit). */
 int senga_get_status(senga_ctx* ctx, int* status);
 
 /* ---- operator-level entry points (unit parity) -----------------------------
@@ -189,6 +192,16 @@ int senga_get_status(senga_ctx* ctx, int* status);
  * and the filter only (the RHS entry points return SENGA_ERR_UNSUPPORTED:
  * no y/z face conditions are built). */
 int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
+
+/* TEMPIN (src/tempin.f:58-524): start-up temperature of the state in the
+ * context (the conserved fields as uploaded, e.g. a restart dump, which
+ * carries no temperature). Per point the energy residual
+ * sum_k rhoY_k e_k(T) + 1/2 rho|u|^2 - rho E is bracketed from the guess trin
+ * (cont.dat's TRIN) in 50 K steps inside [200, 3000] K and bisected until it
+ * is below 1e-4; TRUN, ITNDEX and PRUN are set on the device, and copied to
+ * trun, itndex and prun (host arrays of the interior, each may be NULL).
+ * Failures set status bits 1 and 2 (senga_get_status) instead of stopping. */
+int senga_tempin_host(senga_ctx* ctx, double trin, double* trun, int32_t* itndex, double* prun);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
 
 /* Mixture-averaged transport switches of cont.dat's transport line

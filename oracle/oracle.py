@@ -59,6 +59,7 @@ def _get():
         lib.oracle_rhs.argtypes = [C.c_void_p, dp, dp, dp]
         lib.oracle_deriv.argtypes = [C.c_void_p, C.c_int, dp, dp]
         lib.oracle_chrate.argtypes = [C.c_void_p, dp]
+        lib.oracle_tempin.argtypes = [C.c_void_p, C.c_double, C.c_int, dp, ip, dp, C.POINTER(C.c_long)]
         lib.oracle_chem_scalar.argtypes = [C.c_void_p, C.c_char_p, dp]
         lib.oracle_filter.argtypes = [C.c_void_p, C.c_int]
         lib.oracle_set_adaptive.argtypes = [C.c_void_p, C.c_int]
@@ -144,6 +145,17 @@ class Oracle:
         if _get().oracle_chrate(self.h, _dp(r)) != 0:
             raise RuntimeError("oracle_chrate: " + _get().oracle_last_error().decode())
         return r
+
+    def tempin(self, trin, maxbis=200):
+        """TEMPIN on the state set last (its U register): T, ITNDEX, p and
+        (bracket failures, bisection-limit failures)."""
+        t = np.empty(self.shape)
+        it = np.empty(self.shape, dtype=np.int32)
+        p = np.empty(self.shape)
+        nf = (C.c_long * 2)()
+        _get().oracle_tempin(self.h, float(trin), int(maxbis), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)), _dp(p),
+                             nf)
+        return t, it, p, (nf[0], nf[1])
 
     def deriv(self, kind, f):
         a = np.ascontiguousarray(f, dtype=np.float64)

@@ -983,6 +983,114 @@ struct Oracle {
     if (failed) throw std::runtime_error("oracle TEMPER: Newton iteration failed to converge");
   }
 
+  // ---- TEMPIN: src/tempin.f:58-524 (start-up T and p by bisection) ----
+  // Per point over the interior: residual R(T) = sum_k rhoY_k e_k(T)
+  // + 1/2 rho|u|^2 - rho E with every species' interval located at T
+  // (:75-140); from the guess TRIN step by TININC = 50 K up (R < 0, :150-250)
+  // or down (R > 0, :258-352) until R changes sign, within [TLIMLO, TLIMHI] =
+  // [200, 3000] K, then bisect (:364-436) until |R| < TOLTMP = 1e-4; then
+  // ITNDEX, cp_mix and p = T rho R_mix (:444-508). Returns the number of
+  // points whose bracket left [TLIMLO, TLIMHI] (where the source stops) and
+  // of points still unconverged after maxbis bisections (the source bisects
+  // without limit); T is left at the last iterate there.
+  std::pair<long, long> tempin(double trin, int maxbis) {
+    const double TOLTMP = 1.0e-4, TININC = 5.0e1, TLIMLO = 2.0e2, TLIMHI = 3.0e3;
+    long nbracket = 0, nbisect = 0;
+    for (int kc = 1; kc <= nz; ++kc)
+      for (int jc = 1; jc <= ny; ++jc)
+        for (int ic = 1; ic <= nx; ++ic) {
+          const double ukuk = (urhs(ic, jc, kc) * urhs(ic, jc, kc) + vrhs(ic, jc, kc) * vrhs(ic, jc, kc) +
+                               wrhs(ic, jc, kc) * wrhs(ic, jc, kc)) / drhs(ic, jc, kc);
+          const double tuk2me = 0.5 * ukuk - erhs(ic, jc, kc);
+          auto resid = [&](double tempor) {
+            double tcoeff[NCTMAX + 1];
+            tcoeff[0] = tuk2me;
+            for (int icp = 1; icp <= NCTMAX; ++icp) tcoeff[icp] = 0.0;
+            for (int is = 1; is <= nspec; ++is) {
+              int itint = 1;
+              while (tempor > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
+              const int k2 = Chem::c2(itint, is);
+              const double y = yrhs[is - 1](ic, jc, kc);
+              tcoeff[0] = tcoeff[0] + y * ch.amascp[Chem::c3(ch.ncenth[k2], itint, is)];
+              tcoeff[1] = tcoeff[1] + y * ch.amasct[Chem::c3(1, itint, is)];
+              for (int icp = 2; icp <= ch.ncpoly[k2] && icp <= NCTMAX; ++icp)
+                tcoeff[icp] = tcoeff[icp] + y * ch.amasct[Chem::c3(icp, itint, is)];
+            }
+            double r = tcoeff[NCTMAX];
+            for (int icp = NCTMAX - 1; icp >= 1; --icp) r = tcoeff[icp] + r * tempor;
+            return tcoeff[0] + r * tempor;
+          };
+          double tlower = TLIMLO, tupper = TLIMHI, tempor = trin;
+          bool fnconv = true, lost = false;
+          double r = resid(tempor);
+          if (std::fabs(r) < TOLTMP) {
+            fnconv = false;
+          } else if (r < 0.0) {
+            for (;;) {  // too low: step up
+              tlower = tempor;
+              tempor = tempor + TININC;
+              r = resid(tempor);
+              if (std::fabs(r) < TOLTMP) { fnconv = false; break; }
+              if (r < 0.0) {
+                if (tempor < TLIMHI) continue;
+                lost = true;
+                break;
+              }
+              if (r > 0.0) tupper = tempor;
+              break;
+            }
+          } else if (r > 0.0) {
+            for (;;) {  // too high: step down
+              tupper = tempor;
+              tempor = tempor - TININC;
+              r = resid(tempor);
+              if (std::fabs(r) < TOLTMP) { fnconv = false; break; }
+              if (r > 0.0) {
+                if (tempor > TLIMLO) continue;
+                lost = true;
+                break;
+              }
+              if (r < 0.0) tlower = tempor;
+              break;
+            }
+          }
+          if (lost) {
+            ++nbracket;
+          } else if (fnconv) {
+            int it = 0;
+            for (; it < maxbis; ++it) {
+              tempor = 0.5 * (tlower + tupper);
+              r = resid(tempor);
+              if (std::fabs(r) < TOLTMP) break;
+              if (r < 0.0) tlower = tempor;
+              else if (r > 0.0) tupper = tempor;
+              else break;  // NaN: the source leaves the loop too
+            }
+            if (it == maxbis) ++nbisect;
+          }
+          trun(ic, jc, kc) = tempor;
+          int itnew = 0;
+          double tr = 0.0, st7 = 0.0;
+          for (int is = 1; is <= nspec; ++is) {
+            int itint = 1;
+            while (tempor > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
+            int pw = 1;
+            for (int q = 0; q < is - 1; ++q) pw *= NTBASE;
+            itnew = itnew + (itint - 1) * pw;
+            const int k2 = Chem::c2(itint, is);
+            double cpf = ch.amascp[Chem::c3(ch.ncpoly[k2], itint, is)];
+            for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) cpf = cpf * tempor + ch.amascp[Chem::c3(icp, itint, is)];
+            tr = tr + yrhs[is - 1](ic, jc, kc) * cpf;
+            st7 = st7 + yrhs[is - 1](ic, jc, kc) * ch.rgspec[is - 1];
+          }
+          itndex(ic, jc, kc) = itnew;
+          transp(ic, jc, kc) = tr / drhs(ic, jc, kc);
+          store7(ic, jc, kc) = st7;
+          prun(ic, jc, kc) = tempor * st7;
+        }
+    return {nbracket, nbisect};
+  }
+
   // ---- CHRATE: src/chrate.f:146-741 (per point; same operation order) ----
   void chrate_point(int ic, int jc, int kc) {
     const double YSMALL = 1.0e-30, YDENOM = 1.0e-15, CLNTEN = std::log(10.0);
@@ -2035,6 +2143,24 @@ int oracle_set_state(void* h, const double* fields, const double* t, const int32
         int ii = wrap(i, o->nx), jj = wrap(j, o->ny), kk = wrap(k, o->nz);
         o->trun(i, j, k) = o->trun(ii, jj, kk);
         o->itndex(i, j, k) = o->itndex(ii, jj, kk);
+      }
+  return 0;
+}
+
+// TEMPIN on the state set last; T, ITNDEX and p of the interior (each may
+// be null); nfail[0] = points whose bracket left [200, 3000] K, nfail[1] =
+// points unconverged after maxbis bisections.
+int oracle_tempin(void* h, double trin, int maxbis, double* t, int32_t* itn, double* p, long* nfail) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  const auto fails = o->tempin(trin, maxbis);
+  if (nfail) { nfail[0] = fails.first; nfail[1] = fails.second; }
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j)
+      for (int i = 1; i <= o->nx; ++i) {
+        size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
+        if (t) t[q] = o->trun(i, j, k);
+        if (itn) itn[q] = o->itndex(i, j, k);
+        if (p) p[q] = o->prun(i, j, k);
       }
   return 0;
 }

@@ -485,6 +485,20 @@ int senga_get_status(senga_ctx* c, int* status) {
   });
 }
 
+int senga_tempin_host(senga_ctx* c, double trin, double* trun, int32_t* itndex, double* prun) {
+  if (!c) return fail(SENGA_ERR_ARG, "senga_tempin_host: null context");
+  if (!(trin > 0.0)) return fail(SENGA_ERR_ARG, "senga_tempin_host: trin must be a positive temperature");
+  return guard([&] {
+    const int64_t n = c->geo.n;
+    launch_tempin(n, c->nspec, c->f.uin, c->d_chem, trin, c->f.t, c->f.itn, c->f.p, c->d_status, c->stream);
+    CK(cudaGetLastError());
+    if (trun) CK(cudaMemcpyAsync(trun, c->f.t, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (itndex) CK(cudaMemcpyAsync(itndex, c->f.itn, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (prun) CK(cudaMemcpyAsync(prun, c->f.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
 int senga_deriv(senga_ctx* c, int kind, const double* f, double* out) {
   if (!c || !f || !out || kind < 0 || kind > 8) return fail(SENGA_ERR_ARG, "senga_deriv: bad argument");
   return guard([&] {

@@ -164,6 +164,7 @@ def _load():
         "senga_filter_field_host": (ip, [vp, ip, dp, dp]),
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
+        "senga_tempin_host": (ip, [vp, C.c_double, dp, i32p, dp]),
         "senga_temper_host": (ip, [vp, dp, dp]),
         "senga_chrate_host": (ip, [vp, dp]),
         "senga_batch_create": (ip, [ip, C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), ip, C.POINTER(vp)]),
@@ -494,6 +495,16 @@ class Box:
         return r
 
     # ---- derivative family (FUNCTN interior array -> FDERIV) ----
+    def tempin(self, trin):
+        """TEMPIN on the uploaded conserved state: (T, ITNDEX, p) of every
+        point, also left on the device for the next step."""
+        t = np.empty(self.shape)
+        it = np.empty(self.shape, dtype=np.int32)
+        p = np.empty(self.shape)
+        _check(lib.senga_tempin_host(self.h, float(trin), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)), _dp(p)),
+               "senga_tempin_host")
+        return t, it, p
+
     def deriv(self, kind, f):
         a = np.ascontiguousarray(f, dtype=np.float64)
         assert a.shape == self.shape
