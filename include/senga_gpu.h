@@ -202,6 +202,17 @@ int senga_deriv(senga_ctx* ctx, int kind, const double* f, double* out);
  * trun, itndex and prun (host arrays of the interior, each may be NULL).
  * Failures set status bits 1 and 2 (senga_get_status) instead of stopping. */
 int senga_tempin_host(senga_ctx* ctx, double trin, double* trun, int32_t* itndex, double* prun);
+
+/* Initial flame FLAMIN (src/flamin.f:44-322) and INDATA's conversion of the
+ * start-up primitives to the conserved state (src/indata.f:1233-1394), on the
+ * device: a planar flame across x, progress (1 + erf((x - 5 mm)/0.5 mm))/2,
+ * between the reactant (Y_1 = 0.011606960, Y_2 = 0.230295282, T = trin) and
+ * the product (Y_2 = 0.139255233, Y_3 = 0.102581446, T = 1417.2 K) states as
+ * the reference codes them (the last species the remainder), pressure prin,
+ * u = drin urin / rho, v and w from the host arrays (interior, NULL = 0).
+ * Sets both registers, TRUN and ITNDEX, as senga_upload_state_host would. */
+int senga_flamin(senga_ctx* ctx, double trin, double prin, double drin, double urin, const double* v,
+                 const double* w);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
 
 /* Mixture-averaged transport switches of cont.dat's transport line

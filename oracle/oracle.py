@@ -59,6 +59,7 @@ def _get():
         lib.oracle_rhs.argtypes = [C.c_void_p, dp, dp, dp]
         lib.oracle_deriv.argtypes = [C.c_void_p, C.c_int, dp, dp]
         lib.oracle_chrate.argtypes = [C.c_void_p, dp]
+        lib.oracle_flamin.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, dp, dp]
         lib.oracle_tempin.argtypes = [C.c_void_p, C.c_double, C.c_int, dp, ip, dp, C.POINTER(C.c_long)]
         lib.oracle_chem_scalar.argtypes = [C.c_void_p, C.c_char_p, dp]
         lib.oracle_filter.argtypes = [C.c_void_p, C.c_int]
@@ -145,6 +146,14 @@ class Oracle:
         if _get().oracle_chrate(self.h, _dp(r)) != 0:
             raise RuntimeError("oracle_chrate: " + _get().oracle_last_error().decode())
         return r
+
+    def flamin(self, trin, prin, drin, urin, v=None, w=None):
+        """FLAMIN's planar flame and INDATA's conversion to the conserved state."""
+        va = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        if _get().oracle_flamin(self.h, float(trin), float(prin), float(drin), float(urin),
+                                None if va is None else _dp(va), None if wa is None else _dp(wa)) != 0:
+            raise RuntimeError("oracle_flamin: " + _get().oracle_last_error().decode())
 
     def tempin(self, trin, maxbis=200):
         """TEMPIN on the state set last (its U register): T, ITNDEX, p and

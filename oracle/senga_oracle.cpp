@@ -983,6 +983,91 @@ struct Oracle {
     if (failed) throw std::runtime_error("oracle TEMPER: Newton iteration failed to converge");
   }
 
+  // ---- FLAMIN: src/flamin.f:44-322, then INDATA's conversion of the
+  // primitives to the conserved registers, src/indata.f:1233-1394 ----
+  // ERFUNC (src/erfunc.f:40-79): Abramowitz and Stegun 7.1.26.
+  static double erfunc(double argmnt) {
+    const double pcoeff = 0.3275911;
+    const double ecoeff[5] = {0.254829592, -0.284496736, 1.421413741, -1.453152027, 1.061405429};
+    const double zvalue = std::fabs(argmnt);
+    const double tvalue = 1.0 / (1.0 + pcoeff * zvalue);
+    double etotal = ecoeff[4];
+    for (int ic = 3; ic >= 0; --ic) etotal = ecoeff[ic] + etotal * tvalue;
+    etotal = etotal * tvalue;
+    const double r = 1.0 - etotal * std::exp(-zvalue * zvalue);
+    return argmnt < 0.0 ? -r : r;
+  }
+  // v, w: interior arrays (x fastest) or null for zero
+  void flamin(double trin, double prin, double drin, double urin, const double* v, const double* w) {
+    const double clocat = 5.0e-3, cthick = 5.0e-4;
+    const double trinr = trin, trinp = (double)1417.2f;  // a default REAL constant in the source
+    std::vector<double> yrinr(nspec, 0.0), yrinp(nspec + 1, 0.0);
+    yrinr[0] = 1.1606960e-2;
+    yrinr[1] = 2.30295282e-1;
+    yrinp[1] = 1.39255233e-1;
+    yrinp[2] = 1.02581446e-1;  // with three species this is the remainder, overwritten below
+    double sr = 0.0, sp = 0.0;
+    for (int is = 0; is < nspec - 1; ++is) { sr = sr + yrinr[is]; sp = sp + yrinp[is]; }
+    yrinr[nspec - 1] = 1.0 - sr;
+    yrinp[nspec - 1] = 1.0 - sp;
+    const double deltag = cf.xgdlen / (double)(float)(nx - 1);
+    std::vector<double> crin(nx + 1);
+    for (int ic = 1; ic <= nx; ++ic) {
+      const double xcoord = (double)(float)(ic - 1) * deltag;
+      crin[ic] = 0.5 * (1.0 + erfunc((xcoord - clocat) / cthick));
+    }
+    for (int kc = 1; kc <= nz; ++kc)
+      for (int jc = 1; jc <= ny; ++jc)
+        for (int ic = 1; ic <= nx; ++ic) {
+          const size_t q = (size_t)(ic - 1) + (size_t)nx * ((jc - 1) + (size_t)ny * (kc - 1));
+          double y[64];
+          double ylast = 0.0;
+          for (int is = 0; is < nspec - 1; ++is) {
+            y[is] = yrinr[is] + crin[ic] * (yrinp[is] - yrinr[is]);
+            ylast = ylast + y[is];
+          }
+          y[nspec - 1] = 1.0 - ylast;
+          const double t = trinr + crin[ic] * (trinp - trinr);
+          double st1 = 0.0;
+          for (int is = 0; is < nspec; ++is) st1 = st1 + ch.rgspec[is] * y[is];
+          const double dflam = prin / (st1 * t);
+          const double u = drin * urin / dflam;
+          // INDATA: density from PRUN = PRIN, interval index, energy, products
+          const double rt = st1 * t;
+          const double rho = prin / rt;
+          int itnew = 0;
+          double e = 0.0;
+          for (int is = 1; is <= nspec; ++is) {
+            int itint = 1;
+            while (t > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
+            int pw = 1;
+            for (int qq = 0; qq < is - 1; ++qq) pw *= NTBASE;
+            itnew = itnew + (itint - 1) * pw;
+            const int k2 = Chem::c2(itint, is);
+            double fornow = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
+            for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) fornow = fornow * t + ch.amasch[Chem::c3(icp, itint, is)];
+            fornow = ch.amasch[Chem::c3(ch.ncenth[k2], itint, is)] + fornow * t;
+            e = e + fornow * y[is - 1];
+          }
+          const double vv = v ? v[q] : 0.0, ww = w ? w[q] : 0.0;
+          e = e - rt + 0.5 * (u * u + vv * vv + ww * ww);
+          drun(ic, jc, kc) = rho;
+          urun(ic, jc, kc) = rho * u;
+          vrun(ic, jc, kc) = rho * vv;
+          wrun(ic, jc, kc) = rho * ww;
+          erun(ic, jc, kc) = rho * e;
+          for (int is = 0; is < nspec; ++is) yrun[is](ic, jc, kc) = rho * y[is];
+          drhs(ic, jc, kc) = drun(ic, jc, kc);
+          urhs(ic, jc, kc) = urun(ic, jc, kc);
+          vrhs(ic, jc, kc) = vrun(ic, jc, kc);
+          wrhs(ic, jc, kc) = wrun(ic, jc, kc);
+          erhs(ic, jc, kc) = erun(ic, jc, kc);
+          for (int is = 0; is < nspec; ++is) yrhs[is](ic, jc, kc) = yrun[is](ic, jc, kc);
+          trun(ic, jc, kc) = t;
+          itndex(ic, jc, kc) = itnew;
+        }
+  }
+
   // ---- TEMPIN: src/tempin.f:58-524 (start-up T and p by bisection) ----
   // Per point over the interior: residual R(T) = sum_k rhoY_k e_k(T)
   // + 1/2 rho|u|^2 - rho E with every species' interval located at T
@@ -2145,6 +2230,22 @@ int oracle_set_state(void* h, const double* fields, const double* t, const int32
         o->itndex(i, j, k) = o->itndex(ii, jj, kk);
       }
   return 0;
+}
+
+int oracle_set_state(void* h, const double* fields, const double* t, const int32_t* itn);
+int oracle_get_state(void* h, double* fields, double* t, int32_t* itn);
+
+// FLAMIN + INDATA's conversion: sets both registers, T and ITNDEX (their
+// halo copies refreshed through a get/set round trip).
+int oracle_flamin(void* h, double trin, double prin, double drin, double urin, const double* v, const double* w) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  if (o->nspec < 2) { g_err = "oracle_flamin: needs at least two species"; return 1; }
+  o->flamin(trin, prin, drin, urin, v, w);
+  const size_t n = (size_t)o->nx * o->ny * o->nz;
+  std::vector<double> f((size_t)(5 + o->nspec) * n), t(n);
+  std::vector<int32_t> itn(n);
+  oracle_get_state(h, f.data(), t.data(), itn.data());
+  return oracle_set_state(h, f.data(), t.data(), itn.data());
 }
 
 // TEMPIN on the state set last; T, ITNDEX and p of the interior (each may

@@ -485,6 +485,29 @@ int senga_get_status(senga_ctx* c, int* status) {
   });
 }
 
+int senga_flamin(senga_ctx* c, double trin, double prin, double drin, double urin, const double* v,
+                 const double* w) {
+  if (!c) return fail(SENGA_ERR_ARG, "senga_flamin: null context");
+  if (c->nspec < 2) return fail(SENGA_ERR_ARG, "senga_flamin: needs at least two species");
+  if (!(trin > 0.0) || !(prin > 0.0)) return fail(SENGA_ERR_ARG, "senga_flamin: trin and prin must be positive");
+  return guard([&] {
+    const int64_t n = c->geo.n;
+    struct Staged {  // v and w on the device for the one launch, freed on every path
+      double* p = nullptr;
+      ~Staged() { if (p) cudaFree(p); }
+    } dv, dw;
+    if (v) CK(cudaMalloc(&dv.p, n * sizeof(double)));
+    if (w) CK(cudaMalloc(&dw.p, n * sizeof(double)));
+    if (v) CK(cudaMemcpyAsync(dv.p, v, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (w) CK(cudaMemcpyAsync(dw.p, w, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    launch_flamin(c->geo, c->nspec, c->cfg.xgdlen, trin, prin, drin, urin, c->d_chem, dv.p, dw.p, c->f.run, c->f.uin,
+                  c->f.t, c->f.itn, c->stream);
+    CK(cudaGetLastError());
+    if (c->f.err) CK(cudaMemsetAsync(c->f.err, 0, (size_t)c->nc * n * sizeof(double), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
 int senga_tempin_host(senga_ctx* c, double trin, double* trun, int32_t* itndex, double* prun) {
   if (!c) return fail(SENGA_ERR_ARG, "senga_tempin_host: null context");
   if (!(trin > 0.0)) return fail(SENGA_ERR_ARG, "senga_tempin_host: trin must be a positive temperature");

@@ -185,6 +185,9 @@ int launch_mixt(const Geo& g, const Fields& f, const MixtParams& m, const senga_
                 int nspec, cudaStream_t s);
 
 // Post-processing record fields (post.cu): D, u, v, w, E, T, p, Y_k.
+void launch_flamin(const Geo& g, int nspec, double xgdlen, double trin, double prin, double drin, double urin,
+                   const senga_chem* dchem, const double* v, const double* w, double* run, double* uin, double* t,
+                   int32_t* itn, cudaStream_t s);
 void launch_tempin(int64_t n, int nspec, const double* U, const senga_chem* dchem, double trin, double* t,
                    int32_t* itn, double* p, unsigned int* status, cudaStream_t s);
 void launch_post(int64_t n, int nspec, const double* run, const double* t, const double* p, double* out,

@@ -165,6 +165,7 @@ def _load():
         "senga_deriv": (ip, [vp, ip, vp, vp]),
         "senga_deriv_host": (ip, [vp, ip, dp, dp]),
         "senga_tempin_host": (ip, [vp, C.c_double, dp, i32p, dp]),
+        "senga_flamin": (ip, [vp, C.c_double, C.c_double, C.c_double, C.c_double, dp, dp]),
         "senga_temper_host": (ip, [vp, dp, dp]),
         "senga_chrate_host": (ip, [vp, dp]),
         "senga_batch_create": (ip, [ip, C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), ip, C.POINTER(vp)]),
@@ -495,6 +496,14 @@ class Box:
         return r
 
     # ---- derivative family (FUNCTN interior array -> FDERIV) ----
+    def flamin(self, trin, prin, drin, urin, v=None, w=None):
+        """FLAMIN's planar flame and INDATA's conversion to the conserved
+        state on the device (v, w: (nz, ny, nx) arrays or None for zero)."""
+        va = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        _check(lib.senga_flamin(self.h, float(trin), float(prin), float(drin), float(urin),
+                                None if va is None else _dp(va), None if wa is None else _dp(wa)), "senga_flamin")
+
     def tempin(self, trin):
         """TEMPIN on the uploaded conserved state: (T, ITNDEX, p) of every
         point, also left on the device for the next step."""
