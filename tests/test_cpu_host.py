@@ -77,6 +77,11 @@ def test_bad_inputs_return_status_not_abort():
         senga.Box((16, 16, 16), (1e-3,) * 3, chem, diff, 1e-8, nend=(2, 2, 1, 3, 2, 2))
     with pytest.raises(senga.SengaError, match="status 1"):  # bounded x needs 12 points
         senga.Box((11, 16, 16), (1e-3,) * 3, chem, diff, 1e-8, nend=(1, 1, 2, 2, 2, 2))
+    # start-up entry points refuse a missing context before touching the device
+    t = np.zeros(8)
+    assert senga.lib.senga_tempin_host(None, 300.0, senga._dp(t), None, None) == 1
+    assert senga.lib.senga_flamin(None, 300.0, 101325.0, 1.0, 1.0, None, None) == 1
+    assert senga.lib.senga_deriv_host(None, 0, senga._dp(t), senga._dp(t)) == 1
 
 
 def test_integf_spectrum_moment():
