@@ -3,7 +3,7 @@
 ctypes wrapper of liboracle.so, the CPU restatement of the reference's
 RHSCAL/RHSVEL/TEMPER/CHRATE/derivatives/LINCOM path (senga_oracle.cpp).
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
-it, and only as the checker or the timed CPU baseline, never as the product.
+it, and only to check results or as the timed CPU baseline, never as the product.
 Parity unpinned against outputs of the reference: it is Fortran and no
 Fortran compiler exists in this build environment, and the reference ships
 no tests. The oracle is pinned by known-answer tests instead
