@@ -424,13 +424,18 @@ int senga_server_set_max_points(senga_server* s, int64_t max_points);
  *   state  : nc = 5+nspec conserved interior arrays (read)
  *   trun   : T seed in, T after TEMPER out;  itndex: interval index in/out
  *   rhs    : nc interior arrays, R(U) out
- *   status : optional device word, bit 0 set on TEMPER non-convergence
- *            (cleared by the call); NULL uses an internal word
+ *   status : device word (required), bit 0 set on TEMPER non-convergence
+ *            (cleared by the call)
  *   stream : cudaStream_t to run on (NULL = default stream); asynchronous.
- * A box needs (14 + 4*nspec)*8 bytes of scratch per grid point; larger boxes
- * are rejected with SENGA_ERR_ARG. Every call reuses the same array, so calls
- * that overlap on the GPU race. The first call on a device (with it current)
- * looks up the array's device address; make it before any stream capture. */
+ * Periodic boxes of any extent (one point in the unused directions of 1D and
+ * 2D runs). A box needs (14 + 4*nspec)*8 bytes of scratch per grid point;
+ * larger boxes are rejected with SENGA_ERR_ARG. Every call reuses the same
+ * array, so calls that overlap on the GPU race. The first call on a device
+ * (with it current) looks up the array's device address; make it before any
+ * stream capture. Under CUDA's lazy module loading (the default) that first
+ * call is also when the array and the kernels' code are loaded onto the
+ * device: a host that reserves all free device memory at start-up makes one
+ * call per device before it does (or sets CUDA_MODULE_LOADING=EAGER). */
 #define SENGA_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
 int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff,
                       const double* state, double* trun, int32_t* itndex, double* rhs,

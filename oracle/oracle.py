@@ -72,6 +72,9 @@ def _get():
         lib.oracle_set_bc.argtypes = [C.c_void_p, C.POINTER(_Bc)]
         lib.oracle_tstep.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int)]
         lib.oracle_filter_field.argtypes = [C.c_void_p, C.c_int, dp, dp]
+        lib.oracle_chem_table.argtypes = [C.c_char_p, C.c_char_p, dp, C.c_int]
+        lib.oracle_substage.argtypes = [C.c_void_p, C.c_int]
+        lib.oracle_set_threads.argtypes = [C.c_int]
         _lib = lib
     return _lib
 
@@ -132,6 +135,15 @@ class Oracle:
     def step(self, nsteps=1):
         if _get().oracle_step(self.h, nsteps) != 0:
             raise RuntimeError("oracle_step: " + _get().oracle_last_error().decode())
+
+    def substage(self, irk):
+        """One RK substage irk (1..5); BOUNTT (and ADAPTT) follow the fifth."""
+        if _get().oracle_substage(self.h, int(irk)) != 0:
+            raise RuntimeError("oracle_substage: " + _get().oracle_last_error().decode())
+
+    @staticmethod
+    def set_threads(n):
+        _get().oracle_set_threads(int(n))
 
     def rhs(self):
         r = np.empty((self.nc,) + self.shape)
@@ -228,6 +240,34 @@ class Oracle:
         v = C.c_double()
         _get().oracle_chem_scalar(self.h, name.encode(), C.byref(v))
         return v.value
+
+
+class OracleChem:
+    """chem.dat tables read by the oracle's own CHEMIN restatement, with the
+    table(name) / nspec interface of the device library's Chem; for callers
+    that must not load the device library (the CPU reference arm)."""
+
+    _SHAPES = {"ntint": (9,), "rgspec": (9,), "wmolar": (9,), "ncpoly": (9, 2), "ncenth": (9, 2),
+               "tinthi": (9, 2), "tintlo": (9, 2), "amasch": (9, 2, 7), "amascp": (9, 2, 7)}
+    _INT = ("ntint", "ncpoly", "ncenth")
+
+    def __init__(self, path):
+        self.path = path
+        self._cache = {}
+        self.nspec = int(self._read("nspec", (1,))[0])
+
+    def _read(self, name, shape):
+        out = np.empty(int(np.prod(shape)))
+        cnt = _get().oracle_chem_table(self.path.encode(), name.encode(), _dp(out), out.size)
+        if cnt < 0:
+            raise RuntimeError("oracle_chem_table: " + _get().oracle_last_error().decode())
+        return out.reshape(shape)
+
+    def table(self, name):
+        if name not in self._cache:
+            a = self._read(name, self._SHAPES[name])
+            self._cache[name] = a.astype(np.int32) if name in self._INT else a
+        return self._cache[name]
 
 
 def turbin(shape, inseed, const0, ck0):

@@ -2535,3 +2535,67 @@ int oracle_chem_scalar(void* h, const char* name, double* out) {
 }
 
 }  // extern "C"
+
+extern "C" {
+// Chemistry tables of a chem.dat file read by the oracle's own CHEMIN
+// restatement (read_chem, src/chemin.f:146-344,822-983), for callers that
+// build initial states without the device library (the CPU reference arm of
+// the benchmark). Table `name` goes to out (at most cap elements, integer
+// tables widened to double) in the layout [ispec][itint][icoef]; returns the
+// element count, or -1 (unknown name, short buffer, unreadable file).
+int oracle_chem_table(const char* path, const char* name, double* out, int cap) {
+  try {
+    orc::Chem c;
+    orc::read_chem(path, c);
+    const std::string n(name);
+    auto put = [&](const auto* a, int cnt) {
+      if (cnt > cap) return -1;
+      for (int i = 0; i < cnt; ++i) out[i] = (double)a[i];
+      return cnt;
+    };
+    const int s2 = orc::NSPCMX * orc::NTINMX, s3 = s2 * orc::NCOFMX;
+    if (n == "nspec") { const int v = c.nspec; return put(&v, 1); }
+    if (n == "ntint") return put(c.ntint, orc::NSPCMX);
+    if (n == "ncpoly") return put(c.ncpoly, s2);
+    if (n == "ncenth") return put(c.ncenth, s2);
+    if (n == "tinthi") return put(c.tinthi, s2);
+    if (n == "tintlo") return put(c.tintlo, s2);
+    if (n == "amasch") return put(c.amasch, s3);
+    if (n == "amascp") return put(c.amascp, s3);
+    if (n == "rgspec") return put(c.rgspec, orc::NSPCMX);
+    if (n == "wmolar") return put(c.wmolar, orc::NSPCMX);
+    g_err = "oracle_chem_table: unknown table " + n;
+    return -1;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+}  // extern "C"
+
+extern "C" {
+// One RK substage irk (1..5) of the reference's time step (src/senga2.f:113-159:
+// BOUNDT, RHSCAL/RHSVEL, BOUNDS, LINCOM or FINCOM on the last), with BOUNTT
+// and ADAPTT after the fifth as in oracle_step.
+int oracle_substage(void* h, int irk) {
+  try {
+    auto* o = static_cast<orc::Oracle*>(h);
+    if (irk < 1 || irk > 5) throw std::runtime_error("oracle_substage: irk must be 1..5");
+    o->boundt();
+    o->rhs();
+    o->bounds();
+    o->lincom(irk, irk == 5);
+    if (irk == 5) {
+      o->bountt();
+      if (o->fladpt) o->adaptt();
+    }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+// OpenMP threads of the oracle's loops (the CPU baseline times 1 and all).
+void oracle_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+}  // extern "C"

@@ -208,7 +208,7 @@ def ignition_box(shape_xyz, seed, uprime, tpeak, chem_path=CHEM_1STEP):
                 fields=fields, T=T, itn=itn, dt=dt, nend=(NPERI,) * 6)
 
 
-def make_case(name, n=None, seed=1234, scale_n=None, shape=None):
+def make_case(name, n=None, seed=1234, scale_n=None, shape=None, chem_reader=None):
     """Named workloads. Returns dict with shape (nx,ny,nz), lengths, chem/diff
     paths, fields (nc,nz,ny,nx), T, itn and a CFL-0.5 dt.
 
@@ -238,8 +238,12 @@ def make_case(name, n=None, seed=1234, scale_n=None, shape=None):
                   pressure, Soret and Dufour terms are all active.
     `n` overrides the grid extent (cubic) for smaller test instances;
     `shape` = (nx, ny, nz) gives h2_pool and flame_inout a non-cubic grid.
+    `chem_reader` is the class that reads chem.dat (path -> object with
+    nspec and table(name)); the default is the device library's Chem.
     """
-    from senga import Chem  # noqa: local import keeps this module numpy-only
+    if chem_reader is None:
+        from senga import Chem as chem_reader  # noqa: local import keeps this module numpy-only
+    Chem = chem_reader
     rng = np.random.default_rng(seed)
     if name == "ignition32":
         nn = n or 32

@@ -21,10 +21,15 @@
 //     (different streams, or different host threads) race on the array;
 //   * the first call on a device, with that device current, looks up the
 //     device addresses of the file-scope arrays (cudaGetSymbolAddress); make
-//     that first call before any stream capture.
+//     that first call before any stream capture. Under CUDA's lazy module
+//     loading (the default of recent CUDA releases) that first call is also
+//     when the array and the kernels' code are loaded onto the device, so a
+//     host that reserves all free device memory at start-up makes one call
+//     per device before it does (or runs with CUDA_MODULE_LOADING=EAGER);
+//   * the status word is required: it is the only place a TEMPER
+//     non-convergence is reported.
 #include <cuda_runtime.h>
 
-#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -40,14 +45,16 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 static __device__ __align__(256) senga_chem g_noalloc_chem;
 static __device__ __align__(256) senga_diff g_noalloc_diff;
-static __device__ __align__(256) unsigned int g_noalloc_status;
+
+// Transport tables of constant-Lewis runs (diff == NULL): a zeroed table at a
+// fixed host address, the source of the table copy below.
+const senga_diff kNoDiff = {};
 
 struct DevicePtrs {
   bool ready = false;
   double* scratch = nullptr;
   senga_chem* chem = nullptr;
   senga_diff* diff = nullptr;
-  unsigned int* status = nullptr;
 };
 DevicePtrs g_ptrs[kMaxDevices];
 std::mutex g_mutex;
@@ -62,7 +69,6 @@ int setup(int dev, DevicePtrs& out) {
     cudaError_t e = cudaGetSymbolAddress((void**)&p.scratch, g_noalloc_scratch);
     if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p.chem, g_noalloc_chem);
     if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p.diff, g_noalloc_diff);
-    if (e == cudaSuccess) e = cudaGetSymbolAddress((void**)&p.status, g_noalloc_status);
     if (e != cudaSuccess)
       return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: cudaGetSymbolAddress: ") +
                                              cudaGetErrorString(e));
@@ -77,7 +83,7 @@ int setup(int dev, DevicePtrs& out) {
 extern "C" int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff,
                                  const double* state, double* trun, int32_t* itndex, double* rhs,
                                  unsigned int* status, void* stream) {
-  if (!cfg || !chem || !state || !trun || !itndex || !rhs)
+  if (!cfg || !chem || !state || !trun || !itndex || !rhs || !status)
     return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: null argument");
   const int nspec = chem->nspec;
   if (nspec < 1 || nspec > SENGA_NSPCMX) return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: nspec out of range");
@@ -85,7 +91,9 @@ extern "C" int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem
   const double len[3] = {cfg->xgdlen, cfg->ygdlen, cfg->zgdlen};
   senga::Geo g{};
   for (int d = 0; d < 3; ++d) {
-    if (n3[d] < 11) return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: grid extent must be at least 11 points");
+    // any periodic extent, as for a context (one point in the unused
+    // directions of 1D and 2D runs)
+    if (n3[d] < 1) return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: grid extent must be at least 1 point");
     if (cfg->nend[2 * d] != SENGA_NPERI || cfg->nend[2 * d + 1] != SENGA_NPERI)
       return senga::fail(SENGA_ERR_UNSUPPORTED, "senga_rhs_noalloc: periodic boxes only");
     g.per[d] = 1;
@@ -111,12 +119,10 @@ extern "C" int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem
   if (rc != SENGA_OK) return rc;
 
   cudaStream_t s = (cudaStream_t)stream;
-  senga_diff dz;
-  if (!diff) std::memset(&dz, 0, sizeof(dz));
+  const senga_diff& dz = diff ? *diff : kNoDiff;
   e = cudaMemcpyAsync(ptr.chem, chem, sizeof(senga_chem), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ptr.diff, diff ? diff : &dz, sizeof(senga_diff), cudaMemcpyHostToDevice, s);
-  unsigned int* st = status ? status : ptr.status;
-  if (e == cudaSuccess) e = cudaMemsetAsync(st, 0, sizeof(unsigned int), s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ptr.diff, &dz, sizeof(senga_diff), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(unsigned int), s);
   if (e != cudaSuccess) return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: ") + cudaGetErrorString(e));
 
   // carve the scratch fields; the caller's rhs buffer is the accumulator
@@ -149,10 +155,10 @@ extern "C" int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem
   f.vc = take(3);
   f.vtmp = take(1);
   f.rhs = rhs;
-  f.status = st;
+  f.status = status;
 
   const int flmavt = diff ? diff->flmavt : 0;
-  senga::launch_thermo(g, f, ptr.chem, ptr.diff, nspec, flmavt, senga::select_mech(*chem, diff ? *diff : dz), s);
+  senga::launch_thermo(g, f, ptr.chem, ptr.diff, nspec, flmavt, senga::select_mech(*chem, dz), s);
   senga::launch_flow(g, f, nspec, s);
   senga::launch_species_a(g, f, nspec, s);
   senga::RK rk{0.0, 0.0, 0.0, -1};

@@ -13,7 +13,8 @@
   lowered by 5250 K * R/W so that T_ad = 300 + 5250/3.5 = 1800 K at constant
   pressure, unit Lewis numbers.
 
-Usage: python make_data.py [reference_root]
+Usage: python make_data.py <reference_root>   (or SENGA_REFERENCE_ROOT set)
+Without a reference root only chem_1step.dat is rewritten.
 """
 import os
 import shutil
@@ -57,13 +58,13 @@ def one_step_chem():
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SENGA_REFERENCE_ROOT", "")
     with open(os.path.join(HERE, "chem_1step.dat"), "w") as fh:
         fh.write(one_step_chem())
     for src, dst in (("input/chem.dat", "chem_h2.dat"), ("input/diff.dat", "diff_h2.dat"),
                      ("input/radn.dat", "radn_h2.dat")):
         path = os.path.join(ref, src)
-        if os.path.exists(path):
+        if ref and os.path.exists(path):
             shutil.copyfile(path, os.path.join(HERE, dst))
 
 

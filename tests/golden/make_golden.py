@@ -13,9 +13,10 @@
    pin of the oracle, and a GPU parity fixture that needs no oracle at run
    time.
 
-Run from the repository root:  python tests/golden/make_golden.py
-(reads the reference sources under /root/reference; the GPU box never runs
-this script).
+Run from the repository root:
+  python tests/golden/make_golden.py <reference_root>
+(or with SENGA_REFERENCE_ROOT set; it reads the reference's Fortran sources
+under <reference_root>/src. The GPU box never runs this script.)
 """
 import json
 import os
@@ -27,7 +28,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/src"
+REF = os.path.join(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SENGA_REFERENCE_ROOT", ""), "src")
 sys.path.insert(0, os.path.join(ROOT, "senga-versiona_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
