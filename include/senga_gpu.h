@@ -214,6 +214,18 @@ int senga_tempin_host(senga_ctx* ctx, double trin, double* trun, int32_t* itndex
 int senga_flamin(senga_ctx* ctx, double trin, double prin, double drin, double urin, const double* v,
                  const double* w);
 int senga_deriv_host(senga_ctx* ctx, int kind, const double* f, double* out);
+/* The same nine operators on the reference's own argument shapes
+ * (src/dfbydx.f:36-37): f_big is FUNCTN(NXBIGL:NXBIGR, NYBIGL:NYBIGR,
+ * NZBIGL:NZBIGR) with NHALO = 5 points on every side, i.e. (nx+10)(ny+10)
+ * (nz+10) doubles, x fastest, the interior starting at offset 5 in each
+ * direction; out is FDERIV(NXSIZE, NYSIZE, NZSIZE), the nx*ny*nz interior.
+ * Periodic directions read their neighbours from the halo as the caller
+ * filled it (PARFER's periodic copies, or a neighbour rank's planes), as the
+ * reference does; bounded directions use the one-sided closures and never
+ * read their halo. senga_deriv_big takes device pointers (asynchronous on
+ * the context's stream), senga_deriv_big_host host pointers. */
+int senga_deriv_big(senga_ctx* ctx, int kind, const double* f_big, double* out);
+int senga_deriv_big_host(senga_ctx* ctx, int kind, const double* f_big, double* out);
 
 /* Mixture-averaged transport switches of cont.dat's transport line
  * (NFMIXW, NFMIXP, NFMSOR, NFMDUF, WMLTDR; src/contin.f:205): molar-mass

@@ -490,6 +490,47 @@ __global__ void k_deriv(Geo g, int kind, const double* __restrict__ in, double* 
   out[q] = r;
 }
 
+// The same operators on the reference's own array shape: `in` is the
+// halo-extended FUNCTN(1-5:nx+5, 1-5:ny+5, 1-5:nz+5) (x fastest) and the
+// result the interior FDERIV(nx, ny, nz) (src/dfbydx.f:36-37). Neighbours are
+// read from the halo as given (PARFER's copies in a periodic direction, or a
+// neighbour rank's planes), never folded; a bounded direction uses the
+// one-sided closures, which read interior points only.
+__global__ void k_deriv_big(Geo g, int kind, const double* __restrict__ in, double* __restrict__ out) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.n) return;
+  const Pt pt = point_of(g, q);
+  constexpr int H = 5;
+  const int64_t bx = g.nx + 2 * H, bxy = bx * (g.ny + 2 * H);
+  const int64_t qb = (pt.i + H) + bx * (pt.j + H) + bxy * (pt.k + H);
+  const int64_t st[3] = {1, bx, bxy};
+  const int c3[3] = {pt.i, pt.j, pt.k};
+  const int n3[3] = {g.nx, g.ny, g.nz};
+  auto f = [&](int64_t o) { return __ldg(in + qb + o); };
+  double r = 0.0;
+  if (kind < 6) {
+    const int d = kind % 3;
+    auto v = [&](int m) { return f(m * st[d]); };
+    r = kind < 3 ? d1core(v, c3[d], n3[d], g.per[d]) * g.ovd[d] : d2core(v, c3[d], n3[d], g.per[d]) * g.ovd2[d];
+  } else {
+    const int da = kind == 8 ? 1 : 0, db = kind == 6 ? 1 : 2;
+    auto v = [&](int ma, int mb) { return f(ma * st[da] + mb * st[db]); };
+    if (!g.per[db]) {
+      constexpr int kFar = 1 << 20;
+      const int ca = c3[da], cb = c3[db];
+      const int la = g.per[da] ? kFar : ca, ra = g.per[da] ? kFar : n3[da] - 1 - ca;
+      const int lb = cb, rb = n3[db] - 1 - cb;
+      r = dmcore_ends(v, la < ra ? la : ra, ra < la, lb < rb ? lb : rb, rb < lb);
+    } else if (!g.per[da]) {
+      r = dmcore_b(v, c3[da], n3[da]);
+    } else {
+      r = dmcore(v);
+    }
+    r = r * g.ovd[da] * g.ovd[db];
+  }
+  out[q] = r;
+}
+
 inline unsigned grid_of(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 }  // namespace
@@ -540,6 +581,10 @@ int thermo_block() { return kBlock; }
 
 void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s) {
   k_deriv<<<grid_of(g.n), kBlock, 0, s>>>(g, kind, in, out);
+}
+
+void launch_deriv_big(const Geo& g, int kind, const double* in, double* out, cudaStream_t s) {
+  k_deriv_big<<<grid_of(g.n), kBlock, 0, s>>>(g, kind, in, out);
 }
 
 }  // namespace senga

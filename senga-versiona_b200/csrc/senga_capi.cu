@@ -545,6 +545,42 @@ int senga_deriv_host(senga_ctx* c, int kind, const double* f, double* out) {
   });
 }
 
+int senga_deriv_big(senga_ctx* c, int kind, const double* f_big, double* out) {
+  if (!c || !f_big || !out || kind < 0 || kind > 8) return fail(SENGA_ERR_ARG, "senga_deriv_big: bad argument");
+  return guard([&] {
+    launch_deriv_big(c->geo, kind, f_big, out, c->stream);
+    CK(cudaGetLastError());
+  });
+}
+
+int senga_deriv_big_host(senga_ctx* c, int kind, const double* f_big, double* out) {
+  if (!c || !f_big || !out || kind < 0 || kind > 8) return fail(SENGA_ERR_ARG, "senga_deriv_big_host: bad argument");
+  return guard([&] {
+    const Geo& g = c->geo;
+    const size_t nbig = (size_t)(g.nx + 10) * (g.ny + 10) * (g.nz + 10);
+    // the context's rhs scratch (nc interior arrays) holds operand and
+    // result when the halo-extended array fits beside one interior array;
+    // thin boxes (a 1D run's 1 x 1 planes) take a temporary buffer
+    double* tmp = nullptr;
+    double* din = c->f.rhs;
+    double* dout = c->f.rhs + nbig;
+    if (nbig + (size_t)g.n > (size_t)c->nc * (size_t)g.n) {
+      CK(cudaMalloc(&tmp, (nbig + (size_t)g.n) * sizeof(double)));
+      din = tmp;
+      dout = tmp + nbig;
+    }
+    cudaError_t e = cudaMemcpyAsync(din, f_big, nbig * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+      launch_deriv_big(g, kind, din, dout, c->stream);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, (size_t)g.n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (tmp) cudaFree(tmp);
+    CK(e);
+  });
+}
+
 int senga_keep_rates(senga_ctx* c, int on) {
   if (!c) return fail(SENGA_ERR_ARG, "senga_keep_rates: null context");
   return guard([&] {

@@ -135,6 +135,8 @@ void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, 
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s,
                          const ZDec& zd = ZDec{});
 void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s);
+// the same on a halo-extended input (5 points per side), interior output
+void launch_deriv_big(const Geo& g, int kind, const double* in, double* out, cudaStream_t s);
 // Batched ensemble (kernels.cu, kernels_tiled.cu): all boxes periodic, one
 // mechanism; grid = persistent CTA count.
 void tile_shape(int* tx, int* ty, int* tz);

@@ -186,6 +186,8 @@ def _load():
                                     C.POINTER(C.c_int64)]),
         "senga_rhs_noalloc": (ip, [C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), vp, vp, vp, vp, vp,
                                    vp]),
+        "senga_deriv_big": (ip, [vp, ip, vp, vp]),
+        "senga_deriv_big_host": (ip, [vp, ip, dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -519,6 +521,15 @@ class Box:
         assert a.shape == self.shape
         out = np.empty_like(a)
         _check(lib.senga_deriv_host(self.h, kind, _dp(a), _dp(out)), "senga_deriv_host")
+        return out
+
+    def deriv_big(self, kind, f_big):
+        """The operator on a halo-extended array (5 points per side, shape
+        (nz+10, ny+10, nx+10)); returns the interior result."""
+        a = np.ascontiguousarray(f_big, dtype=np.float64)
+        assert a.shape == tuple(m + 10 for m in self.shape)
+        out = np.empty(self.shape)
+        _check(lib.senga_deriv_big_host(self.h, kind, _dp(a), _dp(out)), "senga_deriv_big_host")
         return out
 
     def set_nscbc(self, bc):
