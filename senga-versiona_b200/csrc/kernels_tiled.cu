@@ -14,6 +14,9 @@
 // different order (FP64 rounding differences only).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+#include <string>
+
 #include "senga_internal.h"
 #include "tiles.cuh"
 
@@ -50,11 +53,29 @@ using SCol = Column<SZ_>;
 constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 3 * SSlab::SIZE;
 constexpr int kSpecRkSmem = 2 * SSlab::SIZE;
 
-template <bool P>
+// Staging of a plain field: bulk copies on the TMA engine (B) or per-element
+// cp.async; and the wait for the group staged last (B: one mbarrier phase of
+// `bytes`, a CTA-uniform barrier; returns true when the CTA must give up).
+template <bool B, int NW, class Buf, class FO>
+__device__ __forceinline__ void stage_plain(const Buf& b, const FO& fo, const Geo& g, const Origin& o,
+                                            const double* src, uint64_t* bar) {
+  if constexpr (B) b.stage_bulk(fo, o.x0, g.nx, src, bar);
+  else b.template stage<NW>(fo, Ld{src});
+}
+template <bool B>
+__device__ __forceinline__ bool sync_staged(BulkBar& bb, unsigned bytes, unsigned int* status) {
+  if constexpr (B) return bb.wait(bytes, status);
+  tile_sync();
+  return false;
+}
+
+template <bool P, bool B = false>
 __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const Origin o, double* sm,
-                                          Folds<FX, FY, FZ>& fo, const ZDec& zd) {
+                                          Folds<FX, FY, FZ>& fo, const ZDec& zd, uint64_t* bar = nullptr) {
   const int tx = threadIdx.x % FX, ty = threadIdx.x / FX;
   fo.init(g, o, zd);
+  BulkBar bb{bar, 0u};
+  if (B && threadIdx.x == 0) mbar_init(bar, 1);
   tile_sync();
   TP tp[FZ];
 #pragma unroll
@@ -69,11 +90,12 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     const FYRow brv{sm + FXRow::SIZE};
     const FZCol brw{sm + FXRow::SIZE + FYRow::SIZE};
     const FStar bE{sm + FXRow::SIZE + FYRow::SIZE + FZCol::SIZE};
-    bru.stage<FNW>(fo, Ld{U + n});
-    brv.stage<FNW>(fo, Ld{U + 2 * n});
-    brw.stage<FNW>(fo, Ld{U + 3 * n});
-    bE.stage<FNW>(fo, Ld{f.e});
-    tile_sync();
+    stage_plain<B, FNW>(bru, fo, g, o, U + n, bar);
+    stage_plain<B, FNW>(brv, fo, g, o, U + 2 * n, bar);
+    stage_plain<B, FNW>(brw, fo, g, o, U + 3 * n, bar);
+    stage_plain<B, FNW>(bE, fo, g, o, f.e, bar);
+    if (sync_staged<B>(bb, FXRow::kBulkBytes + FYRow::kBulkBytes + FZCol::kBulkBytes + FStar::kBulkBytes, f.status))
+      return;
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
@@ -84,14 +106,14 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
       rE[z] = -0.5 * (s4 + d1<0, P>(g, t, bE) * bru.v(t.x, t.y, t.z) + d1<1, P>(g, t, bE) * brv.v(t.x, t.y, t.z) +
                       d1<2, P>(g, t, bE) * brw.v(t.x, t.y, t.z));
     }
-    tile_sync();
+    tile_sync_async();
   }
   // ---- phase 2: heat conduction ----
   {
     const FStar bT{sm}, bL{sm + FStar::SIZE};
-    bT.stage<FNW>(fo, Ld{f.t});
-    bL.stage<FNW>(fo, Ld{f.lam});
-    tile_sync();
+    stage_plain<B, FNW>(bT, fo, g, o, f.t, bar);
+    stage_plain<B, FNW>(bL, fo, g, o, f.lam, bar);
+    if (sync_staged<B>(bb, 2 * FStar::kBulkBytes, f.status)) return;
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
@@ -101,7 +123,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
                        d1<2, P>(g, t, bL) * d1<2, P>(g, t, bT));
       rE[z] = rE[z] + ((con ? 0.0 : d2<0, P>(g, t, bT)) + d2<1, P>(g, t, bT) + d2<2, P>(g, t, bT)) * bL.v(t.x, t.y, t.z);
     }
-    tile_sync();
+    tile_sync_async();
   }
   // ---- phase 3: pressure gradient (of p - p(1,1,1)) and pressure work ----
   {
@@ -153,16 +175,16 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
       S6[z] = S6[z] + d1<1, P>(g, t, bB);
       S6[z] = S6[z] + d1<2, P>(g, t, bC);
     }
-    tile_sync();
+    tile_sync_async();
   }
   // ---- phase 5: velocity derivatives, viscous stresses and work ----
   const FStar bM{sm};
   const FBox bX{sm + FStar::SIZE};
-  bM.stage<FNW>(fo, Ld{f.mu});
+  stage_plain<B, FNW>(bM, fo, g, o, f.mu, bar);
   double mux[FZ], muy[FZ], muz[FZ], ux[FZ], uy[FZ], uz[FZ], vx[FZ], vy[FZ], vz[FZ];
   // 5a: u
-  bX.stage<FNW>(fo, Ld{f.vel});
-  tile_sync();
+  stage_plain<B, FNW>(bX, fo, g, o, f.vel, bar);
+  if (sync_staged<B>(bb, FStar::kBulkBytes + FBox::kBulkBytes, f.status)) return;
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
     const TP& t = tp[z];
@@ -202,10 +224,10 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
   }
-  tile_sync();
+  tile_sync_async();
   // 5b: v
-  bX.stage<FNW>(fo, Ld{f.vel + n});
-  tile_sync();
+  stage_plain<B, FNW>(bX, fo, g, o, f.vel + n, bar);
+  if (sync_staged<B>(bb, FBox::kBulkBytes, f.status)) return;
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
     const TP& t = tp[z];
@@ -241,10 +263,10 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
   }
-  tile_sync();
+  tile_sync_async();
   // 5c: w, then the first-derivative products
-  bX.stage<FNW>(fo, Ld{f.vel + 2 * n});
-  tile_sync();
+  stage_plain<B, FNW>(bX, fo, g, o, f.vel + 2 * n, bar);
+  if (sync_staged<B>(bb, FBox::kBulkBytes, f.status)) return;
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
     const TP& t = tp[z];
@@ -341,11 +363,13 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
 }
 
 // -------------------------------------------------------------------------
-template <bool P>
+template <bool P, bool B = false>
 __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int nspec, const Origin o, double* sm,
-                                             Folds<SX_, SY_, SZ_>& fo, const ZDec& zd) {
+                                             Folds<SX_, SY_, SZ_>& fo, const ZDec& zd, uint64_t* bar = nullptr) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
   fo.init(g, o, zd);
+  BulkBar bb{bar, 0u};
+  if (B && threadIdx.x == 0) mbar_init(bar, 1);
   tile_sync();
   TP tp[SZ_];
 #pragma unroll
@@ -357,11 +381,13 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
   const SSlab bS{sm + SXRow::SIZE + SYRow::SIZE};
   const SSlab bH{sm + SXRow::SIZE + SYRow::SIZE + SSlab::SIZE};
   const SSlab bR{sm + SXRow::SIZE + SYRow::SIZE + 2 * SSlab::SIZE};
-  bru.stage<SNW>(fo, Ld{U + n});
-  brv.stage<SNW>(fo, Ld{U + 2 * n});
+  stage_plain<B, SNW>(bru, fo, g, o, U + n, bar);
+  stage_plain<B, SNW>(brv, fo, g, o, U + 2 * n, bar);
   // copies run one stage ahead: Y_s while the previous species' rho D and
   // h are used, rho D and h of species s while Y_s is used
-  if (nspec > 0) bS.stage<SNW>(fo, Ld{f.y});
+  if (nspec > 0) stage_plain<B, SNW>(bS, fo, g, o, f.y, bar);
+  // bytes of the group in flight (bulk path): rho u, rho v and Y_0 first
+  unsigned inflight = SXRow::kBulkBytes + SYRow::kBulkBytes + SSlab::kBulkBytes;
   SCol rw;
   rw.load(fo, tx, ty, Ld{U + 3 * n});
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
@@ -377,9 +403,12 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
     {
       SCol cy;
       cy.load(fo, tx, ty, Ld{f.y + s * n});
-      tile_sync();  // Y_s has landed in bS; the rho D and h slabs are free
-      bR.stage<SNW>(fo, Ld{f.rd + s * n});
-      bH.stage<SNW>(fo, Ld{f.h + s * n});
+      // Y_s has landed in bS; the rho D and h slabs are free
+      if (B) fence_proxy_async();
+      if (sync_staged<B>(bb, inflight, f.status)) return;
+      stage_plain<B, SNW>(bR, fo, g, o, f.rd + s * n, bar);
+      stage_plain<B, SNW>(bH, fo, g, o, f.h + s * n, bar);
+      inflight = 2 * SSlab::kBulkBytes;
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -440,8 +469,11 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       SCol cd, ch;
       cd.load(fo, tx, ty, Ld{f.rd + s * n});
       ch.load(fo, tx, ty, Ld{f.h + s * n});
-      tile_sync();  // rho D_s, h_s have landed; every thread is done with Y_s
-      if (s + 1 < nspec) bS.stage<SNW>(fo, Ld{f.y + (s + 1) * n});
+      // rho D_s, h_s have landed; every thread is done with Y_s
+      if (B) fence_proxy_async();
+      if (sync_staged<B>(bb, inflight, f.status)) return;
+      if (s + 1 < nspec) stage_plain<B, SNW>(bS, fo, g, o, f.y + (s + 1) * n, bar);
+      inflight = SSlab::kBulkBytes;
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -482,12 +514,14 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
 }
 
 // -------------------------------------------------------------------------
-template <bool P>
+template <bool P, bool B = false>
 __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, int nspec, const RK& rk,
                                                 const Origin o, double* sm, Folds<SX_, SY_, SZ_>& fo,
-                                                const ZDec& zd) {
+                                                const ZDec& zd, uint64_t* bar = nullptr) {
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
   fo.init(g, o, zd);
+  BulkBar bb{bar, 0u};
+  if (B && threadIdx.x == 0) mbar_init(bar, 1);
   tile_sync();
   TP tp[SZ_];
 #pragma unroll
@@ -536,9 +570,9 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
   {
     SCol cm;
     cm.load(fo, tx, ty, Ld{f.hmix});
-    bS.stage<SNW>(fo, Ld{f.hmix});
-    tile_sync();
-    if (nspec > 0) slab(0).stage<SNW>(fo, Ld{f.y});
+    stage_plain<B, SNW>(bS, fo, g, o, f.hmix, bar);
+    if (sync_staged<B>(bb, SSlab::kBulkBytes, f.status)) return;
+    if (nspec > 0) stage_plain<B, SNW>(slab(0), fo, g, o, f.y, bar);
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
@@ -558,8 +592,9 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     SCol cy;
     cy.load(fo, tx, ty, Ld{f.y + s * n});
     // Y_s has landed in slab(s); every thread is done with the other slab
-    tile_sync();
-    if (s + 1 < nspec) slab(s + 1).stage<SNW>(fo, Ld{f.y + (s + 1) * n});
+    if (B) fence_proxy_async();
+    if (sync_staged<B>(bb, SSlab::kBulkBytes, f.status)) return;
+    if (s + 1 < nspec) stage_plain<B, SNW>(slab(s + 1), fo, g, o, f.y + (s + 1) * n, bar);
     const SSlab bY = slab(s);
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
@@ -586,25 +621,31 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
 #endif
 
 // ---- single-box launches: one CTA per tile ----
-template <bool P>
+// B: plain fields staged by bulk copies on the TMA engine (all-periodic
+// boxes of even nx, one context, 16-byte aligned fields; the launcher checks)
+template <bool P, bool B>
 __global__ void __launch_bounds__(FX* FY, SENGA_FLOW_MINB) k_flow_t(Geo g, Fields f, ZDec zd) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
   __shared__ Folds<FX, FY, FZ> fo;
-  flow_tile<P>(g, f, Origin{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ}, sm, fo, zd);
+  __shared__ uint64_t bar;
+  flow_tile<P, B>(g, f, Origin{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ}, sm, fo, zd, &bar);
 }
-template <bool P>
+template <bool P, bool B>
 __global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB) k_species_t(Geo g, Fields f, int nspec, ZDec zd) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
-  species_tile<P>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm, fo,
-                  zd);
+  __shared__ uint64_t bar;
+  species_tile<P, B>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm,
+                     fo, zd, &bar);
 }
-template <bool P>
+template <bool P, bool B>
 __global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB) k_species_rk_t(Geo g, Fields f, int nspec, RK rk, ZDec zd) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(16) double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
-  species_rk_tile<P>(g, f, nspec, rk, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_},
-                     sm, fo, zd);
+  __shared__ uint64_t bar;
+  species_rk_tile<P, B>(g, f, nspec, rk,
+                        Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm, fo, zd,
+                        &bar);
 }
 
 // ---- batched launches: one CTA per (box, tile) work item; box descriptors
@@ -651,9 +692,14 @@ void set_attrs() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
   if (done[dev]) return;
-  cudaFuncSetAttribute(k_flow_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
-  cudaFuncSetAttribute(k_species_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
-  cudaFuncSetAttribute(k_species_rk_t<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
+  cudaFuncSetAttribute(k_flow_t<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
+  cudaFuncSetAttribute(k_species_t<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
+  cudaFuncSetAttribute(k_species_rk_t<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
+  if (P) {
+    cudaFuncSetAttribute(k_flow_t<P, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
+    cudaFuncSetAttribute(k_species_t<P, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
+    cudaFuncSetAttribute(k_species_rk_t<P, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
+  }
   cudaFuncSetAttribute(k_flow_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
   cudaFuncSetAttribute(k_species_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
   cudaFuncSetAttribute(k_species_rk_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
@@ -662,35 +708,61 @@ void set_attrs() {
 
 bool all_periodic(const Geo& g) { return g.per[0] && g.per[1] && g.per[2]; }
 
+bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// The bulk (TMA engine) staging applies to all-periodic boxes of one context
+// with even nx whose staged fields start on 16-byte boundaries; SENGA_STAGE=
+// cpasync in the environment keeps every box on per-element copies.
+bool bulk_ok(const Geo& g, const Fields& f, const ZDec& zd) {
+  static const bool off = [] {
+    const char* e = getenv("SENGA_STAGE");
+    return e && std::string(e) == "cpasync";
+  }();
+  if (off || !all_periodic(g) || zd.nr > 1 || (g.nx & 1)) return false;
+  const void* ptrs[] = {f.uin, f.e, f.t, f.lam, f.mu, f.vel, f.y, f.rd, f.h, f.hmix};
+  for (const void* p : ptrs)
+    if (p && !al16(p)) return false;
+  return true;
+}
+
 }  // namespace
 
 void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    k_flow_t<true><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
+    if (bulk_ok(g, f, zd))
+      k_flow_t<true, true><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
+    else
+      k_flow_t<true, false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
   } else {
     set_attrs<false>();
-    k_flow_t<false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
+    k_flow_t<false, false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
   }
 }
 
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    k_species_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
+    if (bulk_ok(g, f, zd))
+      k_species_t<true, true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
+    else
+      k_species_t<true, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
   } else {
     set_attrs<false>();
-    k_species_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
+    k_species_t<false, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
   }
 }
 
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    k_species_rk_t<true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
+    if (bulk_ok(g, f, zd))
+      k_species_rk_t<true, true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
+    else
+      k_species_rk_t<true, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
   } else {
     set_attrs<false>();
-    k_species_rk_t<false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
+    k_species_rk_t<false, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
   }
 }
 

@@ -9,11 +9,20 @@
 // of src/parfer.f:840-873); in a bounded direction they are clamped and never
 // read, because the one-sided closures only look inward.
 //
-// Buffer layouts (doubles):
-//   Star : slab[TZ][TY+2H][TX+2H] + zhalo[2H][TY][TX]   first/second derivatives
+// Buffer layouts (doubles; SX = TX + 2*XH, one column more than the 5-point
+// halo on each side so that every row starts on a 16-byte boundary):
+//   Star : slab[TZ][TY+2H][SX] + zhalo[2H][TY][TX]   first/second derivatives
 //          in x, y, z (+ xy corners for the xy mixed derivative when loaded)
-//   Box  : [TZ+2H][TY+2H][TX+2H]                         all mixed derivatives
-//   XRow : [TZ][TY][TX+2H]    YRow : [TZ][TY+2H][TX]    ZCol : [TZ+2H][TY][TX]
+//   Box  : [TZ+2H][TY+2H][SX]                         all mixed derivatives
+//   XRow : [TZ][TY][SX]    YRow : [TZ][TY+2H][TX]    ZCol : [TZ+2H][TY][TX]
+//
+// Two ways of filling them. stage(): per-element cp.async by every thread
+// (any box). stage_bulk(): each row is one bulk copy on the TMA engine
+// (cp.async.bulk, completion counted on an mbarrier), split in two where a
+// periodic x direction wraps; no LSU instruction per element. The bulk path
+// needs an all-periodic box of even nx, 16-byte aligned fields and one
+// context (the launcher checks), because each copy must start on a 16-byte
+// boundary and be a multiple of 16 bytes long.
 #pragma once
 #include <cstdint>
 
@@ -23,6 +32,7 @@ namespace senga {
 namespace tile {
 
 constexpr int H = 5;
+constexpr int XH = 6;  // x halo allocated in shared memory (5 read + 1 for alignment)
 
 struct Origin {
   int x0, y0, z0;
@@ -81,6 +91,101 @@ __device__ __forceinline__ void tile_sync() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
 }
+// tile_sync before bulk copies overwrite buffers that threads read or wrote:
+// every thread orders its own shared-memory accesses before the async proxy
+__device__ __forceinline__ void tile_sync_async() {
+  asm volatile("cp.async.wait_all;\n fence.proxy.async.shared::cta;\n" ::: "memory");
+  __syncthreads();
+}
+// ---- bulk copies on the TMA engine, completion on an mbarrier ----
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// the single arrival of a phase, announcing the bytes its copies will deliver
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// prior generic-proxy accesses of shared memory by this thread are ordered
+// before its later bulk copies (which write through the async proxy)
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_g2s(double* dst, const double* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Waits for phase `parity` of bar to complete, for at most about one second
+// of SM clock; returns false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > (1ll << 31)) return false;
+  }
+}
+
+// Status bit set when a stencil kernel's bulk copies did not complete in
+// time (the tile's results are then not written).
+constexpr unsigned kStatusStageTimeout = 8u;
+
+// One mbarrier driving the bulk fills of a tile, phase by phase.
+struct BulkBar {
+  uint64_t* bar;
+  unsigned parity;
+  // thread 0 announces the bytes of this phase's copies (issued by any
+  // threads, before or after); everyone then waits. Returns true when the
+  // CTA must give up (a time-out anywhere in the CTA), uniformly.
+  __device__ __forceinline__ bool wait(unsigned bytes, unsigned int* status) {
+    if (threadIdx.x == 0) mbar_expect_tx(bar, bytes);
+    bool ok = mbar_wait(bar, parity);
+    parity ^= 1u;
+    if (!ok) {
+      // give the copies in flight a second bound to land before leaving
+      mbar_wait(bar, parity ^ 1u);
+      if (status) atomicOr(status, kStatusStageTimeout);
+    }
+    return __syncthreads_or(!ok) != 0;
+  }
+};
+
+// Bulk copies of NR rows: row r covers global x in [x0 + XLO, x0 + XLO + XL)
+// at the folded (y, z) that rowyz(r) gives and lands at dst[d*DS + (x - XLO)].
+// The periodic x range is cut at every wrap; with nx, x0 + XLO and XL even
+// every piece starts on an even x and has an even length, i.e. 16-byte
+// aligned and a multiple of 16 bytes. Rows are spread over the CTA's threads.
+template <int XL, int XLO, int NR, class FO, class RowYZ>
+__device__ __forceinline__ void stage_bulk(double* dst, int DS, const FO& fo, int x0, int nx, const RowYZ& rowyz,
+                                           const double* src, uint64_t* bar) {
+  static_assert(XL % 2 == 0 && XLO % 2 == 0, "bulk rows must be 16-byte aligned");
+  for (int r = threadIdx.x; r < NR; r += blockDim.x) {
+    int y, z, d;
+    rowyz(r, y, z, d);
+    const double* row = src + fo.oy[y + H] + fo.oz[z + H];
+    double* drow = dst + d * DS;
+    int c = x0 + XLO;
+    const int e = c + XL;
+    int xs = c % nx;
+    if (xs < 0) xs += nx;
+    int off = 0;
+    while (c < e) {
+      const int len = min(e - c, nx - xs);
+      bulk_g2s(drow + off, row + xs, (unsigned)len * 8u, bar);
+      off += len;
+      c += len;
+      xs = 0;
+    }
+  }
+}
+
 template <class F>
 struct PlainLoad {
   static constexpr bool value = false;
@@ -144,12 +249,12 @@ __device__ __forceinline__ void stage_rows(double* dst, int DS, const FO& fo, co
 
 template <int TX, int TY, int TZ>
 struct Star {
-  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H;
+  static constexpr int SX = TX + 2 * XH, SY = TY + 2 * H;
   static constexpr int SLAB = TZ * SY * SX;
   static constexpr int SIZE = SLAB + 2 * H * TY * TX;
   double* p;
   __device__ __forceinline__ double v(int x, int y, int z) const {
-    if (z >= 0 && z < TZ) return p[(z * SY + (y + H)) * SX + (x + H)];
+    if (z >= 0 && z < TZ) return p[(z * SY + (y + H)) * SX + (x + XH)];
     const int zz = z < 0 ? z + H : z - TZ + H;
     return p[SLAB + (zz * TY + y) * TX + x];
   }
@@ -157,13 +262,13 @@ struct Star {
   template <int NW, bool XYC = false, class F>
   __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
     // in-tile rows of every in-tile plane, with the x halos
-    stage_rows<SX, -H, TY * TZ, NW>(p, SX, fo,
-                                    [](int r, int& y, int& z, int& d) {
-                                      y = r % TY;
-                                      z = r / TY;
-                                      d = z * SY + y + H;
-                                    },
-                                    f);
+    stage_rows<TX + 2 * H, -H, TY * TZ, NW>(p + (XH - H), SX, fo,
+                                            [](int r, int& y, int& z, int& d) {
+                                              y = r % TY;
+                                              z = r / TY;
+                                              d = z * SY + y + H;
+                                            },
+                                            f);
     // the y-halo rows of every in-tile plane (with or without the corners)
     auto yh = [](int r, int& y, int& z, int& d) {
       const int k = r % (2 * H);
@@ -171,8 +276,8 @@ struct Star {
       z = r / (2 * H);
       d = z * SY + y + H;
     };
-    if (XYC) stage_rows<SX, -H, 2 * H * TZ, NW>(p, SX, fo, yh, f);
-    else stage_rows<TX, 0, 2 * H * TZ, NW>(p + H, SX, fo, yh, f);
+    if (XYC) stage_rows<TX + 2 * H, -H, 2 * H * TZ, NW>(p + (XH - H), SX, fo, yh, f);
+    else stage_rows<TX, 0, 2 * H * TZ, NW>(p + XH, SX, fo, yh, f);
     // z halos: in-tile rows of the 2H planes below and above the tile
     stage_rows<TX, 0, 2 * H * TY, NW>(p + SLAB, TX, fo,
                                       [](int r, int& y, int& z, int& d) {
@@ -183,41 +288,86 @@ struct Star {
                                       },
                                       f);
   }
+  // bulk form: every row one copy (y-halo rows always with the corners)
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)(SX * (TY * TZ + 2 * H * TZ) + TX * 2 * H * TY);
+  __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
+    tile::stage_bulk<SX, -XH, TY * TZ + 2 * H * TZ>(p, SX, fo, x0, nx,
+                                                   [](int r, int& y, int& z, int& d) {
+                                                     if (r < TY * TZ) {
+                                                       y = r % TY;
+                                                       z = r / TY;
+                                                     } else {
+                                                       const int q = r - TY * TZ, k = q % (2 * H);
+                                                       y = k < H ? k - H : TY + k - H;
+                                                       z = q / (2 * H);
+                                                     }
+                                                     d = z * SY + y + H;
+                                                   },
+                                                   src, bar);
+    tile::stage_bulk<TX, 0, 2 * H * TY>(p + SLAB, TX, fo, x0, nx,
+                                        [](int r, int& y, int& z, int& d) {
+                                          y = r % TY;
+                                          const int zz = r / TY;
+                                          z = zz < H ? zz - H : TZ + zz - H;
+                                          d = r;
+                                        },
+                                        src, bar);
+  }
 };
 
 template <int TX, int TY, int TZ>
 struct Box {
-  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H, SZ = TZ + 2 * H;
+  static constexpr int SX = TX + 2 * XH, SY = TY + 2 * H, SZ = TZ + 2 * H;
   static constexpr int SIZE = SX * SY * SZ;
   double* p;
-  __device__ __forceinline__ double v(int x, int y, int z) const { return p[((z + H) * SY + (y + H)) * SX + (x + H)]; }
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[((z + H) * SY + (y + H)) * SX + (x + XH)]; }
   template <int NW, class F>
   __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
-    stage_rows<SX, -H, SY * SZ, NW>(p, SX, fo,
-                                    [](int r, int& y, int& z, int& d) {
-                                      y = r % SY - H;
-                                      z = r / SY - H;
-                                      d = r;
-                                    },
-                                    f);
+    stage_rows<TX + 2 * H, -H, SY * SZ, NW>(p + (XH - H), SX, fo,
+                                            [](int r, int& y, int& z, int& d) {
+                                              y = r % SY - H;
+                                              z = r / SY - H;
+                                              d = r;
+                                            },
+                                            f);
+  }
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)(SX * SY * SZ);
+  __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
+    tile::stage_bulk<SX, -XH, SY * SZ>(p, SX, fo, x0, nx,
+                                      [](int r, int& y, int& z, int& d) {
+                                        y = r % SY - H;
+                                        z = r / SY - H;
+                                        d = r;
+                                      },
+                                      src, bar);
   }
 };
 
 // One-direction halo buffers (for fluxes differentiated along one axis only)
 template <int TX, int TY, int TZ>
 struct XRow {
-  static constexpr int SX = TX + 2 * H, SIZE = TZ * TY * SX;
+  static constexpr int SX = TX + 2 * XH, SIZE = TZ * TY * SX;
   double* p;
-  __device__ __forceinline__ double v(int x, int y, int z) const { return p[(z * TY + y) * SX + (x + H)]; }
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[(z * TY + y) * SX + (x + XH)]; }
   template <int NW, class F>
   __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
-    stage_rows<SX, -H, TY * TZ, NW>(p, SX, fo,
-                                    [](int r, int& y, int& z, int& d) {
-                                      y = r % TY;
-                                      z = r / TY;
-                                      d = r;
-                                    },
-                                    f);
+    stage_rows<TX + 2 * H, -H, TY * TZ, NW>(p + (XH - H), SX, fo,
+                                            [](int r, int& y, int& z, int& d) {
+                                              y = r % TY;
+                                              z = r / TY;
+                                              d = r;
+                                            },
+                                            f);
+  }
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)SIZE;
+  __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
+    tile::stage_bulk<SX, -XH, TY * TZ>(p, SX, fo, x0, nx,
+                                      [](int r, int& y, int& z, int& d) {
+                                        y = r % TY;
+                                        z = r / TY;
+                                        d = r;
+                                      },
+                                      src, bar);
   }
 };
 template <int TX, int TY, int TZ>
@@ -235,6 +385,16 @@ struct YRow {
                                    },
                                    f);
   }
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)SIZE;
+  __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
+    tile::stage_bulk<TX, 0, SY * TZ>(p, TX, fo, x0, nx,
+                                     [](int r, int& y, int& z, int& d) {
+                                       y = r % SY - H;
+                                       z = r / SY;
+                                       d = r;
+                                     },
+                                     src, bar);
+  }
 };
 template <int TX, int TY, int TZ>
 struct ZCol {
@@ -251,6 +411,16 @@ struct ZCol {
                                    },
                                    f);
   }
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)SIZE;
+  __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
+    tile::stage_bulk<TX, 0, TY * SZ>(p, TX, fo, x0, nx,
+                                     [](int r, int& y, int& z, int& d) {
+                                       y = r % TY;
+                                       z = r / TY - H;
+                                       d = r;
+                                     },
+                                     src, bar);
+  }
 };
 
 // Slab: the in-tile planes with x and y halos only, [TZ][TY+2H][TX+2H]. Used
@@ -258,27 +428,38 @@ struct ZCol {
 // z-halo values of a column are only read by the thread that owns it.
 template <int TX, int TY, int TZ>
 struct Slab {
-  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H;
+  static constexpr int SX = TX + 2 * XH, SY = TY + 2 * H;
   static constexpr int SIZE = TZ * SY * SX;
   double* p;
-  __device__ __forceinline__ double v(int x, int y, int z) const { return p[(z * SY + (y + H)) * SX + (x + H)]; }
+  __device__ __forceinline__ double v(int x, int y, int z) const { return p[(z * SY + (y + H)) * SX + (x + XH)]; }
   template <int NW, bool XYC = false, class F>
   __device__ void stage(const Folds<TX, TY, TZ>& fo, const F& f) const {
-    stage_rows<SX, -H, TY * TZ, NW>(p, SX, fo,
-                                    [](int r, int& y, int& z, int& d) {
-                                      y = r % TY;
-                                      z = r / TY;
-                                      d = z * SY + y + H;
-                                    },
-                                    f);
+    stage_rows<TX + 2 * H, -H, TY * TZ, NW>(p + (XH - H), SX, fo,
+                                            [](int r, int& y, int& z, int& d) {
+                                              y = r % TY;
+                                              z = r / TY;
+                                              d = z * SY + y + H;
+                                            },
+                                            f);
     auto yh = [](int r, int& y, int& z, int& d) {
       const int k = r % (2 * H);
       y = k < H ? k - H : TY + k - H;
       z = r / (2 * H);
       d = z * SY + y + H;
     };
-    if (XYC) stage_rows<SX, -H, 2 * H * TZ, NW>(p, SX, fo, yh, f);
-    else stage_rows<TX, 0, 2 * H * TZ, NW>(p + H, SX, fo, yh, f);
+    if (XYC) stage_rows<TX + 2 * H, -H, 2 * H * TZ, NW>(p + (XH - H), SX, fo, yh, f);
+    else stage_rows<TX, 0, 2 * H * TZ, NW>(p + XH, SX, fo, yh, f);
+  }
+  // bulk form: full rows, y halo with corners
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)SIZE;
+  __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
+    tile::stage_bulk<SX, -XH, SY * TZ>(p, SX, fo, x0, nx,
+                                      [](int r, int& y, int& z, int& d) {
+                                        y = r % SY - H;
+                                        z = r / SY;
+                                        d = r;
+                                      },
+                                      src, bar);
   }
 };
 
