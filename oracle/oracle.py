@@ -248,8 +248,10 @@ class OracleChem:
     that must not load the device library (the CPU reference arm)."""
 
     _SHAPES = {"ntint": (9,), "rgspec": (9,), "wmolar": (9,), "ncpoly": (9, 2), "ncenth": (9, 2),
-               "tinthi": (9, 2), "tintlo": (9, 2), "amasch": (9, 2, 7), "amascp": (9, 2, 7)}
-    _INT = ("ntint", "ncpoly", "ncenth")
+               "tinthi": (9, 2), "tintlo": (9, 2), "amasch": (9, 2, 7), "amascp": (9, 2, 7),
+               "ntroe": (1,), "nsrif": (1,), "nlind": (1,), "mtlist": (21,), "mslist": (21,), "mllist": (21,),
+               "rctroe": (10, 12), "rcsrif": (10, 8), "rclind": (10, 4)}
+    _INT = ("ntint", "ncpoly", "ncenth", "ntroe", "nsrif", "nlind", "mtlist", "mslist", "mllist")
 
     def __init__(self, path):
         self.path = path

@@ -2564,6 +2564,15 @@ int oracle_chem_table(const char* path, const char* name, double* out, int cap) 
     if (n == "amascp") return put(c.amascp, s3);
     if (n == "rgspec") return put(c.rgspec, orc::NSPCMX);
     if (n == "wmolar") return put(c.wmolar, orc::NSPCMX);
+    if (n == "ntroe") { const int v = c.ntroe; return put(&v, 1); }
+    if (n == "nsrif") { const int v = c.nsrif; return put(&v, 1); }
+    if (n == "nlind") { const int v = c.nlind; return put(&v, 1); }
+    if (n == "mtlist") return put(c.mtlist, orc::NSTPMX);
+    if (n == "mslist") return put(c.mslist, orc::NSTPMX);
+    if (n == "mllist") return put(c.mllist, orc::NSTPMX);
+    if (n == "rctroe") return put(c.rctroe, orc::NLLMAX * 12);
+    if (n == "rcsrif") return put(c.rcsrif, orc::NLLMAX * 8);
+    if (n == "rclind") return put(c.rclind, orc::NLLMAX * 4);
     g_err = "oracle_chem_table: unknown table " + n;
     return -1;
   } catch (std::exception& e) {
