@@ -177,6 +177,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="grid extent (cubic); 256 is the named workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the 128^3 flame and the batched ensemble measured beside the headline")
     ap.add_argument("--workload", default="h2_kernels", choices=["h2_kernels", "ensemble", "serve", "flame"],
                     help="h2_kernels: the 256^3 headline; ensemble: 64 batched boxes vs one at a time; "
                          "serve: Poisson request stream through the serving loop; "
@@ -365,6 +367,24 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cpu = cpu_baseline_sample(min(args.n, 128))
+    extras = None
+    if not args.no_extras and world == 1:
+        # the other named single-GPU workloads, device-timed on the same
+        # GPU: the 128^3 NSCBC flame (20 steps, filter every 10) and the
+        # 64-box ensemble (50 steps) batched against one box at a time
+        box.close()
+        import workloads
+
+        fl = workloads.run_flame(steps=20, warmup=3, device=local)
+        en = workloads.run_ensemble(steps=50, warmup=3, nbox=64, device=local)
+        extras = {
+            "flame_128": {"workload": "flame_inout_128^3_H2_nscbc_I3_O1, filter every 10 steps", "steps": 20,
+                          "value": fl["gpsu_s"], "unit": unit, "ms_per_step": 1e3 * fl["seconds"] / 20,
+                          "finite": fl["finite"], "status_word": fl["status_word"]},
+            "ensemble_64": {"workload": "64 boxes, axes from {32,48,64,96}, 1-step chemistry", "steps": 50,
+                            "points": en["points"], "batched_value": en["batched_gpsu_s"],
+                            "sequential_value": en["sequential_gpsu_s"], "unit": unit,
+                            "batched_vs_sequential": en["speedup"], "status_word": en["status_word"]}}
     line = {
         "metric": metric, "value": gpsu, "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -379,6 +399,7 @@ def main():
         "compulsory_bytes_per_gpsu": compulsory_bytes_per_gpsu(chem.nspec),
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "workloads": extras,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "status_word": status,

@@ -42,9 +42,8 @@ using FYRow = YRow<FX, FY, FZ>;
 using FZCol = ZCol<FX, FY, FZ>;
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
-constexpr int kFlowSmem =
-    cmax(cmax(FXRow::SIZE + FYRow::SIZE + FZCol::SIZE + FStar::SIZE, 2 * FStar::SIZE),
-         cmax(cmax(FXRow::SIZE + 2 * FStar::SIZE, FYRow::SIZE + FStar::SIZE + FZCol::SIZE), FStar::SIZE + FBox::SIZE));
+constexpr int kFlowSmem = cmax(cmax(FXRow::SIZE + FYRow::SIZE + FZCol::SIZE + FStar::SIZE, 2 * FStar::SIZE),
+                                cmax(3 * FXRow::SIZE + 3 * FYRow::SIZE, FStar::SIZE + FBox::SIZE));
 
 using SSlab = Slab<SX_, SY_, SZ_>;
 using SXRow = XRow<SX_, SY_, SZ_>;
@@ -106,7 +105,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
       rE[z] = -0.5 * (s4 + d1<0, P>(g, t, bE) * bru.v(t.x, t.y, t.z) + d1<1, P>(g, t, bE) * brv.v(t.x, t.y, t.z) +
                       d1<2, P>(g, t, bE) * brw.v(t.x, t.y, t.z));
     }
-    tile_sync_async();
+    tile_sync();
   }
   // ---- phase 2: heat conduction ----
   {
@@ -123,58 +122,72 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
                        d1<2, P>(g, t, bL) * d1<2, P>(g, t, bT));
       rE[z] = rE[z] + ((con ? 0.0 : d2<0, P>(g, t, bT)) + d2<1, P>(g, t, bT) + d2<2, P>(g, t, bT)) * bL.v(t.x, t.y, t.z);
     }
-    tile_sync_async();
+    tile_sync();
   }
   // ---- phase 3: pressure gradient (of p - p(1,1,1)) and pressure work ----
   {
-    const FStar bP{sm};
-    bP.stage<FNW>(fo, LdSub{f.p, __ldg(f.p + zd.base[0])});  // p(1,1,1) lives in slab 0
-    tile_sync();
+    const FStar bPr{sm};
+    const double p111 = __ldg(f.p + zd.base[0]);  // p(1,1,1) lives in slab 0
+    auto phase3 = [&](const auto& bP) {
 #pragma unroll
-    for (int z = 0; z < FZ; ++z) {
-      const TP& t = tp[z];
-      const double px = d1<0, P>(g, t, bP), py = d1<1, P>(g, t, bP), pz = d1<2, P>(g, t, bP);
-      rU[z] = -px;
-      rV[z] = -py;
-      rW[z] = -pz;
-      rE[z] = rE[z] - __ldg(f.vel + t.q) * px - __ldg(f.vel + n + t.q) * py - __ldg(f.vel + 2 * n + t.q) * pz;
+      for (int z = 0; z < FZ; ++z) {
+        const TP& t = tp[z];
+        const double px = d1<0, P>(g, t, bP), py = d1<1, P>(g, t, bP), pz = d1<2, P>(g, t, bP);
+        rU[z] = -px;
+        rV[z] = -py;
+        rW[z] = -pz;
+        rE[z] = rE[z] - __ldg(f.vel + t.q) * px - __ldg(f.vel + n + t.q) * py - __ldg(f.vel + 2 * n + t.q) * pz;
+      }
+    };
+    if constexpr (B) {
+      // raw p by bulk copies, p(1,1,1) subtracted where read: the same
+      // subtraction as staging p - p(1,1,1), so the same values
+      bPr.stage_bulk(fo, o.x0, g.nx, f.p, bar);
+      if (bb.wait(FStar::kBulkBytes, f.status)) return;
+      phase3(Shifted<FStar>{bPr, p111});
+    } else {
+      bPr.stage<FNW>(fo, LdSub{f.p, p111});
+      tile_sync();
+      phase3(bPr);
     }
     tile_sync();
   }
   // ---- phase 4: momentum fluxes d/dx_j (rho u_i u_j) ----
+  // x and y derivatives from products staged in x rows and y rows, z
+  // derivatives from products of register z-columns; each flux summed x, y,
+  // z in that order
   double S4[FZ], S5[FZ], S6[FZ];
   {
-    const FXRow bA{sm};
-    const FStar bB{sm + FXRow::SIZE}, bC{sm + FXRow::SIZE + FStar::SIZE};
-    bA.stage<FNW>(fo, LdMul{U + n, f.vel});
-    bB.stage<FNW>(fo, LdMul{U + n, f.vel + n});
-    bC.stage<FNW>(fo, LdMul{U + n, f.vel + 2 * n});
+    const FXRow xA{sm}, xB{sm + FXRow::SIZE}, xC{sm + 2 * FXRow::SIZE};
+    double* const sy = sm + 3 * FXRow::SIZE;
+    const FYRow yA{sy}, yB{sy + FYRow::SIZE}, yC{sy + 2 * FYRow::SIZE};
+    xA.stage<FNW>(fo, LdMul{U + n, f.vel});               // rho u u
+    xB.stage<FNW>(fo, LdMul{U + n, f.vel + n});           // rho u v
+    xC.stage<FNW>(fo, LdMul{U + n, f.vel + 2 * n});       // rho u w
+    yA.stage<FNW>(fo, LdMul{U + n, f.vel + n});           // rho u v
+    yB.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + n});       // rho v v
+    yC.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + 2 * n});   // rho v w
+    Column<FZ> cw, cm;
+    cw.load(fo, tx, ty, Ld{f.vel + 2 * n});
+    cm.load(fo, tx, ty, Ld{U + n});
     tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
-      S4[z] = d1<0, P>(g, t, bA) + d1<1, P>(g, t, bB) + d1<2, P>(g, t, bC);
-      S5[z] = d1<0, P>(g, t, bB);
-      S6[z] = d1<0, P>(g, t, bC);
+      S4[z] = d1<0, P>(g, t, xA);
+      S5[z] = d1<0, P>(g, t, xB);
+      S6[z] = d1<0, P>(g, t, xC);
+      S4[z] = S4[z] + d1<1, P>(g, t, yA);
+      S5[z] = S5[z] + d1<1, P>(g, t, yB);
+      S6[z] = S6[z] + d1<1, P>(g, t, yC);
+      S4[z] = S4[z] + d1zp<P>(g, t, cm, cw);  // rho u w
     }
-    tile_sync();
-  }
-  {
-    const FYRow bA{sm};
-    const FStar bB{sm + FYRow::SIZE};
-    const FZCol bC{sm + FYRow::SIZE + FStar::SIZE};
-    bA.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + n});
-    bB.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + 2 * n});
-    bC.stage<FNW>(fo, LdMul{U + 3 * n, f.vel + 2 * n});
-    tile_sync();
+    cm.load(fo, tx, ty, Ld{U + 2 * n});
 #pragma unroll
-    for (int z = 0; z < FZ; ++z) {
-      const TP& t = tp[z];
-      S5[z] = S5[z] + d1<1, P>(g, t, bA);
-      S5[z] = S5[z] + d1<2, P>(g, t, bB);
-      S6[z] = S6[z] + d1<1, P>(g, t, bB);
-      S6[z] = S6[z] + d1<2, P>(g, t, bC);
-    }
+    for (int z = 0; z < FZ; ++z) S5[z] = S5[z] + d1zp<P>(g, tp[z], cm, cw);  // rho v w
+    cm.load(fo, tx, ty, Ld{U + 3 * n});
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) S6[z] = S6[z] + d1zp<P>(g, tp[z], cm, cw);  // rho w w
     tile_sync_async();
   }
   // ---- phase 5: velocity derivatives, viscous stresses and work ----
@@ -224,7 +237,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
   }
-  tile_sync_async();
+  tile_sync();
   // 5b: v
   stage_plain<B, FNW>(bX, fo, g, o, f.vel + n, bar);
   if (sync_staged<B>(bb, FBox::kBulkBytes, f.status)) return;
@@ -263,7 +276,7 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     rW[z] += fn;
     rE[z] = rE[z] + wq * fn;
   }
-  tile_sync_async();
+  tile_sync();
   // 5c: w, then the first-derivative products
   stage_plain<B, FNW>(bX, fo, g, o, f.vel + 2 * n, bar);
   if (sync_staged<B>(bb, FBox::kBulkBytes, f.status)) return;
@@ -404,7 +417,6 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       SCol cy;
       cy.load(fo, tx, ty, Ld{f.y + s * n});
       // Y_s has landed in bS; the rho D and h slabs are free
-      if (B) fence_proxy_async();
       if (sync_staged<B>(bb, inflight, f.status)) return;
       stage_plain<B, SNW>(bR, fo, g, o, f.rd + s * n, bar);
       stage_plain<B, SNW>(bH, fo, g, o, f.h + s * n, bar);
@@ -470,7 +482,6 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       cd.load(fo, tx, ty, Ld{f.rd + s * n});
       ch.load(fo, tx, ty, Ld{f.h + s * n});
       // rho D_s, h_s have landed; every thread is done with Y_s
-      if (B) fence_proxy_async();
       if (sync_staged<B>(bb, inflight, f.status)) return;
       if (s + 1 < nspec) stage_plain<B, SNW>(bS, fo, g, o, f.y + (s + 1) * n, bar);
       inflight = SSlab::kBulkBytes;
@@ -592,7 +603,6 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     SCol cy;
     cy.load(fo, tx, ty, Ld{f.y + s * n});
     // Y_s has landed in slab(s); every thread is done with the other slab
-    if (B) fence_proxy_async();
     if (sync_staged<B>(bb, SSlab::kBulkBytes, f.status)) return;
     if (s + 1 < nspec) stage_plain<B, SNW>(slab(s + 1), fo, g, o, f.y + (s + 1) * n, bar);
     const SSlab bY = slab(s);
@@ -710,16 +720,17 @@ bool all_periodic(const Geo& g) { return g.per[0] && g.per[1] && g.per[2]; }
 
 bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-// The bulk (TMA engine) staging applies to all-periodic boxes of one context
-// with even nx whose staged fields start on 16-byte boundaries; SENGA_STAGE=
-// cpasync in the environment keeps every box on per-element copies.
+// Bulk staging (rows copied by the TMA engine) is opt-in: SENGA_STAGE=bulk
+// in the environment. It applies to all-periodic boxes of one context with
+// even nx whose staged fields start on 16-byte boundaries. Measured on the
+// 256^3 H2 box it is slower than the per-element cp.async fills for the
+// species kernels (8.2 against 6.5 ms per launch; one 256-352 byte copy per
+// tile row) and even for flow, so the per-element fills are the default.
 bool bulk_ok(const Geo& g, const Fields& f, const ZDec& zd) {
-  static const bool off = [] {
-    const char* e = getenv("SENGA_STAGE");
-    return e && std::string(e) == "cpasync";
-  }();
-  if (off || !all_periodic(g) || zd.nr > 1 || (g.nx & 1)) return false;
-  const void* ptrs[] = {f.uin, f.e, f.t, f.lam, f.mu, f.vel, f.y, f.rd, f.h, f.hmix};
+  const char* e = getenv("SENGA_STAGE");  // read per launch (or graph capture)
+  const bool on = e && std::string(e) == "bulk";
+  if (!on || !all_periodic(g) || zd.nr > 1 || (g.nx & 1)) return false;
+  const void* ptrs[] = {f.uin, f.e, f.t, f.lam, f.mu, f.vel, f.y, f.rd, f.h, f.hmix, f.p};
   for (const void* p : ptrs)
     if (p && !al16(p)) return false;
   return true;

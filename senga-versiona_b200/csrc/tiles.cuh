@@ -17,12 +17,12 @@
 //   XRow : [TZ][TY][SX]    YRow : [TZ][TY+2H][TX]    ZCol : [TZ+2H][TY][TX]
 //
 // Two ways of filling them. stage(): per-element cp.async by every thread
-// (any box). stage_bulk(): each row is one bulk copy on the TMA engine
-// (cp.async.bulk, completion counted on an mbarrier), split in two where a
-// periodic x direction wraps; no LSU instruction per element. The bulk path
-// needs an all-periodic box of even nx, 16-byte aligned fields and one
-// context (the launcher checks), because each copy must start on a 16-byte
-// boundary and be a multiple of 16 bytes long.
+// (any box; the default). stage_bulk(): each row is one bulk copy on the TMA
+// engine (cp.async.bulk, completion counted on an mbarrier), split in two
+// where a periodic x direction wraps; no LSU instruction per element. The
+// bulk path needs an all-periodic box of even nx, 16-byte aligned fields and
+// one context (the launcher checks), because each copy must start on a
+// 16-byte boundary and be a multiple of 16 bytes long.
 #pragma once
 #include <cstdint>
 
@@ -91,16 +91,22 @@ __device__ __forceinline__ void tile_sync() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
 }
-// tile_sync before bulk copies overwrite buffers that threads read or wrote:
-// every thread orders its own shared-memory accesses before the async proxy
+// tile_sync before bulk copies overwrite buffers that threads wrote with
+// ordinary stores: every thread orders its writes before the async proxy
+// (after reads alone the barrier suffices)
 __device__ __forceinline__ void tile_sync_async() {
   asm volatile("cp.async.wait_all;\n fence.proxy.async.shared::cta;\n" ::: "memory");
   __syncthreads();
 }
 // ---- bulk copies on the TMA engine, completion on an mbarrier ----
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+// initialise, and make the initialised barrier visible to the async proxy
+// (the TMA engine) before any copy can signal it
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n fence.mbarrier_init.release.cluster;\n" ::"r"(
+                   smem_u32(bar)),
+               "r"(count)
+               : "memory");
 }
 // the single arrival of a phase, announcing the bytes its copies will deliver
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
@@ -288,22 +294,25 @@ struct Star {
                                       },
                                       f);
   }
-  // bulk form: every row one copy (y-halo rows always with the corners)
-  static constexpr unsigned kBulkBytes = 8u * (unsigned)(SX * (TY * TZ + 2 * H * TZ) + TX * 2 * H * TY);
+  // bulk form: every row one copy; the y-halo rows without the corners
+  // (the bulk-staged Stars feed first and second derivatives only)
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)(SX * TY * TZ + TX * 2 * H * TZ + TX * 2 * H * TY);
   __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
-    tile::stage_bulk<SX, -XH, TY * TZ + 2 * H * TZ>(p, SX, fo, x0, nx,
-                                                   [](int r, int& y, int& z, int& d) {
-                                                     if (r < TY * TZ) {
-                                                       y = r % TY;
-                                                       z = r / TY;
-                                                     } else {
-                                                       const int q = r - TY * TZ, k = q % (2 * H);
-                                                       y = k < H ? k - H : TY + k - H;
-                                                       z = q / (2 * H);
-                                                     }
-                                                     d = z * SY + y + H;
-                                                   },
-                                                   src, bar);
+    tile::stage_bulk<SX, -XH, TY * TZ>(p, SX, fo, x0, nx,
+                                      [](int r, int& y, int& z, int& d) {
+                                        y = r % TY;
+                                        z = r / TY;
+                                        d = z * SY + y + H;
+                                      },
+                                      src, bar);
+    tile::stage_bulk<TX, 0, 2 * H * TZ>(p + XH, SX, fo, x0, nx,
+                                        [](int r, int& y, int& z, int& d) {
+                                          const int k = r % (2 * H);
+                                          y = k < H ? k - H : TY + k - H;
+                                          z = r / (2 * H);
+                                          d = z * SY + y + H;
+                                        },
+                                        src, bar);
     tile::stage_bulk<TX, 0, 2 * H * TY>(p + SLAB, TX, fo, x0, nx,
                                         [](int r, int& y, int& z, int& d) {
                                           y = r % TY;
@@ -450,16 +459,25 @@ struct Slab {
     if (XYC) stage_rows<TX + 2 * H, -H, 2 * H * TZ, NW>(p + (XH - H), SX, fo, yh, f);
     else stage_rows<TX, 0, 2 * H * TZ, NW>(p + XH, SX, fo, yh, f);
   }
-  // bulk form: full rows, y halo with corners
-  static constexpr unsigned kBulkBytes = 8u * (unsigned)SIZE;
+  // bulk form: the in-tile rows with their x halos, the y-halo rows without
+  // the corners (the same footprint as the per-element form)
+  static constexpr unsigned kBulkBytes = 8u * (unsigned)(SX * TY * TZ + TX * 2 * H * TZ);
   __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
-    tile::stage_bulk<SX, -XH, SY * TZ>(p, SX, fo, x0, nx,
+    tile::stage_bulk<SX, -XH, TY * TZ>(p, SX, fo, x0, nx,
                                       [](int r, int& y, int& z, int& d) {
-                                        y = r % SY - H;
-                                        z = r / SY;
-                                        d = r;
+                                        y = r % TY;
+                                        z = r / TY;
+                                        d = z * SY + y + H;
                                       },
                                       src, bar);
+    tile::stage_bulk<TX, 0, 2 * H * TZ>(p + XH, SX, fo, x0, nx,
+                                        [](int r, int& y, int& z, int& d) {
+                                          const int k = r % (2 * H);
+                                          y = k < H ? k - H : TY + k - H;
+                                          z = r / (2 * H);
+                                          d = z * SY + y + H;
+                                        },
+                                        src, bar);
   }
 };
 
@@ -475,6 +493,15 @@ struct Column {
 #pragma unroll
     for (int k = 0; k < TZ + 2 * H; ++k) c[k] = f(b + fo.oz[k]);
   }
+};
+
+// A staged buffer read with a constant subtracted from every value (the
+// pressure gradient of p - p(1,1,1), src/rhsvel.f:741-746).
+template <class Buf>
+struct Shifted {
+  Buf b;
+  double c;
+  __device__ __forceinline__ double v(int x, int y, int z) const { return b.v(x, y, z) - c; }
 };
 
 // A grid point of the tile as seen by one thread.
@@ -538,18 +565,21 @@ __device__ __forceinline__ double dm(const Geo& g, const TP& t, const B& b) {
   return dmcore(v) * g.ovd[DA] * g.ovd[DB];
 }
 
-// z derivatives from a register column (z in-tile, compile-time after unrolling)
+// z derivatives from a register column (z in-tile, compile-time after
+// unrolling). z is periodic on every box these tile kernels run on (boxes
+// bounded in y or z are refused before any right-hand-side launch), so the
+// interior scheme is compiled in and the column stays in registers.
 template <bool P, int TZ>
 __device__ __forceinline__ double d1z(const Geo& g, const TP& t, const Column<TZ>& col) {
-  return d1core([&](int m) { return col.c[t.z + H + m]; }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd[2];
+  return d1core([&](int m) { return col.c[t.z + H + m]; }, t.gz, g.nz, 1) * g.ovd[2];
 }
 template <bool P, int TZ>
 __device__ __forceinline__ double d2z(const Geo& g, const TP& t, const Column<TZ>& col) {
-  return d2core([&](int m) { return col.c[t.z + H + m]; }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd2[2];
+  return d2core([&](int m) { return col.c[t.z + H + m]; }, t.gz, g.nz, 1) * g.ovd2[2];
 }
 template <bool P, int TZ>
 __device__ __forceinline__ double d1zp(const Geo& g, const TP& t, const Column<TZ>& a, const Column<TZ>& b) {
-  return d1core([&](int m) { return a.c[t.z + H + m] * b.c[t.z + H + m]; }, t.gz, g.nz, P ? 1 : g.per[2]) * g.ovd[2];
+  return d1core([&](int m) { return a.c[t.z + H + m] * b.c[t.z + H + m]; }, t.gz, g.nz, 1) * g.ovd[2];
 }
 
 }  // namespace tile

@@ -85,6 +85,9 @@ def test_falloff_rates_rhs_and_steps_match_oracle():
     rr, tr, _ = ref.rhs()
     for k in range(rr.shape[0]):
         assert rel_linf(r[k], rr[k]) <= TOL, f"RHS field {k}"
+    # rhs() leaves R(U) in the U register: start the steps from the state
+    box.upload(c["fields"], c["T"], c["itn"])
+    ref.upload(c["fields"], c["T"], c["itn"])
     box.step(3)
     ref.step(3)
     g, tg, _ = box.download()
