@@ -61,6 +61,28 @@ __device__ __forceinline__ void stage_plain(const Buf& b, const FO& fo, const Ge
   if constexpr (B) b.stage_bulk(fo, o.x0, g.nx, src, bar);
   else b.template stage<NW>(fo, Ld{src});
 }
+// Tensor maps of the species kernels (tensor-copy mode): the Y, rho D and h
+// families as 4-D tensors [species][z][y][x] with boxes of one slab
+// (SX x (TY+2H) x TZ), and the U register [field][z][y][x] with the x-row and
+// y-row boxes of rho u and rho v; hmix as a one-field 4-D tensor.
+struct SpecMaps {
+  CUtensorMap y, rd, h, ux, vy;
+};
+struct RkMaps {
+  CUtensorMap y, hm;
+};
+// a tile whose halo-extended x and y ranges lie inside the box takes one
+// tensor copy per buffer; tiles at the periodic wrap copy rows
+// (tensor copies land on 128-byte aligned buffers: the dynamic shared
+// memory base is checked, the buffer offsets are multiples of 128 bytes)
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ bool tensor_tile(const Geo& g, const Origin& o, const double* sm) {
+  return (smem_u32(sm) & 127u) == 0 && o.x0 >= XH && o.x0 + TX + XH <= g.nx && o.y0 >= H &&
+         o.y0 + TY + H <= g.ny && o.z0 + TZ <= g.nz;
+}
+static_assert((8 * SXRow::SIZE) % 128 == 0 && (8 * SYRow::SIZE) % 128 == 0 && (8 * SSlab::SIZE) % 128 == 0,
+              "tensor-copy buffers start on 128-byte boundaries");
+
 template <bool B>
 __device__ __forceinline__ bool sync_staged(BulkBar& bb, unsigned bytes, unsigned int* status) {
   if constexpr (B) return bb.wait(bytes, status);
@@ -376,9 +398,23 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
 }
 
 // -------------------------------------------------------------------------
-template <bool P, bool B = false>
+// M: 0 per-element cp.async, 1 bulk row copies, 2 one tensor copy per buffer
+// for tiles away from the wrap (bulk rows for the others)
+template <bool P, int M = 0>
 __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int nspec, const Origin o, double* sm,
-                                             Folds<SX_, SY_, SZ_>& fo, const ZDec& zd, uint64_t* bar = nullptr) {
+                                             Folds<SX_, SY_, SZ_>& fo, const ZDec& zd, uint64_t* bar = nullptr,
+                                             const SpecMaps* tm = nullptr) {
+  constexpr bool B = M > 0;
+  const bool tens = M == 2 && tensor_tile<SX_, SY_, SZ_>(g, o, sm);
+  constexpr unsigned kSlabT = 8u * SSlab::SIZE;  // a tensor copy fills the whole slab
+  const unsigned slab_bytes = tens ? kSlabT : SSlab::kBulkBytes;
+  auto stage_f = [&](const SSlab& b, const CUtensorMap* m, int s, const double* src) {
+    if (tens) {
+      if (threadIdx.x == 0) tma_load_4d(b.p, m, o.x0 - XH, o.y0 - H, o.z0, s, bar);
+    } else {
+      stage_plain<B, SNW>(b, fo, g, o, src, bar);
+    }
+  };
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
   fo.init(g, o, zd);
   BulkBar bb{bar, 0u};
@@ -394,13 +430,20 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
   const SSlab bS{sm + SXRow::SIZE + SYRow::SIZE};
   const SSlab bH{sm + SXRow::SIZE + SYRow::SIZE + SSlab::SIZE};
   const SSlab bR{sm + SXRow::SIZE + SYRow::SIZE + 2 * SSlab::SIZE};
-  stage_plain<B, SNW>(bru, fo, g, o, U + n, bar);
-  stage_plain<B, SNW>(brv, fo, g, o, U + 2 * n, bar);
+  if (tens) {
+    if (threadIdx.x == 0) {
+      tma_load_4d(bru.p, &tm->ux, o.x0 - XH, o.y0, o.z0, 1, bar);
+      tma_load_4d(brv.p, &tm->vy, o.x0, o.y0 - H, o.z0, 2, bar);
+    }
+  } else {
+    stage_plain<B, SNW>(bru, fo, g, o, U + n, bar);
+    stage_plain<B, SNW>(brv, fo, g, o, U + 2 * n, bar);
+  }
   // copies run one stage ahead: Y_s while the previous species' rho D and
   // h are used, rho D and h of species s while Y_s is used
-  if (nspec > 0) stage_plain<B, SNW>(bS, fo, g, o, f.y, bar);
-  // bytes of the group in flight (bulk path): rho u, rho v and Y_0 first
-  unsigned inflight = SXRow::kBulkBytes + SYRow::kBulkBytes + SSlab::kBulkBytes;
+  if (nspec > 0) stage_f(bS, tm ? &tm->y : nullptr, 0, f.y);
+  // bytes of the group in flight (bulk paths): rho u, rho v and Y_0 first
+  unsigned inflight = SXRow::kBulkBytes + SYRow::kBulkBytes + slab_bytes;
   SCol rw;
   rw.load(fo, tx, ty, Ld{U + 3 * n});
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
@@ -418,9 +461,9 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       cy.load(fo, tx, ty, Ld{f.y + s * n});
       // Y_s has landed in bS; the rho D and h slabs are free
       if (sync_staged<B>(bb, inflight, f.status)) return;
-      stage_plain<B, SNW>(bR, fo, g, o, f.rd + s * n, bar);
-      stage_plain<B, SNW>(bH, fo, g, o, f.h + s * n, bar);
-      inflight = 2 * SSlab::kBulkBytes;
+      stage_f(bR, tm ? &tm->rd : nullptr, s, f.rd + s * n);
+      stage_f(bH, tm ? &tm->h : nullptr, s, f.h + s * n);
+      inflight = 2 * slab_bytes;
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -483,8 +526,8 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       ch.load(fo, tx, ty, Ld{f.h + s * n});
       // rho D_s, h_s have landed; every thread is done with Y_s
       if (sync_staged<B>(bb, inflight, f.status)) return;
-      if (s + 1 < nspec) stage_plain<B, SNW>(bS, fo, g, o, f.y + (s + 1) * n, bar);
-      inflight = SSlab::kBulkBytes;
+      if (s + 1 < nspec) stage_f(bS, tm ? &tm->y : nullptr, s + 1, f.y + (s + 1) * n);
+      inflight = slab_bytes;
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
@@ -525,10 +568,20 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
 }
 
 // -------------------------------------------------------------------------
-template <bool P, bool B = false>
+template <bool P, int M = 0>
 __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, int nspec, const RK& rk,
                                                 const Origin o, double* sm, Folds<SX_, SY_, SZ_>& fo,
-                                                const ZDec& zd, uint64_t* bar = nullptr) {
+                                                const ZDec& zd, uint64_t* bar = nullptr, const RkMaps* tm = nullptr) {
+  constexpr bool B = M > 0;
+  const bool tens = M == 2 && tensor_tile<SX_, SY_, SZ_>(g, o, sm);
+  const unsigned slab_bytes = tens ? 8u * SSlab::SIZE : SSlab::kBulkBytes;
+  auto stage_f = [&](const SSlab& b, const CUtensorMap* m, int s, const double* src) {
+    if (tens) {
+      if (threadIdx.x == 0) tma_load_4d(b.p, m, o.x0 - XH, o.y0 - H, o.z0, s, bar);
+    } else {
+      stage_plain<B, SNW>(b, fo, g, o, src, bar);
+    }
+  };
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
   fo.init(g, o, zd);
   BulkBar bb{bar, 0u};
@@ -581,9 +634,9 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
   {
     SCol cm;
     cm.load(fo, tx, ty, Ld{f.hmix});
-    stage_plain<B, SNW>(bS, fo, g, o, f.hmix, bar);
-    if (sync_staged<B>(bb, SSlab::kBulkBytes, f.status)) return;
-    if (nspec > 0) stage_plain<B, SNW>(slab(0), fo, g, o, f.y, bar);
+    stage_f(bS, tm ? &tm->hm : nullptr, 0, f.hmix);
+    if (sync_staged<B>(bb, slab_bytes, f.status)) return;
+    if (nspec > 0) stage_f(slab(0), tm ? &tm->y : nullptr, 0, f.y);
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
@@ -603,8 +656,8 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     SCol cy;
     cy.load(fo, tx, ty, Ld{f.y + s * n});
     // Y_s has landed in slab(s); every thread is done with the other slab
-    if (sync_staged<B>(bb, SSlab::kBulkBytes, f.status)) return;
-    if (s + 1 < nspec) stage_plain<B, SNW>(slab(s + 1), fo, g, o, f.y + (s + 1) * n, bar);
+    if (sync_staged<B>(bb, slab_bytes, f.status)) return;
+    if (s + 1 < nspec) stage_f(slab(s + 1), tm ? &tm->y : nullptr, s + 1, f.y + (s + 1) * n);
     const SSlab bY = slab(s);
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
@@ -640,22 +693,24 @@ __global__ void __launch_bounds__(FX* FY, SENGA_FLOW_MINB) k_flow_t(Geo g, Field
   __shared__ uint64_t bar;
   flow_tile<P, B>(g, f, Origin{(int)blockIdx.x * FX, (int)blockIdx.y * FY, (int)blockIdx.z * FZ}, sm, fo, zd, &bar);
 }
-template <bool P, bool B>
-__global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB) k_species_t(Geo g, Fields f, int nspec, ZDec zd) {
-  extern __shared__ __align__(16) double sm[];
+template <bool P, int M>
+__global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB)
+    k_species_t(Geo g, Fields f, int nspec, ZDec zd, const __grid_constant__ SpecMaps tm) {
+  extern __shared__ __align__(128) double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
   __shared__ uint64_t bar;
-  species_tile<P, B>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm,
-                     fo, zd, &bar);
+  species_tile<P, M>(g, f, nspec, Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm,
+                     fo, zd, &bar, &tm);
 }
-template <bool P, bool B>
-__global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB) k_species_rk_t(Geo g, Fields f, int nspec, RK rk, ZDec zd) {
-  extern __shared__ __align__(16) double sm[];
+template <bool P, int M>
+__global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB)
+    k_species_rk_t(Geo g, Fields f, int nspec, RK rk, ZDec zd, const __grid_constant__ RkMaps tm) {
+  extern __shared__ __align__(128) double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
   __shared__ uint64_t bar;
-  species_rk_tile<P, B>(g, f, nspec, rk,
+  species_rk_tile<P, M>(g, f, nspec, rk,
                         Origin{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_}, sm, fo, zd,
-                        &bar);
+                        &bar, &tm);
 }
 
 // ---- batched launches: one CTA per (box, tile) work item; box descriptors
@@ -703,12 +758,16 @@ void set_attrs() {
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
   if (done[dev]) return;
   cudaFuncSetAttribute(k_flow_t<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
-  cudaFuncSetAttribute(k_species_t<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
-  cudaFuncSetAttribute(k_species_rk_t<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
+  cudaFuncSetAttribute(k_species_t<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
+  cudaFuncSetAttribute(k_species_rk_t<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
   if (P) {
     cudaFuncSetAttribute(k_flow_t<P, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
-    cudaFuncSetAttribute(k_species_t<P, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
-    cudaFuncSetAttribute(k_species_rk_t<P, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecRkSmem * 8);
+    cudaFuncSetAttribute(k_species_t<P, P ? 1 : 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
+    cudaFuncSetAttribute(k_species_rk_t<P, P ? 1 : 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kSpecRkSmem * 8);
+    cudaFuncSetAttribute(k_species_t<P, P ? 2 : 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
+    cudaFuncSetAttribute(k_species_rk_t<P, P ? 2 : 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kSpecRkSmem * 8);
   }
   cudaFuncSetAttribute(k_flow_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFlowSmem * 8);
   cudaFuncSetAttribute(k_species_b<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecSmem * 8);
@@ -720,20 +779,53 @@ bool all_periodic(const Geo& g) { return g.per[0] && g.per[1] && g.per[2]; }
 
 bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-// Bulk staging (rows copied by the TMA engine) is opt-in: SENGA_STAGE=bulk
-// in the environment. It applies to all-periodic boxes of one context with
-// even nx whose staged fields start on 16-byte boundaries. Measured on the
-// 256^3 H2 box it is slower than the per-element cp.async fills for the
-// species kernels (8.2 against 6.5 ms per launch; one 256-352 byte copy per
-// tile row) and even for flow, so the per-element fills are the default.
-bool bulk_ok(const Geo& g, const Fields& f, const ZDec& zd) {
-  const char* e = getenv("SENGA_STAGE");  // read per launch (or graph capture)
-  const bool on = e && std::string(e) == "bulk";
-  if (!on || !all_periodic(g) || zd.nr > 1 || (g.nx & 1)) return false;
+// Staging mode of the stencil tiles, from SENGA_STAGE (read at every launch
+// or graph capture): unset or "cpasync" per-element cp.async; "bulk" rows
+// copied by the TMA engine; "tma" one tensor copy per buffer for tiles away
+// from the periodic wrap (rows for the others; the species kernels). The
+// bulk and tensor modes apply to all-periodic boxes of one context with even
+// nx whose staged fields start on 16-byte boundaries; others use cp.async.
+// Measured on the 256^3 H2 box, bulk rows are slower than the per-element
+// fills for the species kernels (8.2 against 6.5 ms per launch; one 256-352
+// byte copy per tile row) and equal for flow.
+int stage_mode(const Geo& g, const Fields& f, const ZDec& zd) {
+  const char* e = getenv("SENGA_STAGE");
+  const int m = !e ? 0 : std::string(e) == "bulk" ? 1 : std::string(e) == "tma" ? 2 : 0;
+  if (!m || !all_periodic(g) || zd.nr > 1 || (g.nx & 1)) return 0;
   const void* ptrs[] = {f.uin, f.e, f.t, f.lam, f.mu, f.vel, f.y, f.rd, f.h, f.hmix, f.p};
   for (const void* p : ptrs)
-    if (p && !al16(p)) return false;
-  return true;
+    if (p && !al16(p)) return 0;
+  return m;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encoder() {
+  static EncodeTiled fn = [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiled) nullptr;
+    return (EncodeTiled)ptr;
+  }();
+  return fn;
+}
+// [k][z][y][x] FP64 tensor of nk fields of the box, x fastest, box
+// bx x by x bz x 1; returns false when the encoder refuses it
+bool make_map(CUtensorMap* m, const double* base, const Geo& g, int nk, unsigned bx, unsigned by, unsigned bz) {
+  EncodeTiled enc = encoder();
+  if (!enc || !base) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, (cuuint64_t)nk};
+  const cuuint64_t strides[3] = {(cuuint64_t)g.nx * 8, (cuuint64_t)g.nx * g.ny * 8, (cuuint64_t)g.n * 8};
+  const cuuint32_t box[4] = {bx, by, bz, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 }  // namespace
@@ -741,7 +833,7 @@ bool bulk_ok(const Geo& g, const Fields& f, const ZDec& zd) {
 void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    if (bulk_ok(g, f, zd))
+    if (stage_mode(g, f, zd) == 1)  // rows; the tensor mode covers the species kernels only
       k_flow_t<true, true><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
     else
       k_flow_t<true, false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
@@ -752,28 +844,41 @@ void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s, const ZDec&
 }
 
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd) {
+  const dim3 grid = tiles(g, SX_, SY_, SZ_);
+  SpecMaps tm{};
   if (all_periodic(g)) {
     set_attrs<true>();
-    if (bulk_ok(g, f, zd))
-      k_species_t<true, true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
-    else
-      k_species_t<true, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
+    int m = stage_mode(g, f, zd);
+    if (m == 2 && !(make_map(&tm.y, f.y, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
+                    make_map(&tm.rd, f.rd, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
+                    make_map(&tm.h, f.h, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
+                    make_map(&tm.ux, f.uin, g, 5 + nspec, SXRow::SX, SY_, SZ_) &&
+                    make_map(&tm.vy, f.uin, g, 5 + nspec, SX_, SYRow::SY, SZ_)))
+      m = 1;
+    if (m == 2) k_species_t<true, 2><<<grid, SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd, tm);
+    else if (m == 1) k_species_t<true, 1><<<grid, SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd, tm);
+    else k_species_t<true, 0><<<grid, SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd, tm);
   } else {
     set_attrs<false>();
-    k_species_t<false, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd);
+    k_species_t<false, 0><<<grid, SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd, tm);
   }
 }
 
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s, const ZDec& zd) {
+  const dim3 grid = tiles(g, SX_, SY_, SZ_);
+  RkMaps tm{};
   if (all_periodic(g)) {
     set_attrs<true>();
-    if (bulk_ok(g, f, zd))
-      k_species_rk_t<true, true><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
-    else
-      k_species_rk_t<true, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
+    int m = stage_mode(g, f, zd);
+    if (m == 2 && !(make_map(&tm.y, f.y, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
+                    make_map(&tm.hm, f.hmix, g, 1, SSlab::SX, SSlab::SY, SZ_)))
+      m = 1;
+    if (m == 2) k_species_rk_t<true, 2><<<grid, SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd, tm);
+    else if (m == 1) k_species_rk_t<true, 1><<<grid, SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd, tm);
+    else k_species_rk_t<true, 0><<<grid, SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd, tm);
   } else {
     set_attrs<false>();
-    k_species_rk_t<false, false><<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd);
+    k_species_rk_t<false, 0><<<grid, SX_ * SY_, kSpecRkSmem * 8, s>>>(g, f, nspec, rk, zd, tm);
   }
 }
 

@@ -24,6 +24,8 @@
 // one context (the launcher checks), because each copy must start on a
 // 16-byte boundary and be a multiple of 16 bytes long.
 #pragma once
+#include <cuda.h>  // CUtensorMap (the descriptor type only)
+
 #include <cstdint>
 
 #include "stencil.cuh"
@@ -121,6 +123,18 @@ __device__ __forceinline__ void bulk_g2s(double* dst, const double* src, unsigne
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
           smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// One tiled tensor copy (TMA) of a 4-D box starting at coordinates
+// {c0 (x, innermost), c1, c2, c3} of the tensor `map` describes, into dst
+// (128-byte aligned), completion counted on bar. The map lives in the
+// kernel's parameter space (a __grid_constant__ argument).
+__device__ __forceinline__ void tma_load_4d(double* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
 }
 // Waits for phase `parity` of bar to complete, for at most about one second

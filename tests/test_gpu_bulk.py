@@ -1,6 +1,7 @@
 """Stencil tiles filled by bulk copies on the TMA engine (all-periodic boxes
-of even nx; opt-in with SENGA_STAGE=bulk, which the library reads at every
-launch) against the oracle.
+of even nx; opt-in with SENGA_STAGE=bulk for row copies or SENGA_STAGE=tma
+for one tensor copy per buffer on tiles away from the wrap, which the
+library reads at every launch) against the oracle.
 
 Each staged row spans the tile's x range plus six points on either side; in a
 periodic box it is cut where x wraps, and a box narrower than one row wraps
@@ -18,12 +19,13 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
 CASES = [("h2_pool", (10, 12, 8)), ("h2_pool", (34, 9, 7)), ("h2_pool", (46, 12, 6)), ("h2_pool", (2, 14, 10)),
-         ("ignition32", None)]
+         ("h2_pool", (96, 40, 6)), ("ignition32", None)]
 
 
+@pytest.mark.parametrize("mode", ["bulk", "tma"])
 @pytest.mark.parametrize("name,shape", CASES, ids=[f"{n}-{'x'.join(map(str, s)) if s else '20^3'}" for n, s in CASES])
-def test_bulk_staged_tiles_match_oracle(name, shape, monkeypatch):
-    monkeypatch.setenv("SENGA_STAGE", "bulk")
+def test_bulk_staged_tiles_match_oracle(name, shape, mode, monkeypatch):
+    monkeypatch.setenv("SENGA_STAGE", mode)
     import cases
     import senga
     from oracle import Oracle
