@@ -780,17 +780,27 @@ bool all_periodic(const Geo& g) { return g.per[0] && g.per[1] && g.per[2]; }
 bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 // Staging mode of the stencil tiles, from SENGA_STAGE (read at every launch
-// or graph capture): unset or "cpasync" per-element cp.async; "bulk" rows
-// copied by the TMA engine; "tma" one tensor copy per buffer for tiles away
-// from the periodic wrap (rows for the others; the species kernels). The
-// bulk and tensor modes apply to all-periodic boxes of one context with even
-// nx whose staged fields start on 16-byte boundaries; others use cp.async.
-// Measured on the 256^3 H2 box, bulk rows are slower than the per-element
-// fills for the species kernels (8.2 against 6.5 ms per launch; one 256-352
-// byte copy per tile row) and equal for flow.
-int stage_mode(const Geo& g, const Fields& f, const ZDec& zd) {
+// or graph capture): 0 per-element cp.async, 1 rows copied by the TMA engine,
+// 2 one tensor copy per buffer for tiles away from the periodic wrap (rows
+// for the others; species kernels). Unset: rows for flow, cp.async for the
+// species kernels; "cpasync", "bulk", "tma" force one mode ("tma" leaves flow
+// on rows). Bulk and tensor modes apply to all-periodic boxes of one context
+// with even nx whose staged fields start on 16-byte boundaries; other boxes
+// use cp.async. Measured per launch on the 256^3 H2 box (cp.async / rows /
+// tensor): flow 5.13 / 4.92 / -, species 6.47 / 8.18 / 8.28, species+RK
+// 2.95 / 3.21 / 3.44 ms. The species kernels read their z neighbours from
+// register columns loaded through L1, which the cp.async.ca fills of the
+// same tile warm; copies on the TMA engine bypass L1, so those loads go to
+// L2 (long-scoreboard stalls 7.9 against 1.4 per issue). Flow's buffers hold
+// their z halos in shared memory and gain from the rows.
+enum Kern { KFlow, KSpecies };
+int stage_mode(const Geo& g, const Fields& f, const ZDec& zd, Kern k) {
   const char* e = getenv("SENGA_STAGE");
-  const int m = !e ? 0 : std::string(e) == "bulk" ? 1 : std::string(e) == "tma" ? 2 : 0;
+  const std::string v = e ? e : "";
+  int m = k == KFlow ? 1 : 0;
+  if (v == "cpasync") m = 0;
+  else if (v == "bulk") m = 1;
+  else if (v == "tma") m = k == KFlow ? 1 : 2;
   if (!m || !all_periodic(g) || zd.nr > 1 || (g.nx & 1)) return 0;
   const void* ptrs[] = {f.uin, f.e, f.t, f.lam, f.mu, f.vel, f.y, f.rd, f.h, f.hmix, f.p};
   for (const void* p : ptrs)
@@ -833,7 +843,7 @@ bool make_map(CUtensorMap* m, const double* base, const Geo& g, int nk, unsigned
 void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s, const ZDec& zd) {
   if (all_periodic(g)) {
     set_attrs<true>();
-    if (stage_mode(g, f, zd) == 1)  // rows; the tensor mode covers the species kernels only
+    if (stage_mode(g, f, zd, KFlow) == 1)
       k_flow_t<true, true><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
     else
       k_flow_t<true, false><<<tiles(g, FX, FY, FZ), FX * FY, kFlowSmem * 8, s>>>(g, f, zd);
@@ -848,7 +858,7 @@ void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, 
   SpecMaps tm{};
   if (all_periodic(g)) {
     set_attrs<true>();
-    int m = stage_mode(g, f, zd);
+    int m = stage_mode(g, f, zd, KSpecies);
     if (m == 2 && !(make_map(&tm.y, f.y, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
                     make_map(&tm.rd, f.rd, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
                     make_map(&tm.h, f.h, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
@@ -869,7 +879,7 @@ void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk,
   RkMaps tm{};
   if (all_periodic(g)) {
     set_attrs<true>();
-    int m = stage_mode(g, f, zd);
+    int m = stage_mode(g, f, zd, KSpecies);
     if (m == 2 && !(make_map(&tm.y, f.y, g, nspec, SSlab::SX, SSlab::SY, SZ_) &&
                     make_map(&tm.hm, f.hmix, g, 1, SSlab::SX, SSlab::SY, SZ_)))
       m = 1;

@@ -1,7 +1,8 @@
-"""Stencil tiles filled by bulk copies on the TMA engine (all-periodic boxes
-of even nx; opt-in with SENGA_STAGE=bulk for row copies or SENGA_STAGE=tma
-for one tensor copy per buffer on tiles away from the wrap, which the
-library reads at every launch) against the oracle.
+"""The three ways of filling the stencil tiles of an all-periodic box of
+even nx against the oracle: per-element cp.async (SENGA_STAGE=cpasync), rows
+copied by the TMA engine (bulk), one tensor copy per buffer on tiles away
+from the wrap (tma); the library reads SENGA_STAGE at every launch, and by
+default fills flow's tiles by rows and the species kernels' by cp.async.
 
 Each staged row spans the tile's x range plus six points on either side; in a
 periodic box it is cut where x wraps, and a box narrower than one row wraps
@@ -22,7 +23,7 @@ CASES = [("h2_pool", (10, 12, 8)), ("h2_pool", (34, 9, 7)), ("h2_pool", (46, 12,
          ("h2_pool", (96, 40, 6)), ("ignition32", None)]
 
 
-@pytest.mark.parametrize("mode", ["bulk", "tma"])
+@pytest.mark.parametrize("mode", ["cpasync", "bulk", "tma"])
 @pytest.mark.parametrize("name,shape", CASES, ids=[f"{n}-{'x'.join(map(str, s)) if s else '20^3'}" for n, s in CASES])
 def test_bulk_staged_tiles_match_oracle(name, shape, mode, monkeypatch):
     monkeypatch.setenv("SENGA_STAGE", mode)
