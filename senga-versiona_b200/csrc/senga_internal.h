@@ -134,6 +134,10 @@ void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd = ZDec{});
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s,
                          const ZDec& zd = ZDec{});
+// species + RK update marching along z (kernels_zmarch.cu); false when the
+// box does not qualify (the caller then launches the tiled form)
+bool launch_species_b_rk_z(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s,
+                           const ZDec& zd);
 void launch_deriv(const Geo& g, int kind, const double* in, double* out, cudaStream_t s);
 // the same on a halo-extended input (5 points per side), interior output
 void launch_deriv_big(const Geo& g, int kind, const double* in, double* out, cudaStream_t s);
