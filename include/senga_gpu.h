@@ -254,6 +254,14 @@ int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
 
 /* NSCBC x faces (bounded x, NBOUND on both x faces; y, z periodic). xl and
  * xr each take one of the built kinds; inflow on one face at most.
+ * 12: I2 subsonic reflecting inflow with specified temperature (NSBCI2):
+ *   u = u_in (constant, NXxPRM(1)=1; negative through x-right), v = w = 0,
+ *   T = t_in (TRIN) and the mass fractions y_in imposed on the inflow plane
+ *   from its current density, which alone is integrated there (BOUNDT
+ *   src/boundt.f:81-176 left, 495- right; BOUNTT src/bountt.f:84-200 left,
+ *   590- right; ranges src/bcinit.f:458-480), its right-hand side corrected
+ *   by the wave amplitudes of BOUNDS (src/bounds.f:522-608 left, 1600-1684
+ *   right).
  * 13: I3 subsonic inflow with constant velocity (NXxPRM(1)=1): u = u_in
  *   (negative for inflow through x-right), v = w = 0, density rho_in (DRIN),
  *   mass fractions y_in (YRIN) imposed on the inflow plane (BOUNDT
@@ -277,6 +285,7 @@ typedef struct senga_nscbc {
   double y_in[SENGA_NSPCMX];
   double p_inf, sigma, eta;
   int pio, bet_local;
+  double t_in; /* I2: imposed inflow temperature TRIN [K] */
 } senga_nscbc;
 int senga_set_nscbc(senga_ctx* ctx, const senga_nscbc* bc);
 

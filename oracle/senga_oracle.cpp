@@ -565,9 +565,14 @@ struct Oracle {
   // (bounds.f:213-372 O1 left, 610-675 I3 left, 1296-1450 O1 right, 1688-
   // I3 right; boundt.f:177, 591; bountt.f:203, 709); y and z periodic. Both
   // O1 faces take the same outflow parameters.
-  static constexpr int BC_NONE = 0, BC_I3 = 13, BC_O1 = 21;
+  // Also I2, subsonic reflecting inflow with specified temperature (NSBCI2,
+  // bounds.f:522-608 x-left, 1600-1684 x-right; boundt.f:81-176, 495-; bountt.f:
+  // 84-200, 590-; ranges bcinit.f:458-480): u (BCUTXL NXLPRM(1)=1), T = TRIN
+  // (BCTTXL) and the mass fractions (BCYTXL) imposed from the face density,
+  // which alone is integrated.
+  static constexpr int BC_NONE = 0, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21;
   int bcxl = BC_NONE, bcxr = BC_NONE;
-  double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0;
+  double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0, tin = 0.0;
   int pio_xr = 0, betloc_xr = 0;
   bool fxlcnv = false, fxrcnv = false;
   int istald = 1, istalu = 1, istalv = 1, istalw = 1, istale = 1, istaly = 1;
@@ -598,10 +603,11 @@ struct Oracle {
     });
   }
   void set_bc(int xl, int xr, double u_in, double rho_in, const double* y_in, double p_inf, double sigma,
-              double eta, int pio, int betloc) {
-    auto ok = [](int k) { return k == BC_NONE || k == BC_I3 || k == BC_O1; };
-    if (!ok(xl) || !ok(xr) || (xl == BC_I3 && xr == BC_I3))
-      throw std::runtime_error("oracle: NSCBC restated for I3 and O1 x faces (not inflow on both)");
+              double eta, int pio, int betloc, double t_in = 0.0) {
+    auto ok = [](int k) { return k == BC_NONE || k == BC_I2 || k == BC_I3 || k == BC_O1; };
+    auto inflow = [](int k) { return k == BC_I2 || k == BC_I3; };
+    if (!ok(xl) || !ok(xr) || (inflow(xl) && inflow(xr)))
+      throw std::runtime_error("oracle: NSCBC restated for I2, I3 and O1 x faces (not inflow on both)");
     if ((xl != BC_NONE && nendxl != NBOUND) || (xr != BC_NONE && nendxr != NBOUND))
       throw std::runtime_error("oracle: NSCBC faces need NBOUND end conditions");
     bcxl = xl;
@@ -613,6 +619,7 @@ struct Oracle {
     cobcxr = sigma * (1.0 - eta) / (2.0 * cf.xgdlen);  // COBCXL/COBCXR, src/bcinit.f:309,324
     pio_xr = pio;
     betloc_xr = betloc;
+    tin = t_in;
     fxlcnv = xl != BC_NONE;
     fxrcnv = xr != BC_NONE;
     istold = istolu = istolv = istolw = istole = istoly = istol;
@@ -624,6 +631,8 @@ struct Oracle {
       fxrvsn = true;
       istold = istolu = istolv = istolw = istoly = istol - 1;
     }
+    if (xl == BC_I2) istalu = istalv = istalw = istale = istaly = istal + 1;  // src/bcinit.f:458-468: FXLCNV
+    if (xr == BC_I2) istolu = istolv = istolw = istole = istoly = istol - 1;  // src/bcinit.f:472-480: FXRCNV
     if (xl == BC_O1) fxlvst = fxlcon = fxladb = fxldif = true;  // src/bcinit.f:299-311
     if (xr == BC_O1) {  // FXRCNV, FXRVST, FXRCON, FXRADB, FXRDIF (src/bcinit.f:314-326)
       fxrvst = fxrcon = fxradb = fxrdif = true;
@@ -631,9 +640,65 @@ struct Oracle {
     fxl.init(ny * nz, nspec);
     fxr.init(ny * nz, nspec);
   }
+  // I2 face (boundt.f:81-176 / bountt.f:84-200): ITNDEX of TRIN, then the
+  // conserved velocity, energy and species from the current face density;
+  // both = BOUNTT (the S register too, their errors zeroed; the density and
+  // its error are left alone)
+  void impose_i2(bool both) {
+    const int ic = bcxl == BC_I2 ? istal : istol;
+    const double t = tin, u = uin, v = 0.0, w = 0.0;
+    for (int kc = kstal; kc <= kstol; ++kc)
+      for (int jc = jstal; jc <= jstol; ++jc) {
+        int itnew = 0;
+        for (int is = 1; is <= nspec; ++is) {
+          int itint = 1;
+          while (t > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
+          int pw = 1;
+          for (int qq = 0; qq < is - 1; ++qq) pw *= NTBASE;
+          itnew = itnew + (itint - 1) * pw;
+        }
+        itndex(ic, jc, kc) = itnew;
+        const double d = drhs(ic, jc, kc);
+        urhs(ic, jc, kc) = d * u;
+        vrhs(ic, jc, kc) = d * v;
+        wrhs(ic, jc, kc) = d * w;
+        double er = 0.5 * (u * u + v * v + w * w);
+        er = d * er;
+        for (int is = 1; is <= nspec; ++is) {
+          const int itint = 1 + (itnew / ipow(NTBASE, is - 1)) % NTBASE;
+          const int k2 = Chem::c2(itint, is);
+          double fornow = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
+          for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) fornow = fornow * t + ch.amasch[Chem::c3(icp, itint, is)];
+          fornow = ch.amasch[Chem::c3(ch.ncenth[k2], itint, is)] + fornow * t;
+          yrhs[is - 1](ic, jc, kc) = d * yin[is - 1];
+          er = er + (fornow - ch.rgspec[is - 1] * t) * yrhs[is - 1](ic, jc, kc);
+          if (both) {
+            yrun[is - 1](ic, jc, kc) = yrhs[is - 1](ic, jc, kc);
+            yerr[is - 1](ic, jc, kc) = 0.0;
+          }
+        }
+        erhs(ic, jc, kc) = er;
+        if (both) {
+          urun(ic, jc, kc) = urhs(ic, jc, kc);
+          vrun(ic, jc, kc) = vrhs(ic, jc, kc);
+          wrun(ic, jc, kc) = wrhs(ic, jc, kc);
+          erun(ic, jc, kc) = erhs(ic, jc, kc);
+          uerr(ic, jc, kc) = 0.0;
+          verr(ic, jc, kc) = 0.0;
+          werr(ic, jc, kc) = 0.0;
+          eerr(ic, jc, kc) = 0.0;
+        }
+      }
+  }
+  static int ipow(int b, int e) {
+    int r = 1;
+    for (int k = 0; k < e; ++k) r *= b;
+    return r;
+  }
   // BOUNDT, I3 at x-left: impose the inflow state on the U register (DRHS..YRHS
   // at ISTAL; src/boundt.f:177-200 with BCDTXL, BCUTXL NXLPRM(1)=1, BCYTXL)
   void boundt() {
+    if (bcxl == BC_I2 || bcxr == BC_I2) impose_i2(false);
     if (bcxl != BC_I3 && bcxr != BC_I3) return;
     const int ic = bcxl == BC_I3 ? istal : istol;  // boundt.f:177 (x-left), 591 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
@@ -648,6 +713,7 @@ struct Oracle {
   // BOUNTT, I3 at x-left: both registers at ISTAL set to the inflow state, its
   // error zeroed (src/bountt.f:203-252)
   void bountt() {
+    if (bcxl == BC_I2 || bcxr == BC_I2) impose_i2(true);
     if (bcxl != BC_I3 && bcxr != BC_I3) return;
     const int ic = bcxl == BC_I3 ? istal : istol;  // bountt.f:203 (x-left), 709 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
@@ -728,6 +794,39 @@ struct Oracle {
             erhs(istal, jc, kc) = erhs(istal, jc, kc) - bcly * F.d[q] * F.h[qs];
           }
     }
+    // I2 (bounds.f:522-608 x-left, 1600-1684 x-right): u, T, Y imposed with
+    // zero time derivatives (DUDT = DTDT = DYDT = 0); only DRHS is corrected
+    auto i2 = [&](Face& F, bool left) {
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      std::vector<double> sydt(m, 0.0), sorp(m, 0.0);
+      for (int is = 0; is < nspec; ++is)
+        for (int q = 0; q < m; ++q) {
+          sydt[q] = sydt[q] + 0.0 * ch.rgspec[is];
+          sorp[q] = sorp[q] + F.h[is * m + q] * F.rate[is * m + q];
+        }
+      for (int q = 0; q < m; ++q) {
+        sydt[q] = sydt[q] / F.r[q];
+        sorp[q] = -sorp[q] * gam1[q];
+      }
+      const int ic = left ? istal : istol;
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          const double fornow = F.d[q] * acou[q] * F.bcl1[q];
+          double bcl1 = 0.5 * (F.u[q] - acou[q]) * (F.bcl5[q] - fornow);
+          double bcl2 = F.u[q] * (F.bcl2[q] - F.bcl5[q] * ova2[q]);
+          double bcl5 = 0.5 * (F.u[q] + acou[q]) * (F.bcl5[q] + fornow);
+          if (left) {  // L1 unchanged
+            bcl5 = bcl1 - F.d[q] * acou[q] * 0.0 - bcl5;
+          } else {  // L5 unchanged
+            bcl1 = bcl5 + F.d[q] * acou[q] * 0.0 - bcl1;
+          }
+          bcl2 = gam1[q] * ova2[q] * (bcl1 + bcl5) + F.d[q] * (0.0 / F.t[q] - sorp[q] / F.p[q] + sydt[q]) - bcl2;
+          drhs(ic, jc, kc) = drhs(ic, jc, kc) - bcl2 - (left ? bcl5 : bcl1) * ova2[q];
+        }
+    };
+    if (bcxl == BC_I2) i2(fxl, true);
+    if (bcxr == BC_I2) i2(fxr, false);
     if (bcxl == BC_O1) {  // bounds.f:213-372: L5 (entering from the left) relaxed
       Face& F = fxl;
       prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
@@ -2326,11 +2425,12 @@ struct oracle_bc {
   double y_in[9];
   double p_inf, sigma, eta;
   int pio, bet_local;
+  double t_in;
 };
 int oracle_set_bc(void* h, const oracle_bc* b) {
   try {
     static_cast<orc::Oracle*>(h)->set_bc(b->xl, b->xr, b->u_in, b->rho_in, b->y_in, b->p_inf, b->sigma, b->eta, b->pio,
-                                         b->bet_local);
+                                         b->bet_local, b->t_in);
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

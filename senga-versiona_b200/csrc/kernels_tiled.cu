@@ -602,6 +602,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
       return;
     }
     if (!P && (bf & BF_IMPOSED) && fld != 4) return;
+    if (!P && (bf & BF_IMPOSED_D) && fld != 0) return;
     if (f.err) f.err[idx] = f.err[idx] + rk.err * R;
     if (!rk.last) {
       const double s = f.run[idx];

@@ -1,8 +1,9 @@
 // Navier-Stokes characteristic boundary conditions on the x faces.
 //
 // Restated from the reference (I3 subsonic inflow with constant velocity,
-// NXxPRM(1)=1, and O1 partially non-reflecting outflow, on either x face;
-// inflow on one face at most; both O1 faces take the same parameters):
+// NXxPRM(1)=1, I2 subsonic reflecting inflow with specified temperature,
+// and O1 partially non-reflecting outflow, on either x face; inflow on one
+// face at most; both O1 faces take the same parameters):
 //   BOUNDT  src/boundt.f:177-200 (x-left), 591- (x-right)   impose the
 //           inflow state on the U register
 //   face data gathered inside RHSCAL/RHSVEL (src/rhscal.f:70-90,159-180,
@@ -53,14 +54,55 @@ __device__ __forceinline__ double dd_sub(const Geo& g, const double* a, double c
   return d1core([&](int m) { return at<DIR>(g, a, i, j, k, m) - c0; }, c, n, g.per[DIR]) * g.ovd[DIR];
 }
 
-__global__ void __launch_bounds__(kFaceBlock) k_boundt(Geo g, Fields f, NscbcParams bc, int nspec, int both) {
+__global__ void __launch_bounds__(kFaceBlock)
+    k_boundt(Geo g, Fields f, NscbcParams bc, int nspec, int both, const senga_chem* chem) {
   const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
   if (jk >= g.ny * g.nz) return;
   const int64_t n = g.n;
-  const int i = bc.xl == 13 ? 0 : g.nx - 1;  // the inflow plane
+  const bool left = bc.xl == 13 || bc.xl == 12;
+  const int kind = left ? bc.xl : bc.xr;
+  const int i = left ? 0 : g.nx - 1;  // the inflow plane
   const int64_t q = (int64_t)i + (int64_t)g.nx * jk;
-  const double r = bc.rho_in;
   double* regs[2] = {f.uin, f.run};
+  if (kind == 12) {
+    // I2 (boundt.f:81-176, bountt.f:84-200): ITNDEX of TRIN, then velocity,
+    // energy and species from the face density of the U register
+    const double t = bc.t_in, u = bc.u_in, v = 0.0, w = 0.0;
+    int32_t itn = 0;
+    for (int s = 0; s < nspec; ++s) {
+      int it = 0;
+      while (t > chem->tinthi[s][it] && it + 1 < chem->ntint[s]) ++it;
+      itn += it << (2 * s);
+    }
+    f.itn[q] = itn;
+    const double d = f.uin[q];
+    double e = 0.5 * (u * u + v * v + w * w);
+    e = d * e;
+    double ys[SENGA_NSPCMX];
+    for (int s = 0; s < nspec; ++s) {
+      const int it = (itn >> (2 * s)) & 3;
+      const double* c = chem->amasch[s][it];
+      double h = c[chem->ncpoly[s][it] - 1];
+      for (int icp = chem->ncpom1[s][it]; icp >= 1; --icp) h = h * t + c[icp - 1];
+      h = c[chem->ncenth[s][it] - 1] + h * t;
+      ys[s] = d * bc.y_in[s];
+      e = e + (h - chem->rgspec[s] * t) * ys[s];
+    }
+    for (int r = 0; r < (both ? 2 : 1); ++r) {
+      double* U = regs[r];
+      U[n + q] = d * u;
+      U[2 * n + q] = d * v;
+      U[3 * n + q] = d * w;
+      U[4 * n + q] = e;
+      for (int s = 0; s < nspec; ++s) U[(5 + s) * n + q] = ys[s];
+    }
+    if (both && f.err) {  // BOUNTT: error of the imposed fields zeroed (not the density's)
+      for (int fl = 1; fl < 5; ++fl) f.err[fl * n + q] = 0.0;
+      for (int s = 0; s < nspec; ++s) f.err[(5 + s) * n + q] = 0.0;
+    }
+    return;
+  }
+  const double r = bc.rho_in;
   for (int w = 0; w < (both ? 2 : 1); ++w) {
     double* U = regs[w];
     U[q] = r;
@@ -111,7 +153,23 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
   double* corr = f.face + (int64_t)side * nc * nyz + jk;
   for (int fl = 0; fl < nc; ++fl) corr[(int64_t)fl * nyz] = 0.0;
   auto hprime = [&](int s) { return f.h[s * n + q] - cp * t * chem->rgspec[s] / rr; };
-  if (kind == 13 && side == 1) {  // I3 inflow at x-right (bounds.f:1688-): L1 enters
+  if (kind == 12) {  // I2 inflow (bounds.f:522-608 left, 1600-1684 right): u, T, Y imposed, DRHS corrected
+    double sydt = 0.0, sorp = 0.0;
+    for (int s = 0; s < nspec; ++s) {
+      sydt = sydt + 0.0 * chem->rgspec[s];
+      sorp = sorp + hprime(s) * f.wdot[s * n + q];
+    }
+    sydt = sydt / rr;
+    sorp = -sorp * gam1;
+    const double fornow = d * acou * bcl1;
+    double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
+    double b2 = u * (bcl2 - bcl5 * ova2);
+    double b5 = 0.5 * (u + acou) * (bcl5 + fornow);
+    if (side == 0) b5 = b1 - d * acou * 0.0 - b5;  // L1 unchanged
+    else b1 = b5 + d * acou * 0.0 - b1;            // L5 unchanged
+    b2 = gam1 * ova2 * (b1 + b5) + d * (0.0 / t - sorp / p + sydt) - b2;
+    corr[0] = -b2 - (side == 0 ? b5 : b1) * ova2;
+  } else if (kind == 13 && side == 1) {  // I3 inflow at x-right (bounds.f:1688-): L1 enters
     double fornow = d * acou * bcl1;
     double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
     double b2 = u * (bcl2 - bcl5 * ova2);
@@ -228,10 +286,11 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
 
 }  // namespace
 
-void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both, cudaStream_t s) {
-  if (bc.xl != 13 && bc.xr != 13) return;
+void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both,
+                   const senga_chem* dchem, cudaStream_t s) {
+  if (bc.xl != 13 && bc.xr != 13 && bc.xl != 12 && bc.xr != 12) return;
   const int nyz = g.ny * g.nz;
-  k_boundt<<<(nyz + kFaceBlock - 1) / kFaceBlock, kFaceBlock, 0, s>>>(g, f, bc, nspec, both ? 1 : 0);
+  k_boundt<<<(nyz + kFaceBlock - 1) / kFaceBlock, kFaceBlock, 0, s>>>(g, f, bc, nspec, both ? 1 : 0, dchem);
 }
 
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,

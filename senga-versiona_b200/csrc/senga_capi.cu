@@ -143,7 +143,7 @@ void require_rhs(const senga_ctx* c) {
 
 void run_rhs(senga_ctx* c) {
   require_rhs(c);
-  if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->stream);  // BOUNDT
+  if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->d_chem, c->stream);  // BOUNDT
   launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
   if (c->rrte)  // RRTE = RATE (src/rhscal.f:828)
     CK(cudaMemcpyAsync(c->rrte, c->f.wdot, (size_t)c->nspec * c->geo.n * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -381,7 +381,7 @@ int senga_step(senga_ctx* c, int nsteps) {
   return guard([&] {
     for (int s = 0; s < nsteps; ++s) {
       for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
-      if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->stream);  // BOUNTT
+      if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->d_chem, c->stream);  // BOUNTT
       if (c->cfg.adaptive) adaptt(c);
     }
     CK(cudaGetLastError());
@@ -397,7 +397,7 @@ int senga_step_graph(senga_ctx* c, int nsteps) {
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
-      if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->stream);  // BOUNTT
+      if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->d_chem, c->stream);  // BOUNTT
       CK(cudaStreamEndCapture(c->stream, &gr));
       CK(cudaGraphInstantiate(&c->graph, gr, 0));
       CK(cudaGraphDestroy(gr));
@@ -695,10 +695,13 @@ int senga_set_radiation(senga_ctx* c, const senga_radn* r) {
 
 int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
   if (!c || !b) return fail(SENGA_ERR_ARG, "senga_set_nscbc: null argument");
-  auto kind_ok = [](int k) { return k == 13 || k == 21; };
-  if (!kind_ok(b->xl) || !kind_ok(b->xr) || (b->xl == 13 && b->xr == 13))
-    return fail(SENGA_ERR_UNSUPPORTED,
-                "senga_set_nscbc: built face kinds are I3 (13) and O1 (21) on either x face, inflow on one at most");
+  auto kind_ok = [](int k) { return k == 12 || k == 13 || k == 21; };
+  auto inflow = [](int k) { return k == 12 || k == 13; };
+  if (!kind_ok(b->xl) || !kind_ok(b->xr) || (inflow(b->xl) && inflow(b->xr)))
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I2 (12), I3 (13) and O1 (21) on either "
+                                       "x face, inflow on one at most");
+  if ((b->xl == 12 || b->xr == 12) && !(b->t_in > 0.0))
+    return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I2 inflow needs t_in > 0");
   if (c->geo.per[0] || b->xl == 0 || b->xr == 0)
     return fail(SENGA_ERR_ARG, "senga_set_nscbc: needs a bounded x direction and a kind on both x faces");
   if (b->rho_in <= 0.0 || b->p_inf <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: rho_in and p_inf must be > 0");
@@ -716,10 +719,14 @@ int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
     p.xlen = c->cfg.xgdlen;
     p.pio = b->pio;
     p.betloc = b->bet_local;
-    // face-plane flags of src/bcinit.f:299-326,560-586: I3 -> FxxCNV,
-    // FxxVSN, the plane imposed; O1 -> FxxCNV, FxxVST, FxxCON, FxxADB, FxxDIF
+    p.t_in = b->t_in;
+    // face-plane flags of src/bcinit.f:299-326,458-480,560-586: I3 -> FxxCNV,
+    // FxxVSN, the plane imposed; I2 -> FxxCNV, all but the density imposed;
+    // O1 -> FxxCNV, FxxVST, FxxCON, FxxADB, FxxDIF
     auto bits = [](int kind) {
-      return kind == 13 ? (BF_VSN | BF_NSCBC | BF_IMPOSED) : (BF_VST | BF_CON | BF_DIF | BF_NSCBC);
+      return kind == 13   ? (BF_VSN | BF_NSCBC | BF_IMPOSED)
+             : kind == 12 ? (BF_NSCBC | BF_IMPOSED_D)
+                          : (BF_VST | BF_CON | BF_DIF | BF_NSCBC);
     };
     c->geo.bxl = bits(b->xl);
     c->geo.bxr = bits(b->xr);

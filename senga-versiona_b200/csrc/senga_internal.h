@@ -56,6 +56,7 @@ enum : int {
   BF_DIF = 8,       // FxxDIF and FxxADB: species diffusion and its enthalpy flux
   BF_NSCBC = 16,    // BOUNDS corrections are added to the plane's RHS
   BF_IMPOSED = 32,  // I3 inflow: D, U, V, W, Y are imposed, not integrated
+  BF_IMPOSED_D = 64,  // I2 inflow: U, V, W, E, Y are imposed, only D integrated
 };
 __host__ __device__ __forceinline__ int face_bits(const Geo& g, int gx) {
   return gx == 0 ? g.bxl : (gx == g.nx - 1 ? g.bxr : 0);
@@ -151,16 +152,18 @@ void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchu
 // work item; `phase` selects one of them (0, 1, 2) or all three (-1).
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
-// NSCBC x faces (nscbc.cu): face kinds 0 (none), 13 (I3 inflow, x-left),
-// 21 (O1 outflow, x-right) and their parameters.
+// NSCBC x faces (nscbc.cu): face kinds 0 (none), 12 (I2 inflow), 13 (I3
+// inflow), 21 (O1 outflow) on either face, and their parameters.
 struct NscbcParams {
   int xl, xr;
   double u_in, rho_in, y_in[SENGA_NSPCMX];  // I3: RXLPRM(1), DRIN, YRIN
+  double t_in;                              // I2: TRIN
   double p_inf, cobc, bet, xlen;            // O1: PINFXR, COBCXR, BET, XGDLEN
   int pio, betloc;                          // O1: NXRPRM(1), NXRPRM(2)
 };
 // BOUNDT (both = false) or BOUNTT (both = true: U and S registers, error zeroed)
-void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both, cudaStream_t s);
+void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both,
+                   const senga_chem* dchem, cudaStream_t s);
 // face data + BOUNDS corrections into f.face, after the thermochemistry kernel
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,
                  cudaStream_t s);

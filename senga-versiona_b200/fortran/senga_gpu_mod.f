@@ -89,13 +89,15 @@ C     RADCIN's radiation tables (src/radcin.f:80-220)
         REAL(C_DOUBLE) :: AKPRAD(SNCFRM, SNSPCM)
         REAL(C_DOUBLE) :: TREFRN
       END TYPE
-C     NSCBC x faces: kinds 13 (I3 inflow) / 21 (O1 outflow) and parameters
+C     NSCBC x faces: kinds 12 (I2 inflow), 13 (I3 inflow), 21 (O1
+C     outflow) and parameters (T_IN: TRIN of an I2 inflow)
       TYPE, BIND(C) :: SENGA_NSCBC
         INTEGER(C_INT) :: XL, XR
         REAL(C_DOUBLE) :: U_IN, RHO_IN
         REAL(C_DOUBLE) :: Y_IN(SNSPCM)
         REAL(C_DOUBLE) :: P_INF, SIGMA, ETA
         INTEGER(C_INT) :: PIO, BET_LOCAL
+        REAL(C_DOUBLE) :: T_IN
       END TYPE
       INTERFACE
         INTEGER(C_INT) FUNCTION SENGA_CHEM_LOAD(PATH, CHEM)

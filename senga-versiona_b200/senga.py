@@ -93,11 +93,11 @@ class ConfigT(C.Structure):
 
 
 class NscbcT(C.Structure):
-    """senga_nscbc: I3 inflow (x-left) / O1 outflow (x-right) parameters."""
+    """senga_nscbc: x-face kinds (12 I2 inflow, 13 I3 inflow, 21 O1 outflow) and parameters."""
 
     _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
                 ("y_in", C.c_double * NSPCMX), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
-                ("pio", C.c_int), ("bet_local", C.c_int)]
+                ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double)]
 
 
 NCFRMX = 6
@@ -542,6 +542,7 @@ class Box:
             b.y_in[i] = v
         b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
+        b.t_in = bc.get("t_in", 0.0)
         _check(lib.senga_set_nscbc(self.h, C.byref(b)), "senga_set_nscbc")
 
     def set_transport(self, mixw=False, mixp=False, soret=False, dufour=False, wmltdr=5.0):
