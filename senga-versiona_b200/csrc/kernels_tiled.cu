@@ -42,9 +42,8 @@ using FYRow = YRow<FX, FY, FZ>;
 using FZCol = ZCol<FX, FY, FZ>;
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
-constexpr int kFlowSmem =
-    cmax(cmax(FXRow::SIZE + FYRow::SIZE + FZCol::SIZE + FStar::SIZE, 2 * FStar::SIZE),
-         cmax(cmax(FStar::SIZE + 4 * FXRow::SIZE + 4 * FYRow::SIZE, 4 * FZCol::SIZE), FStar::SIZE + FBox::SIZE));
+constexpr int kFlowSmem = cmax(cmax(FXRow::SIZE + FYRow::SIZE + FZCol::SIZE + FStar::SIZE, 2 * FStar::SIZE),
+                                cmax(3 * FXRow::SIZE + 3 * FYRow::SIZE, FStar::SIZE + FBox::SIZE));
 
 using SSlab = Slab<SX_, SY_, SZ_>;
 using SXRow = XRow<SX_, SY_, SZ_>;
@@ -147,64 +146,71 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     }
     tile_sync();
   }
-  // ---- phase 3: pressure gradient (of p - p(1,1,1)), pressure work and the
-  // x and y momentum fluxes d/dx_j (rho u_i u_j) ----
-  // Raw fields are staged and the products formed where read (the product,
-  // then the differences: the same arithmetic as staging the products);
-  // p(1,1,1) is subtracted where p is read (the same subtraction as staging
-  // p - p(1,1,1)). Each flux is summed x, y, z in that order.
-  double S4[FZ], S5[FZ], S6[FZ];
+  // ---- phase 3: pressure gradient (of p - p(1,1,1)) and pressure work ----
   {
     const FStar bPr{sm};
-    double* const s1 = sm + FStar::SIZE;
-    const FXRow xru{s1}, xu{s1 + FXRow::SIZE}, xv{s1 + 2 * FXRow::SIZE}, xw{s1 + 3 * FXRow::SIZE};
-    double* const s2 = s1 + 4 * FXRow::SIZE;
-    const FYRow yru{s2}, yrv{s2 + FYRow::SIZE}, yv{s2 + 2 * FYRow::SIZE}, yw{s2 + 3 * FYRow::SIZE};
-    stage_plain<B, FNW>(bPr, fo, g, o, f.p, bar);
-    stage_plain<B, FNW>(xru, fo, g, o, U + n, bar);
-    stage_plain<B, FNW>(xu, fo, g, o, f.vel, bar);
-    stage_plain<B, FNW>(xv, fo, g, o, f.vel + n, bar);
-    stage_plain<B, FNW>(xw, fo, g, o, f.vel + 2 * n, bar);
-    stage_plain<B, FNW>(yru, fo, g, o, U + n, bar);
-    stage_plain<B, FNW>(yrv, fo, g, o, U + 2 * n, bar);
-    stage_plain<B, FNW>(yv, fo, g, o, f.vel + n, bar);
-    stage_plain<B, FNW>(yw, fo, g, o, f.vel + 2 * n, bar);
     const double p111 = __ldg(f.p + zd.base[0]);  // p(1,1,1) lives in slab 0
-    if (sync_staged<B>(bb, FStar::kBulkBytes + 4 * FXRow::kBulkBytes + 4 * FYRow::kBulkBytes, f.status)) return;
-    const Shifted<FStar> bP{bPr, p111};
+    auto phase3 = [&](const auto& bP) {
 #pragma unroll
-    for (int z = 0; z < FZ; ++z) {
-      const TP& t = tp[z];
-      const double px = d1<0, P>(g, t, bP), py = d1<1, P>(g, t, bP), pz = d1<2, P>(g, t, bP);
-      rU[z] = -px;
-      rV[z] = -py;
-      rW[z] = -pz;
-      rE[z] = rE[z] - xu.v(t.x, t.y, t.z) * px - xv.v(t.x, t.y, t.z) * py - xw.v(t.x, t.y, t.z) * pz;
-      S4[z] = d1p<0, P>(g, t, xru, xu);  // rho u u
-      S5[z] = d1p<0, P>(g, t, xru, xv);  // rho u v
-      S6[z] = d1p<0, P>(g, t, xru, xw);  // rho u w
-      S4[z] = S4[z] + d1p<1, P>(g, t, yru, yv);  // rho u v
-      S5[z] = S5[z] + d1p<1, P>(g, t, yrv, yv);  // rho v v
-      S6[z] = S6[z] + d1p<1, P>(g, t, yrv, yw);  // rho v w
+      for (int z = 0; z < FZ; ++z) {
+        const TP& t = tp[z];
+        const double px = d1<0, P>(g, t, bP), py = d1<1, P>(g, t, bP), pz = d1<2, P>(g, t, bP);
+        rU[z] = -px;
+        rV[z] = -py;
+        rW[z] = -pz;
+        rE[z] = rE[z] - __ldg(f.vel + t.q) * px - __ldg(f.vel + n + t.q) * py - __ldg(f.vel + 2 * n + t.q) * pz;
+      }
+    };
+    if constexpr (B) {
+      // raw p by bulk copies, p(1,1,1) subtracted where read: the same
+      // subtraction as staging p - p(1,1,1), so the same values
+      bPr.stage_bulk(fo, o.x0, g.nx, f.p, bar);
+      if (bb.wait(FStar::kBulkBytes, f.status)) return;
+      phase3(Shifted<FStar>{bPr, p111});
+    } else {
+      bPr.stage<FNW>(fo, LdSub{f.p, p111});
+      tile_sync();
+      phase3(bPr);
     }
     tile_sync();
   }
-  // ---- phase 4: z momentum fluxes ----
+  // ---- phase 4: momentum fluxes d/dx_j (rho u_i u_j) ----
+  // x and y derivatives from products staged in x rows and y rows, z
+  // derivatives from products of register z-columns; each flux summed x, y,
+  // z in that order
+  double S4[FZ], S5[FZ], S6[FZ];
   {
-    const FZCol zru{sm}, zrv{sm + FZCol::SIZE}, zrw{sm + 2 * FZCol::SIZE}, zw{sm + 3 * FZCol::SIZE};
-    stage_plain<B, FNW>(zru, fo, g, o, U + n, bar);
-    stage_plain<B, FNW>(zrv, fo, g, o, U + 2 * n, bar);
-    stage_plain<B, FNW>(zrw, fo, g, o, U + 3 * n, bar);
-    stage_plain<B, FNW>(zw, fo, g, o, f.vel + 2 * n, bar);
-    if (sync_staged<B>(bb, 4 * FZCol::kBulkBytes, f.status)) return;
+    const FXRow xA{sm}, xB{sm + FXRow::SIZE}, xC{sm + 2 * FXRow::SIZE};
+    double* const sy = sm + 3 * FXRow::SIZE;
+    const FYRow yA{sy}, yB{sy + FYRow::SIZE}, yC{sy + 2 * FYRow::SIZE};
+    xA.stage<FNW>(fo, LdMul{U + n, f.vel});               // rho u u
+    xB.stage<FNW>(fo, LdMul{U + n, f.vel + n});           // rho u v
+    xC.stage<FNW>(fo, LdMul{U + n, f.vel + 2 * n});       // rho u w
+    yA.stage<FNW>(fo, LdMul{U + n, f.vel + n});           // rho u v
+    yB.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + n});       // rho v v
+    yC.stage<FNW>(fo, LdMul{U + 2 * n, f.vel + 2 * n});   // rho v w
+    Column<FZ> cw, cm;
+    cw.load(fo, tx, ty, Ld{f.vel + 2 * n});
+    cm.load(fo, tx, ty, Ld{U + n});
+    tile_sync();
 #pragma unroll
     for (int z = 0; z < FZ; ++z) {
       const TP& t = tp[z];
-      S4[z] = S4[z] + d1p<2, P>(g, t, zru, zw);  // rho u w
-      S5[z] = S5[z] + d1p<2, P>(g, t, zrv, zw);  // rho v w
-      S6[z] = S6[z] + d1p<2, P>(g, t, zrw, zw);  // rho w w
+      S4[z] = d1<0, P>(g, t, xA);
+      S5[z] = d1<0, P>(g, t, xB);
+      S6[z] = d1<0, P>(g, t, xC);
+      S4[z] = S4[z] + d1<1, P>(g, t, yA);
+      S5[z] = S5[z] + d1<1, P>(g, t, yB);
+      S6[z] = S6[z] + d1<1, P>(g, t, yC);
+      S4[z] = S4[z] + d1zp<P>(g, t, cm, cw);  // rho u w
     }
-    tile_sync();
+    cm.load(fo, tx, ty, Ld{U + 2 * n});
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) S5[z] = S5[z] + d1zp<P>(g, tp[z], cm, cw);  // rho v w
+    cm.load(fo, tx, ty, Ld{U + 3 * n});
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) S6[z] = S6[z] + d1zp<P>(g, tp[z], cm, cw);  // rho w w
+    tile_sync_async();
   }
   // ---- phase 5: velocity derivatives, viscous stresses and work ----
   const FStar bM{sm};
