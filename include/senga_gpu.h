@@ -275,8 +275,23 @@ int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
  *   src/bounds.f:213-372 left, 1296-1450 right; viscous shear, conduction
  *   and diffusion zeroed on the plane (FxxVST, FxxCON, FxxDIF, FxxADB). Two
  *   O1 faces share these parameters.
+ * 31: W1 adiabatic no-slip wall (NSBCW1), on either or both faces, no
+ *   parameters: the wall temperature is the zero-gradient extrapolation
+ *   (48 T1 - 36 T2 + 16 T3 - 3 T4)/25 of the four planes inward, momentum
+ *   is zero and rho E the internal energy at that temperature (BOUNDT
+ *   src/boundt.f:243-356 left, 657-768 right; BOUNTT src/bountt.f:290-428,
+ *   767-); the density and species right-hand sides take the reflected
+ *   wave of BOUNDS (src/bounds.f:917-1056, 1833-1974), momentum and energy
+ *   right-hand sides are zero; the wall diffusion flux enters the species
+ *   rates (src/rhscal.f:1698-1760); after each RK update every wall mass
+ *   fraction is the clipped zero-gradient extrapolation of the updated
+ *   state (src/lincom.f:171-210, src/fincom.f:171-210). Conduction and
+ *   diffusion are zeroed on the plane (FxxCON, FxxDIF, FxxADB). The wall
+ *   runs with the base transport: with senga_set_transport switches on,
+ *   either call returns SENGA_ERR_UNSUPPORTED.
  * Face data and wave amplitudes are computed after the thermochemistry
  * kernel and added to the face planes' right-hand side in the RK epilogue.
+ * rho_in must be > 0 with an I3 face, p_inf > 0 with an O1 face.
  * Other face kinds return SENGA_ERR_UNSUPPORTED. Stepping a box with a
  * bounded x direction needs this call first. */
 typedef struct senga_nscbc {

@@ -186,8 +186,8 @@ class Oracle:
         return out
 
     def set_bc(self, bc):
-        """NSCBC x faces: bc = dict(xl, xr in {0, 12, 13, 21}, u_in, rho_in, y_in, p_inf,
-        sigma, eta, pio=0, bet_local=0, t_in (I2))."""
+        """NSCBC x faces: bc = dict(xl, xr in {0, 12, 13, 21, 31}, u_in, rho_in, y_in, p_inf,
+        sigma, eta, pio=0, bet_local=0, t_in (I2)); 31 is the W1 wall."""
         b = _Bc()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
         b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)

@@ -570,11 +570,20 @@ struct Oracle {
   // 84-200, 590-; ranges bcinit.f:458-480): u (BCUTXL NXLPRM(1)=1), T = TRIN
   // (BCTTXL) and the mass fractions (BCYTXL) imposed from the face density,
   // which alone is integrated.
-  static constexpr int BC_NONE = 0, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21;
+  // And W1, the adiabatic no-slip wall (NSBCW1; flags and ranges bcinit.f:
+  // 702-735, wall state boundt.f:243-356 x-left, 657-768 x-right; bountt.f:
+  // 290-428, 767-; wave amplitudes bounds.f:917-1056, 1833-1974; the wall
+  // flux terms FxxCNW rhscal.f:610-660 and FxxDFW rhscal.f:1698-1760; the
+  // zero-gradient mass fractions of lincom.f:171-210, fincom.f:171-210), on
+  // either or both x faces, with the base transport (the molar-mass,
+  // pressure and thermal-diffusion branches carry wall terms of their own
+  // that are not restated).
+  static constexpr int BC_NONE = 0, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21, BC_W1 = 31;
   int bcxl = BC_NONE, bcxr = BC_NONE;
   double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0, tin = 0.0;
   int pio_xr = 0, betloc_xr = 0;
   bool fxlcnv = false, fxrcnv = false;
+  bool fxlcnw = false, fxrcnw = false, fxldfw = false, fxrdfw = false;
   int istald = 1, istalu = 1, istalv = 1, istalw = 1, istale = 1, istaly = 1;
   int istold = 0, istolu = 0, istolv = 0, istolw = 0, istole = 0, istoly = 0;
   struct Face {
@@ -604,10 +613,12 @@ struct Oracle {
   }
   void set_bc(int xl, int xr, double u_in, double rho_in, const double* y_in, double p_inf, double sigma,
               double eta, int pio, int betloc, double t_in = 0.0) {
-    auto ok = [](int k) { return k == BC_NONE || k == BC_I2 || k == BC_I3 || k == BC_O1; };
+    auto ok = [](int k) { return k == BC_NONE || k == BC_I2 || k == BC_I3 || k == BC_O1 || k == BC_W1; };
     auto inflow = [](int k) { return k == BC_I2 || k == BC_I3; };
     if (!ok(xl) || !ok(xr) || (inflow(xl) && inflow(xr)))
-      throw std::runtime_error("oracle: NSCBC restated for I2, I3 and O1 x faces (not inflow on both)");
+      throw std::runtime_error("oracle: NSCBC restated for I2, I3, O1 and W1 x faces (not inflow on both)");
+    if ((xl == BC_W1 || xr == BC_W1) && (df.flmixw || df.flmixp || df.flmixt))
+      throw std::runtime_error("oracle: W1 walls restated for the base transport only");
     if ((xl != BC_NONE && nendxl != NBOUND) || (xr != BC_NONE && nendxr != NBOUND))
       throw std::runtime_error("oracle: NSCBC faces need NBOUND end conditions");
     bcxl = xl;
@@ -636,6 +647,14 @@ struct Oracle {
     if (xl == BC_O1) fxlvst = fxlcon = fxladb = fxldif = true;  // src/bcinit.f:299-311
     if (xr == BC_O1) {  // FXRCNV, FXRVST, FXRCON, FXRADB, FXRDIF (src/bcinit.f:314-326)
       fxrvst = fxrcon = fxradb = fxrdif = true;
+    }
+    if (xl == BC_W1) {  // src/bcinit.f:702-717: FXLCON FXLADB FXLDIF FXLCNW FXLDFW; U,V,W from ISTAP1
+      fxlcon = fxladb = fxldif = fxlcnw = fxldfw = true;
+      istalu = istalv = istalw = istal + 1;
+    }
+    if (xr == BC_W1) {  // src/bcinit.f:721-735: the same on the right; U,V,W to ISTOM1
+      fxrcon = fxradb = fxrdif = fxrcnw = fxrdfw = true;
+      istolu = istolv = istolw = istol - 1;
     }
     fxl.init(ny * nz, nspec);
     fxr.init(ny * nz, nspec);
@@ -695,10 +714,101 @@ struct Oracle {
     for (int k = 0; k < e; ++k) r *= b;
     return r;
   }
+  // ITNDEX of one temperature (the interval search of boundt.f:262-290)
+  int interval_of(double t) const {
+    int itnew = 0;
+    for (int is = 1; is <= nspec; ++is) {
+      int itint = 1;
+      while (t > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
+      itnew = itnew + (itint - 1) * ipow(NTBASE, is - 1);
+    }
+    return itnew;
+  }
+  // W1 wall temperature: T_w = (48 T_1 - 36 T_2 + 16 T_3 - 3 T_4)/25 over the
+  // four planes inward of the wall (zero normal gradient to fourth order;
+  // boundt.f:252-260, bounds.f:925-933, bountt.f:307-315; BOUNDS and BOUNTT
+  // at x-left read plane 5 for ISTAL+4, the same plane on a single rank)
+  double wall_t(int ic, int st, int jc, int kc) {
+    return (48.0 * trun(ic + st, jc, kc) - 36.0 * trun(ic + 2 * st, jc, kc) + 16.0 * trun(ic + 3 * st, jc, kc) -
+            3.0 * trun(ic + 4 * st, jc, kc)) /
+           25.0;
+  }
+  // W1 wall plane (boundt.f:243-356 / 657-768): T extrapolated, its ITNDEX,
+  // zero momentum and rho E = sum_k (h_k(T) - R_k T) rho Y_k on the U
+  // register; both = BOUNTT (bountt.f:290-428 / 767-): the S register's
+  // momentum and energy too, their errors zeroed
+  void impose_w1(bool left, bool both) {
+    const int ic = left ? istal : istol, st = left ? 1 : -1;
+    for (int kc = kstal; kc <= kstol; ++kc)
+      for (int jc = jstal; jc <= jstol; ++jc) {
+        const double t = wall_t(ic, st, jc, kc);
+        trun(ic, jc, kc) = t;
+        const int itnew = interval_of(t);
+        itndex(ic, jc, kc) = itnew;
+        urhs(ic, jc, kc) = 0.0;
+        vrhs(ic, jc, kc) = 0.0;
+        wrhs(ic, jc, kc) = 0.0;
+        double er = 0.0;
+        er = drhs(ic, jc, kc) * er;
+        for (int is = 1; is <= nspec; ++is) {
+          const int itint = 1 + (itnew / ipow(NTBASE, is - 1)) % NTBASE;
+          const int k2 = Chem::c2(itint, is);
+          double fornow = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
+          for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) fornow = fornow * t + ch.amasch[Chem::c3(icp, itint, is)];
+          fornow = ch.amasch[Chem::c3(ch.ncenth[k2], itint, is)] + fornow * t;
+          er = er + (fornow - ch.rgspec[is - 1] * t) * yrhs[is - 1](ic, jc, kc);
+        }
+        erhs(ic, jc, kc) = er;
+        if (both) {
+          urun(ic, jc, kc) = 0.0;
+          vrun(ic, jc, kc) = 0.0;
+          wrun(ic, jc, kc) = 0.0;
+          uerr(ic, jc, kc) = 0.0;
+          verr(ic, jc, kc) = 0.0;
+          werr(ic, jc, kc) = 0.0;
+          erun(ic, jc, kc) = erhs(ic, jc, kc);
+          eerr(ic, jc, kc) = 0.0;
+        }
+      }
+  }
+  // one-sided fourth-order x derivative at the wall plane of the product
+  // a*b over the wall and the four planes inward (the FxxCNW/FxxDFW terms,
+  // rhscal.f:615-623, 640-648; single-precision literals as coded)
+  double wall_deriv(Field& a, Field& b, int ic, int st, int jc, int kc) {
+    double f[5];
+    for (int k = 0; k < 5; ++k) f[k] = a(ic + k * st, jc, kc) * b(ic + k * st, jc, kc);
+    const double c0 = (double)(25.0f / 12.0f), c3 = (double)(4.0f / 3.0f);
+    if (st > 0) return ((-c0) * f[0] + (4.0) * f[1] - (3.0) * f[2] + c3 * f[3] - (1.0 / 4.0) * f[4]) / fd.deltax;
+    return (c0 * f[0] - (4.0) * f[1] + (3.0) * f[2] - c3 * f[3] + (1.0 / 4.0) * f[4]) / fd.deltax;
+  }
+  // LINCOM/FINCOM at a W1 wall (lincom.f:171-210, fincom.f:171-210): every
+  // mass fraction of the updated U register extrapolated with zero normal
+  // gradient, Y_w = (12/25)(4 Y_1 - 3 Y_2 + (4/3) Y_3 - Y_4/4), clipped to
+  // [0, 1], times the wall density, into both registers
+  void wall_species(bool left) {
+    const int ic = left ? istal : istol, st = left ? 1 : -1;
+    const double c1 = (double)(12.0f / 25.0f), c3 = (double)(4.0f / 3.0f);
+    for (int is = 0; is < nspec; ++is)
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const double t1 = yrhs[is](ic + st, jc, kc) / drhs(ic + st, jc, kc);
+          const double t2 = yrhs[is](ic + 2 * st, jc, kc) / drhs(ic + 2 * st, jc, kc);
+          const double t3 = yrhs[is](ic + 3 * st, jc, kc) / drhs(ic + 3 * st, jc, kc);
+          const double t4 = yrhs[is](ic + 4 * st, jc, kc) / drhs(ic + 4 * st, jc, kc);
+          double yw = c1 * (4.0 * t1 - 3.0 * t2 + c3 * t3 - (1.0 / 4.0 * t4));
+          yw = std::min(1.0, yw);
+          yw = std::max(0.0, yw);
+          yw = drhs(ic, jc, kc) * yw;
+          yrun[is](ic, jc, kc) = yw;
+          yrhs[is](ic, jc, kc) = yw;
+        }
+  }
   // BOUNDT, I3 at x-left: impose the inflow state on the U register (DRHS..YRHS
   // at ISTAL; src/boundt.f:177-200 with BCDTXL, BCUTXL NXLPRM(1)=1, BCYTXL)
   void boundt() {
     if (bcxl == BC_I2 || bcxr == BC_I2) impose_i2(false);
+    if (bcxl == BC_W1) impose_w1(true, false);
+    if (bcxr == BC_W1) impose_w1(false, false);
     if (bcxl != BC_I3 && bcxr != BC_I3) return;
     const int ic = bcxl == BC_I3 ? istal : istol;  // boundt.f:177 (x-left), 591 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
@@ -714,6 +824,8 @@ struct Oracle {
   // error zeroed (src/bountt.f:203-252)
   void bountt() {
     if (bcxl == BC_I2 || bcxr == BC_I2) impose_i2(true);
+    if (bcxl == BC_W1) impose_w1(true, true);
+    if (bcxr == BC_W1) impose_w1(false, true);
     if (bcxl != BC_I3 && bcxr != BC_I3) return;
     const int ic = bcxl == BC_I3 ? istal : istol;  // bountt.f:203 (x-left), 709 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
@@ -827,6 +939,39 @@ struct Oracle {
     };
     if (bcxl == BC_I2) i2(fxl, true);
     if (bcxr == BC_I2) i2(fxr, false);
+    // W1 (bounds.f:917-1056 x-left, 1833-1974 x-right): the wall temperature
+    // re-extrapolated; the outgoing wave reflected (L5 = L1 - L5 on the left,
+    // L1 = L5 - L1 on the right), L2..L4 and LY zero; the momentum and
+    // energy RHS vanish and the density and species RHS take the reflected
+    // wave
+    auto w1 = [&](Face& F, bool left) {
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      const int ic = left ? istal : istol;
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) trun(ic, jc, kc) = wall_t(ic, left ? 1 : -1, jc, kc);
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          const double fornow = F.d[q] * acou[q] * F.bcl1[q];
+          double bcl1 = 0.5 * (F.u[q] - acou[q]) * (F.bcl5[q] - fornow);
+          double bcl2 = F.u[q] * (F.bcl2[q] - F.bcl5[q] * ova2[q]);
+          double bcl5 = 0.5 * (F.u[q] + acou[q]) * (F.bcl5[q] + fornow);
+          if (left) bcl5 = bcl1 - bcl5;
+          else bcl1 = bcl5 - bcl1;
+          bcl2 = 0.0;
+          const double lw = left ? bcl5 : bcl1;
+          if (left) drhs(ic, jc, kc) = drhs(ic, jc, kc) - bcl2 - bcl5 * ova2[q];
+          else drhs(ic, jc, kc) = drhs(ic, jc, kc) - bcl1 * ova2[q] - bcl2;
+          urhs(ic, jc, kc) = 0.0;
+          vrhs(ic, jc, kc) = 0.0;
+          wrhs(ic, jc, kc) = 0.0;
+          erhs(ic, jc, kc) = 0.0;
+          for (int is = 0; is < nspec; ++is)
+            yrhs[is](ic, jc, kc) = yrhs[is](ic, jc, kc) - (bcl2 + lw * ova2[q]) * F.y[is * m + q];
+        }
+    };
+    if (bcxl == BC_W1) w1(fxl, true);
+    if (bcxr == BC_W1) w1(fxr, false);
     if (bcxl == BC_O1) {  // bounds.f:213-372: L5 (entering from the left) relaxed
       Face& F = fxl;
       prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
@@ -1495,6 +1640,8 @@ struct Oracle {
   // Dufour, molar-mass limit): src/diffin.f:384-406, WMLTOL 1e-3 (:34).
   void set_transport(bool mixw, bool mixp, bool soret, bool dufour, double wmltdr) {
     if (!df.flmavt) throw std::runtime_error("transport switches need mixture-averaged transport");
+    if ((bcxl == BC_W1 || bcxr == BC_W1) && (mixw || mixp || soret || dufour))
+      throw std::runtime_error("oracle: W1 walls restated for the base transport only");
     df.flmixw = mixw;
     df.flmixp = mixp;
     df.flmixt = false;
@@ -1573,6 +1720,12 @@ struct Oracle {
     STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + (store4(ic, jc, kc) * store1(ic, jc, kc) +
                                                store5(ic, jc, kc) * store2(ic, jc, kc) +
                                                store6(ic, jc, kc) * store3(ic, jc, kc));
+    // rhscal.f:610-660: W1 wall, one-sided derivative of lambda dT/dx
+    for (int kc = kstal; kc <= kstol; ++kc)
+      for (int jc = jstal; jc <= jstol; ++jc) {
+        if (fxlcnw) erhs(istal, jc, kc) = erhs(istal, jc, kc) + wall_deriv(store7, store1, istal, 1, jc, kc);
+        if (fxrcnw) erhs(istol, jc, kc) = erhs(istol, jc, kc) + wall_deriv(store7, store1, istol, -1, jc, kc);
+      }
     d2fdx2(trun, store1); d2fdy2(trun, store2); d2fdz2(trun, store3);
     zx(fxlcon, fxrcon, store1); zy(fylcon, fyrcon, store2); zz(fzlcon, fzrcon, store3);
     STD3 erhs(ic, jc, kc) = erhs(ic, jc, kc) + (store1(ic, jc, kc) + store2(ic, jc, kc) + store3(ic, jc, kc)) *
@@ -1713,6 +1866,18 @@ struct Oracle {
                    store6(ic, jc, kc) * store3(ic, jc, kc);
         erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * store7(ic, jc, kc);
       }
+      // rhscal.f:1698-1760: W1 wall, one-sided derivative of rho D dY/dx
+      // added to the rate, VTMP and (times h_k) the energy
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc)
+          for (int side = 0; side < 2; ++side) {
+            if (!(side == 0 ? fxldfw : fxrdfw)) continue;
+            const int ic = side == 0 ? istal : istol;
+            const double fornow = wall_deriv(store7, store1, ic, side == 0 ? 1 : -1, jc, kc);
+            rt(ic, jc, kc) = rt(ic, jc, kc) + fornow;
+            vtmp(ic, jc, kc) = vtmp(ic, jc, kc) + fornow;
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) + fornow * utmp(ic, jc, kc);
+          }
       STD3 store4(ic, jc, kc) = store7(ic, jc, kc);
       BIG3 store7(ic, jc, kc) = y(ic, jc, kc);
       d2fdx2(store7, store1); d2fdy2(store7, store2); d2fdz2(store7, store3);
@@ -2078,6 +2243,8 @@ struct Oracle {
     rkupdate(wrun, wrhs, werr, irk, last, istalw, istolw);
     rkupdate(erun, erhs, eerr, irk, last, istale, istole);
     for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last, istaly, istoly);
+    if (bcxl == BC_W1) wall_species(true);
+    if (bcxr == BC_W1) wall_species(false);
   }
 
   // ---- explicit filter: src/flinit.f:42-…, src/filtrx.f:56-295 (+y, z),

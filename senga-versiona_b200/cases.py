@@ -229,6 +229,13 @@ def make_case(name, n=None, seed=1234, scale_n=None, shape=None, chem_reader=Non
                   composition of complete H2 -> H2O conversion; mean flow
                   1.25 m/s plus Passot-Pouquet turbulence u' = 2 m/s,
                   l = 1.5 mm. The result carries "bc" for the face setup.
+    wall_box    : 32^3, 10 mm, H2/air mixture-averaged; W1 adiabatic no-slip
+                  walls on both x faces, y and z periodic. Two seeded hot
+                  kernels (r = 1 mm, 800 K -> 1600 K, the h2_pool
+                  composition) near either wall, Passot-Pouquet turbulence
+                  u' = 2 m/s, l = 1.5 mm, damped by sin^2(pi x / L) so that
+                  the velocity vanishes on the walls; uniform 101325 Pa.
+                  The result carries "bc" for the face setup.
     h2_pool     : 32^3 periodic, 10 mm, H2/air mixture-averaged with a
                   radical pool: the h2_kernels layout (4 seeded kernels
                   r = 1 mm, 800 K -> 1600 K) with the kernels' composition
@@ -308,6 +315,38 @@ def make_case(name, n=None, seed=1234, scale_n=None, shape=None, chem_reader=Non
         dt = stable_dt(chem, fields, T, lengths, shp)
         return dict(name=name, shape=shape_xyz, lengths=lengths, chem=chem_path, diff=diff_path, fields=fields, T=T,
                     itn=itn, dt=dt, nend=(1, 1, NPERI, NPERI, NPERI, NPERI), bc=bc)
+    elif name == "wall_box":
+        nn = n or 32
+        shape_xyz = tuple(shape) if shape else (nn, nn, nn)
+        L = 1.0e-2
+        lengths = (L, L, L)
+        chem_path, diff_path = CHEM_H2, DIFF_H2
+        chem = Chem(chem_path)
+        shp = shape_xyz[::-1]
+        centres = [(rng.uniform(0.5e-3, 2.0e-3), rng.uniform(0.0, L), rng.uniform(0.0, L)),
+                   (L - rng.uniform(1.0e-3, 3.0e-3), rng.uniform(0.0, L), rng.uniform(0.0, L))]
+        T = hot_kernels(shp, lengths, centres, 1.0e-3, 800.0, 1600.0)
+        prog = (T - 800.0) / 800.0
+        wm = chem.table("wmolar")
+        mass = np.array([2 * wm[0], wm[1], 3.76 * wm[8]])
+        yu = np.zeros(9)
+        yu[0], yu[1], yu[8] = mass / mass.sum()
+        yb = np.array([0.01, 0.12, 0.14, 0.004, 0.012, 0.002, 0.0005, 0.0002, 0.0])
+        yb[8] = 1.0 - yb[:8].sum()
+        Y = np.array([yu[k] + (yb[k] - yu[k]) * prog for k in range(9)])
+        u, v, w = passot_pouquet(shp, lengths, 2.0, 1.5e-3, seed)
+        x = np.arange(shape_xyz[0]) * (L / (shape_xyz[0] - 1))
+        damp = np.broadcast_to(np.sin(math.pi * x / L) ** 2, shp)
+        damp = np.where(np.abs(damp) < 1e-30, 0.0, damp)
+        u, v, w = u * damp, v * damp, w * damp
+        for a in (u, v, w):
+            a[..., 0] = 0.0
+            a[..., -1] = 0.0
+        p = np.full(shp, 101325.0)
+        fields, itn = conserved(chem, p, T, u, v, w, Y)
+        dt = stable_dt(chem, fields, T, lengths, shp)
+        return dict(name=name, shape=shape_xyz, lengths=lengths, chem=chem_path, diff=diff_path, fields=fields, T=T,
+                    itn=itn, dt=dt, nend=(1, 1, NPERI, NPERI, NPERI, NPERI), bc=dict(xl=31, xr=31))
     elif name == "h2_pool":
         nn = n or 32
         shape_xyz = tuple(shape) if shape else (nn, nn, nn)

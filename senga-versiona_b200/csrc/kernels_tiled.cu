@@ -594,8 +594,9 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
   const SSlab bS{sm};
   const int nc = 5 + nspec;
   // bf: x-face bits of the point; NSCBC planes add the BOUNDS correction
-  // (precomputed per face point) and an I3 inflow plane integrates only E
-  // (src/bcinit.f ranges ISTALD..ISTALY start at ISTAP1)
+  // (precomputed per face point), an I3 inflow plane integrates only E, an
+  // I2 plane only D, a W1 wall has zero momentum and energy RHS and
+  // integrates neither momentum (src/bcinit.f ranges ISTALD..ISTALY)
   auto advance = [&](int fld, const TP& t, int bf, double R) {
     const int64_t q = t.q;
     const int64_t idx = (int64_t)fld * n + q;
@@ -603,12 +604,14 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
       const int side = t.gx == 0 ? 0 : 1;
       R = R + f.face[((int64_t)side * nc + fld) * ((int64_t)g.ny * g.nz) + t.gy + (int64_t)g.ny * t.gz];
     }
+    if (!P && (bf & BF_WALL) && fld >= 1 && fld <= 4) R = 0.0;
     if (rk.last < 0) {  // right-hand side only
       f.rhs[idx] = R;
       return;
     }
     if (!P && (bf & BF_IMPOSED) && fld != 4) return;
     if (!P && (bf & BF_IMPOSED_D) && fld != 0) return;
+    if (!P && (bf & BF_WALL) && fld >= 1 && fld <= 3) return;
     if (f.err) f.err[idx] = f.err[idx] + rk.err * R;
     if (!rk.last) {
       const double s = f.run[idx];

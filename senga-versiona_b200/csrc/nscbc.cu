@@ -2,8 +2,9 @@
 //
 // Restated from the reference (I3 subsonic inflow with constant velocity,
 // NXxPRM(1)=1, I2 subsonic reflecting inflow with specified temperature,
-// and O1 partially non-reflecting outflow, on either x face; inflow on one
-// face at most; both O1 faces take the same parameters):
+// O1 partially non-reflecting outflow and W1 adiabatic no-slip wall, on
+// either x face; inflow on one face at most; both O1 faces take the same
+// parameters):
 //   BOUNDT  src/boundt.f:177-200 (x-left), 591- (x-right)   impose the
 //           inflow state on the U register
 //   face data gathered inside RHSCAL/RHSVEL (src/rhscal.f:70-90,159-180,
@@ -14,6 +15,11 @@
 //           (O1 right), 1688- (I3 right)
 //   BOUNTT  src/bountt.f:203-252 (x-left), 709- (x-right)   both registers
 //           of the inflow plane reset
+//   W1      boundt.f:243-356, 657-768 and bountt.f:290-428, 767- (wall
+//           temperature extrapolated, zero momentum, internal energy);
+//           bounds.f:917-1056, 1833-1974 (reflected wave); rhscal.f:1698-1760
+//           (wall diffusion flux); lincom.f/fincom.f:171-210 (zero-gradient
+//           mass fractions)
 // Every face quantity is a pointwise value or a derivative at the face plane,
 // so one thread per face point computes them from the thermochemistry
 // kernel's outputs and the U register right after that kernel (before the
@@ -54,37 +60,75 @@ __device__ __forceinline__ double dd_sub(const Geo& g, const double* a, double c
   return d1core([&](int m) { return at<DIR>(g, a, i, j, k, m) - c0; }, c, n, g.per[DIR]) * g.ovd[DIR];
 }
 
+// h_k(T) per unit mass of interval `it` (AMASCH polynomial, boundt.f:316-324)
+__device__ __forceinline__ double enthalpy(const senga_chem* chem, int s, int it, double t) {
+  const double* c = chem->amasch[s][it];
+  double h = c[chem->ncpoly[s][it] - 1];
+  for (int icp = chem->ncpom1[s][it]; icp >= 1; --icp) h = h * t + c[icp - 1];
+  return c[chem->ncenth[s][it] - 1] + h * t;
+}
+__device__ __forceinline__ int32_t interval_index(const senga_chem* chem, int nspec, double t) {
+  int32_t itn = 0;
+  for (int s = 0; s < nspec; ++s) {
+    int it = 0;
+    while (t > chem->tinthi[s][it] && it + 1 < chem->ntint[s]) ++it;
+    itn += it << (2 * s);
+  }
+  return itn;
+}
+// W1 wall temperature (boundt.f:252-260): T_w = (48 T_1 - 36 T_2 + 16 T_3 -
+// 3 T_4)/25 over the four planes inward, st = +1 (x-left) or -1 (x-right)
+__device__ __forceinline__ double wall_t(const double* t, int64_t q, int st) {
+  return (48.0 * t[q + st] - 36.0 * t[q + 2 * st] + 16.0 * t[q + 3 * st] - 3.0 * t[q + 4 * st]) / 25.0;
+}
+
+// one thread per face point; blockIdx.y = side (0: x-left, 1: x-right)
 __global__ void __launch_bounds__(kFaceBlock)
     k_boundt(Geo g, Fields f, NscbcParams bc, int nspec, int both, const senga_chem* chem) {
   const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
   if (jk >= g.ny * g.nz) return;
   const int64_t n = g.n;
-  const bool left = bc.xl == 13 || bc.xl == 12;
-  const int kind = left ? bc.xl : bc.xr;
-  const int i = left ? 0 : g.nx - 1;  // the inflow plane
+  const int side = blockIdx.y;
+  const int kind = side == 0 ? bc.xl : bc.xr;
+  if (kind != 12 && kind != 13 && kind != 31) return;
+  const int i = side == 0 ? 0 : g.nx - 1;  // the face plane
   const int64_t q = (int64_t)i + (int64_t)g.nx * jk;
   double* regs[2] = {f.uin, f.run};
+  if (kind == 31) {
+    // W1 (boundt.f:243-356 / 657-768; bountt.f:290-428 / 767-): wall
+    // temperature from the last TEMPER's planes inward, its ITNDEX, zero
+    // momentum, rho E = sum_k (h_k(T) - R_k T) rho Y_k
+    const double t = wall_t(f.t, q, side == 0 ? 1 : -1);
+    f.t[q] = t;
+    const int32_t itn = interval_index(chem, nspec, t);
+    f.itn[q] = itn;
+    double e = 0.0;
+    e = f.uin[q] * e;
+    for (int s = 0; s < nspec; ++s)
+      e = e + (enthalpy(chem, s, (itn >> (2 * s)) & 3, t) - chem->rgspec[s] * t) * f.uin[(5 + s) * n + q];
+    for (int r = 0; r < (both ? 2 : 1); ++r) {
+      double* U = regs[r];
+      U[n + q] = 0.0;
+      U[2 * n + q] = 0.0;
+      U[3 * n + q] = 0.0;
+      U[4 * n + q] = e;
+    }
+    if (both && f.err)  // BOUNTT: momentum and energy errors zeroed
+      for (int fl = 1; fl < 5; ++fl) f.err[fl * n + q] = 0.0;
+    return;
+  }
   if (kind == 12) {
     // I2 (boundt.f:81-176, bountt.f:84-200): ITNDEX of TRIN, then velocity,
     // energy and species from the face density of the U register
     const double t = bc.t_in, u = bc.u_in, v = 0.0, w = 0.0;
-    int32_t itn = 0;
-    for (int s = 0; s < nspec; ++s) {
-      int it = 0;
-      while (t > chem->tinthi[s][it] && it + 1 < chem->ntint[s]) ++it;
-      itn += it << (2 * s);
-    }
+    const int32_t itn = interval_index(chem, nspec, t);
     f.itn[q] = itn;
     const double d = f.uin[q];
     double e = 0.5 * (u * u + v * v + w * w);
     e = d * e;
     double ys[SENGA_NSPCMX];
     for (int s = 0; s < nspec; ++s) {
-      const int it = (itn >> (2 * s)) & 3;
-      const double* c = chem->amasch[s][it];
-      double h = c[chem->ncpoly[s][it] - 1];
-      for (int icp = chem->ncpom1[s][it]; icp >= 1; --icp) h = h * t + c[icp - 1];
-      h = c[chem->ncenth[s][it] - 1] + h * t;
+      const double h = enthalpy(chem, s, (itn >> (2 * s)) & 3, t);
       ys[s] = d * bc.y_in[s];
       e = e + (h - chem->rgspec[s] * t) * ys[s];
     }
@@ -169,6 +213,17 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     else b1 = b5 + d * acou * 0.0 - b1;            // L5 unchanged
     b2 = gam1 * ova2 * (b1 + b5) + d * (0.0 / t - sorp / p + sydt) - b2;
     corr[0] = -b2 - (side == 0 ? b5 : b1) * ova2;
+  } else if (kind == 31) {  // W1 wall (bounds.f:917-1056 left, 1833-1974 right)
+    // the outgoing wave reflected (L5 = L1 - L5 on the left, L1 = L5 - L1 on
+    // the right), L2 = L3 = L4 = LY = 0; U, V, W, E RHS zeroed in the RK
+    // epilogue (BF_WALL)
+    const double fornow = d * acou * bcl1;
+    const double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
+    const double b5 = 0.5 * (u + acou) * (bcl5 + fornow);
+    const double lw = side == 0 ? b1 - b5 : b5 - b1;
+    const double b2 = 0.0;
+    corr[0] = side == 0 ? -b2 - lw * ova2 : -lw * ova2 - b2;
+    for (int s = 0; s < nspec; ++s) corr[(int64_t)(5 + s) * nyz] = -(b2 + lw * ova2) * f.y[s * n + q];
   } else if (kind == 13 && side == 1) {  // I3 inflow at x-right (bounds.f:1688-): L1 enters
     double fornow = d * acou * bcl1;
     double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
@@ -284,13 +339,82 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
   }
 }
 
+// W1 wall diffusion flux (rhscal.f:1698-1760, base transport): the one-sided
+// fourth-order x derivative at the wall of rho D_k dY_k/dx over the wall and
+// the four planes inward, added to species k's rate and to VTMP (its energy
+// part is dropped: BOUNDS zeroes the wall's energy RHS).
+__global__ void __launch_bounds__(kFaceBlock) k_wall_flux(Geo g, Fields f, NscbcParams bc, int nspec) {
+  const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
+  const int side = blockIdx.y;
+  if (jk >= g.ny * g.nz || (side == 0 ? bc.xl : bc.xr) != 31) return;
+  const int j = jk % g.ny, k = jk / g.ny;
+  const int i = side == 0 ? 0 : g.nx - 1, st = side == 0 ? 1 : -1;
+  const int64_t n = g.n, q = (int64_t)i + (int64_t)g.nx * jk;
+  const double c0 = (double)(25.0f / 12.0f), c3 = (double)(4.0f / 3.0f);  // single-precision literals as coded
+  double vt = f.vtmp[q];
+  for (int s = 0; s < nspec; ++s) {
+    double fv[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m)
+      fv[m] = f.rd[s * n + q + m * st] * dd<0>(g, f.y + s * n, i + m * st, j, k);
+    const double w = side == 0 ? ((-c0) * fv[0] + 4.0 * fv[1] - 3.0 * fv[2] + c3 * fv[3] - 0.25 * fv[4]) * g.ovd[0]
+                               : (c0 * fv[0] - 4.0 * fv[1] + 3.0 * fv[2] - c3 * fv[3] + 0.25 * fv[4]) * g.ovd[0];
+    f.wdot[s * n + q] = f.wdot[s * n + q] + w;
+    vt = vt + w;
+  }
+  f.vtmp[q] = vt;
+}
+
+// After the RK update at a W1 wall: the wall temperature re-extrapolated
+// from this substage's TEMPER (bounds.f:925-933) and, when rk, every mass
+// fraction of the updated U register extrapolated with zero normal gradient,
+// Y_w = (12/25)(4 Y_1 - 3 Y_2 + (4/3) Y_3 - Y_4/4), clipped to [0, 1], times
+// the wall density, into both registers (lincom.f:171-210, fincom.f:171-210).
+__global__ void __launch_bounds__(kFaceBlock) k_wall_fix(Geo g, Fields f, NscbcParams bc, int nspec, int rk) {
+  const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
+  const int side = blockIdx.y;
+  if (jk >= g.ny * g.nz || (side == 0 ? bc.xl : bc.xr) != 31) return;
+  const int st = side == 0 ? 1 : -1;
+  const int64_t n = g.n, q = (side == 0 ? 0 : g.nx - 1) + (int64_t)g.nx * jk;
+  f.t[q] = wall_t(f.t, q, st);
+  if (!rk) return;
+  const double* U = f.uout;
+  const double c1 = (double)(12.0f / 25.0f), c3 = (double)(4.0f / 3.0f);
+  for (int s = 0; s < nspec; ++s) {
+    const double* y = U + (5 + s) * n;
+    const double t1 = y[q + st] / U[q + st], t2 = y[q + 2 * st] / U[q + 2 * st];
+    const double t3 = y[q + 3 * st] / U[q + 3 * st], t4 = y[q + 4 * st] / U[q + 4 * st];
+    double yw = c1 * (4.0 * t1 - 3.0 * t2 + c3 * t3 - (0.25 * t4));
+    yw = fmin(1.0, yw);
+    yw = fmax(0.0, yw);
+    yw = U[q] * yw;
+    f.run[(5 + s) * n + q] = yw;
+    f.uout[(5 + s) * n + q] = yw;
+  }
+}
+
 }  // namespace
+
+bool has_wall(const NscbcParams& bc) { return bc.xl == 31 || bc.xr == 31; }
 
 void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both,
                    const senga_chem* dchem, cudaStream_t s) {
-  if (bc.xl != 13 && bc.xr != 13 && bc.xl != 12 && bc.xr != 12) return;
+  auto imposed = [](int k) { return k == 12 || k == 13 || k == 31; };
+  if (!imposed(bc.xl) && !imposed(bc.xr)) return;
   const int nyz = g.ny * g.nz;
-  k_boundt<<<(nyz + kFaceBlock - 1) / kFaceBlock, kFaceBlock, 0, s>>>(g, f, bc, nspec, both ? 1 : 0, dchem);
+  k_boundt<<<dim3((nyz + kFaceBlock - 1) / kFaceBlock, 2), kFaceBlock, 0, s>>>(g, f, bc, nspec, both ? 1 : 0, dchem);
+}
+
+void launch_wall_flux(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, cudaStream_t s) {
+  if (!has_wall(bc)) return;
+  const int nyz = g.ny * g.nz;
+  k_wall_flux<<<dim3((nyz + kFaceBlock - 1) / kFaceBlock, 2), kFaceBlock, 0, s>>>(g, f, bc, nspec);
+}
+
+void launch_wall_fix(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool rk, cudaStream_t s) {
+  if (!has_wall(bc)) return;
+  const int nyz = g.ny * g.nz;
+  k_wall_fix<<<dim3((nyz + kFaceBlock - 1) / kFaceBlock, 2), kFaceBlock, 0, s>>>(g, f, bc, nspec, rk ? 1 : 0);
 }
 
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,

@@ -153,12 +153,14 @@ void run_rhs(senga_ctx* c) {
   if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);  // RADCAL
   launch_species_a(c->geo, c->f, c->nspec, c->stream);
   if (c->mixt) launch_mixt(c->geo, c->f, c->mx, c->d_chem, c->d_diff, c->nspec, c->stream);
+  if (c->nscbc) launch_wall_flux(c->geo, c->f, c->bc, c->nspec, c->stream);  // W1 wall diffusion flux
 }
 
 void run_substage(senga_ctx* c, int irk) {
   run_rhs(c);
   RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
   launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+  if (c->nscbc) launch_wall_fix(c->geo, c->f, c->bc, c->nspec, true, c->stream);  // W1: LINCOM/FINCOM wall Y
 }
 
 // ADAPTT (src/adaptt.f:53-330) after a step: error maxima on the device, the
@@ -413,6 +415,7 @@ int senga_rhs_host(senga_ctx* c, double* rhs, double* trun, double* prun) {
     run_rhs(c);
     RK rk{0.0, 0.0, 0.0, -1};  // last = -1: write R(U) into the rhs fields only
     launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+    if (c->nscbc) launch_wall_fix(c->geo, c->f, c->bc, c->nspec, false, c->stream);  // BOUNDS: wall T
     CK(cudaGetLastError());
     const int64_t n = c->geo.n;
     CK(cudaMemcpyAsync(rhs, c->f.rhs, (size_t)c->nc * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -430,21 +433,31 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
     for (auto& e : ev) CK(cudaEventCreate(&e));
     for (int k = 0; k < 4; ++k) ms[k] = 0.0;
     int nl = 0;
+    // the face kernels of an NSCBC box are timed with the kernel they follow
+    const bool imposed = c->nscbc && (c->bc.xl == 12 || c->bc.xl == 13 || c->bc.xl == 31 || c->bc.xr == 12 ||
+                                      c->bc.xr == 13 || c->bc.xr == 31);
+    const bool wall = c->nscbc && has_wall(c->bc);
+    const int nface = c->nscbc ? 1 + (imposed ? 1 : 0) + (wall ? 2 : 0) : 0;
     for (int irk = 1; irk <= 5; ++irk) {
       const int b = (irk - 1) * 4;
       CK(cudaEventRecord(ev[b], c->stream));
+      if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->d_chem, c->stream);
       const int nth = launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
       CK(cudaEventRecord(ev[b + 1], c->stream));
+      if (c->nscbc) launch_face(c->geo, c->f, c->bc, c->nspec, c->d_chem, c->stream);
       launch_flow(c->geo, c->f, c->nspec, c->stream);
       if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);
       CK(cudaEventRecord(ev[b + 2], c->stream));
       launch_species_a(c->geo, c->f, c->nspec, c->stream);
       const int nmx = c->mixt ? launch_mixt(c->geo, c->f, c->mx, c->d_chem, c->d_diff, c->nspec, c->stream) : 0;
+      if (c->nscbc) launch_wall_flux(c->geo, c->f, c->bc, c->nspec, c->stream);
       CK(cudaEventRecord(ev[b + 3], c->stream));
       RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
       launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+      if (c->nscbc) launch_wall_fix(c->geo, c->f, c->bc, c->nspec, true, c->stream);
+      if (irk == 5 && imposed) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->d_chem, c->stream);  // BOUNTT
       CK(cudaEventRecord(irk < 5 ? ev[b + 4] : ev[20], c->stream));
-      nl += 3 + nth + (c->rad ? 1 : 0) + nmx;
+      nl += 3 + nth + (c->rad ? 1 : 0) + nmx + nface + (irk == 5 && imposed ? 1 : 0);
     }
     CK(cudaStreamSynchronize(c->stream));
     for (int irk = 1; irk <= 5; ++irk) {
@@ -623,6 +636,8 @@ int senga_set_transport(senga_ctx* c, int mixw, int mixp, int soret, int dufour,
   return guard([&] {
     if ((mixw || mixp || soret || dufour) && !c->diff.flmavt)
       throw Error(SENGA_ERR_ARG, "senga_set_transport: the switches need mixture-averaged transport (diff.dat)");
+    if ((mixw || mixp || soret || dufour) && c->nscbc && has_wall(c->bc))
+      throw Error(SENGA_ERR_UNSUPPORTED, "senga_set_transport: a W1 wall runs with the base transport only");
     CK(cudaStreamSynchronize(c->stream));
     cudaFree(c->mixt_pool);
     c->mixt_pool = nullptr;
@@ -695,16 +710,22 @@ int senga_set_radiation(senga_ctx* c, const senga_radn* r) {
 
 int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
   if (!c || !b) return fail(SENGA_ERR_ARG, "senga_set_nscbc: null argument");
-  auto kind_ok = [](int k) { return k == 12 || k == 13 || k == 21; };
+  auto kind_ok = [](int k) { return k == 12 || k == 13 || k == 21 || k == 31; };
   auto inflow = [](int k) { return k == 12 || k == 13; };
+  auto either = [b](int k) { return b->xl == k || b->xr == k; };
   if (!kind_ok(b->xl) || !kind_ok(b->xr) || (inflow(b->xl) && inflow(b->xr)))
-    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I2 (12), I3 (13) and O1 (21) on either "
-                                       "x face, inflow on one at most");
-  if ((b->xl == 12 || b->xr == 12) && !(b->t_in > 0.0))
-    return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I2 inflow needs t_in > 0");
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I2 (12), I3 (13), O1 (21) and W1 (31) "
+                                       "on either x face, inflow on one at most");
+  if (either(12) && !(b->t_in > 0.0)) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I2 inflow needs t_in > 0");
   if (c->geo.per[0] || b->xl == 0 || b->xr == 0)
     return fail(SENGA_ERR_ARG, "senga_set_nscbc: needs a bounded x direction and a kind on both x faces");
-  if (b->rho_in <= 0.0 || b->p_inf <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: rho_in and p_inf must be > 0");
+  if (either(13) && b->rho_in <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I3 inflow needs rho_in > 0");
+  if (either(21) && b->p_inf <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an O1 outflow needs p_inf > 0");
+  // the molar-mass, pressure and thermal-diffusion branches carry wall flux
+  // terms of their own (rhscal.f:2116-, 2512-, 2925-, 3111-) not built here
+  if (either(31) && c->mixt)
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: a W1 wall runs with the base transport only "
+                                       "(senga_set_transport switches off)");
   return guard([&] {
     NscbcParams& p = c->bc;
     p = NscbcParams{};
@@ -720,12 +741,14 @@ int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
     p.pio = b->pio;
     p.betloc = b->bet_local;
     p.t_in = b->t_in;
-    // face-plane flags of src/bcinit.f:299-326,458-480,560-586: I3 -> FxxCNV,
-    // FxxVSN, the plane imposed; I2 -> FxxCNV, all but the density imposed;
-    // O1 -> FxxCNV, FxxVST, FxxCON, FxxADB, FxxDIF
+    // face-plane flags of src/bcinit.f:299-326,458-480,560-586,702-735: I3 ->
+    // FxxCNV, FxxVSN, the plane imposed; I2 -> FxxCNV, all but the density
+    // imposed; O1 -> FxxCNV, FxxVST, FxxCON, FxxADB, FxxDIF; W1 -> FxxCNV,
+    // FxxCON, FxxADB, FxxDIF, FxxCNW, FxxDFW, momentum not integrated
     auto bits = [](int kind) {
       return kind == 13   ? (BF_VSN | BF_NSCBC | BF_IMPOSED)
              : kind == 12 ? (BF_NSCBC | BF_IMPOSED_D)
+             : kind == 31 ? (BF_CON | BF_DIF | BF_NSCBC | BF_WALL)
                           : (BF_VST | BF_CON | BF_DIF | BF_NSCBC);
     };
     c->geo.bxl = bits(b->xl);

@@ -57,6 +57,7 @@ enum : int {
   BF_NSCBC = 16,    // BOUNDS corrections are added to the plane's RHS
   BF_IMPOSED = 32,  // I3 inflow: D, U, V, W, Y are imposed, not integrated
   BF_IMPOSED_D = 64,  // I2 inflow: U, V, W, E, Y are imposed, only D integrated
+  BF_WALL = 128,      // W1 wall: U, V, W, E RHS zero; U, V, W not integrated
 };
 __host__ __device__ __forceinline__ int face_bits(const Geo& g, int gx) {
   return gx == 0 ? g.bxl : (gx == g.nx - 1 ? g.bxr : 0);
@@ -153,7 +154,8 @@ void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchu
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
 // NSCBC x faces (nscbc.cu): face kinds 0 (none), 12 (I2 inflow), 13 (I3
-// inflow), 21 (O1 outflow) on either face, and their parameters.
+// inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall) on either face,
+// and their parameters.
 struct NscbcParams {
   int xl, xr;
   double u_in, rho_in, y_in[SENGA_NSPCMX];  // I3: RXLPRM(1), DRIN, YRIN
@@ -167,6 +169,12 @@ void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nsp
 // face data + BOUNDS corrections into f.face, after the thermochemistry kernel
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,
                  cudaStream_t s);
+// W1 walls: the wall diffusion-flux terms added to the species rate and VTMP
+// (after the species kernel), and the wall temperature plus, when rk, the
+// zero-gradient mass fractions of the updated state (after the RK update)
+bool has_wall(const NscbcParams& bc);
+void launch_wall_flux(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, cudaStream_t s);
+void launch_wall_fix(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool rk, cudaStream_t s);
 
 // RADCAL (radiation.cu): radiating species (0-based), their polynomials,
 // gas constants, 4 STEFBO and TREFRN^4.

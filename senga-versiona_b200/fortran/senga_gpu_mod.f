@@ -90,7 +90,8 @@ C     RADCIN's radiation tables (src/radcin.f:80-220)
         REAL(C_DOUBLE) :: TREFRN
       END TYPE
 C     NSCBC x faces: kinds 12 (I2 inflow), 13 (I3 inflow), 21 (O1
-C     outflow) and parameters (T_IN: TRIN of an I2 inflow)
+C     outflow), 31 (W1 adiabatic no-slip wall) and parameters (T_IN:
+C     TRIN of an I2 inflow)
       TYPE, BIND(C) :: SENGA_NSCBC
         INTEGER(C_INT) :: XL, XR
         REAL(C_DOUBLE) :: U_IN, RHO_IN

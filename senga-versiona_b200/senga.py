@@ -533,8 +533,9 @@ class Box:
         return out
 
     def set_nscbc(self, bc):
-        """NSCBC x faces from a dict (xl, xr in {13, 21}, u_in, rho_in, y_in, p_inf,
-        sigma, eta, pio, bet_local)."""
+        """NSCBC x faces from a dict (xl, xr in {0, 12, 13, 21, 31}, u_in, rho_in,
+        y_in, p_inf, sigma, eta, pio, bet_local, t_in); 12 I2 inflow, 13 I3
+        inflow, 21 O1 outflow, 31 W1 adiabatic no-slip wall."""
         b = NscbcT()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
         b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
