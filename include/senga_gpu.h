@@ -289,9 +289,19 @@ int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
  *   diffusion are zeroed on the plane (FxxCON, FxxDIF, FxxADB). The wall
  *   runs with the base transport: with senga_set_transport switches on,
  *   either call returns SENGA_ERR_UNSUPPORTED.
+ * 32: W2 isothermal no-slip wall (NSBCW2), on either or both faces: the
+ *   wall temperature t_wall[side] is imposed with zero momentum and rho E
+ *   the internal energy at it, on the U register by BOUNDT and on both
+ *   registers by BOUNTT (src/boundt.f:358-470, src/bountt.f:429-560 and
+ *   their x-right blocks); neither momentum nor energy is integrated on the
+ *   wall (ranges src/bcinit.f:822-855); the density and species take the
+ *   reflected wave as for W1 (src/bounds.f:1058-1190, 1975-), the wall
+ *   diffusion flux and the zero-gradient mass fractions as for W1; only
+ *   diffusion is zeroed on the plane (FxxDIF). Base transport only.
  * Face data and wave amplitudes are computed after the thermochemistry
  * kernel and added to the face planes' right-hand side in the RK epilogue.
- * rho_in must be > 0 with an I3 face, p_inf > 0 with an O1 face.
+ * rho_in must be > 0 with an I3 face, p_inf > 0 with an O1 face, t_wall > 0
+ * on a W2 face.
  * Other face kinds return SENGA_ERR_UNSUPPORTED. Stepping a box with a
  * bounded x direction needs this call first. */
 typedef struct senga_nscbc {
@@ -300,7 +310,8 @@ typedef struct senga_nscbc {
   double y_in[SENGA_NSPCMX];
   double p_inf, sigma, eta;
   int pio, bet_local;
-  double t_in; /* I2: imposed inflow temperature TRIN [K] */
+  double t_in;      /* I2: imposed inflow temperature TRIN [K] */
+  double t_wall[2]; /* W2: wall temperature of the x-left, x-right face (RXLPRM(1), RXRPRM(1)) [K] */
 } senga_nscbc;
 int senga_set_nscbc(senga_ctx* ctx, const senga_nscbc* bc);
 

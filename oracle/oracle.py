@@ -27,7 +27,8 @@ def build():
 class _Bc(C.Structure):
     _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
                 ("y_in", C.c_double * 9), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
-                ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double)]
+                ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double),
+                ("t_wall", C.c_double * 2)]
 
 
 class _Cfg(C.Structure):
@@ -186,8 +187,9 @@ class Oracle:
         return out
 
     def set_bc(self, bc):
-        """NSCBC x faces: bc = dict(xl, xr in {0, 12, 13, 21, 31}, u_in, rho_in, y_in, p_inf,
-        sigma, eta, pio=0, bet_local=0, t_in (I2)); 31 is the W1 wall."""
+        """NSCBC x faces: bc = dict(xl, xr in {0, 12, 13, 21, 31, 32}, u_in, rho_in, y_in,
+        p_inf, sigma, eta, pio=0, bet_local=0, t_in (I2), t_wall (W2: x-left,
+        x-right)); 31 is the W1 wall, 32 the W2 wall."""
         b = _Bc()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
         b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
@@ -196,6 +198,7 @@ class Oracle:
         b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
         b.t_in = bc.get("t_in", 0.0)
+        b.t_wall[0], b.t_wall[1] = bc.get("t_wall", (0.0, 0.0))
         if _get().oracle_set_bc(self.h, C.byref(b)) != 0:
             raise RuntimeError("oracle_set_bc: " + _get().oracle_last_error().decode())
 

@@ -577,10 +577,16 @@ struct Oracle {
   // zero-gradient mass fractions of lincom.f:171-210, fincom.f:171-210), on
   // either or both x faces, with the base transport (the molar-mass,
   // pressure and thermal-diffusion branches carry wall terms of their own
-  // that are not restated).
-  static constexpr int BC_NONE = 0, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21, BC_W1 = 31;
+  // that are not restated). And W2, the isothermal no-slip wall (NSBCW2;
+  // bcinit.f:822-855, boundt.f:358-470 and its x-right block, bountt.f:
+  // 429-560 and its x-right block, bounds.f:1058-1190, 1975-): the wall
+  // temperature RXxPRM(1) imposed, FxxDIF and FxxDFW only, neither momentum
+  // nor energy integrated on the wall.
+  static constexpr int BC_NONE = 0, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21, BC_W1 = 31, BC_W2 = 32;
   int bcxl = BC_NONE, bcxr = BC_NONE;
   double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0, tin = 0.0;
+  double twall[2] = {0.0, 0.0};  // W2: RXLPRM(1), RXRPRM(1)
+  static bool is_wall(int k) { return k == BC_W1 || k == BC_W2; }
   int pio_xr = 0, betloc_xr = 0;
   bool fxlcnv = false, fxrcnv = false;
   bool fxlcnw = false, fxrcnw = false, fxldfw = false, fxrdfw = false;
@@ -612,13 +618,17 @@ struct Oracle {
     });
   }
   void set_bc(int xl, int xr, double u_in, double rho_in, const double* y_in, double p_inf, double sigma,
-              double eta, int pio, int betloc, double t_in = 0.0) {
-    auto ok = [](int k) { return k == BC_NONE || k == BC_I2 || k == BC_I3 || k == BC_O1 || k == BC_W1; };
+              double eta, int pio, int betloc, double t_in = 0.0, double t_wall_l = 0.0, double t_wall_r = 0.0) {
+    auto ok = [](int k) { return k == BC_NONE || k == BC_I2 || k == BC_I3 || k == BC_O1 || k == BC_W1 || k == BC_W2; };
     auto inflow = [](int k) { return k == BC_I2 || k == BC_I3; };
     if (!ok(xl) || !ok(xr) || (inflow(xl) && inflow(xr)))
-      throw std::runtime_error("oracle: NSCBC restated for I2, I3, O1 and W1 x faces (not inflow on both)");
-    if ((xl == BC_W1 || xr == BC_W1) && (df.flmixw || df.flmixp || df.flmixt))
-      throw std::runtime_error("oracle: W1 walls restated for the base transport only");
+      throw std::runtime_error("oracle: NSCBC restated for I2, I3, O1, W1 and W2 x faces (not inflow on both)");
+    if ((is_wall(xl) || is_wall(xr)) && (df.flmixw || df.flmixp || df.flmixt))
+      throw std::runtime_error("oracle: W1/W2 walls restated for the base transport only");
+    if ((xl == BC_W2 && !(t_wall_l > 0.0)) || (xr == BC_W2 && !(t_wall_r > 0.0)))
+      throw std::runtime_error("oracle: a W2 wall needs its temperature > 0");
+    twall[0] = t_wall_l;
+    twall[1] = t_wall_r;
     if ((xl != BC_NONE && nendxl != NBOUND) || (xr != BC_NONE && nendxr != NBOUND))
       throw std::runtime_error("oracle: NSCBC faces need NBOUND end conditions");
     bcxl = xl;
@@ -655,6 +665,14 @@ struct Oracle {
     if (xr == BC_W1) {  // src/bcinit.f:721-735: the same on the right; U,V,W to ISTOM1
       fxrcon = fxradb = fxrdif = fxrcnw = fxrdfw = true;
       istolu = istolv = istolw = istol - 1;
+    }
+    if (xl == BC_W2) {  // src/bcinit.f:822-837: FXLDIF FXLADW FXLDFW; U,V,W,E from ISTAP1
+      fxldif = fxldfw = true;
+      istalu = istalv = istalw = istale = istal + 1;
+    }
+    if (xr == BC_W2) {  // src/bcinit.f:840-855: the same on the right
+      fxrdif = fxrdfw = true;
+      istolu = istolv = istolw = istole = istol - 1;
     }
     fxl.init(ny * nz, nspec);
     fxr.init(ny * nz, nspec);
@@ -736,13 +754,15 @@ struct Oracle {
   // W1 wall plane (boundt.f:243-356 / 657-768): T extrapolated, its ITNDEX,
   // zero momentum and rho E = sum_k (h_k(T) - R_k T) rho Y_k on the U
   // register; both = BOUNTT (bountt.f:290-428 / 767-): the S register's
-  // momentum and energy too, their errors zeroed
-  void impose_w1(bool left, bool both) {
+  // momentum and energy too, their errors zeroed. W2 (boundt.f:358-470,
+  // bountt.f:429-560): the same with T = RXxPRM(1), TRUN left as it is.
+  void impose_wall(bool left, bool both) {
     const int ic = left ? istal : istol, st = left ? 1 : -1;
+    const bool w2 = (left ? bcxl : bcxr) == BC_W2;
     for (int kc = kstal; kc <= kstol; ++kc)
       for (int jc = jstal; jc <= jstol; ++jc) {
-        const double t = wall_t(ic, st, jc, kc);
-        trun(ic, jc, kc) = t;
+        const double t = w2 ? twall[left ? 0 : 1] : wall_t(ic, st, jc, kc);
+        if (!w2) trun(ic, jc, kc) = t;
         const int itnew = interval_of(t);
         itndex(ic, jc, kc) = itnew;
         urhs(ic, jc, kc) = 0.0;
@@ -807,8 +827,8 @@ struct Oracle {
   // at ISTAL; src/boundt.f:177-200 with BCDTXL, BCUTXL NXLPRM(1)=1, BCYTXL)
   void boundt() {
     if (bcxl == BC_I2 || bcxr == BC_I2) impose_i2(false);
-    if (bcxl == BC_W1) impose_w1(true, false);
-    if (bcxr == BC_W1) impose_w1(false, false);
+    if (is_wall(bcxl)) impose_wall(true, false);
+    if (is_wall(bcxr)) impose_wall(false, false);
     if (bcxl != BC_I3 && bcxr != BC_I3) return;
     const int ic = bcxl == BC_I3 ? istal : istol;  // boundt.f:177 (x-left), 591 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
@@ -824,8 +844,8 @@ struct Oracle {
   // error zeroed (src/bountt.f:203-252)
   void bountt() {
     if (bcxl == BC_I2 || bcxr == BC_I2) impose_i2(true);
-    if (bcxl == BC_W1) impose_w1(true, true);
-    if (bcxr == BC_W1) impose_w1(false, true);
+    if (is_wall(bcxl)) impose_wall(true, true);
+    if (is_wall(bcxr)) impose_wall(false, true);
     if (bcxl != BC_I3 && bcxr != BC_I3) return;
     const int ic = bcxl == BC_I3 ? istal : istol;  // bountt.f:203 (x-left), 709 (x-right)
     for (int kc = kstal; kc <= kstol; ++kc)
@@ -944,11 +964,13 @@ struct Oracle {
     // L1 = L5 - L1 on the right), L2..L4 and LY zero; the momentum and
     // energy RHS vanish and the density and species RHS take the reflected
     // wave
+    // W2 (bounds.f:1058-1190, 1975-): the same without the temperature
     auto w1 = [&](Face& F, bool left) {
       prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
       const int ic = left ? istal : istol;
-      for (int kc = kstal; kc <= kstol; ++kc)
-        for (int jc = jstal; jc <= jstol; ++jc) trun(ic, jc, kc) = wall_t(ic, left ? 1 : -1, jc, kc);
+      if ((left ? bcxl : bcxr) == BC_W1)
+        for (int kc = kstal; kc <= kstol; ++kc)
+          for (int jc = jstal; jc <= jstol; ++jc) trun(ic, jc, kc) = wall_t(ic, left ? 1 : -1, jc, kc);
       for (int kc = kstal; kc <= kstol; ++kc)
         for (int jc = jstal; jc <= jstol; ++jc) {
           const int q = fj(jc, kc);
@@ -970,8 +992,8 @@ struct Oracle {
             yrhs[is](ic, jc, kc) = yrhs[is](ic, jc, kc) - (bcl2 + lw * ova2[q]) * F.y[is * m + q];
         }
     };
-    if (bcxl == BC_W1) w1(fxl, true);
-    if (bcxr == BC_W1) w1(fxr, false);
+    if (is_wall(bcxl)) w1(fxl, true);
+    if (is_wall(bcxr)) w1(fxr, false);
     if (bcxl == BC_O1) {  // bounds.f:213-372: L5 (entering from the left) relaxed
       Face& F = fxl;
       prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
@@ -1640,8 +1662,8 @@ struct Oracle {
   // Dufour, molar-mass limit): src/diffin.f:384-406, WMLTOL 1e-3 (:34).
   void set_transport(bool mixw, bool mixp, bool soret, bool dufour, double wmltdr) {
     if (!df.flmavt) throw std::runtime_error("transport switches need mixture-averaged transport");
-    if ((bcxl == BC_W1 || bcxr == BC_W1) && (mixw || mixp || soret || dufour))
-      throw std::runtime_error("oracle: W1 walls restated for the base transport only");
+    if ((is_wall(bcxl) || is_wall(bcxr)) && (mixw || mixp || soret || dufour))
+      throw std::runtime_error("oracle: W1/W2 walls restated for the base transport only");
     df.flmixw = mixw;
     df.flmixp = mixp;
     df.flmixt = false;
@@ -2243,8 +2265,8 @@ struct Oracle {
     rkupdate(wrun, wrhs, werr, irk, last, istalw, istolw);
     rkupdate(erun, erhs, eerr, irk, last, istale, istole);
     for (int is = 0; is < nspec; ++is) rkupdate(yrun[is], yrhs[is], yerr[is], irk, last, istaly, istoly);
-    if (bcxl == BC_W1) wall_species(true);
-    if (bcxr == BC_W1) wall_species(false);
+    if (is_wall(bcxl)) wall_species(true);
+    if (is_wall(bcxr)) wall_species(false);
   }
 
   // ---- explicit filter: src/flinit.f:42-…, src/filtrx.f:56-295 (+y, z),
@@ -2585,7 +2607,7 @@ int oracle_rhs(void* h, double* rhs_out, double* t_out, double* p_out) {
   }
 }
 
-// NSCBC x faces (I3 inflow at x-left, O1 outflow at x-right; 0 = none).
+// NSCBC x faces (kinds 12, 13, 21, 31, 32 on either face; 0 = none).
 struct oracle_bc {
   int xl, xr;
   double u_in, rho_in;
@@ -2593,11 +2615,12 @@ struct oracle_bc {
   double p_inf, sigma, eta;
   int pio, bet_local;
   double t_in;
+  double t_wall[2];
 };
 int oracle_set_bc(void* h, const oracle_bc* b) {
   try {
     static_cast<orc::Oracle*>(h)->set_bc(b->xl, b->xr, b->u_in, b->rho_in, b->y_in, b->p_inf, b->sigma, b->eta, b->pio,
-                                         b->bet_local, b->t_in);
+                                         b->bet_local, b->t_in, b->t_wall[0], b->t_wall[1]);
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

@@ -595,8 +595,10 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
   const int nc = 5 + nspec;
   // bf: x-face bits of the point; NSCBC planes add the BOUNDS correction
   // (precomputed per face point), an I3 inflow plane integrates only E, an
-  // I2 plane only D, a W1 wall has zero momentum and energy RHS and
-  // integrates neither momentum (src/bcinit.f ranges ISTALD..ISTALY)
+  // I2 plane only D, a wall has zero momentum and energy RHS and integrates
+  // no momentum (src/bcinit.f ranges ISTALD..ISTALY; a W2 wall's energy,
+  // left out of the range too, is advanced by a zero RHS, which leaves both
+  // registers where BOUNDT put them)
   auto advance = [&](int fld, const TP& t, int bf, double R) {
     const int64_t q = t.q;
     const int64_t idx = (int64_t)fld * n + q;

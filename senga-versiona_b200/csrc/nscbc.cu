@@ -2,9 +2,9 @@
 //
 // Restated from the reference (I3 subsonic inflow with constant velocity,
 // NXxPRM(1)=1, I2 subsonic reflecting inflow with specified temperature,
-// O1 partially non-reflecting outflow and W1 adiabatic no-slip wall, on
-// either x face; inflow on one face at most; both O1 faces take the same
-// parameters):
+// O1 partially non-reflecting outflow, W1 adiabatic and W2 isothermal
+// no-slip walls, on either x face; inflow on one face at most; both O1 faces
+// take the same parameters):
 //   BOUNDT  src/boundt.f:177-200 (x-left), 591- (x-right)   impose the
 //           inflow state on the U register
 //   face data gathered inside RHSCAL/RHSVEL (src/rhscal.f:70-90,159-180,
@@ -20,6 +20,9 @@
 //           bounds.f:917-1056, 1833-1974 (reflected wave); rhscal.f:1698-1760
 //           (wall diffusion flux); lincom.f/fincom.f:171-210 (zero-gradient
 //           mass fractions)
+//   W2      the same with the wall temperature imposed (boundt.f:358-470,
+//           bountt.f:429-560 and their x-right blocks; bounds.f:1058-1190,
+//           1975-), energy not integrated on the wall
 // Every face quantity is a pointwise value or a derivative at the face plane,
 // so one thread per face point computes them from the thermochemistry
 // kernel's outputs and the U register right after that kernel (before the
@@ -90,16 +93,22 @@ __global__ void __launch_bounds__(kFaceBlock)
   const int64_t n = g.n;
   const int side = blockIdx.y;
   const int kind = side == 0 ? bc.xl : bc.xr;
-  if (kind != 12 && kind != 13 && kind != 31) return;
+  if (kind != 12 && kind != 13 && kind != 31 && kind != 32) return;
   const int i = side == 0 ? 0 : g.nx - 1;  // the face plane
   const int64_t q = (int64_t)i + (int64_t)g.nx * jk;
   double* regs[2] = {f.uin, f.run};
-  if (kind == 31) {
+  if (kind == 31 || kind == 32) {
     // W1 (boundt.f:243-356 / 657-768; bountt.f:290-428 / 767-): wall
     // temperature from the last TEMPER's planes inward, its ITNDEX, zero
-    // momentum, rho E = sum_k (h_k(T) - R_k T) rho Y_k
-    const double t = wall_t(f.t, q, side == 0 ? 1 : -1);
-    f.t[q] = t;
+    // momentum, rho E = sum_k (h_k(T) - R_k T) rho Y_k. W2 (boundt.f:
+    // 358-470, bountt.f:429-560): the imposed temperature, TRUN untouched.
+    double t;
+    if (kind == 31) {
+      t = wall_t(f.t, q, side == 0 ? 1 : -1);
+      f.t[q] = t;
+    } else {
+      t = bc.t_wall[side];
+    }
     const int32_t itn = interval_index(chem, nspec, t);
     f.itn[q] = itn;
     double e = 0.0;
@@ -213,7 +222,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     else b1 = b5 + d * acou * 0.0 - b1;            // L5 unchanged
     b2 = gam1 * ova2 * (b1 + b5) + d * (0.0 / t - sorp / p + sydt) - b2;
     corr[0] = -b2 - (side == 0 ? b5 : b1) * ova2;
-  } else if (kind == 31) {  // W1 wall (bounds.f:917-1056 left, 1833-1974 right)
+  } else if (kind == 31 || kind == 32) {  // W1/W2 wall (bounds.f:917-1056, 1058-1190 left; 1833-1974, 1975- right)
     // the outgoing wave reflected (L5 = L1 - L5 on the left, L1 = L5 - L1 on
     // the right), L2 = L3 = L4 = LY = 0; U, V, W, E RHS zeroed in the RK
     // epilogue (BF_WALL)
@@ -346,7 +355,8 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
 __global__ void __launch_bounds__(kFaceBlock) k_wall_flux(Geo g, Fields f, NscbcParams bc, int nspec) {
   const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
   const int side = blockIdx.y;
-  if (jk >= g.ny * g.nz || (side == 0 ? bc.xl : bc.xr) != 31) return;
+  const int kind = side == 0 ? bc.xl : bc.xr;
+  if (jk >= g.ny * g.nz || (kind != 31 && kind != 32)) return;
   const int j = jk % g.ny, k = jk / g.ny;
   const int i = side == 0 ? 0 : g.nx - 1, st = side == 0 ? 1 : -1;
   const int64_t n = g.n, q = (int64_t)i + (int64_t)g.nx * jk;
@@ -366,17 +376,19 @@ __global__ void __launch_bounds__(kFaceBlock) k_wall_flux(Geo g, Fields f, Nscbc
 }
 
 // After the RK update at a W1 wall: the wall temperature re-extrapolated
-// from this substage's TEMPER (bounds.f:925-933) and, when rk, every mass
+// from this substage's TEMPER (bounds.f:925-933; not at a W2 wall) and, at
+// either wall when rk, every mass
 // fraction of the updated U register extrapolated with zero normal gradient,
 // Y_w = (12/25)(4 Y_1 - 3 Y_2 + (4/3) Y_3 - Y_4/4), clipped to [0, 1], times
 // the wall density, into both registers (lincom.f:171-210, fincom.f:171-210).
 __global__ void __launch_bounds__(kFaceBlock) k_wall_fix(Geo g, Fields f, NscbcParams bc, int nspec, int rk) {
   const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
   const int side = blockIdx.y;
-  if (jk >= g.ny * g.nz || (side == 0 ? bc.xl : bc.xr) != 31) return;
+  const int kind = side == 0 ? bc.xl : bc.xr;
+  if (jk >= g.ny * g.nz || (kind != 31 && kind != 32)) return;
   const int st = side == 0 ? 1 : -1;
   const int64_t n = g.n, q = (side == 0 ? 0 : g.nx - 1) + (int64_t)g.nx * jk;
-  f.t[q] = wall_t(f.t, q, st);
+  if (kind == 31) f.t[q] = wall_t(f.t, q, st);
   if (!rk) return;
   const double* U = f.uout;
   const double c1 = (double)(12.0f / 25.0f), c3 = (double)(4.0f / 3.0f);
@@ -395,11 +407,11 @@ __global__ void __launch_bounds__(kFaceBlock) k_wall_fix(Geo g, Fields f, NscbcP
 
 }  // namespace
 
-bool has_wall(const NscbcParams& bc) { return bc.xl == 31 || bc.xr == 31; }
+bool has_wall(const NscbcParams& bc) { return bc.xl == 31 || bc.xr == 31 || bc.xl == 32 || bc.xr == 32; }
 
 void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both,
                    const senga_chem* dchem, cudaStream_t s) {
-  auto imposed = [](int k) { return k == 12 || k == 13 || k == 31; };
+  auto imposed = [](int k) { return k == 12 || k == 13 || k == 31 || k == 32; };
   if (!imposed(bc.xl) && !imposed(bc.xr)) return;
   const int nyz = g.ny * g.nz;
   k_boundt<<<dim3((nyz + kFaceBlock - 1) / kFaceBlock, 2), kFaceBlock, 0, s>>>(g, f, bc, nspec, both ? 1 : 0, dchem);

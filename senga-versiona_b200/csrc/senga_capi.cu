@@ -434,8 +434,8 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
     for (int k = 0; k < 4; ++k) ms[k] = 0.0;
     int nl = 0;
     // the face kernels of an NSCBC box are timed with the kernel they follow
-    const bool imposed = c->nscbc && (c->bc.xl == 12 || c->bc.xl == 13 || c->bc.xl == 31 || c->bc.xr == 12 ||
-                                      c->bc.xr == 13 || c->bc.xr == 31);
+    const bool imposed = c->nscbc && (c->bc.xl == 12 || c->bc.xl == 13 || c->bc.xr == 12 || c->bc.xr == 13 ||
+                                      has_wall(c->bc));
     const bool wall = c->nscbc && has_wall(c->bc);
     const int nface = c->nscbc ? 1 + (imposed ? 1 : 0) + (wall ? 2 : 0) : 0;
     for (int irk = 1; irk <= 5; ++irk) {
@@ -637,7 +637,7 @@ int senga_set_transport(senga_ctx* c, int mixw, int mixp, int soret, int dufour,
     if ((mixw || mixp || soret || dufour) && !c->diff.flmavt)
       throw Error(SENGA_ERR_ARG, "senga_set_transport: the switches need mixture-averaged transport (diff.dat)");
     if ((mixw || mixp || soret || dufour) && c->nscbc && has_wall(c->bc))
-      throw Error(SENGA_ERR_UNSUPPORTED, "senga_set_transport: a W1 wall runs with the base transport only");
+      throw Error(SENGA_ERR_UNSUPPORTED, "senga_set_transport: a W1/W2 wall runs with the base transport only");
     CK(cudaStreamSynchronize(c->stream));
     cudaFree(c->mixt_pool);
     c->mixt_pool = nullptr;
@@ -710,21 +710,23 @@ int senga_set_radiation(senga_ctx* c, const senga_radn* r) {
 
 int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
   if (!c || !b) return fail(SENGA_ERR_ARG, "senga_set_nscbc: null argument");
-  auto kind_ok = [](int k) { return k == 12 || k == 13 || k == 21 || k == 31; };
+  auto kind_ok = [](int k) { return k == 12 || k == 13 || k == 21 || k == 31 || k == 32; };
   auto inflow = [](int k) { return k == 12 || k == 13; };
   auto either = [b](int k) { return b->xl == k || b->xr == k; };
   if (!kind_ok(b->xl) || !kind_ok(b->xr) || (inflow(b->xl) && inflow(b->xr)))
-    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I2 (12), I3 (13), O1 (21) and W1 (31) "
-                                       "on either x face, inflow on one at most");
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I2 (12), I3 (13), O1 (21), W1 (31) and "
+                                       "W2 (32) on either x face, inflow on one at most");
   if (either(12) && !(b->t_in > 0.0)) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I2 inflow needs t_in > 0");
   if (c->geo.per[0] || b->xl == 0 || b->xr == 0)
     return fail(SENGA_ERR_ARG, "senga_set_nscbc: needs a bounded x direction and a kind on both x faces");
   if (either(13) && b->rho_in <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I3 inflow needs rho_in > 0");
   if (either(21) && b->p_inf <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an O1 outflow needs p_inf > 0");
+  if ((b->xl == 32 && !(b->t_wall[0] > 0.0)) || (b->xr == 32 && !(b->t_wall[1] > 0.0)))
+    return fail(SENGA_ERR_ARG, "senga_set_nscbc: a W2 wall needs its t_wall > 0");
   // the molar-mass, pressure and thermal-diffusion branches carry wall flux
   // terms of their own (rhscal.f:2116-, 2512-, 2925-, 3111-) not built here
-  if (either(31) && c->mixt)
-    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: a W1 wall runs with the base transport only "
+  if ((either(31) || either(32)) && c->mixt)
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: a W1/W2 wall runs with the base transport only "
                                        "(senga_set_transport switches off)");
   return guard([&] {
     NscbcParams& p = c->bc;
@@ -741,14 +743,18 @@ int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
     p.pio = b->pio;
     p.betloc = b->bet_local;
     p.t_in = b->t_in;
+    p.t_wall[0] = b->t_wall[0];
+    p.t_wall[1] = b->t_wall[1];
     // face-plane flags of src/bcinit.f:299-326,458-480,560-586,702-735: I3 ->
     // FxxCNV, FxxVSN, the plane imposed; I2 -> FxxCNV, all but the density
     // imposed; O1 -> FxxCNV, FxxVST, FxxCON, FxxADB, FxxDIF; W1 -> FxxCNV,
-    // FxxCON, FxxADB, FxxDIF, FxxCNW, FxxDFW, momentum not integrated
+    // FxxCON, FxxADB, FxxDIF, FxxCNW, FxxDFW, momentum not integrated; W2
+    // -> FxxCNV, FxxDIF, FxxDFW, momentum and energy not integrated
     auto bits = [](int kind) {
       return kind == 13   ? (BF_VSN | BF_NSCBC | BF_IMPOSED)
              : kind == 12 ? (BF_NSCBC | BF_IMPOSED_D)
              : kind == 31 ? (BF_CON | BF_DIF | BF_NSCBC | BF_WALL)
+             : kind == 32 ? (BF_DIF | BF_NSCBC | BF_WALL)
                           : (BF_VST | BF_CON | BF_DIF | BF_NSCBC);
     };
     c->geo.bxl = bits(b->xl);

@@ -57,7 +57,7 @@ enum : int {
   BF_NSCBC = 16,    // BOUNDS corrections are added to the plane's RHS
   BF_IMPOSED = 32,  // I3 inflow: D, U, V, W, Y are imposed, not integrated
   BF_IMPOSED_D = 64,  // I2 inflow: U, V, W, E, Y are imposed, only D integrated
-  BF_WALL = 128,      // W1 wall: U, V, W, E RHS zero; U, V, W not integrated
+  BF_WALL = 128,      // W1/W2 wall: U, V, W, E RHS zero; U, V, W not integrated (W2: nor E)
 };
 __host__ __device__ __forceinline__ int face_bits(const Geo& g, int gx) {
   return gx == 0 ? g.bxl : (gx == g.nx - 1 ? g.bxr : 0);
@@ -154,12 +154,13 @@ void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchu
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
 // NSCBC x faces (nscbc.cu): face kinds 0 (none), 12 (I2 inflow), 13 (I3
-// inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall) on either face,
-// and their parameters.
+// inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall), 32 (W2
+// isothermal no-slip wall) on either face, and their parameters.
 struct NscbcParams {
   int xl, xr;
   double u_in, rho_in, y_in[SENGA_NSPCMX];  // I3: RXLPRM(1), DRIN, YRIN
   double t_in;                              // I2: TRIN
+  double t_wall[2];                         // W2: RXLPRM(1), RXRPRM(1)
   double p_inf, cobc, bet, xlen;            // O1: PINFXR, COBCXR, BET, XGDLEN
   int pio, betloc;                          // O1: NXRPRM(1), NXRPRM(2)
 };
@@ -169,7 +170,7 @@ void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nsp
 // face data + BOUNDS corrections into f.face, after the thermochemistry kernel
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,
                  cudaStream_t s);
-// W1 walls: the wall diffusion-flux terms added to the species rate and VTMP
+// W1/W2 walls: the wall diffusion-flux terms added to the species rate and VTMP
 // (after the species kernel), and the wall temperature plus, when rk, the
 // zero-gradient mass fractions of the updated state (after the RK update)
 bool has_wall(const NscbcParams& bc);

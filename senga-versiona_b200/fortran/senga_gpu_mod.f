@@ -90,8 +90,9 @@ C     RADCIN's radiation tables (src/radcin.f:80-220)
         REAL(C_DOUBLE) :: TREFRN
       END TYPE
 C     NSCBC x faces: kinds 12 (I2 inflow), 13 (I3 inflow), 21 (O1
-C     outflow), 31 (W1 adiabatic no-slip wall) and parameters (T_IN:
-C     TRIN of an I2 inflow)
+C     outflow), 31 (W1 adiabatic no-slip wall), 32 (W2 isothermal
+C     no-slip wall) and parameters (T_IN: TRIN of an I2 inflow; T_WALL:
+C     RXLPRM(1), RXRPRM(1) of W2 walls)
       TYPE, BIND(C) :: SENGA_NSCBC
         INTEGER(C_INT) :: XL, XR
         REAL(C_DOUBLE) :: U_IN, RHO_IN
@@ -99,6 +100,7 @@ C     TRIN of an I2 inflow)
         REAL(C_DOUBLE) :: P_INF, SIGMA, ETA
         INTEGER(C_INT) :: PIO, BET_LOCAL
         REAL(C_DOUBLE) :: T_IN
+        REAL(C_DOUBLE) :: T_WALL(2)
       END TYPE
       INTERFACE
         INTEGER(C_INT) FUNCTION SENGA_CHEM_LOAD(PATH, CHEM)

@@ -97,7 +97,8 @@ class NscbcT(C.Structure):
 
     _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
                 ("y_in", C.c_double * NSPCMX), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
-                ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double)]
+                ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double),
+                ("t_wall", C.c_double * 2)]
 
 
 NCFRMX = 6
@@ -534,8 +535,9 @@ class Box:
 
     def set_nscbc(self, bc):
         """NSCBC x faces from a dict (xl, xr in {0, 12, 13, 21, 31}, u_in, rho_in,
-        y_in, p_inf, sigma, eta, pio, bet_local, t_in); 12 I2 inflow, 13 I3
-        inflow, 21 O1 outflow, 31 W1 adiabatic no-slip wall."""
+        y_in, p_inf, sigma, eta, pio, bet_local, t_in, t_wall); 12 I2 inflow,
+        13 I3 inflow, 21 O1 outflow, 31 W1 adiabatic no-slip wall, 32 W2
+        isothermal no-slip wall (t_wall: x-left, x-right temperatures)."""
         b = NscbcT()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
         b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
@@ -544,6 +546,7 @@ class Box:
         b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
         b.t_in = bc.get("t_in", 0.0)
+        b.t_wall[0], b.t_wall[1] = bc.get("t_wall", (0.0, 0.0))
         _check(lib.senga_set_nscbc(self.h, C.byref(b)), "senga_set_nscbc")
 
     def set_transport(self, mixw=False, mixp=False, soret=False, dufour=False, wmltdr=5.0):

@@ -1,19 +1,27 @@
-"""The W1 wall (NSBCW1, adiabatic no-slip): flags and integration ranges
-bcinit.f:702-735; wall state boundt.f:243-356 (x-left), 657-768 (x-right)
-and bountt.f:290-428, 767-; wave amplitudes bounds.f:917-1056, 1833-1974;
-wall flux terms rhscal.f:610-660 (FxxCNW) and 1698-1760 (FxxDFW); zero-
-gradient mass fractions lincom.f:171-210, fincom.f:171-210.
+"""The no-slip walls on the x faces.
+
+W1 (NSBCW1, adiabatic): flags and integration ranges bcinit.f:702-735; wall
+state boundt.f:243-356 (x-left), 657-768 (x-right) and bountt.f:290-428,
+767-; wave amplitudes bounds.f:917-1056, 1833-1974; wall flux terms
+rhscal.f:610-660 (FxxCNW) and 1698-1760 (FxxDFW); zero-gradient mass
+fractions lincom.f:171-210, fincom.f:171-210.
+W2 (NSBCW2, isothermal): flags and ranges bcinit.f:822-855; the wall
+temperature RXxPRM(1) imposed by boundt.f:358-470 and bountt.f:429-560 (and
+their x-right blocks); the same wave amplitudes (bounds.f:1058-1190, 1975-),
+wall diffusion flux and zero-gradient mass fractions as W1; neither momentum
+nor energy integrated on the wall.
 
 CPU (oracle): the mirror image of the two-wall box (x -> L - x, u -> -u) has
 the mirror image of the RHS and of the state after three steps; on the wall
 planes the momentum stays zero, the temperature is the fourth-order
-zero-gradient extrapolation of the four planes inward, every mass fraction
-the clipped extrapolation of the updated state, and the energy the
-internal energy at that temperature, while the density is integrated. The
-molar-mass, pressure and thermal-diffusion branches have wall terms of
-their own that are not restated, so both sides refuse them with a wall.
-GPU: two walls, and a wall with an O1 outflow opposite, against the oracle
-(RHS and three RK steps, field-normalised relative L-infinity 1e-10)."""
+zero-gradient extrapolation of the four planes inward (W1) or the imposed
+one (W2), every mass fraction the clipped extrapolation of the updated
+state, and the energy the internal energy at that temperature, while the
+density is integrated. The molar-mass, pressure and thermal-diffusion
+branches have wall terms of their own that are not restated, so both sides
+refuse them with a wall. GPU: two walls of either kind, a W1 and a W2 wall,
+and a wall with an O1 outflow opposite, against the oracle (RHS and three
+RK steps, field-normalised relative L-infinity 1e-10)."""
 import numpy as np
 import pytest
 
@@ -28,17 +36,21 @@ def _mirror(a):
     return m
 
 
-def _case(shape=(16, 8, 6), seed=5):
+TWALL = (760.0, 830.0)
+
+
+def _case(shape=(16, 8, 6), seed=5, kind=31):
     import cases
 
     c = cases.make_case("wall_box", seed=seed, shape=shape)
-    return c, dict(c["bc"])
+    return c, dict(c["bc"], xl=kind, xr=kind, t_wall=TWALL)
 
 
 def _mirrored(c, bc):
     cm = dict(c, fields=_mirror(c["fields"]), T=np.ascontiguousarray(c["T"][..., ::-1]),
               itn=np.ascontiguousarray(c["itn"][..., ::-1]))
-    return cm, dict(bc, xl=bc["xr"], xr=bc["xl"])
+    tw = bc.get("t_wall", (0.0, 0.0))
+    return cm, dict(bc, xl=bc["xr"], xr=bc["xl"], t_wall=(tw[1], tw[0]))
 
 
 def _oracle(c, bc):
@@ -50,8 +62,9 @@ def _oracle(c, bc):
     return o
 
 
-def test_w1_mirror_symmetry_in_the_oracle():
-    c, bc = _case()
+@pytest.mark.parametrize("kind", [31, 32], ids=["W1", "W2"])
+def test_wall_mirror_symmetry_in_the_oracle(kind):
+    c, bc = _case(kind=kind)
     cm, bcm = _mirrored(c, bc)
     ra, ta, _ = _oracle(c, bc).rhs()
     rb, tb, _ = _oracle(cm, bcm).rhs()
@@ -68,11 +81,12 @@ def test_w1_mirror_symmetry_in_the_oracle():
         assert rel_linf(fb[fl], _mirror(fa)[fl]) <= 1e-12, fl
 
 
-def test_w1_wall_planes_after_steps():
+@pytest.mark.parametrize("kind", [31, 32], ids=["W1", "W2"])
+def test_wall_planes_after_steps(kind):
     import cases
     from oracle import OracleChem
 
-    c, bc = _case()
+    c, bc = _case(kind=kind)
     o = _oracle(c, bc)
     r, _, _ = o.rhs()
     for fl in (1, 2, 3, 4):  # BOUNDS: momentum and energy RHS vanish on the walls
@@ -87,9 +101,13 @@ def test_w1_wall_planes_after_steps():
         assert np.max(np.abs(d - c["fields"][0][..., w])) > 0.0  # the density is integrated
         for fl in (1, 2, 3):
             assert np.max(np.abs(f[fl][..., w])) == 0.0
-        tt = [t[..., w + k * st] for k in range(1, 5)]
-        tw = (48.0 * tt[0] - 36.0 * tt[1] + 16.0 * tt[2] - 3.0 * tt[3]) / 25.0
-        assert np.array_equal(t[..., w], tw)
+        if kind == 31:
+            tt = [t[..., w + k * st] for k in range(1, 5)]
+            tw = (48.0 * tt[0] - 36.0 * tt[1] + 16.0 * tt[2] - 3.0 * tt[3]) / 25.0
+            assert np.array_equal(t[..., w], tw)
+        else:  # TRUN keeps TEMPER's value, converged onto the imposed temperature
+            tw = np.full_like(d, TWALL[0 if w == 0 else 1])
+            assert np.allclose(t[..., w], tw, rtol=0, atol=1e-6)
         y = f[5:] / f[0]
         yy = [y[:, ..., w + k * st] for k in range(1, 5)]
         yw = np.float32(12.0 / 25.0).astype(np.float64) * (
@@ -103,7 +121,7 @@ def test_w1_wall_planes_after_steps():
         assert rel_linf(f[4][..., w], e) <= 1e-13
 
 
-def test_w1_refuses_the_transport_branches_without_restated_wall_terms():
+def test_walls_refuse_the_transport_branches_without_restated_wall_terms():
     from oracle import Oracle
 
     c, bc = _case()
@@ -115,16 +133,19 @@ def test_w1_refuses_the_transport_branches_without_restated_wall_terms():
     o2.set_transport(soret=True)
     with pytest.raises(RuntimeError, match="W1"):
         o2.set_bc(bc)
+    with pytest.raises(RuntimeError, match="W2"):
+        o2.set_bc(dict(bc, xl=32, xr=32))
 
 
-CASES = [("walls", dict(xl=31, xr=31)), ("wall-outflow", dict(xl=31, xr=21, p_inf=101325.0, sigma=0.287,
-                                                                      eta=1.0e-3))]
+O1 = dict(p_inf=101325.0, sigma=0.287, eta=1.0e-3)
+CASES = [("W1-W1", dict(xl=31, xr=31)), ("W1-O1", dict(xl=31, xr=21, **O1)), ("W2-W2", dict(xl=32, xr=32)),
+         ("W2-W1", dict(xl=32, xr=31)), ("W2-O1", dict(xl=32, xr=21, **O1))]
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,faces", CASES, ids=[n for n, _ in CASES])
 @pytest.mark.parametrize("mirrored", [False, True], ids=["as-is", "mirrored"])
-def test_gpu_w1_matches_oracle(name, faces, mirrored):
+def test_gpu_walls_match_oracle(name, faces, mirrored):
     import senga
 
     c, bc = _case(shape=(24, 10, 8), seed=9)
@@ -153,3 +174,24 @@ def test_gpu_w1_matches_oracle(name, faces, mirrored):
         assert rel_linf(g[fl], o[fl]) <= TOL, f"state field {fl}"
     assert rel_linf(tg, to) <= TOL
     assert np.array_equal(ig, io)
+
+
+@pytest.mark.gpu
+def test_gpu_wall_refusals():
+    """A W2 face without its temperature, and a wall together with the
+    transport switches (in either order), are refused by the library."""
+    import senga
+
+    c, bc = _case(shape=(16, 8, 6), kind=32)
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(c["diff"], chem)
+    box = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"], nend=c["nend"])
+    with pytest.raises(RuntimeError, match="t_wall"):
+        box.set_nscbc(dict(bc, t_wall=(0.0, 800.0)))
+    box.set_nscbc(bc)
+    with pytest.raises(RuntimeError, match="base transport"):
+        box.set_transport(mixw=True)
+    box2 = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"], nend=c["nend"])
+    box2.set_transport(soret=True)
+    with pytest.raises(RuntimeError, match="base transport"):
+        box2.set_nscbc(dict(bc, xl=31, xr=31))
