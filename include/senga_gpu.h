@@ -477,9 +477,11 @@ int senga_server_set_max_points(senga_server* s, int64_t max_points);
  * Periodic boxes of any extent (one point in the unused directions of 1D and
  * 2D runs). A box needs (14 + 4*nspec)*8 bytes of scratch per grid point;
  * larger boxes are rejected with SENGA_ERR_ARG. Every call reuses the same
- * array, so calls that overlap on the GPU race. The first call on a device
- * (with it current) looks up the array's device address; make it before any
- * stream capture. Under CUDA's lazy module loading (the default) that first
+ * array, so calls that overlap on the GPU race. The tables are copied from
+ * the host structs at every call, so the call cannot be captured into a CUDA
+ * graph: on a capturing stream it returns SENGA_ERR_UNSUPPORTED and queues
+ * nothing. The first call on a device (with it current) looks up the
+ * array's device address. Under CUDA's lazy module loading (the default) that first
  * call is also when the array and the kernels' code are loaded onto the
  * device: a host that reserves all free device memory at start-up makes one
  * call per device before it does (or sets CUDA_MODULE_LOADING=EAGER). */

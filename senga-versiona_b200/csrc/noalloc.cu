@@ -114,11 +114,20 @@ extern "C" int senga_rhs_noalloc(const senga_config* cfg, const senga_chem* chem
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return senga::fail(SENGA_ERR_ARG, "senga_rhs_noalloc: device ordinal too large");
+  cudaStream_t s = (cudaStream_t)stream;
+  // the tables go up from pageable host memory on every call: a captured
+  // copy node would read the caller's host structs again at each replay,
+  // so the call refuses to be captured (checked before the first call's
+  // symbol lookup, which a capture would not allow either)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return senga::fail(SENGA_ERR_CUDA, std::string("senga_rhs_noalloc: ") + cudaGetErrorString(e));
+  if (cap != cudaStreamCaptureStatusNone)
+    return senga::fail(SENGA_ERR_UNSUPPORTED, "senga_rhs_noalloc: the call cannot be captured into a CUDA graph");
   DevicePtrs ptr;
   int rc = setup(dev, ptr);
   if (rc != SENGA_OK) return rc;
 
-  cudaStream_t s = (cudaStream_t)stream;
   const senga_diff& dz = diff ? *diff : kNoDiff;
   e = cudaMemcpyAsync(ptr.chem, chem, sizeof(senga_chem), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ptr.diff, &dz, sizeof(senga_diff), cudaMemcpyHostToDevice, s);

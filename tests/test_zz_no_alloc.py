@@ -123,3 +123,35 @@ def test_rhs_noalloc_requires_a_status_word():
     rc = senga.lib.senga_rhs_noalloc(C.byref(cfg), C.byref(chem.t), None, 1, 1, 1, 1, None, None)
     assert rc == 1
     assert b"null argument" in senga.lib.senga_last_error()
+
+
+def test_rhs_noalloc_refuses_stream_capture():
+    """The tables are copied from host structs at every call, so the call
+    refuses a capturing stream with SENGA_ERR_UNSUPPORTED and queues
+    nothing (the capture ends cleanly, with an empty graph)."""
+    import warnings
+
+    import torch
+
+    import cases
+    import senga
+
+    chem = senga.Chem(cases.CHEM_1STEP)
+    cfg = senga.ConfigT()
+    cfg.nx = cfg.ny = cfg.nz = 16
+    cfg.xgdlen = cfg.ygdlen = cfg.zgdlen = 1e-3
+    for i in range(6):
+        cfg.nend[i] = senga.NPERI
+    cfg.tstep = 1e-9
+    dev = torch.device("cuda", 0)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    side = torch.cuda.Stream(dev)
+    g = torch.cuda.CUDAGraph()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")  # the empty-graph warning
+        with torch.cuda.graph(g, stream=side):
+            rc = senga.lib.senga_rhs_noalloc(C.byref(cfg), C.byref(chem.t), None, 1, 1, 1, 1, status.data_ptr(),
+                                             side.cuda_stream)
+    assert rc == 5
+    assert b"captured" in senga.lib.senga_last_error()
+    torch.cuda.synchronize(dev)
