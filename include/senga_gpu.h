@@ -176,7 +176,10 @@ int senga_fp64_peak(int device, double* tflops);
 /* Status word of the last steps: bit 0 = TEMPER non-convergence; bit 1 =
  * TEMPIN found no sign change of the energy residual in [200, 3000] K (the
  * reference stops there); bit 2 = TEMPIN still unconverged after 200
- * bisections (the reference bisects without limit). */
+ * bisections (the reference bisects without limit); bit 3 = a stencil tile's
+ * bulk copies did not land within about a second (the tile's results are
+ * not written); bit 4 = a wait of the persistent batch kernel ran out (the
+ * launch was abandoned). */
 int senga_get_status(senga_ctx* ctx, int* status);
 
 /* ---- operator-level entry points (unit parity) -----------------------------
@@ -416,13 +419,22 @@ int senga_post_read(const char* path, int nx, int ny, int nz, int nspec, int nsp
 /* ---- batched ensembles --------------------------------------------------------
  * No counterpart in the reference (it runs one box per MPI job). Many
  * independent periodic boxes of uneven sizes, one mechanism, each with its own
- * dt (cfgs[i].tstep): per substage, one launch per kernel family for every 64
- * boxes, over a device work-list of (box, tile) items (stencil kernels: one
- * CTA per item; pointwise kernel: a persistent grid striding over 256-point
- * chunks); the RK step is captured once as a CUDA graph.
- * senga_batch_autotune times candidate persistent grid sizes of the pointwise
- * kernel on the uploaded state (saved and restored) and keeps the fastest;
- * it reports that grid and the number of stencil CTAs per launch. */
+ * dt (cfgs[i].tstep). A substage runs in one of two forms, per table of up to
+ * 64 boxes: one persistent launch whose resident CTAs take every box's
+ * thermochemistry chunks, flow, species and species+RK tiles from one
+ * phase-major device work list (each phase of a box starts when the box's
+ * previous phase has completed; bounded waits, status bit 4 on time-out), or
+ * four launches (a pointwise kernel striding over 256-point chunks, then one
+ * CTA per (box, tile) item for each stencil kernel). The RK step is captured
+ * once as a CUDA graph. senga_batch_autotune times one RK step of the
+ * uploaded state (saved and restored) for each candidate (the persistent
+ * kernel at 1..k resident CTAs per SM, the four launches at several pointwise
+ * grid sizes) and keeps the fastest; it reports the number of stencil CTAs
+ * per launch of the four-launch form and the pointwise grid; senga_batch_form
+ * reports the form in use (persistent = 1) and its grid. SENGA_BATCH=persist
+ * or =launches in the environment (read at senga_batch_create) keeps the
+ * batch, and its autotuner, to one form; unset, the four launches run until
+ * the autotuner picks. */
 typedef struct senga_batch senga_batch;
 int senga_batch_create(int nbox, const senga_config* cfgs, const senga_chem* chem, const senga_diff* diff,
                        int device, senga_batch** out);
@@ -432,6 +444,7 @@ int senga_batch_upload_host(senga_batch* b, int ibox, const double* fields, cons
 int senga_batch_download_host(senga_batch* b, int ibox, double* fields, double* trun, int32_t* itndex);
 int senga_batch_step(senga_batch* b, int nsteps);
 int senga_batch_autotune(senga_batch* b, int* grid_stencil, int* grid_thermo);
+int senga_batch_form(senga_batch* b, int* persistent, int* grid);
 int senga_batch_sync(senga_batch* b);
 void* senga_batch_stream(senga_batch* b);
 int senga_batch_status(senga_batch* b, int* status);

@@ -4,11 +4,19 @@
 // share one mechanism. All their fields live in one HBM arena (first-fit
 // allocator over a single device allocation); each box has a descriptor
 // (geometry, field pointers, the five RK coefficient triples of its own dt).
-// One RK substage of the whole ensemble is four persistent launches: the
-// pointwise thermochemistry over (box, 256-point chunk) items and the three
-// stencil kernels over (box, tile) items; a full RK step (20 launches) is
-// captured once as a CUDA graph and replayed. An autotuner times candidate
-// persistent grid sizes on the live ensemble and keeps the fastest.
+// One RK substage of the whole ensemble runs in one of two forms:
+//   * persistent: one launch per substage (per table of up to 64 boxes) of
+//     the kernel of persist.cu, whose resident CTAs take the thermochemistry
+//     chunks and the flow, species and species+RK tiles of every box from one
+//     phase-major work list, each phase of a box starting when the box's
+//     previous phase has completed;
+//   * four launches: the pointwise thermochemistry over (box, 256-point
+//     chunk) items and the three stencil kernels over (box, tile) items.
+// The RK step (five substages) is captured once as a CUDA graph and
+// replayed. The autotuner times one RK step of the live ensemble for each
+// candidate (the persistent kernel at 1..k resident CTAs per SM; the four
+// launches at several thermochemistry grid sizes) and keeps the fastest;
+// SENGA_BATCH=persist or =launches restricts it to one form.
 //
 // The serving loop (senga_server_*) keeps an Ensemble whose membership
 // changes between RK steps: requests are admitted as soon as the arena has
@@ -20,6 +28,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -155,6 +164,8 @@ class Ensemble {
   Arena arena;
   std::vector<Member*> active;
   int grid_stencil = 0, grid_thermo = 0;
+  bool persist = false;  // one persistent launch per substage
+  int grid_persist = 0;
 
   void init(const senga_chem& c, const senga_diff* d, int dev, size_t arena_bytes) {
     chem = c;
@@ -177,12 +188,20 @@ class Ensemble {
     CKE(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     sms_ = sms;
     grid_thermo = 4 * sms;
+    persist_occ_ = std::max(1, persist_ctas_per_sm(mech, nspec, diff.flmavt));
+    grid_persist = persist_occ_ * sms;
+    const char* e = std::getenv("SENGA_BATCH");
+    form_ = e ? std::string(e) : std::string();
+    persist = form_ == "persist";
   }
   void destroy() {
     drop_graph();
     if (stream) cudaStreamSynchronize(stream);
     cudaFree(d_items_);
     cudaFree(d_chunks_);
+    cudaFree(d_pitems_);
+    cudaFree(d_need_);
+    cudaFree(d_ctr_);
     cudaFree(d_chem);
     cudaFree(d_diff);
     cudaFree(d_status);
@@ -302,12 +321,48 @@ class Ensemble {
       grid_stencil = (int)items.size();
       gr.nchunks = (int)chunks.size() - gr.chunk0;
     }
+    // persistent form: per table, the chunks then three copies of the tiles
+    // (flow, species, species+RK), and the items of every (box, phase)
+    std::vector<WorkItem> pitems;
+    std::vector<int> need((size_t)groups_.size() * 4 * kTableBoxes, 0);
+    for (size_t gi = 0; gi < groups_.size(); ++gi) {
+      Group& gr = groups_[gi];
+      gr.pitem0 = (int)pitems.size();
+      gr.poff[0] = 0;
+      for (int c = 0; c < gr.nchunks; ++c) pitems.push_back(chunks[gr.chunk0 + c]);
+      for (int ph = 1; ph < 4; ++ph) {
+        gr.poff[ph] = (int)pitems.size() - gr.pitem0;
+        for (int k = 0; k < gr.nitems; ++k) pitems.push_back(items[gr.item0 + k]);
+      }
+      gr.poff[4] = (int)pitems.size() - gr.pitem0;
+      int* nd = need.data() + gi * 4 * kTableBoxes;
+      for (int c = 0; c < gr.nchunks; ++c) ++nd[4 * chunks[gr.chunk0 + c].box];
+      for (int k = 0; k < gr.nitems; ++k)
+        for (int ph = 1; ph < 4; ++ph) ++nd[4 * items[gr.item0 + k].box + ph];
+    }
     upload_vec(items, &d_items_, &cap_items_);
     upload_vec(chunks, &d_chunks_, &cap_chunks_);
+    upload_vec(pitems, &d_pitems_, &cap_pitems_);
+    upload_vec(need, &d_need_, &cap_need_);
+    std::vector<int> zeros((size_t)groups_.size() * kPersistCounters, 0);
+    upload_vec(zeros, &d_ctr_, &cap_ctr_);
     CKE(cudaStreamSynchronize(stream));
   }
   void substage(int irk) {
     if (active.empty()) return;
+    if (persist) {
+      for (size_t gi = 0; gi < groups_.size(); ++gi) {
+        const Group& gr = groups_[gi];
+        PersistArgs a{};
+        a.items = d_pitems_ + gr.pitem0;
+        for (int k = 0; k < 5; ++k) a.off[k] = gr.poff[k];
+        a.need = d_need_ + gi * 4 * kTableBoxes;
+        a.ctr = d_ctr_ + gi * kPersistCounters;
+        a.irk = irk - 1;
+        launch_batch_persist(*gr.table, a, grid_persist, mech, d_chem, d_diff, nspec, diff.flmavt, stream);
+      }
+      return;
+    }
     for (const Group& gr : groups_)
       launch_batch_thermo(*gr.table, d_chunks_ + gr.chunk0, gr.nchunks, std::min(grid_thermo, gr.nchunks), mech,
                           d_chem, d_diff, nspec, diff.flmavt, stream);
@@ -328,9 +383,10 @@ class Ensemble {
     for (int s = 0; s < nsteps; ++s) CKE(cudaGraphLaunch(graph_, stream));
     CKE(cudaGetLastError());
   }
-  // Times one RK step per candidate persistent grid of the pointwise kernel
-  // on the live ensemble (state saved and restored) and keeps the fastest.
-  // The stencil kernels launch one CTA per tile and have nothing to tune.
+  // Times one RK step per candidate on the live ensemble (state saved and
+  // restored) and keeps the fastest: the persistent kernel at 1..k resident
+  // CTAs per SM (k its occupancy), the four launches at 2..32 pointwise CTAs
+  // per SM (their stencil kernels launch one CTA per tile).
   void autotune() {
     if (active.empty()) return;
     // save registers, T and ITNDEX of every member
@@ -350,11 +406,21 @@ class Ensemble {
     cudaEvent_t e0, e1;
     CKE(cudaEventCreate(&e0));
     CKE(cudaEventCreate(&e1));
-    const int th_opts[] = {2, 4, 8, 16, 32};
+    struct Cand {
+      bool persist;
+      int grid;
+    };
+    std::vector<Cand> cands;
+    if (form_ != "launches")
+      for (int k = 1; k <= persist_occ_; ++k) cands.push_back(Cand{true, k * sms_});
+    if (form_ != "persist")
+      for (int t : {2, 4, 8, 16, 32}) cands.push_back(Cand{false, t * sms_});
     float best = 1e30f;
-    int bth = grid_thermo;
-    for (int t : th_opts) {
-      grid_thermo = t * sms_;
+    Cand win = cands.front();
+    for (const Cand& cd : cands) {
+      persist = cd.persist;
+      if (cd.persist) grid_persist = cd.grid;
+      else grid_thermo = cd.grid;
       for (int irk = 1; irk <= 5; ++irk) substage(irk);  // warm
       CKE(cudaEventRecord(e0, stream));
       for (int irk = 1; irk <= 5; ++irk) substage(irk);
@@ -364,10 +430,12 @@ class Ensemble {
       CKE(cudaEventElapsedTime(&ms, e0, e1));
       if (ms < best) {
         best = ms;
-        bth = grid_thermo;
+        win = cd;
       }
     }
-    grid_thermo = bth;
+    persist = win.persist;
+    if (win.persist) grid_persist = win.grid;
+    else grid_thermo = win.grid;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     for (size_t k = 0; k < active.size(); ++k) {
@@ -401,14 +469,20 @@ class Ensemble {
     CKE(cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
   }
   int sms_ = 148;
+  int persist_occ_ = 1;
+  std::string form_;  // SENGA_BATCH: "persist", "launches" or empty (both)
   struct Group {
     std::unique_ptr<BoxTable> table;
     int item0 = 0, nitems = 0, chunk0 = 0, nchunks = 0;
+    int pitem0 = 0, poff[5] = {};
   };
   std::vector<Group> groups_;
   WorkItem* d_items_ = nullptr;
   WorkItem* d_chunks_ = nullptr;
-  size_t cap_items_ = 0, cap_chunks_ = 0;
+  WorkItem* d_pitems_ = nullptr;
+  int* d_need_ = nullptr;
+  int* d_ctr_ = nullptr;
+  size_t cap_items_ = 0, cap_chunks_ = 0, cap_pitems_ = 0, cap_need_ = 0, cap_ctr_ = 0;
   cudaGraphExec_t graph_ = nullptr;
 };
 
@@ -509,6 +583,13 @@ int senga_batch_autotune(senga_batch* b, int* grid_stencil, int* grid_thermo) {
     if (grid_stencil) *grid_stencil = b->ens.grid_stencil;
     if (grid_thermo) *grid_thermo = b->ens.grid_thermo;
   });
+}
+
+int senga_batch_form(senga_batch* b, int* persistent, int* grid) {
+  if (!b) return fail(SENGA_ERR_ARG, "senga_batch_form: null batch");
+  if (persistent) *persistent = b->ens.persist ? 1 : 0;
+  if (grid) *grid = b->ens.persist ? b->ens.grid_persist : b->ens.grid_thermo;
+  return SENGA_OK;
 }
 
 int senga_batch_sync(senga_batch* b) {

@@ -18,6 +18,9 @@ struct Error : std::runtime_error {
 // Records the message as the thread's last error and returns the code.
 int fail(int code, const std::string& msg);
 
+// THRD, TTHD, FTHD of the reference (1/3, 2/3, 4/3 formed as it forms them)
+constexpr double kThrd = 1.0 / 3.0, kTthd = 2.0 * kThrd, kFthd = 2.0 * kTthd;
+
 // Field slots of the conserved register (reference: DRHS,URHS,VRHS,WRHS,ERHS,
 // YRHS(:,:,:,k)).
 enum : int { F_RHO = 0, F_RU = 1, F_RV = 2, F_RW = 3, F_RE = 4, F_Y0 = 5 };
@@ -123,6 +126,24 @@ struct BoxTable {
 };
 static_assert(sizeof(BoxTable) + 256 <= 32764, "a kernel's parameters are limited to 32764 bytes");
 
+// One persistent launch per RK substage of a batch (persist.cu): the
+// phase-major work list of one table's boxes (thermochemistry chunks, flow
+// tiles, species tiles, species+RK tiles), where each phase starts (off[0..3];
+// off[4] = total), the items of each (box, phase) pair, and the launch's
+// counters ([0] dispenser, [1] abort flag, [2 + 4 box + phase] completed
+// items), which the launcher zeroes on the stream before the kernel.
+constexpr int kPersistCounters = 2 + 4 * kTableBoxes;
+struct PersistArgs {
+  const WorkItem* items;
+  int off[5];
+  const int* need;  // [4 * box + phase]
+  int* ctr;         // kPersistCounters ints
+  int irk;          // substage, 0-based
+};
+static_assert(sizeof(BoxTable) + sizeof(PersistArgs) + 64 <= 32764, "persistent launch parameters");
+// status bit of a persistent launch whose dependency wait ran out
+constexpr unsigned kStatusPersistTimeout = 16u;
+
 // Launchers (kernels.cu).
 // Mechanism-specialised thermochemistry: 0 = table-driven (any chem.dat),
 // otherwise the id of a generated policy whose constants equal the loaded
@@ -151,6 +172,10 @@ void launch_batch_thermo(const BoxTable& boxes, const WorkItem* chunks, int nchu
                          const senga_chem* dchem, const senga_diff* ddiff, int nspec, int flmavt, cudaStream_t s);
 // Flow, species and species+RK phases of substage irk (0-based), one CTA per
 // work item; `phase` selects one of them (0, 1, 2) or all three (-1).
+// resident CTAs per SM of the persistent kernel for a mechanism (occupancy)
+int persist_ctas_per_sm(int mech, int nspec, int flmavt);
+void launch_batch_persist(const BoxTable& boxes, const PersistArgs& a, int grid, int mech, const senga_chem* dchem,
+                          const senga_diff* ddiff, int nspec, int flmavt, cudaStream_t s);
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
 // NSCBC x faces (nscbc.cu): face kinds 0 (none), 12 (I2 inflow), 13 (I3

@@ -277,20 +277,37 @@ __device__ __forceinline__ double DM(const Geo& g, const Pt& p, const F& f) {
 }
 
 // ---- accessors ----
-struct Ld {
-  const double* __restrict__ a;
-  __device__ __forceinline__ double operator()(int64_t q) const { return __ldg(a + q); }
+// Field loads of the stencil kernels. NC = true: through the read-only data
+// path (ld.global.nc), for launches in which no CTA writes the field. The
+// persistent batch kernel reads fields that other CTAs of the same launch
+// wrote (behind an acquire on a completion counter), so it takes NC = false:
+// ordinary (coherent) global loads, cached in L1, which the acquire of the
+// completion counter orders after the producers' writes.
+template <bool NC>
+__device__ __forceinline__ double ldf(const double* p) {
+  if constexpr (NC) return __ldg(p);
+  else return __ldca(p);  // ld.global.ca: global space, cached in L1, coherent
+}
+template <bool NC = true>
+struct LdT {
+  const double* a;
+  __device__ __forceinline__ double operator()(int64_t q) const { return ldf<NC>(a + q); }
 };
-struct LdMul {
-  const double* __restrict__ a;
-  const double* __restrict__ b;
-  __device__ __forceinline__ double operator()(int64_t q) const { return __ldg(a + q) * __ldg(b + q); }
+template <bool NC = true>
+struct LdMulT {
+  const double* a;
+  const double* b;
+  __device__ __forceinline__ double operator()(int64_t q) const { return ldf<NC>(a + q) * ldf<NC>(b + q); }
 };
-struct LdSub {
-  const double* __restrict__ a;
+template <bool NC = true>
+struct LdSubT {
+  const double* a;
   double c;
-  __device__ __forceinline__ double operator()(int64_t q) const { return __ldg(a + q) - c; }
+  __device__ __forceinline__ double operator()(int64_t q) const { return ldf<NC>(a + q) - c; }
 };
+using Ld = LdT<true>;
+using LdMul = LdMulT<true>;
+using LdSub = LdSubT<true>;
 
 __device__ __forceinline__ Pt point_of(const Geo& g, int64_t q) {
   Pt p;

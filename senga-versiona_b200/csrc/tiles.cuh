@@ -210,8 +210,8 @@ template <class F>
 struct PlainLoad {
   static constexpr bool value = false;
 };
-template <>
-struct PlainLoad<Ld> {
+template <bool NC>
+struct PlainLoad<LdT<NC>> {
   static constexpr bool value = true;
 };
 

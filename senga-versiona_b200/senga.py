@@ -175,6 +175,7 @@ def _load():
         "senga_batch_download_host": (ip, [vp, ip, dp, dp, i32p]),
         "senga_batch_step": (ip, [vp, ip]),
         "senga_batch_autotune": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "senga_batch_form": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "senga_batch_sync": (ip, [vp]),
         "senga_batch_stream": (vp, [vp]),
         "senga_batch_status": (ip, [vp, C.POINTER(C.c_int)]),
@@ -682,7 +683,14 @@ class Batch:
     def autotune(self):
         a, b = C.c_int(), C.c_int()
         _check(lib.senga_batch_autotune(self.h, C.byref(a), C.byref(b)), "senga_batch_autotune")
-        return {"grid_stencil": a.value, "grid_thermo": b.value}
+        return dict(grid_stencil=a.value, grid_thermo=b.value, **self.form())
+
+    def form(self):
+        """The substage form in use: persistent (one launch per substage and
+        table of 64 boxes) or four launches, and its grid."""
+        p, g = C.c_int(), C.c_int()
+        _check(lib.senga_batch_form(self.h, C.byref(p), C.byref(g)), "senga_batch_form")
+        return {"persistent": bool(p.value), "grid": g.value}
 
     @property
     def stream(self):

@@ -218,3 +218,23 @@ def run_serve(nreq=2000, rate=20.0, seed=2024, device=0, arena_frac=0.6, max_poi
             "busy_gpsu_s": gpsu / max(1e-9, wall - reqs[0]["t"]), "sequential_gpsu_s": gpsu / t_seq,
             "sequential_s": t_seq, "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_latency_s": float(lat.mean()), "arena_bytes": arena, "max_points_per_tick": max_points}
+
+
+if __name__ == "__main__":
+    # python senga-versiona_b200/workloads.py ensemble [steps] [persist|launches|auto]
+    import json
+    import os
+    import sys
+
+    what = sys.argv[1] if len(sys.argv) > 1 else "ensemble"
+    if what != "ensemble":
+        raise SystemExit("usage: workloads.py ensemble [steps] [persist|launches|auto]")
+    nsteps = int(sys.argv[2]) if len(sys.argv) > 2 else 20
+    form = sys.argv[3] if len(sys.argv) > 3 else "auto"
+    if form == "auto":
+        os.environ.pop("SENGA_BATCH", None)
+    else:
+        os.environ["SENGA_BATCH"] = form
+    r = run_ensemble(steps=nsteps, warmup=3)
+    print(json.dumps({"form": form, **{k: r[k] for k in ("batched_gpsu_s", "sequential_gpsu_s", "speedup",
+                                                          "autotune", "status_word", "boxes", "points")}}))

@@ -35,9 +35,16 @@ def _alone(c, chem, diff, nsteps):
     return box.download()
 
 
-def test_batch_matches_boxes_run_alone():
+@pytest.mark.parametrize("form", ["persist", "launches", "auto"])
+def test_batch_matches_boxes_run_alone(form, monkeypatch):
+    """Both substage forms (one persistent launch, or four launches), and the
+    one the autotuner picks."""
     import senga
 
+    if form != "auto":
+        monkeypatch.setenv("SENGA_BATCH", form)
+    else:
+        monkeypatch.delenv("SENGA_BATCH", raising=False)
     cs = _ensemble_cases()
     chem = senga.Chem(cs[0]["chem"])
     diff = senga.Diff(None, chem)
@@ -45,9 +52,12 @@ def test_batch_matches_boxes_run_alone():
     for i, c in enumerate(cs):
         b.upload(i, c["fields"], c["T"], c["itn"])
     tuned = b.autotune()
-    assert tuned["grid_stencil"] > 0 and tuned["grid_thermo"] > 0
+    assert tuned["grid_stencil"] > 0 and tuned["grid_thermo"] > 0 and tuned["grid"] > 0
+    if form != "auto":
+        assert tuned["persistent"] == (form == "persist")
     b.step(2)
     b.sync()
+    assert b.status() == 0
     for i, c in enumerate(cs):
         got, tg, _ = b.download(i)
         want, tw, _ = _alone(c, chem, diff, 2)
@@ -56,12 +66,16 @@ def test_batch_matches_boxes_run_alone():
         assert rel_linf(tg, tw) <= TOL
 
 
-def test_server_results_equal_alone_and_in_the_mix():
+@pytest.mark.parametrize("form", ["persist", "launches"])
+def test_server_results_equal_alone_and_in_the_mix(form, monkeypatch):
     """Requests of different sizes and lengths, an arena that holds only a
     few boxes at a time: requests wait for room, are batched while running,
-    and each result equals the same request run alone."""
+    and each result equals the same request run alone (either substage
+    form)."""
     import senga
     import cases
+
+    monkeypatch.setenv("SENGA_BATCH", form)
 
     reqs = []
     for k, (seed, n, nsteps) in enumerate(((31, 16, 3), (32, 24, 1), (33, 16, 2), (34, 20, 4), (35, 16, 2))):
