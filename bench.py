@@ -68,7 +68,10 @@ def kernel_bytes_per_point(nspec, adaptive=False):
     flow = 8 * (4 + 3 + 1 + 1 + 1 + 1 + 1) + 8 * (5 + 1)
     species_a = 8 * (3 + 1 + 1 + 4 * S) + 8 * (S + 3 + 1 + 1)
     species_b = 8 * (3 + 1 + 5 + 1 + 2 * S + nc) + 8 * (2 * nc) + (16 * nc if adaptive else 0)
-    return {"thermo": thermo, "flow": flow, "species_a": species_a, "species_b_rk": species_b}
+    # the two species kernels as one: reads rho u, rho v, rho w, the flow RHS
+    # (5), DIVM, Y_k, rho D_k, h_k, the CHRATE rate, h_mix, S; writes S and U
+    species = 8 * (3 + 5 + 1 + 4 * S + 1 + nc) + 8 * (2 * nc) + (16 * nc if adaptive else 0)
+    return {"thermo": thermo, "flow": flow, "species_a": species_a, "species_b_rk": species_b, "species": species}
 
 
 class Clocks:
@@ -246,6 +249,7 @@ def main():
     box.upload(c["fields"], c["T"], c["itn"])
     npts = c["shape"][0] * c["shape"][1] * c["shape"][2]
     workload["thermochemistry_kernel"] = {0: "table-driven", 1: "generated 1-step", 2: "generated H2"}[box.info()["mech"]]
+    workload["species_kernels"] = "fused: one launch per substage" if box.species_fused() else "separate"
 
     def barrier():
         if world > 1:
@@ -357,7 +361,7 @@ def main():
         ach = kb[k] * npts / (launch_ms / 1e3) / 1e9
         kern[k] = {"ms_per_launch": launch_ms, "share": t_ms / tot, "alg_bytes_per_point": kb[k],
                    "achieved_gbs": ach, "frac_hbm": ach / hbm}
-    stencil = max(("flow", "species_a", "species_b_rk"), key=lambda k: prof[k])
+    stencil = max((k for k in ("flow", "species_a", "species_b_rk", "species") if k in prof), key=lambda k: prof[k])
     dom = max(prof, key=prof.get)
     rk = kern[stencil]
     tpp = dram_traffic_per_point().get(stencil)

@@ -160,8 +160,16 @@ int senga_rhs_host(senga_ctx* ctx, double* rhs, double* trun, double* prun);
 /* One RK step (5 substages) with CUDA events around every kernel launch on
  * the context's stream; ms[4] receives the summed time of the four kernel
  * families (thermo, flow, species_a, species_b+RK), *launches their count.
+ * With the species kernels fused (senga_ctx_species_fused) the one species
+ * launch is timed as species_a and ms[3] holds only the face kernels, if any.
  * Advances the state like senga_step(ctx, 1). */
 int senga_profile_step(senga_ctx* ctx, double* ms, int* launches);
+/* *fused_kernels = 1 when the context runs the species kernel and the
+ * species+RK kernel as one launch per substage: all-periodic boxes without
+ * the transport switches when SENGA_FUSE=1 is set (the rates, correction
+ * velocity, VTMP and energy RHS then stay on chip between the two passes;
+ * off by default, since the two kernels measure faster). */
+int senga_ctx_species_fused(senga_ctx* ctx, int* fused_kernels);
 
 /* Context facts: *mech = thermochemistry kernel in use (0 table-driven, 1 the
  * generated one-step R->P kernel, 2 the generated H2/air kernel), and the

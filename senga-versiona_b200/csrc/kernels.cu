@@ -44,10 +44,12 @@ __global__ void __launch_bounds__(kBlock, ThermoOcc<M>::blocks) k_thermo(Geo g, 
   if (q >= g.n) return;
   thermo_point(g, f, m, q);
 }
-// The two halves of the thermochemistry: PART 1 at two blocks per SM (the
-// mixture-averaged transport needs ~128 registers), PART 2 (CHRATE) at three.
+// The two halves of the thermochemistry: PART 1 at three blocks per SM (the
+// mixture-averaged transport wants ~128 registers; at 80 it spills some, and
+// the extra warps still win: 5.17 against 5.35 ms per substage on the 256^3
+// H2 box), PART 2 (CHRATE) at three.
 #ifndef SENGA_THERMO_P1_MINB
-#define SENGA_THERMO_P1_MINB 2
+#define SENGA_THERMO_P1_MINB 3
 #endif
 #ifndef SENGA_THERMO_P2_MINB
 #define SENGA_THERMO_P2_MINB 3

@@ -58,10 +58,25 @@ __global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB)
                         &bar, &tm);
 }
 
+// Species pass and species+RK pass of one tile in one CTA, for all-periodic
+// boxes of one context without the transport switches: the species rates
+// stay in this CTA's shared memory and V_c, VTMP and the energy RHS in
+// registers between the passes, instead of going through HBM (WDOT, VC,
+// VTMP, RHS(E): 28 doubles written and read back per point).
+constexpr int kSpecFusedSmem = kSpecSmem + kCarryRate;
+__global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB) k_species_fused_t(Geo g, Fields f, int nspec, RK rk) {
+  extern __shared__ __align__(128) double sm[];
+  __shared__ Folds<SX_, SY_, SZ_> fo;
+  SpecCarry c;
+  c.rate = sm + kSpecSmem;
+  const Origin o{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_};
+  species_tile<true, 0, true, true>(g, f, nspec, o, sm, fo, ZDec{}, nullptr, nullptr, &c);
+  species_rk_tile<true, 0, true, true>(g, f, nspec, rk, o, sm, fo, ZDec{}, nullptr, nullptr, &c);
+}
+
 // ---- batched launches: one CTA per (box, tile) work item; box descriptors
-// come from the launch's parameter table. (A persistent form that strides
-// over the items keeps per-tile state live across iterations and spills
-// ~2 KB per thread in the flow kernel; one CTA per item does not.) ----
+// come from the launch's parameter table (persist.cu runs the same tile
+// functions as one persistent launch per substage) ----
 template <bool P>
 __global__ void __launch_bounds__(FX* FY, 2) k_flow_b(const __grid_constant__ BoxTable t,
                                                       const WorkItem* __restrict__ items) {
@@ -217,6 +232,27 @@ void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, 
     set_attrs<false>();
     k_species_t<false, 0><<<grid, SX_ * SY_, kSpecSmem * 8, s>>>(g, f, nspec, zd, tm);
   }
+}
+
+// Opt-in (SENGA_FUSE=1, read at every launch or graph capture): measured on
+// the 256^3 H2 box, the fused kernel takes 9.53 ms per substage against
+// 6.48 + 2.93 ms for the two kernels. It saves 224 B per point of HBM
+// traffic, but its RK pass runs at the species pass's two CTAs per SM
+// (128 registers) instead of four, and is latency-bound there.
+bool species_fusable(const Geo& g, const ZDec& zd) {
+  const char* e = getenv("SENGA_FUSE");
+  return all_periodic(g) && zd.nr == 1 && e && std::string(e) == "1";
+}
+
+void launch_species_fused(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s) {
+  static bool attr[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  if (!attr[dev]) {
+    cudaFuncSetAttribute(k_species_fused_t, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpecFusedSmem * 8);
+    attr[dev] = true;
+  }
+  k_species_fused_t<<<tiles(g, SX_, SY_, SZ_), SX_ * SY_, kSpecFusedSmem * 8, s>>>(g, f, nspec, rk);
 }
 
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s, const ZDec& zd) {

@@ -141,25 +141,45 @@ void require_rhs(const senga_ctx* c) {
     throw Error(SENGA_ERR_UNSUPPORTED, "a bounded x direction needs its face conditions (senga_set_nscbc)");
 }
 
+// species kernel and species+RK kernel as one launch (launch_species_fused)
+bool fused(const senga_ctx* c) { return !c->mixt && !c->nscbc && species_fusable(c->geo); }
+
+// the fields the thermochemistry kernel writes: the momentum copy only for
+// the fused species kernel
+Fields thermo_fields(const senga_ctx* c) {
+  Fields f = c->f;
+  if (!fused(c)) f.mom = nullptr;
+  return f;
+}
+
+// Everything of a substage up to the species kernel; with fused species
+// kernels that kernel is left to the caller's species+RK launch.
 void run_rhs(senga_ctx* c) {
   require_rhs(c);
   if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->d_chem, c->stream);  // BOUNDT
-  launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+  launch_thermo(c->geo, thermo_fields(c), c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
   if (c->rrte)  // RRTE = RATE (src/rhscal.f:828)
     CK(cudaMemcpyAsync(c->rrte, c->f.wdot, (size_t)c->nspec * c->geo.n * sizeof(double), cudaMemcpyDeviceToDevice,
                        c->stream));
   if (c->nscbc) launch_face(c->geo, c->f, c->bc, c->nspec, c->d_chem, c->stream);  // face data + BOUNDS
   launch_flow(c->geo, c->f, c->nspec, c->stream);
   if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);  // RADCAL
+  if (fused(c)) return;
   launch_species_a(c->geo, c->f, c->nspec, c->stream);
   if (c->mixt) launch_mixt(c->geo, c->f, c->mx, c->d_chem, c->d_diff, c->nspec, c->stream);
   if (c->nscbc) launch_wall_flux(c->geo, c->f, c->bc, c->nspec, c->stream);  // W1 wall diffusion flux
 }
 
+// the species+RK work after run_rhs (rk.last = -1: the RHS only)
+void run_species_rk(senga_ctx* c, const RK& rk) {
+  if (fused(c)) launch_species_fused(c->geo, c->f, c->nspec, rk, c->stream);
+  else launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+}
+
 void run_substage(senga_ctx* c, int irk) {
   run_rhs(c);
   RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
-  launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+  run_species_rk(c, rk);
   if (c->nscbc) launch_wall_fix(c->geo, c->f, c->bc, c->nspec, true, c->stream);  // W1: LINCOM/FINCOM wall Y
 }
 
@@ -256,8 +276,8 @@ int senga_ctx_create(const senga_config* cfg, const senga_chem* chem, const seng
     const int64_t n = c->geo.n;
     const int S = c->nspec, nc = c->nc;
     // pool layout (doubles): run nc | u nc | err nc? | t | p lam lcp mu | rd S | h S |
-    // hmix | wdot S | vel 3 | e | y S | rhs nc | divm | vc 3 | vtmp | itn (int32, n/2 doubles)
-    const int64_t per_point = (int64_t)nc * 2 + (cfg->adaptive ? nc : 0) + 1 + 4 + 3 * S + 1 + 3 + 1 + S + nc + 1 + 3 + 1;
+    // hmix | wdot S | vel 3 | e | y S | rhs nc | divm | vc 3 | vtmp | mom 3 | itn (int32, n/2 doubles)
+    const int64_t per_point = (int64_t)nc * 2 + (cfg->adaptive ? nc : 0) + 1 + 4 + 3 * S + 1 + 3 + 1 + S + nc + 1 + 3 + 1 + 3;
     const int64_t total = per_point * n + (n + 1) / 2 + 64;
     CK(cudaMalloc(&c->pool, (size_t)total * sizeof(double)));
     CK(cudaMemsetAsync(c->pool, 0, (size_t)total * sizeof(double), c->stream));
@@ -288,6 +308,7 @@ int senga_ctx_create(const senga_config* cfg, const senga_chem* chem, const seng
     f.divm = take(1);
     f.vc = take(3);
     f.vtmp = take(1);
+    f.mom = take(3);
     f.itn = reinterpret_cast<int32_t*>(p);
     f.status = c->d_status;
     CK(cudaStreamSynchronize(c->stream));
@@ -414,7 +435,7 @@ int senga_rhs_host(senga_ctx* c, double* rhs, double* trun, double* prun) {
   return guard([&] {
     run_rhs(c);
     RK rk{0.0, 0.0, 0.0, -1};  // last = -1: write R(U) into the rhs fields only
-    launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+    run_species_rk(c, rk);
     if (c->nscbc) launch_wall_fix(c->geo, c->f, c->bc, c->nspec, false, c->stream);  // BOUNDS: wall T
     CK(cudaGetLastError());
     const int64_t n = c->geo.n;
@@ -442,22 +463,26 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
       const int b = (irk - 1) * 4;
       CK(cudaEventRecord(ev[b], c->stream));
       if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->d_chem, c->stream);
-      const int nth = launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+      const int nth =
+          launch_thermo(c->geo, thermo_fields(c), c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
       CK(cudaEventRecord(ev[b + 1], c->stream));
       if (c->nscbc) launch_face(c->geo, c->f, c->bc, c->nspec, c->d_chem, c->stream);
       launch_flow(c->geo, c->f, c->nspec, c->stream);
       if (c->rad) launch_radcal(c->geo, c->f, c->rp, c->stream);
       CK(cudaEventRecord(ev[b + 2], c->stream));
-      launch_species_a(c->geo, c->f, c->nspec, c->stream);
+      RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
+      // fused species kernels: the one launch is timed as the species
+      // kernel, the species+RK interval is then empty
+      if (fused(c)) launch_species_fused(c->geo, c->f, c->nspec, rk, c->stream);
+      else launch_species_a(c->geo, c->f, c->nspec, c->stream);
       const int nmx = c->mixt ? launch_mixt(c->geo, c->f, c->mx, c->d_chem, c->d_diff, c->nspec, c->stream) : 0;
       if (c->nscbc) launch_wall_flux(c->geo, c->f, c->bc, c->nspec, c->stream);
       CK(cudaEventRecord(ev[b + 3], c->stream));
-      RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
-      launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
+      if (!fused(c)) launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream);
       if (c->nscbc) launch_wall_fix(c->geo, c->f, c->bc, c->nspec, true, c->stream);
       if (irk == 5 && imposed) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->d_chem, c->stream);  // BOUNTT
       CK(cudaEventRecord(irk < 5 ? ev[b + 4] : ev[20], c->stream));
-      nl += 3 + nth + (c->rad ? 1 : 0) + nmx + nface + (irk == 5 && imposed ? 1 : 0);
+      nl += (fused(c) ? 2 : 3) + nth + (c->rad ? 1 : 0) + nmx + nface + (irk == 5 && imposed ? 1 : 0);
     }
     CK(cudaStreamSynchronize(c->stream));
     for (int irk = 1; irk <= 5; ++irk) {
@@ -473,6 +498,12 @@ int senga_profile_step(senga_ctx* c, double* ms, int* launches) {
   });
 }
 
+int senga_ctx_species_fused(senga_ctx* c, int* fused_kernels) {
+  if (!c || !fused_kernels) return fail(SENGA_ERR_ARG, "senga_ctx_species_fused: null argument");
+  *fused_kernels = fused(c) ? 1 : 0;
+  return SENGA_OK;
+}
+
 int senga_ctx_info(senga_ctx* c, int* mech, int64_t* device_bytes) {
   if (!c) return fail(SENGA_ERR_ARG, "senga_ctx_info: null context");
   if (mech) *mech = c->mech;
@@ -482,7 +513,7 @@ int senga_ctx_info(senga_ctx* c, int* mech, int64_t* device_bytes) {
     (void)a;
     const int64_t n = c->geo.n;
     const int S = c->nspec, nc = c->nc;
-    bytes = (size_t)((int64_t)(3 * nc + 4 * S + 15 + (c->cfg.adaptive ? nc : 0)) * n + (n + 1) / 2 + 64) * sizeof(double);
+    bytes = (size_t)((int64_t)(3 * nc + 4 * S + 18 + (c->cfg.adaptive ? nc : 0)) * n + (n + 1) / 2 + 64) * sizeof(double);
     *device_bytes = (int64_t)bytes;
   }
   return SENGA_OK;
@@ -818,7 +849,7 @@ int senga_filter_field_host(senga_ctx* c, int mode, const double* f, double* out
 int senga_temper_host(senga_ctx* c, double* trun, double* prun) {
   if (!c) return fail(SENGA_ERR_ARG, "null context");
   return guard([&] {
-    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+    launch_thermo(c->geo, thermo_fields(c), c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
     CK(cudaGetLastError());
     const int64_t n = c->geo.n;
     if (trun) CK(cudaMemcpyAsync(trun, c->f.t, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -830,7 +861,7 @@ int senga_temper_host(senga_ctx* c, double* trun, double* prun) {
 int senga_chrate_host(senga_ctx* c, double* rate) {
   if (!c || !rate) return fail(SENGA_ERR_ARG, "senga_chrate_host: null argument");
   return guard([&] {
-    launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+    launch_thermo(c->geo, thermo_fields(c), c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(rate, c->f.wdot, (size_t)c->nspec * c->geo.n * sizeof(double), cudaMemcpyDeviceToHost,
                        c->stream));
@@ -1007,7 +1038,7 @@ int senga_zgroup_step(senga_zgroup* g, int nsteps) {
         for (int r = 0; r < g->nr; ++r) {
           senga_ctx* c = g->ctx[r];
           CK(cudaSetDevice(c->cfg.device));
-          launch_thermo(c->geo, c->f, c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
+          launch_thermo(c->geo, thermo_fields(c), c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
         }
         zgroup_barrier(g);
         for (int r = 0; r < g->nr; ++r) {

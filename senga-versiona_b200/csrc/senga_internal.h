@@ -90,6 +90,8 @@ struct Fields {
   double* divm;   // DIVM
   double* vc;     // diffusion correction velocity [3][n] (UCOR,VCOR,WCOR)
   double* vtmp;   // divergence of correction flux (VTMP)
+  double* mom;    // rho u, rho v, rho w as the thermochemistry kernel read them [3][n]: the
+                  // fused species kernel reads these, since its RK pass rewrites U (or nullptr)
   unsigned int* status;  // device status word
   // NSCBC boxes only (nullptr otherwise)
   double* cp;     // cp_mix after TEMPER (STRGxx source)
@@ -157,6 +159,11 @@ void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd = ZDec{});
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s,
                          const ZDec& zd = ZDec{});
+// the species kernel and the species+RK kernel as one (all-periodic boxes of
+// one context, when SENGA_FUSE=1 is set): the caller launches it in place of
+// both, after the flow kernel (and RADCAL)
+bool species_fusable(const Geo& g, const ZDec& zd = ZDec{});
+void launch_species_fused(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s);
 // species + RK update marching along z (kernels_zmarch.cu); false when the
 // box does not qualify (the caller then launches the tiled form)
 bool launch_species_b_rk_z(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s,

@@ -369,6 +369,11 @@ __device__ __forceinline__ void thermo_point(const Geo& g, const Fields& f, cons
   f.vel[q] = ru / rho;
   f.vel[n + q] = rv / rho;
   f.vel[2 * n + q] = rw / rho;
+  if (f.mom) {
+    f.mom[q] = ru;
+    f.mom[n + q] = rv;
+    f.mom[2 * n + q] = rw;
+  }
   f.e[q] = re / rho;
 
   // ---- transport properties ----

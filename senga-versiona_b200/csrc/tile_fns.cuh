@@ -398,12 +398,23 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
 }
 
 // -------------------------------------------------------------------------
+// What the species pass hands to the species+RK pass when both run in one
+// CTA (KEEP): each thread's correction velocity, VTMP and energy RHS in
+// registers, the species rates in this CTA's shared memory (rate[(s * SZ_ +
+// z) * 256 + thread]); without KEEP they go through the global scratch
+// fields VC, VTMP, RHS(E) and WDOT.
+struct SpecCarry {
+  double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_];
+  double* rate;
+};
+constexpr int kCarryRate = SENGA_NSPCMX * SZ_ * SX_ * SY_;  // doubles of shared memory
+
 // M: 0 per-element cp.async, 1 bulk row copies, 2 one tensor copy per buffer
 // for tiles away from the wrap (bulk rows for the others)
-template <bool P, int M = 0, bool NC = true>
+template <bool P, int M = 0, bool NC = true, bool KEEP = false>
 __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int nspec, const Origin o, double* sm,
                                              Folds<SX_, SY_, SZ_>& fo, const ZDec& zd, uint64_t* bar = nullptr,
-                                             const SpecMaps* tm = nullptr) {
+                                             const SpecMaps* tm = nullptr, SpecCarry* carry = nullptr) {
   constexpr bool B = M > 0;
   const bool tens = M == 2 && tensor_tile<SX_, SY_, SZ_>(g, o, sm);
   constexpr unsigned kSlabT = 8u * SSlab::SIZE;  // a tensor copy fills the whole slab
@@ -424,7 +435,11 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) tp[z] = make_tp(g, o, tx, ty, z);
   const int64_t n = g.n;
-  const double* U = f.uin;
+  // rho u, rho v, rho w: fields 1..3 of U, or (KEEP) their copy, since this
+  // CTA's RK pass and those of its neighbours rewrite U while tiles still read it
+  const double* const ru = KEEP ? f.mom : f.uin + n;
+  const double* const rv = KEEP ? f.mom + n : f.uin + 2 * n;
+  const double* const rw = KEEP ? f.mom + 2 * n : f.uin + 3 * n;
   const SXRow bru{sm};
   const SYRow brv{sm + SXRow::SIZE};
   const SSlab bS{sm + SXRow::SIZE + SYRow::SIZE};
@@ -436,16 +451,16 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       tma_load_4d(brv.p, &tm->vy, o.x0, o.y0 - H, o.z0, 2, bar);
     }
   } else {
-    stage_plain<B, SNW, NC>(bru, fo, g, o, U + n, bar);
-    stage_plain<B, SNW, NC>(brv, fo, g, o, U + 2 * n, bar);
+    stage_plain<B, SNW, NC>(bru, fo, g, o, ru, bar);
+    stage_plain<B, SNW, NC>(brv, fo, g, o, rv, bar);
   }
   // copies run one stage ahead: Y_s while the previous species' rho D and
   // h are used, rho D and h of species s while Y_s is used
   if (nspec > 0) stage_f(bS, tm ? &tm->y : nullptr, 0, f.y);
   // bytes of the group in flight (bulk paths): rho u, rho v and Y_0 first
   unsigned inflight = SXRow::kBulkBytes + SYRow::kBulkBytes + slab_bytes;
-  SCol rw;
-  rw.load(fo, tx, ty, LdT<NC>{U + 3 * n});
+  SCol rwc;
+  rwc.load(fo, tx, ty, LdT<NC>{rw});
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) {
@@ -499,17 +514,17 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
             d2y = d2core([&](int m) { return yv[m + H]; }, t.gy, g.ny, 1) * g.ovd2[1];
             vc = fv[H];
           }
-          r = r - 0.5 * (d1px + d1py + d1zp<P>(g, t, cy, rw));
+          r = r - 0.5 * (d1px + d1py + d1zp<P>(g, t, cy, rwc));
           yz[z] = d1z<P>(g, t, cy);
-          r = r - 0.5 * (yx[z] * uc + yy[z] * vc + yz[z] * rw.c[z + H]);
+          r = r - 0.5 * (yx[z] * uc + yy[z] * vc + yz[z] * rwc.c[z + H]);
           rate[z] = r;
           fn3[z] = d2x + d2y + d2z<P>(g, t, cy);  // Laplacian for now
         } else {
-          r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1zp<P>(g, t, cy, rw));
+          r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1zp<P>(g, t, cy, rwc));
           yx[z] = d1<0, P>(g, t, bS);
           yy[z] = d1<1, P>(g, t, bS);
           yz[z] = d1z<P>(g, t, cy);
-          r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * rw.c[z + H]);
+          r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * rwc.c[z + H]);
           rate[z] = r;
           // FxxDIF/FxxADB zero the x diffusive terms on the face plane (rhscal.f:1581-1955)
           const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
@@ -551,12 +566,21 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
                            d1z<P>(g, t, ch) * yz[z];
         rE[z] = rE[z] + fn2 * rd[z];
         rE[z] = rE[z] + fn3[z] * hk;
-        if (t.valid) f.wdot[s * n + t.q] = rate[z];
+        if constexpr (KEEP) carry->rate[(s * SZ_ + z) * (SX_ * SY_) + threadIdx.x] = rate[z];
+        else if (t.valid) f.wdot[s * n + t.q] = rate[z];
       }
     }
   }
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) {
+    if constexpr (KEEP) {
+      carry->vcx[z] = vcx[z];
+      carry->vcy[z] = vcy[z];
+      carry->vcz[z] = vcz[z];
+      carry->vt[z] = vt[z];
+      carry->rE[z] = rE[z];
+      continue;
+    }
     const TP& t = tp[z];
     if (!t.valid) continue;
     f.vc[t.q] = vcx[z];
@@ -568,10 +592,11 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
 }
 
 // -------------------------------------------------------------------------
-template <bool P, int M = 0, bool NC = true>
+template <bool P, int M = 0, bool NC = true, bool KEEP = false>
 __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, int nspec, const RK& rk,
                                                 const Origin o, double* sm, Folds<SX_, SY_, SZ_>& fo,
-                                                const ZDec& zd, uint64_t* bar = nullptr, const RkMaps* tm = nullptr) {
+                                                const ZDec& zd, uint64_t* bar = nullptr, const RkMaps* tm = nullptr,
+                                                const SpecCarry* carry = nullptr) {
   constexpr bool B = M > 0;
   const bool tens = M == 2 && tensor_tile<SX_, SY_, SZ_>(g, o, sm);
   const unsigned slab_bytes = tens ? 8u * SSlab::SIZE : SSlab::kBulkBytes;
@@ -583,7 +608,9 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     }
   };
   const int tx = threadIdx.x % SX_, ty = threadIdx.x / SX_;
-  fo.init(g, o, zd);
+  // KEEP: the species pass of this CTA built the same tables; the barrier
+  // below also ends its reads of the buffers this pass fills
+  if constexpr (!KEEP) fo.init(g, o, zd);
   BulkBar bb{bar, 0u};
   if (B && threadIdx.x == 0) mbar_init(bar, 1);
   tile_sync();
@@ -628,6 +655,13 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_];
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) {
+    if constexpr (KEEP) {
+      vcx[z] = carry->vcx[z];
+      vcy[z] = carry->vcy[z];
+      vcz[z] = carry->vcz[z];
+      vt[z] = carry->vt[z];
+      continue;
+    }
     const int64_t q = tp[z].q;
     vcx[z] = f.vc[q];
     vcy[z] = f.vc[n + q];
@@ -650,7 +684,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
       const int bf = P ? 0 : face_bits(g, t.gx);
       // FxxDIF/FxxADB: x gradient term and VTMP vanish on the face (rhscal.f:3782-3839)
       const bool dif = bf & BF_DIF;
-      const double rE = f.rhs[4 * n + t.q] - cm.c[z + H] * (dif ? 0.0 : vt[z]) -
+      const double rE = (KEEP ? carry->rE[z] : f.rhs[4 * n + t.q]) - cm.c[z + H] * (dif ? 0.0 : vt[z]) -
                         (dif ? 0.0 : d1<0, P>(g, t, bS) * vcx[z]) - d1<1, P>(g, t, bS) * vcy[z] -
                         d1z<P>(g, t, cm) * vcz[z];
 #pragma unroll
@@ -671,7 +705,8 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
       if (!t.valid) continue;
       const int bf = P ? 0 : face_bits(g, t.gx);
       const bool dif = bf & BF_DIF;  // rhscal.f:3919: x gradient of Y zeroed on the face
-      const double R = f.wdot[s * n + t.q] - cy.c[z + H] * vt[z] - (dif ? 0.0 : d1<0, P>(g, t, bY) * vcx[z]) -
+      const double rate = KEEP ? carry->rate[(s * SZ_ + z) * (SX_ * SY_) + threadIdx.x] : f.wdot[s * n + t.q];
+      const double R = rate - cy.c[z + H] * vt[z] - (dif ? 0.0 : d1<0, P>(g, t, bY) * vcx[z]) -
                        d1<1, P>(g, t, bY) * vcy[z] - d1z<P>(g, t, cy) * vcz[z];
       advance(5 + s, t, bf, R);
     }

@@ -138,6 +138,7 @@ def _load():
         "senga_get_status": (ip, [vp, C.POINTER(C.c_int)]),
         "senga_profile_step": (ip, [vp, dp, C.POINTER(C.c_int)]),
         "senga_ctx_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
+        "senga_ctx_species_fused": (ip, [vp, C.POINTER(C.c_int)]),
         "senga_fp64_peak": (ip, [ip, dp]),
         "senga_filter": (ip, [vp, ip]),
         "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
@@ -463,11 +464,21 @@ class Box:
 
     def profile_step(self):
         """One RK step with per-kernel-family CUDA-event timing:
-        ({'thermo','flow','species_a','species_b_rk'} -> ms, launches)."""
+        ({'thermo','flow','species_a','species_b_rk'} -> ms, launches), or
+        with the species kernels fused ({'thermo','flow','species'} -> ms,
+        launches)."""
         ms = np.zeros(4)
         nl = C.c_int()
         _check(lib.senga_profile_step(self.h, _dp(ms), C.byref(nl)), "senga_profile_step")
+        if self.species_fused():
+            return {"thermo": ms[0], "flow": ms[1], "species": ms[2] + ms[3]}, nl.value
         return dict(zip(("thermo", "flow", "species_a", "species_b_rk"), ms.tolist())), nl.value
+
+    def species_fused(self):
+        """True when the species and species+RK kernels run as one launch."""
+        v = C.c_int()
+        _check(lib.senga_ctx_species_fused(self.h, C.byref(v)), "senga_ctx_species_fused")
+        return bool(v.value)
 
     def info(self):
         """{'mech': thermochemistry kernel id, 'device_bytes': bytes held}."""
