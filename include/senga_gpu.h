@@ -265,6 +265,13 @@ int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
 
 /* NSCBC x faces (bounded x, NBOUND on both x faces; y, z periodic). xl and
  * xr each take one of the built kinds; inflow on one face at most.
+ * 11: I1 subsonic non-reflecting laminar inflow (NSBCI1), no parameters:
+ *   nothing is imposed; the incoming wave amplitude is the chemistry source
+ *   term alone (its pressure-relaxation coefficient COBCxx is set by BCINIT
+ *   only for an O1 face, so it is zero), the transverse and species waves
+ *   are zero, and every conserved right-hand side of the plane is corrected
+ *   (BOUNDS src/bounds.f:387-520 left, 1465-1598 right); normal viscous
+ *   stress zeroed on the plane (FxxVSN, src/bcinit.f:396-407).
  * 12: I2 subsonic reflecting inflow with specified temperature (NSBCI2):
  *   u = u_in (constant, NXxPRM(1)=1; negative through x-right), v = w = 0,
  *   T = t_in (TRIN) and the mass fractions y_in imposed on the inflow plane

@@ -187,7 +187,7 @@ class Oracle:
         return out
 
     def set_bc(self, bc):
-        """NSCBC x faces: bc = dict(xl, xr in {0, 12, 13, 21, 31, 32}, u_in, rho_in, y_in,
+        """NSCBC x faces: bc = dict(xl, xr in {0, 11, 12, 13, 21, 31, 32}, u_in, rho_in, y_in,
         p_inf, sigma, eta, pio=0, bet_local=0, t_in (I2), t_wall (W2: x-left,
         x-right)); 31 is the W1 wall, 32 the W2 wall."""
         b = _Bc()

@@ -582,7 +582,12 @@ struct Oracle {
   // 429-560 and its x-right block, bounds.f:1058-1190, 1975-): the wall
   // temperature RXxPRM(1) imposed, FxxDIF and FxxDFW only, neither momentum
   // nor energy integrated on the wall.
-  static constexpr int BC_NONE = 0, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21, BC_W1 = 31, BC_W2 = 32;
+  // And I1, the subsonic non-reflecting laminar inflow (NSBCI1; flags
+  // bcinit.f:396-407; wave amplitudes bounds.f:387-520 x-left, 1465-1598
+  // x-right): no imposed state; the incoming wave takes the chemistry source
+  // and COBCxx (PINFxx - p), where COBCxx and PINFxx are set by BCINIT only
+  // for an O1 face (bcinit.f:309-310, 324-325) and so are zero here.
+  static constexpr int BC_NONE = 0, BC_I1 = 11, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21, BC_W1 = 31, BC_W2 = 32;
   int bcxl = BC_NONE, bcxr = BC_NONE;
   double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0, tin = 0.0;
   double twall[2] = {0.0, 0.0};  // W2: RXLPRM(1), RXRPRM(1)
@@ -619,10 +624,12 @@ struct Oracle {
   }
   void set_bc(int xl, int xr, double u_in, double rho_in, const double* y_in, double p_inf, double sigma,
               double eta, int pio, int betloc, double t_in = 0.0, double t_wall_l = 0.0, double t_wall_r = 0.0) {
-    auto ok = [](int k) { return k == BC_NONE || k == BC_I2 || k == BC_I3 || k == BC_O1 || k == BC_W1 || k == BC_W2; };
-    auto inflow = [](int k) { return k == BC_I2 || k == BC_I3; };
+    auto ok = [](int k) {
+      return k == BC_NONE || k == BC_I1 || k == BC_I2 || k == BC_I3 || k == BC_O1 || k == BC_W1 || k == BC_W2;
+    };
+    auto inflow = [](int k) { return k == BC_I1 || k == BC_I2 || k == BC_I3; };
     if (!ok(xl) || !ok(xr) || (inflow(xl) && inflow(xr)))
-      throw std::runtime_error("oracle: NSCBC restated for I2, I3, O1, W1 and W2 x faces (not inflow on both)");
+      throw std::runtime_error("oracle: NSCBC restated for I1, I2, I3, O1, W1 and W2 x faces (not inflow on both)");
     if ((is_wall(xl) || is_wall(xr)) && (df.flmixw || df.flmixp || df.flmixt))
       throw std::runtime_error("oracle: W1/W2 walls restated for the base transport only");
     if ((xl == BC_W2 && !(t_wall_l > 0.0)) || (xr == BC_W2 && !(t_wall_r > 0.0)))
@@ -652,6 +659,8 @@ struct Oracle {
       fxrvsn = true;
       istold = istolu = istolv = istolw = istoly = istol - 1;
     }
+    if (xl == BC_I1) fxlvsn = true;  // src/bcinit.f:396-400: FXLCNV, FXLVSN
+    if (xr == BC_I1) fxrvsn = true;  // src/bcinit.f:403-407: FXRCNV, FXRVSN
     if (xl == BC_I2) istalu = istalv = istalw = istale = istaly = istal + 1;  // src/bcinit.f:458-468: FXLCNV
     if (xr == BC_I2) istolu = istolv = istolw = istole = istoly = istol - 1;  // src/bcinit.f:472-480: FXRCNV
     if (xl == BC_O1) fxlvst = fxlcon = fxladb = fxldif = true;  // src/bcinit.f:299-311
@@ -959,6 +968,61 @@ struct Oracle {
     };
     if (bcxl == BC_I2) i2(fxl, true);
     if (bcxr == BC_I2) i2(fxr, false);
+    // I1 (bounds.f:387-520 x-left, 1465-1598 x-right): the incoming wave
+    // (L5 on the left, L1 on the right) = SORP/2 + COBC (p - PINF) with COBC
+    // and PINF zero, L2..L4 and LY (the transverse waves and species) zero,
+    // the outgoing wave unchanged; every conserved RHS corrected
+    auto i1 = [&](Face& F, bool left) {
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      std::vector<double> sorp(m, 0.0);
+      for (int is = 0; is < nspec; ++is)
+        for (int q = 0; q < m; ++q) sorp[q] = sorp[q] + F.h[is * m + q] * F.rate[is * m + q];
+      for (int q = 0; q < m; ++q) sorp[q] = -sorp[q] * gam1[q];
+      const double cobc = 0.0, pinf = 0.0;  // COBCxx, PINFxx of a face that is not O1
+      const int ic = left ? istal : istol;
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          const double fornow = F.d[q] * acou[q] * F.bcl1[q];
+          double bcl1 = 0.5 * (F.u[q] - acou[q]) * (F.bcl5[q] - fornow);
+          double bcl2 = F.u[q] * (F.bcl2[q] - F.bcl5[q] * ova2[q]);
+          double bcl3 = F.u[q] * F.bcl3[q];
+          double bcl4 = F.u[q] * F.bcl4[q];
+          double bcl5 = 0.5 * (F.u[q] + acou[q]) * (F.bcl5[q] + fornow);
+          bcl2 = -bcl2;
+          bcl3 = -bcl3;
+          bcl4 = -bcl4;
+          const double d = F.d[q], u = F.u[q], v = F.v[q], w = F.w[q], e = F.e[q];
+          if (left) {
+            bcl5 = 0.5 * sorp[q] + cobc * acou[q] * (F.p[q] - pinf) - bcl5;
+            drhs(ic, jc, kc) = drhs(ic, jc, kc) - bcl2 - bcl5 * ova2[q];
+            urhs(ic, jc, kc) = urhs(ic, jc, kc) - bcl2 * u - bcl5 * ova2[q] * (u + acou[q]);
+            vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - bcl2 * v - bcl3 * d - bcl5 * ova2[q] * v;
+            wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - bcl2 * w - bcl4 * d - bcl5 * ova2[q] * w;
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - bcl2 * e - bcl3 * d * v - bcl4 * d * w -
+                               bcl5 * (ova2[q] * e + u / acou[q] + ovgm[q]);
+          } else {
+            bcl1 = 0.5 * sorp[q] + cobc * acou[q] * (F.p[q] - pinf) - bcl1;
+            drhs(ic, jc, kc) = drhs(ic, jc, kc) - bcl1 * ova2[q] - bcl2;
+            urhs(ic, jc, kc) = urhs(ic, jc, kc) - bcl1 * ova2[q] * (u - acou[q]) - bcl2 * u;
+            vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - bcl1 * ova2[q] * v - bcl2 * v - bcl3 * d;
+            wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - bcl1 * ova2[q] * w - bcl2 * w - bcl4 * d;
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - bcl1 * (ova2[q] * e - u / acou[q] + ovgm[q]) - bcl2 * e -
+                               bcl3 * d * v - bcl4 * d * w;
+          }
+          const double lw = left ? bcl5 : bcl1;
+          for (int is = 0; is < nspec; ++is) {
+            const int qs = is * m + q;
+            double bcly = u * F.bcly[qs];
+            bcly = F.rate[qs] / d - bcly;
+            const double fn = bcly * d;
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - fn * F.h[qs];
+            yrhs[is](ic, jc, kc) = yrhs[is](ic, jc, kc) - (bcl2 + lw * ova2[q]) * F.y[qs] - fn;
+          }
+        }
+    };
+    if (bcxl == BC_I1) i1(fxl, true);
+    if (bcxr == BC_I1) i1(fxr, false);
     // W1 (bounds.f:917-1056 x-left, 1833-1974 x-right): the wall temperature
     // re-extrapolated; the outgoing wave reflected (L5 = L1 - L5 on the left,
     // L1 = L5 - L1 on the right), L2..L4 and LY zero; the momentum and

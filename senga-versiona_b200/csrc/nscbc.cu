@@ -1,6 +1,7 @@
 // Navier-Stokes characteristic boundary conditions on the x faces.
 //
-// Restated from the reference (I3 subsonic inflow with constant velocity,
+// Restated from the reference (I1 subsonic non-reflecting laminar inflow,
+// I3 subsonic inflow with constant velocity,
 // NXxPRM(1)=1, I2 subsonic reflecting inflow with specified temperature,
 // O1 partially non-reflecting outflow, W1 adiabatic and W2 isothermal
 // no-slip walls, on either x face; inflow on one face at most; both O1 faces
@@ -222,6 +223,45 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     else b1 = b5 + d * acou * 0.0 - b1;            // L5 unchanged
     b2 = gam1 * ova2 * (b1 + b5) + d * (0.0 / t - sorp / p + sydt) - b2;
     corr[0] = -b2 - (side == 0 ? b5 : b1) * ova2;
+  } else if (kind == 11) {  // I1 inflow (bounds.f:387-520 left, 1465-1598 right): nothing imposed
+    double sorp = 0.0;
+    for (int s = 0; s < nspec; ++s) sorp = sorp + hprime(s) * f.wdot[s * n + q];
+    sorp = -sorp * gam1;
+    const double cobc = 0.0, pinf = 0.0;  // COBCxx, PINFxx: set by BCINIT only for an O1 face
+    const double fornow = d * acou * bcl1;
+    double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
+    double b2 = u * (bcl2 - bcl5 * ova2);
+    double b3 = u * bcl3;
+    double b4 = u * bcl4;
+    double b5 = 0.5 * (u + acou) * (bcl5 + fornow);
+    b2 = -b2;
+    b3 = -b3;
+    b4 = -b4;
+    double ce;
+    if (side == 0) {  // L5 enters
+      b5 = 0.5 * sorp + cobc * acou * (p - pinf) - b5;
+      corr[0] = -b2 - b5 * ova2;
+      corr[(int64_t)nyz] = -b2 * u - b5 * ova2 * (u + acou);
+      corr[2 * (int64_t)nyz] = -b2 * v - b3 * d - b5 * ova2 * v;
+      corr[3 * (int64_t)nyz] = -b2 * w - b4 * d - b5 * ova2 * w;
+      ce = -b2 * e - b3 * d * v - b4 * d * w - b5 * (ova2 * e + u / acou + ovgm);
+    } else {  // L1 enters
+      b1 = 0.5 * sorp + cobc * acou * (p - pinf) - b1;
+      corr[0] = -b1 * ova2 - b2;
+      corr[(int64_t)nyz] = -b1 * ova2 * (u - acou) - b2 * u;
+      corr[2 * (int64_t)nyz] = -b1 * ova2 * v - b2 * v - b3 * d;
+      corr[3 * (int64_t)nyz] = -b1 * ova2 * w - b2 * w - b4 * d;
+      ce = -b1 * (ova2 * e - u / acou + ovgm) - b2 * e - b3 * d * v - b4 * d * w;
+    }
+    const double lw = side == 0 ? b5 : b1;
+    for (int s = 0; s < nspec; ++s) {
+      double bcly = u * dd<0>(g, f.y + s * n, i, j, k);
+      bcly = f.wdot[s * n + q] / d - bcly;
+      const double fn = bcly * d;
+      ce = ce - fn * hprime(s);
+      corr[(int64_t)(5 + s) * nyz] = -(b2 + lw * ova2) * f.y[s * n + q] - fn;
+    }
+    corr[4 * (int64_t)nyz] = ce;
   } else if (kind == 31 || kind == 32) {  // W1/W2 wall (bounds.f:917-1056, 1058-1190 left; 1833-1974, 1975- right)
     // the outgoing wave reflected (L5 = L1 - L5 on the left, L1 = L5 - L1 on
     // the right), L2 = L3 = L4 = LY = 0; U, V, W, E RHS zeroed in the RK

@@ -185,9 +185,9 @@ void launch_batch_persist(const BoxTable& boxes, const PersistArgs& a, int grid,
                           const senga_diff* ddiff, int nspec, int flmavt, cudaStream_t s);
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
-// NSCBC x faces (nscbc.cu): face kinds 0 (none), 12 (I2 inflow), 13 (I3
-// inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall), 32 (W2
-// isothermal no-slip wall) on either face, and their parameters.
+// NSCBC x faces (nscbc.cu): face kinds 0 (none), 11 (I1 inflow), 12 (I2
+// inflow), 13 (I3 inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall),
+// 32 (W2 isothermal no-slip wall) on either face, and their parameters.
 struct NscbcParams {
   int xl, xr;
   double u_in, rho_in, y_in[SENGA_NSPCMX];  // I3: RXLPRM(1), DRIN, YRIN

@@ -89,10 +89,10 @@ C     RADCIN's radiation tables (src/radcin.f:80-220)
         REAL(C_DOUBLE) :: AKPRAD(SNCFRM, SNSPCM)
         REAL(C_DOUBLE) :: TREFRN
       END TYPE
-C     NSCBC x faces: kinds 12 (I2 inflow), 13 (I3 inflow), 21 (O1
-C     outflow), 31 (W1 adiabatic no-slip wall), 32 (W2 isothermal
-C     no-slip wall) and parameters (T_IN: TRIN of an I2 inflow; T_WALL:
-C     RXLPRM(1), RXRPRM(1) of W2 walls)
+C     NSCBC x faces: kinds 11 (I1 inflow), 12 (I2 inflow), 13 (I3
+C     inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall), 32 (W2
+C     isothermal no-slip wall) and parameters (T_IN: TRIN of an I2
+C     inflow; T_WALL: RXLPRM(1), RXRPRM(1) of W2 walls)
       TYPE, BIND(C) :: SENGA_NSCBC
         INTEGER(C_INT) :: XL, XR
         REAL(C_DOUBLE) :: U_IN, RHO_IN

@@ -93,7 +93,8 @@ class ConfigT(C.Structure):
 
 
 class NscbcT(C.Structure):
-    """senga_nscbc: x-face kinds (12 I2 inflow, 13 I3 inflow, 21 O1 outflow) and parameters."""
+    """senga_nscbc: x-face kinds (11 I1, 12 I2, 13 I3 inflow, 21 O1 outflow, 31 W1, 32 W2 wall) and
+    parameters."""
 
     _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
                 ("y_in", C.c_double * NSPCMX), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
@@ -547,9 +548,10 @@ class Box:
 
     def set_nscbc(self, bc):
         """NSCBC x faces from a dict (xl, xr in {0, 12, 13, 21, 31}, u_in, rho_in,
-        y_in, p_inf, sigma, eta, pio, bet_local, t_in, t_wall); 12 I2 inflow,
-        13 I3 inflow, 21 O1 outflow, 31 W1 adiabatic no-slip wall, 32 W2
-        isothermal no-slip wall (t_wall: x-left, x-right temperatures)."""
+        y_in, p_inf, sigma, eta, pio, bet_local, t_in, t_wall); 11 I1
+        inflow, 12 I2 inflow, 13 I3 inflow, 21 O1 outflow, 31 W1 adiabatic
+        no-slip wall, 32 W2 isothermal no-slip wall (t_wall: x-left, x-right
+        temperatures)."""
         b = NscbcT()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
         b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
