@@ -272,6 +272,14 @@ int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
  *   are zero, and every conserved right-hand side of the plane is corrected
  *   (BOUNDS src/bounds.f:387-520 left, 1465-1598 right); normal viscous
  *   stress zeroed on the plane (FxxVSN, src/bcinit.f:396-407).
+ * 14: I4 inflow after Lodato et al. (NSBCI4), coded in the reference for
+ *   the x-left face only (bounds.f:686-845; flags src/bcinit.f:653-658):
+ *   nothing imposed; the waves L2..L5 and LY are relaxed towards the targets
+ *   u = u_in, v = w = 0, T = t_in, Y = y_in (BCUTXL NXLPRM(1)=1, BCTTXL,
+ *   BCYTXL) with the coefficients nrieta[1..5] (NRIETA2..6 = RXLPRC(2..6))
+ *   over XGDLEN, plus the transverse terms TT2..TT6 of the face (bounds.f:
+ *   185-204); L1 leaves unchanged; normal viscous stress zeroed on the plane.
+ *   An I4 face on x-right returns SENGA_ERR_UNSUPPORTED.
  * 12: I2 subsonic reflecting inflow with specified temperature (NSBCI2):
  *   u = u_in (constant, NXxPRM(1)=1; negative through x-right), v = w = 0,
  *   T = t_in (TRIN) and the mass fractions y_in imposed on the inflow plane
@@ -330,6 +338,7 @@ typedef struct senga_nscbc {
   int pio, bet_local;
   double t_in;      /* I2: imposed inflow temperature TRIN [K] */
   double t_wall[2]; /* W2: wall temperature of the x-left, x-right face (RXLPRM(1), RXRPRM(1)) [K] */
+  double nrieta[6]; /* I4: relaxation coefficients NRIETA1..6 = RXLPRC(1..6) (the first is unused) */
 } senga_nscbc;
 int senga_set_nscbc(senga_ctx* ctx, const senga_nscbc* bc);
 

@@ -28,7 +28,7 @@ class _Bc(C.Structure):
     _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
                 ("y_in", C.c_double * 9), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
                 ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double),
-                ("t_wall", C.c_double * 2)]
+                ("t_wall", C.c_double * 2), ("nrieta", C.c_double * 6)]
 
 
 class _Cfg(C.Structure):
@@ -187,9 +187,11 @@ class Oracle:
         return out
 
     def set_bc(self, bc):
-        """NSCBC x faces: bc = dict(xl, xr in {0, 11, 12, 13, 21, 31, 32}, u_in, rho_in, y_in,
-        p_inf, sigma, eta, pio=0, bet_local=0, t_in (I2), t_wall (W2: x-left,
-        x-right)); 31 is the W1 wall, 32 the W2 wall."""
+        """NSCBC x faces: bc = dict(xl, xr in {0, 11, 12, 13, 14, 21, 31, 32}, u_in, rho_in,
+        y_in, p_inf, sigma, eta, pio=0, bet_local=0, t_in (I2; the I4 target),
+        t_wall (W2: x-left, x-right), nrieta (I4: six relaxation
+        coefficients)); 14 (I4) on the x-left face only; 31 is the W1 wall,
+        32 the W2 wall."""
         b = _Bc()
         b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
         b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
@@ -199,6 +201,8 @@ class Oracle:
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
         b.t_in = bc.get("t_in", 0.0)
         b.t_wall[0], b.t_wall[1] = bc.get("t_wall", (0.0, 0.0))
+        for i, v in enumerate(bc.get("nrieta", ())):
+            b.nrieta[i] = v
         if _get().oracle_set_bc(self.h, C.byref(b)) != 0:
             raise RuntimeError("oracle_set_bc: " + _get().oracle_last_error().decode())
 

@@ -587,7 +587,14 @@ struct Oracle {
   // x-right): no imposed state; the incoming wave takes the chemistry source
   // and COBCxx (PINFxx - p), where COBCxx and PINFxx are set by BCINIT only
   // for an O1 face (bcinit.f:309-310, 324-325) and so are zero here.
-  static constexpr int BC_NONE = 0, BC_I1 = 11, BC_I2 = 12, BC_I3 = 13, BC_O1 = 21, BC_W1 = 31, BC_W2 = 32;
+  // And I4, the Lodato-type inflow (NSBCI4; flags bcinit.f:653-666; wave
+  // amplitudes bounds.f:686-845, coded for the x-left face only): the waves
+  // relaxed towards the target u, v = w = 0, T and Y (BCUTXL NXLPRM(1)=1,
+  // BCTTXL, BCYTXL) with the coefficients NRIETA1..6 = RXLPRC(1..6) and the
+  // transverse terms TT2..TT6 (bounds.f:185-204); nothing imposed.
+  static constexpr int BC_NONE = 0, BC_I1 = 11, BC_I2 = 12, BC_I3 = 13, BC_I4 = 14, BC_O1 = 21, BC_W1 = 31,
+                       BC_W2 = 32;
+  double nrieta[6] = {};
   int bcxl = BC_NONE, bcxr = BC_NONE;
   double uin = 0.0, rhoin = 0.0, yin[NSPCMX] = {}, pinfxr = 0.0, cobcxr = 0.0, tin = 0.0;
   double twall[2] = {0.0, 0.0};  // W2: RXLPRM(1), RXRPRM(1)
@@ -623,13 +630,18 @@ struct Oracle {
     });
   }
   void set_bc(int xl, int xr, double u_in, double rho_in, const double* y_in, double p_inf, double sigma,
-              double eta, int pio, int betloc, double t_in = 0.0, double t_wall_l = 0.0, double t_wall_r = 0.0) {
+              double eta, int pio, int betloc, double t_in = 0.0, double t_wall_l = 0.0, double t_wall_r = 0.0,
+              const double* nri = nullptr) {
     auto ok = [](int k) {
-      return k == BC_NONE || k == BC_I1 || k == BC_I2 || k == BC_I3 || k == BC_O1 || k == BC_W1 || k == BC_W2;
+      return k == BC_NONE || k == BC_I1 || k == BC_I2 || k == BC_I3 || k == BC_I4 || k == BC_O1 || k == BC_W1 ||
+             k == BC_W2;
     };
-    auto inflow = [](int k) { return k == BC_I1 || k == BC_I2 || k == BC_I3; };
+    auto inflow = [](int k) { return k == BC_I1 || k == BC_I2 || k == BC_I3 || k == BC_I4; };
     if (!ok(xl) || !ok(xr) || (inflow(xl) && inflow(xr)))
-      throw std::runtime_error("oracle: NSCBC restated for I1, I2, I3, O1, W1 and W2 x faces (not inflow on both)");
+      throw std::runtime_error("oracle: NSCBC restated for I1, I2, I3, I4, O1, W1 and W2 x faces (not inflow on both)");
+    if (xr == BC_I4) throw std::runtime_error("oracle: I4 is coded for the x-left face only (bounds.f:686)");
+    if (xl == BC_I4 && !(t_in > 0.0)) throw std::runtime_error("oracle: an I4 inflow needs its target temperature");
+    for (int k = 0; k < 6; ++k) nrieta[k] = nri ? nri[k] : 0.0;
     if ((is_wall(xl) || is_wall(xr)) && (df.flmixw || df.flmixp || df.flmixt))
       throw std::runtime_error("oracle: W1/W2 walls restated for the base transport only");
     if ((xl == BC_W2 && !(t_wall_l > 0.0)) || (xr == BC_W2 && !(t_wall_r > 0.0)))
@@ -660,6 +672,7 @@ struct Oracle {
       istold = istolu = istolv = istolw = istoly = istol - 1;
     }
     if (xl == BC_I1) fxlvsn = true;  // src/bcinit.f:396-400: FXLCNV, FXLVSN
+    if (xl == BC_I4) fxlvsn = true;  // src/bcinit.f:653-658: FXLCNV, FXLVSN
     if (xr == BC_I1) fxrvsn = true;  // src/bcinit.f:403-407: FXRCNV, FXRVSN
     if (xl == BC_I2) istalu = istalv = istalw = istale = istaly = istal + 1;  // src/bcinit.f:458-468: FXLCNV
     if (xr == BC_I2) istolu = istolv = istolw = istole = istoly = istol - 1;  // src/bcinit.f:472-480: FXRCNV
@@ -1023,6 +1036,49 @@ struct Oracle {
     };
     if (bcxl == BC_I1) i1(fxl, true);
     if (bcxr == BC_I1) i1(fxr, false);
+    // I4 at x-left (bounds.f:686-845): the face's current u, v, w, T, Y
+    // (STLxXL) against the targets (STRxXL after BCUTXL/BCTTXL/BCYTXL); L1
+    // unchanged, L2..L5 and LY relaxed towards the targets plus their
+    // transverse terms
+    if (bcxl == BC_I4) {
+      Face& F = fxl;
+      prelim(F, gam1, ovgm, acou, ova2, tt1, tt5);
+      const double m2max = 0.001;  // bounds.f:101
+      const double xl = cf.xgdlen;
+      const double n2 = nrieta[1], n3 = nrieta[2], n4 = nrieta[3], n5 = nrieta[4], n6 = nrieta[5];
+      for (int kc = kstal; kc <= kstol; ++kc)
+        for (int jc = jstal; jc <= jstol; ++jc) {
+          const int q = fj(jc, kc);
+          const double d = F.d[q], c = acou[q];
+          const double lu = F.u[q], lv = F.v[q], lw = F.w[q], lt = F.t[q];
+          const double tt2 = c * c * F.t1b[q] - F.t51b[q] - (gam1[q] + 1.0) * F.t52b[q];
+          const double tt3 = F.t3b[q], tt4 = F.t4b[q];
+          const double fornow = d * c * F.bcl1[q];
+          double bcl2 = lu * (F.bcl2[q] - F.bcl5[q] * ova2[q]);
+          double bcl3 = lu * F.bcl3[q];
+          double bcl4 = lu * F.bcl4[q];
+          double bcl5 = 0.5 * (lu + c) * (F.bcl5[q] + fornow);
+          bcl2 = n2 * d * F.r[q] / (xl * c) * (lt - tin) + tt2 * ova2[q] - bcl2;
+          bcl3 = n3 * c / xl * (lv - 0.0) + tt3 - bcl3;
+          bcl4 = n4 * c / xl * (lw - 0.0) + tt4 - bcl4;
+          bcl5 = n5 * d * c * c * (1.0 - m2max) / (2.0 * xl) * (lu - uin) + 0.5 * tt5[q] - bcl5;
+          const int ic = istal;
+          drhs(ic, jc, kc) = drhs(ic, jc, kc) - bcl2 - bcl5 * ova2[q];
+          urhs(ic, jc, kc) = urhs(ic, jc, kc) - bcl2 * lu - bcl5 * ova2[q] * (lu + c);
+          vrhs(ic, jc, kc) = vrhs(ic, jc, kc) - bcl2 * lv - bcl3 * d - bcl5 * ova2[q] * lv;
+          wrhs(ic, jc, kc) = wrhs(ic, jc, kc) - bcl2 * lw - bcl4 * d - bcl5 * ova2[q] * lw;
+          erhs(ic, jc, kc) = erhs(ic, jc, kc) - bcl2 * F.e[q] - bcl3 * d * lv - bcl4 * d * lw -
+                             bcl5 * (ova2[q] * F.e[q] + lu / c + ovgm[q]);
+          for (int is = 0; is < nspec; ++is) {
+            const int qs = is * m + q;
+            double bcly = lu * F.bcly[qs];
+            bcly = n6 * c / xl * (F.y[qs] - yin[is]) + F.t6b[qs] - bcly;
+            const double fn = bcly * d;
+            erhs(ic, jc, kc) = erhs(ic, jc, kc) - fn * F.h[qs];
+            yrhs[is](ic, jc, kc) = yrhs[is](ic, jc, kc) - (bcl2 + bcl5 * ova2[q]) * F.y[qs] - fn;
+          }
+        }
+    }
     // W1 (bounds.f:917-1056 x-left, 1833-1974 x-right): the wall temperature
     // re-extrapolated; the outgoing wave reflected (L5 = L1 - L5 on the left,
     // L1 = L5 - L1 on the right), L2..L4 and LY zero; the momentum and
@@ -2680,11 +2736,12 @@ struct oracle_bc {
   int pio, bet_local;
   double t_in;
   double t_wall[2];
+  double nrieta[6];
 };
 int oracle_set_bc(void* h, const oracle_bc* b) {
   try {
     static_cast<orc::Oracle*>(h)->set_bc(b->xl, b->xr, b->u_in, b->rho_in, b->y_in, b->p_inf, b->sigma, b->eta, b->pio,
-                                         b->bet_local, b->t_in, b->t_wall[0], b->t_wall[1]);
+                                         b->bet_local, b->t_in, b->t_wall[0], b->t_wall[1], b->nrieta);
     return 0;
   } catch (std::exception& e) {
     g_err = e.what();

@@ -1,6 +1,7 @@
 // Navier-Stokes characteristic boundary conditions on the x faces.
 //
 // Restated from the reference (I1 subsonic non-reflecting laminar inflow,
+// I4 Lodato-type inflow relaxed towards targets (x-left, as coded),
 // I3 subsonic inflow with constant velocity,
 // NXxPRM(1)=1, I2 subsonic reflecting inflow with specified temperature,
 // O1 partially non-reflecting outflow, W1 adiabatic and W2 isothermal
@@ -223,6 +224,41 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     else b1 = b5 + d * acou * 0.0 - b1;            // L5 unchanged
     b2 = gam1 * ova2 * (b1 + b5) + d * (0.0 / t - sorp / p + sydt) - b2;
     corr[0] = -b2 - (side == 0 ? b5 : b1) * ova2;
+  } else if (kind == 14) {  // I4 inflow at x-left (bounds.f:686-845): waves relaxed towards the targets
+    const double m2max = 0.001;  // bounds.f:101
+    const double xl = bc.xlen, c = acou;
+    const double n2 = bc.nrieta[1], n3 = bc.nrieta[2], n4 = bc.nrieta[3], n5 = bc.nrieta[4], n6 = bc.nrieta[5];
+    // transverse terms (bounds.f:185-204 from rhscal.f:159-180, rhsvel.f:62-200, 764-800)
+    const double t1b = -(dd<1>(g, U + 2 * n, i, j, k) + dd<2>(g, U + 3 * n, i, j, k));
+    const double rho_inv = 1.0 / d;
+    const double t3b = -v * dd<1>(g, vel + n, i, j, k) - w * dd<2>(g, vel + n, i, j, k) - py * rho_inv;
+    const double t4b = -v * dd<1>(g, vel + 2 * n, i, j, k) - w * dd<2>(g, vel + 2 * n, i, j, k) - pz * rho_inv;
+    const double tt2 = c * c * t1b - t51b - (gam1 + 1.0) * t52b;
+    const double tt5 = t51b + t52b * (gam1 + 1.0) + d * c * t2b;
+    const double fornow = d * c * bcl1;
+    double b2 = u * (bcl2 - bcl5 * ova2);
+    double b3 = u * bcl3;
+    double b4 = u * bcl4;
+    double b5 = 0.5 * (u + c) * (bcl5 + fornow);
+    b2 = n2 * d * rr / (xl * c) * (t - bc.t_in) + tt2 * ova2 - b2;
+    b3 = n3 * c / xl * (v - 0.0) + t3b - b3;
+    b4 = n4 * c / xl * (w - 0.0) + t4b - b4;
+    b5 = n5 * d * c * c * (1.0 - m2max) / (2.0 * xl) * (u - bc.u_in) + 0.5 * tt5 - b5;
+    corr[0] = -b2 - b5 * ova2;
+    corr[(int64_t)nyz] = -b2 * u - b5 * ova2 * (u + c);
+    corr[2 * (int64_t)nyz] = -b2 * v - b3 * d - b5 * ova2 * v;
+    corr[3 * (int64_t)nyz] = -b2 * w - b4 * d - b5 * ova2 * w;
+    double ce = -b2 * e - b3 * d * v - b4 * d * w - b5 * (ova2 * e + u / c + ovgm);
+    for (int s = 0; s < nspec; ++s) {
+      const double* ys = f.y + s * n;
+      const double t6b = -dd<1>(g, ys, i, j, k) * v - dd<2>(g, ys, i, j, k) * w;
+      double bcly = u * dd<0>(g, ys, i, j, k);
+      bcly = n6 * c / xl * (ys[q] - bc.y_in[s]) + t6b - bcly;
+      const double fn = bcly * d;
+      ce = ce - fn * hprime(s);
+      corr[(int64_t)(5 + s) * nyz] = -(b2 + b5 * ova2) * ys[q] - fn;
+    }
+    corr[4 * (int64_t)nyz] = ce;
   } else if (kind == 11) {  // I1 inflow (bounds.f:387-520 left, 1465-1598 right): nothing imposed
     double sorp = 0.0;
     for (int s = 0; s < nspec; ++s) sorp = sorp + hprime(s) * f.wdot[s * n + q];

@@ -741,12 +741,15 @@ int senga_set_radiation(senga_ctx* c, const senga_radn* r) {
 
 int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
   if (!c || !b) return fail(SENGA_ERR_ARG, "senga_set_nscbc: null argument");
-  auto kind_ok = [](int k) { return k == 11 || k == 12 || k == 13 || k == 21 || k == 31 || k == 32; };
-  auto inflow = [](int k) { return k == 11 || k == 12 || k == 13; };
+  auto kind_ok = [](int k) { return k == 11 || k == 12 || k == 13 || k == 14 || k == 21 || k == 31 || k == 32; };
+  auto inflow = [](int k) { return k == 11 || k == 12 || k == 13 || k == 14; };
   auto either = [b](int k) { return b->xl == k || b->xr == k; };
   if (!kind_ok(b->xl) || !kind_ok(b->xr) || (inflow(b->xl) && inflow(b->xr)))
-    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I1 (11), I2 (12), I3 (13), O1 (21), "
-                                       "W1 (31) and W2 (32) on either x face, inflow on one at most");
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: built face kinds are I1 (11), I2 (12), I3 (13), I4 (14, "
+                                       "x-left), O1 (21), W1 (31) and W2 (32), inflow on one x face at most");
+  if (b->xr == 14)
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: the I4 inflow is coded for the x-left face only");
+  if (b->xl == 14 && !(b->t_in > 0.0)) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I4 inflow needs t_in > 0");
   if (either(12) && !(b->t_in > 0.0)) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an I2 inflow needs t_in > 0");
   if (c->geo.per[0] || b->xl == 0 || b->xr == 0)
     return fail(SENGA_ERR_ARG, "senga_set_nscbc: needs a bounded x direction and a kind on both x faces");
@@ -776,14 +779,15 @@ int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
     p.t_in = b->t_in;
     p.t_wall[0] = b->t_wall[0];
     p.t_wall[1] = b->t_wall[1];
-    // face-plane flags of src/bcinit.f:299-326,396-407,458-480,560-586,702-735,
-    // 822-855: I1 -> FxxCNV, FxxVSN, every field integrated; I3 ->
+    for (int k = 0; k < 6; ++k) p.nrieta[k] = b->nrieta[k];
+    // face-plane flags of src/bcinit.f:299-326,396-407,458-480,560-586,653-666,
+    // 702-735,822-855: I1, I4 -> FxxCNV, FxxVSN, every field integrated; I3 ->
     // FxxCNV, FxxVSN, the plane imposed; I2 -> FxxCNV, all but the density
     // imposed; O1 -> FxxCNV, FxxVST, FxxCON, FxxADB, FxxDIF; W1 -> FxxCNV,
     // FxxCON, FxxADB, FxxDIF, FxxCNW, FxxDFW, momentum not integrated; W2
     // -> FxxCNV, FxxDIF, FxxDFW, momentum and energy not integrated
     auto bits = [](int kind) {
-      return kind == 11   ? (BF_VSN | BF_NSCBC)
+      return kind == 11 || kind == 14 ? (BF_VSN | BF_NSCBC)
              : kind == 13 ? (BF_VSN | BF_NSCBC | BF_IMPOSED)
              : kind == 12 ? (BF_NSCBC | BF_IMPOSED_D)
              : kind == 31 ? (BF_CON | BF_DIF | BF_NSCBC | BF_WALL)

@@ -186,13 +186,15 @@ void launch_batch_persist(const BoxTable& boxes, const PersistArgs& a, int grid,
 void launch_batch_stencil(const BoxTable& boxes, const WorkItem* items, int nitems, int irk, int phase,
                           cudaStream_t s);
 // NSCBC x faces (nscbc.cu): face kinds 0 (none), 11 (I1 inflow), 12 (I2
-// inflow), 13 (I3 inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall),
-// 32 (W2 isothermal no-slip wall) on either face, and their parameters.
+// inflow), 13 (I3 inflow), 14 (I4 inflow, x-left), 21 (O1 outflow), 31 (W1
+// adiabatic no-slip wall), 32 (W2 isothermal no-slip wall), and their
+// parameters.
 struct NscbcParams {
   int xl, xr;
   double u_in, rho_in, y_in[SENGA_NSPCMX];  // I3: RXLPRM(1), DRIN, YRIN
   double t_in;                              // I2: TRIN
   double t_wall[2];                         // W2: RXLPRM(1), RXRPRM(1)
+  double nrieta[6];                         // I4: NRIETA1..6 = RXLPRC(1..6)
   double p_inf, cobc, bet, xlen;            // O1: PINFXR, COBCXR, BET, XGDLEN
   int pio, betloc;                          // O1: NXRPRM(1), NXRPRM(2)
 };

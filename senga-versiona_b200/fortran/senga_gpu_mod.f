@@ -90,9 +90,10 @@ C     RADCIN's radiation tables (src/radcin.f:80-220)
         REAL(C_DOUBLE) :: TREFRN
       END TYPE
 C     NSCBC x faces: kinds 11 (I1 inflow), 12 (I2 inflow), 13 (I3
-C     inflow), 21 (O1 outflow), 31 (W1 adiabatic no-slip wall), 32 (W2
-C     isothermal no-slip wall) and parameters (T_IN: TRIN of an I2
-C     inflow; T_WALL: RXLPRM(1), RXRPRM(1) of W2 walls)
+C     inflow), 14 (I4 inflow, x-left), 21 (O1 outflow), 31 (W1
+C     adiabatic no-slip wall), 32 (W2 isothermal no-slip wall) and
+C     parameters (T_IN: TRIN of an I2 inflow, the I4 target; T_WALL:
+C     RXLPRM(1), RXRPRM(1) of W2 walls; NRIETA: RXLPRC(1..6) of I4)
       TYPE, BIND(C) :: SENGA_NSCBC
         INTEGER(C_INT) :: XL, XR
         REAL(C_DOUBLE) :: U_IN, RHO_IN
@@ -101,6 +102,7 @@ C     inflow; T_WALL: RXLPRM(1), RXRPRM(1) of W2 walls)
         INTEGER(C_INT) :: PIO, BET_LOCAL
         REAL(C_DOUBLE) :: T_IN
         REAL(C_DOUBLE) :: T_WALL(2)
+        REAL(C_DOUBLE) :: NRIETA(6)
       END TYPE
       INTERFACE
         INTEGER(C_INT) FUNCTION SENGA_CHEM_LOAD(PATH, CHEM)

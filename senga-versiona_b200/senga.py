@@ -93,13 +93,13 @@ class ConfigT(C.Structure):
 
 
 class NscbcT(C.Structure):
-    """senga_nscbc: x-face kinds (11 I1, 12 I2, 13 I3 inflow, 21 O1 outflow, 31 W1, 32 W2 wall) and
-    parameters."""
+    """senga_nscbc: x-face kinds (11 I1, 12 I2, 13 I3, 14 I4 inflow, 21 O1 outflow, 31 W1, 32 W2 wall)
+    and parameters."""
 
     _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
                 ("y_in", C.c_double * NSPCMX), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
                 ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double),
-                ("t_wall", C.c_double * 2)]
+                ("t_wall", C.c_double * 2), ("nrieta", C.c_double * 6)]
 
 
 NCFRMX = 6
@@ -548,8 +548,9 @@ class Box:
 
     def set_nscbc(self, bc):
         """NSCBC x faces from a dict (xl, xr in {0, 12, 13, 21, 31}, u_in, rho_in,
-        y_in, p_inf, sigma, eta, pio, bet_local, t_in, t_wall); 11 I1
-        inflow, 12 I2 inflow, 13 I3 inflow, 21 O1 outflow, 31 W1 adiabatic
+        y_in, p_inf, sigma, eta, pio, bet_local, t_in, t_wall, nrieta); 11 I1
+        inflow, 12 I2 inflow, 13 I3 inflow, 14 I4 inflow (x-left; nrieta:
+        its six relaxation coefficients), 21 O1 outflow, 31 W1 adiabatic
         no-slip wall, 32 W2 isothermal no-slip wall (t_wall: x-left, x-right
         temperatures)."""
         b = NscbcT()
@@ -561,6 +562,8 @@ class Box:
         b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
         b.t_in = bc.get("t_in", 0.0)
         b.t_wall[0], b.t_wall[1] = bc.get("t_wall", (0.0, 0.0))
+        for i, v in enumerate(bc.get("nrieta", ())):
+            b.nrieta[i] = v
         _check(lib.senga_set_nscbc(self.h, C.byref(b)), "senga_set_nscbc")
 
     def set_transport(self, mixw=False, mixp=False, soret=False, dufour=False, wmltdr=5.0):
