@@ -50,7 +50,10 @@ using SXRow = XRow<SX_, SY_, SZ_>;
 using SYRow = YRow<SX_, SY_, SZ_>;
 using SCol = Column<SZ_>;
 constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 3 * SSlab::SIZE;
-constexpr int kSpecRkSmem = 2 * SSlab::SIZE;
+// species+RK: two slabs, then the prefetched S register and rate of the next
+// species' own points, double-buffered: [buffer][run | rate][z][thread]
+constexpr int kRkPre = 2 * SZ_ * SX_ * SY_;
+constexpr int kSpecRkSmem = 2 * SSlab::SIZE + 2 * kRkPre;
 
 // Staging of a plain field: bulk copies on the TMA engine (B) or per-element
 // cp.async; and the wait for the group staged last (B: one mbarrier phase of
@@ -626,7 +629,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
   // no momentum (src/bcinit.f ranges ISTALD..ISTALY; a W2 wall's energy,
   // left out of the range too, is advanced by a zero RHS, which leaves both
   // registers where BOUNDT put them)
-  auto advance = [&](int fld, const TP& t, int bf, double R) {
+  auto advance = [&](int fld, const TP& t, int bf, double R, const double* srun = nullptr) {
     const int64_t q = t.q;
     const int64_t idx = (int64_t)fld * n + q;
     if (!P && (bf & BF_NSCBC)) {
@@ -642,14 +645,31 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     if (!P && (bf & BF_IMPOSED_D) && fld != 0) return;
     if (!P && (bf & BF_WALL) && fld >= 1 && fld <= 3) return;
     if (f.err) f.err[idx] = f.err[idx] + rk.err * R;
+    const double s0 = srun ? *srun : f.run[idx];
     if (!rk.last) {
-      const double s = f.run[idx];
-      f.run[idx] = s + rk.lhs * R;
-      f.uout[idx] = s + rk.rhs * R;
+      f.run[idx] = s0 + rk.lhs * R;
+      f.uout[idx] = s0 + rk.rhs * R;
     } else {
-      const double s = f.run[idx] + rk.lhs * R;
+      const double s = s0 + rk.lhs * R;
       f.run[idx] = s;
       f.uout[idx] = s;
+    }
+  };
+  // per-element staging (cp.async), not fused: the S register and rate of
+  // each species' own points are copied into shared memory together with
+  // its slab, one species ahead, so their latency overlaps the previous
+  // species' work; a thread reads back only the slots it copied
+  constexpr bool PRE = M == 0 && !KEEP;
+  double* const pre = sm + 2 * SSlab::SIZE;
+  auto prefetch = [&](int s) {
+    if constexpr (PRE) {
+      double* b = pre + (s & 1) * kRkPre;
+#pragma unroll
+      for (int z = 0; z < SZ_; ++z) {
+        if (!tp[z].valid) continue;
+        cp_async8(b + z * (SX_ * SY_) + threadIdx.x, f.run + (int64_t)(5 + s) * n + tp[z].q);
+        cp_async8(b + (SZ_ + z) * (SX_ * SY_) + threadIdx.x, f.wdot + (int64_t)s * n + tp[z].q);
+      }
     }
   };
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_];
@@ -676,7 +696,10 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     cm.load(fo, tx, ty, LdT<NC>{f.hmix});
     stage_f(bS, tm ? &tm->hm : nullptr, 0, f.hmix);
     if (sync_staged<B>(bb, slab_bytes, f.status)) return;
-    if (nspec > 0) stage_f(slab(0), tm ? &tm->y : nullptr, 0, f.y);
+    if (nspec > 0) {
+      stage_f(slab(0), tm ? &tm->y : nullptr, 0, f.y);
+      prefetch(0);
+    }
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
@@ -697,18 +720,24 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
     cy.load(fo, tx, ty, LdT<NC>{f.y + s * n});
     // Y_s has landed in slab(s); every thread is done with the other slab
     if (sync_staged<B>(bb, slab_bytes, f.status)) return;
-    if (s + 1 < nspec) stage_f(slab(s + 1), tm ? &tm->y : nullptr, s + 1, f.y + (s + 1) * n);
+    if (s + 1 < nspec) {
+      stage_f(slab(s + 1), tm ? &tm->y : nullptr, s + 1, f.y + (s + 1) * n);
+      prefetch(s + 1);
+    }
     const SSlab bY = slab(s);
+    const double* const pb = pre + (s & 1) * kRkPre;
 #pragma unroll
     for (int z = 0; z < SZ_; ++z) {
       const TP& t = tp[z];
       if (!t.valid) continue;
       const int bf = P ? 0 : face_bits(g, t.gx);
       const bool dif = bf & BF_DIF;  // rhscal.f:3919: x gradient of Y zeroed on the face
-      const double rate = KEEP ? carry->rate[(s * SZ_ + z) * (SX_ * SY_) + threadIdx.x] : f.wdot[s * n + t.q];
+      const double rate = KEEP  ? carry->rate[(s * SZ_ + z) * (SX_ * SY_) + threadIdx.x]
+                          : PRE ? pb[(SZ_ + z) * (SX_ * SY_) + threadIdx.x]
+                                : f.wdot[s * n + t.q];
       const double R = rate - cy.c[z + H] * vt[z] - (dif ? 0.0 : d1<0, P>(g, t, bY) * vcx[z]) -
                        d1<1, P>(g, t, bY) * vcy[z] - d1z<P>(g, t, cy) * vcz[z];
-      advance(5 + s, t, bf, R);
+      advance(5 + s, t, bf, R, PRE ? pb + z * (SX_ * SY_) + threadIdx.x : nullptr);
     }
   }
 }
