@@ -655,11 +655,14 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
       f.uout[idx] = s;
     }
   };
-  // per-element staging (cp.async), not fused: the S register and rate of
-  // each species' own points are copied into shared memory together with
-  // its slab, one species ahead, so their latency overlaps the previous
-  // species' work; a thread reads back only the slots it copied
+  // per-element staging (cp.async), not fused: the rate of each species'
+  // own points, and in the RK form their S register, are copied into shared
+  // memory together with its slab, one species ahead, so their latency
+  // overlaps the previous species' work; a thread reads back only the slots
+  // it copied. The RHS-only form has no S register (its pointer may be null)
+  // and copies only the rate.
   constexpr bool PRE = M == 0 && !KEEP;
+  const bool pre_run = PRE && rk.last >= 0 && f.run != nullptr;
   double* const pre = sm + 2 * SSlab::SIZE;
   auto prefetch = [&](int s) {
     if constexpr (PRE) {
@@ -667,7 +670,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
 #pragma unroll
       for (int z = 0; z < SZ_; ++z) {
         if (!tp[z].valid) continue;
-        cp_async8(b + z * (SX_ * SY_) + threadIdx.x, f.run + (int64_t)(5 + s) * n + tp[z].q);
+        if (pre_run) cp_async8(b + z * (SX_ * SY_) + threadIdx.x, f.run + (int64_t)(5 + s) * n + tp[z].q);
         cp_async8(b + (SZ_ + z) * (SX_ * SY_) + threadIdx.x, f.wdot + (int64_t)s * n + tp[z].q);
       }
     }
@@ -737,7 +740,7 @@ __device__ __forceinline__ void species_rk_tile(const Geo& g, const Fields& f, i
                                 : f.wdot[s * n + t.q];
       const double R = rate - cy.c[z + H] * vt[z] - (dif ? 0.0 : d1<0, P>(g, t, bY) * vcx[z]) -
                        d1<1, P>(g, t, bY) * vcy[z] - d1z<P>(g, t, cy) * vcz[z];
-      advance(5 + s, t, bf, R, PRE ? pb + z * (SX_ * SY_) + threadIdx.x : nullptr);
+      advance(5 + s, t, bf, R, pre_run ? pb + z * (SX_ * SY_) + threadIdx.x : nullptr);
     }
   }
 }
