@@ -381,6 +381,10 @@ def main():
 
         fl = workloads.run_flame(steps=20, warmup=3, device=local)
         en = workloads.run_ensemble(steps=50, warmup=3, nbox=64, device=local)
+        # the serving workload's request stream cut to its first 300 requests
+        # (Poisson 20/s, the ensemble's box distribution plus 10% 128^3
+        # cases, 20-200 steps each), so that the default run stays short
+        sv = workloads.run_serve(nreq=300, device=local)
         extras = {
             "flame_128": {"workload": "flame_inout_128^3_H2_nscbc_I3_O1, filter every 10 steps", "steps": 20,
                           "value": fl["gpsu_s"], "unit": unit, "ms_per_step": 1e3 * fl["seconds"] / 20,
@@ -388,7 +392,12 @@ def main():
             "ensemble_64": {"workload": "64 boxes, axes from {32,48,64,96}, 1-step chemistry", "steps": 50,
                             "points": en["points"], "batched_value": en["batched_gpsu_s"],
                             "sequential_value": en["sequential_gpsu_s"], "unit": unit,
-                            "batched_vs_sequential": en["speedup"], "status_word": en["status_word"]}}
+                            "batched_vs_sequential": en["speedup"], "status_word": en["status_word"]},
+            "serve_300": {"workload": "first 300 requests of the serving stream (Poisson 20/s, 1-step chemistry, "
+                                      "boxes from {32,48,64,96}^3 plus 10% 128^3, 20-200 steps)",
+                          "requests": sv["requests"], "wall_s": sv["wall_s"], "served_value": sv["served_gpsu_s"],
+                          "sequential_value": sv["sequential_gpsu_s"], "unit": unit, "p50_s": sv["p50_s"],
+                          "p99_s": sv["p99_s"], "mean_latency_s": sv["mean_latency_s"]}}
     line = {
         "metric": metric, "value": gpsu, "unit": unit, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",

@@ -478,8 +478,13 @@ int senga_batch_status(senga_batch* b, int* status);
  * request (one periodic box, its initial state and a number of RK steps) is
  * admitted, first come first served, as soon as the device arena of
  * arena_bytes has room for its fields; all admitted requests advance one RK
- * step per senga_server_tick in one batched graph; finished requests are
- * copied back and their memory freed. Times are seconds since creation. */
+ * step per senga_server_tick in one batched launch sequence; finished
+ * requests are copied back and their memory freed. A tick queues its step
+ * and returns: it waits on the device only while two steps are already in
+ * flight. Uploads and results pass through a page-locked staging ring, and
+ * a request counts as active (senga_server_result refuses it) until its
+ * result has landed in host memory; *finished counts the results that
+ * landed during the tick. Times are seconds since creation. */
 typedef struct senga_server senga_server;
 int senga_server_create(size_t arena_bytes, const senga_chem* chem, const senga_diff* diff, int device,
                         senga_server** out);

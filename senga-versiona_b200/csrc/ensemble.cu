@@ -22,8 +22,13 @@
 // changes between RK steps: requests are admitted as soon as the arena has
 // room for their fields (admission by HBM footprint), every active request
 // advances one RK step per tick together with all the others, and finished
-// requests are copied back to the host and their memory released. The graph
-// is re-captured only when membership changes.
+// requests are copied back to the host and their memory released. A tick
+// never waits for the device except to keep at most two steps queued: every
+// copy goes through page-locked staging (so it queues behind the kernels
+// instead of waiting for them), work lists are uploaded in stream order, the
+// steps are launched kernel by kernel (membership changes most ticks), and a
+// result is handed to the host by an event callback once its download has
+// completed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,6 +36,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -139,6 +145,84 @@ void check_box(const senga_config& c) {
   if (c.tstep <= 0.0) throw Error(SENGA_ERR_ARG, "tstep must be positive");
 }
 
+// Page-locked staging for the serving loop's copies: a FIFO ring of chunks,
+// each released once the copy through it has completed (its event) and, for
+// a download, once the host has taken the data out. Copies from page-locked
+// memory run on the stream without waiting for the kernels queued before
+// them, so admitting or retiring a request never stalls the device.
+class PinnedRing {
+ public:
+  struct Chunk {
+    size_t off = 0, len = 0;
+    cudaEvent_t ev = nullptr;
+    std::function<void(const char*)> done;  // run on the host once the copy has completed
+  };
+  void init(size_t bytes) {
+    cap_ = bytes;
+    CKE(cudaMallocHost(&base_, cap_));
+  }
+  void release_all() {
+    for (Chunk& c : q_)
+      if (c.ev) cudaEventDestroy(c.ev);
+    q_.clear();
+    if (base_) cudaFreeHost(base_);
+    base_ = nullptr;
+  }
+  // a chunk of `bytes` (rounded up to 256); waits for the oldest copies when
+  // the ring is full
+  Chunk* take(size_t bytes) {
+    bytes = (bytes + 255) / 256 * 256;
+    if (bytes > cap_) throw Error(SENGA_ERR_NOMEM, "pinned staging smaller than one request");
+    for (;;) {
+      reclaim();
+      size_t off = 0;
+      if (!q_.empty()) {
+        const size_t tail = q_.back().off + q_.back().len, head = q_.front().off;
+        if (tail >= head) {  // free: [tail, cap) and [0, head)
+          if (cap_ - tail >= bytes) off = tail;
+          else if (head >= bytes) off = 0;
+          else off = SIZE_MAX;
+        } else {  // free: [tail, head)
+          off = head - tail >= bytes ? tail : SIZE_MAX;
+        }
+      }
+      if (off != SIZE_MAX) {
+        Chunk c;
+        c.off = off;
+        c.len = bytes;
+        CKE(cudaEventCreateWithFlags(&c.ev, cudaEventDisableTiming));
+        q_.push_back(c);
+        return &q_.back();
+      }
+      // full: wait for the oldest chunk's copy
+      CKE(cudaEventSynchronize(q_.front().ev));
+    }
+  }
+  // wait for the oldest copy in flight (false when none)
+  bool wait_oldest() {
+    if (q_.empty()) return false;
+    CKE(cudaEventSynchronize(q_.front().ev));
+    reclaim();
+    return true;
+  }
+  char* ptr(const Chunk* c) const { return static_cast<char*>(base_) + c->off; }
+  // retire the completed chunks from the head (copies on one stream complete
+  // in order), running their host callbacks
+  void reclaim() {
+    while (!q_.empty() && cudaEventQuery(q_.front().ev) == cudaSuccess) {
+      Chunk c = q_.front();
+      q_.pop_front();
+      if (c.done) c.done(static_cast<const char*>(base_) + c.off);
+      cudaEventDestroy(c.ev);
+    }
+  }
+
+ private:
+  void* base_ = nullptr;
+  size_t cap_ = 0;
+  std::deque<Chunk> q_;
+};
+
 struct Member {
   int id = -1;
   senga_config cfg{};
@@ -150,6 +234,7 @@ struct Member {
   // serving: host copies of the initial state until admission, result after
   std::vector<double> h_fields, h_t;
   std::vector<int32_t> h_itn;
+  bool finishing = false;  // serving: last step queued, result not yet on the host
 };
 
 class Ensemble {
@@ -290,7 +375,7 @@ class Ensemble {
 
   // rebuild descriptors and work lists of the active members: boxes go into
   // tables of kTableBoxes, each with its contiguous run of tiles and chunks
-  void rebuild() {
+  void rebuild(PinnedRing* ring = nullptr) {
     drop_graph();
     groups_.clear();
     grid_stencil = 0;
@@ -340,11 +425,19 @@ class Ensemble {
       for (int k = 0; k < gr.nitems; ++k)
         for (int ph = 1; ph < 4; ++ph) ++nd[4 * items[gr.item0 + k].box + ph];
     }
+    std::vector<int> zeros((size_t)groups_.size() * kPersistCounters, 0);
+    if (ring) {  // serving: through the page-locked ring, stream-ordered, no wait
+      staged_upload(*ring, items, &d_items_, &cap_items_);
+      staged_upload(*ring, chunks, &d_chunks_, &cap_chunks_);
+      staged_upload(*ring, pitems, &d_pitems_, &cap_pitems_);
+      staged_upload(*ring, need, &d_need_, &cap_need_);
+      staged_upload(*ring, zeros, &d_ctr_, &cap_ctr_);
+      return;
+    }
     upload_vec(items, &d_items_, &cap_items_);
     upload_vec(chunks, &d_chunks_, &cap_chunks_);
     upload_vec(pitems, &d_pitems_, &cap_pitems_);
     upload_vec(need, &d_need_, &cap_need_);
-    std::vector<int> zeros((size_t)groups_.size() * kPersistCounters, 0);
     upload_vec(zeros, &d_ctr_, &cap_ctr_);
     CKE(cudaStreamSynchronize(stream));
   }
@@ -369,6 +462,12 @@ class Ensemble {
     for (int phase = 0; phase < 3; ++phase)
       for (const Group& gr : groups_)
         launch_batch_stencil(*gr.table, d_items_ + gr.item0, gr.nitems, irk - 1, phase, stream);
+  }
+  // one RK step launched kernel by kernel (the serving loop: its membership
+  // changes most ticks, so a graph would be captured anew each time)
+  void step_direct() {
+    for (int irk = 1; irk <= 5; ++irk) substage(irk);
+    CKE(cudaGetLastError());
   }
   void step_graph(int nsteps) {
     if (active.empty()) return;
@@ -457,6 +556,22 @@ class Ensemble {
   }
 
  private:
+  // the same through a page-locked chunk; a device array that must grow is
+  // reallocated with room to spare (cudaFree waits for the device)
+  template <class T>
+  void staged_upload(PinnedRing& ring, const std::vector<T>& v, T** d, size_t* cap) {
+    if (v.empty()) return;
+    if (v.size() > *cap) {
+      cudaFree(*d);
+      *d = nullptr;
+      CKE(cudaMalloc(d, 2 * v.size() * sizeof(T)));
+      *cap = 2 * v.size();
+    }
+    PinnedRing::Chunk* c = ring.take(v.size() * sizeof(T));
+    std::memcpy(ring.ptr(c), v.data(), v.size() * sizeof(T));
+    CKE(cudaMemcpyAsync(*d, ring.ptr(c), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    CKE(cudaEventRecord(c->ev, stream));
+  }
   template <class T>
   void upload_vec(const std::vector<T>& v, T** d, size_t* cap) {
     if (v.empty()) return;
@@ -612,6 +727,10 @@ int senga_batch_status(senga_batch* b, int* status) {
 }  // extern "C"
 
 // ============================================================================
+// page-locked staging of the serving loop; a request's state (and result)
+// may take half of it
+constexpr size_t kRingBytes = size_t(4) << 30;
+
 struct senga_server {
   Ensemble ens;
   std::map<int, Member*> all;  // every request ever submitted, by id
@@ -620,6 +739,11 @@ struct senga_server {
   int64_t gpsu_done = 0;
   double t0 = 0.0;
   int64_t max_points = 0;  // admission cap on the grid points advanced per tick (0: arena only)
+  PinnedRing ring;         // page-locked staging of every copy the loop makes
+  int64_t finishing_points = 0;  // points of requests whose results are still on the way
+  int finishing = 0, observed = 0;
+  cudaEvent_t step_ev[2] = {};  // the last two steps queued: at most two run ahead
+  int64_t steps_queued = 0;
 };
 
 extern "C" {
@@ -631,10 +755,12 @@ int senga_server_create(size_t arena_bytes, const senga_chem* chem, const senga_
   senga_server* s = new senga_server();
   int rc = guard2([&] {
     s->ens.init(*chem, diff, device, arena_bytes);
+    s->ring.init(kRingBytes);
     s->t0 = now_s();
   });
   if (rc != SENGA_OK) {
     s->ens.destroy();
+    s->ring.release_all();
     delete s;
     return rc;
   }
@@ -651,6 +777,7 @@ int senga_server_set_max_points(senga_server* s, int64_t max_points) {
 int senga_server_destroy(senga_server* s) {
   if (!s) return SENGA_OK;
   s->ens.destroy();
+  s->ring.release_all();
   for (auto& kv : s->all) delete kv.second;
   delete s;
   return SENGA_OK;
@@ -664,6 +791,9 @@ int senga_server_submit(senga_server* s, const senga_config* cfg, const double* 
     check_box(*cfg);
     if (box_bytes(*cfg, s->ens.nspec) > s->ens.arena.capacity())
       throw Error(SENGA_ERR_NOMEM, "senga_server_submit: request larger than the arena");
+    const size_t state_bytes = (size_t)cfg->nx * cfg->ny * cfg->nz * ((6 + s->ens.nspec) * sizeof(double) + 4);
+    if (2 * state_bytes > kRingBytes)
+      throw Error(SENGA_ERR_NOMEM, "senga_server_submit: request larger than half the page-locked staging");
     Member* m = new Member();
     m->id = s->next_id++;
     m->cfg = *cfg;
@@ -686,27 +816,45 @@ int senga_server_tick(senga_server* s, int* finished) {
   if (!s) return fail(SENGA_ERR_ARG, "senga_server_tick: null server");
   return guard2([&] {
     Ensemble& E = s->ens;
+    const int before = s->observed;
+    s->ring.reclaim();  // results that have arrived
     bool changed = false;
-    int64_t active_points = 0;
+    int64_t active_points = s->finishing_points;
     for (const Member* a : E.active) active_points += a->desc.g.n;
     while (!s->pending.empty()) {
       Member* m = s->pending.front();
       const int64_t n = (int64_t)m->cfg.nx * m->cfg.ny * m->cfg.nz;
       // the cap keeps a tick short, so requests run to completion in arrival
       // order instead of all sharing a slow tick; one request always fits
-      if (s->max_points > 0 && !E.active.empty() && active_points + n > s->max_points) break;
+      if (s->max_points > 0 && active_points > 0 && active_points + n > s->max_points) break;
       if (!E.place(*m)) break;  // admission by HBM footprint, first come first served
       active_points += n;
-      E.upload(*m, m->h_fields.data(), m->h_t.data(), m->h_itn.data());
+      // the initial state through a page-locked chunk: the copy is queued
+      // behind the kernels already on the stream, the host does not wait
+      const size_t fb = m->h_fields.size() * sizeof(double), tb = m->h_t.size() * sizeof(double);
+      const size_t ib = m->h_itn.size() * sizeof(int32_t);
+      PinnedRing::Chunk* c = s->ring.take(fb + tb + ib);
+      char* hp = s->ring.ptr(c);
+      std::memcpy(hp, m->h_fields.data(), fb);
+      std::memcpy(hp + fb, m->h_t.data(), tb);
+      std::memcpy(hp + fb + tb, m->h_itn.data(), ib);
+      E.upload(*m, reinterpret_cast<const double*>(hp), reinterpret_cast<const double*>(hp + fb),
+               reinterpret_cast<const int32_t*>(hp + fb + tb));
+      CKE(cudaEventRecord(c->ev, E.stream));
       m->t_admit = now_s() - s->t0;
       E.active.push_back(m);
       s->pending.pop_front();
       changed = true;
     }
-    if (changed) E.rebuild();
-    int done = 0;
+    if (changed) E.rebuild(&s->ring);
     if (!E.active.empty()) {
-      E.step_graph(1);
+      // at most two steps in flight ahead of the host
+      cudaEvent_t& ev = s->step_ev[s->steps_queued & 1];
+      if (!ev) CKE(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      else if (s->steps_queued >= 2) CKE(cudaEventSynchronize(ev));
+      E.step_direct();
+      CKE(cudaEventRecord(ev, E.stream));
+      ++s->steps_queued;
       std::vector<Member*> keep;
       std::vector<Member*> fin;
       for (Member* m : E.active) {
@@ -715,20 +863,42 @@ int senga_server_tick(senga_server* s, int* finished) {
         s->gpsu_done += 5 * m->desc.g.n;
         (m->steps_left > 0 ? keep : fin).push_back(m);
       }
-      if (!fin.empty()) {
-        for (Member* m : fin) E.download(*m, m->h_fields.data(), m->h_t.data(), m->h_itn.data());
-        CKE(cudaStreamSynchronize(E.stream));
-        const double t = now_s() - s->t0;
-        for (Member* m : fin) {
-          m->t_done = t;
-          E.unplace(*m);
-        }
-        E.active = keep;
-        E.rebuild();
-        done = (int)fin.size();
+      for (Member* m : fin) {
+        // the result through a page-locked chunk, copied out on the host
+        // once the download has completed; the arena room is reused in
+        // stream order
+        const size_t fb = m->h_fields.size() * sizeof(double), tb = m->h_t.size() * sizeof(double);
+        const size_t ib = m->h_itn.size() * sizeof(int32_t);
+        PinnedRing::Chunk* c = s->ring.take(fb + tb + ib);
+        char* hp = s->ring.ptr(c);
+        E.download(*m, reinterpret_cast<double*>(hp), reinterpret_cast<double*>(hp + fb),
+                   reinterpret_cast<int32_t*>(hp + fb + tb));
+        CKE(cudaEventRecord(c->ev, E.stream));
+        const int64_t n = m->desc.g.n;
+        m->finishing = true;
+        s->finishing_points += n;
+        s->finishing += 1;
+        c->done = [s, m, fb, tb, ib, n](const char* p) {
+          std::memcpy(m->h_fields.data(), p, fb);
+          std::memcpy(m->h_t.data(), p + fb, tb);
+          std::memcpy(m->h_itn.data(), p + fb + tb, ib);
+          m->t_done = now_s() - s->t0;
+          m->finishing = false;
+          s->finishing_points -= n;
+          s->finishing -= 1;
+          s->observed += 1;
+        };
+        E.unplace(*m);
       }
+      if (!fin.empty()) {
+        E.active = keep;
+        E.rebuild(&s->ring);
+      }
+    } else if (s->finishing > 0) {
+      s->ring.wait_oldest();  // nothing to run: wait for results on the way
     }
-    if (finished) *finished = done;
+    s->ring.reclaim();
+    if (finished) *finished = s->observed - before;
   });
 }
 
@@ -740,7 +910,8 @@ int senga_server_result(senga_server* s, int request_id, double* fields, double*
   auto it = s->all.find(request_id);
   if (it == s->all.end()) return fail(SENGA_ERR_ARG, "senga_server_result: unknown request");
   Member* m = it->second;
-  if (m->steps_left > 0 || m->t_done == 0.0) return fail(SENGA_ERR_ARG, "senga_server_result: not finished");
+  if (m->steps_left > 0 || m->finishing || m->t_done == 0.0)
+    return fail(SENGA_ERR_ARG, "senga_server_result: not finished");
   if (fields) std::memcpy(fields, m->h_fields.data(), m->h_fields.size() * sizeof(double));
   if (trun) std::memcpy(trun, m->h_t.data(), m->h_t.size() * sizeof(double));
   if (itn) std::memcpy(itn, m->h_itn.data(), m->h_itn.size() * sizeof(int32_t));
@@ -755,7 +926,8 @@ int senga_server_result(senga_server* s, int request_id, double* fields, double*
 // active/pending counts, grid-point substage updates so far, arena free bytes
 int senga_server_stats(senga_server* s, int* active, int* pending, int64_t* gpsu, int64_t* free_bytes) {
   if (!s) return fail(SENGA_ERR_ARG, "senga_server_stats: null server");
-  if (active) *active = (int)s->ens.active.size();
+  // requests whose results are still on the way count as active
+  if (active) *active = (int)s->ens.active.size() + s->finishing;
   if (pending) *pending = (int)s->pending.size();
   if (gpsu) *gpsu = s->gpsu_done;
   if (free_bytes) *free_bytes = (int64_t)s->ens.arena.free_bytes();
