@@ -170,6 +170,12 @@ int senga_profile_step(senga_ctx* ctx, double* ms, int* launches);
  * velocity, VTMP and energy RHS then stay on chip between the two passes;
  * off by default, since the two kernels measure faster). */
 int senga_ctx_species_fused(senga_ctx* ctx, int* fused_kernels);
+/* *mma = 1 when the context's species kernel takes its x derivatives on the
+ * FP64 tensor cores (band-matrix mma): all-periodic boxes of one context
+ * whose extents are multiples of 8, when SENGA_SPECIES_MMA=1 is set (read at
+ * every launch or graph capture; off by default, since the stencil form
+ * measures faster); the other boxes run the stencil form. */
+int senga_ctx_species_mma(senga_ctx* ctx, int* mma);
 
 /* Context facts: *mech = thermochemistry kernel in use (0 table-driven, 1 the
  * generated one-step R->P kernel, 2 the generated H2/air kernel), and the

@@ -214,6 +214,10 @@ void launch_flow(const Geo& g, const Fields& f, int, cudaStream_t s, const ZDec&
 }
 
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd) {
+  if (species_mma_ok(g, f, zd)) {
+    launch_species_mma(g, f, nspec, s);
+    return;
+  }
   const dim3 grid = tiles(g, SX_, SY_, SZ_);
   SpecMaps tm{};
   if (all_periodic(g)) {

@@ -504,6 +504,12 @@ int senga_ctx_species_fused(senga_ctx* c, int* fused_kernels) {
   return SENGA_OK;
 }
 
+int senga_ctx_species_mma(senga_ctx* c, int* mma) {
+  if (!c || !mma) return fail(SENGA_ERR_ARG, "senga_ctx_species_mma: null argument");
+  *mma = !fused(c) && species_mma_ok(c->geo, c->f, ZDec{}) ? 1 : 0;
+  return SENGA_OK;
+}
+
 int senga_ctx_info(senga_ctx* c, int* mech, int64_t* device_bytes) {
   if (!c) return fail(SENGA_ERR_ARG, "senga_ctx_info: null context");
   if (mech) *mech = c->mech;

@@ -159,6 +159,11 @@ void launch_flow(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const
 void launch_species_a(const Geo& g, const Fields& f, int nspec, cudaStream_t s, const ZDec& zd = ZDec{});
 void launch_species_b_rk(const Geo& g, const Fields& f, int nspec, const RK& rk, cudaStream_t s,
                          const ZDec& zd = ZDec{});
+// the species kernel with its x derivatives on the FP64 tensor cores
+// (species_mma.cu): all-periodic boxes of one context with extents that are
+// multiples of 8; launch_species_a takes it when species_mma_ok
+bool species_mma_ok(const Geo& g, const Fields& f, const ZDec& zd);
+void launch_species_mma(const Geo& g, const Fields& f, int nspec, cudaStream_t s);
 // the species kernel and the species+RK kernel as one (all-periodic boxes of
 // one context, when SENGA_FUSE=1 is set): the caller launches it in place of
 // both, after the flow kernel (and RADCAL)

@@ -140,6 +140,7 @@ def _load():
         "senga_profile_step": (ip, [vp, dp, C.POINTER(C.c_int)]),
         "senga_ctx_info": (ip, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64)]),
         "senga_ctx_species_fused": (ip, [vp, C.POINTER(C.c_int)]),
+        "senga_ctx_species_mma": (ip, [vp, C.POINTER(C.c_int)]),
         "senga_fp64_peak": (ip, [ip, dp]),
         "senga_filter": (ip, [vp, ip]),
         "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
@@ -479,6 +480,14 @@ class Box:
         """True when the species and species+RK kernels run as one launch."""
         v = C.c_int()
         _check(lib.senga_ctx_species_fused(self.h, C.byref(v)), "senga_ctx_species_fused")
+        return bool(v.value)
+
+    def species_mma(self):
+        """True when the species kernel takes its x derivatives on the FP64
+        tensor cores (SENGA_SPECIES_MMA=1, all-periodic boxes with extents that
+        are multiples of 8)."""
+        v = C.c_int()
+        _check(lib.senga_ctx_species_mma(self.h, C.byref(v)), "senga_ctx_species_mma")
         return bool(v.value)
 
     def info(self):
