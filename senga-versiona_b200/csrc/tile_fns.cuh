@@ -49,7 +49,9 @@ using SSlab = Slab<SX_, SY_, SZ_>;
 using SXRow = XRow<SX_, SY_, SZ_>;
 using SYRow = YRow<SX_, SY_, SZ_>;
 using SCol = Column<SZ_>;
-constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 3 * SSlab::SIZE;
+// the species kernel's rho w z-columns: one per thread, [k][thread]
+constexpr int kSpecColW = (SZ_ + 2 * H) * SX_ * SY_;
+constexpr int kSpecSmem = SXRow::SIZE + SYRow::SIZE + 3 * SSlab::SIZE + kSpecColW;
 // species+RK: two slabs, then the prefetched S register and rate of the next
 // species' own points, double-buffered: [buffer][run | rate][z][thread]
 constexpr int kRkPre = 2 * SZ_ * SX_ * SY_;
@@ -462,8 +464,16 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
   if (nspec > 0) stage_f(bS, tm ? &tm->y : nullptr, 0, f.y);
   // bytes of the group in flight (bulk paths): rho u, rho v and Y_0 first
   unsigned inflight = SXRow::kBulkBytes + SYRow::kBulkBytes + slab_bytes;
-  SCol rwc;
-  rwc.load(fo, tx, ty, LdT<NC>{rw});
+  // this thread's rho w z-column, kept in shared memory across the species
+  // loop (in registers it would take 24 of them for the whole loop)
+  double* const colw = sm + SXRow::SIZE + SYRow::SIZE + 3 * SSlab::SIZE;
+  {
+    SCol rwc;
+    rwc.load(fo, tx, ty, LdT<NC>{rw});
+#pragma unroll
+    for (int k = 0; k < SZ_ + 2 * H; ++k) colw[k * (SX_ * SY_) + threadIdx.x] = rwc.c[k];
+  }
+  auto wcol = [&](int k) { return colw[k * (SX_ * SY_) + threadIdx.x]; };
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) {
@@ -517,17 +527,17 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
             d2y = d2core([&](int m) { return yv[m + H]; }, t.gy, g.ny, 1) * g.ovd2[1];
             vc = fv[H];
           }
-          r = r - 0.5 * (d1px + d1py + d1zp<P>(g, t, cy, rwc));
+          r = r - 0.5 * (d1px + d1py + d1core([&](int m) { return cy.c[t.z + H + m] * wcol(t.z + H + m); }, t.gz, g.nz, 1) * g.ovd[2]);
           yz[z] = d1z<P>(g, t, cy);
-          r = r - 0.5 * (yx[z] * uc + yy[z] * vc + yz[z] * rwc.c[z + H]);
+          r = r - 0.5 * (yx[z] * uc + yy[z] * vc + yz[z] * wcol(z + H));
           rate[z] = r;
           fn3[z] = d2x + d2y + d2z<P>(g, t, cy);  // Laplacian for now
         } else {
-          r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1zp<P>(g, t, cy, rwc));
+          r = r - 0.5 * (d1p<0, P>(g, t, bS, bru) + d1p<1, P>(g, t, bS, brv) + d1core([&](int m) { return cy.c[t.z + H + m] * wcol(t.z + H + m); }, t.gz, g.nz, 1) * g.ovd[2]);
           yx[z] = d1<0, P>(g, t, bS);
           yy[z] = d1<1, P>(g, t, bS);
           yz[z] = d1z<P>(g, t, cy);
-          r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * rwc.c[z + H]);
+          r = r - 0.5 * (yx[z] * bru.v(t.x, t.y, t.z) + yy[z] * brv.v(t.x, t.y, t.z) + yz[z] * wcol(z + H));
           rate[z] = r;
           // FxxDIF/FxxADB zero the x diffusive terms on the face plane (rhscal.f:1581-1955)
           const bool dif = !P && (face_bits(g, t.gx) & BF_DIF);
