@@ -63,12 +63,12 @@ __global__ void __launch_bounds__(SX_* SY_, SENGA_SPECRK_MINB)
 // stay in this CTA's shared memory and V_c, VTMP and the energy RHS in
 // registers between the passes, instead of going through HBM (WDOT, VC,
 // VTMP, RHS(E): 28 doubles written and read back per point).
-constexpr int kSpecFusedSmem = kSpecSmem + kCarryRate;
+constexpr int kSpecFusedSmem = kSpecSmem - kSpecColW + kCarryRate;  // rates in place of the rho w slots
 __global__ void __launch_bounds__(SX_* SY_, SENGA_SPEC_MINB) k_species_fused_t(Geo g, Fields f, int nspec, RK rk) {
   extern __shared__ __align__(128) double sm[];
   __shared__ Folds<SX_, SY_, SZ_> fo;
   SpecCarry c;
-  c.rate = sm + kSpecSmem;
+  c.rate = sm + (kSpecSmem - kSpecColW);
   const Origin o{(int)blockIdx.x * SX_, (int)blockIdx.y * SY_, (int)blockIdx.z * SZ_};
   species_tile<true, 0, true, true>(g, f, nspec, o, sm, fo, ZDec{}, nullptr, nullptr, &c);
   species_rk_tile<true, 0, true, true>(g, f, nspec, rk, o, sm, fo, ZDec{}, nullptr, nullptr, &c);

@@ -465,15 +465,20 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
   // bytes of the group in flight (bulk paths): rho u, rho v and Y_0 first
   unsigned inflight = SXRow::kBulkBytes + SYRow::kBulkBytes + slab_bytes;
   // this thread's rho w z-column, kept in shared memory across the species
-  // loop (in registers it would take 24 of them for the whole loop)
+  // loop (in registers it would take 24 of them for the whole loop); the
+  // fused kernel (KEEP), whose shared memory holds the species rates past
+  // the slabs, keeps it in registers
   double* const colw = sm + SXRow::SIZE + SYRow::SIZE + 3 * SSlab::SIZE;
-  {
-    SCol rwc;
-    rwc.load(fo, tx, ty, LdT<NC>{rw});
+  SCol rwc;
+  rwc.load(fo, tx, ty, LdT<NC>{rw});
+  if constexpr (!KEEP) {
 #pragma unroll
     for (int k = 0; k < SZ_ + 2 * H; ++k) colw[k * (SX_ * SY_) + threadIdx.x] = rwc.c[k];
   }
-  auto wcol = [&](int k) { return colw[k * (SX_ * SY_) + threadIdx.x]; };
+  auto wcol = [&](int k) {
+    if constexpr (KEEP) return rwc.c[k];
+    else return colw[k * (SX_ * SY_) + threadIdx.x];
+  };
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_], dvm[SZ_];
 #pragma unroll
   for (int z = 0; z < SZ_; ++z) {
