@@ -25,9 +25,11 @@
 extern "C" {
 #endif
 
-/* Table dimensions: src/com_senga2.h:80-100,189 */
-#define SENGA_NSPCMX 9
-#define SENGA_NSTPMX 21
+/* Table dimensions: src/com_senga2.h:80-100,189. NSPCMX and NSTPMX are those
+ * of the reference's largest shipped case (src/casefiles/68step/com_senga2.h:74),
+ * so every mechanism it ships (1, 4, 21, 25 and 68 steps) fits. */
+#define SENGA_NSPCMX 18
+#define SENGA_NSTPMX 68
 #define SENGA_NTINMX 2
 #define SENGA_NCOFMX 7
 #define SENGA_NSSMAX 10
@@ -35,6 +37,12 @@ extern "C" {
 #define SENGA_NLLMAX 10
 #define SENGA_NDCFMX 4
 #define SENGA_NCFRMX 6
+
+/* ITNDEX, the temperature-interval index of every species at a point:
+ * base-4 digits, SENGA_NSPIMX species per 32-bit word (src/com_senga2.h:93-98).
+ * Every ITNDEX array below holds (nspec + 14) / 15 interior int32 arrays, one
+ * per word, words slowest: one array up to 15 species, two for 16 to 18. */
+#define SENGA_NSPIMX 15
 
 /* End conditions per face: src/com_senga2.h (NOBC/NBOUND/NPERI) */
 #define SENGA_NOBC 0

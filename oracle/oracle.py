@@ -26,7 +26,7 @@ def build():
 
 class _Bc(C.Structure):
     _fields_ = [("xl", C.c_int), ("xr", C.c_int), ("u_in", C.c_double), ("rho_in", C.c_double),
-                ("y_in", C.c_double * 9), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
+                ("y_in", C.c_double * 18), ("p_inf", C.c_double), ("sigma", C.c_double), ("eta", C.c_double),
                 ("pio", C.c_int), ("bet_local", C.c_int), ("t_in", C.c_double),
                 ("t_wall", C.c_double * 2), ("nrieta", C.c_double * 6)]
 
@@ -120,16 +120,22 @@ class Oracle:
         except Exception:
             pass
 
+    def _itn_shape(self):
+        """ITNDEX arrays: 15 species per word, words slowest beyond one."""
+        nw = (self.nspec + 14) // 15
+        return self.shape if nw == 1 else (nw,) + self.shape
+
     def upload(self, fields, trun, itndex):
         f = np.ascontiguousarray(fields, dtype=np.float64)
         t = np.ascontiguousarray(trun, dtype=np.float64)
         it = np.ascontiguousarray(itndex, dtype=np.int32)
+        assert it.shape == self._itn_shape()
         _get().oracle_set_state(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)))
 
     def download(self):
         f = np.empty((self.nc,) + self.shape)
         t = np.empty(self.shape)
-        it = np.empty(self.shape, dtype=np.int32)
+        it = np.empty(self._itn_shape(), dtype=np.int32)
         _get().oracle_get_state(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)))
         return f, t, it
 
@@ -172,7 +178,7 @@ class Oracle:
         """TEMPIN on the state set last (its U register): T, ITNDEX, p and
         (bracket failures, bisection-limit failures)."""
         t = np.empty(self.shape)
-        it = np.empty(self.shape, dtype=np.int32)
+        it = np.empty(self._itn_shape(), dtype=np.int32)
         p = np.empty(self.shape)
         nf = (C.c_long * 2)()
         _get().oracle_tempin(self.h, float(trin), int(maxbis), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)), _dp(p),
@@ -255,10 +261,11 @@ class OracleChem:
     table(name) / nspec interface of the device library's Chem; for callers
     that must not load the device library (the CPU reference arm)."""
 
-    _SHAPES = {"ntint": (9,), "rgspec": (9,), "wmolar": (9,), "ncpoly": (9, 2), "ncenth": (9, 2),
-               "tinthi": (9, 2), "tintlo": (9, 2), "amasch": (9, 2, 7), "amascp": (9, 2, 7),
-               "ntroe": (1,), "nsrif": (1,), "nlind": (1,), "mtlist": (21,), "mslist": (21,), "mllist": (21,),
-               "rctroe": (10, 12), "rcsrif": (10, 8), "rclind": (10, 4)}
+    NSPCMX, NSTPMX = 18, 68  # the oracle's table dimensions (oracle_tables.hpp)
+    _SHAPES = {"ntint": (NSPCMX,), "rgspec": (NSPCMX,), "wmolar": (NSPCMX,), "ncpoly": (NSPCMX, 2),
+               "ncenth": (NSPCMX, 2), "tinthi": (NSPCMX, 2), "tintlo": (NSPCMX, 2), "amasch": (NSPCMX, 2, 7),
+               "amascp": (NSPCMX, 2, 7), "ntroe": (1,), "nsrif": (1,), "nlind": (1,), "mtlist": (NSTPMX,),
+               "mslist": (NSTPMX,), "mllist": (NSTPMX,), "rctroe": (10, 12), "rcsrif": (10, 8), "rclind": (10, 4)}
     _INT = ("ntint", "ncpoly", "ncenth", "ntroe", "nsrif", "nlind", "mtlist", "mslist", "mllist")
 
     def __init__(self, path):

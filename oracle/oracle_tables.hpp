@@ -24,7 +24,9 @@
 namespace orc {
 
 // Dimensions (src/com_senga2.h:80-100)
-constexpr int NSPCMX = 9, NSTPMX = 21, NTINMX = 2, NCOFMX = 7, NCTMAX = 5;
+// NSPCMX and NSTPMX as the reference's largest shipped case compiles them
+// (src/casefiles/68step/com_senga2.h:74)
+constexpr int NSPCMX = 18, NSTPMX = 68, NTINMX = 2, NCOFMX = 7, NCTMAX = 5;
 constexpr int NSPIMX = 15, NTBASE = 4, NINTMX = 2, NBDYMX = 10;
 constexpr int NSSMAX = 10, NRSMAX = 10, NLLMAX = 10;
 constexpr int NDCFMX = 4, NVCFMX = 4, NCCFMX = 4;

@@ -73,6 +73,9 @@ struct IField {
   inline int32_t& operator()(int i, int j, int k) {
     return v[(size_t)(i - 1 + NHALO) + (size_t)bx * ((size_t)(j - 1 + NHALO) + (size_t)by * (size_t)(k - 1 + NHALO))];
   }
+  inline int32_t operator()(int i, int j, int k) const {
+    return v[(size_t)(i - 1 + NHALO) + (size_t)bx * ((size_t)(j - 1 + NHALO) + (size_t)by * (size_t)(k - 1 + NHALO))];
+  }
 };
 
 // FD coefficients, src/dfinit.f:42-482 (interior, closures, mixed).
@@ -164,7 +167,34 @@ struct Oracle {
   Field wd1x, wd1y, wd1z, wd2x, wd2y, wd2z, pd1x, pd1y, pd1z, pd2x, pd2y, pd2z;
   Field td1x, td1y, td1z, td2x, td2y, td2z, tdrmix;
   bool flmsor[NSPCMX] = {}, flmduf[NSPCMX] = {}, flmtdr[NSPCMX] = {};
-  IField itndex;
+  // ITNDEX(IC,JC,KC,IINDEX): NINTMX words per point, NSPIMX species a word
+  // in base NTBASE (src/com_senga2.h:93-98)
+  IField itndex[NINTMX];
+  // one point's ITNDEX; species is (1-based) is digit IPOWER = IS -
+  // (IINDEX-1)*NSPIMX - 1 of word IINDEX = 1 + (IS-1)/NSPIMX
+  // (src/temper.f:92-96, 196-200)
+  struct Itn {
+    int w[NINTMX] = {};
+    void add(int is, int itint) {
+      const int iw = (is - 1) / NSPIMX;
+      w[iw] = w[iw] + (itint - 1) * ipow(NTBASE, is - iw * NSPIMX - 1);
+    }
+    int get(int is) const {
+      const int iw = (is - 1) / NSPIMX;
+      const int icoef2 = ipow(NTBASE, is - iw * NSPIMX - 1), icoef1 = icoef2 * NTBASE;
+      return 1 + (w[iw] % icoef1) / icoef2;
+    }
+  };
+  // words an interior ITNDEX array carries: enough for nspec species
+  int nword() const { return 1 + (nspec - 1) / NSPIMX; }
+  Itn itn_at(int ic, int jc, int kc) const {
+    Itn v;
+    for (int w = 0; w < NINTMX; ++w) v.w[w] = itndex[w](ic, jc, kc);
+    return v;
+  }
+  void itn_put(int ic, int jc, int kc, const Itn& v) {
+    for (int w = 0; w < NINTMX; ++w) itndex[w](ic, jc, kc) = v.w[w];
+  }
   Field wk1, wk2, wk3, wk4;  // chrate STORE1..4 counterparts
 
   void init(const Config& c, const std::string& chem, const std::string& diff) {
@@ -198,7 +228,7 @@ struct Oracle {
       for (auto& f : v) f.init(nx, ny, nz);
     };
     mk(yrun); mk(yrhs); mk(yerr); mk(rate); mk(rrte);
-    itndex.init(nx, ny, nz);
+    for (auto& f : itndex) f.init(nx, ny, nz);
     dtinit(c.tstep);
     tstep_now = c.tstep;
   }
@@ -708,15 +738,13 @@ struct Oracle {
     const double t = tin, u = uin, v = 0.0, w = 0.0;
     for (int kc = kstal; kc <= kstol; ++kc)
       for (int jc = jstal; jc <= jstol; ++jc) {
-        int itnew = 0;
+        Itn itnew;
         for (int is = 1; is <= nspec; ++is) {
           int itint = 1;
           while (t > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
-          int pw = 1;
-          for (int qq = 0; qq < is - 1; ++qq) pw *= NTBASE;
-          itnew = itnew + (itint - 1) * pw;
+          itnew.add(is, itint);
         }
-        itndex(ic, jc, kc) = itnew;
+        itn_put(ic, jc, kc, itnew);
         const double d = drhs(ic, jc, kc);
         urhs(ic, jc, kc) = d * u;
         vrhs(ic, jc, kc) = d * v;
@@ -724,7 +752,7 @@ struct Oracle {
         double er = 0.5 * (u * u + v * v + w * w);
         er = d * er;
         for (int is = 1; is <= nspec; ++is) {
-          const int itint = 1 + (itnew / ipow(NTBASE, is - 1)) % NTBASE;
+          const int itint = itnew.get(is);
           const int k2 = Chem::c2(itint, is);
           double fornow = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
           for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) fornow = fornow * t + ch.amasch[Chem::c3(icp, itint, is)];
@@ -755,12 +783,12 @@ struct Oracle {
     return r;
   }
   // ITNDEX of one temperature (the interval search of boundt.f:262-290)
-  int interval_of(double t) const {
-    int itnew = 0;
+  Itn interval_of(double t) const {
+    Itn itnew;
     for (int is = 1; is <= nspec; ++is) {
       int itint = 1;
       while (t > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
-      itnew = itnew + (itint - 1) * ipow(NTBASE, is - 1);
+      itnew.add(is, itint);
     }
     return itnew;
   }
@@ -785,15 +813,15 @@ struct Oracle {
       for (int jc = jstal; jc <= jstol; ++jc) {
         const double t = w2 ? twall[left ? 0 : 1] : wall_t(ic, st, jc, kc);
         if (!w2) trun(ic, jc, kc) = t;
-        const int itnew = interval_of(t);
-        itndex(ic, jc, kc) = itnew;
+        const Itn itnew = interval_of(t);
+        itn_put(ic, jc, kc, itnew);
         urhs(ic, jc, kc) = 0.0;
         vrhs(ic, jc, kc) = 0.0;
         wrhs(ic, jc, kc) = 0.0;
         double er = 0.0;
         er = drhs(ic, jc, kc) * er;
         for (int is = 1; is <= nspec; ++is) {
-          const int itint = 1 + (itnew / ipow(NTBASE, is - 1)) % NTBASE;
+          const int itint = itnew.get(is);
           const int k2 = Chem::c2(itint, is);
           double fornow = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
           for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) fornow = fornow * t + ch.amasch[Chem::c3(icp, itint, is)];
@@ -1312,13 +1340,9 @@ struct Oracle {
           tcoeff[0] = 0.5 * ukuk - erhs(ic, jc, kc);
           for (int icp = 1; icp <= NCTMAX; ++icp) { tcoeff[icp] = 0.0; tderiv[icp] = 0.0; }
           double st7 = 0.0;
-          int itn = itndex(ic, jc, kc);
+          const Itn itn = itn_at(ic, jc, kc);
           for (int is = 1; is <= nspec; ++is) {
-            int ipower = is - 1;
-            int icoef2 = 1;
-            for (int q = 0; q < ipower; ++q) icoef2 *= NTBASE;
-            int icoef1 = icoef2 * NTBASE;
-            int itint = 1 + (itn % icoef1) / icoef2;
+            int itint = itn.get(is);
             double y = yrhs[is - 1](ic, jc, kc);
             int k2 = Chem::c2(itint, is);
             tcoeff[0] = tcoeff[0] + y * ch.amascp[Chem::c3(ch.ncenth[k2], itint, is)];
@@ -1347,21 +1371,19 @@ struct Oracle {
             break;
           }
           trun(ic, jc, kc) = tempor;
-          int itnew = 0;
+          Itn itnew;
           double tr = 0.0;
           for (int is = 1; is <= nspec; ++is) {
             int itint = 1;
             while (trun(ic, jc, kc) > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
-            int p = 1;
-            for (int q = 0; q < is - 1; ++q) p *= NTBASE;
-            itnew = itnew + (itint - 1) * p;
+            itnew.add(is, itint);
             int k2 = Chem::c2(itint, is);
             double cpf = ch.amascp[Chem::c3(ch.ncpoly[k2], itint, is)];
             for (int icp = ch.ncpom1[k2]; icp >= 1; --icp)
               cpf = cpf * trun(ic, jc, kc) + ch.amascp[Chem::c3(icp, itint, is)];
             tr = tr + yrhs[is - 1](ic, jc, kc) * cpf;
           }
-          itndex(ic, jc, kc) = itnew;
+          itn_put(ic, jc, kc, itnew);
           transp(ic, jc, kc) = tr / drhs(ic, jc, kc);
           store7(ic, jc, kc) = st7;
           prun(ic, jc, kc) = trun(ic, jc, kc) * store7(ic, jc, kc);
@@ -1421,14 +1443,12 @@ struct Oracle {
           // INDATA: density from PRUN = PRIN, interval index, energy, products
           const double rt = st1 * t;
           const double rho = prin / rt;
-          int itnew = 0;
+          Itn itnew;
           double e = 0.0;
           for (int is = 1; is <= nspec; ++is) {
             int itint = 1;
             while (t > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
-            int pw = 1;
-            for (int qq = 0; qq < is - 1; ++qq) pw *= NTBASE;
-            itnew = itnew + (itint - 1) * pw;
+            itnew.add(is, itint);
             const int k2 = Chem::c2(itint, is);
             double fornow = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
             for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) fornow = fornow * t + ch.amasch[Chem::c3(icp, itint, is)];
@@ -1450,7 +1470,7 @@ struct Oracle {
           erhs(ic, jc, kc) = erun(ic, jc, kc);
           for (int is = 0; is < nspec; ++is) yrhs[is](ic, jc, kc) = yrun[is](ic, jc, kc);
           trun(ic, jc, kc) = t;
-          itndex(ic, jc, kc) = itnew;
+          itn_put(ic, jc, kc, itnew);
         }
   }
 
@@ -1540,21 +1560,19 @@ struct Oracle {
             if (it == maxbis) ++nbisect;
           }
           trun(ic, jc, kc) = tempor;
-          int itnew = 0;
+          Itn itnew;
           double tr = 0.0, st7 = 0.0;
           for (int is = 1; is <= nspec; ++is) {
             int itint = 1;
             while (tempor > ch.tinthi[Chem::c2(itint, is)] && itint < ch.ntint[is - 1]) ++itint;
-            int pw = 1;
-            for (int q = 0; q < is - 1; ++q) pw *= NTBASE;
-            itnew = itnew + (itint - 1) * pw;
+            itnew.add(is, itint);
             const int k2 = Chem::c2(itint, is);
             double cpf = ch.amascp[Chem::c3(ch.ncpoly[k2], itint, is)];
             for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) cpf = cpf * tempor + ch.amascp[Chem::c3(icp, itint, is)];
             tr = tr + yrhs[is - 1](ic, jc, kc) * cpf;
             st7 = st7 + yrhs[is - 1](ic, jc, kc) * ch.rgspec[is - 1];
           }
-          itndex(ic, jc, kc) = itnew;
+          itn_put(ic, jc, kc, itnew);
           transp(ic, jc, kc) = tr / drhs(ic, jc, kc);
           store7(ic, jc, kc) = st7;
           prun(ic, jc, kc) = tempor * st7;
@@ -1566,7 +1584,7 @@ struct Oracle {
   void chrate_point(int ic, int jc, int kc) {
     const double YSMALL = 1.0e-30, YDENOM = 1.0e-15, CLNTEN = std::log(10.0);
     double T = trun(ic, jc, kc);
-    int itn = itndex(ic, jc, kc);
+    const Itn itn = itn_at(ic, jc, kc);
     for (int is = 1; is <= nspec; ++is) rate[is - 1](ic, jc, kc) = 0.0;
     // STORE3 keeps the last third-body concentration across steps, as in the
     // reference (a falloff step without its own third body would reuse it).
@@ -1656,9 +1674,7 @@ struct Oracle {
       if (ch.mglist[ist - 1] != 0) {
         for (int isl = 1; isl <= ch.nsslen[ist - 1]; ++isl) {
           int is = ch.nsspec[Chem::ss(isl, ist)];
-          int p = 1;
-          for (int q = 0; q < is - 1; ++q) p *= NTBASE;
-          int itint = 1 + (itn % (p * NTBASE)) / p;
+          int itint = itn.get(is);
           int k2 = Chem::c2(itint, is);
           double g = ch.amolgb[Chem::c3(ch.ncpoly[k2], itint, is)];
           for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) g = ch.amolgb[Chem::c3(icp, itint, is)] + g * T;
@@ -1971,11 +1987,8 @@ struct Oracle {
         wcor(ic, jc, kc) = wcor(ic, jc, kc) + store7(ic, jc, kc) * store3(ic, jc, kc);
       }
       {
-        int p = 1;
-        for (int q = 0; q < is - 1; ++q) p *= NTBASE;
-        const int icoef2 = p, icoef1 = p * NTBASE;
         BIG3 {
-          int itint = 1 + (itndex(ic, jc, kc) % icoef1) / icoef2;
+          int itint = itn_at(ic, jc, kc).get(is);
           int k2 = Chem::c2(itint, is);
           double f = ch.amasch[Chem::c3(ch.ncpoly[k2], itint, is)];
           for (int icp = ch.ncpom1[k2]; icp >= 1; --icp) f = f * trun(ic, jc, kc) + ch.amasch[Chem::c3(icp, itint, is)];
@@ -2627,7 +2640,7 @@ int oracle_set_state(void* h, const double* fields, const double* t, const int32
       for (int i = 1; i <= o->nx; ++i) {
         size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
         o->trun(i, j, k) = t[q];
-        o->itndex(i, j, k) = itn[q];
+        for (int w = 0; w < o->nword(); ++w) o->itndex[w](i, j, k) = itn[w * n + q];
       }
   auto wrap = [&](int a, int n_) { return ((a - 1) % n_ + n_) % n_ + 1; };
   for (int k = o->kstab; k <= o->kstob; ++k)
@@ -2635,7 +2648,7 @@ int oracle_set_state(void* h, const double* fields, const double* t, const int32
       for (int i = o->istab; i <= o->istob; ++i) {
         int ii = wrap(i, o->nx), jj = wrap(j, o->ny), kk = wrap(k, o->nz);
         o->trun(i, j, k) = o->trun(ii, jj, kk);
-        o->itndex(i, j, k) = o->itndex(ii, jj, kk);
+        for (auto& f : o->itndex) f(i, j, k) = f(ii, jj, kk);
       }
   return 0;
 }
@@ -2651,7 +2664,7 @@ int oracle_flamin(void* h, double trin, double prin, double drin, double urin, c
   o->flamin(trin, prin, drin, urin, v, w);
   const size_t n = (size_t)o->nx * o->ny * o->nz;
   std::vector<double> f((size_t)(5 + o->nspec) * n), t(n);
-  std::vector<int32_t> itn(n);
+  std::vector<int32_t> itn((size_t)o->nword() * n);
   oracle_get_state(h, f.data(), t.data(), itn.data());
   return oracle_set_state(h, f.data(), t.data(), itn.data());
 }
@@ -2663,12 +2676,14 @@ int oracle_tempin(void* h, double trin, int maxbis, double* t, int32_t* itn, dou
   auto* o = static_cast<orc::Oracle*>(h);
   const auto fails = o->tempin(trin, maxbis);
   if (nfail) { nfail[0] = fails.first; nfail[1] = fails.second; }
+  const size_t n = (size_t)o->nx * o->ny * o->nz;
   for (int k = 1; k <= o->nz; ++k)
     for (int j = 1; j <= o->ny; ++j)
       for (int i = 1; i <= o->nx; ++i) {
         size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
         if (t) t[q] = o->trun(i, j, k);
-        if (itn) itn[q] = o->itndex(i, j, k);
+        if (itn)
+          for (int w = 0; w < o->nword(); ++w) itn[w * n + q] = o->itndex[w](i, j, k);
         if (p) p[q] = o->prun(i, j, k);
       }
   return 0;
@@ -2685,7 +2700,8 @@ int oracle_get_state(void* h, double* fields, double* t, int32_t* itn) {
         size_t q = (size_t)(i - 1) + (size_t)o->nx * ((j - 1) + (size_t)o->ny * (k - 1));
         for (size_t f = 0; f < run.size(); ++f) fields[f * n + q] = (*run[f])(i, j, k);
         if (t) t[q] = o->trun(i, j, k);
-        if (itn) itn[q] = o->itndex(i, j, k);
+        if (itn)
+          for (int w = 0; w < o->nword(); ++w) itn[w * n + q] = o->itndex[w](i, j, k);
       }
   return 0;
 }
@@ -2731,7 +2747,7 @@ int oracle_rhs(void* h, double* rhs_out, double* t_out, double* p_out) {
 struct oracle_bc {
   int xl, xr;
   double u_in, rho_in;
-  double y_in[9];
+  double y_in[orc::NSPCMX];
   double p_inf, sigma, eta;
   int pio, bet_local;
   double t_in;

@@ -28,16 +28,26 @@ NPERI = 2
 
 
 def interval_index(chem, T):
-    """ITNDEX: 2 bits per species holding the thermo interval of T."""
-    itn = np.zeros(T.shape, dtype=np.int32)
+    """ITNDEX: base-4 digits (2 bits) per species holding the thermo interval
+    of T, 15 species per 32-bit word; shaped like T up to 15 species, else
+    (words,) + T.shape, words slowest."""
+    nw = (chem.nspec + 14) // 15
+    itn = np.zeros((nw,) + T.shape, dtype=np.int32)
     ntint = chem.table("ntint")
     tinthi = chem.table("tinthi")
     for s in range(chem.nspec):
         it = np.zeros(T.shape, dtype=np.int32)
         for k in range(ntint[s] - 1):
             it = np.where((it == k) & (T > tinthi[s, k]), k + 1, it)
-        itn += it << (2 * s)
-    return itn
+        itn[s // 15] += it << (2 * (s % 15))
+    return itn[0] if nw == 1 else itn
+
+
+def interval_of(itn, s, grid_ndim):
+    """Interval (0-based) of species s from an ITNDEX array over a grid of
+    grid_ndim dimensions."""
+    word = itn if itn.ndim == grid_ndim else itn[s // 15]
+    return (word >> (2 * (s % 15))) & 3
 
 
 def species_enthalpy(chem, s, T, itn):
@@ -45,7 +55,7 @@ def species_enthalpy(chem, s, T, itn):
     ncpoly = chem.table("ncpoly")
     ncenth = chem.table("ncenth")
     amasch = chem.table("amasch")
-    it = (itn >> (2 * s)) & 3
+    it = interval_of(itn, s, T.ndim)
     h = np.zeros(T.shape)
     for k in np.unique(it):
         m = it == k
@@ -170,7 +180,7 @@ def stable_dt(chem, fields, T, lengths, shape, cfl=0.5):
     cp = np.zeros(T.shape)
     ncpoly = chem.table("ncpoly")
     for s in range(chem.nspec):
-        it = (itn >> (2 * s)) & 3
+        it = interval_of(itn, s, T.ndim)
         for k in np.unique(it):
             m = it == k
             c = amascp[s, k]

@@ -257,6 +257,10 @@ class Ensemble {
     if (d) diff = *d;
     else std::memset(&diff, 0, sizeof(diff));
     nspec = c.nspec;
+    // the batched thermochemistry kernels are built for up to 9 species
+    // (one ITNDEX word); the larger mechanisms run as single contexts
+    if (nspec < 1 || nspec > 9)
+      throw Error(SENGA_ERR_UNSUPPORTED, "batched ensembles and the serving loop take mechanisms of at most 9 species");
     nc = 5 + nspec;
     device = dev;
     mech = select_mech(chem, diff);

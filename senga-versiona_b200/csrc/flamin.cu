@@ -11,6 +11,7 @@
 // u = DRIN URIN / rho (:300-318). INDATA then: rho = PRIN / (T sum_k R_k Y_k),
 // ITNDEX from T, E = sum_k Y_k h_k(T) - T sum_k R_k Y_k + |u|^2/2 and the
 // conserved products rho (1, u, v, w, E, Y_k) (:1233-1394).
+#include "itndex.cuh"
 #include "senga_internal.h"
 
 namespace senga {
@@ -63,12 +64,12 @@ __global__ void __launch_bounds__(kBlock) k_flamin(FlaminArgs a, const senga_che
   const double u = a.flxmas / (a.prin / (st1 * T));  // FLAMIN's own density
   const double rt = st1 * T;
   const double rho = a.prin / rt;
-  int32_t code = 0;
+  uint64_t code = 0;
   double e = 0.0;
   for (int s = 0; s < a.nspec; ++s) {
     int it = 0;
     while (T > C->tinthi[s][it] && it + 1 < C->ntint[s]) ++it;
-    code += it << (2 * s);
+    code += (uint64_t)it << (2 * s);
     const double* ch = C->amasch[s][it];
     double h = ch[C->ncpoly[s][it] - 1];
     for (int icp = C->ncpom1[s][it]; icp >= 1; --icp) h = h * T + ch[icp - 1];
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(kBlock) k_flamin(FlaminArgs a, const senga_che
     uin[f * n + q] = c[f];
   }
   t[q] = T;
-  itn[q] = code;
+  itn_store(itn, n, q, a.nspec, code);
 }
 
 }  // namespace

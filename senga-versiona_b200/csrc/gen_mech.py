@@ -274,8 +274,9 @@ def gen(tag, c, d):
     w(f"  static constexpr int NS = {ns};")
     w(f"  static constexpr bool MAVT = {'true' if mavt else 'false'};")
     w("  __device__ __forceinline__ bool has(int) const { return true; }")
+    w("  __device__ __forceinline__ int count() const { return NS; }")
     # ---- temper coefficients
-    w("  __device__ __forceinline__ void temper_coeffs(const double (&ry)[NS], int32_t itn0, double (&tc)[6], double (&td)[6], double& rmix) const {")
+    w("  __device__ __forceinline__ void temper_coeffs(const double (&ry)[NS], uint64_t itn0, double (&tc)[6], double (&td)[6], double& rmix) const {")
     for s in range(ns):
         w(f"    {{ const int it = (itn0 >> {2 * s}) & 1; const double y = ry[{s}];")
         nint = c["ntint"][s]
@@ -296,12 +297,12 @@ def gen(tag, c, d):
         w(f"      rmix = rmix + y * {h(c['rgspec'][s])}; }}")
     w("  }")
     # ---- locate + cp
-    w("  __device__ __forceinline__ void locate(double T, const double (&ry)[NS], int32_t& itn, double& cpsum) const {")
+    w("  __device__ __forceinline__ void locate(double T, const double (&ry)[NS], uint64_t& itn, double& cpsum) const {")
     w("    itn = 0; cpsum = 0.0;")
     for s in range(ns):
         np_ = c["ncpoly"][s][0]
         if c["ntint"][s] > 1:
-            w(f"    {{ const int it = T > {h(c['tinthi'][s][0])} ? 1 : 0; itn += it << {2 * s};")
+            w(f"    {{ const int it = T > {h(c['tinthi'][s][0])} ? 1 : 0; itn += (uint64_t)it << {2 * s};")
         else:
             w("    { const int it = 0; (void)it;")
         cp0, cp1 = c["amascp"][s][0], (c["amascp"][s][1] if c["ntint"][s] > 1 else c["amascp"][s][0])
@@ -354,7 +355,7 @@ def gen(tag, c, d):
         w("    for (int s = 0; s < NS; ++s) rd[s] = 0.0;")
     w("  }")
     # ---- enthalpy
-    w("  __device__ __forceinline__ void enthalpy(double T, int32_t itn, double (&hk)[NS]) const {")
+    w("  __device__ __forceinline__ void enthalpy(double T, uint64_t itn, double (&hk)[NS]) const {")
     for s in range(ns):
         np_, nh = c["ncpoly"][s][0], c["ncenth"][s][0]
         a0 = c["amasch"][s][0]
@@ -365,7 +366,7 @@ def gen(tag, c, d):
         w(f"      hk[{s}] = {sel('it', h(a0[nh - 1]), h(a1[nh - 1]))} + v * T; }}")
     w("  }")
     # ---- CHRATE
-    w("  __device__ __forceinline__ void chrate(double T, int32_t itn, const double (&ry)[NS], double (&rate)[NS]) const {")
+    w("  __device__ __forceinline__ void chrate(double T, uint64_t itn, const double (&ry)[NS], double (&rate)[NS]) const {")
     w("    const double lnT = log(T); const double ovT = 1.0 / T; (void)itn;")
     for s in range(ns):
         w(f"    rate[{s}] = 0.0;")

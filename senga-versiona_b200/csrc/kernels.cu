@@ -160,9 +160,12 @@ int launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const 
   } else if (nspec <= 2) {
     if (flmavt) k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<2, true>{dchem, ddiff, nspec});
     else k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<2, false>{dchem, ddiff, nspec});
-  } else {
+  } else if (nspec <= 9) {
     if (flmavt) k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<9, true>{dchem, ddiff, nspec});
     else k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<9, false>{dchem, ddiff, nspec});
+  } else {  // the reference's larger casefile mechanisms (16 and 18 species)
+    if (flmavt) k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<SENGA_NSPCMX, true>{dchem, ddiff, nspec});
+    else k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<SENGA_NSPCMX, false>{dchem, ddiff, nspec});
   }
   return 1;
 }

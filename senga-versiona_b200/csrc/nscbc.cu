@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include "senga_internal.h"
+#include "itndex.cuh"
 #include "stencil.cuh"
 
 namespace senga {
@@ -72,12 +73,12 @@ __device__ __forceinline__ double enthalpy(const senga_chem* chem, int s, int it
   for (int icp = chem->ncpom1[s][it]; icp >= 1; --icp) h = h * t + c[icp - 1];
   return c[chem->ncenth[s][it] - 1] + h * t;
 }
-__device__ __forceinline__ int32_t interval_index(const senga_chem* chem, int nspec, double t) {
-  int32_t itn = 0;
+__device__ __forceinline__ uint64_t interval_index(const senga_chem* chem, int nspec, double t) {
+  uint64_t itn = 0;
   for (int s = 0; s < nspec; ++s) {
     int it = 0;
     while (t > chem->tinthi[s][it] && it + 1 < chem->ntint[s]) ++it;
-    itn += it << (2 * s);
+    itn += (uint64_t)it << (2 * s);
   }
   return itn;
 }
@@ -111,12 +112,12 @@ __global__ void __launch_bounds__(kFaceBlock)
     } else {
       t = bc.t_wall[side];
     }
-    const int32_t itn = interval_index(chem, nspec, t);
-    f.itn[q] = itn;
+    const uint64_t itn = interval_index(chem, nspec, t);
+    itn_store(f.itn, n, q, nspec, itn);
     double e = 0.0;
     e = f.uin[q] * e;
     for (int s = 0; s < nspec; ++s)
-      e = e + (enthalpy(chem, s, (itn >> (2 * s)) & 3, t) - chem->rgspec[s] * t) * f.uin[(5 + s) * n + q];
+      e = e + (enthalpy(chem, s, (int)(itn >> (2 * s)) & 3, t) - chem->rgspec[s] * t) * f.uin[(5 + s) * n + q];
     for (int r = 0; r < (both ? 2 : 1); ++r) {
       double* U = regs[r];
       U[n + q] = 0.0;
@@ -132,14 +133,14 @@ __global__ void __launch_bounds__(kFaceBlock)
     // I2 (boundt.f:81-176, bountt.f:84-200): ITNDEX of TRIN, then velocity,
     // energy and species from the face density of the U register
     const double t = bc.t_in, u = bc.u_in, v = 0.0, w = 0.0;
-    const int32_t itn = interval_index(chem, nspec, t);
-    f.itn[q] = itn;
+    const uint64_t itn = interval_index(chem, nspec, t);
+    itn_store(f.itn, n, q, nspec, itn);
     const double d = f.uin[q];
     double e = 0.5 * (u * u + v * v + w * w);
     e = d * e;
     double ys[SENGA_NSPCMX];
     for (int s = 0; s < nspec; ++s) {
-      const double h = enthalpy(chem, s, (itn >> (2 * s)) & 3, t);
+      const double h = enthalpy(chem, s, (int)(itn >> (2 * s)) & 3, t);
       ys[s] = d * bc.y_in[s];
       e = e + (h - chem->rgspec[s] * t) * ys[s];
     }

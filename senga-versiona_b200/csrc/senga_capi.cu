@@ -142,7 +142,9 @@ void require_rhs(const senga_ctx* c) {
 }
 
 // species kernel and species+RK kernel as one launch (launch_species_fused)
-bool fused(const senga_ctx* c) { return !c->mixt && !c->nscbc && species_fusable(c->geo); }
+bool fused(const senga_ctx* c) {
+  return !c->mixt && !c->nscbc && c->nspec <= 9 && species_fusable(c->geo);  // the rates of 9 species fit on chip
+}
 
 // the fields the thermochemistry kernel writes: the momentum copy only for
 // the fused species kernel
@@ -276,9 +278,9 @@ int senga_ctx_create(const senga_config* cfg, const senga_chem* chem, const seng
     const int64_t n = c->geo.n;
     const int S = c->nspec, nc = c->nc;
     // pool layout (doubles): run nc | u nc | err nc? | t | p lam lcp mu | rd S | h S |
-    // hmix | wdot S | vel 3 | e | y S | rhs nc | divm | vc 3 | vtmp | mom 3 | itn (int32, n/2 doubles)
+    // hmix | wdot S | vel 3 | e | y S | rhs nc | divm | vc 3 | vtmp | mom 3 | itn (int32 words)
     const int64_t per_point = (int64_t)nc * 2 + (cfg->adaptive ? nc : 0) + 1 + 4 + 3 * S + 1 + 3 + 1 + S + nc + 1 + 3 + 1 + 3;
-    const int64_t total = per_point * n + (n + 1) / 2 + 64;
+    const int64_t total = per_point * n + (itn_words(S) * n + 1) / 2 + 64;
     CK(cudaMalloc(&c->pool, (size_t)total * sizeof(double)));
     CK(cudaMemsetAsync(c->pool, 0, (size_t)total * sizeof(double), c->stream));
     double* p = c->pool;
@@ -352,7 +354,8 @@ int senga_upload_state_host(senga_ctx* c, const double* fields, const double* tr
     CK(cudaMemcpyAsync(c->f.run, fields, bytes, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->f.uin, c->f.run, bytes, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->f.t, trun, c->geo.n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->f.itn, itn, c->geo.n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.itn, itn, itn_words(c->nspec) * c->geo.n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       c->stream));
     if (c->f.err) CK(cudaMemsetAsync(c->f.err, 0, bytes, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });
@@ -365,7 +368,8 @@ int senga_upload_state_async(senga_ctx* c, const double* fields, const double* t
     CK(cudaMemcpyAsync(c->f.run, fields, bytes, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->f.uin, c->f.run, bytes, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->f.t, trun, c->geo.n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->f.itn, itn, c->geo.n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->f.itn, itn, itn_words(c->nspec) * c->geo.n * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       c->stream));
     if (c->f.err) CK(cudaMemsetAsync(c->f.err, 0, bytes, c->stream));
   });
 }
@@ -376,7 +380,9 @@ int senga_download_state_async(senga_ctx* c, double* fields, double* trun, int32
     const size_t bytes = (size_t)c->nc * c->geo.n * sizeof(double);
     CK(cudaMemcpyAsync(fields, c->f.run, bytes, cudaMemcpyDeviceToHost, c->stream));
     if (trun) CK(cudaMemcpyAsync(trun, c->f.t, c->geo.n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (itn) CK(cudaMemcpyAsync(itn, c->f.itn, c->geo.n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (itn)
+      CK(cudaMemcpyAsync(itn, c->f.itn, itn_words(c->nspec) * c->geo.n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                         c->stream));
   });
 }
 
@@ -386,7 +392,9 @@ int senga_download_state_host(senga_ctx* c, double* fields, double* trun, int32_
     const size_t bytes = (size_t)c->nc * c->geo.n * sizeof(double);
     CK(cudaMemcpyAsync(fields, c->f.run, bytes, cudaMemcpyDeviceToHost, c->stream));
     if (trun) CK(cudaMemcpyAsync(trun, c->f.t, c->geo.n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (itn) CK(cudaMemcpyAsync(itn, c->f.itn, c->geo.n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (itn)
+      CK(cudaMemcpyAsync(itn, c->f.itn, itn_words(c->nspec) * c->geo.n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                         c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });
 }
@@ -566,7 +574,9 @@ int senga_tempin_host(senga_ctx* c, double trin, double* trun, int32_t* itndex, 
     launch_tempin(n, c->nspec, c->f.uin, c->d_chem, trin, c->f.t, c->f.itn, c->f.p, c->d_status, c->stream);
     CK(cudaGetLastError());
     if (trun) CK(cudaMemcpyAsync(trun, c->f.t, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (itndex) CK(cudaMemcpyAsync(itndex, c->f.itn, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (itndex)
+      CK(cudaMemcpyAsync(itndex, c->f.itn, itn_words(c->nspec) * n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                         c->stream));
     if (prun) CK(cudaMemcpyAsync(prun, c->f.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   });
@@ -1017,7 +1027,9 @@ int senga_zgroup_upload_host(senga_zgroup* g, const double* fields, const double
                            c->stream));
       CK(cudaMemcpyAsync(c->f.uin, c->f.run, (size_t)g->nc * nl * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
       CK(cudaMemcpyAsync(c->f.t, trun + r * nl, nl * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-      CK(cudaMemcpyAsync(c->f.itn, itn + r * nl, nl * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+      for (int w = 0; w < itn_words(c->nspec); ++w)  // one interior array per ITNDEX word
+        CK(cudaMemcpyAsync(c->f.itn + w * nl, itn + w * ng + r * nl, nl * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           c->stream));
     }
     for (int r = 0; r < g->nr; ++r) CK(cudaStreamSynchronize(g->ctx[r]->stream));
   });
@@ -1035,7 +1047,10 @@ int senga_zgroup_download_host(senga_zgroup* g, double* fields, double* trun, in
         CK(cudaMemcpyAsync(fields + fl * ng + r * nl, c->f.run + fl * nl, nl * sizeof(double), cudaMemcpyDeviceToHost,
                            c->stream));
       if (trun) CK(cudaMemcpyAsync(trun + r * nl, c->f.t, nl * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-      if (itn) CK(cudaMemcpyAsync(itn + r * nl, c->f.itn, nl * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+      if (itn)
+        for (int w = 0; w < itn_words(c->nspec); ++w)
+          CK(cudaMemcpyAsync(itn + w * ng + r * nl, c->f.itn + w * nl, nl * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             c->stream));
     }
     for (int r = 0; r < g->nr; ++r) CK(cudaStreamSynchronize(g->ctx[r]->stream));
   });

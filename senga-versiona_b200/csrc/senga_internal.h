@@ -67,13 +67,17 @@ __host__ __device__ __forceinline__ int face_bits(const Geo& g, int gx) {
 }
 
 // Device pointers of one box's registers and per-substage scratch.
+// 32-bit words of ITNDEX per grid point: base-4 digits, SENGA_NSPIMX species
+// a word (src/com_senga2.h:93-98); the words of a field are stored slowest
+constexpr int itn_words(int nspec) { return (nspec + SENGA_NSPIMX - 1) / SENGA_NSPIMX; }
+
 struct Fields {
   double* run;    // S register  [nc][n]   (xRUN)
   double* uin;    // U register read this substage  [nc][n] (xRHS on entry)
   double* uout;   // U register written by the RK update
   double* err;    // error register [nc][n] or nullptr (fixed dt)
   double* t;      // TRUN
-  int32_t* itn;   // ITNDEX (2 bits per species)
+  int32_t* itn;   // ITNDEX [itn_words(nspec)][n] (2 bits per species, 15 species a word)
   // scratch
   double* p;      // PRUN
   double* lam;    // thermal conductivity lambda

@@ -11,6 +11,7 @@
 // for bit. Where the source stops (no sign change inside the limits) the
 // point keeps its last iterate and sets status bit 1; the source bisects
 // without limit, here 200 halvings at most, after which status bit 2 is set.
+#include "itndex.cuh"
 #include "senga_internal.h"
 
 namespace senga {
@@ -105,14 +106,14 @@ __global__ void __launch_bounds__(kBlock) k_tempin(int64_t n, int nspec, const d
     }
     if (it == maxbis) atomicOr(status, 4u);
   }
-  int32_t code = 0;
+  uint64_t code = 0;
   double rmix = 0.0;
   for (int s = 0; s < nspec; ++s) {
-    code += interval_at(C, s, T) << (2 * s);
+    code += (uint64_t)interval_at(C, s, T) << (2 * s);
     rmix = __dadd_rn(rmix, __dmul_rn(ry[s], C->rgspec[s]));
   }
   t[q] = T;
-  itn[q] = code;
+  itn_store(itn, n, q, nspec, code);
   p[q] = __dmul_rn(T, rmix);
 }
 

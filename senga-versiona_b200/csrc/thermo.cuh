@@ -11,6 +11,7 @@
 
 #include <cstdint>
 
+#include "itndex.cuh"
 #include "mech_gen.cuh"
 #include "senga_internal.h"
 
@@ -24,7 +25,7 @@ constexpr int kBlock = 256;
 
 // Interval of species s packed in ITNDEX (2 bits per species). NTINMX = 2,
 // so only 0/1 are valid; the mask keeps a corrupt upload inside the tables.
-__device__ __forceinline__ int tint_of(int32_t itn, int s) { return (itn >> (2 * s)) & 1; }
+__device__ __forceinline__ int tint_of(uint64_t itn, int s) { return (int)(itn >> (2 * s)) & 1; }
 
 // Select-by-index update of a register array (keeps the array in registers
 // when the index comes from a table).
@@ -49,7 +50,7 @@ __device__ __forceinline__ double get_at(const double (&a)[NSM], int k) {
 // evaluates the same expressions per step, so the values are identical.
 template <int NSM>
 __device__ void chrate_point(const senga_chem* __restrict__ C, int nspec, const double (&ry)[NSM], double T,
-                             int32_t itn, double (&rate)[NSM]) {
+                             uint64_t itn, double (&rate)[NSM]) {
   const double lnT = log(T);
   const double ovT = 1.0 / T;
   double gib[NSM];
@@ -163,8 +164,9 @@ struct MechTables {
   int nspec;
 
   __device__ __forceinline__ bool has(int s) const { return s < nspec; }
+  __device__ __forceinline__ int count() const { return nspec; }
 
-  __device__ __forceinline__ void temper_coeffs(const double (&ry)[NS], int32_t itn0, double (&tc)[6], double (&td)[6],
+  __device__ __forceinline__ void temper_coeffs(const double (&ry)[NS], uint64_t itn0, double (&tc)[6], double (&td)[6],
                                                 double& rmix) const {
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
@@ -185,7 +187,7 @@ struct MechTables {
     }
   }
   // new interval index and sum_k rho Y_k cp_k (divided by rho by the caller)
-  __device__ __forceinline__ void locate(double T, const double (&ry)[NS], int32_t& itn, double& cpsum) const {
+  __device__ __forceinline__ void locate(double T, const double (&ry)[NS], uint64_t& itn, double& cpsum) const {
     itn = 0;
     cpsum = 0.0;
 #pragma unroll
@@ -193,7 +195,7 @@ struct MechTables {
       if (s >= nspec) continue;
       int it = 0;
       while (T > C->tinthi[s][it] && it + 1 < C->ntint[s]) ++it;
-      itn += it << (2 * s);
+      itn += (uint64_t)it << (2 * s);
       const int np = C->ncpoly[s][it];
       const double* cp = C->amascp[s][it];
       double c = cp[np - 1];
@@ -275,7 +277,7 @@ struct MechTables {
       mu = mu + y[s] * C->ovwmol[s] * (mk[s] / cc);
     }
   }
-  __device__ __forceinline__ void enthalpy(double T, int32_t itn, double (&h)[NS]) const {
+  __device__ __forceinline__ void enthalpy(double T, uint64_t itn, double (&h)[NS]) const {
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       h[s] = 0.0;
@@ -288,7 +290,7 @@ struct MechTables {
       h[s] = ch[C->ncenth[s][it] - 1] + v * T;
     }
   }
-  __device__ __forceinline__ void chrate(double T, int32_t itn, const double (&ry)[NS], double (&rate)[NS]) const {
+  __device__ __forceinline__ void chrate(double T, uint64_t itn, const double (&ry)[NS], double (&rate)[NS]) const {
     chrate_point<NS>(C, nspec, ry, T, itn, rate);
   }
 };
@@ -308,7 +310,7 @@ __device__ __forceinline__ void thermo_point(const Geo& g, const Fields& f, cons
   for (int s = 0; s < NS; ++s) ry[s] = m.has(s) ? U[(5 + s) * n + q] : 0.0;
   if (PART == 2) {
     double rate[NS];
-    m.chrate(f.t[q], f.itn[q], ry, rate);
+    m.chrate(f.t[q], itn_load(f, n, q, m.count()), ry, rate);
 #pragma unroll
     for (int s = 0; s < NS; ++s)
       if (m.has(s)) f.wdot[s * n + q] = rate[s];
@@ -323,7 +325,7 @@ __device__ __forceinline__ void thermo_point(const Geo& g, const Fields& f, cons
 #pragma unroll
   for (int i = 1; i < 6; ++i) tc[i] = td[i] = 0.0;
   double rmix = 0.0;
-  m.temper_coeffs(ry, f.itn[q], tc, td, rmix);
+  m.temper_coeffs(ry, itn_load(f, n, q, m.count()), tc, td, rmix);
   const double toltmp = (double)1.0e-10f;  // TOLTMP is a single-precision literal
   double T = f.t[q];
   int iters = 1;
@@ -346,13 +348,13 @@ __device__ __forceinline__ void thermo_point(const Geo& g, const Fields& f, cons
     }
     break;
   }
-  int32_t itn;
+  uint64_t itn;
   double cpm;
   m.locate(T, ry, itn, cpm);
   cpm = cpm / rho;
   const double p = T * rmix;
   f.t[q] = T;
-  f.itn[q] = itn;
+  itn_store(f.itn, n, q, m.count(), itn);
   f.p[q] = p;
   if (f.cp) {  // NSCBC face data (cp_mix, rho R_mix of TEMPER)
     f.cp[q] = cpm;

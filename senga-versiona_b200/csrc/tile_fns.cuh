@@ -412,7 +412,8 @@ struct SpecCarry {
   double vcx[SZ_], vcy[SZ_], vcz[SZ_], vt[SZ_], rE[SZ_];
   double* rate;
 };
-constexpr int kCarryRate = SENGA_NSPCMX * SZ_ * SX_ * SY_;  // doubles of shared memory
+constexpr int kFuseMaxSpec = 9;  // species the fused kernel carries on chip
+constexpr int kCarryRate = kFuseMaxSpec * SZ_ * SX_ * SY_;  // doubles of shared memory
 
 // M: 0 per-element cp.async, 1 bulk row copies, 2 one tensor copy per buffer
 // for tiles away from the wrap (bulk rows for the others)

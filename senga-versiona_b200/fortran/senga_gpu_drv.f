@@ -12,9 +12,10 @@ C                                           CALL GPUGET
 C
 C     Interior (std) ranges only cross the boundary; the conserved fields
 C     are packed field-slowest (rho, rho u, rho v, rho w, rho E, rho Y_k),
-C     as include/senga_gpu.h states. ITNDEX's first word carries the
-C     intervals of up to 15 species in base NTBASE = 4 (src/temper.f:
-C     195-201), the packing of the device's 32-bit index.
+C     as include/senga_gpu.h states. ITNDEX crosses as its first
+C     1 + (NSPEC-1)/NSPIMX words, each carrying the intervals of NSPIMX =
+C     15 species in base NTBASE = 4 (src/temper.f:195-201), the packing of
+C     the device's index.
 
       SUBROUTINE GPUINI
       USE ISO_C_BINDING
@@ -59,10 +60,12 @@ C     COMMON registers -> device (both RK registers = xRUN)
       USE SENGA_GPU
       INCLUDE 'com_senga2.h'
       DOUBLE PRECISION, ALLOCATABLE :: FLDS(:,:,:,:), TSTD(:,:,:)
-      INTEGER(C_INT32_T), ALLOCATABLE :: ISTD(:,:,:)
-      INTEGER IC,JC,KC,ISPEC,ISTAT
+      INTEGER(C_INT32_T), ALLOCATABLE :: ISTD(:,:,:,:)
+      INTEGER IC,JC,KC,ISPEC,ISTAT,IW,NWORD
+      NWORD = 1 + (NSPEC-1)/NSPIMX
       ALLOCATE(FLDS(NXNODE,NYNODE,NZNODE,5+NSPEC))
-      ALLOCATE(TSTD(NXNODE,NYNODE,NZNODE), ISTD(NXNODE,NYNODE,NZNODE))
+      ALLOCATE(TSTD(NXNODE,NYNODE,NZNODE))
+      ALLOCATE(ISTD(NXNODE,NYNODE,NZNODE,NWORD))
       DO KC = 1,NZNODE
         DO JC = 1,NYNODE
           DO IC = 1,NXNODE
@@ -75,7 +78,9 @@ C     COMMON registers -> device (both RK registers = xRUN)
               FLDS(IC,JC,KC,5+ISPEC) = YRUN(IC,JC,KC,ISPEC)
             ENDDO
             TSTD(IC,JC,KC) = TRUN(IC,JC,KC)
-            ISTD(IC,JC,KC) = ITNDEX(IC,JC,KC,1)
+            DO IW = 1,NWORD
+              ISTD(IC,JC,KC,IW) = ITNDEX(IC,JC,KC,IW)
+            ENDDO
           ENDDO
         ENDDO
       ENDDO
@@ -114,10 +119,12 @@ C     device -> COMMON registers (xRUN, and xRHS = xRUN as after FINCOM)
       USE SENGA_GPU
       INCLUDE 'com_senga2.h'
       DOUBLE PRECISION, ALLOCATABLE :: FLDS(:,:,:,:), TSTD(:,:,:)
-      INTEGER(C_INT32_T), ALLOCATABLE :: ISTD(:,:,:)
-      INTEGER IC,JC,KC,ISPEC,ISTAT
+      INTEGER(C_INT32_T), ALLOCATABLE :: ISTD(:,:,:,:)
+      INTEGER IC,JC,KC,ISPEC,ISTAT,IW,NWORD
+      NWORD = 1 + (NSPEC-1)/NSPIMX
       ALLOCATE(FLDS(NXNODE,NYNODE,NZNODE,5+NSPEC))
-      ALLOCATE(TSTD(NXNODE,NYNODE,NZNODE), ISTD(NXNODE,NYNODE,NZNODE))
+      ALLOCATE(TSTD(NXNODE,NYNODE,NZNODE))
+      ALLOCATE(ISTD(NXNODE,NYNODE,NZNODE,NWORD))
       ISTAT = SENGA_DOWNLOAD_STATE_HOST(GPUCTX, FLDS, TSTD, ISTD)
       IF(ISTAT.NE.0)CALL GPUERR('senga_download_state_host', ISTAT)
       DO KC = 1,NZNODE
@@ -138,7 +145,9 @@ C     device -> COMMON registers (xRUN, and xRHS = xRUN as after FINCOM)
               YRHS(IC,JC,KC,ISPEC) = FLDS(IC,JC,KC,5+ISPEC)
             ENDDO
             TRUN(IC,JC,KC) = TSTD(IC,JC,KC)
-            ITNDEX(IC,JC,KC,1) = ISTD(IC,JC,KC)
+            DO IW = 1,NWORD
+              ITNDEX(IC,JC,KC,IW) = ISTD(IC,JC,KC,IW)
+            ENDDO
           ENDDO
         ENDDO
       ENDDO

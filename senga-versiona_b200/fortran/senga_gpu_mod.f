@@ -7,7 +7,9 @@ C
 C     Every BIND(C) type mirrors one struct of include/senga_gpu.h member by
 C     member; C arrays [a][b][c] appear here as (c,b,a). The table bounds
 C     equal the header's SENGA_* constants, which equal the reference's
-C     PARAMETERs (src/com_senga2.h:80-98,181-187). A CPU test of the
+C     PARAMETERs (src/com_senga2.h:80-98,181-187), NSPCMX and NSTPMX those
+C     of its largest shipped case (src/casefiles/68step/com_senga2.h:74): a
+C     host compiled with smaller tables fills the leading part of each. A CPU test of the
 C     repository (tests/test_fortran_binding.py) parses this file and the
 C     header and checks member order, types and extents against each other.
 C     Every entry point returns 0 on success and a positive senga_status
@@ -15,10 +17,12 @@ C     code otherwise; SENGA_LAST_ERROR gives the message.
       MODULE SENGA_GPU
       USE ISO_C_BINDING
       IMPLICIT NONE
-      INTEGER, PARAMETER :: SNSPCM = 9, SNSTPM = 21, SNTINM = 2
+      INTEGER, PARAMETER :: SNSPCM = 18, SNSTPM = 68, SNTINM = 2
       INTEGER, PARAMETER :: SNCOFM = 7, SNSSMX = 10, SNBDYM = 10
       INTEGER, PARAMETER :: SNLLMX = 10, SNDCFM = 4, SNCFRM = 6
       INTEGER, PARAMETER :: SNOBC = 0, SNBOUN = 1, SNPERI = 2
+C     ITNDEX arrays: (NSPEC + 14)/15 words per point, words slowest
+      INTEGER, PARAMETER :: SNSPIM = 15
 C     COMMON/CHEMIC after CHEMIN (src/com_senga2.h:121-178)
       TYPE, BIND(C) :: SENGA_CHEM
         INTEGER(C_INT) :: NSPEC, NSTEP, NBODY, NGIBB, NLIND, NTROE

@@ -22,7 +22,20 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsenga_gpu.so")
 DATA = os.path.join(HERE, "data")
 
-NSPCMX, NSTPMX, NTINMX, NCOFMX, NSSMAX, NBDYMX, NLLMAX, NDCFMX = 9, 21, 2, 7, 10, 10, 10, 4
+NSPCMX, NSTPMX, NTINMX, NCOFMX, NSSMAX, NBDYMX, NLLMAX, NDCFMX = 18, 68, 2, 7, 10, 10, 10, 4
+NSPIMX = 15  # species per ITNDEX word
+
+
+def itn_words(nspec):
+    """32-bit ITNDEX words per grid point (base-4 digits, 15 species a word)."""
+    return (nspec + NSPIMX - 1) // NSPIMX
+
+
+def itn_shape(nspec, shape):
+    """Host shape of an ITNDEX array: the grid's for up to 15 species, else
+    (words,) + the grid's, words slowest."""
+    w = itn_words(nspec)
+    return tuple(shape) if w == 1 else (w,) + tuple(shape)
 NOBC, NBOUND, NPERI = 0, 1, 2
 
 
@@ -341,7 +354,8 @@ class ZGroup:
         f = np.ascontiguousarray(fields, dtype=np.float64)
         t = np.ascontiguousarray(trun, dtype=np.float64)
         it = np.ascontiguousarray(itndex, dtype=np.int32)
-        assert f.shape == (self.nc,) + self.shape and t.shape == self.shape and it.shape == self.shape
+        assert f.shape == (self.nc,) + self.shape and t.shape == self.shape
+        assert it.shape == itn_shape(self.nspec, self.shape)
         _check(lib.senga_zgroup_upload_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
                "senga_zgroup_upload_host")
 
@@ -354,7 +368,7 @@ class ZGroup:
     def download(self):
         f = np.empty((self.nc,) + self.shape)
         t = np.empty(self.shape)
-        it = np.empty(self.shape, dtype=np.int32)
+        it = np.empty(itn_shape(self.nspec, self.shape), dtype=np.int32)
         _check(lib.senga_zgroup_download_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
                "senga_zgroup_download_host")
         return f, t, it
@@ -429,7 +443,8 @@ class Box:
         f = np.ascontiguousarray(fields, dtype=np.float64)
         t = np.ascontiguousarray(trun, dtype=np.float64)
         it = np.ascontiguousarray(itndex, dtype=np.int32)
-        assert f.shape == (self.nc,) + self.shape and t.shape == self.shape and it.shape == self.shape
+        assert f.shape == (self.nc,) + self.shape and t.shape == self.shape
+        assert it.shape == itn_shape(self.nspec, self.shape)
         _check(lib.senga_upload_state_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
                "upload")
 
@@ -439,12 +454,12 @@ class Box:
         if out is None:
             f = np.empty((self.nc,) + self.shape)
             t = np.empty(self.shape)
-            it = np.empty(self.shape, dtype=np.int32)
+            it = np.empty(itn_shape(self.nspec, self.shape), dtype=np.int32)
         else:
             f, t, it = out
             assert f.shape == (self.nc,) + self.shape and f.dtype == np.float64 and f.flags.c_contiguous
             assert t.shape == self.shape and t.dtype == np.float64 and t.flags.c_contiguous
-            assert it.shape == self.shape and it.dtype == np.int32 and it.flags.c_contiguous
+            assert it.shape == itn_shape(self.nspec, self.shape) and it.dtype == np.int32 and it.flags.c_contiguous
         _check(lib.senga_download_state_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
                "download")
         return f, t, it
@@ -533,7 +548,7 @@ class Box:
         """TEMPIN on the uploaded conserved state: (T, ITNDEX, p) of every
         point, also left on the device for the next step."""
         t = np.empty(self.shape)
-        it = np.empty(self.shape, dtype=np.int32)
+        it = np.empty(itn_shape(self.nspec, self.shape), dtype=np.int32)
         p = np.empty(self.shape)
         _check(lib.senga_tempin_host(self.h, float(trin), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32)), _dp(p)),
                "senga_tempin_host")
@@ -587,7 +602,8 @@ class Box:
         sync()."""
         for a, dt in ((fields, np.float64), (trun, np.float64), (itndex, np.int32)):
             assert a.dtype == dt and a.flags.c_contiguous
-        assert fields.shape == (self.nc,) + self.shape and trun.shape == self.shape and itndex.shape == self.shape
+        assert fields.shape == (self.nc,) + self.shape and trun.shape == self.shape
+        assert itndex.shape == itn_shape(self.nspec, self.shape)
         _check(lib.senga_upload_state_async(self.h, _dp(fields), _dp(trun),
                                             itndex.ctypes.data_as(C.POINTER(C.c_int32))), "senga_upload_state_async")
 
@@ -596,7 +612,8 @@ class Box:
         sync()."""
         for a, dt in ((fields, np.float64), (trun, np.float64), (itndex, np.int32)):
             assert a.dtype == dt and a.flags.c_contiguous and a.flags.writeable
-        assert fields.shape == (self.nc,) + self.shape and trun.shape == self.shape and itndex.shape == self.shape
+        assert fields.shape == (self.nc,) + self.shape and trun.shape == self.shape
+        assert itndex.shape == itn_shape(self.nspec, self.shape)
         _check(lib.senga_download_state_async(self.h, _dp(fields), _dp(trun),
                                               itndex.ctypes.data_as(C.POINTER(C.c_int32))), "senga_download_state_async")
 

@@ -175,7 +175,10 @@ def casefile_dump():
     (src/casefiles/21step/dmpi0000000.dat, the same grid, 9 species: a
     freely propagating 1D flame that the case restarts from with inflow at
     2.05 m/s, NSCBC I3/O1 x faces and every transport switch on), and the
-    1-step and 4-step cases' mechanisms (with the 4-step restart state)."""
+    1-step and 4-step cases' mechanisms (with the 4-step restart state), and
+    the 25-step and 68-step methane cases' mechanisms and restart states
+    (16 and 18 species: the reference compiles these with NSPCMX = 16/18,
+    NSTPMX = 35/68, src/casefiles/{25,68}step/com_senga2.h)."""
     import shutil
 
     shutil.copyfile(os.path.join(REF, "casefiles", "1step", "dmpi0000000.dat"),
@@ -189,6 +192,10 @@ def casefile_dump():
     for src, dst in (("1step/chem.dat", "casefile_1step_chem.dat"), ("4step/chem.dat", "casefile_4step_chem.dat"),
                      ("4step/diff.dat", "casefile_4step_diff.dat"), ("4step/dmpi0000000.dat", "dmpi_4step_1001.dat")):
         shutil.copyfile(os.path.join(REF, "casefiles", src), os.path.join(HERE, dst))
+    for case in ("25step", "68step"):
+        for src, dst in (("chem.dat", f"casefile_{case}_chem.dat"), ("diff.dat", f"casefile_{case}_diff.dat"),
+                         ("dmpi0000000.dat", f"dmpi_{case}_1001.dat")):
+            shutil.copyfile(os.path.join(REF, "casefiles", case, src), os.path.join(HERE, dst))
 
 
 def main():

@@ -1,4 +1,5 @@
-"""The reference's own 1D restart cases (src/casefiles/{1step,4step,21step}:
+"""The reference's own 1D restart cases (src/casefiles/{1step,4step,21step,
+25step,68step}:
 cont.dat, chem.dat, diff.dat and the formatted restart dump, copied under
 tests/golden/): 1001 x 1 x 1 points over 10 mm, NSCBC I3 inflow and O1
 outflow (p_inf 1e5 Pa, sigma 0.287, eta 1e-3), one-point periodic y and z,
@@ -6,7 +7,8 @@ adaptive steps. 1step: single-step R -> P, constant-Lewis transport, inflow
 0.39 m/s. 4step: 8-species 6-step mechanism, mixture-averaged transport
 with the molar-mass, pressure, Soret and Dufour switches on, inflow 0.5
 m/s. 21step: the H2/air mechanism of the named workloads, every switch on,
-inflow 2.05 m/s.
+inflow 2.05 m/s. 25step and 68step: methane/air with 16 and 18 species
+(ITNDEX in two words per point), every switch on, inflow 0.39 m/s.
 
 CPU: the bisection start-up temperature agrees with the oracle's TEMPER.
 GPU: RHS, fixed-step and adaptive-step runs against the oracle, field-
@@ -35,6 +37,11 @@ CASES = {
               {0: 5.5045872e-2, 1: 2.20183486e-1, 7: 7.24770642e-1}, ALL),
     "21step": (None, None, "dmpi_21step_1001.dat", 2.05,
                {0: 2.8312571e-2, 1: 2.26500566e-1, 8: 7.45186863e-1}, ALL),
+    # methane/air, 16 and 18 species: ITNDEX takes two words per point
+    "25step": ("casefile_25step_chem.dat", "casefile_25step_diff.dat", "dmpi_25step_1001.dat", 0.39,
+               {0: 5.5045872e-2, 1: 2.20183486e-1, 15: 7.24770642e-1}, ALL),
+    "68step": ("casefile_68step_chem.dat", "casefile_68step_diff.dat", "dmpi_68step_1001.dat", 0.39,
+               {0: 5.5045872e-2, 1: 2.20183486e-1, 17: 7.24770642e-1}, ALL),
 }
 
 

@@ -111,7 +111,7 @@ def _c_size(members):
 def test_parameters_equal_header_constants():
     defines, _, _ = _header()
     params, _, _, _ = _module()
-    pairs = {"SNSPCM": "SENGA_NSPCMX", "SNSTPM": "SENGA_NSTPMX", "SNTINM": "SENGA_NTINMX", "SNCOFM": "SENGA_NCOFMX",
+    pairs = {"SNSPCM": "SENGA_NSPCMX", "SNSTPM": "SENGA_NSTPMX", "SNSPIM": "SENGA_NSPIMX", "SNTINM": "SENGA_NTINMX", "SNCOFM": "SENGA_NCOFMX",
              "SNSSMX": "SENGA_NSSMAX", "SNBDYM": "SENGA_NBDYMX", "SNLLMX": "SENGA_NLLMAX", "SNDCFM": "SENGA_NDCFMX",
              "SNCFRM": "SENGA_NCFRMX", "SNOBC": "SENGA_NOBC", "SNBOUN": "SENGA_NBOUND", "SNPERI": "SENGA_NPERI"}
     for f, c in pairs.items():
