@@ -414,12 +414,18 @@ int senga_dump_read(const char* path, int formatted, int nspcmx, int* dims, doub
  * periodic box; the stencil kernels read each tile's z halo directly from the
  * slab that owns those planes (peer loads between GPUs, with peer access
  * enabled at creation), and the slabs' streams wait on one another's events
- * between the phases of every substage. Fully periodic boxes with a fixed
+ * between the phases of every substage. Boxes periodic in y and z (x
+ * periodic, or bounded with NSCBC faces: senga_zgroup_set_nscbc) with a fixed
  * time step; fields/trun/itn are the whole box in the senga_upload_state_host
  * layout. */
 typedef struct senga_zgroup senga_zgroup;
 int senga_zgroup_create(const senga_config* cfg, const senga_chem* chem, const senga_diff* diff, int nslabs,
                         const int* devices, senga_zgroup** out);
+/* NSCBC x faces of a z-split box (x bounded on both faces, cfg.nend): the
+ * same conditions as senga_set_nscbc, set on every slab (each holds its
+ * ny x nz/nslabs part of both x faces); needed before the first step. The
+ * transport switches and radiation are not available on a z-split box. */
+int senga_zgroup_set_nscbc(senga_zgroup* g, const senga_nscbc* bc);
 int senga_zgroup_upload_host(senga_zgroup* g, const double* fields, const double* trun, const int32_t* itndex);
 int senga_zgroup_step(senga_zgroup* g, int nsteps);
 int senga_zgroup_sync(senga_zgroup* g);

@@ -43,27 +43,39 @@ namespace {
 constexpr int kFaceBlock = 128;
 
 // value m points along DIR from (i, j, k); y and z periodic, x bounded (the
-// closures read only inward points)
+// closures read only inward points). A box split along z (zd.nr > 1) reads
+// the z neighbours from the slab that owns their plane.
 template <int DIR>
-__device__ __forceinline__ double at(const Geo& g, const double* a, int i, int j, int k, int m) {
+__device__ __forceinline__ double at(const Geo& g, const ZDec& zd, const double* a, int i, int j, int k, int m) {
   if (DIR == 0) i += m;
   if (DIR == 1) j = ((j + m) % g.ny + g.ny) % g.ny;
-  if (DIR == 2) k = ((k + m) % g.nz + g.nz) % g.nz;
-  return a[(int64_t)i + (int64_t)g.nx * (j + (int64_t)g.ny * k)];
+  int64_t base = 0;
+  if (DIR == 2) {
+    if (zd.nr > 1) {
+      const int zg = ((zd.rank * g.nz + k + m) % zd.nzg + zd.nzg) % zd.nzg;
+      const int r = zg / g.nz;
+      base = zd.base[r];
+      k = zg - r * g.nz;
+    } else {
+      k = ((k + m) % g.nz + g.nz) % g.nz;
+    }
+  }
+  return a[base + (int64_t)i + (int64_t)g.nx * (j + (int64_t)g.ny * k)];
 }
 template <int DIR>
-__device__ __forceinline__ double dd(const Geo& g, const double* a, int i, int j, int k) {
+__device__ __forceinline__ double dd(const Geo& g, const ZDec& zd, const double* a, int i, int j, int k) {
   const int c = DIR == 0 ? i : DIR == 1 ? j : k;
   const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
-  return d1core([&](int m) { return at<DIR>(g, a, i, j, k, m); }, c, n, g.per[DIR]) * g.ovd[DIR];
+  return d1core([&](int m) { return at<DIR>(g, zd, a, i, j, k, m); }, c, n, g.per[DIR]) * g.ovd[DIR];
 }
 // derivative of (a - c) along DIR: the pressure gradient of RHSVEL is taken of
 // p - p(1,1,1) (src/rhsvel.f:730-752)
 template <int DIR>
-__device__ __forceinline__ double dd_sub(const Geo& g, const double* a, double c0, int i, int j, int k) {
+__device__ __forceinline__ double dd_sub(const Geo& g, const ZDec& zd, const double* a, double c0, int i, int j,
+                                         int k) {
   const int c = DIR == 0 ? i : DIR == 1 ? j : k;
   const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
-  return d1core([&](int m) { return at<DIR>(g, a, i, j, k, m) - c0; }, c, n, g.per[DIR]) * g.ovd[DIR];
+  return d1core([&](int m) { return at<DIR>(g, zd, a, i, j, k, m) - c0; }, c, n, g.per[DIR]) * g.ovd[DIR];
 }
 
 // h_k(T) per unit mass of interval `it` (AMASCH polynomial, boundt.f:316-324)
@@ -173,7 +185,8 @@ __global__ void __launch_bounds__(kFaceBlock)
   }
 }
 
-__global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParams bc, int nspec, const senga_chem* chem) {
+__global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParams bc, int nspec, const senga_chem* chem,
+                                                   ZDec zd) {
   const int nyz = g.ny * g.nz;
   const int jk = blockIdx.x * kFaceBlock + threadIdx.x;
   const int side = blockIdx.y;  // 0: x-left, 1: x-right
@@ -186,18 +199,18 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
   const int nc = 5 + nspec;
   const double* U = f.uin;
   const double* vel = f.vel;
-  const double pref = __ldg(f.p);
+  const double pref = __ldg(f.p + zd.base[0]);  // p(1,1,1) lives in slab 0
   // ---- face data ----
   const double d = U[q], u = vel[q], v = vel[n + q], w = vel[2 * n + q];
   const double p = f.p[q], t = f.t[q], rr = f.rmix[q] / d, cp = f.cp[q];
   double e = f.e[q];
-  const double bcl1 = dd<0>(g, vel, i, j, k), bcl2 = dd<0>(g, U, i, j, k);
-  const double bcl3 = dd<0>(g, vel + n, i, j, k), bcl4 = dd<0>(g, vel + 2 * n, i, j, k);
-  const double bcl5 = dd_sub<0>(g, f.p, pref, i, j, k);
-  const double t2b = -v * dd<1>(g, vel, i, j, k) - w * dd<2>(g, vel, i, j, k);
-  const double py = dd_sub<1>(g, f.p, pref, i, j, k), pz = dd_sub<2>(g, f.p, pref, i, j, k);
+  const double bcl1 = dd<0>(g, zd, vel, i, j, k), bcl2 = dd<0>(g, zd, U, i, j, k);
+  const double bcl3 = dd<0>(g, zd, vel + n, i, j, k), bcl4 = dd<0>(g, zd, vel + 2 * n, i, j, k);
+  const double bcl5 = dd_sub<0>(g, zd, f.p, pref, i, j, k);
+  const double t2b = -v * dd<1>(g, zd, vel, i, j, k) - w * dd<2>(g, zd, vel, i, j, k);
+  const double py = dd_sub<1>(g, zd, f.p, pref, i, j, k), pz = dd_sub<2>(g, zd, f.p, pref, i, j, k);
   const double t51b = -v * py - w * pz;
-  const double t52b = -p * (dd<1>(g, vel + n, i, j, k) + dd<2>(g, vel + 2 * n, i, j, k));
+  const double t52b = -p * (dd<1>(g, zd, vel + n, i, j, k) + dd<2>(g, zd, vel + 2 * n, i, j, k));
   // ---- BOUNDS preliminaries (bounds.f:115-157 / 1198-1240) ----
   double gam1 = cp - rr;
   e = e - gam1 * t;
@@ -230,10 +243,10 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     const double xl = bc.xlen, c = acou;
     const double n2 = bc.nrieta[1], n3 = bc.nrieta[2], n4 = bc.nrieta[3], n5 = bc.nrieta[4], n6 = bc.nrieta[5];
     // transverse terms (bounds.f:185-204 from rhscal.f:159-180, rhsvel.f:62-200, 764-800)
-    const double t1b = -(dd<1>(g, U + 2 * n, i, j, k) + dd<2>(g, U + 3 * n, i, j, k));
+    const double t1b = -(dd<1>(g, zd, U + 2 * n, i, j, k) + dd<2>(g, zd, U + 3 * n, i, j, k));
     const double rho_inv = 1.0 / d;
-    const double t3b = -v * dd<1>(g, vel + n, i, j, k) - w * dd<2>(g, vel + n, i, j, k) - py * rho_inv;
-    const double t4b = -v * dd<1>(g, vel + 2 * n, i, j, k) - w * dd<2>(g, vel + 2 * n, i, j, k) - pz * rho_inv;
+    const double t3b = -v * dd<1>(g, zd, vel + n, i, j, k) - w * dd<2>(g, zd, vel + n, i, j, k) - py * rho_inv;
+    const double t4b = -v * dd<1>(g, zd, vel + 2 * n, i, j, k) - w * dd<2>(g, zd, vel + 2 * n, i, j, k) - pz * rho_inv;
     const double tt2 = c * c * t1b - t51b - (gam1 + 1.0) * t52b;
     const double tt5 = t51b + t52b * (gam1 + 1.0) + d * c * t2b;
     const double fornow = d * c * bcl1;
@@ -252,8 +265,8 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     double ce = -b2 * e - b3 * d * v - b4 * d * w - b5 * (ova2 * e + u / c + ovgm);
     for (int s = 0; s < nspec; ++s) {
       const double* ys = f.y + s * n;
-      const double t6b = -dd<1>(g, ys, i, j, k) * v - dd<2>(g, ys, i, j, k) * w;
-      double bcly = u * dd<0>(g, ys, i, j, k);
+      const double t6b = -dd<1>(g, zd, ys, i, j, k) * v - dd<2>(g, zd, ys, i, j, k) * w;
+      double bcly = u * dd<0>(g, zd, ys, i, j, k);
       bcly = n6 * c / xl * (ys[q] - bc.y_in[s]) + t6b - bcly;
       const double fn = bcly * d;
       ce = ce - fn * hprime(s);
@@ -292,7 +305,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     }
     const double lw = side == 0 ? b5 : b1;
     for (int s = 0; s < nspec; ++s) {
-      double bcly = u * dd<0>(g, f.y + s * n, i, j, k);
+      double bcly = u * dd<0>(g, zd, f.y + s * n, i, j, k);
       bcly = f.wdot[s * n + q] / d - bcly;
       const double fn = bcly * d;
       ce = ce - fn * hprime(s);
@@ -324,7 +337,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     b4 = -0.0 - b4;
     double ce = -b1 * (ova2 * e - u / acou + ovgm) - b2 * e - b3 * d * v - b4 * d * w;
     for (int s = 0; s < nspec; ++s) {
-      const double bcly = f.wdot[s * n + q] / d - 0.0 - u * dd<0>(g, f.y + s * n, i, j, k);
+      const double bcly = f.wdot[s * n + q] / d - 0.0 - u * dd<0>(g, zd, f.y + s * n, i, j, k);
       ce = ce - bcly * d * hprime(s);
     }
     corr[4 * (int64_t)nyz] = ce;
@@ -352,7 +365,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
       corr[3 * (int64_t)nyz] = -b2 * w - b4 * d - b5 * ova2 * w;
       double ce = -b2 * e - b3 * d * v - b4 * d * w - b5 * (ova2 * e + u / acou + ovgm);
       for (int s = 0; s < nspec; ++s) {
-        const double fn = dd<0>(g, f.y + s * n, i, j, k) * d;
+        const double fn = dd<0>(g, zd, f.y + s * n, i, j, k) * d;
         ce = ce - fn * hprime(s);
         corr[(int64_t)(5 + s) * nyz] = -(b2 + b5 * ova2) * f.y[s * n + q] - fn;
       }
@@ -380,7 +393,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
     b5 = fornow - b5;
     double ce = -b2 * e - b3 * d * v - b4 * d * w - b5 * (ova2 * e + u / acou + ovgm);
     for (int s = 0; s < nspec; ++s) {
-      const double bcly = f.wdot[s * n + q] / d - 0.0 - u * dd<0>(g, f.y + s * n, i, j, k);
+      const double bcly = f.wdot[s * n + q] / d - 0.0 - u * dd<0>(g, zd, f.y + s * n, i, j, k);
       ce = ce - bcly * d * hprime(s);
     }
     corr[4 * (int64_t)nyz] = ce;
@@ -408,7 +421,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
       corr[3 * (int64_t)nyz] = -b1 * ova2 * w - b2 * w - b4 * d;
       double ce = -b1 * (ova2 * e - u / acou + ovgm) - b2 * e - b3 * d * v - b4 * d * w;
       for (int s = 0; s < nspec; ++s) {
-        const double fn = dd<0>(g, f.y + s * n, i, j, k) * d;
+        const double fn = dd<0>(g, zd, f.y + s * n, i, j, k) * d;
         ce = ce - fn * hprime(s);
         corr[(int64_t)(5 + s) * nyz] = -(b2 + b1 * ova2) * f.y[s * n + q] - fn;
       }
@@ -443,7 +456,7 @@ __global__ void __launch_bounds__(kFaceBlock) k_wall_flux(Geo g, Fields f, Nscbc
     double fv[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m)
-      fv[m] = f.rd[s * n + q + m * st] * dd<0>(g, f.y + s * n, i + m * st, j, k);
+      fv[m] = f.rd[s * n + q + m * st] * dd<0>(g, ZDec{}, f.y + s * n, i + m * st, j, k);  // x only: own slab
     const double w = side == 0 ? ((-c0) * fv[0] + 4.0 * fv[1] - 3.0 * fv[2] + c3 * fv[3] - 0.25 * fv[4]) * g.ovd[0]
                                : (c0 * fv[0] - 4.0 * fv[1] + 3.0 * fv[2] - c3 * fv[3] + 0.25 * fv[4]) * g.ovd[0];
     f.wdot[s * n + q] = f.wdot[s * n + q] + w;
@@ -507,9 +520,9 @@ void launch_wall_fix(const Geo& g, const Fields& f, const NscbcParams& bc, int n
 }
 
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,
-                 cudaStream_t s) {
+                 cudaStream_t s, const ZDec& zd) {
   const int nyz = g.ny * g.nz;
-  k_face<<<dim3((nyz + kFaceBlock - 1) / kFaceBlock, 2), kFaceBlock, 0, s>>>(g, f, bc, nspec, dchem);
+  k_face<<<dim3((nyz + kFaceBlock - 1) / kFaceBlock, 2), kFaceBlock, 0, s>>>(g, f, bc, nspec, dchem, zd);
 }
 
 }  // namespace senga

@@ -948,9 +948,15 @@ int senga_zgroup_create(const senga_config* cfg, const senga_chem* chem, const s
                         const int* devices, senga_zgroup** out) {
   if (!cfg || !chem || !diff || !out || nslabs < 1 || nslabs > kMaxZRanks)
     return fail(SENGA_ERR_ARG, "senga_zgroup_create: bad argument (1..16 slabs)");
-  for (int k = 0; k < 6; ++k)
+  // y and z periodic; x periodic, or bounded on both faces with NSCBC face
+  // conditions (senga_zgroup_set_nscbc), whose face kernels read only their
+  // own slab's face planes
+  for (int k = 2; k < 6; ++k)
     if (cfg->nend[k] != SENGA_NPERI)
-      return fail(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: z-split boxes must be periodic in every direction");
+      return fail(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: z-split boxes must be periodic in y and z");
+  if (!((cfg->nend[0] == SENGA_NPERI && cfg->nend[1] == SENGA_NPERI) ||
+        (cfg->nend[0] == SENGA_NBOUND && cfg->nend[1] == SENGA_NBOUND)))
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: x must be periodic or bounded on both faces");
   if (cfg->adaptive) return fail(SENGA_ERR_UNSUPPORTED, "senga_zgroup_create: fixed time step only");
   if (cfg->nz % nslabs != 0) return fail(SENGA_ERR_ARG, "senga_zgroup_create: nz must divide into equal slabs");
   *out = nullptr;
@@ -1056,23 +1062,42 @@ int senga_zgroup_download_host(senga_zgroup* g, double* fields, double* trun, in
   });
 }
 
+int senga_zgroup_set_nscbc(senga_zgroup* g, const senga_nscbc* b) {
+  if (!g || !b) return fail(SENGA_ERR_ARG, "senga_zgroup_set_nscbc: null argument");
+  DeviceGuard dg;
+  for (int r = 0; r < g->nr; ++r) {
+    if (cudaSetDevice(g->ctx[r]->cfg.device) != cudaSuccess)
+      return fail(SENGA_ERR_CUDA, "senga_zgroup_set_nscbc: cudaSetDevice");
+    const int rc = senga_set_nscbc(g->ctx[r], b);  // every slab: its ny x nz/nr part of both x faces
+    if (rc != SENGA_OK) return rc;
+  }
+  return SENGA_OK;
+}
+
 int senga_zgroup_step(senga_zgroup* g, int nsteps) {
   if (!g || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_zgroup_step: bad argument");
   DeviceGuard dg;
   return guard([&] {
+    for (int r = 0; r < g->nr; ++r) require_rhs(g->ctx[r]);
     for (int s = 0; s < nsteps; ++s)
       for (int irk = 1; irk <= 5; ++irk) {
+        // the substage sequence of run_substage, with a barrier between the
+        // phases that read z halos of what other slabs write
         for (int r = 0; r < g->nr; ++r) {
           senga_ctx* c = g->ctx[r];
           CK(cudaSetDevice(c->cfg.device));
+          if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, false, c->d_chem, c->stream);  // BOUNDT
           launch_thermo(c->geo, thermo_fields(c), c->d_chem, c->d_diff, c->nspec, c->diff.flmavt, c->mech, c->stream);
         }
         zgroup_barrier(g);
         for (int r = 0; r < g->nr; ++r) {
           senga_ctx* c = g->ctx[r];
           CK(cudaSetDevice(c->cfg.device));
+          // face data + BOUNDS: transverse z derivatives read the neighbouring slabs
+          if (c->nscbc) launch_face(c->geo, c->f, c->bc, c->nspec, c->d_chem, c->stream, g->zd[r]);
           launch_flow(c->geo, c->f, c->nspec, c->stream, g->zd[r]);
           launch_species_a(c->geo, c->f, c->nspec, c->stream, g->zd[r]);
+          if (c->nscbc) launch_wall_flux(c->geo, c->f, c->bc, c->nspec, c->stream);  // W1 wall diffusion flux
         }
         zgroup_barrier(g);
         for (int r = 0; r < g->nr; ++r) {
@@ -1080,6 +1105,9 @@ int senga_zgroup_step(senga_zgroup* g, int nsteps) {
           CK(cudaSetDevice(c->cfg.device));
           RK rk{c->rklhs[irk - 1], c->rkrhs[irk - 1], c->rkerr[irk - 1], irk == 5 ? 1 : 0};
           launch_species_b_rk(c->geo, c->f, c->nspec, rk, c->stream, g->zd[r]);
+          if (c->nscbc) launch_wall_fix(c->geo, c->f, c->bc, c->nspec, true, c->stream);  // W1: LINCOM/FINCOM wall Y
+          // BOUNTT after the step's last substage (own face planes only)
+          if (irk == 5 && c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->d_chem, c->stream);
         }
         zgroup_barrier(g);
       }

@@ -211,8 +211,10 @@ struct NscbcParams {
 void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both,
                    const senga_chem* dchem, cudaStream_t s);
 // face data + BOUNDS corrections into f.face, after the thermochemistry kernel
+// (zd: a box split along z reads the transverse z derivatives' neighbours,
+// and p(1,1,1), from the slabs that own them)
 void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, const senga_chem* dchem,
-                 cudaStream_t s);
+                 cudaStream_t s, const ZDec& zd = ZDec{});
 // W1/W2 walls: the wall diffusion-flux terms added to the species rate and VTMP
 // (after the species kernel), and the wall temperature plus, when rk, the
 // zero-gradient mass fractions of the updated state (after the RK update)

@@ -162,6 +162,7 @@ def _load():
         "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
         "senga_set_transport": (ip, [vp, ip, ip, ip, ip, C.c_double]),
         "senga_keep_rates": (ip, [vp, ip]),
+        "senga_zgroup_set_nscbc": (ip, [vp, C.POINTER(NscbcT)]),
         "senga_zgroup_create": (ip, [C.POINTER(ConfigT), C.POINTER(ChemT), C.POINTER(DiffT), ip, C.POINTER(ip),
                                      C.POINTER(vp)]),
         "senga_zgroup_upload_host": (ip, [vp, dp, dp, i32p]),
@@ -326,12 +327,29 @@ class Diff:
         return bool(self.t.flmavt)
 
 
-class ZGroup:
-    """One periodic box split along z into `nslabs` contexts (on `devices`,
-    default all on `device`); the stencils read z halos from the neighbouring
-    slabs directly."""
+def nscbc_struct(bc):
+    """senga_nscbc from a dict (see Box.set_nscbc)."""
+    b = NscbcT()
+    b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
+    b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
+    for i, v in enumerate(bc.get("y_in", ())):
+        b.y_in[i] = v
+    b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
+    b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
+    b.t_in = bc.get("t_in", 0.0)
+    b.t_wall[0], b.t_wall[1] = bc.get("t_wall", (0.0, 0.0))
+    for i, v in enumerate(bc.get("nrieta", ())):
+        b.nrieta[i] = v
+    return b
 
-    def __init__(self, shape, lengths, chem, diff, tstep, nslabs, devices=None, device=0):
+
+class ZGroup:
+    """One box split along z into `nslabs` contexts (on `devices`, default
+    all on `device`); the stencils read z halos from the neighbouring slabs
+    directly. y and z periodic; x periodic, or bounded (nend) with NSCBC
+    faces set by set_nscbc."""
+
+    def __init__(self, shape, lengths, chem, diff, tstep, nslabs, devices=None, device=0, nend=(NPERI,) * 6):
         nx, ny, nz = shape
         self.shape = (nz, ny, nx)
         self.nspec = chem.nspec
@@ -340,7 +358,7 @@ class ZGroup:
         cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
         cfg.xgdlen, cfg.ygdlen, cfg.zgdlen = lengths
         for i in range(6):
-            cfg.nend[i] = NPERI
+            cfg.nend[i] = nend[i]
         cfg.tstep = tstep
         cfg.adaptive = 0
         cfg.device = device
@@ -358,6 +376,10 @@ class ZGroup:
         assert it.shape == itn_shape(self.nspec, self.shape)
         _check(lib.senga_zgroup_upload_host(self.h, _dp(f), _dp(t), it.ctypes.data_as(C.POINTER(C.c_int32))),
                "senga_zgroup_upload_host")
+
+    def set_nscbc(self, bc):
+        """NSCBC x faces on every slab, from a dict as Box.set_nscbc takes."""
+        _check(lib.senga_zgroup_set_nscbc(self.h, C.byref(nscbc_struct(bc))), "senga_zgroup_set_nscbc")
 
     def step(self, nsteps=1):
         _check(lib.senga_zgroup_step(self.h, nsteps), "senga_zgroup_step")
@@ -577,18 +599,7 @@ class Box:
         its six relaxation coefficients), 21 O1 outflow, 31 W1 adiabatic
         no-slip wall, 32 W2 isothermal no-slip wall (t_wall: x-left, x-right
         temperatures)."""
-        b = NscbcT()
-        b.xl, b.xr = bc.get("xl", 0), bc.get("xr", 0)
-        b.u_in, b.rho_in = bc.get("u_in", 0.0), bc.get("rho_in", 0.0)
-        for i, v in enumerate(bc.get("y_in", ())):
-            b.y_in[i] = v
-        b.p_inf, b.sigma, b.eta = bc.get("p_inf", 0.0), bc.get("sigma", 0.0), bc.get("eta", 0.0)
-        b.pio, b.bet_local = bc.get("pio", 0), bc.get("bet_local", 0)
-        b.t_in = bc.get("t_in", 0.0)
-        b.t_wall[0], b.t_wall[1] = bc.get("t_wall", (0.0, 0.0))
-        for i, v in enumerate(bc.get("nrieta", ())):
-            b.nrieta[i] = v
-        _check(lib.senga_set_nscbc(self.h, C.byref(b)), "senga_set_nscbc")
+        _check(lib.senga_set_nscbc(self.h, C.byref(nscbc_struct(bc))), "senga_set_nscbc")
 
     def set_transport(self, mixw=False, mixp=False, soret=False, dufour=False, wmltdr=5.0):
         """cont.dat transport switches: molar-mass and pressure diffusion,
