@@ -356,6 +356,28 @@ typedef struct senga_nscbc {
 } senga_nscbc;
 int senga_set_nscbc(senga_ctx* ctx, const senga_nscbc* bc);
 
+/* Synthetic turbulent inflow velocity on an I3 inflow at x-left: the
+ * reference's digital filter (src/inflow.f, M. Klein's method) with the
+ * velocity option of BCUTXL NXLPRM(1) = 4 (src/bcutxl.f:476-510). Every RK
+ * step first draws three random planes with the reference's RAN1 (host,
+ * serial), filters them with Gaussian kernels of length scales lny, lnz (in
+ * grid spacings; half-widths nfy, nfz) on the device, correlates them in
+ * time over lnx spacings of the mean inflow u_in, and removes their face
+ * means; the face then takes u = u_in + u' + coflow, v = v', w = 0 and the
+ * matching time derivatives. Velocity only (NXLPRM(2) = 0); the reference's
+ * PARAMETERs are lnx = lny = lnz = 30, nfy = nfz = 60. itime is the step
+ * number of the next step (ITIME, which seeds RAN1 each step). Set after
+ * senga_set_nscbc; the steps then run without graph capture (the random
+ * planes are drawn on the host every step). */
+typedef struct senga_synth_inflow {
+  double urms;   /* RXLPRM(2): fluctuation amplitude [m/s] */
+  double coflow; /* RXLPRM(4): added to the inflow velocity [m/s] */
+  int lnx, lny, lnz;
+  int nfy, nfz;
+  int itime;
+} senga_synth_inflow;
+int senga_set_synthetic_inflow(senga_ctx* ctx, const senga_synth_inflow* p);
+
 /* Adaptive time step (cfg.adaptive = 1, the reference's NSTPSW = 1):
  * ADAPTT (src/adaptt.f:53-330) runs after every step of senga_step /
  * senga_step_graph (the latter then launches kernels per step, since dt

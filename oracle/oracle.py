@@ -71,6 +71,7 @@ def _get():
         lib.oracle_ranuni.argtypes = [C.c_int, C.c_int64, dp]
         lib.oracle_set_transport.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
         lib.oracle_set_bc.argtypes = [C.c_void_p, C.POINTER(_Bc)]
+        lib.oracle_set_synth.argtypes = [C.c_void_p, C.c_double, C.c_double] + [C.c_int] * 6
         lib.oracle_tstep.argtypes = [C.c_void_p, dp, dp, C.POINTER(C.c_int)]
         lib.oracle_filter_field.argtypes = [C.c_void_p, C.c_int, dp, dp]
         lib.oracle_chem_table.argtypes = [C.c_char_p, C.c_char_p, dp, C.c_int]
@@ -211,6 +212,13 @@ class Oracle:
             b.nrieta[i] = v
         if _get().oracle_set_bc(self.h, C.byref(b)) != 0:
             raise RuntimeError("oracle_set_bc: " + _get().oracle_last_error().decode())
+
+    def set_synth(self, urms, coflow=0.0, lnx=30, lny=30, lnz=30, nfy=60, nfz=60, itime0=1):
+        """Synthetic turbulent inflow velocity on the I3 x-left face (inflow.f,
+        BCUTXL NXLPRM(1) = 4); itime0: the step number of the next step."""
+        if _get().oracle_set_synth(self.h, float(urms), float(coflow), int(lnx), int(lny), int(lnz), int(nfy),
+                                   int(nfz), int(itime0)) != 0:
+            raise RuntimeError("oracle_set_synth: " + _get().oracle_last_error().decode())
 
     def set_radiation(self, radn_path, trefrn=300.0):
         """RADCAL on (radn.dat path, TREFRN) or off (radn_path None)."""

@@ -873,8 +873,158 @@ struct Oracle {
           yrhs[is](ic, jc, kc) = yw;
         }
   }
+  // ---- synthetic turbulent inflow velocity (src/inflow.f, called once per
+  // time step from src/senga2.f:100-103 when NXLPRM(1) = 4; its consumer is
+  // BCUTXL, src/bcutxl.f:476-510). One rank, velocity only (NXLPRM(2) = 0),
+  // USTEAD = 1 as coded, VFAC = 1 ----
+  bool synth = false;
+  double syn_urms = 0.0, syn_coflow = 0.0;  // RXLPRM(2), RXLPRM(4)
+  int syn_lnx = 30, syn_lny = 30, syn_lnz = 30, syn_nfy = 60, syn_nfz = 60;  // LNX..NFZ (com_senga2.h:54-56)
+  int itime = 1;                                                            // ITIME (JTIME of the step)
+  std::vector<double> uinf1, uinf2, vinf1, vinf2, winf1, winf2;            // (JC,KC): (jc-1) + ny*(kc-1)
+  int ran_iv[32] = {}, ran_iy = 0;                                          // RAN1's SAVEd state
+  // RAN1 (src/inflow.f:448-475): Numerical Recipes' ran1, the minimal
+  // standard generator (Park and Miller, Schrage's multiplication) with the
+  // Bays-Durham shuffle, in single precision, mapped to (2r - 1)/0.577
+  float ran1(int& idum) {
+    const int IA = 16807, IM = 2147483647, IQ = 127773, IR = 2836, NTAB = 32, NDIV = 1 + (IM - 1) / NTAB;
+    const float AM = 1.0f / (float)IM, EPS = 1.2e-7f, RNMX = 1.0f - EPS;
+    int j, k;
+    if (idum <= 0 || ran_iy == 0) {
+      idum = std::max(-idum, 1);
+      for (j = NTAB + 8; j >= 1; --j) {
+        k = idum / IQ;
+        idum = IA * (idum - k * IQ) - IR * k;
+        if (idum < 0) idum = idum + IM;
+        if (j <= NTAB) ran_iv[j - 1] = idum;
+      }
+      ran_iy = ran_iv[0];
+    }
+    k = idum / IQ;
+    idum = IA * (idum - k * IQ) - IR * k;
+    if (idum < 0) idum = idum + IM;
+    j = 1 + ran_iy / NDIV;
+    ran_iy = ran_iv[j - 1];
+    ran_iv[j - 1] = idum;
+    float r = std::min(AM * (float)ran_iy, RNMX);
+    r = (r * 2.0f - 1.0f) / 0.577f;
+    return r;
+  }
+  int fjk(int jc, int kc) const { return (jc - 1) + ny * (kc - 1); }
+  // INFLOW (src/inflow.f:78-420 for one rank, JFILTSTART = KFILTSTART = 0)
+  void inflow() {
+    const int NFY = syn_nfy, NFZ = syn_nfz;
+    const double delx = cf.xgdlen / (double)(float)(nx - 1);  // XGDLEN/REAL(NXGLBL-1)
+    const double umean = uin, tstp = tstep_now, urms = syn_urms;
+    const double theta = (double)syn_lnx * delx / umean;
+    const double phi = 1.0 - tstp / theta;
+    const double pi = 4.0 * std::atan(1.0);
+    std::vector<double> ay(2 * NFY + 1), az(2 * NFZ + 1);
+    double norm = 0.0;
+    for (int jc = -NFY; jc <= NFY; ++jc) {
+      ay[jc + NFY] = std::exp(-pi * jc * jc / (2 * syn_lny * syn_lny));
+      norm = norm + ay[jc + NFY] * ay[jc + NFY];
+    }
+    norm = std::sqrt(norm);
+    for (int jc = -NFY; jc <= NFY; ++jc) ay[jc + NFY] = ay[jc + NFY] / norm;
+    norm = 0.0;
+    for (int kc = -NFZ; kc <= NFZ; ++kc) {
+      az[kc + NFZ] = std::exp(-pi * kc * kc / (2 * syn_lnz * syn_lnz));
+      norm = norm + az[kc + NFZ] * az[kc + NFZ];
+    }
+    norm = std::sqrt(norm);
+    for (int kc = -NFZ; kc <= NFZ; ++kc) az[kc + NFZ] = az[kc + NFZ] / norm;
+    // random planes over JC = 1-NFY..NY+NFY, KC = 1-NFZ..NZ+NFZ, drawn with
+    // JC outermost; then periodic in y (PERIY), not in z (PERIZ = .FALSE.)
+    const int wy = ny + 2 * NFY, wz = nz + 2 * NFZ;
+    auto ri = [&](int jc, int kc) { return (size_t)(jc + NFY - 1) + (size_t)wy * (size_t)(kc + NFZ - 1); };
+    std::vector<double> ur((size_t)wy * wz), vr((size_t)wy * wz), wr((size_t)wy * wz);
+    int intran = itime;
+    for (int jc = 1 - NFY; jc <= ny + NFY; ++jc)
+      for (int kc = 1 - NFZ; kc <= nz + NFZ; ++kc) {
+        ur[ri(jc, kc)] = ran1(intran);
+        vr[ri(jc, kc)] = ran1(intran);
+        wr[ri(jc, kc)] = ran1(intran);
+      }
+    for (int jc = -NFY + 1; jc <= 0; ++jc)
+      for (int kc = 1 - NFZ; kc <= nz + NFZ; ++kc) {
+        ur[ri(jc, kc)] = ur[ri(jc + ny, kc)];
+        vr[ri(jc, kc)] = vr[ri(jc + ny, kc)];
+        wr[ri(jc, kc)] = wr[ri(jc + ny, kc)];
+      }
+    for (int jc = ny + 1; jc <= ny + NFY; ++jc)
+      for (int kc = 1 - NFZ; kc <= nz + NFZ; ++kc) {
+        ur[ri(jc, kc)] = ur[ri(jc - ny, kc)];
+        vr[ri(jc, kc)] = vr[ri(jc - ny, kc)];
+        wr[ri(jc, kc)] = wr[ri(jc - ny, kc)];
+      }
+    // filtered in y (UFOLD over KC = 1-NFZ..NZ+NFZ), then in z (UFILT)
+    auto fo = [&](int jc, int kc) { return (size_t)(jc - 1) + (size_t)ny * (size_t)(kc + NFZ - 1); };
+    std::vector<double> uf((size_t)ny * wz, 0.0), vf((size_t)ny * wz, 0.0), wf((size_t)ny * wz, 0.0);
+    for (int jc = 1; jc <= ny; ++jc)
+      for (int kc = 1 - NFZ; kc <= nz + NFZ; ++kc)
+        for (int j2 = -NFY; j2 <= NFY; ++j2) {
+          uf[fo(jc, kc)] = uf[fo(jc, kc)] + ur[ri(jc + j2, kc)] * ay[j2 + NFY];
+          vf[fo(jc, kc)] = vf[fo(jc, kc)] + vr[ri(jc + j2, kc)] * ay[j2 + NFY];
+          wf[fo(jc, kc)] = wf[fo(jc, kc)] + wr[ri(jc + j2, kc)] * ay[j2 + NFY];
+        }
+    const size_t m = (size_t)ny * nz;
+    std::vector<double> ufl(m, 0.0), vfl(m, 0.0), wfl(m, 0.0);
+    for (int jc = 1; jc <= ny; ++jc)
+      for (int kc = 1; kc <= nz; ++kc)
+        for (int k2 = -NFZ; k2 <= NFZ; ++k2) {
+          ufl[fjk(jc, kc)] = ufl[fjk(jc, kc)] + uf[fo(jc, kc + k2)] * az[k2 + NFZ];
+          vfl[fjk(jc, kc)] = vfl[fjk(jc, kc)] + vf[fo(jc, kc + k2)] * az[k2 + NFZ];
+          wfl[fjk(jc, kc)] = wfl[fjk(jc, kc)] + wf[fo(jc, kc + k2)] * az[k2 + NFZ];
+        }
+    const double scale = std::sqrt(urms * urms * (1.0 - phi * phi));
+    for (size_t q = 0; q < m; ++q) {
+      ufl[q] = ufl[q] * scale;
+      vfl[q] = vfl[q] * scale;
+      wfl[q] = wfl[q] * scale;
+    }
+    uinf1 = uinf2;
+    vinf1 = vinf2;
+    winf1 = winf2;
+    for (size_t q = 0; q < m; ++q) {
+      uinf2[q] = ufl[q] + phi * uinf1[q];
+      vinf2[q] = vfl[q] + phi * vinf1[q];
+      winf2[q] = wfl[q] + phi * winf1[q];
+    }
+    for (size_t q = 0; q < m; ++q) {  // times USTEAD = 1; WINF2 = 0
+      uinf2[q] = uinf2[q] * 1.0;
+      vinf2[q] = vinf2[q] * 1.0;
+      winf2[q] = 0.0;
+    }
+    for (auto* a : {&uinf2, &vinf2, &winf2}) {  // the face mean removed
+      double sum = 0.0, denom = 0.0;
+      for (int jc = 1; jc <= ny; ++jc)
+        for (int kc = 1; kc <= nz; ++kc) {
+          sum = sum + (*a)[fjk(jc, kc)];
+          denom = denom + 1.0;
+        }
+      for (size_t q = 0; q < m; ++q) (*a)[q] = (*a)[q] - sum / denom;
+    }
+    ++itime;
+  }
+  // BCUTXL: the inflow velocity and its time derivative at (JC,KC): NXLPRM(1)
+  // = 1 (constant U_in) or 4 (src/bcutxl.f:492-505 with VFAC = 1, DVFDT = 0)
+  double struxl(int jc, int kc) const { return synth ? (uin * 1.0 + uinf2[fjk(jc, kc)]) * 1.0 + syn_coflow : uin; }
+  double strvxl(int jc, int kc) const { return synth ? vinf2[fjk(jc, kc)] * 1.0 : 0.0; }
+  double strwxl(int jc, int kc) const { return synth ? winf2[fjk(jc, kc)] * 1.0 : 0.0; }
+  double dudtxl(int jc, int kc) const {
+    return synth ? (uinf2[fjk(jc, kc)] - uinf1[fjk(jc, kc)]) / tstep_now * 1.0 + (uin * 1.0 + uinf2[fjk(jc, kc)]) * 0.0
+                 : 0.0;
+  }
+  double dvdtxl(int jc, int kc) const {
+    return synth ? (vinf2[fjk(jc, kc)] - vinf1[fjk(jc, kc)]) / tstep_now * 1.0 + vinf2[fjk(jc, kc)] * 0.0 : 0.0;
+  }
+  double dwdtxl(int jc, int kc) const {
+    return synth ? (winf2[fjk(jc, kc)] - winf1[fjk(jc, kc)]) / tstep_now * 1.0 + winf2[fjk(jc, kc)] * 0.0 : 0.0;
+  }
+
   // BOUNDT, I3 at x-left: impose the inflow state on the U register (DRHS..YRHS
-  // at ISTAL; src/boundt.f:177-200 with BCDTXL, BCUTXL NXLPRM(1)=1, BCYTXL)
+  // at ISTAL; src/boundt.f:177-200 with BCDTXL, BCUTXL, BCYTXL)
   void boundt() {
     if (bcxl == BC_I2 || bcxr == BC_I2) impose_i2(false);
     if (is_wall(bcxl)) impose_wall(true, false);
@@ -884,9 +1034,9 @@ struct Oracle {
     for (int kc = kstal; kc <= kstol; ++kc)
       for (int jc = jstal; jc <= jstol; ++jc) {
         drhs(ic, jc, kc) = rhoin;
-        urhs(ic, jc, kc) = rhoin * uin;
-        vrhs(ic, jc, kc) = rhoin * 0.0;
-        wrhs(ic, jc, kc) = rhoin * 0.0;
+        urhs(ic, jc, kc) = rhoin * struxl(jc, kc);
+        vrhs(ic, jc, kc) = rhoin * strvxl(jc, kc);
+        wrhs(ic, jc, kc) = rhoin * strwxl(jc, kc);
         for (int is = 0; is < nspec; ++is) yrhs[is](ic, jc, kc) = rhoin * yin[is];
       }
   }
@@ -901,9 +1051,9 @@ struct Oracle {
     for (int kc = kstal; kc <= kstol; ++kc)
       for (int jc = jstal; jc <= jstol; ++jc) {
         drhs(ic, jc, kc) = rhoin;
-        urhs(ic, jc, kc) = rhoin * uin;
-        vrhs(ic, jc, kc) = rhoin * 0.0;
-        wrhs(ic, jc, kc) = rhoin * 0.0;
+        urhs(ic, jc, kc) = rhoin * struxl(jc, kc);
+        vrhs(ic, jc, kc) = rhoin * strvxl(jc, kc);
+        wrhs(ic, jc, kc) = rhoin * strwxl(jc, kc);
         drun(ic, jc, kc) = drhs(ic, jc, kc);
         urun(ic, jc, kc) = urhs(ic, jc, kc);
         vrun(ic, jc, kc) = vrhs(ic, jc, kc);
@@ -959,10 +1109,10 @@ struct Oracle {
           double bcl3 = F.u[q] * F.bcl3[q];
           double bcl4 = F.u[q] * F.bcl4[q];
           double bcl5 = 0.5 * (F.u[q] + acou[q]) * (F.bcl5[q] + fornow);
-          fornow = bcl1 - F.d[q] * acou[q] * 0.0;
+          fornow = bcl1 - F.d[q] * acou[q] * dudtxl(jc, kc);
           bcl2 = -0.0 - ova2[q] * (bcl1 + fornow) - bcl2;
-          bcl3 = -0.0 - bcl3;
-          bcl4 = -0.0 - bcl4;
+          bcl3 = -dvdtxl(jc, kc) - bcl3;
+          bcl4 = -dwdtxl(jc, kc) - bcl4;
           bcl5 = fornow - bcl5;
           double& er = erhs(istal, jc, kc);
           er = er - bcl2 * F.e[q] - bcl3 * F.d[q] * F.v[q] - bcl4 * F.d[q] * F.w[q] -
@@ -2562,6 +2712,7 @@ struct Oracle {
   // no-ops; FLTREM is commented out at senga2.f:178; ADAPTT runs when the
   // step switch asks for adaptive steps, src/dtinit.f:174-175).
   void step() {
+    if (synth) inflow();  // INFLOW ahead of the substages (src/senga2.f:100-103)
     for (int irk = 1; irk <= 5; ++irk) {
       boundt();
       rhs();
@@ -2754,6 +2905,28 @@ struct oracle_bc {
   double t_wall[2];
   double nrieta[6];
 };
+// Synthetic turbulent inflow velocity on an I3 x-left face (NXLPRM(1) = 4,
+// NXLPRM(2) = 0): RXLPRM(2) = urms, RXLPRM(4) = coflow, LNX, LNY, LNZ, NFY,
+// NFZ and the step number of the next step (ITIME); call after oracle_set_bc.
+int oracle_set_synth(void* h, double urms, double coflow, int lnx, int lny, int lnz, int nfy, int nfz,
+                     int itime0) {
+  auto* o = static_cast<orc::Oracle*>(h);
+  if (o->bcxl != orc::Oracle::BC_I3) { g_err = "oracle_set_synth: needs an I3 inflow at x-left"; return 1; }
+  o->synth = true;
+  o->syn_urms = urms;
+  o->syn_coflow = coflow;
+  o->syn_lnx = lnx;
+  o->syn_lny = lny;
+  o->syn_lnz = lnz;
+  o->syn_nfy = nfy;
+  o->syn_nfz = nfz;
+  o->itime = itime0;
+  const size_t m = (size_t)o->ny * o->nz;
+  for (auto* a : {&o->uinf1, &o->uinf2, &o->vinf1, &o->vinf2, &o->winf1, &o->winf2}) a->assign(m, 0.0);
+  o->ran_iy = 0;
+  return 0;
+}
+
 int oracle_set_bc(void* h, const oracle_bc* b) {
   try {
     static_cast<orc::Oracle*>(h)->set_bc(b->xl, b->xr, b->u_in, b->rho_in, b->y_in, b->p_inf, b->sigma, b->eta, b->pio,
@@ -3017,6 +3190,7 @@ int oracle_substage(void* h, int irk) {
   try {
     auto* o = static_cast<orc::Oracle*>(h);
     if (irk < 1 || irk > 5) throw std::runtime_error("oracle_substage: irk must be 1..5");
+    if (irk == 1 && o->synth) o->inflow();
     o->boundt();
     o->rhs();
     o->bounds();

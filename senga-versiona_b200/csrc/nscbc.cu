@@ -171,12 +171,16 @@ __global__ void __launch_bounds__(kFaceBlock)
     return;
   }
   const double r = bc.rho_in;
+  // BCUTXL: constant U_in, or the synthetic inflow (bcutxl.f:492-498, VFAC = 1)
+  const bool syn = bc.uinf2 != nullptr;
+  const double su = syn ? (bc.u_in * 1.0 + bc.uinf2[jk]) * 1.0 + bc.coflow : bc.u_in;
+  const double sv = syn ? bc.vinf2[jk] * 1.0 : 0.0, sw = syn ? bc.winf2[jk] * 1.0 : 0.0;
   for (int w = 0; w < (both ? 2 : 1); ++w) {
     double* U = regs[w];
     U[q] = r;
-    U[n + q] = r * bc.u_in;
-    U[2 * n + q] = r * 0.0;
-    U[3 * n + q] = r * 0.0;
+    U[n + q] = r * su;
+    U[2 * n + q] = r * sv;
+    U[3 * n + q] = r * sw;
     for (int s = 0; s < nspec; ++s) U[(5 + s) * n + q] = r * bc.y_in[s];
   }
   if (both && f.err) {  // BOUNTT: error of the imposed fields zeroed
@@ -379,17 +383,23 @@ __global__ void __launch_bounds__(kFaceBlock) k_face(Geo g, Fields f, NscbcParam
       corr[4 * (int64_t)nyz] = -b5 * (ova2 * e + u / acou + ovgm);
       for (int s = 0; s < nspec; ++s) corr[(int64_t)(5 + s) * nyz] = -b5 * ova2 * f.y[s * n + q];
     }
-  } else if (kind == 13) {  // I3 inflow at x-left, constant u, rho and Y (DUDT = DDDT = DYDT = 0)
+  } else if (kind == 13) {  // I3 inflow at x-left: rho and Y constant (DDDT = DYDT = 0)
+    // DUDT, DVDT, DWDT: zero for a constant u_in; the synthetic inflow's
+    // (bcutxl.f:501-506, VFAC = 1, DVFDT = 0)
+    const bool syn = bc.uinf2 != nullptr;
+    const double dudt = syn ? (bc.uinf2[jk] - bc.uinf1[jk]) / bc.tstep * 1.0 + (bc.u_in * 1.0 + bc.uinf2[jk]) * 0.0 : 0.0;
+    const double dvdt = syn ? (bc.vinf2[jk] - bc.vinf1[jk]) / bc.tstep * 1.0 + bc.vinf2[jk] * 0.0 : 0.0;
+    const double dwdt = syn ? (bc.winf2[jk] - bc.winf1[jk]) / bc.tstep * 1.0 + bc.winf2[jk] * 0.0 : 0.0;
     double fornow = d * acou * bcl1;
     const double b1 = 0.5 * (u - acou) * (bcl5 - fornow);
     double b2 = u * (bcl2 - bcl5 * ova2);
     double b3 = u * bcl3;
     double b4 = u * bcl4;
     double b5 = 0.5 * (u + acou) * (bcl5 + fornow);
-    fornow = b1 - d * acou * 0.0;
+    fornow = b1 - d * acou * dudt;
     b2 = -0.0 - ova2 * (b1 + fornow) - b2;
-    b3 = -0.0 - b3;
-    b4 = -0.0 - b4;
+    b3 = -dvdt - b3;
+    b4 = -dwdt - b4;
     b5 = fornow - b5;
     double ce = -b2 * e - b3 * d * v - b4 * d * w - b5 * (ova2 * e + u / acou + ovgm);
     for (int s = 0; s < nspec; ++s) {

@@ -84,6 +84,7 @@ struct senga_ctx {
   bool nscbc = false;
   NscbcParams bc{};
   double* nscbc_pool = nullptr;
+  SynthInflow* synth = nullptr;  // synthetic inflow velocity (senga_set_synthetic_inflow)
 };
 
 namespace {
@@ -333,6 +334,7 @@ int senga_ctx_destroy(senga_ctx* c) {
   cudaFree(c->d_status);
   cudaFree(c->d_errmax);
   cudaFree(c->nscbc_pool);
+  synth_destroy(c->synth);
   cudaFree(c->mixt_pool);
   cudaFree(c->rrte);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -402,6 +404,7 @@ int senga_download_state_host(senga_ctx* c, double* fields, double* trun, int32_
 int senga_substage(senga_ctx* c, int irkstp) {
   if (!c || irkstp < 1 || irkstp > 5) return fail(SENGA_ERR_ARG, "senga_substage: bad argument");
   return guard([&] {
+    if (irkstp == 1 && c->synth) synth_step(c->synth, c->cfg.xgdlen, c->geo.nx, c->tstep, c->bc, c->stream);
     run_substage(c, irkstp);
     CK(cudaGetLastError());
   });
@@ -411,6 +414,8 @@ int senga_step(senga_ctx* c, int nsteps) {
   if (!c || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_step: bad argument");
   return guard([&] {
     for (int s = 0; s < nsteps; ++s) {
+      // INFLOW ahead of the substages (src/senga2.f:100-103)
+      if (c->synth) synth_step(c->synth, c->cfg.xgdlen, c->geo.nx, c->tstep, c->bc, c->stream);
       for (int irk = 1; irk <= 5; ++irk) run_substage(c, irk);
       if (c->nscbc) launch_boundt(c->geo, c->f, c->bc, c->nspec, true, c->d_chem, c->stream);  // BOUNTT
       if (c->cfg.adaptive) adaptt(c);
@@ -421,7 +426,9 @@ int senga_step(senga_ctx* c, int nsteps) {
 
 int senga_step_graph(senga_ctx* c, int nsteps) {
   if (!c || nsteps < 0) return fail(SENGA_ERR_ARG, "senga_step_graph: bad argument");
-  if (c->cfg.adaptive) return senga_step(c, nsteps);  // dt changes every step: no fixed graph
+  // dt changes every step, or the synthetic inflow draws its planes on the
+  // host every step: no fixed graph
+  if (c->cfg.adaptive || c->synth) return senga_step(c, nsteps);
   return guard([&] {
     if (!c->graph) {
       require_rhs(c);  // before the capture, so a refusal leaves the stream uncaptured
@@ -1059,6 +1066,27 @@ int senga_zgroup_download_host(senga_zgroup* g, double* fields, double* trun, in
                              c->stream));
     }
     for (int r = 0; r < g->nr; ++r) CK(cudaStreamSynchronize(g->ctx[r]->stream));
+  });
+}
+
+int senga_set_synthetic_inflow(senga_ctx* c, const senga_synth_inflow* p) {
+  if (!c || !p) return fail(SENGA_ERR_ARG, "senga_set_synthetic_inflow: null argument");
+  if (!c->nscbc || c->bc.xl != 13)
+    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_synthetic_inflow: needs an I3 inflow at x-left (senga_set_nscbc)");
+  if (!(p->urms >= 0.0) || p->lnx < 1 || p->lny < 1 || p->lnz < 1 || p->nfy < 0 || p->nfz < 0 || p->itime < 1 ||
+      !(c->bc.u_in > 0.0))
+    return fail(SENGA_ERR_ARG, "senga_set_synthetic_inflow: urms >= 0, lengths >= 1, nfy, nfz >= 0, itime >= 1 "
+                               "and a positive inflow velocity");
+  return guard([&] {
+    CK(cudaSetDevice(c->cfg.device));
+    CK(cudaStreamSynchronize(c->stream));
+    synth_destroy(c->synth);
+    c->synth = nullptr;
+    c->synth = synth_create(c->geo.ny, c->geo.nz, *p, c->cfg.device);
+    if (c->graph) {  // a captured step would bypass the per-step planes
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
   });
 }
 

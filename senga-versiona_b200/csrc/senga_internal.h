@@ -206,6 +206,12 @@ struct NscbcParams {
   double nrieta[6];                         // I4: NRIETA1..6 = RXLPRC(1..6)
   double p_inf, cobc, bet, xlen;            // O1: PINFXR, COBCXR, BET, XGDLEN
   int pio, betloc;                          // O1: NXRPRM(1), NXRPRM(2)
+  // synthetic turbulent inflow velocity on an I3 x-left face (BCUTXL NXLPRM(1)
+  // = 4): the INFLOW planes of this and the previous step ([ny*nz] each, y
+  // fastest), RXLPRM(4) and the current step; nullptr: constant u_in
+  const double *uinf1 = nullptr, *uinf2 = nullptr, *vinf1 = nullptr, *vinf2 = nullptr;
+  const double *winf1 = nullptr, *winf2 = nullptr;
+  double coflow = 0.0, tstep = 0.0;
 };
 // BOUNDT (both = false) or BOUNTT (both = true: U and S registers, error zeroed)
 void launch_boundt(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool both,
@@ -219,6 +225,13 @@ void launch_face(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec
 // (after the species kernel), and the wall temperature plus, when rk, the
 // zero-gradient mass fractions of the updated state (after the RK update)
 bool has_wall(const NscbcParams& bc);
+// the synthetic inflow planes of one context (synth_inflow.cu)
+struct SynthInflow;
+SynthInflow* synth_create(int ny, int nz, const senga_synth_inflow& p, int device);
+void synth_destroy(SynthInflow* s);
+// INFLOW for the next step: draws the random planes on the host, filters
+// them on the device, and points bc at this step's planes
+void synth_step(SynthInflow* s, double xgdlen, int nx, double tstep, NscbcParams& bc, cudaStream_t st);
 void launch_wall_flux(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, cudaStream_t s);
 void launch_wall_fix(const Geo& g, const Fields& f, const NscbcParams& bc, int nspec, bool rk, cudaStream_t s);
 

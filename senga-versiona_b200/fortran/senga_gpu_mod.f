@@ -108,6 +108,13 @@ C     RXLPRM(1), RXRPRM(1) of W2 walls; NRIETA: RXLPRC(1..6) of I4)
         REAL(C_DOUBLE) :: T_WALL(2)
         REAL(C_DOUBLE) :: NRIETA(6)
       END TYPE
+C     synthetic inflow velocity: RXLPRM(2), RXLPRM(4), LNX..NFZ, ITIME
+      TYPE, BIND(C) :: SENGA_SYNTH_INFLOW
+        REAL(C_DOUBLE) :: URMS, COFLOW
+        INTEGER(C_INT) :: LNX, LNY, LNZ
+        INTEGER(C_INT) :: NFY, NFZ
+        INTEGER(C_INT) :: ITIME
+      END TYPE
       INTERFACE
         INTEGER(C_INT) FUNCTION SENGA_CHEM_LOAD(PATH, CHEM)
      +      BIND(C, NAME='senga_chem_load')
@@ -183,6 +190,12 @@ C     RXLPRM(1), RXRPRM(1) of W2 walls; NRIETA: RXLPRC(1..6) of I4)
           IMPORT :: C_INT, C_PTR, SENGA_NSCBC
           TYPE(C_PTR), VALUE :: CTX
           TYPE(SENGA_NSCBC) :: BC
+        END FUNCTION
+        INTEGER(C_INT) FUNCTION SENGA_SET_SYNTHETIC_INFLOW(CTX, P)
+     +      BIND(C, NAME='senga_set_synthetic_inflow')
+          IMPORT :: C_INT, C_PTR, SENGA_SYNTH_INFLOW
+          TYPE(C_PTR), VALUE :: CTX
+          TYPE(SENGA_SYNTH_INFLOW) :: P
         END FUNCTION
         INTEGER(C_INT) FUNCTION SENGA_SET_TRANSPORT(CTX, MIXW, MIXP,
      +      SORET, DUFOUR, WMLTDR) BIND(C, NAME='senga_set_transport')

@@ -105,6 +105,13 @@ class ConfigT(C.Structure):
     ]
 
 
+class SynthT(C.Structure):
+    """senga_synth_inflow: synthetic turbulent inflow velocity parameters."""
+
+    _fields_ = [("urms", C.c_double), ("coflow", C.c_double), ("lnx", C.c_int), ("lny", C.c_int),
+                ("lnz", C.c_int), ("nfy", C.c_int), ("nfz", C.c_int), ("itime", C.c_int)]
+
+
 class NscbcT(C.Structure):
     """senga_nscbc: x-face kinds (11 I1, 12 I2, 13 I3, 14 I4 inflow, 21 O1 outflow, 31 W1, 32 W2 wall)
     and parameters."""
@@ -158,6 +165,7 @@ def _load():
         "senga_filter": (ip, [vp, ip]),
         "senga_get_tstep": (ip, [vp, dp, dp, C.POINTER(C.c_int)]),
         "senga_set_nscbc": (ip, [vp, C.POINTER(NscbcT)]),
+        "senga_set_synthetic_inflow": (ip, [vp, C.POINTER(SynthT)]),
         "senga_radn_load": (ip, [C.c_char_p, C.POINTER(ChemT), C.c_double, C.POINTER(RadnT)]),
         "senga_set_radiation": (ip, [vp, C.POINTER(RadnT)]),
         "senga_set_transport": (ip, [vp, ip, ip, ip, ip, C.c_double]),
@@ -600,6 +608,13 @@ class Box:
         no-slip wall, 32 W2 isothermal no-slip wall (t_wall: x-left, x-right
         temperatures)."""
         _check(lib.senga_set_nscbc(self.h, C.byref(nscbc_struct(bc))), "senga_set_nscbc")
+
+    def set_synthetic_inflow(self, urms, coflow=0.0, lnx=30, lny=30, lnz=30, nfy=60, nfz=60, itime=1):
+        """Synthetic turbulent inflow velocity on the I3 x-left face (the
+        reference's digital filter, BCUTXL NXLPRM(1) = 4); itime: the step
+        number of the next step."""
+        p = SynthT(float(urms), float(coflow), int(lnx), int(lny), int(lnz), int(nfy), int(nfz), int(itime))
+        _check(lib.senga_set_synthetic_inflow(self.h, C.byref(p)), "senga_set_synthetic_inflow")
 
     def set_transport(self, mixw=False, mixp=False, soret=False, dufour=False, wmltdr=5.0):
         """cont.dat transport switches: molar-mass and pressure diffusion,

@@ -22,7 +22,7 @@ DRV = os.path.join(ROOT, "senga-versiona_b200", "fortran", "senga_gpu_drv.f")
 HDR = os.path.join(ROOT, "include", "senga_gpu.h")
 
 STRUCTS = {"senga_chem": "SENGA_CHEM", "senga_diff": "SENGA_DIFF", "senga_config": "SENGA_CONFIG",
-           "senga_radn": "SENGA_RADN", "senga_nscbc": "SENGA_NSCBC"}
+           "senga_radn": "SENGA_RADN", "senga_nscbc": "SENGA_NSCBC", "senga_synth_inflow": "SENGA_SYNTH_INFLOW"}
 
 
 def _header():
@@ -135,7 +135,7 @@ def test_bind_c_layout_equals_the_ctypes_mirror(cname):
     import senga
 
     mirror = {"senga_chem": senga.ChemT, "senga_diff": senga.DiffT, "senga_config": senga.ConfigT,
-              "senga_nscbc": senga.NscbcT, "senga_radn": senga.RadnT}[cname]
+              "senga_nscbc": senga.NscbcT, "senga_radn": senga.RadnT, "senga_synth_inflow": senga.SynthT}[cname]
     _, types, _, _ = _module()
     assert _c_size(types[STRUCTS[cname]]) == C.sizeof(mirror)
 
