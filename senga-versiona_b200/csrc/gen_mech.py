@@ -330,6 +330,18 @@ def gen(tag, c, d):
         w("    lam = 0.5 * (c1 + 1.0 / c2);")
         w("    const double wmix = rho * c3;")
         w(f"    const double povr = p / {h(d['pdifgb'])};")
+        # Wilke viscosity before the mixture diffusivities, so that the nine
+        # rho D_k are formed last and stored right after: the square roots
+        # and the diffusivity sums are never live together (fewer registers);
+        # mu_k is taken as sqrt(mu_k)^2 (within an ulp of mu_k)
+        for s in range(ns):
+            w(f"    const double sq{s} = sqrt(exp({poly_expr(d['viscco'][s], 'lt')})); const double rq{s} = 1.0 / sq{s};")
+        w("    mu = 0.0;")
+        for s in range(ns):
+            w("    { double cc = 0.0, fw;")
+            for t in range(ns):
+                w(f"      fw = 1.0 + sq{s} * rq{t} * {h(d['wilko2'][s][t])}; fw = {h(d['wilko1'][s][t])} * fw * fw; cc = cc + y[{t}] * {h(c['ovwmol'][t])} * fw;")
+            w(f"      mu = mu + y[{s}] * {h(c['ovwmol'][s])} * ((sq{s} * sq{s}) / cc); }}")
         w("    double sumy = 0.0;")
         for s in range(ns):
             w(f"    sumy += y[{s}] + {h(DFCTOL)};")
@@ -342,14 +354,6 @@ def gen(tag, c, d):
                 w(f"      den{t} += (y[{s}] + {h(DFCTOL)}) * {h(c['ovwmol'][s])} * inv; }}")
         for s in range(ns):
             w(f"    rd[{s}] = rho * (sumy - (y[{s}] + {h(DFCTOL)})) / (den{s} * wmix);")
-        for s in range(ns):
-            w(f"    const double mk{s} = exp({poly_expr(d['viscco'][s], 'lt')}); const double sq{s} = sqrt(mk{s}); const double rq{s} = 1.0 / sq{s};")
-        w("    mu = 0.0;")
-        for s in range(ns):
-            w("    { double cc = 0.0, fw;")
-            for t in range(ns):
-                w(f"      fw = 1.0 + sq{s} * rq{t} * {h(d['wilko2'][s][t])}; fw = {h(d['wilko1'][s][t])} * fw * fw; cc = cc + y[{t}] * {h(c['ovwmol'][t])} * fw;")
-            w(f"      mu = mu + y[{s}] * {h(c['ovwmol'][s])} * (mk{s} / cc); }}")
     else:
         w("    (void)T; (void)p; (void)rho; (void)ry; (void)y; lam = 0.0; mu = 0.0;")
         w("    for (int s = 0; s < NS; ++s) rd[s] = 0.0;")

@@ -54,8 +54,16 @@ __global__ void __launch_bounds__(kBlock, ThermoOcc<M>::blocks) k_thermo(Geo g, 
 #ifndef SENGA_THERMO_P2_MINB
 #define SENGA_THERMO_P2_MINB 3
 #endif
+#ifndef SENGA_THERMO_P1_BLOCK
+#define SENGA_THERMO_P1_BLOCK kBlock
+#endif
+#ifndef SENGA_THERMO_P2_BLOCK
+#define SENGA_THERMO_P2_BLOCK kBlock
+#endif
+template <int PART>
+constexpr int kPartBlock = PART == 1 ? SENGA_THERMO_P1_BLOCK : SENGA_THERMO_P2_BLOCK;
 template <class M, int PART>
-__global__ void __launch_bounds__(kBlock, PART == 1 ? SENGA_THERMO_P1_MINB : SENGA_THERMO_P2_MINB)
+__global__ void __launch_bounds__(kPartBlock<PART>, PART == 1 ? SENGA_THERMO_P1_MINB : SENGA_THERMO_P2_MINB)
     k_thermo_part(Geo g, Fields f, M m) {
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= g.n) return;
@@ -154,8 +162,10 @@ int launch_thermo(const Geo& g, const Fields& f, const senga_chem* dchem, const 
   if (mech == 1) {
     k_thermo<<<gr, kBlock, 0, s>>>(g, f, gen::Mech_onestep{});
   } else if (mech == 2) {
-    k_thermo_part<gen::Mech_h2, 1><<<gr, kBlock, 0, s>>>(g, f, gen::Mech_h2{});
-    k_thermo_part<gen::Mech_h2, 2><<<gr, kBlock, 0, s>>>(g, f, gen::Mech_h2{});
+    k_thermo_part<gen::Mech_h2, 1>
+        <<<(unsigned)((g.n + kPartBlock<1> - 1) / kPartBlock<1>), kPartBlock<1>, 0, s>>>(g, f, gen::Mech_h2{});
+    k_thermo_part<gen::Mech_h2, 2>
+        <<<(unsigned)((g.n + kPartBlock<2> - 1) / kPartBlock<2>), kPartBlock<2>, 0, s>>>(g, f, gen::Mech_h2{});
     return 2;
   } else if (nspec <= 2) {
     if (flmavt) k_thermo<<<gr, kBlock, 0, s>>>(g, f, MechTables<2, true>{dchem, ddiff, nspec});

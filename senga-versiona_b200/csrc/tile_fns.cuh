@@ -28,12 +28,21 @@ namespace {
 
 using namespace tile;
 
+// Tile shapes (x fastest; every library file is compiled with the same
+// shapes, the launchers and work lists take them from here)
+#ifndef SENGA_TILE_X
+#define SENGA_TILE_X 32
+#endif
+#ifndef SENGA_TILE_Y
+#define SENGA_TILE_Y 8
+#endif
 // flow tile
-constexpr int FX = 32, FY = 8, FZ = 2;
+constexpr int FX = SENGA_TILE_X, FY = SENGA_TILE_Y, FZ = 2;
 constexpr int FNW = FX * FY / 32;
 // species tiles
-constexpr int SX_ = 32, SY_ = 8, SZ_ = 2;
+constexpr int SX_ = SENGA_TILE_X, SY_ = SENGA_TILE_Y, SZ_ = 2;
 constexpr int SNW = SX_ * SY_ / 32;
+static_assert(FX * FY == 256 && SX_ * SY_ == 256, "the stencil kernels run 256 threads per tile");
 
 using FStar = Star<FX, FY, FZ>;
 using FBox = Box<FX, FY, FZ>;
