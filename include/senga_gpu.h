@@ -326,9 +326,12 @@ int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
  *   rates (src/rhscal.f:1698-1760); after each RK update every wall mass
  *   fraction is the clipped zero-gradient extrapolation of the updated
  *   state (src/lincom.f:171-210, src/fincom.f:171-210). Conduction and
- *   diffusion are zeroed on the plane (FxxCON, FxxDIF, FxxADB). The wall
- *   runs with the base transport: with senga_set_transport switches on,
- *   either call returns SENGA_ERR_UNSUPPORTED.
+ *   diffusion are zeroed on the plane (FxxCON, FxxDIF, FxxADB). With the
+ *   senga_set_transport switches on, the molar-mass, pressure and Soret
+ *   branches add their own wall terms to the wall's species rates
+ *   (src/rhscal.f:2116-2175, 2512-2571, 2925-2984); their energy parts and
+ *   the Dufour wall terms reach only the wall's energy right-hand side,
+ *   which is zero.
  * 32: W2 isothermal no-slip wall (NSBCW2), on either or both faces: the
  *   wall temperature t_wall[side] is imposed with zero momentum and rho E
  *   the internal energy at it, on the U register by BOUNDT and on both
@@ -337,7 +340,8 @@ int senga_set_radiation(senga_ctx* ctx, const senga_radn* radn);
  *   wall (ranges src/bcinit.f:822-855); the density and species take the
  *   reflected wave as for W1 (src/bounds.f:1058-1190, 1975-), the wall
  *   diffusion flux and the zero-gradient mass fractions as for W1; only
- *   diffusion is zeroed on the plane (FxxDIF). Base transport only.
+ *   diffusion is zeroed on the plane (FxxDIF). The transport switches add
+ *   their wall terms as for W1.
  * Face data and wave amplitudes are computed after the thermochemistry
  * kernel and added to the face planes' right-hand side in the RK epilogue.
  * rho_in must be > 0 with an I3 face, p_inf > 0 with an O1 face, t_wall > 0

@@ -605,9 +605,8 @@ struct Oracle {
   // 290-428, 767-; wave amplitudes bounds.f:917-1056, 1833-1974; the wall
   // flux terms FxxCNW rhscal.f:610-660 and FxxDFW rhscal.f:1698-1760; the
   // zero-gradient mass fractions of lincom.f:171-210, fincom.f:171-210), on
-  // either or both x faces, with the base transport (the molar-mass,
-  // pressure and thermal-diffusion branches carry wall terms of their own
-  // that are not restated). And W2, the isothermal no-slip wall (NSBCW2;
+  // either or both x faces, with every transport switch (the molar-mass,
+  // pressure and Soret branches' wall terms in wall_branch). And W2, the isothermal no-slip wall (NSBCW2;
   // bcinit.f:822-855, boundt.f:358-470 and its x-right block, bountt.f:
   // 429-560 and its x-right block, bounds.f:1058-1190, 1975-): the wall
   // temperature RXxPRM(1) imposed, FxxDIF and FxxDFW only, neither momentum
@@ -672,8 +671,6 @@ struct Oracle {
     if (xr == BC_I4) throw std::runtime_error("oracle: I4 is coded for the x-left face only (bounds.f:686)");
     if (xl == BC_I4 && !(t_in > 0.0)) throw std::runtime_error("oracle: an I4 inflow needs its target temperature");
     for (int k = 0; k < 6; ++k) nrieta[k] = nri ? nri[k] : 0.0;
-    if ((is_wall(xl) || is_wall(xr)) && (df.flmixw || df.flmixp || df.flmixt))
-      throw std::runtime_error("oracle: W1/W2 walls restated for the base transport only");
     if ((xl == BC_W2 && !(t_wall_l > 0.0)) || (xr == BC_W2 && !(t_wall_r > 0.0)))
       throw std::runtime_error("oracle: a W2 wall needs its temperature > 0");
     twall[0] = t_wall_l;
@@ -1926,7 +1923,29 @@ struct Oracle {
                  store6(ic, jc, kc) * g1z(ic, jc, kc);
       erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * store7(ic, jc, kc);
     }
+    wall_branch(rt, g1x, utmp, nullptr, 0.0);
     second_derivative_terms(rt, g2x, g2y, g2z);
+  }
+  // rhscal.f:2116-2175 (molar mass), 2512-2571 (pressure), 2925-2984
+  // (Soret): at a W1/W2 wall (FxxDFW) the one-sided derivative at the wall
+  // of the branch's driving diffusivity STORE7 times its x gradient, added
+  // to the rate, VTMP and, times UTMP (the Soret block: UTMP + R_k T
+  // TDRMIX_k), the energy of the wall plane. The Dufour branch's wall terms
+  // (rhscal.f:3106-3160 FxxCNW, 3402-3500 FxxADW) reach only the energy RHS
+  // of the wall plane, which BOUNDS sets to zero at either wall, and are not
+  // restated.
+  void wall_branch(Field& rt, Field& g1x, Field& ut, Field* tdr, double rg) {
+    for (int kc = kstal; kc <= kstol; ++kc)
+      for (int jc = jstal; jc <= jstol; ++jc)
+        for (int side = 0; side < 2; ++side) {
+          if (!(side == 0 ? fxldfw : fxrdfw)) continue;
+          const int ic = side == 0 ? istal : istol;
+          const double fornow = wall_deriv(store7, g1x, ic, side == 0 ? 1 : -1, jc, kc);
+          rt(ic, jc, kc) = rt(ic, jc, kc) + fornow;
+          vtmp(ic, jc, kc) = vtmp(ic, jc, kc) + fornow;
+          const double h = tdr ? ut(ic, jc, kc) + rg * trun(ic, jc, kc) * (*tdr)(ic, jc, kc) : ut(ic, jc, kc);
+          erhs(ic, jc, kc) = erhs(ic, jc, kc) + fornow * h;
+        }
   }
   // the second-derivative part of each branch; the zeroing acts on the
   // stored second derivatives themselves, as in the reference
@@ -1948,8 +1967,6 @@ struct Oracle {
   // Dufour, molar-mass limit): src/diffin.f:384-406, WMLTOL 1e-3 (:34).
   void set_transport(bool mixw, bool mixp, bool soret, bool dufour, double wmltdr) {
     if (!df.flmavt) throw std::runtime_error("transport switches need mixture-averaged transport");
-    if ((is_wall(bcxl) || is_wall(bcxr)) && (mixw || mixp || soret || dufour))
-      throw std::runtime_error("oracle: W1/W2 walls restated for the base transport only");
     df.flmixw = mixw;
     df.flmixp = mixp;
     df.flmixt = false;
@@ -2241,6 +2258,7 @@ struct Oracle {
                      store6(ic, jc, kc) * td1z(ic, jc, kc);
           erhs(ic, jc, kc) = erhs(ic, jc, kc) + f * store7(ic, jc, kc);
         }
+        wall_branch(rt, td1x, utmp, &tdrmix, ch.rgspec[is - 1]);
         second_derivative_terms(rt, td2x, td2y, td2z);
       }
     }

@@ -690,8 +690,6 @@ int senga_set_transport(senga_ctx* c, int mixw, int mixp, int soret, int dufour,
   return guard([&] {
     if ((mixw || mixp || soret || dufour) && !c->diff.flmavt)
       throw Error(SENGA_ERR_ARG, "senga_set_transport: the switches need mixture-averaged transport (diff.dat)");
-    if ((mixw || mixp || soret || dufour) && c->nscbc && has_wall(c->bc))
-      throw Error(SENGA_ERR_UNSUPPORTED, "senga_set_transport: a W1/W2 wall runs with the base transport only");
     CK(cudaStreamSynchronize(c->stream));
     cudaFree(c->mixt_pool);
     c->mixt_pool = nullptr;
@@ -780,11 +778,6 @@ int senga_set_nscbc(senga_ctx* c, const senga_nscbc* b) {
   if (either(21) && b->p_inf <= 0.0) return fail(SENGA_ERR_ARG, "senga_set_nscbc: an O1 outflow needs p_inf > 0");
   if ((b->xl == 32 && !(b->t_wall[0] > 0.0)) || (b->xr == 32 && !(b->t_wall[1] > 0.0)))
     return fail(SENGA_ERR_ARG, "senga_set_nscbc: a W2 wall needs its t_wall > 0");
-  // the molar-mass, pressure and thermal-diffusion branches carry wall flux
-  // terms of their own (rhscal.f:2116-, 2512-, 2925-, 3111-) not built here
-  if ((either(31) || either(32)) && c->mixt)
-    return fail(SENGA_ERR_UNSUPPORTED, "senga_set_nscbc: a W1/W2 wall runs with the base transport only "
-                                       "(senga_set_transport switches off)");
   return guard([&] {
     NscbcParams& p = c->bc;
     p = NscbcParams{};

@@ -247,13 +247,55 @@ __global__ void __launch_bounds__(MX* MY, 2) k_mixt_species(Geo g, Fields f, Mix
   }
 }
 
+// Wall terms of the molar-mass, pressure and Soret branches at a W1/W2 wall
+// (FxxDFW: src/rhscal.f:2116-2175, 2512-2571, 2925-2984): the one-sided
+// fourth-order x derivative at the wall of the branch's driving diffusivity
+// times its x gradient (ln W_mix, ln p or ln(T/TDIFGB), first derivatives
+// with the bounded closures), over the wall and the four planes inward,
+// added to the species rate and to VTMP of the wall point. Their energy
+// parts, and the Dufour branch's wall terms (rhscal.f:3106-3160,
+// 3402-3500), reach only the wall's energy RHS, which BOUNDS sets to zero
+// at either wall kind, and are left out. One thread per wall point;
+// blockIdx.y = side.
 template <int BR>
-void launch_branch(const Geo& g, const Fields& f, const MixtParams& m, const senga_chem* dchem, int nspec,
-                   cudaStream_t s) {
+__global__ void __launch_bounds__(kMixBlock) k_mixt_wall(Geo g, Fields f, MixtParams m,
+                                                         const senga_chem* __restrict__ ch, int nspec) {
+  const int jk = blockIdx.x * kMixBlock + threadIdx.x;
+  const int side = blockIdx.y;
+  if (jk >= g.ny * g.nz || !((side == 0 ? g.bxl : g.bxr) & BF_WALL)) return;
+  const int i = side == 0 ? 0 : g.nx - 1, st = side == 0 ? 1 : -1;
+  const int64_t n = g.n, q = (int64_t)i + (int64_t)g.nx * jk;
+  const double* __restrict__ gx = m.g1[BR == kBrW ? 0 : BR == kBrP ? 1 : 2];  // x components
+  const double c0 = (double)(25.0f / 12.0f), c3 = (double)(4.0f / 3.0f);  // single-precision literals as coded
+  double vt = f.vtmp[q];
+  for (int k = 0; k < nspec; ++k) {
+    if (BR == kBrT && !((m.sor >> k) & 1u)) continue;
+    const DrivingF<BR> drv{f.rd + k * n, f.y + k * n, BR == kBrP ? m.wmix : (BR == kBrT ? m.tdrmix + k * n : nullptr),
+                           ch->wmolar[k]};
+    double fv[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) fv[c] = drv(q + c * st) * gx[q + c * st];
+    const double w = side == 0 ? ((-c0) * fv[0] + 4.0 * fv[1] - 3.0 * fv[2] + c3 * fv[3] - 0.25 * fv[4]) * g.ovd[0]
+                               : (c0 * fv[0] - 4.0 * fv[1] + 3.0 * fv[2] - c3 * fv[3] + 0.25 * fv[4]) * g.ovd[0];
+    f.wdot[k * n + q] = f.wdot[k * n + q] + w;
+    vt = vt + w;
+  }
+  f.vtmp[q] = vt;
+}
+
+// launches the branch's tile kernel and, with a wall, its wall terms;
+// returns the number of launches
+template <int BR>
+int launch_branch(const Geo& g, const Fields& f, const MixtParams& m, const senga_chem* dchem, int nspec,
+                  cudaStream_t s) {
   const dim3 grid((unsigned)((g.nx + MX - 1) / MX), (unsigned)((g.ny + MY - 1) / MY), (unsigned)((g.nz + MZ - 1) / MZ));
   const bool per = g.per[0] && g.per[1] && g.per[2];
   if (per) k_mixt_species<BR, true><<<grid, MX * MY, kMixSmem * 8, s>>>(g, f, m, dchem, nspec);
   else k_mixt_species<BR, false><<<grid, MX * MY, kMixSmem * 8, s>>>(g, f, m, dchem, nspec);
+  if (BR == kBrDufour || !((g.bxl | g.bxr) & BF_WALL)) return 1;
+  k_mixt_wall<BR == kBrDufour ? kBrW : BR>
+      <<<dim3((unsigned)((g.ny * g.nz + kMixBlock - 1) / kMixBlock), 2), kMixBlock, 0, s>>>(g, f, m, dchem, nspec);
+  return 2;
 }
 
 inline unsigned grid_of(int64_t n) { return (unsigned)((n + kMixBlock - 1) / kMixBlock); }
@@ -269,10 +311,10 @@ int launch_mixt(const Geo& g, const Fields& f, const MixtParams& m, const senga_
     k_mixt_grad<<<gr, kMixBlock, 0, s>>>(g, m);
     ++nl;
   }
-  if (m.duf) launch_branch<kBrDufour>(g, f, m, dchem, nspec, s), ++nl;
-  if (m.w) launch_branch<kBrW>(g, f, m, dchem, nspec, s), ++nl;
-  if (m.p) launch_branch<kBrP>(g, f, m, dchem, nspec, s), ++nl;
-  if (m.sor) launch_branch<kBrT>(g, f, m, dchem, nspec, s), ++nl;
+  if (m.duf) nl += launch_branch<kBrDufour>(g, f, m, dchem, nspec, s);
+  if (m.w) nl += launch_branch<kBrW>(g, f, m, dchem, nspec, s);
+  if (m.p) nl += launch_branch<kBrP>(g, f, m, dchem, nspec, s);
+  if (m.sor) nl += launch_branch<kBrT>(g, f, m, dchem, nspec, s);
   return nl;
 }
 

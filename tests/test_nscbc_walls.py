@@ -17,11 +17,14 @@ planes the momentum stays zero, the temperature is the fourth-order
 zero-gradient extrapolation of the four planes inward (W1) or the imposed
 one (W2), every mass fraction the clipped extrapolation of the updated
 state, and the energy the internal energy at that temperature, while the
-density is integrated. The molar-mass, pressure and thermal-diffusion
-branches have wall terms of their own that are not restated, so both sides
-refuse them with a wall. GPU: two walls of either kind, a W1 and a W2 wall,
-and a wall with an O1 outflow opposite, against the oracle (RHS and three
-RK steps, field-normalised relative L-infinity 1e-10)."""
+density is integrated. With the transport switches on, the molar-mass,
+pressure and Soret branches add their own wall terms (rhscal.f:2116-2175,
+2512-2571, 2925-2984): the mirror symmetry still holds, and so does
+sum_k YRHS_k = DRHS on every plane, since each wall term enters a species
+rate and VTMP alike. GPU: two walls of either kind, a W1 and a W2 wall, and
+a wall with an O1 outflow opposite, with the base transport and with the
+switches, against the oracle (RHS and three RK steps, field-normalised
+relative L-infinity 1e-10)."""
 import numpy as np
 import pytest
 
@@ -121,20 +124,37 @@ def test_wall_planes_after_steps(kind):
         assert rel_linf(f[4][..., w], e) <= 1e-13
 
 
-def test_walls_refuse_the_transport_branches_without_restated_wall_terms():
+ALL = dict(mixw=True, mixp=True, soret=True, dufour=True)
+SWITCHES = [("mixw", dict(mixw=True)), ("mixp", dict(mixp=True)), ("soret", dict(soret=True)), ("all", ALL)]
+
+
+def _oracle_sw(c, bc, sw):
     from oracle import Oracle
 
-    c, bc = _case()
     o = Oracle(c["shape"], c["lengths"], c["chem"], c["diff"], c["dt"], nend=c["nend"])
     o.set_bc(bc)
-    with pytest.raises(RuntimeError, match="W1"):
-        o.set_transport(mixw=True)
-    o2 = Oracle(c["shape"], c["lengths"], c["chem"], c["diff"], c["dt"], nend=c["nend"])
-    o2.set_transport(soret=True)
-    with pytest.raises(RuntimeError, match="W1"):
-        o2.set_bc(bc)
-    with pytest.raises(RuntimeError, match="W2"):
-        o2.set_bc(dict(bc, xl=32, xr=32))
+    o.set_transport(**sw)
+    o.upload(c["fields"], c["T"], c["itn"])
+    return o
+
+
+OCASES = [(31, "mixw", dict(mixw=True)), (31, "mixp", dict(mixp=True)), (31, "soret", dict(soret=True)),
+          (32, "all", ALL)]
+
+
+@pytest.mark.parametrize("kind,name,sw", OCASES, ids=[f"W{k - 30}-{n}" for k, n, _ in OCASES])
+def test_wall_branch_terms_mirror_and_species_sum_in_the_oracle(kind, name, sw):
+    c, bc = _case(kind=kind)
+    cm, bcm = _mirrored(c, bc)
+    ra, _, _ = _oracle_sw(c, bc, sw).rhs()
+    rb, _, _ = _oracle_sw(cm, bcm, sw).rhs()
+    for fl in range(ra.shape[0]):
+        assert rel_linf(rb[fl], _mirror(ra)[fl]) <= 1e-12, fl
+    # every wall term enters one species rate and VTMP alike
+    assert rel_linf(ra[5:].sum(axis=0), ra[0]) <= 1e-10
+    # the switches change the wall plane's species right-hand side
+    r0, _, _ = _oracle(c, bc).rhs()
+    assert rel_linf(ra[5:, ..., 0], r0[5:, ..., 0]) > 1e-8
 
 
 O1 = dict(p_inf=101325.0, sigma=0.287, eta=1.0e-3)
@@ -178,8 +198,7 @@ def test_gpu_walls_match_oracle(name, faces, mirrored):
 
 @pytest.mark.gpu
 def test_gpu_wall_refusals():
-    """A W2 face without its temperature, and a wall together with the
-    transport switches (in either order), are refused by the library."""
+    """A W2 face without its temperature is refused by the library."""
     import senga
 
     c, bc = _case(shape=(16, 8, 6), kind=32)
@@ -189,9 +208,42 @@ def test_gpu_wall_refusals():
     with pytest.raises(RuntimeError, match="t_wall"):
         box.set_nscbc(dict(bc, t_wall=(0.0, 800.0)))
     box.set_nscbc(bc)
-    with pytest.raises(RuntimeError, match="base transport"):
-        box.set_transport(mixw=True)
-    box2 = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"], nend=c["nend"])
-    box2.set_transport(soret=True)
-    with pytest.raises(RuntimeError, match="base transport"):
-        box2.set_nscbc(dict(bc, xl=31, xr=31))
+    box.set_transport(mixw=True)  # walls run with the transport switches too
+
+
+WCASES = [("W1-W1", dict(xl=31, xr=31)), ("W2-O1", dict(xl=32, xr=21, **O1))]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,faces", WCASES, ids=[n for n, _ in WCASES])
+@pytest.mark.parametrize("sname,sw", SWITCHES, ids=[n for n, _ in SWITCHES])
+@pytest.mark.parametrize("mirrored", [False, True], ids=["as-is", "mirrored"])
+def test_gpu_walls_with_transport_switches_match_oracle(name, faces, sname, sw, mirrored):
+    import senga
+
+    c, bc = _case(shape=(24, 10, 8), seed=9)
+    bc = dict(bc, **faces)
+    if mirrored:
+        c, bc = _mirrored(c, bc)
+    chem = senga.Chem(c["chem"])
+    diff = senga.Diff(c["diff"], chem)
+    box = senga.Box(c["shape"], c["lengths"], chem, diff, c["dt"], nend=c["nend"])
+    box.set_nscbc(bc)
+    box.set_transport(**sw)
+    box.upload(c["fields"], c["T"], c["itn"])
+    r, t, _ = box.rhs()
+    rr, tr, _ = _oracle_sw(c, bc, sw).rhs()
+    assert rel_linf(t, tr) <= TOL
+    for fl in range(rr.shape[0]):
+        assert rel_linf(r[fl], rr[fl]) <= TOL, f"RHS field {fl}"
+    box.upload(c["fields"], c["T"], c["itn"])
+    ref = _oracle_sw(c, bc, sw)
+    box.step(3)
+    ref.step(3)
+    g, tg, ig = box.download()
+    o, to, io = ref.download()
+    assert box.status() == 0
+    for fl in range(o.shape[0]):
+        assert rel_linf(g[fl], o[fl]) <= TOL, f"state field {fl}"
+    assert rel_linf(tg, to) <= TOL
+    assert np.array_equal(ig, io)
