@@ -164,6 +164,17 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
   {
     const FStar bPr{sm};
     const double p111 = ldf<NC>(f.p + zd.base[0]);  // p(1,1,1) lives in slab 0
+    // the point's velocity, loaded before the staging wait so that its
+    // latency overlaps the copies
+    double pu[FZ], pv[FZ], pw[FZ];
+    auto point_vel = [&] {
+#pragma unroll
+      for (int z = 0; z < FZ; ++z) {
+        pu[z] = ldf<NC>(f.vel + tp[z].q);
+        pv[z] = ldf<NC>(f.vel + n + tp[z].q);
+        pw[z] = ldf<NC>(f.vel + 2 * n + tp[z].q);
+      }
+    };
     auto phase3 = [&](const auto& bP) {
 #pragma unroll
       for (int z = 0; z < FZ; ++z) {
@@ -172,17 +183,19 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
         rU[z] = -px;
         rV[z] = -py;
         rW[z] = -pz;
-        rE[z] = rE[z] - ldf<NC>(f.vel + t.q) * px - ldf<NC>(f.vel + n + t.q) * py - ldf<NC>(f.vel + 2 * n + t.q) * pz;
+        rE[z] = rE[z] - pu[z] * px - pv[z] * py - pw[z] * pz;
       }
     };
     if constexpr (B) {
       // raw p by bulk copies, p(1,1,1) subtracted where read: the same
       // subtraction as staging p - p(1,1,1), so the same values
       bPr.stage_bulk(fo, o.x0, g.nx, f.p, bar);
+      point_vel();
       if (bb.wait(FStar::kBulkBytes, f.status)) return;
       phase3(Shifted<FStar>{bPr, p111});
     } else {
       bPr.stage<FNW>(fo, LdSubT<NC>{f.p, p111});
+      point_vel();
       tile_sync();
       phase3(bPr);
     }
@@ -233,6 +246,14 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
   double mux[FZ], muy[FZ], muz[FZ], ux[FZ], uy[FZ], uz[FZ], vx[FZ], vy[FZ], vz[FZ];
   // 5a: u
   stage_plain<B, FNW, NC>(bX, fo, g, o, f.vel, bar);
+  // point values of 5a, loaded before the staging wait
+  double qa[FZ], qb[FZ], qc[FZ];
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) {
+    qa[z] = ldf<NC>(f.vel + n + tp[z].q);
+    qb[z] = ldf<NC>(f.vel + 2 * n + tp[z].q);
+    qc[z] = ldf<NC>(U + n + tp[z].q);
+  }
   if (sync_staged<B>(bb, FStar::kBulkBytes + FBox::kBulkBytes, f.status)) return;
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
@@ -245,11 +266,11 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     uy[z] = d1<1, P>(g, t, bX);
     uz[z] = d1<2, P>(g, t, bX);
     const double uq = bX.v(t.x, t.y, t.z);
-    const double vq = ldf<NC>(f.vel + n + t.q), wq = ldf<NC>(f.vel + 2 * n + t.q);
+    const double vq = qa[z], wq = qb[z];
     // x-face viscous flags (rhsvel.f: FxxVSN normal, FxxVST shear terms zeroed on the plane)
     const int bf = P ? 0 : face_bits(g, t.gx);
     const double vsn = (bf & BF_VSN) ? 0.0 : 1.0, vst = (bf & BF_VST) ? 0.0 : 1.0;
-    rU[z] = rU[z] + -0.5 * (ldf<NC>(U + n + t.q) * ux[z] + (S4[z] + uq * divm[z]));
+    rU[z] = rU[z] + -0.5 * (qc[z] * ux[z] + (S4[z] + uq * divm[z]));
     double fn = vsn * (mu * kFthd * d2<0, P>(g, t, bX));
     rU[z] += fn;
     rE[z] = rE[z] + fn * uq;
@@ -276,6 +297,12 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
   tile_sync();
   // 5b: v
   stage_plain<B, FNW, NC>(bX, fo, g, o, f.vel + n, bar);
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) {
+    qa[z] = ldf<NC>(f.vel + tp[z].q);
+    qb[z] = ldf<NC>(f.vel + 2 * n + tp[z].q);
+    qc[z] = ldf<NC>(U + 2 * n + tp[z].q);
+  }
   if (sync_staged<B>(bb, FBox::kBulkBytes, f.status)) return;
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
@@ -285,10 +312,10 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     vy[z] = d1<1, P>(g, t, bX);
     vz[z] = d1<2, P>(g, t, bX);
     const double vq = bX.v(t.x, t.y, t.z);
-    const double uq = ldf<NC>(f.vel + t.q), wq = ldf<NC>(f.vel + 2 * n + t.q);
+    const double uq = qa[z], wq = qb[z];
     const int bf = P ? 0 : face_bits(g, t.gx);
     const double vsn = (bf & BF_VSN) ? 0.0 : 1.0, vst = (bf & BF_VST) ? 0.0 : 1.0;
-    rV[z] = rV[z] + -0.5 * (ldf<NC>(U + 2 * n + t.q) * vy[z] + (S5[z] + vq * divm[z]));
+    rV[z] = rV[z] + -0.5 * (qc[z] * vy[z] + (S5[z] + vq * divm[z]));
     double fn = mu * kFthd * d2<1, P>(g, t, bX);
     rV[z] += fn;
     rE[z] = rE[z] + fn * vq;
@@ -315,6 +342,14 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
   tile_sync();
   // 5c: w, then the first-derivative products
   stage_plain<B, FNW, NC>(bX, fo, g, o, f.vel + 2 * n, bar);
+  double qd[FZ];
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) {  // (an invalid point has q = 0: in bounds, unused)
+    qa[z] = ldf<NC>(f.vel + tp[z].q);
+    qb[z] = ldf<NC>(f.vel + n + tp[z].q);
+    qc[z] = ldf<NC>(U + tp[z].q);
+    qd[z] = ldf<NC>(U + 3 * n + tp[z].q);
+  }
   if (sync_staged<B>(bb, FBox::kBulkBytes, f.status)) return;
 #pragma unroll
   for (int z = 0; z < FZ; ++z) {
@@ -323,11 +358,11 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     const double mu = bM.v(t.x, t.y, t.z);
     const double wx = d1<0, P>(g, t, bX), wy = d1<1, P>(g, t, bX), wz = d1<2, P>(g, t, bX);
     const double wq = bX.v(t.x, t.y, t.z);
-    const double uq = ldf<NC>(f.vel + t.q), vq = ldf<NC>(f.vel + n + t.q);
-    const double rho = ldf<NC>(U + t.q);
+    const double uq = qa[z], vq = qb[z];
+    const double rho = qc[z];
     const int bf = P ? 0 : face_bits(g, t.gx);
     const double vsn = (bf & BF_VSN) ? 0.0 : 1.0, vst = (bf & BF_VST) ? 0.0 : 1.0;
-    rW[z] = rW[z] + -0.5 * (ldf<NC>(U + 3 * n + t.q) * wz + (S6[z] + wq * divm[z]));
+    rW[z] = rW[z] + -0.5 * (qd[z] * wz + (S6[z] + wq * divm[z]));
     double fn = mu * kFthd * d2<2, P>(g, t, bX);
     rW[z] += fn;
     rE[z] = rE[z] + fn * wq;
