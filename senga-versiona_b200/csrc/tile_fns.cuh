@@ -537,6 +537,11 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
     {
       SCol cy;
       cy.load(fo, tx, ty, LdT<NC>{f.y + s * n});
+      // the chemistry rate of the thread's points, loaded before the wait
+      // (an invalid point has q = 0: in bounds, unused)
+      double w0[SZ_];
+#pragma unroll
+      for (int z = 0; z < SZ_; ++z) w0[z] = f.wdot[s * n + tp[z].q];
       // Y_s has landed in bS; the rho D and h slabs are free
       if (sync_staged<B>(bb, inflight, f.status)) return;
       stage_f(bR, tm ? &tm->rd : nullptr, s, f.rd + s * n);
@@ -546,7 +551,7 @@ __device__ __forceinline__ void species_tile(const Geo& g, const Fields& f, int 
       for (int z = 0; z < SZ_; ++z) {
         const TP& t = tp[z];
         const double yq = cy.c[z + H];
-        double r = f.wdot[s * n + t.q];
+        double r = w0[z];
         r = r - 0.5 * yq * dvm[z];
         if constexpr (P) {
           // all periodic: each staged neighbour of Y, rho u, rho v read once
