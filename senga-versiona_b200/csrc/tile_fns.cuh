@@ -210,12 +210,25 @@ __device__ __forceinline__ void flow_tile(const Geo& g, const Fields& f, const O
     const FXRow xA{sm}, xB{sm + FXRow::SIZE}, xC{sm + 2 * FXRow::SIZE};
     double* const sy = sm + 3 * FXRow::SIZE;
     const FYRow yA{sy}, yB{sy + FYRow::SIZE}, yC{sy + 2 * FYRow::SIZE};
-    xA.stage<FNW>(fo, LdMulT<NC>{U + n, f.vel});               // rho u u
-    xB.stage<FNW>(fo, LdMulT<NC>{U + n, f.vel + n});           // rho u v
-    xC.stage<FNW>(fo, LdMulT<NC>{U + n, f.vel + 2 * n});       // rho u w
-    yA.stage<FNW>(fo, LdMulT<NC>{U + n, f.vel + n});           // rho u v
-    yB.stage<FNW>(fo, LdMulT<NC>{U + 2 * n, f.vel + n});       // rho v v
-    yC.stage<FNW>(fo, LdMulT<NC>{U + 2 * n, f.vel + 2 * n});   // rho v w
+    // the three x-row products share rho u, the three y-row ones v or rho v:
+    // one pass of loads fills each group of three buffers
+    const double* const pru = U + n;
+    const double* const prv = U + 2 * n;
+    const double* const pu = f.vel;
+    const double* const pv = f.vel + n;
+    const double* const pw = f.vel + 2 * n;
+    xA.stage3<FNW, 2>(xB, xC, fo, [=](int64_t q, double& a, double& b, double& c) {
+      const double m = ldf<NC>(pru + q);
+      a = m * ldf<NC>(pu + q);  // rho u u
+      b = m * ldf<NC>(pv + q);  // rho u v
+      c = m * ldf<NC>(pw + q);  // rho u w
+    });
+    yA.stage3<FNW, 3>(yB, yC, fo, [=](int64_t q, double& a, double& b, double& c) {
+      const double v = ldf<NC>(pv + q), m = ldf<NC>(prv + q);
+      a = ldf<NC>(pru + q) * v;  // rho u v
+      b = m * v;                 // rho v v
+      c = m * ldf<NC>(pw + q);   // rho v w
+    });
     Column<FZ> cw, cm;
     cw.load(fo, tx, ty, LdT<NC>{f.vel + 2 * n});
     cm.load(fo, tx, ty, LdT<NC>{U + n});

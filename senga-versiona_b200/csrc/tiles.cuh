@@ -267,6 +267,51 @@ __device__ __forceinline__ void stage_rows(double* dst, int DS, const FO& fo, co
   }
 }
 
+// As stage_rows (register path), for three buffers of the same layout filled
+// from one pass: f(q, v0, v1, v2) forms the three values of point q, so
+// products that share a factor load it once and every round of loads fills
+// three buffers.
+template <int XL, int XLO, int NR, int NW, int UB, class FO, class RowYZ, class F>
+__device__ __forceinline__ void stage_rows3(double* d0, double* d1, double* d2, int DS, const FO& fo,
+                                            const RowYZ& rowyz, const F& f) {
+  constexpr int NK = (XL + 31) / 32;
+  constexpr int ITER = (NR + NW - 1) / NW;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t gx[NK];
+#pragma unroll
+  for (int k = 0; k < NK; ++k) gx[k] = (lane + 32 * k < XL) ? fo.ox[XLO + H + lane + 32 * k] : 0;
+#pragma unroll 1
+  for (int i0 = 0; i0 < ITER; i0 += UB) {
+    double v[UB][NK][3];
+    int drow[UB];
+#pragma unroll
+    for (int u = 0; u < UB; ++u) {
+      const int r = warp + (i0 + u) * NW;
+      drow[u] = -1;
+      if (i0 + u < ITER && r < NR) {
+        int y, z;
+        rowyz(r, y, z, drow[u]);
+        const int64_t base = fo.oy[y + H] + fo.oz[z + H];
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (lane + 32 * k < XL) f(base + gx[k], v[u][k][0], v[u][k][1], v[u][k][2]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UB; ++u)
+      if (drow[u] >= 0) {
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (lane + 32 * k < XL) {
+            const int e = drow[u] * DS + lane + 32 * k;
+            d0[e] = v[u][k][0];
+            d1[e] = v[u][k][1];
+            d2[e] = v[u][k][2];
+          }
+      }
+  }
+}
+
 template <int TX, int TY, int TZ>
 struct Star {
   static constexpr int SX = TX + 2 * XH, SY = TY + 2 * H;
@@ -382,6 +427,17 @@ struct XRow {
                                             },
                                             f);
   }
+  // this buffer and b, c (same shape) from one pass of f (stage_rows3)
+  template <int NW, int UB, class F>
+  __device__ void stage3(const XRow& b, const XRow& c, const Folds<TX, TY, TZ>& fo, const F& f) const {
+    stage_rows3<TX + 2 * H, -H, TY * TZ, NW, UB>(p + (XH - H), b.p + (XH - H), c.p + (XH - H), SX, fo,
+                                                 [](int r, int& y, int& z, int& d) {
+                                                   y = r % TY;
+                                                   z = r / TY;
+                                                   d = r;
+                                                 },
+                                                 f);
+  }
   static constexpr unsigned kBulkBytes = 8u * (unsigned)SIZE;
   __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
     tile::stage_bulk<SX, -XH, TY * TZ>(p, SX, fo, x0, nx,
@@ -407,6 +463,17 @@ struct YRow {
                                      d = r;
                                    },
                                    f);
+  }
+  // this buffer and b, c (same shape) from one pass of f (stage_rows3)
+  template <int NW, int UB, class F>
+  __device__ void stage3(const YRow& b, const YRow& c, const Folds<TX, TY, TZ>& fo, const F& f) const {
+    stage_rows3<TX, 0, SY * TZ, NW, UB>(p, b.p, c.p, TX, fo,
+                                        [](int r, int& y, int& z, int& d) {
+                                          y = r % SY - H;
+                                          z = r / SY;
+                                          d = r;
+                                        },
+                                        f);
   }
   static constexpr unsigned kBulkBytes = 8u * (unsigned)SIZE;
   __device__ void stage_bulk(const Folds<TX, TY, TZ>& fo, int x0, int nx, const double* src, uint64_t* bar) const {
